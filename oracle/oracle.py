@@ -1,0 +1,311 @@
+"""ctypes wrapper over the C oracle (oracle/libmzk_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA product.  Only tests/,
+__graft_entry__.smoke() and bench.py's cpu_baseline / reference legs import
+this module.
+
+Arrays are numpy uint64 arrays in the reference's in-memory layouts:
+Fr elements shape (n, 4) Montgomery, G1 affine points shape (n, 12)
+(x limbs 0..5, y limbs 6..11, Montgomery, identity all-zero).
+"""
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libmzk_oracle.so"
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def _load():
+    if not LIB_PATH.exists():
+        build()
+    lib = ctypes.CDLL(str(LIB_PATH))
+    sz = ctypes.c_size_t
+    i32 = ctypes.c_int
+    u32 = ctypes.c_uint32
+    u64 = ctypes.c_uint64
+    sigs = {
+        "or_fr_mul": (None, [_u64p, _u64p, _u64p]),
+        "or_fr_add": (None, [_u64p, _u64p, _u64p]),
+        "or_fr_sub": (None, [_u64p, _u64p, _u64p]),
+        "or_fr_neg": (None, [_u64p, _u64p]),
+        "or_fr_inv": (None, [_u64p, _u64p]),
+        "or_fr_from_canonical": (None, [_u64p, _u64p]),
+        "or_fr_to_canonical": (None, [_u64p, _u64p]),
+        "or_fr_const": (None, [i32, _u64p]),
+        "or_fp_mul": (None, [_u64p, _u64p, _u64p]),
+        "or_fp_add": (None, [_u64p, _u64p, _u64p]),
+        "or_fp_sub": (None, [_u64p, _u64p, _u64p]),
+        "or_fp_inv": (None, [_u64p, _u64p]),
+        "or_fp_from_canonical": (None, [_u64p, _u64p]),
+        "or_fp_to_canonical": (None, [_u64p, _u64p]),
+        "or_fp_const": (None, [i32, _u64p]),
+        "or_g1_generator": (None, [_u64p]),
+        "or_g1_add": (None, [_u64p, _u64p, _u64p]),
+        "or_g1_double": (None, [_u64p, _u64p]),
+        "or_g1_to_affine": (None, [_u64p, _u64p]),
+        "or_g1_from_affine": (None, [_u64p, _u64p]),
+        "or_g1_is_on_curve_affine": (i32, [_u64p]),
+        "or_g1_mul": (None, [_u64p, _u64p, _u64p]),
+        "or_g1_compress": (None, [_u8p, _u64p]),
+        "or_msm_naive": (None, [_u64p, _u64p, _u64p, sz]),
+        "or_msm_best": (None, [_u64p, _u64p, _u64p, sz, i32]),
+        "or_msm_specific": (None, [_u64p, _u64p, _u64p, sz, i32]),
+        "or_booth_index": (i32, [sz, sz, _u8p]),
+        "or_fr_inner_product": (None, [_u64p, _u64p, _u64p, sz, i32]),
+        "or_rand64": (u64, [u64, u64]),
+        "or_rand_fr": (None, [_u64p, u64, u64, sz, i32]),
+        "or_gen_bases": (None, [_u64p, u64, u64, sz, i32]),
+        "or_compute_twiddles": (None, [_u64p, _u64p, u32]),
+        "or_best_fft": (None, [_u64p, _u64p, u32, i32]),
+        "or_fft_dif_pruned": (None, [_u64p, _u64p, u32, sz, i32]),
+        "or_dft_naive": (None, [_u64p, _u64p, _u64p, sz]),
+        "or_domain_new": (ctypes.c_void_p, [u32, u32]),
+        "or_domain_free": (None, [ctypes.c_void_p]),
+        "or_domain_k": (u32, [ctypes.c_void_p]),
+        "or_domain_extended_k": (u32, [ctypes.c_void_p]),
+        "or_domain_get": (None, [ctypes.c_void_p, i32, i32, _u64p]),
+        "or_domain_lagrange_to_coeff": (None, [ctypes.c_void_p, _u64p, i32]),
+        "or_domain_coeff_to_lagrange": (None, [ctypes.c_void_p, _u64p, i32]),
+        "or_domain_coeff_to_extended": (None, [ctypes.c_void_p, _u64p, _u64p, i32]),
+        "or_domain_extended_to_coeff": (None, [ctypes.c_void_p, _u64p, i32]),
+        "or_domain_extended_to_lagrange": (None, [ctypes.c_void_p, _u64p, _u64p, i32]),
+        "or_domain_divide_by_vanishing_poly": (None, [ctypes.c_void_p, _u64p, i32]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def threads_default():
+    return int(os.environ.get("MZK_ORACLE_THREADS", os.cpu_count() or 1))
+
+
+def P(a):
+    """uint64 pointer to a C-contiguous numpy array."""
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u64p)
+
+
+def u64s(limbs):
+    return np.array([int(x, 16) if isinstance(x, str) else int(x) for x in limbs], dtype=np.uint64)
+
+
+# ---- integers <-> limbs ----
+def to_int(limbs):
+    return sum(int(v) << (64 * i) for i, v in enumerate(np.asarray(limbs, dtype=np.uint64).tolist()))
+
+
+def from_int(v, n):
+    return np.array([(v >> (64 * i)) & (2**64 - 1) for i in range(n)], dtype=np.uint64)
+
+
+# ---- Fr ----
+def fr_const(which):
+    o = np.zeros(4, np.uint64)
+    lib.or_fr_const(which, P(o))
+    return o
+
+
+def fr_op(name, *args):
+    o = np.zeros(4, np.uint64)
+    args = [np.ascontiguousarray(a, dtype=np.uint64) for a in args]
+    getattr(lib, "or_fr_" + name)(P(o), *[P(a) for a in args])
+    return o
+
+
+def fp_op(name, *args):
+    o = np.zeros(6, np.uint64)
+    args = [np.ascontiguousarray(a, dtype=np.uint64) for a in args]
+    getattr(lib, "or_fp_" + name)(P(o), *[P(a) for a in args])
+    return o
+
+
+def fp_const(which):
+    o = np.zeros(6, np.uint64)
+    lib.or_fp_const(which, P(o))
+    return o
+
+
+# ---- G1 ----
+def g1_generator():
+    o = np.zeros(12, np.uint64)
+    lib.or_g1_generator(P(o))
+    return o
+
+
+def g1_mul(aff, scalar_mont):
+    o = np.zeros(12, np.uint64)
+    lib.or_g1_mul(P(o), P(np.ascontiguousarray(aff, np.uint64)), P(np.ascontiguousarray(scalar_mont, np.uint64)))
+    return o
+
+
+def g1_jac_add(a, b):
+    o = np.zeros(18, np.uint64)
+    lib.or_g1_add(P(o), P(np.ascontiguousarray(a, np.uint64)), P(np.ascontiguousarray(b, np.uint64)))
+    return o
+
+
+def g1_jac_double(a):
+    o = np.zeros(18, np.uint64)
+    lib.or_g1_double(P(o), P(np.ascontiguousarray(a, np.uint64)))
+    return o
+
+
+def g1_to_affine(jac):
+    o = np.zeros(12, np.uint64)
+    lib.or_g1_to_affine(P(o), P(np.ascontiguousarray(jac, np.uint64)))
+    return o
+
+
+def g1_from_affine(aff):
+    o = np.zeros(18, np.uint64)
+    lib.or_g1_from_affine(P(o), P(np.ascontiguousarray(aff, np.uint64)))
+    return o
+
+
+def g1_is_on_curve(aff):
+    return bool(lib.or_g1_is_on_curve_affine(P(np.ascontiguousarray(aff, np.uint64))))
+
+
+def g1_compress(aff):
+    o = np.zeros(48, np.uint8)
+    lib.or_g1_compress(o.ctypes.data_as(_u8p), P(np.ascontiguousarray(aff, np.uint64)))
+    return bytes(o)
+
+
+# ---- MSM ----
+def msm_naive(scalars, bases):
+    o = np.zeros(12, np.uint64)
+    lib.or_msm_naive(P(o), P(scalars), P(bases), scalars.shape[0])
+    return o
+
+
+def msm_best(scalars, bases, threads=None):
+    o = np.zeros(12, np.uint64)
+    lib.or_msm_best(P(o), P(scalars), P(bases), scalars.shape[0], threads or threads_default())
+    return o
+
+
+def msm_specific(scalars, bases, threads=None):
+    o = np.zeros(12, np.uint64)
+    lib.or_msm_specific(P(o), P(scalars), P(bases), scalars.shape[0], threads or threads_default())
+    return o
+
+
+def booth_index(window_index, window_size, repr32):
+    b = np.ascontiguousarray(np.frombuffer(bytes(repr32), dtype=np.uint8))
+    return lib.or_booth_index(window_index, window_size, b.ctypes.data_as(_u8p))
+
+
+def fr_inner_product(s, r, threads=None):
+    o = np.zeros(4, np.uint64)
+    lib.or_fr_inner_product(P(o), P(s), P(r), s.shape[0], threads or threads_default())
+    return o
+
+
+# ---- seeded inputs ----
+def rand_fr(seed, n, first=0, threads=None):
+    o = np.zeros((n, 4), np.uint64)
+    lib.or_rand_fr(P(o), seed, first, n, threads or threads_default())
+    return o
+
+
+def gen_bases(seed, n, first=0, threads=None):
+    o = np.zeros((n, 12), np.uint64)
+    lib.or_gen_bases(P(o), seed, first, n, threads or threads_default())
+    return o
+
+
+# ---- FFT ----
+def compute_twiddles(omega, log_n):
+    o = np.zeros(((1 << log_n) // 2, 4), np.uint64)
+    lib.or_compute_twiddles(P(o), P(np.ascontiguousarray(omega, np.uint64)), log_n)
+    return o
+
+
+def best_fft(a, twiddles, log_n, threads=None):
+    a = np.ascontiguousarray(a, np.uint64).copy()
+    lib.or_best_fft(P(a), P(twiddles), log_n, threads or threads_default())
+    return a
+
+
+def fft_dif_pruned(a, twiddles, log_n, n_real, threads=None):
+    a = np.ascontiguousarray(a, np.uint64).copy()
+    lib.or_fft_dif_pruned(P(a), P(twiddles), log_n, n_real, threads or threads_default())
+    return a
+
+
+def dft_naive(a, omega):
+    o = np.zeros_like(a)
+    lib.or_dft_naive(P(o), P(np.ascontiguousarray(a, np.uint64)), P(np.ascontiguousarray(omega, np.uint64)), a.shape[0])
+    return o
+
+
+class Domain:
+    """EvaluationDomain restatement (proofs/src/poly/domain.rs:54-414)."""
+
+    def __init__(self, j, k):
+        self.h = lib.or_domain_new(j, k)
+        self.k = lib.or_domain_k(self.h)
+        self.extended_k = lib.or_domain_extended_k(self.h)
+        self.n = 1 << self.k
+        self.extended_len = 1 << self.extended_k
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_domain_free(self.h)
+            self.h = None
+
+    def get(self, which, idx=0):
+        o = np.zeros(4, np.uint64)
+        lib.or_domain_get(self.h, which, idx, P(o))
+        return o
+
+    def lagrange_to_coeff(self, a, threads=None):
+        a = np.ascontiguousarray(a, np.uint64).copy()
+        lib.or_domain_lagrange_to_coeff(self.h, P(a), threads or threads_default())
+        return a
+
+    def coeff_to_lagrange(self, a, threads=None):
+        a = np.ascontiguousarray(a, np.uint64).copy()
+        lib.or_domain_coeff_to_lagrange(self.h, P(a), threads or threads_default())
+        return a
+
+    def coeff_to_extended(self, a, threads=None):
+        a = np.ascontiguousarray(a, np.uint64)
+        o = np.zeros((self.extended_len, 4), np.uint64)
+        lib.or_domain_coeff_to_extended(self.h, P(a), P(o), threads or threads_default())
+        return o
+
+    def extended_to_coeff(self, a, threads=None):
+        a = np.ascontiguousarray(a, np.uint64).copy()
+        lib.or_domain_extended_to_coeff(self.h, P(a), threads or threads_default())
+        return a
+
+    def extended_to_lagrange(self, a, threads=None):
+        a = np.ascontiguousarray(a, np.uint64).copy()
+        o = np.zeros((self.n, 4), np.uint64)
+        lib.or_domain_extended_to_lagrange(self.h, P(a), P(o), threads or threads_default())
+        return o
+
+    def divide_by_vanishing_poly(self, a, threads=None):
+        a = np.ascontiguousarray(a, np.uint64).copy()
+        lib.or_domain_divide_by_vanishing_poly(self.h, P(a), threads or threads_default())
+        return a
