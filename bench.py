@@ -1,0 +1,320 @@
+#!/usr/bin/env python3
+"""Headline benchmark: BLS12-381 G1 MSM throughput (Mpts/s) at n = 2^24.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full MSM (digit sort, bucket accumulation, bucket reduction,
+window combination, normalisation) over n seeded synthetic points: bases
+[r_i]G and uniform Fr scalars in Montgomery form, generated on the device.
+`value` times K steps with the inputs resident in HBM (2.1 GB of inputs, far
+above the 126 MB L2, so no flush is needed); `e2e` times the same MSM through
+the reference-facing C ABI call with pinned HOST buffers (host->device copies
+inside the timed region).  With N > 1 (torchrun) every rank runs its own MSM
+on its own GPU (replicas, weak scaling; the MSM has no exchange step) and the
+step time is the max over ranks.
+
+`--impl reference` times the CPU restatement of the reference's msm_best
+(curves/src/msm.rs:460-532; the reference is Rust whose arithmetic lives in the
+un-vendored blst crate, so it cannot be built here) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "G1 MSM Mpts/s at 2^24"
+UNIT = "Mpts/s"
+IMAD_PER_FP_MUL = 600        # CIOS, 12 limbs: 2*12^2+12 = 300 products x (lo, hi)
+FP_MUL_PER_MIXED_ADD = 10    # madd-2008-s: 8M + 2S
+IMAD_PER_POINT_REF = 97.0e3  # reference schedule c=17, W=16 at 2^24: 1.628e12 IMAD / 2^24
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--log-n", type=int, default=24)
+    p.add_argument("--cpu-sample-log-n", type=int, default=20)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(log_n):
+    return f"G1 MSM n=2^{log_n}: bases [r_i]G and scalars uniform in Fr (Montgomery), seeded"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu_id), "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append({"sm": float(parts[1]), "max": float(parts[2]), "power": float(parts[3]),
+                             "hw_slowdown": parts[5], "hw_thermal": parts[6], "sw_thermal": parts[7],
+                             "sw_power_cap": parts[8]})
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = sorted({name for r in rows for name, key in
+                          (("hw_slowdown", "hw_slowdown"), ("hw_thermal_slowdown", "hw_thermal"),
+                           ("sw_thermal_slowdown", "sw_thermal"), ("sw_power_cap", "sw_power_cap"))
+                          if r[key].lower() == "active"})
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["max"] for r in rows),
+                "power_w_max": max(r["power"] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+def traffic_from_profiles(c):
+    """DRAM bytes per bucket entry of the accumulate kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "msm_accumulate.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_entry:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+def dist_init(backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, _ = dist_init("gloo")
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    n = 1 << args.cpu_sample_log_n
+    s = O.rand_fr(0xC0FFEE, n, threads=threads)
+    b = O.gen_bases(0xBA5E, n, threads=threads)
+    for _ in range(args.warmup):
+        O.msm_best(s, b, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.msm_best(s, b, threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = n / (ms / 1e3) / 1e6
+    sample = (f"n=2^{args.cpu_sample_log_n} points of the 2^{args.log_n} workload per step (bounded sample); "
+              f"C restatement of msm_best, windows in parallel on {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (CPU)", "data": "synthetic (seeded)",
+        "config": {"workload": workload(args.log_n), "n": 1 << args.log_n, "parallelism": "cpu threads"},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_init("nccl")
+    torch.cuda.set_device(local)
+    from _loader import load
+    mzk = load()
+    ctx = mzk.Context(local)
+    n = 1 << args.log_n
+    ds = ctx.gen_rand_fr(0xC0FFEE + rank, n)
+    db = ctx.gen_bases(0xBA5E + rank, n)
+    imad_peak, fp_mul_rate = ctx.probe_imad_peak()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        ctx.msm_device(ds, db, n)
+    ctx.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    launches0 = ctx.launches
+    gpu_id = local
+    try:
+        uuid = torch.cuda.get_device_properties(local).uuid
+        gpu_id = f"GPU-{uuid}"
+    except Exception:
+        pass
+    sampler = ClockSampler(gpu_id)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.msm_device(ds, db, n)
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop()
+    ctx.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches = ctx.launches - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    phases = ctx.phase_stats()
+    ctx.set_profiling(False)
+    c, windows, entries = ctx.msm_last_shape()
+    value = world * n / (ms / 1e3) / 1e6
+
+    acc_ms, acc_cnt = phases["accumulate"]
+    acc_avg_ms = acc_ms / max(acc_cnt, 1)
+    imad_acc = entries * FP_MUL_PER_MIXED_ADD * IMAD_PER_FP_MUL
+    achieved = imad_acc / (acc_avg_ms / 1e3)
+    tpe = traffic_from_profiles(c)
+    roofline = {
+        "kernel": "k_accumulate (bucket accumulation)", "bound": "imad",
+        "achieved": round(achieved / 1e12, 3), "peak": round(imad_peak / 1e12, 3), "unit": "TIMAD/s",
+        "frac": round(achieved / imad_peak, 4),
+        "traffic": None if tpe is None else round(tpe * entries),
+        "peak_source": "measured in this run by mzk_probe_imad_peak (independent 32-bit mad.lo/mad.hi)",
+        "work": f"{entries} bucket entries x {FP_MUL_PER_MIXED_ADD} Fp mul x {IMAD_PER_FP_MUL} IMAD",
+        "launch_ms": round(acc_avg_ms, 3),
+    }
+    msm_roof = {
+        "achieved": round(IMAD_PER_POINT_REF * n / (ms / 1e3) / 1e12, 3), "unit": "TIMAD/s",
+        "frac": round(IMAD_PER_POINT_REF * n / (ms / 1e3) / imad_peak, 4),
+        "work": "97.0k IMAD per point (reference schedule c=17, 16 windows)",
+    }
+
+    e2e = None
+    if not args.no_e2e:
+        hs = torch.empty(n * 4, dtype=torch.int64, pin_memory=True)
+        hb = torch.empty(n * 12, dtype=torch.int64, pin_memory=True)
+        lib = mzk.lib()
+        mzk._check(lib.mzk_memcpy_d2h(ctx.h, hs.data_ptr(), ds.ptr, n * 32))
+        mzk._check(lib.mzk_memcpy_d2h(ctx.h, hb.data_ptr(), db.ptr, n * 96))
+        s_host = hs.numpy().view(np.uint64).reshape(n, 4)
+        b_host = hb.numpy().view(np.uint64).reshape(n, 12)
+        for _ in range(2):
+            ctx.msm_best(s_host, b_host)
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            ctx.msm_best(s_host, b_host)
+        f1.record(stream)
+        f1.synchronize()
+        ems = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+        e2e = {"value": round(world * n / (ems / 1e3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(ems, 3),
+               "h2d_bytes_per_step": n * 32 + n * 96, "d2h_bytes_per_step": windows * 192 + 4,
+               "api": "mzk_msm_g1 (host pointers, pinned)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        m = 1 << args.cpu_sample_log_n
+        s_cpu = ds.download((m, 4))
+        b_cpu = db.download((m, 12))
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.msm_best(s_cpu, b_cpu, threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(m / dt / 1e6, 4), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"first 2^{args.cpu_sample_log_n} points of the timed inputs, one msm_best call "
+                         f"(C restatement of curves/src/msm.rs:460-532), windows in parallel"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (12-limb Fp / 8-limb Fr Montgomery)",
+            "data": "synthetic (seeded, generated on device)",
+            "config": {"workload": workload(args.log_n), "n": n, "window_c": c, "windows": windows,
+                       "bucket_entries": entries, "l2": "inputs 2.1 GB > 126 MB L2 (no flush)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "roofline_msm": msm_roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clocks,
+            "phases_ms": {k: round(v[0] / max(v[1], 1), 3) for k, v in phases.items()},
+            "fp_mul_rate_g_per_s": round(fp_mul_rate / 1e9, 2),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

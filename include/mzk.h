@@ -1,0 +1,89 @@
+/*
+ * mzk.h — C ABI of the B200 (sm_100a) prover core for midnight-zk.
+ *
+ * Plain pointers and sizes only.  Memory layouts are the reference's own
+ * in-memory layouts, so a Rust caller passes its slices unchanged:
+ *   Fr (midnight `Fq`)   4 x u64 LE, Montgomery R = 2^256   (curves/src/bls12_381/fq.rs:25-29)
+ *   Fp                   6 x u64 LE, Montgomery R = 2^384   (curves/src/bls12_381/fp.rs:96-98)
+ *   G1Affine             {x, y: Fp}, identity all-zero       (blst_p1_affine, g1.rs:34)
+ *   G1Projective         {x, y, z: Fp} Jacobian, identity z=0 (blst_p1, g1.rs:495)
+ *
+ * Every function returns 0 on success or an MZK_ERR_* code; mzk_last_error()
+ * gives the message of the calling thread's last failure.  All entry points
+ * are thread-safe; calls on one context are serialised.  The reference panics
+ * on length mismatch (curves/src/msm.rs:461, proofs/src/poly/domain.rs:250);
+ * the Rust binding turns a non-zero status into that panic.
+ */
+#ifndef MZK_H
+#define MZK_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MZK_OK 0
+#define MZK_ERR_ARG 1
+#define MZK_ERR_OOM 2
+#define MZK_ERR_CUDA 3
+#define MZK_ERR_TIMEOUT 4
+#define MZK_ERR_STATE 5
+
+typedef struct mzk_ctx mzk_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+int mzk_ctx_create(int device, mzk_ctx **out);
+int mzk_ctx_destroy(mzk_ctx *ctx);
+const char *mzk_last_error(void);
+const char *mzk_version(void);
+/* kernels this library launched on ctx since creation */
+uint64_t mzk_ctx_launch_count(const mzk_ctx *ctx);
+/* the stream every call of ctx runs on (cudaStream_t as void*) */
+void *mzk_ctx_stream(mzk_ctx *ctx);
+int mzk_ctx_synchronize(mzk_ctx *ctx);
+/* Per-phase device timing (CUDA events on the launching stream).  Phases of
+ * the MSM: 0 histogram, 1 scan, 2 scatter, 3 accumulate, 4 fixup, 5 reduce.
+ * Turning profiling on resets the totals. */
+int mzk_ctx_set_profiling(mzk_ctx *ctx, int on);
+int mzk_ctx_phase_stats(mzk_ctx *ctx, double *ms_out, uint64_t *count_out, int max_phases);
+/* Integer multiply-add throughput of this GPU (IMAD/s) and 12-limb Montgomery
+ * multiplications per second, measured by microbenchmark kernels. */
+int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s);
+
+/* ---- device memory helpers (for callers without a CUDA runtime) ---------- */
+int mzk_device_alloc(mzk_ctx *ctx, size_t bytes, void **out);
+int mzk_device_free(mzk_ctx *ctx, void *ptr);
+int mzk_memcpy_h2d(mzk_ctx *ctx, void *dst, const void *src, size_t bytes);
+int mzk_memcpy_d2h(mzk_ctx *ctx, void *dst, const void *src, size_t bytes);
+
+/* ---- G1 multi-scalar multiplication ------------------------------------ */
+/*
+ * out = sum_i scalars[i] * bases[i] as a G1Projective (18 u64: x, y, z with
+ * z = 1 in Montgomery form, or all zero for the identity), bit-identical in
+ * affine form to the reference.
+ *
+ * Replaces curves::msm::msm_best<G1Affine> (curves/src/msm.rs:460) and
+ * proofs::poly::kzg::msm::msm_specific<G1Affine> (proofs/src/poly/kzg/msm.rs:174):
+ * zero scalars and identity bases contribute nothing, n == 0 gives the identity.
+ * scalars: n x 4 u64 (Fq, Montgomery); bases: n x 12 u64 (G1Affine). HOST pointers.
+ */
+int mzk_msm_g1(mzk_ctx *ctx, const uint64_t *scalars, const uint64_t *bases, size_t n, uint64_t out[18]);
+/* Same with DEVICE pointers (inputs resident in HBM, e.g. a device SRS). */
+int mzk_msm_g1_device(mzk_ctx *ctx, const uint64_t *d_scalars, const uint64_t *d_bases, size_t n, uint64_t out[18]);
+/* Window width override (0 = automatic), for tuning and tests. */
+int mzk_msm_set_window(mzk_ctx *ctx, int c);
+int mzk_msm_pick_window(size_t n);
+/* Window width, window count and bucket entries (non-zero digits) of the last MSM. */
+int mzk_msm_last_shape(mzk_ctx *ctx, int *c, int *windows, uint64_t *entries);
+
+/* ---- seeded synthetic inputs (benchmarks and tests) -------------------- */
+/* n uniform Fr elements (Montgomery) of stream `seed`, elements first..first+n-1 */
+int mzk_gen_rand_fr_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);
+/* n affine bases [r_i]G with r_i the Fr elements of stream `seed` */
+int mzk_gen_bases_g1_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

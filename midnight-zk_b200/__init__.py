@@ -1,0 +1,237 @@
+"""Host-side mirror of the midnight-zk prover-core interface over the B200 C ABI.
+
+The product is the CUDA library ``lib/libmzkgpu.so`` (sources in ``csrc/``,
+ABI in ``include/mzk.h``).  This module binds it with ctypes and offers the
+reference's operations under the reference's names:
+
+    ctx = Context(0)
+    ctx.msm_best(scalars, bases)        # curves::msm::msm_best      (curves/src/msm.rs:460)
+    ctx.msm_specific(scalars, bases)    # kzg::msm::msm_specific     (proofs/src/poly/kzg/msm.rs:174)
+
+Arrays use the reference's in-memory layouts as numpy uint64: Fr (``Fq``)
+elements shape (n, 4) Montgomery, G1Affine shape (n, 12), G1Projective
+shape (18,) (blst_p1 Jacobian; results come back with z = 1 or all-zero for
+the identity).  There is no CPU fallback: when the library or a CUDA device is
+missing every call raises ``MzkError``.
+
+The directory name is not a Python identifier; ``_loader.load()`` at the
+repository root imports it as ``mzk_b200``.
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libmzkgpu.so"
+HEADER = PKG.parent / "include" / "mzk.h"
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
+_i32 = ctypes.c_int
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+
+# name -> (restype, argtypes); every symbol declared in include/mzk.h
+SIGNATURES = {
+    "mzk_ctx_create": (_i32, [_i32, ctypes.POINTER(_vp)]),
+    "mzk_ctx_destroy": (_i32, [_vp]),
+    "mzk_last_error": (ctypes.c_char_p, []),
+    "mzk_version": (ctypes.c_char_p, []),
+    "mzk_ctx_launch_count": (_u64, [_vp]),
+    "mzk_ctx_stream": (_vp, [_vp]),
+    "mzk_ctx_synchronize": (_i32, [_vp]),
+    "mzk_ctx_set_profiling": (_i32, [_vp, _i32]),
+    "mzk_ctx_phase_stats": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _u64p, _i32]),
+    "mzk_probe_imad_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "mzk_msm_last_shape": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u64p]),
+    "mzk_device_alloc": (_i32, [_vp, _sz, ctypes.POINTER(_vp)]),
+    "mzk_device_free": (_i32, [_vp, _vp]),
+    "mzk_memcpy_h2d": (_i32, [_vp, _vp, _vp, _sz]),
+    "mzk_memcpy_d2h": (_i32, [_vp, _vp, _vp, _sz]),
+    "mzk_msm_g1": (_i32, [_vp, _u64p, _u64p, _sz, _u64p]),
+    "mzk_msm_g1_device": (_i32, [_vp, _vp, _vp, _sz, _u64p]),
+    "mzk_msm_set_window": (_i32, [_vp, _i32]),
+    "mzk_msm_pick_window": (_i32, [_sz]),
+    "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
+    "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
+}
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_CUDA", 4: "ERR_TIMEOUT", 5: "ERR_STATE"}
+
+
+class MzkError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises MzkError when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise MzkError(5, f"{LIB_PATH} is missing: run __graft_entry__.build() (no CPU fallback exists)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise MzkError(status, lib().mzk_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"], "expect C-contiguous uint64 arrays"
+    return a.ctypes.data_as(_u64p)
+
+
+class DeviceBuffer:
+    """Device memory owned through the library (plumbing for tests/bench)."""
+
+    def __init__(self, ctx, nbytes):
+        self.ctx = ctx
+        self.nbytes = int(nbytes)
+        p = _vp()
+        _check(lib().mzk_device_alloc(ctx.h, self.nbytes, ctypes.byref(p)))
+        self.ptr = p.value
+
+    def free(self):
+        if self.ptr:
+            _check(lib().mzk_device_free(self.ctx.h, self.ptr))
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def upload(self, arr):
+        arr = np.ascontiguousarray(arr)
+        assert arr.nbytes <= self.nbytes
+        _check(lib().mzk_memcpy_h2d(self.ctx.h, self.ptr, arr.ctypes.data, arr.nbytes))
+
+    def download(self, shape, dtype=np.uint64):
+        out = np.empty(shape, dtype)
+        assert out.nbytes <= self.nbytes
+        _check(lib().mzk_memcpy_d2h(self.ctx.h, out.ctypes.data, self.ptr, out.nbytes))
+        return out
+
+
+class Context:
+    """One device context (streams, scratch arena) on GPU `device`."""
+
+    def __init__(self, device=0):
+        h = _vp()
+        _check(lib().mzk_ctx_create(device, ctypes.byref(h)))
+        self.h = h.value
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mzk_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def launches(self):
+        return int(lib().mzk_ctx_launch_count(self.h))
+
+    @property
+    def stream(self):
+        return lib().mzk_ctx_stream(self.h)
+
+    def synchronize(self):
+        _check(lib().mzk_ctx_synchronize(self.h))
+
+    def alloc(self, nbytes):
+        return DeviceBuffer(self, nbytes)
+
+    def set_profiling(self, on=True):
+        _check(lib().mzk_ctx_set_profiling(self.h, 1 if on else 0))
+
+    PHASES = ["histogram", "scan", "scatter", "accumulate", "fixup", "reduce"]
+
+    def phase_stats(self):
+        """{phase: (total_ms, count)} of the device time recorded while profiling."""
+        ms = (ctypes.c_double * 16)()
+        cnt = np.zeros(16, np.uint64)
+        _check(lib().mzk_ctx_phase_stats(self.h, ms, _ptr(cnt), 16))
+        return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(self.PHASES)}
+
+    def probe_imad_peak(self):
+        """(IMAD/s, 12-limb Montgomery multiplications/s) of this GPU."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(lib().mzk_probe_imad_peak(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def msm_last_shape(self):
+        c, w, e = _i32(), _i32(), np.zeros(1, np.uint64)
+        _check(lib().mzk_msm_last_shape(self.h, ctypes.byref(c), ctypes.byref(w), _ptr(e)))
+        return c.value, w.value, int(e[0])
+
+    # ---- MSM ----
+    def set_msm_window(self, c):
+        _check(lib().mzk_msm_set_window(self.h, int(c)))
+
+    def msm_best(self, scalars, bases):
+        """sum_i scalars[i] * bases[i] (host arrays) -> G1Projective (18,) uint64."""
+        scalars = np.ascontiguousarray(scalars, np.uint64).reshape(-1, 4)
+        bases = np.ascontiguousarray(bases, np.uint64).reshape(-1, 12)
+        if scalars.shape[0] != bases.shape[0]:
+            # the reference asserts equal lengths (curves/src/msm.rs:461)
+            raise MzkError(1, "msm: coeffs and bases have different lengths")
+        out = np.zeros(18, np.uint64)
+        _check(lib().mzk_msm_g1(self.h, _ptr(scalars), _ptr(bases), scalars.shape[0], _ptr(out)))
+        return out
+
+    msm_specific = msm_best
+
+    def msm_device(self, d_scalars, d_bases, n):
+        """MSM over device-resident inputs (pointers or DeviceBuffers)."""
+        ds = d_scalars.ptr if isinstance(d_scalars, DeviceBuffer) else int(d_scalars)
+        db = d_bases.ptr if isinstance(d_bases, DeviceBuffer) else int(d_bases)
+        out = np.zeros(18, np.uint64)
+        _check(lib().mzk_msm_g1_device(self.h, ds, db, int(n), _ptr(out)))
+        return out
+
+    # ---- synthetic inputs ----
+    def gen_rand_fr(self, seed, n, first=0, out=None):
+        buf = out or self.alloc(n * 32)
+        _check(lib().mzk_gen_rand_fr_device(self.h, seed, first, n, buf.ptr))
+        return buf
+
+    def gen_bases(self, seed, n, first=0, out=None):
+        buf = out or self.alloc(n * 96)
+        _check(lib().mzk_gen_bases_g1_device(self.h, seed, first, n, buf.ptr))
+        return buf
+
+
+def msm_pick_window(n):
+    return int(lib().mzk_msm_pick_window(n))
+
+
+def affine(jac18):
+    """G1Projective with z in {0, 1} -> G1Affine (12,) layout."""
+    return np.ascontiguousarray(jac18[:12])

@@ -1,0 +1,329 @@
+// capi.cu — the extern "C" boundary (include/mzk.h) and the device context.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/mzk.h"
+#include "runtime.hpp"
+
+struct mzk_ctx {
+    mzk::Context impl;
+};
+
+namespace mzk {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+Status Context::ensure(const char* name, size_t bytes, void** out) {
+    if (bytes == 0) bytes = 16;
+    DevBuf& b = bufs[name];
+    if (b.bytes >= bytes) {
+        *out = b.p;
+        return OK;
+    }
+    if (b.p) {
+        // the old buffer may still be read by queued work on our streams
+        cudaStreamSynchronize(stream);
+        cudaStreamSynchronize(copy_stream);
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        set_error(std::string("device allocation of ") + std::to_string(bytes) + " bytes for " + name + " failed: " +
+                  cudaGetErrorString(e));
+        return ERR_OOM;
+    }
+    b.bytes = bytes;
+    *out = b.p;
+    return OK;
+}
+
+Status Context::ensure_pinned(size_t bytes, void** out) {
+    if (pinned_bytes >= bytes) {
+        *out = pinned;
+        return OK;
+    }
+    if (pinned) {
+        cudaStreamSynchronize(stream);
+        cudaFreeHost(pinned);
+        pinned = nullptr;
+        pinned_bytes = 0;
+    }
+    MZK_CUDA_CHECK(cudaMallocHost(&pinned, bytes));
+    pinned_bytes = bytes;
+    *out = pinned;
+    return OK;
+}
+
+Status Context::phase_begin(int phase, cudaStream_t st) {
+    if (!profiling) return OK;
+    if (prof_used >= kMaxEvents / 2) {
+        set_error("profiling: too many open phases");
+        return ERR_STATE;
+    }
+    for (int k = 0; k < 2; k++)
+        if (!prof_ev[2 * prof_used + k]) MZK_CUDA_CHECK(cudaEventCreate(&prof_ev[2 * prof_used + k]));
+    prof_phase[prof_used] = phase;
+    MZK_CUDA_CHECK(cudaEventRecord(prof_ev[2 * prof_used], st));
+    return OK;
+}
+
+Status Context::phase_end(cudaStream_t st) {
+    if (!profiling) return OK;
+    MZK_CUDA_CHECK(cudaEventRecord(prof_ev[2 * prof_used + 1], st));
+    prof_used++;
+    return OK;
+}
+
+void Context::phase_collect() {
+    for (int i = 0; i < prof_used; i++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, prof_ev[2 * i], prof_ev[2 * i + 1]) == cudaSuccess) {
+            phase_ms[prof_phase[i]] += ms;
+            phase_count[prof_phase[i]]++;
+        }
+    }
+    prof_used = 0;
+}
+
+Context::~Context() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
+    for (auto& kv : bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    if (pinned) cudaFreeHost(pinned);
+    if (gen_table) cudaFree(gen_table);
+    if (ev_copy) cudaEventDestroy(ev_copy);
+    for (int i = 0; i < kMaxEvents; i++)
+        if (prof_ev[i]) cudaEventDestroy(prof_ev[i]);
+    if (stream) cudaStreamDestroy(stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+}
+
+}  // namespace mzk
+
+using mzk::Status;
+
+namespace {
+
+struct Guard {
+    mzk_ctx* c;
+    explicit Guard(mzk_ctx* ctx) : c(ctx) {
+        c->impl.mu.lock();
+        cudaSetDevice(c->impl.device);
+    }
+    ~Guard() { c->impl.mu.unlock(); }
+};
+
+int check_ctx(mzk_ctx* ctx) {
+    if (!ctx) {
+        mzk::set_error("null context");
+        return mzk::ERR_ARG;
+    }
+    return mzk::OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mzk_last_error(void) { return mzk::g_last_error.c_str(); }
+const char* mzk_version(void) { return "mzk-b200 0.1 (sm_100a)"; }
+
+int mzk_ctx_create(int device, mzk_ctx** out) {
+    if (!out) {
+        mzk::set_error("null out pointer");
+        return mzk::ERR_ARG;
+    }
+    *out = nullptr;
+    int count = 0;
+    MZK_CUDA_CHECK(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) {
+        mzk::set_error("no CUDA device " + std::to_string(device));
+        return mzk::ERR_ARG;
+    }
+    MZK_CUDA_CHECK(cudaSetDevice(device));
+    mzk_ctx* c = new (std::nothrow) mzk_ctx;
+    if (!c) return mzk::ERR_OOM;
+    c->impl.device = device;
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->impl.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->impl.copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->impl.ev_copy, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        mzk::set_error(std::string("context setup: ") + cudaGetErrorString(e));
+        delete c;
+        return mzk::ERR_CUDA;
+    }
+    if (prop.major != 10) {
+        mzk::set_error("this library is built for sm_100a (B200); device " + std::to_string(device) + " is sm_" +
+                       std::to_string(prop.major) + std::to_string(prop.minor));
+        delete c;
+        return mzk::ERR_STATE;
+    }
+    c->impl.num_sms = prop.multiProcessorCount;
+    *out = c;
+    return mzk::OK;
+}
+
+int mzk_ctx_destroy(mzk_ctx* ctx) {
+    if (!ctx) return mzk::OK;
+    cudaSetDevice(ctx->impl.device);
+    delete ctx;
+    return mzk::OK;
+}
+
+uint64_t mzk_ctx_launch_count(const mzk_ctx* ctx) { return ctx ? ctx->impl.launches : 0; }
+
+void* mzk_ctx_stream(mzk_ctx* ctx) { return ctx ? (void*)ctx->impl.stream : nullptr; }
+
+int mzk_ctx_synchronize(mzk_ctx* ctx) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.copy_stream));
+    return mzk::OK;
+}
+
+int mzk_device_alloc(mzk_ctx* ctx, size_t bytes, void** out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!out) return mzk::ERR_ARG;
+    Guard g(ctx);
+    MZK_CUDA_CHECK(cudaMalloc(out, bytes ? bytes : 16));
+    return mzk::OK;
+}
+
+int mzk_device_free(mzk_ctx* ctx, void* ptr) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaFree(ptr));
+    return mzk::OK;
+}
+
+int mzk_memcpy_h2d(mzk_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_memcpy_d2h(mzk_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_msm_set_window(mzk_ctx* ctx, int c) {
+    if (int s = check_ctx(ctx)) return s;
+    if (c != 0 && (c < 5 || c > 24)) {
+        mzk::set_error("window width must be 0 (auto) or in [5, 24]");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    ctx->impl.msm_window_override = c;
+    return mzk::OK;
+}
+
+int mzk_msm_pick_window(size_t n) { return mzk::msm_pick_window(n); }
+
+int mzk_ctx_set_profiling(mzk_ctx* ctx, int on) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    ctx->impl.profiling = on != 0;
+    if (on) {
+        for (int i = 0; i < mzk::Context::kPhases; i++) {
+            ctx->impl.phase_ms[i] = 0.0;
+            ctx->impl.phase_count[i] = 0;
+        }
+    }
+    return mzk::OK;
+}
+
+int mzk_ctx_phase_stats(mzk_ctx* ctx, double* ms_out, uint64_t* count_out, int max_phases) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    for (int i = 0; i < max_phases && i < mzk::Context::kPhases; i++) {
+        if (ms_out) ms_out[i] = ctx->impl.phase_ms[i];
+        if (count_out) count_out[i] = ctx->impl.phase_count[i];
+    }
+    return mzk::OK;
+}
+
+int mzk_msm_last_shape(mzk_ctx* ctx, int* c, int* windows, uint64_t* entries) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    if (c) *c = ctx->impl.last_c;
+    if (windows) *windows = ctx->impl.last_windows;
+    if (entries) *entries = ctx->impl.last_entries;
+    return mzk::OK;
+}
+
+int mzk_probe_imad_peak(mzk_ctx* ctx, double* imad_per_s, double* fp_mul_per_s) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    return mzk::probe_imad(&ctx->impl, imad_per_s, fp_mul_per_s);
+}
+
+int mzk_msm_g1_device(mzk_ctx* ctx, const uint64_t* d_scalars, const uint64_t* d_bases, size_t n, uint64_t out[18]) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!out || (n && (!d_scalars || !d_bases))) {
+        mzk::set_error("msm: null pointer");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    return mzk::msm_g1_device(&ctx->impl, d_scalars, d_bases, n, out, ctx->impl.stream, nullptr);
+}
+
+int mzk_msm_g1(mzk_ctx* ctx, const uint64_t* scalars, const uint64_t* bases, size_t n, uint64_t out[18]) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!out || (n && (!scalars || !bases))) {
+        mzk::set_error("msm: null pointer");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    if (n == 0) {
+        std::memset(out, 0, 18 * 8);
+        return mzk::OK;
+    }
+    mzk::Context* c = &ctx->impl;
+    void *ds, *db;
+    MZK_TRY(c->ensure("in_scalars", n * 32, &ds));
+    MZK_TRY(c->ensure("in_bases", n * 96, &db));
+    // scalars first on the compute stream (the digit passes need only them),
+    // bases on the copy stream, overlapping the sort
+    MZK_CUDA_CHECK(cudaMemcpyAsync(ds, scalars, n * 32, cudaMemcpyHostToDevice, c->stream));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(db, bases, n * 96, cudaMemcpyHostToDevice, c->copy_stream));
+    MZK_CUDA_CHECK(cudaEventRecord(c->ev_copy, c->copy_stream));
+    return mzk::msm_g1_device(c, ds, db, n, out, c->stream, c->ev_copy);
+}
+
+int mzk_gen_rand_fr_device(mzk_ctx* ctx, uint64_t seed, uint64_t first, size_t n, uint64_t* d_out) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    MZK_TRY(mzk::gen_rand_fr(&ctx->impl, seed, first, n, d_out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_gen_bases_g1_device(mzk_ctx* ctx, uint64_t seed, uint64_t first, size_t n, uint64_t* d_out) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    MZK_TRY(mzk::gen_bases_g1(&ctx->impl, seed, first, n, d_out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,301 @@
+// field.cuh — BLS12-381 Fp (base field) and Fr (scalar field) on sm_100a.
+//
+// Elements are little-endian 32-bit limbs in Montgomery form with the same R
+// as the reference (Fp: R = 2^384, 12 limbs; Fr: R = 2^256, 8 limbs), so the
+// device bytes are exactly the bytes of the reference's `blst_fp` / `blst_fr`
+// (curves/src/bls12_381/fp.rs:96-98, fq.rs:25-29) and no conversion happens
+// at the C ABI.
+//
+// Multiplication is word-serial Montgomery (CIOS) written for the integer
+// multiply-add pipe: every 32x32 partial product is one `mad.lo`/`mad.hi`
+// inside a PTX carry chain.  The products of one row a*b_i are split by the
+// parity of the limb index of `a`: even-index products land on the word pairs
+// (0,1),(2,3),... and odd-index products on (1,2),(3,4),... so each parity is
+// one unbroken carry chain.  Two accumulators hold the running value
+// T = X + 2^32 * Y (X aligned at word 0, Y at word 1); after the reduction
+// zeroes X's low word, dividing by 2^32 is a relabelling: the next X is
+// Y + X[1] and the next Y is X shifted down two words, and that shift is folded
+// into the next row's odd chain.  This column-parity technique is the one
+// published for modular multiplication on NVIDIA GPUs by Emmart and Weems.
+//
+// Fp values are kept lazily reduced in [0, 2p): with 4p < 2^384 the
+// Montgomery product of two such values is again < 2p, so the multiply has no
+// final subtraction and add/sub fold into [0, 2p) with one conditional 2p.
+// `fp_canonical` brings a value to [0, p) for output and comparisons.
+// Fr values are always fully reduced in [0, r) (4r > 2^256 rules out laziness).
+#pragma once
+#include <cstdint>
+
+namespace mzk {
+
+// ---------------------------------------------------------------- params ----
+// Moduli: p from curves/src/bls12_381/fp.rs:20-27, r from fq.rs:43-48.
+// N0 = -m^{-1} mod 2^32, ONE = 2^(32N) mod m, R2 = 2^(64N) mod m.
+struct FpP {
+    static constexpr int N = 12;
+    static constexpr uint32_t N0 = 0xfffcfffdu;
+    __host__ __device__ static constexpr uint32_t mod(int i) {
+        return i == 0 ? 0xffffaaabu : i == 1 ? 0xb9feffffu : i == 2 ? 0xb153ffffu : i == 3 ? 0x1eabfffeu
+             : i == 4 ? 0xf6b0f624u : i == 5 ? 0x6730d2a0u : i == 6 ? 0xf38512bfu : i == 7 ? 0x64774b84u
+             : i == 8 ? 0x434bacd7u : i == 9 ? 0x4b1ba7b6u : i == 10 ? 0x397fe69au : 0x1a0111eau;
+    }
+    __host__ __device__ static constexpr uint32_t mod2(int i) {
+        return i == 0 ? 0xffff5556u : i == 1 ? 0x73fdffffu : i == 2 ? 0x62a7ffffu : i == 3 ? 0x3d57fffdu
+             : i == 4 ? 0xed61ec48u : i == 5 ? 0xce61a541u : i == 6 ? 0xe70a257eu : i == 7 ? 0xc8ee9709u
+             : i == 8 ? 0x869759aeu : i == 9 ? 0x96374f6cu : i == 10 ? 0x72ffcd34u : 0x340223d4u;
+    }
+    __host__ __device__ static constexpr uint32_t one(int i) {
+        return i == 0 ? 0x0002fffdu : i == 1 ? 0x76090000u : i == 2 ? 0xc40c0002u : i == 3 ? 0xebf4000bu
+             : i == 4 ? 0x53c758bau : i == 5 ? 0x5f489857u : i == 6 ? 0x70525745u : i == 7 ? 0x77ce5853u
+             : i == 8 ? 0xa256ec6du : i == 9 ? 0x5c071a97u : i == 10 ? 0xfa80e493u : 0x15f65ec3u;
+    }
+};
+
+struct FrP {
+    static constexpr int N = 8;
+    static constexpr uint32_t N0 = 0xffffffffu;
+    __host__ __device__ static constexpr uint32_t mod(int i) {
+        return i == 0 ? 0x00000001u : i == 1 ? 0xffffffffu : i == 2 ? 0xfffe5bfeu : i == 3 ? 0x53bda402u
+             : i == 4 ? 0x09a1d805u : i == 5 ? 0x3339d808u : i == 6 ? 0x299d7d48u : 0x73eda753u;
+    }
+    __host__ __device__ static constexpr uint32_t one(int i) {
+        return i == 0 ? 0xfffffffeu : i == 1 ? 0x00000001u : i == 2 ? 0x00034802u : i == 3 ? 0x5884b7fau
+             : i == 4 ? 0xecbc4ff5u : i == 5 ? 0x998c4fefu : i == 6 ? 0xacc5056fu : 0x1824b159u;
+    }
+    __host__ __device__ static constexpr uint32_t r2(int i) {
+        return i == 0 ? 0xf3f29c6du : i == 1 ? 0xc999e990u : i == 2 ? 0x87925c23u : i == 3 ? 0x2b6cedcbu
+             : i == 4 ? 0x7254398fu : i == 5 ? 0x05d31496u : i == 6 ? 0x9f59ff11u : 0x0748d9d9u;
+    }
+};
+
+struct Fp { uint32_t l[12]; };
+struct Fr { uint32_t l[8]; };
+
+// ------------------------------------------------------------ PTX pieces ----
+#define MZK_ASM asm volatile
+
+// Montgomery product r = a*b*2^(-32N) mod m for N-limb operands, result in
+// [0, 2m) when a, b < 2m and 4m < 2^(32N) (or a, b < m otherwise).
+template <class P>
+__device__ __forceinline__ void mont_mul_raw(uint32_t* r, const uint32_t* a, const uint32_t* b) {
+    constexpr int N = P::N;
+    uint32_t x[N + 1];  // aligned at word 0, x[N] = overflow word
+    uint32_t y[N];      // aligned at word 1
+    // row 0: plain products, even-index limbs of a into x, odd-index into y
+#pragma unroll
+    for (int j = 0; j < N; j += 2) {
+        MZK_ASM("mul.lo.u32 %0, %2, %3;\n\tmul.hi.u32 %1, %2, %3;" : "=r"(x[j]), "=r"(x[j + 1]) : "r"(a[j]), "r"(b[0]));
+        MZK_ASM("mul.lo.u32 %0, %2, %3;\n\tmul.hi.u32 %1, %2, %3;" : "=r"(y[j]), "=r"(y[j + 1]) : "r"(a[j + 1]), "r"(b[0]));
+    }
+    x[N] = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (i > 0) {
+            // divide the previous row by 2^32 while adding a*b_i:
+            //   new x = y + x[1] + even products, new y = x>>64 + odd products
+            uint32_t nx[N + 1], ny[N];
+            const uint32_t bi = b[i];
+            MZK_ASM("add.cc.u32 %0, %1, %2;" : "=r"(nx[0]) : "r"(y[0]), "r"(x[1]));
+#pragma unroll
+            for (int k = 0; k < N - 2; k += 2) {
+                MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %4;\n\tmadc.hi.cc.u32 %1, %2, %3, %5;"
+                        : "=r"(ny[k]), "=r"(ny[k + 1]) : "r"(a[k + 1]), "r"(bi), "r"(x[k + 2]), "r"(x[k + 3]));
+            }
+            MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %4;\n\tmadc.hi.u32 %1, %2, %3, 0;"
+                    : "=r"(ny[N - 2]), "=r"(ny[N - 1]) : "r"(a[N - 1]), "r"(bi), "r"(x[N]));
+            MZK_ASM("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %4;"
+                    : "+r"(nx[0]), "=r"(nx[1]) : "r"(a[0]), "r"(bi), "r"(y[1]));
+#pragma unroll
+            for (int j = 2; j < N; j += 2) {
+                MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %4;\n\tmadc.hi.cc.u32 %1, %2, %3, %5;"
+                        : "=r"(nx[j]), "=r"(nx[j + 1]) : "r"(a[j]), "r"(bi), "r"(y[j]), "r"(j + 1 < N ? y[j + 1] : 0u));
+            }
+            MZK_ASM("addc.u32 %0, 0, 0;" : "=r"(nx[N]));
+#pragma unroll
+            for (int j = 0; j <= N; j++) x[j] = nx[j];
+#pragma unroll
+            for (int j = 0; j < N; j++) y[j] = ny[j];
+        }
+        // reduction: m zeroes word 0 of x
+        const uint32_t m = x[0] * P::N0;
+        MZK_ASM("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                : "+r"(x[0]), "+r"(x[1]) : "r"(m), "r"(P::mod(0)));
+#pragma unroll
+        for (int j = 2; j < N; j += 2) {
+            MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                    : "+r"(x[j]), "+r"(x[j + 1]) : "r"(m), "r"(P::mod(j)));
+        }
+        MZK_ASM("addc.u32 %0, %0, 0;" : "+r"(x[N]));
+        MZK_ASM("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                : "+r"(y[0]), "+r"(y[1]) : "r"(m), "r"(P::mod(1)));
+#pragma unroll
+        for (int j = 3; j < N - 1; j += 2) {
+            MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                    : "+r"(y[j - 1]), "+r"(y[j]) : "r"(m), "r"(P::mod(j)));
+        }
+        MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.u32 %1, %2, %3, %1;"
+                : "+r"(y[N - 2]), "+r"(y[N - 1]) : "r"(m), "r"(P::mod(N - 1)));
+    }
+    // final division by 2^32: r = y + (x >> 32)
+    MZK_ASM("add.cc.u32 %0, %1, %2;" : "=r"(r[0]) : "r"(y[0]), "r"(x[1]));
+#pragma unroll
+    for (int j = 1; j < N - 1; j++) MZK_ASM("addc.cc.u32 %0, %1, %2;" : "=r"(r[j]) : "r"(y[j]), "r"(x[j + 1]));
+    MZK_ASM("addc.u32 %0, %1, %2;" : "=r"(r[N - 1]) : "r"(y[N - 1]), "r"(x[N]));
+}
+
+// r = a + b (N limbs), returns nothing; caller guarantees no overflow
+template <int N>
+__device__ __forceinline__ void add_n(uint32_t* r, const uint32_t* a, const uint32_t* b) {
+    MZK_ASM("add.cc.u32 %0, %1, %2;" : "=r"(r[0]) : "r"(a[0]), "r"(b[0]));
+#pragma unroll
+    for (int j = 1; j < N - 1; j++) MZK_ASM("addc.cc.u32 %0, %1, %2;" : "=r"(r[j]) : "r"(a[j]), "r"(b[j]));
+    MZK_ASM("addc.u32 %0, %1, %2;" : "=r"(r[N - 1]) : "r"(a[N - 1]), "r"(b[N - 1]));
+}
+// r = a - b, returns borrow mask (0 or 0xffffffff)
+template <int N>
+__device__ __forceinline__ uint32_t sub_n(uint32_t* r, const uint32_t* a, const uint32_t* b) {
+    uint32_t bw;
+    MZK_ASM("sub.cc.u32 %0, %1, %2;" : "=r"(r[0]) : "r"(a[0]), "r"(b[0]));
+#pragma unroll
+    for (int j = 1; j < N; j++) MZK_ASM("subc.cc.u32 %0, %1, %2;" : "=r"(r[j]) : "r"(a[j]), "r"(b[j]));
+    MZK_ASM("subc.u32 %0, 0, 0;" : "=r"(bw));
+    return bw;
+}
+// r = t - M if t >= M else t, with M given limb-wise by the functor
+template <int N, class ModF>
+__device__ __forceinline__ void cond_sub(uint32_t* r, const uint32_t* t, ModF modf) {
+    uint32_t s[N], bw;
+    MZK_ASM("sub.cc.u32 %0, %1, %2;" : "=r"(s[0]) : "r"(t[0]), "r"(modf(0)));
+#pragma unroll
+    for (int j = 1; j < N; j++) MZK_ASM("subc.cc.u32 %0, %1, %2;" : "=r"(s[j]) : "r"(t[j]), "r"(modf(j)));
+    MZK_ASM("subc.u32 %0, 0, 0;" : "=r"(bw));
+#pragma unroll
+    for (int j = 0; j < N; j++) r[j] = (t[j] & bw) | (s[j] & ~bw);
+}
+// r = t + (M & mask)
+template <int N, class ModF>
+__device__ __forceinline__ void add_masked(uint32_t* r, const uint32_t* t, uint32_t mask, ModF modf) {
+    MZK_ASM("add.cc.u32 %0, %1, %2;" : "=r"(r[0]) : "r"(t[0]), "r"(modf(0) & mask));
+#pragma unroll
+    for (int j = 1; j < N - 1; j++) MZK_ASM("addc.cc.u32 %0, %1, %2;" : "=r"(r[j]) : "r"(t[j]), "r"(modf(j) & mask));
+    MZK_ASM("addc.u32 %0, %1, %2;" : "=r"(r[N - 1]) : "r"(t[N - 1]), "r"(modf(N - 1) & mask));
+}
+
+// -------------------------------------------------------------------- Fp ----
+struct FpMod { __device__ __forceinline__ uint32_t operator()(int i) const { return FpP::mod(i); } };
+struct FpMod2 { __device__ __forceinline__ uint32_t operator()(int i) const { return FpP::mod2(i); } };
+
+__device__ __forceinline__ Fp fp_mul(const Fp& a, const Fp& b) {
+    Fp r;
+    mont_mul_raw<FpP>(r.l, a.l, b.l);
+    return r;
+}
+__device__ __forceinline__ Fp fp_sqr(const Fp& a) { return fp_mul(a, a); }
+__device__ __forceinline__ Fp fp_add(const Fp& a, const Fp& b) {
+    Fp t, r;
+    add_n<12>(t.l, a.l, b.l);
+    cond_sub<12>(r.l, t.l, FpMod2());
+    return r;
+}
+__device__ __forceinline__ Fp fp_sub(const Fp& a, const Fp& b) {
+    Fp t, r;
+    uint32_t bw = sub_n<12>(t.l, a.l, b.l);
+    add_masked<12>(r.l, t.l, bw, FpMod2());
+    return r;
+}
+__device__ __forceinline__ Fp fp_dbl(const Fp& a) { return fp_add(a, a); }
+__device__ __forceinline__ Fp fp_neg(const Fp& a) {
+    Fp z;
+#pragma unroll
+    for (int j = 0; j < 12; j++) z.l[j] = 0;
+    return fp_sub(z, a);
+}
+// [0, 2p) -> [0, p)
+__device__ __forceinline__ Fp fp_canonical(const Fp& a) {
+    Fp r;
+    cond_sub<12>(r.l, a.l, FpMod());
+    return r;
+}
+__device__ __forceinline__ bool fp_is_zero_raw(const Fp& a) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int j = 0; j < 12; j++) acc |= a.l[j];
+    return acc == 0;
+}
+// zero modulo p for a lazily reduced value
+__device__ __forceinline__ bool fp_is_zero(const Fp& a) { return fp_is_zero_raw(fp_canonical(a)); }
+__device__ __forceinline__ Fp fp_zero() {
+    Fp r;
+#pragma unroll
+    for (int j = 0; j < 12; j++) r.l[j] = 0;
+    return r;
+}
+__device__ __forceinline__ Fp fp_one() {
+    Fp r;
+#pragma unroll
+    for (int j = 0; j < 12; j++) r.l[j] = FpP::one(j);
+    return r;
+}
+// a^(p-2) by square-and-multiply over the constant exponent p-2 (Fermat);
+// used for single-point normalisation only.
+static __device__ __noinline__ Fp fp_inv(const Fp& a) {
+    Fp acc = fp_one();
+    for (int i = 11; i >= 0; i--) {
+        const uint32_t e = FpP::mod(i) - (i == 0 ? 2u : 0u);
+        for (int bit = 31; bit >= 0; bit--) {
+            acc = fp_sqr(acc);
+            if ((e >> bit) & 1u) acc = fp_mul(acc, a);
+        }
+    }
+    return acc;
+}
+
+// -------------------------------------------------------------------- Fr ----
+struct FrMod { __device__ __forceinline__ uint32_t operator()(int i) const { return FrP::mod(i); } };
+
+__device__ __forceinline__ Fr fr_mul(const Fr& a, const Fr& b) {
+    Fr t, r;
+    mont_mul_raw<FrP>(t.l, a.l, b.l);
+    cond_sub<8>(r.l, t.l, FrMod());
+    return r;
+}
+__device__ __forceinline__ Fr fr_add(const Fr& a, const Fr& b) {
+    Fr t, r;
+    add_n<8>(t.l, a.l, b.l);
+    cond_sub<8>(r.l, t.l, FrMod());
+    return r;
+}
+__device__ __forceinline__ Fr fr_sub(const Fr& a, const Fr& b) {
+    Fr t, r;
+    uint32_t bw = sub_n<8>(t.l, a.l, b.l);
+    add_masked<8>(r.l, t.l, bw, FrMod());
+    return r;
+}
+__device__ __forceinline__ Fr fr_one() {
+    Fr r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.l[j] = FrP::one(j);
+    return r;
+}
+__device__ __forceinline__ Fr fr_zero() {
+    Fr r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.l[j] = 0;
+    return r;
+}
+// Montgomery -> canonical integer (to_repr): multiply by 1
+__device__ __forceinline__ Fr fr_from_mont(const Fr& a) {
+    Fr one_raw;
+#pragma unroll
+    for (int j = 0; j < 8; j++) one_raw.l[j] = j == 0 ? 1u : 0u;
+    return fr_mul(a, one_raw);
+}
+// canonical integer -> Montgomery: multiply by R^2
+__device__ __forceinline__ Fr fr_to_mont(const Fr& a) {
+    Fr r2;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r2.l[j] = FrP::r2(j);
+    return fr_mul(a, r2);
+}
+
+}  // namespace mzk

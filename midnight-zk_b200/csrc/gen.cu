@@ -1,0 +1,133 @@
+// gen.cu — seeded synthetic inputs generated on the device.
+//
+// Benchmarks and tests need 2^24 uniform scalars and bases [r_i]G; building
+// them on the host would take minutes.  Element i depends only on (seed, i),
+// so any slice can be regenerated anywhere (the C oracle implements the same
+// generator for the parity checks):
+//   word ctr of stream `seed` = SplitMix64 finaliser of seed + (ctr+1)*golden
+//   uniform Fr: rejection sampling as Fq::random (curves/src/bls12_381/
+//               fq.rs:382-396), attempt a of element i uses words (i*64+a)*4..+3
+//   bases: [r_i]G by an 8-bit fixed-base table of the generator G
+//          (curves/README.md:96-101), normalised to affine per point.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+#include "ec.cuh"
+#include "host_ec.hpp"
+#include "runtime.hpp"
+
+namespace mzk {
+
+namespace {
+
+__device__ __forceinline__ uint64_t rand64(uint64_t seed, uint64_t ctr) {
+    uint64_t z = seed + (ctr + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// canonical uniform element of [0, r)
+__device__ Fr rand_fr_canonical(uint64_t seed, uint64_t i) {
+    Fr out = fr_zero();
+    for (uint64_t a = 0; a < 64; a++) {
+        uint32_t w[8];
+        for (int k = 0; k < 4; k++) {
+            uint64_t v = rand64(seed, (i * 64 + a) * 4 + (uint64_t)k);
+            if (k == 3) v &= 0x7fffffffffffffffull;
+            w[2 * k] = (uint32_t)v;
+            w[2 * k + 1] = (uint32_t)(v >> 32);
+        }
+        // accept if w < r
+        bool less = false, decided = false;
+        for (int k = 7; k >= 0 && !decided; k--) {
+            if (w[k] != FrP::mod(k)) {
+                less = w[k] < FrP::mod(k);
+                decided = true;
+            }
+        }
+        if (decided && less) {
+            for (int k = 0; k < 8; k++) out.l[k] = w[k];
+            return out;
+        }
+    }
+    return out;
+}
+
+__global__ void k_rand_fr(uint64_t seed, uint64_t first, size_t n, Fr* __restrict__ out) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = fr_to_mont(rand_fr_canonical(seed, first + i));
+}
+
+__global__ void __launch_bounds__(128) k_gen_bases(uint64_t seed, uint64_t first, size_t n,
+                                                   const Affine* __restrict__ table, Affine* __restrict__ out) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Fr r = rand_fr_canonical(seed, first + i);
+        Xyzz acc;
+        xyzz_set_inf(acc);
+        for (int j = 0; j < 32; j++) {
+            const uint32_t v = (r.l[j >> 2] >> (8 * (j & 3))) & 0xffu;
+            if (v) xyzz_add_affine(acc, load_affine(table, (uint32_t)(j * 256) + v));
+        }
+        out[i] = xyzz_to_affine(acc);
+    }
+}
+
+// G1 generator, canonical coordinates (curves/README.md:96-101)
+const uint64_t kGenX[6] = {0xfb3af00adb22c6bbULL, 0x6c55e83ff97a1aefULL, 0xa14e3a3f171bac58ULL,
+                           0xc3688c4f9774b905ULL, 0x2695638c4fa9ac0fULL, 0x17f1d3a73197d794ULL};
+const uint64_t kGenY[6] = {0x0caa232946c5e7e1ULL, 0xd03cc744a2888ae4ULL, 0x00db18cb2c04b3edULL,
+                           0xfcf5e095d5d00af6ULL, 0xa09e30ed741d8ae4ULL, 0x08b3f481e3aaa0f1ULL};
+const uint64_t kFpR2[6] = {0xf4df1f341c341746ULL, 0x0a76e6a609d104f1ULL, 0x8de5476c4c95b6d5ULL,
+                           0x67eb88a9939d83c0ULL, 0x9a793e85b519952dULL, 0x11988fe592cae3aaULL};
+
+Status ensure_gen_table(Context* ctx) {
+    if (ctx->gen_table) return OK;
+    host::Fp6 r2, gx, gy;
+    std::memcpy(r2.l, kFpR2, 48);
+    std::memcpy(gx.l, kGenX, 48);
+    std::memcpy(gy.l, kGenY, 48);
+    host::Xyzz6 base{host::mul(gx, r2), host::mul(gy, r2), host::one(), host::one()};
+    std::vector<uint64_t> table((size_t)32 * 256 * 12, 0);
+    for (int j = 0; j < 32; j++) {
+        host::Xyzz6 acc = host::infinity();
+        for (int v = 1; v < 256; v++) {
+            acc = host::add(acc, base);
+            uint64_t jac[18];
+            host::to_jacobian_normalised(acc, jac);
+            std::memcpy(&table[((size_t)j * 256 + v) * 12], jac, 96);
+        }
+        for (int b = 0; b < 8; b++) base = host::dbl(base);
+    }
+    void* d;
+    MZK_CUDA_CHECK(cudaMalloc(&d, table.size() * 8));
+    MZK_CUDA_CHECK(cudaMemcpy(d, table.data(), table.size() * 8, cudaMemcpyHostToDevice));
+    ctx->gen_table = d;
+    return OK;
+}
+
+}  // namespace
+
+Status gen_rand_fr(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t st) {
+    if (n == 0) return OK;
+    const uint32_t blocks = (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 32);
+    k_rand_fr<<<blocks, 256, 0, st>>>(seed, first, n, static_cast<Fr*>(d_out));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+Status gen_bases_g1(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t st) {
+    if (n == 0) return OK;
+    MZK_TRY(ensure_gen_table(ctx));
+    const uint32_t blocks = (uint32_t)std::min<size_t>((n + 127) / 128, (size_t)ctx->num_sms * 16);
+    k_gen_bases<<<blocks, 128, 0, st>>>(seed, first, n, static_cast<const Affine*>(ctx->gen_table),
+                                        static_cast<Affine*>(d_out));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+}  // namespace mzk

@@ -1,0 +1,518 @@
+// msm.cu — Pippenger multi-scalar multiplication over BLS12-381 G1.
+//
+// Replaces curves::msm::msm_best (curves/src/msm.rs:460-532) and the
+// blst Pippenger behind G1Affine::multi_exp_affine (g1.rs:427-446) that
+// proofs::poly::kzg::msm::msm_specific (kzg/msm.rs:174-201) dispatches to.
+// The result is the same group element; the schedule is built for the GPU:
+//
+//  1. histogram   one thread per scalar: Montgomery -> canonical (one Fr
+//                 multiplication by 1, the reference's `to_repr`), signed
+//                 c-bit window digits d_w in [-2^(c-1), 2^(c-1)], count of
+//                 entries per key (window, |d|-1) with warp-aggregated atomics.
+//  2. scan        exclusive prefix sum of the counts = start of every bucket
+//                 in the sorted entry array (a counting sort).
+//  3. scatter     digits recomputed, each (point index | sign) written to its
+//                 bucket's slice.  Zero digits produce no entry, so zero and
+//                 sparse scalars cost nothing (msm_specific drops zero scalars).
+//  4. accumulate  the sorted entries split into equal chunks, one per thread:
+//                 every thread walks its chunk adding points into an XYZZ
+//                 accumulator (mixed addition, affine bases gathered from HBM).
+//                 Buckets entirely inside a chunk are written directly; a bucket
+//                 cut by a chunk edge leaves partial sums.  Equal chunks keep
+//                 every thread busy whatever the scalar distribution.
+//  5. fixup       the chunk where a cut bucket starts sums its partials.
+//  6. reduce      per window, sum_b (b+1) B_b: running sums over groups of 16
+//                 buckets (one thread per group), then the weighted group sums
+//                 sum_g g R_g by bit planes (plain tree sums), one block each.
+//  7. finish      one thread per window folds the planes into the window sum.
+//  8. host        sum_w 2^(c w) S_w (c doublings between windows) and the
+//                 affine normalisation on the host: a few hundred group
+//                 operations that one GPU thread would take ~1 ms for.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ec.cuh"
+#include "host_ec.hpp"
+#include "runtime.hpp"
+
+namespace mzk {
+
+namespace {
+
+constexpr int kGroupLen = 16;      // buckets per running-sum group
+constexpr int kAccThreads = 128;   // threads per block of the accumulate kernel
+constexpr int kReduceThreads = 128;
+constexpr uint32_t kNoKey = 0xffffffffu;
+
+struct MsmShape {
+    int c;          // window width in bits
+    int windows;    // number of windows
+    uint32_t nb;    // buckets per window = 2^(c-1)
+    uint32_t keys;  // windows * nb
+    uint32_t groups;  // running-sum groups per window = nb / kGroupLen
+    int planes;     // log2(groups)
+};
+
+MsmShape make_shape(int c) {
+    MsmShape s;
+    s.c = c;
+    s.windows = (256 + c - 1) / c;
+    s.nb = 1u << (c - 1);
+    s.keys = s.nb * (uint32_t)s.windows;
+    s.groups = s.nb / kGroupLen;
+    s.planes = 0;
+    while ((1u << s.planes) < s.groups) s.planes++;
+    return s;
+}
+
+__device__ __forceinline__ uint32_t fr_limb(const Fr& s, int i) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) v = (i == j) ? s.l[j] : v;
+    return v;
+}
+
+// bits [bit, bit + c) of the canonical scalar, c <= 31
+__device__ __forceinline__ uint32_t window_bits(const Fr& s, int bit, int c) {
+    const int limb = bit >> 5, sh = bit & 31;
+    uint64_t v = (uint64_t)fr_limb(s, limb) | ((uint64_t)fr_limb(s, limb + 1) << 32);
+    return (uint32_t)(v >> sh) & ((1u << c) - 1u);
+}
+
+__device__ __forceinline__ Fr load_fr(const Fr* p, size_t i) {
+    const uint4* src = reinterpret_cast<const uint4*>(p + i);
+    uint4 a = __ldg(src), b = __ldg(src + 1);
+    Fr r;
+    r.l[0] = a.x; r.l[1] = a.y; r.l[2] = a.z; r.l[3] = a.w;
+    r.l[4] = b.x; r.l[5] = b.y; r.l[6] = b.z; r.l[7] = b.w;
+    return r;
+}
+
+// Signed digit recoding: returns key (window * nb + |d| - 1) or kNoKey for a
+// zero digit, and the sign; carries between windows through `carry`.
+__device__ __forceinline__ uint32_t next_digit(const Fr& s, int w, int c, uint32_t nb, uint32_t& carry, bool& neg) {
+    uint32_t v = window_bits(s, w * c, c) + carry;
+    uint32_t mag;
+    if (v > nb) {  // v - 2^c is negative
+        mag = (1u << c) - v;
+        carry = 1;
+        neg = true;
+    } else {
+        mag = v;
+        carry = 0;
+        neg = false;
+    }
+    return mag == 0 ? kNoKey : (uint32_t)w * nb + (mag - 1);
+}
+
+__global__ void k_histogram(const Fr* __restrict__ scalars, size_t n, int c, int windows, uint32_t nb,
+                            uint32_t* __restrict__ counts) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const size_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        Fr s = valid ? fr_from_mont(load_fr(scalars, i)) : fr_zero();
+        uint32_t carry = 0;
+        for (int w = 0; w < windows; w++) {
+            bool neg;
+            uint32_t key = next_digit(s, w, c, nb, carry, neg);
+            if (!valid) key = kNoKey;
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            if (key != kNoKey && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
+        }
+    }
+}
+
+__global__ void k_scatter(const Fr* __restrict__ scalars, size_t n, int c, int windows, uint32_t nb,
+                          const uint32_t* __restrict__ offsets, uint32_t* __restrict__ fill,
+                          uint32_t* __restrict__ sorted) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const size_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        Fr s = valid ? fr_from_mont(load_fr(scalars, i)) : fr_zero();
+        uint32_t carry = 0;
+        for (int w = 0; w < windows; w++) {
+            bool neg;
+            uint32_t key = next_digit(s, w, c, nb, carry, neg);
+            if (!valid) key = kNoKey;
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            const int leader = __ffs(peers) - 1;
+            uint32_t slot = 0;
+            if (key != kNoKey && lane == leader) slot = atomicAdd(&fill[key], (uint32_t)__popc(peers));
+            slot = __shfl_sync(peers, slot, leader);
+            if (key != kNoKey) {
+                const uint32_t pos = offsets[key] + slot + (uint32_t)__popc(peers & lt_mask);
+                sorted[pos] = (uint32_t)i | (neg ? 0x80000000u : 0u);
+            }
+        }
+    }
+}
+
+// ---- exclusive scan of u32 (3 phases) ----
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem_warp, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) smem_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < (int)(blockDim.x >> 5) ? smem_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        smem_warp[lane] = w;
+    }
+    __syncthreads();
+    total = smem_warp[(blockDim.x >> 5) - 1];
+    uint32_t prefix = warp > 0 ? smem_warp[warp - 1] : 0;
+    __syncthreads();
+    return prefix + x - v;
+}
+
+__global__ void k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t len,
+                             uint32_t* __restrict__ tile_sums) {
+    __shared__ uint32_t sw[32];
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = base + k < len ? in[base + k] : 0;
+        sum += v[k];
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(sum, sw, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < len) out[base + k] = pre;
+        pre += v[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_sums(uint32_t* __restrict__ tile_sums, uint32_t tiles) {
+    __shared__ uint32_t sw[32];
+    uint32_t carry = 0;
+    for (uint32_t b = 0; b < tiles; b += blockDim.x) {
+        const uint32_t i = b + threadIdx.x;
+        uint32_t v = i < tiles ? tile_sums[i] : 0, total;
+        uint32_t pre = block_exclusive_scan(v, sw, total);
+        if (i < tiles) tile_sums[i] = pre + carry;
+        carry += total;
+    }
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t len, const uint32_t* __restrict__ tile_sums) {
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    const uint32_t add = tile_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+        if (base + k < len) out[base + k] += add;
+}
+
+// ---- bucket accumulation ----
+__device__ __forceinline__ uint32_t find_key(const uint32_t* offsets, uint32_t keys, uint32_t pos) {
+    // largest k in [0, keys) with offsets[k] <= pos (offsets[keys] = total > pos)
+    uint32_t lo = 0, hi = keys;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (offsets[mid] <= pos) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void store_xyzz(Xyzz* dst, const Xyzz& v) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(&v);
+#pragma unroll
+    for (int k = 0; k < 12; k++) d[k] = make_uint4(s[4 * k], s[4 * k + 1], s[4 * k + 2], s[4 * k + 3]);
+}
+__device__ __forceinline__ Xyzz load_xyzz(const Xyzz* src) {
+    Xyzz v;
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&v);
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        uint4 q = s[k];
+        d[4 * k] = q.x;
+        d[4 * k + 1] = q.y;
+        d[4 * k + 2] = q.z;
+        d[4 * k + 3] = q.w;
+    }
+    return v;
+}
+
+__device__ __forceinline__ void chunk_range(uint32_t total, uint32_t t, uint32_t nthreads, uint32_t& s, uint32_t& e) {
+    const uint32_t len = (total + nthreads - 1) / nthreads;
+    s = min(total, t * len);
+    e = min(total, s + len);
+}
+
+__global__ void __launch_bounds__(kAccThreads) k_accumulate(const Affine* __restrict__ bases,
+                                                            const uint32_t* __restrict__ sorted,
+                                                            const uint32_t* __restrict__ offsets, uint32_t keys,
+                                                            Xyzz* __restrict__ buckets, Xyzz* __restrict__ partials,
+                                                            int* __restrict__ owner_key) {
+    const uint32_t nthreads = gridDim.x * blockDim.x;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t total = offsets[keys];
+    uint32_t s, e;
+    chunk_range(total, t, nthreads, s, e);
+    owner_key[t] = -1;
+    if (s >= e) return;
+    uint32_t k = find_key(offsets, keys, s);
+    uint32_t pos = s;
+    while (pos < e) {
+        const uint32_t seg_lo = offsets[k], seg_hi = offsets[k + 1];
+        const uint32_t end = min(seg_hi, e);
+        Xyzz acc;
+        xyzz_set_inf(acc);
+        for (uint32_t j = pos; j < end; j++) {
+            const uint32_t ent = __ldg(sorted + j);
+            Affine p = load_affine(bases, ent & 0x7fffffffu);
+            if (aff_is_inf(p)) continue;
+            if (ent >> 31) p.y = fp_neg(p.y);
+            xyzz_add_affine(acc, p);
+        }
+        if (seg_lo >= s && seg_hi <= e) {
+            store_xyzz(&buckets[k], acc);
+        } else if (seg_lo < s) {
+            store_xyzz(&partials[2 * (size_t)t], acc);
+        } else {
+            store_xyzz(&partials[2 * (size_t)t + 1], acc);
+            owner_key[t] = (int)k;
+        }
+        pos = end;
+        // next non-empty key
+        k++;
+        while (k < keys && offsets[k + 1] <= pos) k++;
+    }
+}
+
+__global__ void k_fixup(const uint32_t* __restrict__ offsets, uint32_t keys, const Xyzz* __restrict__ partials,
+                        const int* __restrict__ owner_key, Xyzz* __restrict__ buckets) {
+    const uint32_t nthreads = gridDim.x * blockDim.x;  // same grid as k_accumulate
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = owner_key[t];
+    if (k < 0) return;
+    const uint32_t total = offsets[keys];
+    const uint32_t len = (total + nthreads - 1) / nthreads;
+    const uint32_t last = (offsets[k + 1] - 1) / len;
+    Xyzz acc = load_xyzz(&partials[2 * (size_t)t + 1]);
+    for (uint32_t u = t + 1; u <= last; u++) acc = xyzz_add(acc, load_xyzz(&partials[2 * (size_t)u]));
+    store_xyzz(&buckets[k], acc);
+}
+
+// per (window, group): running sum over kGroupLen buckets, top first
+__global__ void __launch_bounds__(kReduceThreads) k_group_sums(const Xyzz* __restrict__ buckets,
+                                                               const uint32_t* __restrict__ offsets, uint32_t nb,
+                                                               uint32_t groups, uint32_t total_groups,
+                                                               Xyzz* __restrict__ run_out, Xyzz* __restrict__ tot_out) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= total_groups) return;
+    const uint32_t w = gid / groups, g = gid % groups;
+    const uint32_t key0 = w * nb + g * kGroupLen;
+    Xyzz run, tot;
+    xyzz_set_inf(run);
+    xyzz_set_inf(tot);
+    for (int b = kGroupLen - 1; b >= 0; b--) {
+        const uint32_t key = key0 + (uint32_t)b;
+        if (offsets[key + 1] > offsets[key]) run = xyzz_add(run, load_xyzz(&buckets[key]));
+        tot = xyzz_add(tot, run);
+    }
+    store_xyzz(&run_out[gid], run);
+    store_xyzz(&tot_out[gid], tot);
+}
+
+// one block per (window, plane): plane < planes sums R_g over g with bit
+// `plane` set; plane == planes sums T_g over all g.
+__global__ void __launch_bounds__(kReduceThreads) k_plane_sums(const Xyzz* __restrict__ run, const Xyzz* __restrict__ tot,
+                                                               uint32_t groups, int planes, Xyzz* __restrict__ plane_out) {
+    extern __shared__ uint4 smem_raw[];
+    Xyzz* sm = reinterpret_cast<Xyzz*>(smem_raw);
+    const int plane = blockIdx.x % (planes + 1);
+    const uint32_t w = blockIdx.x / (planes + 1);
+    const Xyzz* src = (plane == planes ? tot : run) + (size_t)w * groups;
+    Xyzz acc;
+    xyzz_set_inf(acc);
+    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
+        if (plane == planes || ((g >> plane) & 1u)) acc = xyzz_add(acc, load_xyzz(&src[g]));
+    }
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) sm[threadIdx.x] = xyzz_add(sm[threadIdx.x], sm[threadIdx.x + off]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) store_xyzz(&plane_out[blockIdx.x], sm[0]);
+}
+
+// window sum S_w = T + kGroupLen * sum_j 2^j Q_j
+__global__ void k_window_finish(const Xyzz* __restrict__ planes_in, int planes, int windows, Xyzz* __restrict__ out) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= windows) return;
+    const Xyzz* q = planes_in + (size_t)w * (planes + 1);
+    Xyzz acc;
+    xyzz_set_inf(acc);
+    for (int j = planes - 1; j >= 0; j--) {
+        acc = xyzz_dbl(acc);
+        acc = xyzz_add(acc, load_xyzz(&q[j]));
+    }
+    for (int b = 1; b < kGroupLen; b <<= 1) acc = xyzz_dbl(acc);
+    acc = xyzz_add(acc, load_xyzz(&q[planes]));
+    store_xyzz(&out[w], acc);
+}
+
+Status scan_u32(Context* ctx, const uint32_t* in, uint32_t* out, uint32_t len, cudaStream_t st) {
+    const uint32_t tiles = (len + kScanTile - 1) / kScanTile;
+    void* sums;
+    MZK_TRY(ctx->ensure("scan_sums", (size_t)tiles * 4 + 64, &sums));
+    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(in, out, len, (uint32_t*)sums);
+    MZK_LAUNCH_CHECK(ctx);
+    k_scan_sums<<<1, kScanThreads, 0, st>>>((uint32_t*)sums, tiles);
+    MZK_LAUNCH_CHECK(ctx);
+    k_scan_add<<<tiles, kScanThreads, 0, st>>>(out, len, (const uint32_t*)sums);
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+}  // namespace
+
+// Window width by a cost model: W = ceil(256/c) windows of n mixed additions
+// (10 Fp mul) plus 2 * 2^(c-1) full additions (14 Fp mul) for the bucket sums.
+int msm_pick_window(size_t n) {
+    double best = 1e300;
+    int bc = 8;
+    for (int c = 6; c <= 20; c++) {
+        const int w = (256 + c - 1) / c;
+        const double cost = (double)w * ((double)n * 10.0 + (double)(1u << c) * 14.0 + 2048.0);
+        if (cost < best) {
+            best = cost;
+            bc = c;
+        }
+    }
+    return bc;
+}
+
+Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
+                     cudaStream_t st, cudaEvent_t bases_ready) {
+    std::memset(out18, 0, 18 * 8);
+    if (n == 0) return OK;
+    if (n >= 0x80000000ull) {
+        set_error("msm: n must be < 2^31");
+        return ERR_ARG;
+    }
+    const int c = ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(n);
+    if (c < 5 || c > 24) {
+        set_error("msm: window width must be in [5, 24]");
+        return ERR_ARG;
+    }
+    const MsmShape sh = make_shape(c);
+    const size_t entries_cap = (size_t)sh.windows * n;
+    if (entries_cap >= 0xffffffffull) {
+        set_error("msm: n * windows exceeds 2^32 entries");
+        return ERR_ARG;
+    }
+    // accumulate grid: persistent, sized to fill the GPU once
+    int acc_blocks_per_sm = 0;
+    MZK_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&acc_blocks_per_sm, k_accumulate, kAccThreads, 0));
+    if (acc_blocks_per_sm < 1) acc_blocks_per_sm = 1;
+    const uint32_t acc_blocks = (uint32_t)(ctx->num_sms * acc_blocks_per_sm);
+    const uint32_t acc_threads = acc_blocks * kAccThreads;
+
+    void *counts, *offsets, *sorted, *buckets, *partials, *owner, *run, *tot, *planes, *wsum;
+    MZK_TRY(ctx->ensure("msm_counts", ((size_t)sh.keys + 1) * 4, &counts));
+    MZK_TRY(ctx->ensure("msm_offsets", ((size_t)sh.keys + 1) * 4, &offsets));
+    MZK_TRY(ctx->ensure("msm_sorted", entries_cap * 4, &sorted));
+    MZK_TRY(ctx->ensure("msm_buckets", (size_t)sh.keys * sizeof(Xyzz), &buckets));
+    MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
+    MZK_TRY(ctx->ensure("msm_owner", (size_t)acc_threads * 4, &owner));
+    const size_t total_groups = (size_t)sh.groups * sh.windows;
+    MZK_TRY(ctx->ensure("msm_run", total_groups * sizeof(Xyzz), &run));
+    MZK_TRY(ctx->ensure("msm_tot", total_groups * sizeof(Xyzz), &tot));
+    const size_t nplanes = (size_t)sh.windows * (sh.planes + 1);
+    MZK_TRY(ctx->ensure("msm_planes", nplanes * sizeof(Xyzz), &planes));
+    MZK_TRY(ctx->ensure("msm_wsum", (size_t)sh.windows * sizeof(Xyzz), &wsum));
+    void* host_wsum;
+    MZK_TRY(ctx->ensure_pinned((size_t)sh.windows * sizeof(Xyzz) + 64, &host_wsum));
+
+    const Fr* sc = static_cast<const Fr*>(d_scalars);
+    const Affine* ba = static_cast<const Affine*>(d_bases);
+    const int pt_threads = 256;
+    const uint32_t pt_blocks = (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)ctx->num_sms * 16);
+
+    MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
+    k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)counts);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_SCAN, st));
+    MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets, sh.keys + 1, st));
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
+    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (const uint32_t*)offsets,
+                                                (uint32_t*)counts, (uint32_t*)sorted);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    if (bases_ready) MZK_CUDA_CHECK(cudaStreamWaitEvent(st, bases_ready, 0));
+    MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
+    k_accumulate<<<acc_blocks, kAccThreads, 0, st>>>(ba, (const uint32_t*)sorted, (const uint32_t*)offsets, sh.keys,
+                                                    (Xyzz*)buckets, (Xyzz*)partials, (int*)owner);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_FIXUP, st));
+    k_fixup<<<acc_blocks, kAccThreads, 0, st>>>((const uint32_t*)offsets, sh.keys, (const Xyzz*)partials,
+                                               (const int*)owner, (Xyzz*)buckets);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
+    const uint32_t gblocks = (uint32_t)((total_groups + kReduceThreads - 1) / kReduceThreads);
+    k_group_sums<<<gblocks, kReduceThreads, 0, st>>>((const Xyzz*)buckets, (const uint32_t*)offsets, sh.nb, sh.groups,
+                                                    (uint32_t)total_groups, (Xyzz*)run, (Xyzz*)tot);
+    MZK_LAUNCH_CHECK(ctx);
+    k_plane_sums<<<(uint32_t)nplanes, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
+        (const Xyzz*)run, (const Xyzz*)tot, sh.groups, sh.planes, (Xyzz*)planes);
+    MZK_LAUNCH_CHECK(ctx);
+    k_window_finish<<<(sh.windows + 31) / 32, 32, 0, st>>>((const Xyzz*)planes, sh.planes, sh.windows, (Xyzz*)wsum);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(host_wsum, wsum, (size_t)sh.windows * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
+    uint32_t* host_entries = reinterpret_cast<uint32_t*>(static_cast<char*>(host_wsum) + (size_t)sh.windows * sizeof(Xyzz));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(host_entries, (const uint32_t*)offsets + sh.keys, 4, cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    ctx->phase_collect();
+    ctx->last_c = sh.c;
+    ctx->last_windows = sh.windows;
+    ctx->last_entries = *host_entries;
+
+    // host: sum_w 2^(c w) S_w by Horner, then normalise
+    const host::Xyzz6* hs = static_cast<const host::Xyzz6*>(host_wsum);
+    host::Xyzz6 acc = host::infinity();
+    for (int w = sh.windows - 1; w >= 0; w--) {
+        for (int b = 0; b < sh.c; b++) acc = host::dbl(acc);
+        acc = host::add(acc, host::canon(hs[w]));
+    }
+    host::to_jacobian_normalised(acc, out18);
+    return OK;
+}
+
+}  // namespace mzk

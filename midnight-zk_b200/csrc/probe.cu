@@ -1,0 +1,100 @@
+// probe.cu — microbenchmarks for the roofline denominators of the integer
+// kernels: the integer multiply-add issue rate of the GPU, and the rate the
+// 12-limb Montgomery multiplication of field.cuh reaches on it.
+#include <cuda_runtime.h>
+
+#include "field.cuh"
+#include "runtime.hpp"
+
+namespace mzk {
+
+namespace {
+
+constexpr int kProbeIters = 4096;
+
+// 16 independent 32-bit multiply-adds per iteration (8 low halves, 8 high
+// halves), enough independent chains per warp to saturate the pipe.
+__global__ void k_probe_imad(uint32_t seed, uint32_t* sink) {
+    uint32_t a[8], b[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        a[k] = seed + threadIdx.x * 7u + (uint32_t)k;
+        b[k] = seed ^ (threadIdx.x + 13u * (uint32_t)k);
+    }
+    const uint32_t x = seed | 1u, y = 0x9e3779b9u;
+    for (int it = 0; it < kProbeIters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(x), "r"(y));
+            asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(b[k]) : "r"(x), "r"(y));
+        }
+    }
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc ^= a[k] ^ b[k];
+    if (acc == 0x12345678u) sink[0] = acc;
+}
+
+constexpr int kProbeMulIters = 256;
+
+__global__ void __launch_bounds__(128) k_probe_fp_mul(uint32_t seed, uint32_t* sink) {
+    Fp a, b, c;
+#pragma unroll
+    for (int j = 0; j < 12; j++) {
+        a.l[j] = (seed * (j + 1) + threadIdx.x) & 0x0fffffffu;
+        b.l[j] = (seed ^ (j * 977u)) & 0x0fffffffu;
+        c.l[j] = (seed + j * 31u) & 0x0fffffffu;
+    }
+    for (int it = 0; it < kProbeMulIters; it++) {
+        a = fp_mul(a, b);
+        c = fp_mul(c, b);
+    }
+    uint32_t acc = 0;
+#pragma unroll
+    for (int j = 0; j < 12; j++) acc ^= a.l[j] ^ c.l[j];
+    if (acc == 0x12345678u) sink[0] = acc;
+}
+
+}  // namespace
+
+Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s) {
+    void* sink;
+    MZK_TRY(ctx->ensure("probe_sink", 64, &sink));
+    cudaEvent_t e0, e1;
+    MZK_CUDA_CHECK(cudaEventCreate(&e0));
+    MZK_CUDA_CHECK(cudaEventCreate(&e1));
+    cudaStream_t st = ctx->stream;
+    const uint32_t blocks = (uint32_t)ctx->num_sms * 8, threads = 256;
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+        MZK_CUDA_CHECK(cudaEventRecord(e0, st));
+        k_probe_imad<<<blocks, threads, 0, st>>>(0x1234u + rep, (uint32_t*)sink);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_CUDA_CHECK(cudaEventRecord(e1, st));
+        MZK_CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms;
+        MZK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0 && ms < best) best = ms;
+    }
+    *imad_per_s = (double)blocks * threads * kProbeIters * 16.0 / (best * 1e-3);
+    int per_sm = 0;
+    MZK_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_fp_mul, 128, 0));
+    const uint32_t mblocks = (uint32_t)ctx->num_sms * (uint32_t)(per_sm > 0 ? per_sm : 1) * 4;
+    best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+        MZK_CUDA_CHECK(cudaEventRecord(e0, st));
+        k_probe_fp_mul<<<mblocks, 128, 0, st>>>(0x777u + rep, (uint32_t*)sink);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_CUDA_CHECK(cudaEventRecord(e1, st));
+        MZK_CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms;
+        MZK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0 && ms < best) best = ms;
+    }
+    *fp_mul_per_s = (double)mblocks * 128 * kProbeMulIters * 2.0 / (best * 1e-3);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return OK;
+}
+
+}  // namespace mzk

@@ -1,0 +1,118 @@
+// runtime.hpp — device context of the C ABI: one per (process, GPU).
+//
+// Holds the CUDA streams, a grow-only set of named scratch buffers (so repeated
+// calls of the same size never touch the allocator), a pinned staging buffer
+// for host <-> device copies, and the mutex that makes every entry point safe
+// to call from many host threads (the reference commits from rayon workers,
+// proofs/src/plonk/prover.rs:619-623).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+
+namespace mzk {
+
+enum Status : int {
+    OK = 0,
+    ERR_ARG = 1,
+    ERR_OOM = 2,
+    ERR_CUDA = 3,
+    ERR_TIMEOUT = 4,
+    ERR_STATE = 5,
+};
+
+void set_error(const std::string& msg);
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Context {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;       // compute stream
+    cudaStream_t copy_stream = nullptr;  // host->device copies overlapped with compute
+    cudaEvent_t ev_copy = nullptr;
+    std::recursive_mutex mu;
+    std::map<std::string, DevBuf> bufs;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    int msm_window_override = 0;
+    // fixed-base table of the G1 generator for synthetic inputs (device)
+    void* gen_table = nullptr;
+    // kernels launched by the library since context creation (for reporting)
+    uint64_t launches = 0;
+    // per-phase device timing with CUDA events on the launching stream
+    bool profiling = false;
+    static constexpr int kPhases = 16;
+    static constexpr int kMaxEvents = 2 * kPhases;
+    cudaEvent_t prof_ev[kMaxEvents] = {};
+    int prof_phase[kMaxEvents / 2] = {};
+    int prof_used = 0;
+    double phase_ms[kPhases] = {};
+    uint64_t phase_count[kPhases] = {};
+    // shape of the last MSM: window width, windows, bucket entries processed
+    int last_c = 0, last_windows = 0;
+    uint64_t last_entries = 0;
+
+    // open/close a timed phase on `st` (no-ops unless profiling)
+    Status phase_begin(int phase, cudaStream_t st);
+    Status phase_end(cudaStream_t st);
+    // after a stream sync: fold recorded phase times into the totals
+    void phase_collect();
+
+    // device buffer `name` of at least `bytes` bytes (contents undefined)
+    Status ensure(const char* name, size_t bytes, void** out);
+    Status ensure_pinned(size_t bytes, void** out);
+    ~Context();
+};
+
+#define MZK_CUDA_CHECK(expr)                                                                  \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess) {                                                              \
+            ::mzk::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));             \
+            return _e == cudaErrorMemoryAllocation ? ::mzk::ERR_OOM : ::mzk::ERR_CUDA; \
+        }                                                                                     \
+    } while (0)
+
+#define MZK_LAUNCH_CHECK(ctx)                                                                 \
+    do {                                                                                      \
+        (ctx)->launches++;                                                                    \
+        cudaError_t _e = cudaGetLastError();                                                  \
+        if (_e != cudaSuccess) {                                                              \
+            ::mzk::set_error(std::string("kernel launch: ") + cudaGetErrorString(_e));        \
+            return ::mzk::ERR_CUDA;                                                       \
+        }                                                                                     \
+    } while (0)
+
+#define MZK_TRY(expr)                          \
+    do {                                       \
+        ::mzk::Status _s = (expr);             \
+        if (_s != ::mzk::OK) return _s;    \
+    } while (0)
+
+// ---- MSM (msm.cu) ----
+// scalars: n x 8 u32 (Fr, Montgomery), bases: n x 24 u32 (affine, Montgomery),
+// both device pointers; out: 18 u64 host Jacobian with Z = 1 (identity: zeros).
+// bases_ready (optional): event the compute stream waits on before the
+// first kernel that reads the bases (their upload overlaps the digit sort)
+Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
+                     cudaStream_t stream, cudaEvent_t bases_ready);
+int msm_pick_window(size_t n);
+enum MsmPhase { PH_HISTOGRAM = 0, PH_SCAN, PH_SCATTER, PH_ACCUMULATE, PH_FIXUP, PH_REDUCE, PH_TAIL, PH_COPY };
+
+// ---- microbenchmarks (probe.cu) ----
+// integer multiply-add pipe rate (independent mad.lo/mad.hi, 32-bit) and the
+// rate of full 12-limb Montgomery multiplications, both per second
+Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s);
+
+// ---- synthetic inputs (gen.cu) ----
+Status gen_rand_fr(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t stream);
+Status gen_bases_g1(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t stream);
+
+}  // namespace mzk
