@@ -47,9 +47,12 @@ int mzk_ctx_synchronize(mzk_ctx *ctx);
  * Turning profiling on resets the totals. */
 int mzk_ctx_set_profiling(mzk_ctx *ctx, int on);
 int mzk_ctx_phase_stats(mzk_ctx *ctx, double *ms_out, uint64_t *count_out, int max_phases);
-/* Integer multiply-add throughput of this GPU (IMAD/s) and 12-limb Montgomery
- * multiplications per second, measured by microbenchmark kernels. */
-int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s);
+/* Integer multiply-add throughput of this GPU (IMAD/s, carry-chained
+ * mad.lo.cc/madc.hi pairs as the field code issues them) and 12-limb
+ * Montgomery multiplications per second, measured by microbenchmark kernels.
+ * variants (may be NULL): [0] independent mad.lo+mad.hi, [1] carry-chained
+ * pairs, [2] independent mad.lo only, all in IMAD/s. */
+int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s, double variants[3]);
 
 /* ---- device memory helpers (for callers without a CUDA runtime) ---------- */
 int mzk_device_alloc(mzk_ctx *ctx, size_t bytes, void **out);

@@ -44,7 +44,8 @@ SIGNATURES = {
     "mzk_ctx_synchronize": (_i32, [_vp]),
     "mzk_ctx_set_profiling": (_i32, [_vp, _i32]),
     "mzk_ctx_phase_stats": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _u64p, _i32]),
-    "mzk_probe_imad_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "mzk_probe_imad_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double)]),
     "mzk_msm_last_shape": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u64p]),
     "mzk_device_alloc": (_i32, [_vp, _sz, ctypes.POINTER(_vp)]),
     "mzk_device_free": (_i32, [_vp, _vp]),
@@ -181,10 +182,11 @@ class Context:
         return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(self.PHASES)}
 
     def probe_imad_peak(self):
-        """(IMAD/s, 12-limb Montgomery multiplications/s) of this GPU."""
+        """(IMAD/s, 12-limb Montgomery multiplications/s, {variant: IMAD/s}) of this GPU."""
         a, b = ctypes.c_double(), ctypes.c_double()
-        _check(lib().mzk_probe_imad_peak(self.h, ctypes.byref(a), ctypes.byref(b)))
-        return a.value, b.value
+        v = (ctypes.c_double * 3)()
+        _check(lib().mzk_probe_imad_peak(self.h, ctypes.byref(a), ctypes.byref(b), v))
+        return a.value, b.value, {"mad_lo_hi": v[0], "mad_cc_chain": v[1], "mad_lo": v[2]}
 
     def msm_last_shape(self):
         c, w, e = _i32(), _i32(), np.zeros(1, np.uint64)

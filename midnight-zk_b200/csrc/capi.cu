@@ -271,10 +271,10 @@ int mzk_msm_last_shape(mzk_ctx* ctx, int* c, int* windows, uint64_t* entries) {
     return mzk::OK;
 }
 
-int mzk_probe_imad_peak(mzk_ctx* ctx, double* imad_per_s, double* fp_mul_per_s) {
+int mzk_probe_imad_peak(mzk_ctx* ctx, double* imad_per_s, double* fp_mul_per_s, double variants[3]) {
     if (int s = check_ctx(ctx)) return s;
     Guard g(ctx);
-    return mzk::probe_imad(&ctx->impl, imad_per_s, fp_mul_per_s);
+    return mzk::probe_imad(&ctx->impl, imad_per_s, fp_mul_per_s, variants);
 }
 
 int mzk_msm_g1_device(mzk_ctx* ctx, const uint64_t* d_scalars, const uint64_t* d_bases, size_t n, uint64_t out[18]) {

@@ -99,6 +99,30 @@ __device__ __forceinline__ void xyzz_add_affine(Xyzz& acc, const Affine& q) {
     acc.y = y3;
 }
 
+// madd-2008-s for acc != infinity, scheduled as five pairs of independent
+// multiplications with the fewest live temporaries.
+__device__ __forceinline__ void xyzz_add_affine_fast(Xyzz& acc, const Affine& q) {
+    Fp u2, s2;
+    fp_mul2(u2, q.x, acc.zz, s2, q.y, acc.zzz);
+    const Fp p = fp_sub(u2, acc.x);
+    const Fp r = fp_sub(s2, acc.y);
+    if (fp_is_zero(p)) {  // rare: equal or opposite x (branch not taken is never fetched)
+        if (fp_is_zero(r)) acc = xyzz_dbl_affine(q);
+        else xyzz_set_inf(acc);
+        return;
+    }
+    Fp pp, rr;
+    fp_mul2(pp, p, p, rr, r, r);
+    Fp ppp, q1;
+    fp_mul2(ppp, p, pp, q1, acc.x, pp);
+    fp_mul2(acc.zz, acc.zz, pp, acc.zzz, acc.zzz, ppp);
+    const Fp x3 = fp_sub(fp_sub(rr, ppp), fp_dbl(q1));
+    Fp t1, t2;
+    fp_mul2(t1, r, fp_sub(q1, x3), t2, acc.y, ppp);
+    acc.y = fp_sub(t1, t2);
+    acc.x = x3;
+}
+
 // add-2008-s: a + b for XYZZ points, all special cases
 __device__ __forceinline__ Xyzz xyzz_add(const Xyzz& a, const Xyzz& b) {
     if (xyzz_is_inf(a)) return b;

@@ -190,6 +190,15 @@ __device__ __forceinline__ Fp fp_mul(const Fp& a, const Fp& b) {
     mont_mul_raw<FpP>(r.l, a.l, b.l);
     return r;
 }
+// two independent products in one basic block, so their carry chains can be
+// scheduled side by side
+__device__ __forceinline__ void fp_mul2(Fp& r1, const Fp& a1, const Fp& b1, Fp& r2, const Fp& a2, const Fp& b2) {
+    Fp t1, t2;
+    mont_mul_raw<FpP>(t1.l, a1.l, b1.l);
+    mont_mul_raw<FpP>(t2.l, a2.l, b2.l);
+    r1 = t1;
+    r2 = t2;
+}
 __device__ __forceinline__ Fp fp_sqr(const Fp& a) { return fp_mul(a, a); }
 __device__ __forceinline__ Fp fp_add(const Fp& a, const Fp& b) {
     Fp t, r;

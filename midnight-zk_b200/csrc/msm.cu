@@ -266,6 +266,21 @@ __device__ __forceinline__ void chunk_range(uint32_t total, uint32_t t, uint32_t
     e = min(total, s + len);
 }
 
+// One flat loop over the chunk, so every thread of a warp runs the same number
+// of additions whatever its bucket boundaries; a boundary only costs a short
+// divergent flush.
+__device__ __forceinline__ void flush_bucket(const Xyzz& acc, uint32_t k, uint32_t seg_lo, uint32_t seg_hi, uint32_t s,
+                                             uint32_t e, uint32_t t, Xyzz* buckets, Xyzz* partials, int* owner_key) {
+    if (seg_lo >= s && seg_hi <= e) {
+        store_xyzz(&buckets[k], acc);
+    } else if (seg_lo < s) {
+        store_xyzz(&partials[2 * (size_t)t], acc);
+    } else {
+        store_xyzz(&partials[2 * (size_t)t + 1], acc);
+        owner_key[t] = (int)k;
+    }
+}
+
 __global__ void __launch_bounds__(kAccThreads) k_accumulate(const Affine* __restrict__ bases,
                                                             const uint32_t* __restrict__ sorted,
                                                             const uint32_t* __restrict__ offsets, uint32_t keys,
@@ -279,32 +294,40 @@ __global__ void __launch_bounds__(kAccThreads) k_accumulate(const Affine* __rest
     owner_key[t] = -1;
     if (s >= e) return;
     uint32_t k = find_key(offsets, keys, s);
-    uint32_t pos = s;
-    while (pos < e) {
-        const uint32_t seg_lo = offsets[k], seg_hi = offsets[k + 1];
-        const uint32_t end = min(seg_hi, e);
-        Xyzz acc;
-        xyzz_set_inf(acc);
-        for (uint32_t j = pos; j < end; j++) {
-            const uint32_t ent = __ldg(sorted + j);
-            Affine p = load_affine(bases, ent & 0x7fffffffu);
-            if (aff_is_inf(p)) continue;
-            if (ent >> 31) p.y = fp_neg(p.y);
-            xyzz_add_affine(acc, p);
+    uint32_t seg_lo = offsets[k], seg_hi = offsets[k + 1];
+    Xyzz acc;
+    xyzz_set_inf(acc);
+    // the next entry's base is loaded one iteration ahead to hide the gather latency
+    uint32_t ent = __ldg(sorted + s);
+    Affine nxt = load_affine(bases, ent & 0x7fffffffu);
+    for (uint32_t j = s; j < e; j++) {
+        if (j == seg_hi) {
+            flush_bucket(acc, k, seg_lo, seg_hi, s, e, t, buckets, partials, owner_key);
+            xyzz_set_inf(acc);
+            do {
+                k++;
+                seg_lo = seg_hi;
+                seg_hi = offsets[k + 1];
+            } while (seg_hi <= j);
         }
-        if (seg_lo >= s && seg_hi <= e) {
-            store_xyzz(&buckets[k], acc);
-        } else if (seg_lo < s) {
-            store_xyzz(&partials[2 * (size_t)t], acc);
+        Affine p = nxt;
+        const uint32_t cur = ent;
+        if (j + 1 < e) {
+            ent = __ldg(sorted + j + 1);
+            nxt = load_affine(bases, ent & 0x7fffffffu);
+        }
+        if (aff_is_inf(p)) continue;
+        if (cur >> 31) p.y = fp_neg(p.y);
+        if (xyzz_is_inf(acc)) {
+            acc.x = p.x;
+            acc.y = p.y;
+            acc.zz = fp_one();
+            acc.zzz = fp_one();
         } else {
-            store_xyzz(&partials[2 * (size_t)t + 1], acc);
-            owner_key[t] = (int)k;
+            xyzz_add_affine_fast(acc, p);
         }
-        pos = end;
-        // next non-empty key
-        k++;
-        while (k < keys && offsets[k + 1] <= pos) k++;
     }
+    flush_bucket(acc, k, seg_lo, seg_hi, s, e, t, buckets, partials, owner_key);
 }
 
 __global__ void k_fixup(const uint32_t* __restrict__ offsets, uint32_t keys, const Xyzz* __restrict__ partials,

@@ -35,6 +35,44 @@ __global__ void k_probe_imad(uint32_t seed, uint32_t* sink) {
     if (acc == 0x12345678u) sink[0] = acc;
 }
 
+// The forms the field code issues: carry-chained low/high multiply-adds.
+// Eight independent two-limb chains per iteration (each chain restarts with
+// mad.lo.cc, so chains only share the carry flag by renaming).
+__global__ void k_probe_imad_cc(uint32_t seed, uint32_t* sink) {
+    uint32_t a[8], b[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        a[k] = seed + threadIdx.x * 7u + (uint32_t)k;
+        b[k] = seed ^ (threadIdx.x + 13u * (uint32_t)k);
+    }
+    const uint32_t x = seed | 1u;
+    for (int it = 0; it < kProbeIters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            asm volatile("mad.lo.cc.u32 %0, %0, %2, %1;\n\tmadc.hi.u32 %1, %1, %2, %0;" : "+r"(a[k]), "+r"(b[k]) : "r"(x));
+    }
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc ^= a[k] ^ b[k];
+    if (acc == 0x12345678u) sink[0] = acc;
+}
+
+// 16 independent mad.lo.u32 per iteration (low halves only)
+__global__ void k_probe_imad_lo(uint32_t seed, uint32_t* sink) {
+    uint32_t a[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) a[k] = seed + threadIdx.x * 7u + (uint32_t)k;
+    const uint32_t x = seed | 1u, y = 0x9e3779b9u;
+    for (int it = 0; it < kProbeIters; it++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(x), "r"(y));
+    }
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) acc ^= a[k];
+    if (acc == 0x12345678u) sink[0] = acc;
+}
+
 constexpr int kProbeMulIters = 256;
 
 __global__ void __launch_bounds__(128) k_probe_fp_mul(uint32_t seed, uint32_t* sink) {
@@ -57,7 +95,7 @@ __global__ void __launch_bounds__(128) k_probe_fp_mul(uint32_t seed, uint32_t* s
 
 }  // namespace
 
-Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s) {
+Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s, double* variants) {
     void* sink;
     MZK_TRY(ctx->ensure("probe_sink", 64, &sink));
     cudaEvent_t e0, e1;
@@ -65,18 +103,27 @@ Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s) {
     MZK_CUDA_CHECK(cudaEventCreate(&e1));
     cudaStream_t st = ctx->stream;
     const uint32_t blocks = (uint32_t)ctx->num_sms * 8, threads = 256;
-    float best = 1e30f;
-    for (int rep = 0; rep < 3; rep++) {
-        MZK_CUDA_CHECK(cudaEventRecord(e0, st));
-        k_probe_imad<<<blocks, threads, 0, st>>>(0x1234u + rep, (uint32_t*)sink);
-        MZK_LAUNCH_CHECK(ctx);
-        MZK_CUDA_CHECK(cudaEventRecord(e1, st));
-        MZK_CUDA_CHECK(cudaEventSynchronize(e1));
-        float ms;
-        MZK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-        if (rep > 0 && ms < best) best = ms;
+    double rates[3];
+    for (int v = 0; v < 3; v++) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+            MZK_CUDA_CHECK(cudaEventRecord(e0, st));
+            if (v == 0) k_probe_imad<<<blocks, threads, 0, st>>>(0x1234u + rep, (uint32_t*)sink);
+            else if (v == 1) k_probe_imad_cc<<<blocks, threads, 0, st>>>(0x1234u + rep, (uint32_t*)sink);
+            else k_probe_imad_lo<<<blocks, threads, 0, st>>>(0x1234u + rep, (uint32_t*)sink);
+            MZK_LAUNCH_CHECK(ctx);
+            MZK_CUDA_CHECK(cudaEventRecord(e1, st));
+            MZK_CUDA_CHECK(cudaEventSynchronize(e1));
+            float ms;
+            MZK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0 && ms < best) best = ms;
+        }
+        rates[v] = (double)blocks * threads * kProbeIters * 16.0 / (best * 1e-3);
+        if (variants) variants[v] = rates[v];
     }
-    *imad_per_s = (double)blocks * threads * kProbeIters * 16.0 / (best * 1e-3);
+    // the carry-chained form is what the field arithmetic issues
+    *imad_per_s = rates[1];
+    float best;
     int per_sm = 0;
     MZK_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_fp_mul, 128, 0));
     const uint32_t mblocks = (uint32_t)ctx->num_sms * (uint32_t)(per_sm > 0 ? per_sm : 1) * 4;
