@@ -281,7 +281,7 @@ __device__ __forceinline__ void flush_bucket(const Xyzz& acc, uint32_t k, uint32
     }
 }
 
-__global__ void __launch_bounds__(kAccThreads) k_accumulate(const Affine* __restrict__ bases,
+__global__ void __launch_bounds__(kAccThreads, 1) k_accumulate(const Affine* __restrict__ bases,
                                                             const uint32_t* __restrict__ sorted,
                                                             const uint32_t* __restrict__ offsets, uint32_t keys,
                                                             Xyzz* __restrict__ buckets, Xyzz* __restrict__ partials,
