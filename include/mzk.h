@@ -74,6 +74,21 @@ int mzk_memcpy_d2h(mzk_ctx *ctx, void *dst, const void *src, size_t bytes);
 int mzk_msm_g1(mzk_ctx *ctx, const uint64_t *scalars, const uint64_t *bases, size_t n, uint64_t out[18]);
 /* Same with DEVICE pointers (inputs resident in HBM, e.g. a device SRS). */
 int mzk_msm_g1_device(mzk_ctx *ctx, const uint64_t *d_scalars, const uint64_t *d_bases, size_t n, uint64_t out[18]);
+/*
+ * Allocation-free MSM for callers that cannot allocate device memory (a host
+ * framework that owns all GPU memory and passes an operation only its inputs
+ * and outputs, or code running where the CUDA allocator must not be called).
+ * No counterpart in the reference.  Same inputs and result as
+ * mzk_msm_g1_device, but it needs no context and calls no allocator: its
+ * scratch is one fixed device array of about 21 MB inside this library, held
+ * by every GPU that loads it until the process exits.  n must not exceed
+ * 65536 (larger n returns MZK_ERR_ARG).  The first call on a device looks up
+ * that array's device address (make it before any stream capture).  Runs on
+ * `stream` (NULL: the default stream) and returns when the result is on the
+ * host.  All calls share the array: calls are serialised by a host lock, and
+ * GPU work of two calls that overlapped would race on it.
+ */
+int mzk_msm_g1_noalloc(const uint64_t *d_scalars, const uint64_t *d_bases, size_t n, uint64_t out[18], void *stream);
 /* Window width override (0 = automatic), for tuning and tests. */
 int mzk_msm_set_window(mzk_ctx *ctx, int c);
 int mzk_msm_pick_window(size_t n);

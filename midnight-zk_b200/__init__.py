@@ -53,6 +53,7 @@ SIGNATURES = {
     "mzk_memcpy_d2h": (_i32, [_vp, _vp, _vp, _sz]),
     "mzk_msm_g1": (_i32, [_vp, _u64p, _u64p, _sz, _u64p]),
     "mzk_msm_g1_device": (_i32, [_vp, _vp, _vp, _sz, _u64p]),
+    "mzk_msm_g1_noalloc": (_i32, [_vp, _vp, _sz, _u64p, _vp]),
     "mzk_msm_set_window": (_i32, [_vp, _i32]),
     "mzk_msm_pick_window": (_i32, [_sz]),
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),

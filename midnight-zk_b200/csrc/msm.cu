@@ -33,6 +33,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "ec.cuh"
@@ -539,3 +541,162 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
 }
 
 }  // namespace mzk
+
+namespace mzk {
+
+// ---------------------------------------------------------------------------
+// Allocation-free MSM for callers that cannot allocate device memory.
+//
+// Some hosts own every byte of device memory themselves: a framework that
+// hands a custom operation its input and output buffers but no workspace, a
+// runtime whose memory pool must not be bypassed, or code running where the
+// CUDA allocator may not be called.  For them the MSM below takes its scratch
+// from one file-scope device array of fixed size instead of cudaMalloc.  It
+// serves n <= kNoAllocMaxN points with the window width clamped to [8, 12].
+// Every GPU that loads this library holds the array (about 21 MB) until the
+// process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocMaxN = size_t(1) << 16;
+constexpr int kNoAllocMinC = 8, kNoAllocMaxC = 12;
+constexpr uint32_t kNoAllocAccBlocks = 64;  // fixed accumulate grid (64 x 128 threads)
+constexpr int kNoAllocMaxDevices = 64;
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+// largest key count over the allowed widths: c = 12 gives 22 windows x 2048
+constexpr size_t kNaKeys = 22 * 2048;
+constexpr size_t kNaMaxWindows = 32;  // c = 8
+constexpr size_t kNaAccThreads = (size_t)kNoAllocAccBlocks * kAccThreads;
+constexpr size_t kNaCountsOff = 0;
+constexpr size_t kNaOffsetsOff = kNaCountsOff + align256((kNaKeys + 1) * 4);
+constexpr size_t kNaSortedOff = kNaOffsetsOff + align256((kNaKeys + 1) * 4);
+constexpr size_t kNaBucketsOff = kNaSortedOff + align256(kNaMaxWindows * kNoAllocMaxN * 4);
+constexpr size_t kNaPartialsOff = kNaBucketsOff + align256(kNaKeys * sizeof(Xyzz));
+constexpr size_t kNaOwnerOff = kNaPartialsOff + align256(kNaAccThreads * 2 * sizeof(Xyzz));
+constexpr size_t kNaRunOff = kNaOwnerOff + align256(kNaAccThreads * 4);
+constexpr size_t kNaTotOff = kNaRunOff + align256(kNaKeys / kGroupLen * sizeof(Xyzz));
+constexpr size_t kNaPlanesOff = kNaTotOff + align256(kNaKeys / kGroupLen * sizeof(Xyzz));
+constexpr size_t kNaWsumOff = kNaPlanesOff + align256(kNaMaxWindows * 8 * sizeof(Xyzz));
+constexpr size_t kNaScanOff = kNaWsumOff + align256(kNaMaxWindows * sizeof(Xyzz));
+constexpr size_t kNaBytes = kNaScanOff + align256(64 * 4);
+
+// The scratch itself.  Host code must not use this name as a device address:
+// on the host it is only a stand-in, so kernels get the pointer obtained from
+// cudaGetSymbolAddress below.
+__device__ __align__(256) unsigned char g_msm_noalloc_scratch[kNaBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// exclusive scan into caller-provided tile sums (no allocation)
+Status scan_u32_noalloc(const uint32_t* in, uint32_t* out, uint32_t len, uint32_t* sums, cudaStream_t st) {
+    const uint32_t tiles = (len + kScanTile - 1) / kScanTile;
+    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(in, out, len, sums);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    k_scan_add<<<tiles, kScanThreads, 0, st>>>(out, len, sums);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    return OK;
+}
+
+Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18, cudaStream_t st) {
+    std::memset(out18, 0, 18 * 8);
+    if (n > kNoAllocMaxN) {
+        set_error("mzk_msm_g1_noalloc: n = " + std::to_string(n) + " exceeds the fixed scratch limit of " +
+                  std::to_string(kNoAllocMaxN) + " points; use mzk_msm_g1_device");
+        return ERR_ARG;
+    }
+    if (n == 0) return OK;
+    int dev = 0;
+    MZK_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error("mzk_msm_g1_noalloc: device index out of range");
+        return ERR_ARG;
+    }
+    // one lock for the shared array: calls from several host threads take turns
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        // set-up, once per device, with that device current
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_msm_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error(std::string("mzk_msm_g1_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+            return ERR_CUDA;
+        }
+        int sms = 0;
+        MZK_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        g_noalloc_sms[dev] = sms;
+        g_noalloc_ptr[dev] = p;
+    }
+    unsigned char* base = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+    int c = msm_pick_window(n);
+    c = c < kNoAllocMinC ? kNoAllocMinC : (c > kNoAllocMaxC ? kNoAllocMaxC : c);
+    const MsmShape sh = make_shape(c);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(base + kNaCountsOff);
+    uint32_t* offsets = reinterpret_cast<uint32_t*>(base + kNaOffsetsOff);
+    uint32_t* sorted = reinterpret_cast<uint32_t*>(base + kNaSortedOff);
+    Xyzz* buckets = reinterpret_cast<Xyzz*>(base + kNaBucketsOff);
+    Xyzz* partials = reinterpret_cast<Xyzz*>(base + kNaPartialsOff);
+    int* owner = reinterpret_cast<int*>(base + kNaOwnerOff);
+    Xyzz* run = reinterpret_cast<Xyzz*>(base + kNaRunOff);
+    Xyzz* tot = reinterpret_cast<Xyzz*>(base + kNaTotOff);
+    Xyzz* planes = reinterpret_cast<Xyzz*>(base + kNaPlanesOff);
+    Xyzz* wsum = reinterpret_cast<Xyzz*>(base + kNaWsumOff);
+    uint32_t* scan_sums = reinterpret_cast<uint32_t*>(base + kNaScanOff);
+
+    const Fr* sc = static_cast<const Fr*>(d_scalars);
+    const Affine* ba = static_cast<const Affine*>(d_bases);
+    const int pt_threads = 256;
+    const uint32_t pt_blocks =
+        (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)g_noalloc_sms[dev] * 16);
+    // the array keeps the previous call's contents: zero the counters
+    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
+    k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, counts);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    MZK_TRY(scan_u32_noalloc(counts, offsets, sh.keys + 1, scan_sums, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
+    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, offsets, counts, sorted);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    k_accumulate<<<kNoAllocAccBlocks, kAccThreads, 0, st>>>(ba, sorted, offsets, sh.keys, buckets, partials, owner);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    k_fixup<<<kNoAllocAccBlocks, kAccThreads, 0, st>>>(offsets, sh.keys, partials, owner, buckets);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    const size_t total_groups = (size_t)sh.groups * sh.windows;
+    const uint32_t gblocks = (uint32_t)((total_groups + kReduceThreads - 1) / kReduceThreads);
+    k_group_sums<<<gblocks, kReduceThreads, 0, st>>>(buckets, offsets, sh.nb, sh.groups, (uint32_t)total_groups, run,
+                                                    tot);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    const size_t nplanes = (size_t)sh.windows * (sh.planes + 1);
+    k_plane_sums<<<(uint32_t)nplanes, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(run, tot, sh.groups,
+                                                                                          sh.planes, planes);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    k_window_finish<<<(sh.windows + 31) / 32, 32, 0, st>>>(planes, sh.planes, sh.windows, wsum);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    // window sums to host memory owned by this function (no pinned allocation)
+    host::Xyzz6 hs[kNaMaxWindows];
+    MZK_CUDA_CHECK(cudaMemcpyAsync(hs, wsum, (size_t)sh.windows * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    host::Xyzz6 acc = host::infinity();
+    for (int w = sh.windows - 1; w >= 0; w--) {
+        for (int b = 0; b < sh.c; b++) acc = host::dbl(acc);
+        acc = host::add(acc, host::canon(hs[w]));
+    }
+    host::to_jacobian_normalised(acc, out18);
+    return OK;
+}
+
+}  // namespace
+
+}  // namespace mzk
+
+extern "C" int mzk_msm_g1_noalloc(const uint64_t* d_scalars, const uint64_t* d_bases, size_t n, uint64_t out[18],
+                                  void* stream) {
+    if (!out || (n && (!d_scalars || !d_bases))) {
+        mzk::set_error("mzk_msm_g1_noalloc: null pointer");
+        return mzk::ERR_ARG;
+    }
+    return mzk::msm_g1_noalloc(d_scalars, d_bases, n, out, static_cast<cudaStream_t>(stream));
+}
