@@ -95,6 +95,30 @@ int mzk_msm_pick_window(size_t n);
 /* Window width, window count and bucket entries (non-zero digits) of the last MSM. */
 int mzk_msm_last_shape(mzk_ctx *ctx, int *c, int *windows, uint64_t *entries);
 
+/* ---- EvaluationDomain (proofs/src/poly/domain.rs) ----------------------- */
+typedef struct mzk_domain mzk_domain;
+/* EvaluationDomain::new(j, k) (domain.rs:54-167): n = 2^k, extended domain
+ * 2^extended_k >= n * (j - 1), coset generator zeta; twiddle tables on ctx's GPU. */
+int mzk_domain_create(mzk_ctx *ctx, uint32_t j, uint32_t k, mzk_domain **out);
+int mzk_domain_destroy(mzk_domain *d);
+int mzk_domain_shape(const mzk_domain *d, uint32_t *k, uint32_t *extended_k);
+/* domain constants (Montgomery Fr): 0 omega, 1 omega_inv, 2 extended_omega,
+ * 3 extended_omega_inv, 4 g_coset (zeta), 5 g_coset_inv (zeta^2),
+ * 6 ifft_divisor, 7 extended_ifft_divisor, 8 t_evaluations[idx] (inverted) */
+int mzk_domain_constant(const mzk_domain *d, int which, int idx, uint64_t out[4]);
+/* Operations (op codes) and the reference methods they replace:
+ *   0 coeff_to_lagrange      in n      -> out n       (domain.rs:268)
+ *   1 lagrange_to_coeff      in n      -> out n       (domain.rs:249)
+ *   2 coeff_to_extended      in n      -> out 2^ext_k (domain.rs:285)
+ *   3 extended_to_coeff      in 2^ext_k-> out 2^ext_k (domain.rs:312)
+ *   4 extended_to_lagrange   in 2^ext_k-> out n       (domain.rs:335)
+ *   5 divide_by_vanishing_poly in 2^ext_k -> out 2^ext_k (domain.rs:361)
+ * Elements are Fr (4 x u64 Montgomery).  mzk_domain_op takes HOST buffers
+ * (in and out may be the same buffer when the lengths agree). */
+int mzk_domain_op(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *in, uint64_t *out);
+/* DEVICE buffers; in == out allowed for ops 0, 1, 3, 5; op 4 overwrites in. */
+int mzk_domain_op_device(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *d_in, uint64_t *d_out);
+
 /* ---- seeded synthetic inputs (benchmarks and tests) -------------------- */
 /* n uniform Fr elements (Montgomery) of stream `seed`, elements first..first+n-1 */
 int mzk_gen_rand_fr_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);

@@ -56,6 +56,12 @@ SIGNATURES = {
     "mzk_msm_g1_noalloc": (_i32, [_vp, _vp, _sz, _u64p, _vp]),
     "mzk_msm_set_window": (_i32, [_vp, _i32]),
     "mzk_msm_pick_window": (_i32, [_sz]),
+    "mzk_domain_create": (_i32, [_vp, _u32, _u32, ctypes.POINTER(_vp)]),
+    "mzk_domain_destroy": (_i32, [_vp]),
+    "mzk_domain_shape": (_i32, [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
+    "mzk_domain_constant": (_i32, [_vp, _i32, _i32, _u64p]),
+    "mzk_domain_op": (_i32, [_vp, _vp, _i32, _u64p, _u64p]),
+    "mzk_domain_op_device": (_i32, [_vp, _vp, _i32, _vp, _vp]),
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
     "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
 }
@@ -229,6 +235,82 @@ class Context:
         buf = out or self.alloc(n * 96)
         _check(lib().mzk_gen_bases_g1_device(self.h, seed, first, n, buf.ptr))
         return buf
+
+
+class EvaluationDomain:
+    """EvaluationDomain (proofs/src/poly/domain.rs:34) with its NTTs on the GPU.
+
+    Methods take and return (len, 4) uint64 arrays of Fr in Montgomery form,
+    like the reference's Polynomial values; inputs are not modified.
+    """
+
+    OPS = {"coeff_to_lagrange": 0, "lagrange_to_coeff": 1, "coeff_to_extended": 2,
+           "extended_to_coeff": 3, "extended_to_lagrange": 4, "divide_by_vanishing_poly": 5}
+
+    def __init__(self, ctx, j, k):
+        self.ctx = ctx
+        h = _vp()
+        _check(lib().mzk_domain_create(ctx.h, j, k, ctypes.byref(h)))
+        self.h = h.value
+        kk, ek = _u32(), _u32()
+        _check(lib().mzk_domain_shape(self.h, ctypes.byref(kk), ctypes.byref(ek)))
+        self.k, self.extended_k = kk.value, ek.value
+        self.n, self.extended_len = 1 << self.k, 1 << self.extended_k
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mzk_domain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def constant(self, which, idx=0):
+        out = np.zeros(4, np.uint64)
+        _check(lib().mzk_domain_constant(self.h, which, idx, _ptr(out)))
+        return out
+
+    def _lens(self, op):
+        n, en = self.n, self.extended_len
+        return {0: (n, n), 1: (n, n), 2: (n, en), 3: (en, en), 4: (en, n), 5: (en, en)}[op]
+
+    def _run(self, name, a):
+        op = self.OPS[name]
+        lin, lout = self._lens(op)
+        a = np.ascontiguousarray(a, np.uint64).reshape(-1, 4)
+        if a.shape[0] != lin:
+            # the reference asserts the length (domain.rs:250, :286, :313, :339, :365)
+            raise MzkError(1, f"{name}: expected {lin} elements, got {a.shape[0]}")
+        out = np.zeros((lout, 4), np.uint64)
+        _check(lib().mzk_domain_op(self.ctx.h, self.h, op, _ptr(a), _ptr(out)))
+        return out
+
+    def coeff_to_lagrange(self, a):
+        return self._run("coeff_to_lagrange", a)
+
+    def lagrange_to_coeff(self, a):
+        return self._run("lagrange_to_coeff", a)
+
+    def coeff_to_extended(self, a):
+        return self._run("coeff_to_extended", a)
+
+    def extended_to_coeff(self, a):
+        return self._run("extended_to_coeff", a)
+
+    def extended_to_lagrange(self, a):
+        return self._run("extended_to_lagrange", a)
+
+    def divide_by_vanishing_poly(self, a):
+        return self._run("divide_by_vanishing_poly", a)
+
+    def op_device(self, name, d_in, d_out):
+        """Operation on device buffers (pointers or DeviceBuffers)."""
+        di = d_in.ptr if isinstance(d_in, DeviceBuffer) else int(d_in)
+        do = d_out.ptr if isinstance(d_out, DeviceBuffer) else int(d_out)
+        _check(lib().mzk_domain_op_device(self.ctx.h, self.h, self.OPS[name], di, do))
 
 
 def msm_pick_window(n):

@@ -6,10 +6,16 @@
 #include <string>
 
 #include "../../include/mzk.h"
+#include "ntt.hpp"
 #include "runtime.hpp"
 
 struct mzk_ctx {
     mzk::Context impl;
+};
+
+struct mzk_domain {
+    mzk::Domain* impl = nullptr;
+    mzk_ctx* ctx = nullptr;
 };
 
 namespace mzk {
@@ -323,6 +329,102 @@ int mzk_gen_bases_g1_device(mzk_ctx* ctx, uint64_t seed, uint64_t first, size_t 
     Guard g(ctx);
     MZK_TRY(mzk::gen_bases_g1(&ctx->impl, seed, first, n, d_out, ctx->impl.stream));
     MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+// ---- EvaluationDomain -----------------------------------------------------
+
+int mzk_domain_create(mzk_ctx* ctx, uint32_t j, uint32_t k, mzk_domain** out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!out) return mzk::ERR_ARG;
+    *out = nullptr;
+    Guard g(ctx);
+    mzk::Domain* d = nullptr;
+    MZK_TRY(mzk::domain_create(&ctx->impl, j, k, &d));
+    mzk_domain* h = new (std::nothrow) mzk_domain;
+    if (!h) {
+        delete d;
+        return mzk::ERR_OOM;
+    }
+    h->impl = d;
+    h->ctx = ctx;
+    *out = h;
+    return mzk::OK;
+}
+
+int mzk_domain_destroy(mzk_domain* d) {
+    if (!d) return mzk::OK;
+    Guard g(d->ctx);
+    cudaStreamSynchronize(d->ctx->impl.stream);
+    delete d->impl;
+    delete d;
+    return mzk::OK;
+}
+
+int mzk_domain_shape(const mzk_domain* d, uint32_t* k, uint32_t* extended_k) {
+    if (!d) return mzk::ERR_ARG;
+    if (k) *k = d->impl->k;
+    if (extended_k) *extended_k = d->impl->ext_k;
+    return mzk::OK;
+}
+
+int mzk_domain_constant(const mzk_domain* d, int which, int idx, uint64_t out[4]) {
+    if (!d || !out) return mzk::ERR_ARG;
+    const mzk::Domain* D = d->impl;
+    const mzk::host::Fr4* src = nullptr;
+    switch (which) {
+        case 0: src = &D->omega; break;
+        case 1: src = &D->omega_inv; break;
+        case 2: src = &D->ext_omega; break;
+        case 3: src = &D->ext_omega_inv; break;
+        case 4: src = &D->zeta; break;
+        case 5: src = &D->zeta2; break;
+        case 6: src = &D->ifft_div; break;
+        case 7: src = &D->ext_ifft_div; break;
+        case 8:
+            if (idx < 0 || (size_t)idx >= D->t_inv.size()) return mzk::ERR_ARG;
+            src = &D->t_inv[idx];
+            break;
+        default:
+            mzk::set_error("domain constant: unknown index");
+            return mzk::ERR_ARG;
+    }
+    std::memcpy(out, src->l, 32);
+    return mzk::OK;
+}
+
+int mzk_domain_op_device(mzk_ctx* ctx, mzk_domain* d, int op, const uint64_t* d_in, uint64_t* d_out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || !d_in || !d_out) {
+        mzk::set_error("domain op: null argument");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    MZK_TRY(mzk::domain_op_device(&ctx->impl, d->impl, op, d_in, d_out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_domain_op(mzk_ctx* ctx, mzk_domain* d, int op, const uint64_t* in, uint64_t* out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || !in || !out) {
+        mzk::set_error("domain op: null argument");
+        return mzk::ERR_ARG;
+    }
+    if (op < 0 || op > mzk::OP_DIVIDE_BY_VANISHING) {
+        mzk::set_error("domain op: unknown operation");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    mzk::Context* c = &ctx->impl;
+    const size_t in_len = mzk::domain_op_in_len(d->impl, op), out_len = mzk::domain_op_out_len(d->impl, op);
+    void *din, *dout;
+    MZK_TRY(c->ensure("ntt_in", in_len * 32, &din));
+    MZK_TRY(c->ensure("ntt_out", out_len * 32, &dout));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(din, in, in_len * 32, cudaMemcpyHostToDevice, c->stream));
+    MZK_TRY(mzk::domain_op_device(c, d->impl, op, din, dout, c->stream));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(out, dout, out_len * 32, cudaMemcpyDeviceToHost, c->stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(c->stream));
     return mzk::OK;
 }
 

@@ -150,6 +150,22 @@ __device__ __forceinline__ Xyzz xyzz_add(const Xyzz& a, const Xyzz& b) {
     return o;
 }
 
+__device__ __forceinline__ Fp fp_select(bool c, const Fp& a, const Fp& b) {
+    Fp r;
+#pragma unroll
+    for (int j = 0; j < 12; j++) r.l[j] = c ? a.l[j] : b.l[j];
+    return r;
+}
+// c ? a : b, limb by limb in registers
+__device__ __forceinline__ Xyzz xyzz_select(bool c, const Xyzz& a, const Xyzz& b) {
+    Xyzz r;
+    r.x = fp_select(c, a.x, b.x);
+    r.y = fp_select(c, a.y, b.y);
+    r.zz = fp_select(c, a.zz, b.zz);
+    r.zzz = fp_select(c, a.zzz, b.zzz);
+    return r;
+}
+
 // k * p for a small non-negative k (double-and-add, MSB first)
 __device__ __forceinline__ Xyzz xyzz_mul_small(const Xyzz& p, uint32_t k) {
     Xyzz acc;

@@ -168,3 +168,105 @@ inline void to_jacobian_normalised(const Xyzz6& p, uint64_t out[18]) {
 
 }  // namespace host
 }  // namespace mzk
+
+namespace mzk {
+namespace host {
+
+// ---- Fr (scalar field r, 4 x u64 Montgomery, R = 2^256) for domain set-up ----
+struct Fr4 { uint64_t l[4]; };
+
+static const uint64_t R4[4] = {0xffffffff00000001ULL, 0x53bda402fffe5bfeULL, 0x3339d80809a1d805ULL,
+                               0x73eda753299d7d48ULL};
+static const uint64_t R4_INV = 0xfffffffeffffffffULL;  // -r^{-1} mod 2^64
+static const uint64_t FR_ONE4[4] = {0x00000001fffffffeULL, 0x5884b7fa00034802ULL, 0x998c4fefecbc4ff5ULL,
+                                    0x1824b159acc5056fULL};
+static const uint64_t FR_R2_4[4] = {0xc999e990f3f29c6dULL, 0x2b6cedcb87925c23ULL, 0x05d314967254398fULL,
+                                    0x0748d9d99f59ff11ULL};
+
+inline bool fr_geq(const uint64_t* a, const uint64_t* b) {
+    for (int i = 3; i >= 0; i--)
+        if (a[i] != b[i]) return a[i] > b[i];
+    return true;
+}
+inline Fr4 fr_mul(const Fr4& a, const Fr4& b) {
+    uint64_t t[6] = {0};
+    for (int i = 0; i < 4; i++) {
+        uint64_t c = 0;
+        for (int j = 0; j < 4; j++) {
+            u128 s = (u128)a.l[j] * b.l[i] + t[j] + c;
+            t[j] = (uint64_t)s;
+            c = (uint64_t)(s >> 64);
+        }
+        u128 s = (u128)t[4] + c;
+        t[4] = (uint64_t)s;
+        t[5] = (uint64_t)(s >> 64);
+        uint64_t q = t[0] * R4_INV;
+        s = (u128)q * R4[0] + t[0];
+        c = (uint64_t)(s >> 64);
+        for (int j = 1; j < 4; j++) {
+            s = (u128)q * R4[j] + t[j] + c;
+            t[j - 1] = (uint64_t)s;
+            c = (uint64_t)(s >> 64);
+        }
+        s = (u128)t[4] + c;
+        t[3] = (uint64_t)s;
+        t[4] = t[5] + (uint64_t)(s >> 64);
+    }
+    Fr4 r;
+    if (t[4] || fr_geq(t, R4)) {
+        uint64_t br = 0;
+        for (int i = 0; i < 4; i++) {
+            u128 d = (u128)t[i] - R4[i] - br;
+            t[i] = (uint64_t)d;
+            br = (uint64_t)(d >> 127);
+        }
+    }
+    std::memcpy(r.l, t, 32);
+    return r;
+}
+inline Fr4 fr_sub(const Fr4& a, const Fr4& b) {
+    Fr4 r;
+    uint64_t br = 0;
+    for (int i = 0; i < 4; i++) {
+        u128 d = (u128)a.l[i] - b.l[i] - br;
+        r.l[i] = (uint64_t)d;
+        br = (uint64_t)(d >> 127);
+    }
+    if (br) {
+        uint64_t c = 0;
+        for (int i = 0; i < 4; i++) {
+            u128 s = (u128)r.l[i] + R4[i] + c;
+            r.l[i] = (uint64_t)s;
+            c = (uint64_t)(s >> 64);
+        }
+    }
+    return r;
+}
+inline Fr4 fr_one() {
+    Fr4 r;
+    std::memcpy(r.l, FR_ONE4, 32);
+    return r;
+}
+inline Fr4 fr_from_u64(uint64_t v) {
+    Fr4 a = {{v, 0, 0, 0}}, r2;
+    std::memcpy(r2.l, FR_R2_4, 32);
+    return fr_mul(a, r2);
+}
+inline Fr4 fr_pow(const Fr4& a, const uint64_t* e, int limbs) {
+    Fr4 acc = fr_one();
+    for (int i = limbs * 64 - 1; i >= 0; i--) {
+        acc = fr_mul(acc, acc);
+        if ((e[i / 64] >> (i % 64)) & 1) acc = fr_mul(acc, a);
+    }
+    return acc;
+}
+inline Fr4 fr_inv(const Fr4& a) {
+    uint64_t e[4];
+    std::memcpy(e, R4, 32);
+    e[0] -= 2;
+    return fr_pow(a, e, 4);
+}
+inline bool fr_eq(const Fr4& a, const Fr4& b) { return std::memcmp(a.l, b.l, 32) == 0; }
+
+}  // namespace host
+}  // namespace mzk

@@ -332,8 +332,14 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumulate(const Affine* __r
     flush_bucket(acc, k, seg_lo, seg_hi, s, e, t, buckets, partials, owner_key);
 }
 
+// A cut bucket is finished by the chunk where it starts.  Short spans are summed
+// by that thread; a bucket spanning many chunks (a heavy bucket: scalars 0/1,
+// a nearly empty top window) is queued for k_fixup_long.
+constexpr uint32_t kShortSpan = 32;
+
 __global__ void k_fixup(const uint32_t* __restrict__ offsets, uint32_t keys, const Xyzz* __restrict__ partials,
-                        const int* __restrict__ owner_key, Xyzz* __restrict__ buckets) {
+                        const int* __restrict__ owner_key, Xyzz* __restrict__ buckets, uint32_t* __restrict__ long_count,
+                        uint2* __restrict__ long_list) {
     const uint32_t nthreads = gridDim.x * blockDim.x;  // same grid as k_accumulate
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = owner_key[t];
@@ -341,9 +347,41 @@ __global__ void k_fixup(const uint32_t* __restrict__ offsets, uint32_t keys, con
     const uint32_t total = offsets[keys];
     const uint32_t len = (total + nthreads - 1) / nthreads;
     const uint32_t last = (offsets[k + 1] - 1) / len;
+    if (last - t > kShortSpan) {
+        const uint32_t slot = atomicAdd(long_count, 1u);
+        long_list[slot] = make_uint2(t, last);
+        return;
+    }
     Xyzz acc = load_xyzz(&partials[2 * (size_t)t + 1]);
     for (uint32_t u = t + 1; u <= last; u++) acc = xyzz_add(acc, load_xyzz(&partials[2 * (size_t)u]));
     store_xyzz(&buckets[k], acc);
+}
+
+// one block per queued heavy bucket: strided partial sums, then a tree
+__global__ void __launch_bounds__(kReduceThreads) k_fixup_long(const int* __restrict__ owner_key,
+                                                               const Xyzz* __restrict__ partials,
+                                                               const uint32_t* __restrict__ long_count,
+                                                               const uint2* __restrict__ long_list,
+                                                               Xyzz* __restrict__ buckets) {
+    extern __shared__ uint4 smem_raw[];
+    Xyzz* sm = reinterpret_cast<Xyzz*>(smem_raw);
+    for (uint32_t item = blockIdx.x; item < *long_count; item += gridDim.x) {
+        const uint2 tl = long_list[item];
+        const uint32_t t = tl.x, last = tl.y;
+        Xyzz acc;
+        if (threadIdx.x == 0) acc = load_xyzz(&partials[2 * (size_t)t + 1]);
+        else xyzz_set_inf(acc);
+        for (uint32_t u = t + 1 + threadIdx.x; u <= last; u += blockDim.x)
+            acc = xyzz_add(acc, load_xyzz(&partials[2 * (size_t)u]));
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
+            if ((int)threadIdx.x < off) sm[threadIdx.x] = xyzz_add(sm[threadIdx.x], sm[threadIdx.x + off]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) store_xyzz(&buckets[owner_key[t]], sm[0]);
+        __syncthreads();
+    }
 }
 
 // per (window, group): running sum over kGroupLen buckets, top first
@@ -470,6 +508,9 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     MZK_TRY(ctx->ensure("msm_buckets", (size_t)sh.keys * sizeof(Xyzz), &buckets));
     MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
     MZK_TRY(ctx->ensure("msm_owner", (size_t)acc_threads * 4, &owner));
+    void *long_count, *long_list;
+    MZK_TRY(ctx->ensure("msm_long_count", 64, &long_count));
+    MZK_TRY(ctx->ensure("msm_long_list", (size_t)acc_threads * sizeof(uint2), &long_list));
     const size_t total_groups = (size_t)sh.groups * sh.windows;
     MZK_TRY(ctx->ensure("msm_run", total_groups * sizeof(Xyzz), &run));
     MZK_TRY(ctx->ensure("msm_tot", total_groups * sizeof(Xyzz), &tot));
@@ -505,8 +546,14 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_FIXUP, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(long_count, 0, 4, st));
     k_fixup<<<acc_blocks, kAccThreads, 0, st>>>((const uint32_t*)offsets, sh.keys, (const Xyzz*)partials,
-                                               (const int*)owner, (Xyzz*)buckets);
+                                               (const int*)owner, (Xyzz*)buckets, (uint32_t*)long_count,
+                                               (uint2*)long_list);
+    MZK_LAUNCH_CHECK(ctx);
+    k_fixup_long<<<ctx->num_sms * 2, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
+        (const int*)owner, (const Xyzz*)partials, (const uint32_t*)long_count, (const uint2*)long_list,
+        (Xyzz*)buckets);
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
@@ -579,7 +626,8 @@ constexpr size_t kNaTotOff = kNaRunOff + align256(kNaKeys / kGroupLen * sizeof(X
 constexpr size_t kNaPlanesOff = kNaTotOff + align256(kNaKeys / kGroupLen * sizeof(Xyzz));
 constexpr size_t kNaWsumOff = kNaPlanesOff + align256(kNaMaxWindows * 8 * sizeof(Xyzz));
 constexpr size_t kNaScanOff = kNaWsumOff + align256(kNaMaxWindows * sizeof(Xyzz));
-constexpr size_t kNaBytes = kNaScanOff + align256(64 * 4);
+constexpr size_t kNaLongOff = kNaScanOff + align256(64 * 4);
+constexpr size_t kNaBytes = kNaLongOff + align256(16 + kNaAccThreads * sizeof(uint2));
 
 // The scratch itself.  Host code must not use this name as a device address:
 // on the host it is only a stand-in, so kernels get the pointer obtained from
@@ -662,7 +710,15 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
     MZK_CUDA_CHECK(cudaGetLastError());
     k_accumulate<<<kNoAllocAccBlocks, kAccThreads, 0, st>>>(ba, sorted, offsets, sh.keys, buckets, partials, owner);
     MZK_CUDA_CHECK(cudaGetLastError());
-    k_fixup<<<kNoAllocAccBlocks, kAccThreads, 0, st>>>(offsets, sh.keys, partials, owner, buckets);
+    uint32_t* long_count = reinterpret_cast<uint32_t*>(base + kNaLongOff);
+    uint2* long_list = reinterpret_cast<uint2*>(base + kNaLongOff + 16);
+    MZK_CUDA_CHECK(cudaMemsetAsync(long_count, 0, 4, st));
+    k_fixup<<<kNoAllocAccBlocks, kAccThreads, 0, st>>>(offsets, sh.keys, partials, owner, buckets, long_count,
+                                                       long_list);
+    MZK_CUDA_CHECK(cudaGetLastError());
+    k_fixup_long<<<kNoAllocAccBlocks, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(owner, partials,
+                                                                                          long_count, long_list,
+                                                                                          buckets);
     MZK_CUDA_CHECK(cudaGetLastError());
     const size_t total_groups = (size_t)sh.groups * sh.windows;
     const uint32_t gblocks = (uint32_t)((total_groups + kReduceThreads - 1) / kReduceThreads);

@@ -1,0 +1,41 @@
+// ntt.hpp — device EvaluationDomain (proofs/src/poly/domain.rs:34-49).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "field.cuh"
+#include "host_ec.hpp"
+#include "runtime.hpp"
+
+namespace mzk {
+
+// operation codes of mzk_domain_op_device (include/mzk.h)
+enum DomainOp : int {
+    OP_COEFF_TO_LAGRANGE = 0,
+    OP_LAGRANGE_TO_COEFF = 1,
+    OP_COEFF_TO_EXTENDED = 2,
+    OP_EXTENDED_TO_COEFF = 3,
+    OP_EXTENDED_TO_LAGRANGE = 4,
+    OP_DIVIDE_BY_VANISHING = 5,
+};
+
+struct Domain {
+    uint32_t k = 0, ext_k = 0;
+    host::Fr4 omega, omega_inv, ext_omega, ext_omega_inv, zeta, zeta2, ifft_div, ext_ifft_div;
+    std::vector<host::Fr4> t_inv;  // 1 / t(zeta * ext_omega^i), i < 2^(ext_k - k)
+    // per root (0 omega, 1 omega_inv, 2 ext_omega, 3 ext_omega_inv):
+    // lo[r][i] = w^i (i < 4096), hi[r][i] = w^(4096 i)
+    Fr* tables[4] = {};
+    Fr* lo[4] = {};
+    Fr* hi[4] = {};
+    void* d_tinv = nullptr;
+    ~Domain();
+};
+
+Status domain_create(Context* ctx, uint32_t j, uint32_t k, Domain** out);
+// d_in / d_out device pointers (may alias for the in-place operations)
+Status domain_op_device(Context* ctx, const Domain* d, int op, const void* d_in, void* d_out, cudaStream_t st);
+size_t domain_op_in_len(const Domain* d, int op);
+size_t domain_op_out_len(const Domain* d, int op);
+
+}  // namespace mzk

@@ -1,0 +1,154 @@
+"""EvaluationDomain NTTs on the B200 against the C oracle, bit-exact.
+
+Every operation of proofs/src/poly/domain.rs:249-380 at small and medium k
+(the oracle restates the reference's FFTs), the domain constants of
+EvaluationDomain::new, and at the 2^24 size of the NTT sweep a round trip plus
+spot evaluations of the polynomial by Horner's rule.
+"""
+import numpy as np
+import pytest
+
+from _loader import load
+from oracle import oracle as O
+
+mzk = load()
+pytestmark = pytest.mark.gpu
+
+OPS = ["coeff_to_lagrange", "lagrange_to_coeff", "coeff_to_extended", "extended_to_coeff",
+       "extended_to_lagrange", "divide_by_vanishing_poly"]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = mzk.Context(0)
+    yield c
+    c.close()
+
+
+def oracle_op(dom, name, a):
+    return getattr(dom, name)(a)
+
+
+@pytest.mark.parametrize("j", [2, 3, 5])
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 8, 11, 12, 13, 16])
+def test_domain_ops_match_oracle(ctx, j, k):
+    if j == 2 and k == 1:
+        pytest.skip("extended domain equals the base domain; covered by the other j")
+    g = mzk.EvaluationDomain(ctx, j, k)
+    o = O.Domain(j, k)
+    assert (g.k, g.extended_k) == (o.k, o.extended_k)
+    for which, idx in [(0, 0), (1, 1), (2, 2), (3, 8), (4, 3), (5, 4), (6, 5), (7, 6)]:
+        assert np.array_equal(g.constant(which), o.get(idx)), which
+    for i in range(1 << (g.extended_k - g.k)):
+        assert np.array_equal(g.constant(8, i), o.get(7, i))
+    n, en = g.n, g.extended_len
+    a = O.rand_fr(1000 * j + k, n)
+    e = O.rand_fr(2000 * j + k, en)
+    for name, x in [("coeff_to_lagrange", a), ("lagrange_to_coeff", a), ("coeff_to_extended", a),
+                    ("extended_to_coeff", e), ("extended_to_lagrange", e), ("divide_by_vanishing_poly", e)]:
+        got = getattr(g, name)(x)
+        assert np.array_equal(got, oracle_op(o, name, x)), name
+    g.close()
+
+
+def test_inputs_are_not_modified_and_lengths_checked(ctx):
+    g = mzk.EvaluationDomain(ctx, 5, 6)
+    a = O.rand_fr(5, g.extended_len)
+    keep = a.copy()
+    g.extended_to_lagrange(a)
+    assert np.array_equal(a, keep)
+    with pytest.raises(mzk.MzkError):
+        g.coeff_to_lagrange(O.rand_fr(1, g.n + 1))
+
+
+def test_special_vectors(ctx):
+    k = 10
+    g = mzk.EvaluationDomain(ctx, 5, k)
+    n = g.n
+    zero = np.zeros((n, 4), np.uint64)
+    assert not g.coeff_to_lagrange(zero).any()
+    one = np.tile(O.fr_const(0), (n, 1))
+    # FFT of the constant polynomial 1 is the all-ones vector
+    c = np.zeros((n, 4), np.uint64)
+    c[0] = O.fr_const(0)
+    assert np.array_equal(g.coeff_to_lagrange(c), one)
+    # all-ones evaluations are the constant polynomial 1
+    assert np.array_equal(g.lagrange_to_coeff(one), c)
+    # values equal to r - 1 everywhere (largest canonical element)
+    big = np.tile(O.fr_op("neg", O.fr_const(0)), (n, 1))
+    o = O.Domain(5, k)
+    assert np.array_equal(g.coeff_to_extended(big), o.coeff_to_extended(big))
+
+
+@pytest.mark.parametrize("k", [18, 20])
+def test_medium_sizes_match_oracle(ctx, k):
+    g = mzk.EvaluationDomain(ctx, 5, k)
+    o = O.Domain(5, k)
+    a = O.rand_fr(77 + k, g.n)
+    assert np.array_equal(g.coeff_to_lagrange(a), o.coeff_to_lagrange(a))
+    ext = g.coeff_to_extended(a)
+    assert np.array_equal(ext, o.coeff_to_extended(a))
+    assert np.array_equal(g.extended_to_coeff(ext), o.extended_to_coeff(ext))
+
+
+def horner(coeffs, x):
+    """sum_i coeffs[i] x^i with the oracle's Fr arithmetic (Horner)."""
+    acc = np.zeros(4, np.uint64)
+    for c in coeffs[::-1]:
+        acc = O.fr_op("add", O.fr_op("mul", acc, x), c)
+    return acc
+
+
+def test_ntt_2_24_roundtrip_and_spot_evaluations(ctx):
+    """NTT sweep at n = 2^24 (2^26 extended): round trips are the identity and
+    sampled outputs equal direct evaluations."""
+    k = 24
+    g = mzk.EvaluationDomain(ctx, 5, k)
+    n, en = g.n, g.extended_len
+    da = ctx.gen_rand_fr(0x2424, n)
+    a = da.download((n, 4))
+    d_lag = ctx.alloc(n * 32)
+    g.op_device("coeff_to_lagrange", da, d_lag)
+    lag = d_lag.download((n, 4))
+    d_back = ctx.alloc(n * 32)
+    g.op_device("lagrange_to_coeff", d_lag, d_back)
+    assert np.array_equal(d_back.download((n, 4)), a)
+    d_ext = ctx.alloc(en * 32)
+    g.op_device("coeff_to_extended", da, d_ext)
+    ext = d_ext.download((en, 4))
+    g.op_device("extended_to_coeff", d_ext, d_ext)
+    back = d_ext.download((en, 4))
+    assert np.array_equal(back[:n], a) and not back[n:].any()
+    # spot checks: lag[i] = a(omega^i), ext[i] = a(zeta * ext_omega^i)
+    omega, eomega, zeta = g.constant(0), g.constant(2), g.constant(4)
+    sub = a[:4096].copy()  # evaluate the length-2^24 polynomial in chunks of powers
+    del sub
+
+    def pow_fr(x, e):
+        r = O.fr_const(0)
+        b = x.copy()
+        while e:
+            if e & 1:
+                r = O.fr_op("mul", r, b)
+            b = O.fr_op("mul", b, b)
+            e >>= 1
+        return r
+
+    d_tmp = ctx.alloc(n * 32)
+
+    def eval_at(x):
+        # evaluate on the device-free path: split a into 2^12 blocks of 2^12 coefficients
+        # a(x) = sum_b x^(4096 b) * a_b(x); each a_b(x) by Horner in C would be 2^24 mults,
+        # so use numpy-free oracle ops over a strided reduction
+        acc = np.zeros(4, np.uint64)
+        xb = pow_fr(x, 4096)
+        for blk in range(4095, -1, -1):
+            part = horner(a[blk * 4096:(blk + 1) * 4096], x)
+            acc = O.fr_op("add", O.fr_op("mul", acc, xb), part)
+        return acc
+
+    for i in [0, 1, 12345]:
+        assert np.array_equal(lag[i], eval_at(pow_fr(omega, i)))
+    for i in [0, 7]:
+        assert np.array_equal(ext[i], eval_at(O.fr_op("mul", zeta, pow_fr(eomega, i))))
+    del d_tmp
