@@ -119,6 +119,42 @@ int mzk_domain_op(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *in, uint6
 /* DEVICE buffers; in == out allowed for ops 0, 1, 3, 5; op 4 overwrites in. */
 int mzk_domain_op_device(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *d_in, uint64_t *d_out);
 
+/* ---- quotient evaluation (proofs/src/plonk/evaluation.rs:818-1114) ------ */
+/* Columns are extended-domain (coset) evaluations, 2^extended_k Fr each,
+ * DEVICE pointers, given through HOST arrays of pointers.  Circuit shape: one
+ * standard gate q_l a + q_r b + q_m a b + q_o c + q_c, permutation sets over
+ * advice/fixed columns (chunk_len = cs.degree() - 2 columns each), at most one
+ * logup lookup with one input column and one helper, no trashcans.  Limits:
+ * 16 advice, 16 fixed, 16 permutation columns, 8 sets.  extended_omega and
+ * g_coset are taken from the domain (the fields exist for layout parity with
+ * the CPU restatement). */
+typedef struct {
+    uint32_t k, extended_k;
+    const uint64_t *const *advice; uint32_t n_advice;
+    const uint64_t *const *fixed; uint32_t n_fixed;
+    uint32_t gate_fixed[5];   /* q_l, q_r, q_m, q_o, q_c */
+    uint32_t gate_advice[3];  /* a, b, c */
+    uint32_t n_perm_cols;
+    const uint32_t *perm_col_kind;     /* 0 advice, 1 fixed */
+    const uint32_t *perm_col_index;
+    const uint64_t *const *perm_sigma; /* permutation_pk_cosets, one per column */
+    uint32_t n_perm_sets;
+    const uint64_t *const *perm_z;     /* permutation product cosets, one per set */
+    uint32_t chunk_len;
+    uint32_t blinding_factors;
+    int has_lookup;
+    uint32_t lookup_input_advice, lookup_table_fixed;
+    int32_t lookup_selector_fixed;     /* -1: constant one (no selector) */
+    const uint64_t *lookup_h, *lookup_z, *lookup_m; /* helper, aggregator, multiplicities */
+    const uint64_t *l0, *l_last, *l_active;
+    uint64_t y[4], beta[4], gamma[4], theta[4];
+    uint64_t extended_omega[4], g_coset[4];
+} mzk_quotient_desc;
+/* d_out (2^extended_k Fr) = nu(X) on the extended coset; with divide != 0,
+ * h(X) = nu(X) / (X^n - 1) (evaluate_numerator + divide_by_vanishing_poly,
+ * proofs/src/plonk/prover.rs:664, :713). */
+int mzk_quotient_eval_device(mzk_ctx *ctx, mzk_domain *d, const mzk_quotient_desc *desc, int divide, uint64_t *d_out);
+
 /* ---- seeded synthetic inputs (benchmarks and tests) -------------------- */
 /* n uniform Fr elements (Montgomery) of stream `seed`, elements first..first+n-1 */
 int mzk_gen_rand_fr_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);

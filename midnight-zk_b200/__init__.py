@@ -62,9 +62,75 @@ SIGNATURES = {
     "mzk_domain_constant": (_i32, [_vp, _i32, _i32, _u64p]),
     "mzk_domain_op": (_i32, [_vp, _vp, _i32, _u64p, _u64p]),
     "mzk_domain_op_device": (_i32, [_vp, _vp, _i32, _vp, _vp]),
+    "mzk_quotient_eval_device": (_i32, [_vp, _vp, ctypes.c_void_p, _i32, _vp]),
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
     "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
 }
+
+class QuotientDesc(ctypes.Structure):
+    """mzk_quotient_desc (include/mzk.h): columns of the quotient evaluation."""
+    _fields_ = [
+    ("k", ctypes.c_uint32), ("extended_k", ctypes.c_uint32),
+    ("advice", ctypes.POINTER(ctypes.c_void_p)), ("n_advice", ctypes.c_uint32),
+    ("fixed", ctypes.POINTER(ctypes.c_void_p)), ("n_fixed", ctypes.c_uint32),
+    ("gate_fixed", ctypes.c_uint32 * 5), ("gate_advice", ctypes.c_uint32 * 3),
+    ("n_perm_cols", ctypes.c_uint32),
+    ("perm_col_kind", ctypes.POINTER(ctypes.c_uint32)), ("perm_col_index", ctypes.POINTER(ctypes.c_uint32)),
+    ("perm_sigma", ctypes.POINTER(ctypes.c_void_p)),
+    ("n_perm_sets", ctypes.c_uint32), ("perm_z", ctypes.POINTER(ctypes.c_void_p)),
+    ("chunk_len", ctypes.c_uint32), ("blinding_factors", ctypes.c_uint32),
+    ("has_lookup", ctypes.c_int), ("lookup_input_advice", ctypes.c_uint32), ("lookup_table_fixed", ctypes.c_uint32),
+    ("lookup_selector_fixed", ctypes.c_int32),
+    ("lookup_h", ctypes.c_void_p), ("lookup_z", ctypes.c_void_p), ("lookup_m", ctypes.c_void_p),
+    ("l0", ctypes.c_void_p), ("l_last", ctypes.c_void_p), ("l_active", ctypes.c_void_p),
+    ("y", ctypes.c_uint64 * 4), ("beta", ctypes.c_uint64 * 4), ("gamma", ctypes.c_uint64 * 4),
+    ("theta", ctypes.c_uint64 * 4), ("extended_omega", ctypes.c_uint64 * 4), ("g_coset", ctypes.c_uint64 * 4),
+]
+
+
+def build_quotient_desc(cols, k, extended_k, addr):
+    """Fill a QuotientDesc from `cols` (a dict of column objects and parameters);
+    addr(x) turns each column object into an address (device pointer or host
+    array).  Keeps the pointer arrays alive on the returned object."""
+    d = QuotientDesc()
+    keep = []
+
+    def ptr_array(items):
+        arr = (ctypes.c_void_p * max(1, len(items)))(*[addr(x) for x in items])
+        keep.append(arr)
+        return ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p))
+
+    def u32_array(items):
+        arr = (ctypes.c_uint32 * max(1, len(items)))(*items)
+        keep.append(arr)
+        return ctypes.cast(arr, ctypes.POINTER(ctypes.c_uint32))
+
+    d.k, d.extended_k = k, extended_k
+    d.advice, d.n_advice = ptr_array(cols["advice"]), len(cols["advice"])
+    d.fixed, d.n_fixed = ptr_array(cols["fixed"]), len(cols["fixed"])
+    d.gate_fixed[:] = cols["gate_fixed"]
+    d.gate_advice[:] = cols["gate_advice"]
+    pc = cols.get("perm_cols", [])
+    d.n_perm_cols = len(pc)
+    d.perm_col_kind = u32_array([kind for kind, _ in pc])
+    d.perm_col_index = u32_array([idx for _, idx in pc])
+    d.perm_sigma = ptr_array(cols.get("perm_sigma", []))
+    d.n_perm_sets = len(cols.get("perm_z", []))
+    d.perm_z = ptr_array(cols.get("perm_z", []))
+    d.chunk_len = cols.get("chunk_len", 3)
+    d.blinding_factors = cols.get("blinding_factors", 7)
+    lk = cols.get("lookup")
+    d.has_lookup = 1 if lk else 0
+    if lk:
+        d.lookup_input_advice, d.lookup_table_fixed, d.lookup_selector_fixed = lk["input"], lk["table"], lk["selector"]
+        d.lookup_h, d.lookup_z, d.lookup_m = addr(lk["h"]), addr(lk["z"]), addr(lk["m"])
+    d.l0, d.l_last, d.l_active = addr(cols["l0"]), addr(cols["l_last"]), addr(cols["l_active"])
+    for name in ("y", "beta", "gamma", "theta", "extended_omega", "g_coset"):
+        if name in cols:
+            getattr(d, name)[:] = [int(v) for v in cols[name]]
+    d._keep = keep
+    return d
+
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_CUDA", 4: "ERR_TIMEOUT", 5: "ERR_STATE"}
 
@@ -305,6 +371,11 @@ class EvaluationDomain:
 
     def divide_by_vanishing_poly(self, a):
         return self._run("divide_by_vanishing_poly", a)
+
+    def quotient_eval_device(self, desc, d_out, divide=True):
+        """h(X) (divide) or nu(X) on the extended coset into d_out (device)."""
+        do = d_out.ptr if isinstance(d_out, DeviceBuffer) else int(d_out)
+        _check(lib().mzk_quotient_eval_device(self.ctx.h, self.h, ctypes.byref(desc), 1 if divide else 0, do))
 
     def op_device(self, name, d_in, d_out):
         """Operation on device buffers (pointers or DeviceBuffers)."""

@@ -7,6 +7,7 @@
 
 #include "../../include/mzk.h"
 #include "ntt.hpp"
+#include "quotient.hpp"
 #include "runtime.hpp"
 
 struct mzk_ctx {
@@ -425,6 +426,19 @@ int mzk_domain_op(mzk_ctx* ctx, mzk_domain* d, int op, const uint64_t* in, uint6
     MZK_TRY(mzk::domain_op_device(c, d->impl, op, din, dout, c->stream));
     MZK_CUDA_CHECK(cudaMemcpyAsync(out, dout, out_len * 32, cudaMemcpyDeviceToHost, c->stream));
     MZK_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+    return mzk::OK;
+}
+
+int mzk_quotient_eval_device(mzk_ctx* ctx, mzk_domain* d, const mzk_quotient_desc* desc, int divide,
+                             uint64_t* d_out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || !desc || !d_out) {
+        mzk::set_error("quotient: null argument");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    MZK_TRY(mzk::quotient_eval_device(&ctx->impl, d->impl, desc, divide, d_out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
     return mzk::OK;
 }
 

@@ -1,0 +1,213 @@
+// quotient.cu — fused quotient evaluation over the extended domain.
+//
+// Replaces Evaluator::evaluate_numerator (proofs/src/plonk/evaluation.rs:818-1114)
+// followed by EvaluationDomain::divide_by_vanishing_poly (domain.rs:361-380)
+// for the circuit shape of the single-proof configuration: one standard gate
+// q_l a + q_r b + q_m a b + q_o c + q_c, permutation sets over advice/fixed
+// columns (chunks of cs.degree() - 2 columns), at most one logup lookup with a
+// single input column and a single helper, no trashcans.
+//
+// The reference makes three passes over the 2^extended_k rows (gates, then
+// permutations, then lookups) plus one for the division; here one thread per
+// row reads every column once (coalesced, rotations are whole-row offsets),
+// folds all terms into the y-Horner accumulator in the reference's order and
+// multiplies by 1/t(X) before the single store.  The per-row power w^idx of the
+// permutation's delta term comes from the domain's split twiddle tables.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "../../include/mzk.h"
+#include "field.cuh"
+#include "ntt.hpp"
+#include "quotient.hpp"
+#include "runtime.hpp"
+
+namespace mzk {
+
+namespace {
+
+__device__ __forceinline__ Fr ldfr(const Fr* p, size_t i) {
+    const uint4* s = reinterpret_cast<const uint4*>(p + i);
+    const uint4 a = __ldg(s), b = __ldg(s + 1);
+    Fr r;
+    r.l[0] = a.x; r.l[1] = a.y; r.l[2] = a.z; r.l[3] = a.w;
+    r.l[4] = b.x; r.l[5] = b.y; r.l[6] = b.z; r.l[7] = b.w;
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_quotient(QuotientParams q) {
+    const uint32_t E = 1u << q.log_n;
+    const uint32_t mask = E - 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const Fr one = fr_one();
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < E; idx += stride) {
+        const uint32_t r_next = (idx + (1u << q.log_scale)) & mask;
+        const uint32_t r_last = (idx + (uint32_t)(q.last_rot * (int32_t)(1u << q.log_scale))) & mask;
+        // custom gate (Horner from zero over the single gate polynomial)
+        const Fr a = ldfr(q.advice[q.gate_advice[0]], idx);
+        const Fr b = ldfr(q.advice[q.gate_advice[1]], idx);
+        const Fr c = ldfr(q.advice[q.gate_advice[2]], idx);
+        Fr v = fr_mul(ldfr(q.fixed[q.gate_fixed[0]], idx), a);
+        v = fr_add(v, fr_mul(ldfr(q.fixed[q.gate_fixed[1]], idx), b));
+        v = fr_add(v, fr_mul(fr_mul(a, b), ldfr(q.fixed[q.gate_fixed[2]], idx)));
+        v = fr_add(v, fr_mul(ldfr(q.fixed[q.gate_fixed[3]], idx), c));
+        v = fr_add(v, ldfr(q.fixed[q.gate_fixed[4]], idx));
+        Fr l0 = fr_zero(), la = fr_zero();
+        if (q.n_sets || q.has_lookup) {
+            l0 = ldfr(q.l0, idx);
+            la = ldfr(q.l_active, idx);
+        }
+        if (q.n_sets) {
+            const Fr ll = ldfr(q.l_last, idx);
+            const Fr z0 = ldfr(q.z[0], idx);
+            const Fr zl = ldfr(q.z[q.n_sets - 1], idx);
+            v = fr_add(fr_mul(v, q.y), fr_mul(fr_sub(one, z0), l0));
+            v = fr_add(fr_mul(v, q.y), fr_mul(fr_sub(fr_mul(zl, zl), zl), ll));
+            for (uint32_t s = 1; s < q.n_sets; s++)
+                v = fr_add(fr_mul(v, q.y), fr_mul(fr_sub(ldfr(q.z[s], idx), ldfr(q.z[s - 1], r_last)), l0));
+            // current_delta = beta * g_coset * w^idx
+            Fr ew = q.tlo[idx & 4095u];
+            if (idx >> 12) ew = fr_mul(q.thi[idx >> 12], ew);
+            Fr cur = fr_mul(q.delta_start, ew);
+            uint32_t col = 0;
+            for (uint32_t s = 0; s < q.n_sets; s++) {
+                Fr left = ldfr(q.z[s], r_next);
+                Fr right = ldfr(q.z[s], idx);
+                const uint32_t end = min(col + q.chunk_len, q.n_perm_cols);
+                for (uint32_t j = col; j < end; j++) {
+                    const Fr* colp = q.perm_kind[j] == 0 ? q.advice[q.perm_index[j]] : q.fixed[q.perm_index[j]];
+                    const Fr val = ldfr(colp, idx);
+                    const Fr base = fr_add(val, q.gamma);
+                    left = fr_mul(left, fr_add(base, fr_mul(q.beta, ldfr(q.sigma[j], idx))));
+                    right = fr_mul(right, fr_add(base, cur));
+                    cur = fr_mul(cur, q.delta);
+                }
+                col = end;
+                v = fr_add(fr_mul(v, q.y), fr_mul(fr_sub(left, right), la));
+            }
+        }
+        if (q.has_lookup) {
+            const Fr ll = ldfr(q.l_last, idx);
+            const Fr Z = ldfr(q.lz, idx);
+            const Fr h = ldfr(q.lh, idx);
+            v = fr_add(fr_mul(v, q.y), fr_mul(Z, fr_add(l0, ll)));
+            // single compressed input (Horner over one expression) + beta
+            const Fr f = fr_add(ldfr(q.advice[q.lookup_input], idx), q.beta);
+            v = fr_sub(fr_add(fr_mul(v, q.y), fr_mul(h, f)), one);
+            const Fr tv = fr_add(ldfr(q.fixed[q.lookup_table], idx), q.beta);
+            const Fr sel = q.lookup_selector < 0 ? one : ldfr(q.fixed[q.lookup_selector], idx);
+            Fr u = fr_sub(fr_sub(ldfr(q.lz, r_next), Z), fr_mul(sel, h));
+            u = fr_add(fr_mul(u, tv), ldfr(q.lm, idx));
+            v = fr_add(fr_mul(v, q.y), fr_mul(u, la));
+        }
+        if (q.divide) v = fr_mul(v, q.tinv[idx & (q.tlen - 1)]);
+        q.out[idx] = v;
+    }
+}
+
+Fr fr_from_u64s(const uint64_t* p) {
+    Fr r;
+    std::memcpy(r.l, p, 32);
+    return r;
+}
+
+// DELTA (GENERATOR^(2^S)), curves/src/bls12_381/fq.rs:501-508
+const uint64_t kDelta[4] = {0x70e310d3d146f96aULL, 0x4b64c08919e299e6ULL, 0x51e114186a8b970dULL,
+                            0x6185d06627c067cbULL};
+
+}  // namespace
+
+Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
+                            cudaStream_t st) {
+    if (desc->k != d->k || desc->extended_k != d->ext_k) {
+        set_error("quotient: descriptor k / extended_k differ from the domain's");
+        return ERR_ARG;
+    }
+    if (desc->n_advice > kQMaxAdvice || desc->n_fixed > kQMaxFixed || desc->n_perm_cols > kQMaxPermCols ||
+        desc->n_perm_sets > kQMaxSets) {
+        set_error("quotient: too many columns for the fused kernel");
+        return ERR_ARG;
+    }
+    if (desc->n_perm_sets && (desc->chunk_len == 0 ||
+                              (uint64_t)desc->n_perm_sets * desc->chunk_len < desc->n_perm_cols))
+    {
+        set_error("quotient: permutation sets do not cover the permutation columns");
+        return ERR_ARG;
+    }
+    QuotientParams q;
+    std::memset(&q, 0, sizeof(q));
+    for (uint32_t i = 0; i < desc->n_advice; i++) q.advice[i] = reinterpret_cast<const Fr*>(desc->advice[i]);
+    for (uint32_t i = 0; i < desc->n_fixed; i++) q.fixed[i] = reinterpret_cast<const Fr*>(desc->fixed[i]);
+    for (int i = 0; i < 5; i++) {
+        if (desc->gate_fixed[i] >= desc->n_fixed) {
+            set_error("quotient: gate fixed column out of range");
+            return ERR_ARG;
+        }
+        q.gate_fixed[i] = desc->gate_fixed[i];
+    }
+    for (int i = 0; i < 3; i++) {
+        if (desc->gate_advice[i] >= desc->n_advice) {
+            set_error("quotient: gate advice column out of range");
+            return ERR_ARG;
+        }
+        q.gate_advice[i] = desc->gate_advice[i];
+    }
+    q.n_perm_cols = desc->n_perm_cols;
+    for (uint32_t j = 0; j < desc->n_perm_cols; j++) {
+        const uint32_t kind = desc->perm_col_kind[j], idx = desc->perm_col_index[j];
+        if (kind > 1 || idx >= (kind == 0 ? desc->n_advice : desc->n_fixed)) {
+            set_error("quotient: permutation column out of range");
+            return ERR_ARG;
+        }
+        q.perm_kind[j] = (uint8_t)kind;
+        q.perm_index[j] = (uint8_t)idx;
+        q.sigma[j] = reinterpret_cast<const Fr*>(desc->perm_sigma[j]);
+    }
+    q.n_sets = desc->n_perm_sets;
+    for (uint32_t s = 0; s < desc->n_perm_sets; s++) q.z[s] = reinterpret_cast<const Fr*>(desc->perm_z[s]);
+    q.chunk_len = desc->chunk_len;
+    q.last_rot = -(int32_t)(desc->blinding_factors + 1);
+    q.has_lookup = desc->has_lookup ? 1 : 0;
+    if (q.has_lookup) {
+        if (desc->lookup_input_advice >= desc->n_advice || desc->lookup_table_fixed >= desc->n_fixed ||
+            desc->lookup_selector_fixed >= (int32_t)desc->n_fixed) {
+            set_error("quotient: lookup column out of range");
+            return ERR_ARG;
+        }
+        q.lookup_input = desc->lookup_input_advice;
+        q.lookup_table = desc->lookup_table_fixed;
+        q.lookup_selector = desc->lookup_selector_fixed;
+        q.lh = reinterpret_cast<const Fr*>(desc->lookup_h);
+        q.lz = reinterpret_cast<const Fr*>(desc->lookup_z);
+        q.lm = reinterpret_cast<const Fr*>(desc->lookup_m);
+    }
+    q.l0 = reinterpret_cast<const Fr*>(desc->l0);
+    q.l_last = reinterpret_cast<const Fr*>(desc->l_last);
+    q.l_active = reinterpret_cast<const Fr*>(desc->l_active);
+    q.y = fr_from_u64s(desc->y);
+    q.beta = fr_from_u64s(desc->beta);
+    q.gamma = fr_from_u64s(desc->gamma);
+    q.theta = fr_from_u64s(desc->theta);
+    // beta * g_coset computed on the host (domain constants)
+    host::Fr4 beta4;
+    std::memcpy(beta4.l, desc->beta, 32);
+    const host::Fr4 ds = host::fr_mul(beta4, d->zeta);
+    std::memcpy(q.delta_start.l, ds.l, 32);
+    q.delta = fr_from_u64s(kDelta);
+    q.tlo = d->lo[2];
+    q.thi = d->hi[2];
+    q.tinv = static_cast<const Fr*>(d->d_tinv);
+    q.tlen = (uint32_t)d->t_inv.size();
+    q.divide = divide ? 1 : 0;
+    q.log_n = d->ext_k;
+    q.log_scale = d->ext_k - d->k;
+    q.out = static_cast<Fr*>(d_out);
+    const uint32_t E = 1u << d->ext_k;
+    const uint32_t blocks = (uint32_t)std::min<uint64_t>((E + 255) / 256, (uint64_t)ctx->num_sms * 8);
+    k_quotient<<<blocks, 256, 0, st>>>(q);
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+}  // namespace mzk

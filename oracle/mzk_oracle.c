@@ -1143,3 +1143,163 @@ void or_domain_divide_by_vanishing_poly(const or_domain *d, uint64_t *a, int thr
 #pragma omp parallel for num_threads(threads) schedule(static)
     for (size_t i = 0; i < en; i++) fr_mul(a + 4 * i, a + 4 * i, d->t_evaluations + 4 * (i & mask));
 }
+
+/* ------------------------------------------------------------------------- */
+/* eval_polynomial, proofs/src/utils/arithmetic.rs:59-87: chunked Horner,     */
+/* chunk results scaled by point^start and summed.                           */
+/* ------------------------------------------------------------------------- */
+void or_eval_polynomial(uint64_t out[4], const uint64_t *poly, size_t n, const uint64_t point[4], int threads) {
+    if (threads < 1) threads = 1;
+    size_t chunk = (n + (size_t)threads - 1) / (size_t)threads;
+    if (chunk == 0) chunk = 1;
+    size_t nchunks = (n + chunk - 1) / chunk;
+    u64 *parts = (u64 *)calloc(nchunks ? nchunks : 1, 32);
+#pragma omp parallel for num_threads(threads) schedule(static, 1)
+    for (size_t c = 0; c < nchunks; c++) {
+        size_t lo = c * chunk, hi = lo + chunk > n ? n : lo + chunk;
+        u64 acc[4] = {0}, t[4];
+        for (size_t i = hi; i-- > lo;) {
+            fr_mul(t, acc, point);
+            fr_add(acc, t, poly + 4 * i);
+        }
+        u64 e[1] = {(u64)lo};
+        fr_pow(t, point, e, 1);
+        fr_mul(parts + 4 * c, acc, t);
+    }
+    u64 acc[4] = {0};
+    for (size_t c = 0; c < nchunks; c++) fr_add(acc, acc, parts + 4 * c);
+    memcpy(out, acc, 32);
+    free(parts);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Quotient numerator, proofs/src/plonk/evaluation.rs:818-1114               */
+/* ------------------------------------------------------------------------- */
+/* get_rotation_idx, evaluation.rs:13-16 */
+static size_t rot_idx(size_t idx, int rot, uint32_t log_scale, uint32_t log_n) {
+    size_t mask = ((size_t)1 << log_n) - 1;
+    return (idx + (size_t)((intptr_t)rot << log_scale)) & mask;
+}
+
+void or_quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divide, uint64_t *out, int threads) {
+    if (threads < 1) threads = 1;
+    const uint32_t log_n = d->extended_k, log_scale = d->extended_k - d->k;
+    const size_t E = (size_t)1 << log_n;
+    const int last_rotation = -(int)(d->blinding_factors + 1);
+    u64 delta_start[4];
+    fr_mul(delta_start, d->beta, d->g_coset); /* beta * g_coset (evaluation.rs:864) */
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (size_t idx = 0; idx < E; idx++) {
+        u64 v[4], t[4], u[4], w[4];
+        const size_t r_next = rot_idx(idx, 1, log_scale, log_n);
+        const size_t r_last = rot_idx(idx, last_rotation, log_scale, log_n);
+        /* custom gate: Horner(0, [gate], y) = gate (evaluation.rs:849-852, :680-689) */
+        {
+            const u64 *ql = d->fixed[d->gate_fixed[0]] + 4 * idx, *qr = d->fixed[d->gate_fixed[1]] + 4 * idx;
+            const u64 *qm = d->fixed[d->gate_fixed[2]] + 4 * idx, *qo = d->fixed[d->gate_fixed[3]] + 4 * idx;
+            const u64 *qc = d->fixed[d->gate_fixed[4]] + 4 * idx;
+            const u64 *a = d->advice[d->gate_advice[0]] + 4 * idx, *b = d->advice[d->gate_advice[1]] + 4 * idx;
+            const u64 *c = d->advice[d->gate_advice[2]] + 4 * idx;
+            fr_mul(v, ql, a);
+            fr_mul(t, qr, b);
+            fr_add(v, v, t);
+            fr_mul(t, a, b);
+            fr_mul(t, t, qm);
+            fr_add(v, v, t);
+            fr_mul(t, qo, c);
+            fr_add(v, v, t);
+            fr_add(v, v, qc);
+        }
+        /* permutation (evaluation.rs:857-943) */
+        if (d->n_perm_sets) {
+            const u64 *l0 = d->l0 + 4 * idx, *ll = d->l_last + 4 * idx, *la = d->l_active + 4 * idx;
+            const u64 *z0 = d->perm_z[0] + 4 * idx, *zl = d->perm_z[d->n_perm_sets - 1] + 4 * idx;
+            fr_mul(v, v, d->y);
+            fr_sub(t, FR_R, z0);
+            fr_mul(t, t, l0);
+            fr_add(v, v, t);
+            fr_mul(v, v, d->y);
+            fr_mul(t, zl, zl);
+            fr_sub(t, t, zl);
+            fr_mul(t, t, ll);
+            fr_add(v, v, t);
+            for (uint32_t s = 1; s < d->n_perm_sets; s++) {
+                fr_mul(v, v, d->y);
+                fr_sub(t, d->perm_z[s] + 4 * idx, d->perm_z[s - 1] + 4 * r_last);
+                fr_mul(t, t, l0);
+                fr_add(v, v, t);
+            }
+            /* current_delta = beta * g_coset * omega^idx (omega: extended) */
+            u64 cur[4], ew[4];
+            u64 e1[1] = {(u64)idx};
+            fr_pow(ew, d->extended_omega, e1, 1);
+            fr_mul(cur, delta_start, ew);
+            uint32_t col = 0;
+            for (uint32_t s = 0; s < d->n_perm_sets; s++) {
+                u64 left[4], right[4];
+                memcpy(left, d->perm_z[s] + 4 * r_next, 32);
+                memcpy(right, d->perm_z[s] + 4 * idx, 32);
+                uint32_t end = col + d->chunk_len;
+                if (end > d->n_perm_cols) end = d->n_perm_cols;
+                for (uint32_t j = col; j < end; j++) {
+                    const u64 *val = (d->perm_col_kind[j] == 0 ? d->advice : d->fixed)[d->perm_col_index[j]] + 4 * idx;
+                    fr_mul(t, d->beta, d->perm_sigma[j] + 4 * idx);
+                    fr_add(t, t, val);
+                    fr_add(t, t, d->gamma);
+                    fr_mul(left, left, t);
+                }
+                for (uint32_t j = col; j < end; j++) {
+                    const u64 *val = (d->perm_col_kind[j] == 0 ? d->advice : d->fixed)[d->perm_col_index[j]] + 4 * idx;
+                    fr_add(t, val, cur);
+                    fr_add(t, t, d->gamma);
+                    fr_mul(right, right, t);
+                    fr_mul(cur, cur, FR_DELTA);
+                }
+                col = end;
+                fr_mul(v, v, d->y);
+                fr_sub(t, left, right);
+                fr_mul(t, t, la);
+                fr_add(v, v, t);
+            }
+        }
+        /* lookup (evaluation.rs:1034-1090), one input expression and one helper */
+        if (d->has_lookup) {
+            const u64 *l0 = d->l0 + 4 * idx, *ll = d->l_last + 4 * idx, *la = d->l_active + 4 * idx;
+            const u64 *Z = d->lookup_z + 4 * idx, *h = d->lookup_h + 4 * idx, *m = d->lookup_m + 4 * idx;
+            fr_mul(v, v, d->y);
+            fr_add(t, l0, ll);
+            fr_mul(t, t, Z);
+            fr_add(v, v, t);
+            /* compressed input = Horner(0, [a], theta) = a; product = a + beta;
+               sum of partial products = 1 */
+            u64 f[4];
+            const u64 *a = d->advice[d->lookup_input_advice] + 4 * idx;
+            memset(f, 0, 32);
+            fr_mul(f, f, d->theta);
+            fr_add(f, f, a);
+            fr_add(f, f, d->beta);
+            fr_mul(v, v, d->y);
+            fr_mul(t, h, f);
+            fr_add(v, v, t);
+            fr_sub(v, v, FR_R);
+            /* accumulator: l_active * ((Z(wX) - Z(X) - s*h) * (t + beta) + m) */
+            u64 tbl[4], sel[4];
+            memset(tbl, 0, 32);
+            fr_mul(tbl, tbl, d->theta);
+            fr_add(tbl, tbl, d->fixed[d->lookup_table_fixed] + 4 * idx);
+            fr_add(tbl, tbl, d->beta);
+            if (d->lookup_selector_fixed < 0) memcpy(sel, FR_R, 32);
+            else memcpy(sel, d->fixed[d->lookup_selector_fixed] + 4 * idx, 32);
+            fr_sub(u, d->lookup_z + 4 * r_next, Z);
+            fr_mul(w, sel, h);
+            fr_sub(u, u, w);
+            fr_mul(u, u, tbl);
+            fr_add(u, u, m);
+            fr_mul(u, u, la);
+            fr_mul(v, v, d->y);
+            fr_add(v, v, u);
+        }
+        if (divide) fr_mul(v, v, dom->t_evaluations + 4 * (idx & (dom->t_len - 1)));
+        memcpy(out + 4 * idx, v, 32);
+    }
+}

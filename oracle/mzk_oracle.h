@@ -84,6 +84,8 @@ void or_compute_twiddles(uint64_t *out, const uint64_t omega[4], uint32_t log_n)
 void or_best_fft(uint64_t *a, const uint64_t *twiddles, uint32_t log_n, int threads);
 void or_fft_dif_pruned(uint64_t *a, const uint64_t *twiddles, uint32_t log_n, size_t n_real, int threads);
 void or_dft_naive(uint64_t *out, const uint64_t *a, const uint64_t omega[4], size_t n);
+/* eval_polynomial, proofs/src/utils/arithmetic.rs:59-87 */
+void or_eval_polynomial(uint64_t out[4], const uint64_t *poly, size_t n, const uint64_t point[4], int threads);
 
 /* ---- EvaluationDomain (proofs/src/poly/domain.rs) ---------------------------- */
 typedef struct or_domain or_domain;
@@ -102,6 +104,38 @@ void or_domain_extended_to_coeff(const or_domain *d, uint64_t *a, int threads);
 /* in: 2^extended_k values (destroyed), out: n values */
 void or_domain_extended_to_lagrange(const or_domain *d, uint64_t *a, uint64_t *out, int threads);
 void or_domain_divide_by_vanishing_poly(const or_domain *d, uint64_t *a, int threads);
+
+/* ---- quotient numerator (proofs/src/plonk/evaluation.rs:818-1114) ----------
+ * Restated for the circuit shape of the single-proof configuration: one
+ * standard gate q_l a + q_r b + q_m a b + q_o c + q_c, permutation sets over
+ * advice/fixed columns, at most one logup lookup with one input column and one
+ * helper, no trashcans.  All columns are extended-domain (coset) evaluations
+ * of length 2^extended_k, Fr Montgomery. */
+typedef struct {
+    uint32_t k, extended_k;
+    const uint64_t *const *advice; uint32_t n_advice;
+    const uint64_t *const *fixed; uint32_t n_fixed;
+    uint32_t gate_fixed[5];   /* q_l, q_r, q_m, q_o, q_c */
+    uint32_t gate_advice[3];  /* a, b, c */
+    uint32_t n_perm_cols;
+    const uint32_t *perm_col_kind;   /* 0 advice, 1 fixed */
+    const uint32_t *perm_col_index;
+    const uint64_t *const *perm_sigma; /* n_perm_cols cosets */
+    uint32_t n_perm_sets;
+    const uint64_t *const *perm_z;     /* n_perm_sets cosets */
+    uint32_t chunk_len;                /* cs.degree() - 2 */
+    uint32_t blinding_factors;
+    int has_lookup;
+    uint32_t lookup_input_advice, lookup_table_fixed;
+    int32_t lookup_selector_fixed;     /* -1: constant one */
+    const uint64_t *lookup_h, *lookup_z, *lookup_m;
+    const uint64_t *l0, *l_last, *l_active;
+    uint64_t y[4], beta[4], gamma[4], theta[4];
+    uint64_t extended_omega[4], g_coset[4];
+} or_quotient_desc;
+/* out[i] = numerator nu at extended row i; divide != 0 multiplies by the
+ * inverted vanishing polynomial (divide_by_vanishing_poly, domain.rs:361). */
+void or_quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divide, uint64_t *out, int threads);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,7 @@ def _load():
         "or_best_fft": (None, [_u64p, _u64p, u32, i32]),
         "or_fft_dif_pruned": (None, [_u64p, _u64p, u32, sz, i32]),
         "or_dft_naive": (None, [_u64p, _u64p, _u64p, sz]),
+        "or_eval_polynomial": (None, [_u64p, _u64p, sz, _u64p, i32]),
         "or_domain_new": (ctypes.c_void_p, [u32, u32]),
         "or_domain_free": (None, [ctypes.c_void_p]),
         "or_domain_k": (u32, [ctypes.c_void_p]),
@@ -82,6 +83,7 @@ def _load():
         "or_domain_extended_to_coeff": (None, [ctypes.c_void_p, _u64p, i32]),
         "or_domain_extended_to_lagrange": (None, [ctypes.c_void_p, _u64p, _u64p, i32]),
         "or_domain_divide_by_vanishing_poly": (None, [ctypes.c_void_p, _u64p, i32]),
+        "or_quotient_eval": (None, [ctypes.c_void_p, ctypes.c_void_p, i32, _u64p, i32]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -91,6 +93,27 @@ def _load():
 
 
 lib = _load()
+
+
+class QuotientDesc(ctypes.Structure):
+    """or_quotient_desc (oracle/mzk_oracle.h), host pointers."""
+    _fields_ = [
+    ("k", ctypes.c_uint32), ("extended_k", ctypes.c_uint32),
+    ("advice", ctypes.POINTER(ctypes.c_void_p)), ("n_advice", ctypes.c_uint32),
+    ("fixed", ctypes.POINTER(ctypes.c_void_p)), ("n_fixed", ctypes.c_uint32),
+    ("gate_fixed", ctypes.c_uint32 * 5), ("gate_advice", ctypes.c_uint32 * 3),
+    ("n_perm_cols", ctypes.c_uint32),
+    ("perm_col_kind", ctypes.POINTER(ctypes.c_uint32)), ("perm_col_index", ctypes.POINTER(ctypes.c_uint32)),
+    ("perm_sigma", ctypes.POINTER(ctypes.c_void_p)),
+    ("n_perm_sets", ctypes.c_uint32), ("perm_z", ctypes.POINTER(ctypes.c_void_p)),
+    ("chunk_len", ctypes.c_uint32), ("blinding_factors", ctypes.c_uint32),
+    ("has_lookup", ctypes.c_int), ("lookup_input_advice", ctypes.c_uint32), ("lookup_table_fixed", ctypes.c_uint32),
+    ("lookup_selector_fixed", ctypes.c_int32),
+    ("lookup_h", ctypes.c_void_p), ("lookup_z", ctypes.c_void_p), ("lookup_m", ctypes.c_void_p),
+    ("l0", ctypes.c_void_p), ("l_last", ctypes.c_void_p), ("l_active", ctypes.c_void_p),
+    ("y", ctypes.c_uint64 * 4), ("beta", ctypes.c_uint64 * 4), ("gamma", ctypes.c_uint64 * 4),
+    ("theta", ctypes.c_uint64 * 4), ("extended_omega", ctypes.c_uint64 * 4), ("g_coset", ctypes.c_uint64 * 4),
+]
 
 
 def threads_default():
@@ -258,6 +281,25 @@ def dft_naive(a, omega):
     return o
 
 
+def eval_polynomial(poly, point, threads=None):
+    o = np.zeros(4, np.uint64)
+    poly = np.ascontiguousarray(poly, np.uint64)
+    lib.or_eval_polynomial(P(o), P(poly), poly.shape[0], P(np.ascontiguousarray(point, np.uint64)),
+                           threads or threads_default())
+    return o
+
+
+def fr_pow(x, e):
+    r = fr_const(0)
+    b = np.ascontiguousarray(x, np.uint64).copy()
+    while e:
+        if e & 1:
+            r = fr_op("mul", r, b)
+        b = fr_op("mul", b, b)
+        e >>= 1
+    return r
+
+
 class Domain:
     """EvaluationDomain restatement (proofs/src/poly/domain.rs:54-414)."""
 
@@ -303,6 +345,11 @@ class Domain:
         a = np.ascontiguousarray(a, np.uint64).copy()
         o = np.zeros((self.n, 4), np.uint64)
         lib.or_domain_extended_to_lagrange(self.h, P(a), P(o), threads or threads_default())
+        return o
+
+    def quotient_eval(self, desc, divide=True, threads=None):
+        o = np.zeros((self.extended_len, 4), np.uint64)
+        lib.or_quotient_eval(ctypes.byref(desc), self.h, 1 if divide else 0, P(o), threads or threads_default())
         return o
 
     def divide_by_vanishing_poly(self, a, threads=None):

@@ -314,3 +314,17 @@ def test_divide_by_vanishing_poly():
     evals = O.dft_naive(scaled, d.get(2))
     q = d.divide_by_vanishing_poly(evals)
     assert all(np.array_equal(row, O.fr_const(0)) for row in q)
+
+
+def test_eval_polynomial_matches_horner_and_dft():
+    a = O.rand_fr(91, 1000)
+    x = O.rand_fr(92, 1)[0]
+    acc = np.zeros(4, np.uint64)
+    for c in a[::-1]:
+        acc = O.fr_op("add", O.fr_op("mul", acc, x), c)
+    for threads in (1, 3, 8):
+        assert np.array_equal(O.eval_polynomial(a, x, threads), acc)
+    d = O.Domain(2, 6)
+    b = O.rand_fr(93, 64)
+    lag = d.coeff_to_lagrange(b)
+    assert np.array_equal(lag[5], O.eval_polynomial(b, O.fr_pow(d.get(0), 5)))

@@ -1,0 +1,132 @@
+"""The oracle's quotient restatement against an independent pure-Python
+evaluation of the same formula (proofs/src/plonk/evaluation.rs:818-1114) with
+Python integers, on tiny domains.  CPU only."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+R = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
+MONT = pow(2, 256, R)
+MINV = pow(MONT, -1, R)
+
+
+def val(x):
+    return O.to_int(x) * MINV % R
+
+
+def mont(v):
+    return O.from_int(v % R * MONT % R, 4)
+
+
+def column(seed, E):
+    return O.rand_fr(seed, E)
+
+
+def python_numerator(cols, k, ek, y, beta, gamma, zeta, ext_omega, divide, tinv):
+    E = 1 << ek
+    log_scale = ek - k
+    delta = val(O.fr_const(5))
+    out = []
+    rot = lambda idx, r: (idx + (r << log_scale)) % E
+    A = [[val(c[i]) for i in range(E)] for c in cols["advice"]]
+    F = [[val(c[i]) for i in range(E)] for c in cols["fixed"]]
+    S = [[val(c[i]) for i in range(E)] for c in cols["perm_sigma"]]
+    Z = [[val(c[i]) for i in range(E)] for c in cols["perm_z"]]
+    l0 = [val(cols["l0"][i]) for i in range(E)]
+    ll = [val(cols["l_last"][i]) for i in range(E)]
+    la = [val(cols["l_active"][i]) for i in range(E)]
+    lk = cols.get("lookup")
+    if lk:
+        H = [val(lk["h"][i]) for i in range(E)]
+        LZ = [val(lk["z"][i]) for i in range(E)]
+        LM = [val(lk["m"][i]) for i in range(E)]
+    bf = cols["blinding_factors"]
+    for idx in range(E):
+        a, b, c = (A[j][idx] for j in cols["gate_advice"])
+        ql, qr, qm, qo, qc = (F[j][idx] for j in cols["gate_fixed"])
+        v = (ql * a + qr * b + qm * a * b + qo * c + qc) % R
+        if Z:
+            v = (v * y + (1 - Z[0][idx]) * l0[idx]) % R
+            zl = Z[-1][idx]
+            v = (v * y + (zl * zl - zl) * ll[idx]) % R
+            for s in range(1, len(Z)):
+                v = (v * y + (Z[s][idx] - Z[s - 1][rot(idx, -(bf + 1))]) * l0[idx]) % R
+            cur = beta * zeta * pow(ext_omega, idx, R) % R
+            pc = cols["perm_cols"]
+            for s in range(len(Z)):
+                left, right = Z[s][rot(idx, 1)], Z[s][idx]
+                for j in range(s * 3, min(s * 3 + 3, len(pc))):
+                    kind, ci = pc[j]
+                    x = (A if kind == 0 else F)[ci][idx]
+                    left = left * (x + beta * S[j][idx] + gamma) % R
+                    right = right * (x + cur + gamma) % R
+                    cur = cur * delta % R
+                v = (v * y + (left - right) * la[idx]) % R
+        if lk:
+            v = (v * y + LZ[idx] * (l0[idx] + ll[idx])) % R
+            f = A[lk["input"]][idx] + beta
+            v = (v * y + H[idx] * f - 1) % R
+            t = F[lk["table"]][idx] + beta
+            sel = 1 if lk["selector"] < 0 else F[lk["selector"]][idx]
+            v = (v * y + la[idx] * ((LZ[rot(idx, 1)] - LZ[idx] - sel * H[idx]) * t + LM[idx])) % R
+        if divide:
+            v = v * tinv[idx & (len(tinv) - 1)] % R
+        out.append(v)
+    return out
+
+
+@pytest.mark.parametrize("n_perm,n_sets,sel", [(0, 0, None), (3, 1, -1), (5, 2, 6), (7, 3, 6)])
+def test_oracle_quotient_matches_python(n_perm, n_sets, sel):
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_quotient_gpu import make_columns
+
+    k, j = 2, 5
+    d = O.Domain(j, k)
+    ek = d.extended_k
+    E = 1 << ek
+    cols = make_columns(5 + n_sets, E, n_perm, n_sets, sel)
+    cols["extended_omega"], cols["g_coset"] = d.get(2), d.get(3)
+    keep = []
+
+    def ptrs(items):
+        arr = (ctypes.c_void_p * max(1, len(items)))(*[a.ctypes.data for a in items])
+        keep.append(arr)
+        return ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p))
+
+    def u32s(items):
+        arr = (ctypes.c_uint32 * max(1, len(items)))(*items)
+        keep.append(arr)
+        return ctypes.cast(arr, ctypes.POINTER(ctypes.c_uint32))
+
+    q = O.QuotientDesc()
+    q.k, q.extended_k = k, ek
+    q.advice, q.n_advice = ptrs(cols["advice"]), 3
+    q.fixed, q.n_fixed = ptrs(cols["fixed"]), 7
+    q.gate_fixed[:] = cols["gate_fixed"]
+    q.gate_advice[:] = cols["gate_advice"]
+    q.n_perm_cols = n_perm
+    q.perm_col_kind = u32s([a for a, _ in cols["perm_cols"]])
+    q.perm_col_index = u32s([b for _, b in cols["perm_cols"]])
+    q.perm_sigma = ptrs(cols["perm_sigma"])
+    q.n_perm_sets = n_sets
+    q.perm_z = ptrs(cols["perm_z"])
+    q.chunk_len, q.blinding_factors = 3, 7
+    if sel is not None:
+        lk = cols["lookup"]
+        q.has_lookup = 1
+        q.lookup_input_advice, q.lookup_table_fixed, q.lookup_selector_fixed = 0, 5, sel
+        q.lookup_h, q.lookup_z, q.lookup_m = lk["h"].ctypes.data, lk["z"].ctypes.data, lk["m"].ctypes.data
+    q.l0, q.l_last, q.l_active = cols["l0"].ctypes.data, cols["l_last"].ctypes.data, cols["l_active"].ctypes.data
+    for name in ("y", "beta", "gamma", "theta", "extended_omega", "g_coset"):
+        getattr(q, name)[:] = [int(v) for v in cols[name]]
+    tinv = [val(d.get(7, i)) for i in range(1 << (ek - k))]
+    for divide in (False, True):
+        got = d.quotient_eval(q, divide)
+        want = python_numerator(cols, k, ek, val(cols["y"]), val(cols["beta"]), val(cols["gamma"]),
+                                val(d.get(3)), val(d.get(2)), divide, tinv)
+        assert [val(x) for x in got] == want
