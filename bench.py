@@ -48,6 +48,8 @@ def parse_args():
     p.add_argument("--cpu-sample-log-n", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true", help="skip the NTT and quotient lines")
+    p.add_argument("--ntt-log-n", type=int, default=24)
     return p.parse_args()
 
 
@@ -120,6 +122,75 @@ def traffic_from_profiles(c):
     return None
 
 
+IMAD_PER_FR_MUL = 272  # CIOS, 8 limbs: 2*8^2+8 = 136 products x (lo, hi)
+
+
+def measure_ntt(mzk, ctx, stream, log_n, reps):
+    """EvaluationDomain NTTs at n = 2^log_n (extended 2^(log_n+2)), inputs resident."""
+    import torch
+    n, en = 1 << log_n, 1 << (log_n + 2)
+    dom = mzk.EvaluationDomain(ctx, 5, log_n)
+    da = ctx.gen_rand_fr(0x7007, n)
+    de = ctx.alloc(en * 32)
+    ops = [  # name, in, out, transform size, algorithmic bytes
+        ("coeff_to_lagrange", da, da, n, 64 * n),
+        ("lagrange_to_coeff", da, da, n, 64 * n),
+        ("coeff_to_extended", da, de, en, 32 * n + 32 * en),
+        ("extended_to_coeff", de, de, en, 64 * en),
+    ]
+    out = {}
+    for name, src, dst, size, nbytes in ops:
+        dom.op_device(name, src, dst)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            dom.op_device(name, src, dst)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        lg = size.bit_length() - 1
+        imad = (size // 2) * lg * IMAD_PER_FR_MUL
+        out[name] = {"n": size, "ms": round(ms, 3), "elements_per_s": round(size / (ms / 1e3), 1),
+                     "hbm_gbs_algorithmic": round(nbytes / (ms / 1e3) / 1e9, 1),
+                     "imad_t_per_s": round(imad / (ms / 1e3) / 1e12, 3)}
+    dom.close()
+    return out
+
+
+def measure_quotient(mzk, ctx, stream, k, reps):
+    """Fused quotient evaluation for the k-row proof circuit (extended 2^(k+2) rows)."""
+    import torch
+    E = 1 << (k + 2)
+    dom = mzk.EvaluationDomain(ctx, 5, k)
+    seed = iter(range(1000, 2000))
+    col = lambda: ctx.gen_rand_fr(next(seed), E)
+    cols = {
+        "advice": [col() for _ in range(3)], "fixed": [col() for _ in range(7)],
+        "gate_fixed": [0, 1, 2, 3, 4], "gate_advice": [0, 1, 2],
+        "perm_cols": [(0, 0), (0, 1), (0, 2)], "perm_sigma": [col() for _ in range(3)], "perm_z": [col()],
+        "chunk_len": 3, "blinding_factors": 7, "l0": col(), "l_last": col(), "l_active": col(),
+        "lookup": {"input": 0, "table": 5, "selector": -1, "h": col(), "z": col(), "m": col()},
+    }
+    import numpy as np
+    for name in ("y", "beta", "gamma", "theta"):
+        cols[name] = np.array([7, 0, 0, 0], np.uint64)
+    desc = mzk.build_quotient_desc(cols, k, k + 2, lambda b: b.ptr)
+    out = ctx.alloc(E * 32)
+    dom.quotient_eval_device(desc, out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        dom.quotient_eval_device(desc, out)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    ncols = 3 + 7 + 3 + 1 + 3 + 3
+    dom.close()
+    return {"rows": E, "ms": round(ms, 3), "rows_per_s": round(E / (ms / 1e3), 1),
+            "hbm_gbs_algorithmic": round((ncols + 1) * 32 * E / (ms / 1e3) / 1e9, 1),
+            "columns_read": ncols}
+
+
 def dist_init(backend):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -184,6 +255,7 @@ def run_ours(args):
     db = ctx.gen_bases(0xBA5E + rank, n)
     imad_peak, fp_mul_rate, imad_variants = ctx.probe_imad_peak()
     # the Montgomery multiplication issues ~588 IMAD; its measured rate bounds the pipe from below
+    madd_rate = imad_variants.pop("madd_regs")
     imad_peak = max(imad_peak, max(imad_variants.values()), fp_mul_rate * IMAD_PER_FP_MUL_ISSUED)
     stream = torch.cuda.ExternalStream(ctx.stream)
 
@@ -277,6 +349,14 @@ def run_ours(args):
                "h2d_bytes_per_step": n * 32 + n * 96, "d2h_bytes_per_step": windows * 192 + 4,
                "api": "mzk_msm_g1 (host pointers, pinned)"}
 
+    extra_ntt = extra_q = None
+    if not args.no_extras:
+        del ds, db
+        extra_ntt = measure_ntt(mzk, ctx, stream, args.ntt_log_n, 5)
+        extra_q = measure_quotient(mzk, ctx, stream, 18, 5)
+        ds = ctx.gen_rand_fr(0xC0FFEE + rank, n)
+        db = ctx.gen_bases(0xBA5E + rank, n)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -305,6 +385,8 @@ def run_ours(args):
             "phases_ms": {k: round(v[0] / max(v[1], 1), 3) for k, v in phases.items()},
             "fp_mul_rate_g_per_s": round(fp_mul_rate / 1e9, 2),
             "imad_probe_t_per_s": {k: round(v / 1e12, 3) for k, v in imad_variants.items()},
+            "madd_in_registers_g_per_s": round(madd_rate / 1e9, 3),
+            "ntt": extra_ntt, "quotient_k18": extra_q,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -51,8 +51,9 @@ int mzk_ctx_phase_stats(mzk_ctx *ctx, double *ms_out, uint64_t *count_out, int m
  * mad.lo.cc/madc.hi pairs as the field code issues them) and 12-limb
  * Montgomery multiplications per second, measured by microbenchmark kernels.
  * variants (may be NULL): [0] independent mad.lo+mad.hi, [1] carry-chained
- * pairs, [2] independent mad.lo only, all in IMAD/s. */
-int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s, double variants[3]);
+ * pairs, [2] independent mad.lo only (IMAD/s), [3] mixed XYZZ additions per
+ * second with operands in registers. */
+int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s, double variants[4]);
 
 /* ---- device memory helpers (for callers without a CUDA runtime) ---------- */
 int mzk_device_alloc(mzk_ctx *ctx, size_t bytes, void **out);
@@ -89,6 +90,18 @@ int mzk_msm_g1_device(mzk_ctx *ctx, const uint64_t *d_scalars, const uint64_t *d
  * GPU work of two calls that overlapped would race on it.
  */
 int mzk_msm_g1_noalloc(const uint64_t *d_scalars, const uint64_t *d_bases, size_t n, uint64_t out[18], void *stream);
+/* Batched MSMs over one shared device SRS: item m is
+ * sum_i scalars_m[i] * bases[base_offset_m + i] for i < n_m (commit_many's
+ * `bases[..size]` prefix, proofs/src/poly/kzg/mod.rs:98-103, with any offset).
+ * All items are sorted together and accumulated in one load-balanced launch.
+ * out: count x 18 u64 G1Projective results, in item order. */
+typedef struct {
+    const uint64_t *d_scalars; /* n x 4 u64 Fq, DEVICE */
+    uint64_t base_offset;
+    uint64_t n;
+} mzk_msm_batch_item;
+int mzk_msm_g1_batch_device(mzk_ctx *ctx, const uint64_t *d_bases, size_t bases_len, const mzk_msm_batch_item *items,
+                            size_t count, uint64_t *out);
 /* Window width override (0 = automatic), for tuning and tests. */
 int mzk_msm_set_window(mzk_ctx *ctx, int c);
 int mzk_msm_pick_window(size_t n);

@@ -54,6 +54,7 @@ SIGNATURES = {
     "mzk_msm_g1": (_i32, [_vp, _u64p, _u64p, _sz, _u64p]),
     "mzk_msm_g1_device": (_i32, [_vp, _vp, _vp, _sz, _u64p]),
     "mzk_msm_g1_noalloc": (_i32, [_vp, _vp, _sz, _u64p, _vp]),
+    "mzk_msm_g1_batch_device": (_i32, [_vp, _vp, _sz, _vp, _sz, _u64p]),
     "mzk_msm_set_window": (_i32, [_vp, _i32]),
     "mzk_msm_pick_window": (_i32, [_sz]),
     "mzk_domain_create": (_i32, [_vp, _u32, _u32, ctypes.POINTER(_vp)]),
@@ -66,6 +67,11 @@ SIGNATURES = {
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
     "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
 }
+
+class MsmBatchItem(ctypes.Structure):
+    """mzk_msm_batch_item (include/mzk.h)."""
+    _fields_ = [("d_scalars", ctypes.c_void_p), ("base_offset", ctypes.c_uint64), ("n", ctypes.c_uint64)]
+
 
 class QuotientDesc(ctypes.Structure):
     """mzk_quotient_desc (include/mzk.h): columns of the quotient evaluation."""
@@ -257,9 +263,9 @@ class Context:
     def probe_imad_peak(self):
         """(IMAD/s, 12-limb Montgomery multiplications/s, {variant: IMAD/s}) of this GPU."""
         a, b = ctypes.c_double(), ctypes.c_double()
-        v = (ctypes.c_double * 3)()
+        v = (ctypes.c_double * 4)()
         _check(lib().mzk_probe_imad_peak(self.h, ctypes.byref(a), ctypes.byref(b), v))
-        return a.value, b.value, {"mad_lo_hi": v[0], "mad_cc_chain": v[1], "mad_lo": v[2]}
+        return a.value, b.value, {"mad_lo_hi": v[0], "mad_cc_chain": v[1], "mad_lo": v[2], "madd_regs": v[3]}
 
     def msm_last_shape(self):
         c, w, e = _i32(), _i32(), np.zeros(1, np.uint64)
@@ -290,6 +296,17 @@ class Context:
         out = np.zeros(18, np.uint64)
         _check(lib().mzk_msm_g1_device(self.h, ds, db, int(n), _ptr(out)))
         return out
+
+    def msm_batch_device(self, d_bases, bases_len, items):
+        """items: [(d_scalars, base_offset, n)] -> (len(items), 18) uint64 G1Projective."""
+        arr = (MsmBatchItem * max(1, len(items)))()
+        for i, (ds, off, n) in enumerate(items):
+            arr[i].d_scalars = ds.ptr if isinstance(ds, DeviceBuffer) else int(ds)
+            arr[i].base_offset, arr[i].n = int(off), int(n)
+        db = d_bases.ptr if isinstance(d_bases, DeviceBuffer) else int(d_bases)
+        out = np.zeros((max(1, len(items)), 18), np.uint64)
+        _check(lib().mzk_msm_g1_batch_device(self.h, db, int(bases_len), ctypes.addressof(arr), len(items), _ptr(out)))
+        return out[:len(items)]
 
     # ---- synthetic inputs ----
     def gen_rand_fr(self, seed, n, first=0, out=None):

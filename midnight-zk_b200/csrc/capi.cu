@@ -278,7 +278,7 @@ int mzk_msm_last_shape(mzk_ctx* ctx, int* c, int* windows, uint64_t* entries) {
     return mzk::OK;
 }
 
-int mzk_probe_imad_peak(mzk_ctx* ctx, double* imad_per_s, double* fp_mul_per_s, double variants[3]) {
+int mzk_probe_imad_peak(mzk_ctx* ctx, double* imad_per_s, double* fp_mul_per_s, double variants[4]) {
     if (int s = check_ctx(ctx)) return s;
     Guard g(ctx);
     return mzk::probe_imad(&ctx->impl, imad_per_s, fp_mul_per_s, variants);
@@ -440,6 +440,19 @@ int mzk_quotient_eval_device(mzk_ctx* ctx, mzk_domain* d, const mzk_quotient_des
     MZK_TRY(mzk::quotient_eval_device(&ctx->impl, d->impl, desc, divide, d_out, ctx->impl.stream));
     MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
     return mzk::OK;
+}
+
+int mzk_msm_g1_batch_device(mzk_ctx* ctx, const uint64_t* d_bases, size_t bases_len, const mzk_msm_batch_item* items,
+                            size_t count, uint64_t* out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!out || (count && (!items || !d_bases))) {
+        mzk::set_error("msm batch: null pointer");
+        return mzk::ERR_ARG;
+    }
+    static_assert(sizeof(mzk_msm_batch_item) == sizeof(mzk::BatchItem), "batch item layout");
+    Guard g(ctx);
+    return mzk::msm_g1_batch_device(&ctx->impl, d_bases, bases_len, reinterpret_cast<const mzk::BatchItem*>(items),
+                                    count, out, ctx->impl.stream);
 }
 
 }  // extern "C"

@@ -592,6 +592,312 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
 namespace mzk {
 
 // ---------------------------------------------------------------------------
+// Batched MSMs over one shared device SRS.
+//
+// Many MSMs (a proof's commitments, or many proofs' commitments) run as one
+// MSM of MSMs: every item keeps its own window width, its keys are laid out
+// back to back in one key space, so ONE counting sort orders all entries and
+// ONE accumulate launch balances the work of all items across the GPU (an
+// item of 2^12 points and one of 2^22 share the same chunks).  Only the final
+// combination of each item's window sums is per item.  Bases of item m are
+// bases[base_offset_m .. base_offset_m + n_m), like commit_many's
+// `bases[..size]` prefix of the SRS (proofs/src/poly/kzg/mod.rs:98-103).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BatchItemDev {
+    const Fr* scalars;
+    uint32_t n, point_start, base_offset;
+    uint32_t c, windows, nb, key_start;
+};
+
+struct BatchWinDev {
+    uint32_t key_start, nb, group_start, plane_block_start;
+    int planes;
+};
+
+__device__ __forceinline__ uint32_t find_item(const BatchItemDev* items, uint32_t n_items, uint32_t p) {
+    uint32_t lo = 0, hi = n_items;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (items[mid].point_start <= p) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <bool kScatter>
+__global__ void k_digits_batch(const BatchItemDev* __restrict__ items, uint32_t n_items, uint32_t total_points,
+                               int max_windows, uint32_t* __restrict__ counts_or_fill,
+                               const uint32_t* __restrict__ offsets, uint32_t* __restrict__ sorted) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total_points; base += stride) {
+        const uint32_t p = base + threadIdx.x;
+        const bool valid = p < total_points;
+        BatchItemDev it = items[valid ? find_item(items, n_items, p) : 0];
+        const uint32_t local = p - it.point_start;
+        Fr s = valid ? fr_from_mont(load_fr(it.scalars, local)) : fr_zero();
+        uint32_t carry = 0;
+        for (int w = 0; w < max_windows; w++) {
+            bool neg = false;
+            uint32_t key = kNoKey;
+            if (valid && w < (int)it.windows) {
+                key = next_digit(s, w, (int)it.c, it.nb, carry, neg);
+                if (key != kNoKey) key += it.key_start;
+            }
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            const int leader = __ffs(peers) - 1;
+            if (!kScatter) {
+                if (key != kNoKey && lane == leader) atomicAdd(&counts_or_fill[key], (uint32_t)__popc(peers));
+            } else {
+                uint32_t slot = 0;
+                if (key != kNoKey && lane == leader) slot = atomicAdd(&counts_or_fill[key], (uint32_t)__popc(peers));
+                slot = __shfl_sync(peers, slot, leader);
+                if (key != kNoKey) {
+                    const uint32_t pos = offsets[key] + slot + (uint32_t)__popc(peers & lt_mask);
+                    sorted[pos] = (it.base_offset + local) | (neg ? 0x80000000u : 0u);
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t find_win_by_group(const BatchWinDev* wins, uint32_t n_wins, uint32_t g) {
+    uint32_t lo = 0, hi = n_wins;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (wins[mid].group_start <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_group_sums_batch(const Xyzz* __restrict__ buckets,
+                                                                     const uint32_t* __restrict__ offsets,
+                                                                     const BatchWinDev* __restrict__ wins,
+                                                                     uint32_t n_wins, uint32_t total_groups,
+                                                                     Xyzz* __restrict__ run_out,
+                                                                     Xyzz* __restrict__ tot_out) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= total_groups) return;
+    const BatchWinDev wd = wins[find_win_by_group(wins, n_wins, gid)];
+    const uint32_t key0 = wd.key_start + (gid - wd.group_start) * kGroupLen;
+    Xyzz run, tot;
+    xyzz_set_inf(run);
+    xyzz_set_inf(tot);
+    for (int b = kGroupLen - 1; b >= 0; b--) {
+        const uint32_t key = key0 + (uint32_t)b;
+        if (offsets[key + 1] > offsets[key]) run = xyzz_add(run, load_xyzz(&buckets[key]));
+        tot = xyzz_add(tot, run);
+    }
+    store_xyzz(&run_out[gid], run);
+    store_xyzz(&tot_out[gid], tot);
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_plane_sums_batch(const Xyzz* __restrict__ run,
+                                                                     const Xyzz* __restrict__ tot,
+                                                                     const BatchWinDev* __restrict__ wins,
+                                                                     uint32_t n_wins, Xyzz* __restrict__ plane_out) {
+    extern __shared__ uint4 smem_raw[];
+    Xyzz* sm = reinterpret_cast<Xyzz*>(smem_raw);
+    // block -> (window, plane)
+    uint32_t lo = 0, hi = n_wins;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (wins[mid].plane_block_start <= blockIdx.x) lo = mid;
+        else hi = mid;
+    }
+    const BatchWinDev wd = wins[lo];
+    const int plane = (int)(blockIdx.x - wd.plane_block_start);
+    const uint32_t groups = wd.nb / kGroupLen;
+    const Xyzz* src = (plane == wd.planes ? tot : run) + wd.group_start;
+    Xyzz acc;
+    xyzz_set_inf(acc);
+    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x)
+        if (plane == wd.planes || ((g >> plane) & 1u)) acc = xyzz_add(acc, load_xyzz(&src[g]));
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) sm[threadIdx.x] = xyzz_add(sm[threadIdx.x], sm[threadIdx.x + off]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) store_xyzz(&plane_out[blockIdx.x], sm[0]);
+}
+
+__global__ void k_window_finish_batch(const Xyzz* __restrict__ planes_in, const BatchWinDev* __restrict__ wins,
+                                      uint32_t n_wins, Xyzz* __restrict__ out) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n_wins) return;
+    const BatchWinDev wd = wins[w];
+    const Xyzz* q = planes_in + wd.plane_block_start;
+    Xyzz acc;
+    xyzz_set_inf(acc);
+    for (int j = wd.planes - 1; j >= 0; j--) {
+        acc = xyzz_dbl(acc);
+        acc = xyzz_add(acc, load_xyzz(&q[j]));
+    }
+    for (int b = 1; b < kGroupLen; b <<= 1) acc = xyzz_dbl(acc);
+    acc = xyzz_add(acc, load_xyzz(&q[wd.planes]));
+    store_xyzz(&out[w], acc);
+}
+
+}  // namespace
+
+Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, const BatchItem* items, size_t count,
+                           uint64_t* out, cudaStream_t st) {
+    std::memset(out, 0, count * 18 * 8);
+    std::vector<BatchItemDev> hi;
+    std::vector<BatchWinDev> hw;
+    std::vector<size_t> item_of;  // position in `items` of every device item
+    uint64_t points = 0, keys = 0, entries = 0, groups = 0, plane_blocks = 0;
+    int max_windows = 0;
+    for (size_t m = 0; m < count; m++) {
+        const BatchItem& it = items[m];
+        if (it.n == 0) continue;
+        if (!it.d_scalars) {
+            set_error("msm batch: null scalars in item " + std::to_string(m));
+            return ERR_ARG;
+        }
+        if (it.base_offset + it.n > bases_len || it.base_offset + it.n >= 0x80000000ull) {
+            set_error("msm batch: item " + std::to_string(m) + " reads past the bases");
+            return ERR_ARG;
+        }
+        const int c = ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(it.n);
+        const MsmShape sh = make_shape(c);
+        BatchItemDev d;
+        d.scalars = static_cast<const Fr*>(it.d_scalars);
+        d.n = (uint32_t)it.n;
+        d.point_start = (uint32_t)points;
+        d.base_offset = (uint32_t)it.base_offset;
+        d.c = (uint32_t)sh.c;
+        d.windows = (uint32_t)sh.windows;
+        d.nb = sh.nb;
+        d.key_start = (uint32_t)keys;
+        for (int w = 0; w < sh.windows; w++) {
+            BatchWinDev wd;
+            wd.key_start = (uint32_t)(keys + (uint64_t)w * sh.nb);
+            wd.nb = sh.nb;
+            wd.group_start = (uint32_t)groups;
+            wd.plane_block_start = (uint32_t)plane_blocks;
+            wd.planes = sh.planes;
+            hw.push_back(wd);
+            groups += sh.groups;
+            plane_blocks += (uint64_t)sh.planes + 1;
+        }
+        points += it.n;
+        keys += sh.keys;
+        entries += (uint64_t)sh.windows * it.n;
+        max_windows = std::max(max_windows, sh.windows);
+        hi.push_back(d);
+        item_of.push_back(m);
+    }
+    if (hi.empty()) return OK;
+    if (points >= 0xffffffffull || keys >= 0xffffffffull || entries >= 0xffffffffull) {
+        set_error("msm batch: more than 2^32 points, keys or entries");
+        return ERR_ARG;
+    }
+    int acc_blocks_per_sm = 0;
+    MZK_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&acc_blocks_per_sm, k_accumulate, kAccThreads, 0));
+    if (acc_blocks_per_sm < 1) acc_blocks_per_sm = 1;
+    const uint32_t acc_blocks = (uint32_t)(ctx->num_sms * acc_blocks_per_sm);
+    const uint32_t acc_threads = acc_blocks * kAccThreads;
+    const size_t n_wins = hw.size();
+    void *d_items, *d_wins, *counts, *offsets, *sorted, *buckets, *partials, *owner, *long_count, *long_list, *run, *tot,
+        *planes, *wsum;
+    MZK_TRY(ctx->ensure("batch_items", hi.size() * sizeof(BatchItemDev), &d_items));
+    MZK_TRY(ctx->ensure("batch_wins", n_wins * sizeof(BatchWinDev), &d_wins));
+    MZK_TRY(ctx->ensure("msm_counts", (keys + 1) * 4, &counts));
+    MZK_TRY(ctx->ensure("msm_offsets", (keys + 1) * 4, &offsets));
+    MZK_TRY(ctx->ensure("msm_sorted", entries * 4, &sorted));
+    MZK_TRY(ctx->ensure("msm_buckets", keys * sizeof(Xyzz), &buckets));
+    MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
+    MZK_TRY(ctx->ensure("msm_owner", (size_t)acc_threads * 4, &owner));
+    MZK_TRY(ctx->ensure("msm_long_count", 64, &long_count));
+    MZK_TRY(ctx->ensure("msm_long_list", (size_t)acc_threads * sizeof(uint2), &long_list));
+    MZK_TRY(ctx->ensure("msm_run", groups * sizeof(Xyzz), &run));
+    MZK_TRY(ctx->ensure("msm_tot", groups * sizeof(Xyzz), &tot));
+    MZK_TRY(ctx->ensure("msm_planes", plane_blocks * sizeof(Xyzz), &planes));
+    MZK_TRY(ctx->ensure("msm_wsum", n_wins * sizeof(Xyzz), &wsum));
+    void* host_wsum;
+    MZK_TRY(ctx->ensure_pinned(n_wins * sizeof(Xyzz) + 64, &host_wsum));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_items, hi.data(), hi.size() * sizeof(BatchItemDev), cudaMemcpyHostToDevice, st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, hw.data(), n_wins * sizeof(BatchWinDev), cudaMemcpyHostToDevice, st));
+
+    const uint32_t n_items = (uint32_t)hi.size();
+    const int pt_threads = 256;
+    const uint32_t pt_blocks =
+        (uint32_t)std::min<uint64_t>((points + pt_threads - 1) / pt_threads, (uint64_t)ctx->num_sms * 16);
+    MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, (keys + 1) * 4, st));
+    k_digits_batch<false><<<pt_blocks, pt_threads, 0, st>>>((const BatchItemDev*)d_items, n_items, (uint32_t)points,
+                                                           max_windows, (uint32_t*)counts, nullptr, nullptr);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_SCAN, st));
+    MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets, (uint32_t)keys + 1, st));
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, (keys + 1) * 4, st));
+    k_digits_batch<true><<<pt_blocks, pt_threads, 0, st>>>((const BatchItemDev*)d_items, n_items, (uint32_t)points,
+                                                          max_windows, (uint32_t*)counts, (const uint32_t*)offsets,
+                                                          (uint32_t*)sorted);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
+    k_accumulate<<<acc_blocks, kAccThreads, 0, st>>>(static_cast<const Affine*>(d_bases), (const uint32_t*)sorted,
+                                                    (const uint32_t*)offsets, (uint32_t)keys, (Xyzz*)buckets,
+                                                    (Xyzz*)partials, (int*)owner);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_FIXUP, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(long_count, 0, 4, st));
+    k_fixup<<<acc_blocks, kAccThreads, 0, st>>>((const uint32_t*)offsets, (uint32_t)keys, (const Xyzz*)partials,
+                                               (const int*)owner, (Xyzz*)buckets, (uint32_t*)long_count,
+                                               (uint2*)long_list);
+    MZK_LAUNCH_CHECK(ctx);
+    k_fixup_long<<<ctx->num_sms * 2, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
+        (const int*)owner, (const Xyzz*)partials, (const uint32_t*)long_count, (const uint2*)long_list,
+        (Xyzz*)buckets);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
+    k_group_sums_batch<<<(uint32_t)((groups + kReduceThreads - 1) / kReduceThreads), kReduceThreads, 0, st>>>(
+        (const Xyzz*)buckets, (const uint32_t*)offsets, (const BatchWinDev*)d_wins, (uint32_t)n_wins,
+        (uint32_t)groups, (Xyzz*)run, (Xyzz*)tot);
+    MZK_LAUNCH_CHECK(ctx);
+    k_plane_sums_batch<<<(uint32_t)plane_blocks, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
+        (const Xyzz*)run, (const Xyzz*)tot, (const BatchWinDev*)d_wins, (uint32_t)n_wins, (Xyzz*)planes);
+    MZK_LAUNCH_CHECK(ctx);
+    k_window_finish_batch<<<(uint32_t)((n_wins + 31) / 32), 32, 0, st>>>((const Xyzz*)planes,
+                                                                        (const BatchWinDev*)d_wins, (uint32_t)n_wins,
+                                                                        (Xyzz*)wsum);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(ctx->phase_end(st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(host_wsum, wsum, n_wins * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    ctx->phase_collect();
+    const host::Xyzz6* hs = static_cast<const host::Xyzz6*>(host_wsum);
+    size_t w0 = 0;
+    for (size_t i = 0; i < hi.size(); i++) {
+        host::Xyzz6 acc = host::infinity();
+        for (int w = (int)hi[i].windows - 1; w >= 0; w--) {
+            for (uint32_t b = 0; b < hi[i].c; b++) acc = host::dbl(acc);
+            acc = host::add(acc, host::canon(hs[w0 + w]));
+        }
+        w0 += hi[i].windows;
+        host::to_jacobian_normalised(acc, out + 18 * item_of[i]);
+    }
+    ctx->last_entries = entries;
+    return OK;
+}
+
+}  // namespace mzk
+
+namespace mzk {
+
+// ---------------------------------------------------------------------------
 // Allocation-free MSM for callers that cannot allocate device memory.
 //
 // Some hosts own every byte of device memory themselves: a framework that

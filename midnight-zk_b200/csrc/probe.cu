@@ -3,6 +3,7 @@
 // 12-limb Montgomery multiplication of field.cuh reaches on it.
 #include <cuda_runtime.h>
 
+#include "ec.cuh"
 #include "field.cuh"
 #include "runtime.hpp"
 
@@ -93,6 +94,29 @@ __global__ void __launch_bounds__(128) k_probe_fp_mul(uint32_t seed, uint32_t* s
     if (acc == 0x12345678u) sink[0] = acc;
 }
 
+// The bucket-accumulation inner step alone: mixed XYZZ additions of a point
+// held in registers, no memory traffic; isolates the cost of the addition code.
+constexpr int kProbeMaddIters = 64;
+
+__global__ void __launch_bounds__(128, 1) k_probe_madd(uint32_t seed, uint32_t* sink) {
+    Affine p;
+    Xyzz acc;
+#pragma unroll
+    for (int j = 0; j < 12; j++) {
+        p.x.l[j] = (seed * (j + 3) + threadIdx.x) & 0x0fffffffu;
+        p.y.l[j] = (seed ^ (j * 131u + threadIdx.x)) & 0x0fffffffu;
+        acc.x.l[j] = (seed + j * 17u) & 0x0fffffffu;
+        acc.y.l[j] = (seed * 7u + j) & 0x0fffffffu;
+        acc.zz.l[j] = (seed ^ (j * 5u)) & 0x0fffffffu;
+        acc.zzz.l[j] = (seed + 99u * j) & 0x0fffffffu;
+    }
+    for (int it = 0; it < kProbeMaddIters; it++) xyzz_add_affine_fast(acc, p);
+    uint32_t r = 0;
+#pragma unroll
+    for (int j = 0; j < 12; j++) r ^= acc.x.l[j] ^ acc.y.l[j] ^ acc.zz.l[j] ^ acc.zzz.l[j];
+    if (r == 0x12345678u) sink[0] = r;
+}
+
 }  // namespace
 
 Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s, double* variants) {
@@ -139,6 +163,22 @@ Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s, double
         if (rep > 0 && ms < best) best = ms;
     }
     *fp_mul_per_s = (double)mblocks * 128 * kProbeMulIters * 2.0 / (best * 1e-3);
+    if (variants) {
+        // variants[3]: mixed additions per second of the accumulation step in registers
+        const uint32_t ablocks = (uint32_t)ctx->num_sms * 2 * 8;
+        best = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+            MZK_CUDA_CHECK(cudaEventRecord(e0, st));
+            k_probe_madd<<<ablocks, 128, 0, st>>>(0x999u + rep, (uint32_t*)sink);
+            MZK_LAUNCH_CHECK(ctx);
+            MZK_CUDA_CHECK(cudaEventRecord(e1, st));
+            MZK_CUDA_CHECK(cudaEventSynchronize(e1));
+            float ms;
+            MZK_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0 && ms < best) best = ms;
+        }
+        variants[3] = (double)ablocks * 128 * kProbeMaddIters / (best * 1e-3);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return OK;

@@ -104,6 +104,15 @@ struct Context {
 Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
                      cudaStream_t stream, cudaEvent_t bases_ready);
 int msm_pick_window(size_t n);
+// one MSM of a batch: scalars (device) against bases[base_offset, base_offset + n)
+struct BatchItem {
+    const void* d_scalars;
+    uint64_t base_offset;
+    uint64_t n;
+};
+// out: count x 18 u64 (host), results in item order
+Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, const BatchItem* items, size_t count,
+                           uint64_t* out, cudaStream_t stream);
 enum MsmPhase { PH_HISTOGRAM = 0, PH_SCAN, PH_SCATTER, PH_ACCUMULATE, PH_FIXUP, PH_REDUCE, PH_TAIL, PH_COPY };
 
 // ---- microbenchmarks (probe.cu) ----
