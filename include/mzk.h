@@ -168,6 +168,17 @@ typedef struct {
  * proofs/src/plonk/prover.rs:664, :713). */
 int mzk_quotient_eval_device(mzk_ctx *ctx, mzk_domain *d, const mzk_quotient_desc *desc, int divide, uint64_t *d_out);
 
+/* compute_h_poly (proofs/src/plonk/prover.rs:701-771) on the device, without
+ * the transcript writes: h = nu / t, extended_to_coeff, truncated to
+ * (n-1)*qdeg and split into qdeg limbs of n - 1 coefficients, inter-limb
+ * blinding with the caller's `blinds` ((qdeg-1) x 4 u64 Montgomery, host;
+ * blind_quotient_limbs draws them from OsRng, prover.rs:774-785), every limb
+ * padded to n and committed against the monomial SRS d_srs_g[0..n).
+ * out_commitments: qdeg x 18 u64 G1Projective (host); d_limbs_out: optional
+ * DEVICE buffer of qdeg x n Fr receiving the limbs.  qdeg = j - 1 of the domain. */
+int mzk_compute_h_poly_device(mzk_ctx *ctx, mzk_domain *d, const mzk_quotient_desc *desc, const uint64_t *d_srs_g,
+                              size_t srs_len, const uint64_t *blinds, uint64_t *out_commitments, uint64_t *d_limbs_out);
+
 /* ---- seeded synthetic inputs (benchmarks and tests) -------------------- */
 /* n uniform Fr elements (Montgomery) of stream `seed`, elements first..first+n-1 */
 int mzk_gen_rand_fr_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);

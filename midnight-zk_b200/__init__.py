@@ -64,6 +64,7 @@ SIGNATURES = {
     "mzk_domain_op": (_i32, [_vp, _vp, _i32, _u64p, _u64p]),
     "mzk_domain_op_device": (_i32, [_vp, _vp, _i32, _vp, _vp]),
     "mzk_quotient_eval_device": (_i32, [_vp, _vp, ctypes.c_void_p, _i32, _vp]),
+    "mzk_compute_h_poly_device": (_i32, [_vp, _vp, ctypes.c_void_p, _vp, _sz, _u64p, _u64p, _vp]),
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
     "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
 }
@@ -339,6 +340,7 @@ class EvaluationDomain:
         _check(lib().mzk_domain_shape(self.h, ctypes.byref(kk), ctypes.byref(ek)))
         self.k, self.extended_k = kk.value, ek.value
         self.n, self.extended_len = 1 << self.k, 1 << self.extended_k
+        self.quotient_poly_degree = j - 1
 
     def close(self):
         if getattr(self, "h", None):
@@ -393,6 +395,18 @@ class EvaluationDomain:
         """h(X) (divide) or nu(X) on the extended coset into d_out (device)."""
         do = d_out.ptr if isinstance(d_out, DeviceBuffer) else int(d_out)
         _check(lib().mzk_quotient_eval_device(self.ctx.h, self.h, ctypes.byref(desc), 1 if divide else 0, do))
+
+    def compute_h_poly_device(self, desc, d_srs_g, srs_len, blinds, d_limbs_out=None):
+        """compute_h_poly on the device: (qdeg, 18) limb commitments."""
+        qdeg = self.quotient_poly_degree
+        blinds = np.ascontiguousarray(blinds, np.uint64).reshape(-1, 4)
+        assert blinds.shape[0] == qdeg - 1
+        out = np.zeros((qdeg, 18), np.uint64)
+        dg = d_srs_g.ptr if isinstance(d_srs_g, DeviceBuffer) else int(d_srs_g)
+        dl = 0 if d_limbs_out is None else (d_limbs_out.ptr if isinstance(d_limbs_out, DeviceBuffer) else int(d_limbs_out))
+        _check(lib().mzk_compute_h_poly_device(self.ctx.h, self.h, ctypes.byref(desc), dg, int(srs_len),
+                                               _ptr(blinds), _ptr(out), dl or None))
+        return out
 
     def op_device(self, name, d_in, d_out):
         """Operation on device buffers (pointers or DeviceBuffers)."""

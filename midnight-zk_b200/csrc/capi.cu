@@ -455,4 +455,17 @@ int mzk_msm_g1_batch_device(mzk_ctx* ctx, const uint64_t* d_bases, size_t bases_
                                     count, out, ctx->impl.stream);
 }
 
+int mzk_compute_h_poly_device(mzk_ctx* ctx, mzk_domain* d, const mzk_quotient_desc* desc, const uint64_t* d_srs_g,
+                              size_t srs_len, const uint64_t* blinds, uint64_t* out_commitments,
+                              uint64_t* d_limbs_out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || !desc || !d_srs_g || !blinds || !out_commitments) {
+        mzk::set_error("compute_h_poly: null argument");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    return mzk::compute_h_poly_device(&ctx->impl, d->impl, desc, d_srs_g, srs_len, blinds, out_commitments,
+                                      d_limbs_out, ctx->impl.stream);
+}
+
 }  // extern "C"

@@ -60,19 +60,38 @@ struct PassArgs {
     Fr pre[3];
 };
 
+// Shared-memory tiles hold Fr elements as two planes of 16-byte halves, so a
+// warp's element accesses are contiguous 128-bit loads without bank conflicts
+// (a 32-byte element read word by word at a 32-byte stride conflicts 8-way).
+struct FrPlanes {
+    uint4* lo;
+    uint4* hi;
+    __device__ __forceinline__ Fr get(uint32_t i) const {
+        const uint4 a = lo[i], b = hi[i];
+        Fr r;
+        r.l[0] = a.x; r.l[1] = a.y; r.l[2] = a.z; r.l[3] = a.w;
+        r.l[4] = b.x; r.l[5] = b.y; r.l[6] = b.z; r.l[7] = b.w;
+        return r;
+    }
+    __device__ __forceinline__ void set(uint32_t i, const Fr& v) const {
+        lo[i] = make_uint4(v.l[0], v.l[1], v.l[2], v.l[3]);
+        hi[i] = make_uint4(v.l[4], v.l[5], v.l[6], v.l[7]);
+    }
+};
+
 __global__ void __launch_bounds__(kNttThreads) k_ntt_dif_pass(PassArgs a) {
     extern __shared__ uint4 smem_raw[];
-    Fr* sx = reinterpret_cast<Fr*>(smem_raw);
     const uint32_t N = 1u << a.log_n;
     const uint32_t R = 1u << a.log_r;
     const uint32_t log_m = a.log_s - a.log_r;  // columns per segment = 2^log_m
     const uint32_t tile = min(kTile, N);
     const uint32_t log_b = (31 - __clz(tile)) - a.log_r;  // columns per block = 2^log_b
     const uint32_t B = 1u << log_b;
-    Fr* sw = sx + tile;  // w_R^u for u < R/2
+    const FrPlanes sx{smem_raw, smem_raw + tile};
+    const FrPlanes sw{smem_raw + 2 * tile, smem_raw + 2 * tile + R / 2};  // w_R^u for u < R/2
     const uint32_t c0 = blockIdx.x << log_b;
 
-    for (uint32_t u = threadIdx.x; u < R / 2; u += blockDim.x) sw[u] = root_pow(a.tlo, a.thi, u << (a.log_n - a.log_r));
+    for (uint32_t u = threadIdx.x; u < R / 2; u += blockDim.x) sw.set(u, root_pow(a.tlo, a.thi, u << (a.log_n - a.log_r)));
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         const uint32_t m = e >> log_b, b = e & (B - 1);
         const uint32_t c = c0 + b;
@@ -85,7 +104,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_dif_pass(PassArgs a) {
                 if (r3) v = fr_mul(v, a.pre[r3]);
             }
         }
-        sx[e] = v;
+        sx.set(e, v);
     }
     __syncthreads();
     for (uint32_t s = 0; s < a.log_r; s++) {
@@ -96,11 +115,11 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_dif_pass(PassArgs a) {
             const uint32_t pos = p & (h - 1);
             const uint32_t m0 = ((p >> log_h) << (log_h + 1)) + pos;
             const uint32_t i0 = (m0 << log_b) + b, i1 = ((m0 + h) << log_b) + b;
-            const Fr x0 = sx[i0], x1 = sx[i1];
-            sx[i0] = fr_add(x0, x1);
+            const Fr x0 = sx.get(i0), x1 = sx.get(i1);
+            sx.set(i0, fr_add(x0, x1));
             Fr v = fr_sub(x0, x1);
-            if (pos) v = fr_mul(v, sw[pos << s]);
-            sx[i1] = v;
+            if (pos) v = fr_mul(v, sw.get(pos << s));
+            sx.set(i1, v);
         }
         __syncthreads();
     }
@@ -109,7 +128,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_dif_pass(PassArgs a) {
         const uint32_t c = c0 + b;
         const uint32_t j = c & ((1u << log_m) - 1);
         const uint32_t idx = ((c >> log_m) << a.log_s) + (m << log_m) + j;
-        Fr v = sx[e];
+        Fr v = sx.get(e);
         if (a.twiddle_after && j) {
             const uint32_t k1 = __brev(m) >> (32 - a.log_r);
             const uint32_t ex = (j * k1) << (a.log_n - a.log_s);  // (N/S) j k1 < N
@@ -212,6 +231,7 @@ Status domain_create(Context* ctx, uint32_t j, uint32_t k, Domain** out) {
     Domain* d = new Domain();
     d->k = k;
     d->ext_k = ext_k;
+    d->quotient_poly_degree = (uint32_t)qdeg;
     host::Fr4 ext_omega;
     std::memcpy(ext_omega.l, kRootOfUnity, 32);
     for (uint32_t i = ext_k; i < 32; i++) ext_omega = host::fr_mul(ext_omega, ext_omega);

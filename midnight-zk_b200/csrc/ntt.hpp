@@ -21,6 +21,7 @@ enum DomainOp : int {
 
 struct Domain {
     uint32_t k = 0, ext_k = 0;
+    uint32_t quotient_poly_degree = 0;  // j - 1
     host::Fr4 omega, omega_inv, ext_omega, ext_omega_inv, zeta, zeta2, ifft_div, ext_ifft_div;
     std::vector<host::Fr4> t_inv;  // 1 / t(zeta * ext_omega^i), i < 2^(ext_k - k)
     // per root (0 omega, 1 omega_inv, 2 ext_omega, 3 ext_omega_inv):

@@ -15,7 +15,9 @@
 // permutation's delta term comes from the domain's split twiddle tables.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "../../include/mzk.h"
 #include "field.cuh"
@@ -208,6 +210,64 @@ Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_de
     k_quotient<<<blocks, 256, 0, st>>>(q);
     MZK_LAUNCH_CHECK(ctx);
     return OK;
+}
+
+namespace {
+
+// limb i (length n) = h[i (n-1) .. (i+1)(n-1)) followed by blind[i] (zero for
+// the last limb), and limb i's first element minus blind[i-1] for i >= 1
+// (blind_quotient_limbs, proofs/src/plonk/prover.rs:774-785)
+__global__ void k_split_limbs(const Fr* __restrict__ h, uint32_t n, uint32_t limbs, const Fr* __restrict__ blinds,
+                              Fr* __restrict__ out) {
+    const uint32_t total = n * limbs;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const uint32_t i = t / n, j = t % n;
+        Fr v;
+        if (j < n - 1) v = h[(size_t)i * (n - 1) + j];
+        else v = i + 1 < limbs ? blinds[i] : fr_zero();
+        if (j == 0 && i > 0) v = fr_sub(v, blinds[i - 1]);
+        out[t] = v;
+    }
+}
+
+}  // namespace
+
+Status compute_h_poly_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, const void* d_srs_g,
+                             size_t srs_len, const uint64_t* blinds, uint64_t* commitments, void* d_limbs_out,
+                             cudaStream_t st) {
+    const uint32_t n = 1u << d->k, en = 1u << d->ext_k, limbs = d->quotient_poly_degree;
+    if (limbs < 2) {
+        set_error("compute_h_poly: quotient degree below 2 has no limbs to blind");
+        return ERR_ARG;
+    }
+    if (srs_len < n) {
+        set_error("compute_h_poly: monomial SRS shorter than n");
+        return ERR_ARG;
+    }
+    if ((uint64_t)(n - 1) * limbs > en) {
+        set_error("compute_h_poly: extended domain too small for the quotient degree");
+        return ERR_ARG;
+    }
+    void *hbuf, *limbs_buf, *dblinds;
+    MZK_TRY(ctx->ensure("hpoly_ext", (size_t)en * sizeof(Fr), &hbuf));
+    if (d_limbs_out) limbs_buf = d_limbs_out;
+    else MZK_TRY(ctx->ensure("hpoly_limbs", (size_t)limbs * n * sizeof(Fr), &limbs_buf));
+    MZK_TRY(ctx->ensure("hpoly_blinds", (size_t)limbs * sizeof(Fr), &dblinds));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dblinds, blinds, (size_t)(limbs - 1) * sizeof(Fr), cudaMemcpyHostToDevice, st));
+    MZK_TRY(quotient_eval_device(ctx, d, desc, 1, hbuf, st));
+    MZK_TRY(domain_op_device(ctx, d, OP_EXTENDED_TO_COEFF, hbuf, hbuf, st));
+    const uint32_t total = n * limbs;
+    k_split_limbs<<<(uint32_t)std::min<uint64_t>((total + 255) / 256, (uint64_t)ctx->num_sms * 8), 256, 0, st>>>(
+        static_cast<const Fr*>(hbuf), n, limbs, static_cast<const Fr*>(dblinds), static_cast<Fr*>(limbs_buf));
+    MZK_LAUNCH_CHECK(ctx);
+    std::vector<BatchItem> items(limbs);
+    for (uint32_t i = 0; i < limbs; i++) {
+        items[i].d_scalars = static_cast<const Fr*>(limbs_buf) + (size_t)i * n;
+        items[i].base_offset = 0;
+        items[i].n = n;
+    }
+    return msm_g1_batch_device(ctx, d_srs_g, srs_len, items.data(), limbs, commitments, st);
 }
 
 }  // namespace mzk

@@ -31,6 +31,12 @@ struct QuotientParams {
     int32_t divide;
 };
 
+// compute_h_poly (proofs/src/plonk/prover.rs:701-771) without the transcript:
+// commitments: quotient_poly_degree x 18 u64 (host); blinds: (limbs - 1) x 4
+// u64 (host); d_limbs_out (optional, device): limbs x n Fr
+Status compute_h_poly_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, const void* d_srs_g,
+                             size_t srs_len, const uint64_t* blinds, uint64_t* commitments, void* d_limbs_out,
+                             cudaStream_t st);
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st);
 
