@@ -46,10 +46,7 @@ namespace mzk {
 namespace {
 
 constexpr int kGroupLen = 16;      // buckets per running-sum group
-#ifndef MZK_ACC_THREADS
-#define MZK_ACC_THREADS 128
-#endif
-constexpr int kAccThreads = MZK_ACC_THREADS;  // threads per block of the accumulate kernel
+constexpr int kAccThreads = 128;   // threads per block of the accumulate kernel
 constexpr int kReduceThreads = 128;
 constexpr uint32_t kNoKey = 0xffffffffu;
 
@@ -158,50 +155,6 @@ __global__ void k_scatter(const Fr* __restrict__ scalars, size_t n, int c, int w
                 sorted[pos] = (uint32_t)i | (neg ? 0x80000000u : 0u);
             }
         }
-    }
-}
-
-// Histogram that also stores every digit: digits[w * n + i] = key | sign << 31
-// (kNoKey for a zero digit), written coalesced, so the scatter can run window
-// by window without recomputing digits.
-__global__ void k_histogram_store(const Fr* __restrict__ scalars, size_t n, int c, int windows, uint32_t nb,
-                                  uint32_t* __restrict__ counts, uint32_t* __restrict__ digits) {
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-        const size_t i = base + threadIdx.x;
-        const bool valid = i < n;
-        Fr s = valid ? fr_from_mont(load_fr(scalars, i)) : fr_zero();
-        uint32_t carry = 0;
-        for (int w = 0; w < windows; w++) {
-            bool neg;
-            uint32_t key = next_digit(s, w, c, nb, carry, neg);
-            if (!valid) key = kNoKey;
-            const uint32_t peers = __match_any_sync(0xffffffffu, key);
-            if (key != kNoKey && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
-            if (valid) digits[(size_t)w * n + i] = key == kNoKey ? kNoKey : (key | (neg ? 0x80000000u : 0u));
-        }
-    }
-}
-
-// Scatter of one window per grid row (blockIdx.y): the window's slice of the
-// sorted array (n entries at most) stays resident in L2 while it is filled.
-__global__ void k_scatter_window(const uint32_t* __restrict__ digits, size_t n, const uint32_t* __restrict__ offsets,
-                                 uint32_t* __restrict__ fill, uint32_t* __restrict__ sorted) {
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    const uint32_t* dw = digits + (size_t)blockIdx.y * n;
-    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-        const size_t i = base + threadIdx.x;
-        const uint32_t d = i < n ? dw[i] : kNoKey;
-        const uint32_t key = d == kNoKey ? kNoKey : (d & 0x7fffffffu);
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(peers) - 1;
-        uint32_t slot = 0;
-        if (key != kNoKey && lane == leader) slot = atomicAdd(&fill[key], (uint32_t)__popc(peers));
-        slot = __shfl_sync(peers, slot, leader);
-        if (key != kNoKey) sorted[offsets[key] + slot + (uint32_t)__popc(peers & lt_mask)] = (uint32_t)i | (d & 0x80000000u);
     }
 }
 
@@ -572,12 +525,9 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     const int pt_threads = 256;
     const uint32_t pt_blocks = (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)ctx->num_sms * 16);
 
-    void* digits;
-    MZK_TRY(ctx->ensure("msm_digits", entries_cap * 4, &digits));
     MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
-    k_histogram_store<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)counts,
-                                                        (uint32_t*)digits);
+    k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)counts);
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCAN, st));
@@ -585,13 +535,9 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
-    {
-        const uint32_t wx = (uint32_t)std::max<size_t>(
-            1, std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)ctx->num_sms * 8 / sh.windows + 1));
-        k_scatter_window<<<dim3(wx, (uint32_t)sh.windows), pt_threads, 0, st>>>(
-            (const uint32_t*)digits, n, (const uint32_t*)offsets, (uint32_t*)counts, (uint32_t*)sorted);
-        MZK_LAUNCH_CHECK(ctx);
-    }
+    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (const uint32_t*)offsets,
+                                                (uint32_t*)counts, (uint32_t*)sorted);
+    MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     if (bases_ready) MZK_CUDA_CHECK(cudaStreamWaitEvent(st, bases_ready, 0));
     MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
