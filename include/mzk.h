@@ -179,6 +179,54 @@ int mzk_quotient_eval_device(mzk_ctx *ctx, mzk_domain *d, const mzk_quotient_des
 int mzk_compute_h_poly_device(mzk_ctx *ctx, mzk_domain *d, const mzk_quotient_desc *desc, const uint64_t *d_srs_g,
                               size_t srs_len, const uint64_t *blinds, uint64_t *out_commitments, uint64_t *d_limbs_out);
 
+/* ---- device part of create_proof (proofs/src/plonk/prover.rs:432) ------- */
+/* Circuit shape of the single-proof configuration: advice a, b, c under the
+ * gate q_l a + q_r b + q_m a b + q_o c + q_c, one permutation set over a, b, c,
+ * one logup lookup of a into the fixed table column (selector column 6),
+ * degree 5 (j = 5: four quotient limbs).  Resident proving-key data: */
+typedef struct {
+    uint32_t k;
+    const uint64_t *fixed_ext[7];  /* q_l, q_r, q_m, q_o, q_c, table, lookup selector (extended coset), DEVICE */
+    const uint64_t *sigma_ext[3];  /* permutation_pk_cosets of a, b, c, DEVICE */
+    const uint64_t *l0_ext, *l_last_ext, *l_active_ext;
+    const uint64_t *srs;           /* DEVICE G1Affine array holding the four bases below */
+    uint64_t srs_len;              /* points in srs */
+    uint64_t off_g, off_lagrange, off_lagrange_delta, off_lagrange_double_delta; /* ParamsKZG::bases, params.rs:83-93 */
+    uint32_t blinding_factors;
+} mzk_proving_key_desc;
+/* One proof's witness (Lagrange form, DEVICE, n Fr each) and challenges. */
+typedef struct {
+    const uint64_t *advice[3];     /* a, b, c */
+    const uint64_t *perm_z;        /* permutation product */
+    const uint64_t *lookup_m, *lookup_h, *lookup_Z; /* logup multiplicities, helper, aggregator */
+    uint64_t y[4], beta[4], gamma[4], theta[4];
+    uint64_t quotient_blinds[3][4];
+} mzk_proof_job;
+/* For each job: commitments (out: count x 11 x 18 u64 G1Projective, in the
+ * order a, b, c, m (delta), z (delta), Z (double delta), h, quotient limbs
+ * 0..3), lagrange_to_coeff and coeff_to_extended of the seven witness
+ * polynomials, compute_h_poly.  All jobs' MSMs run as two batched MSMs. */
+int mzk_prove_core_device(mzk_ctx *ctx, mzk_domain *d, const mzk_proving_key_desc *pk, const mzk_proof_job *jobs,
+                          size_t count, uint64_t *out);
+
+/* ---- proving service (continuous batching over the proof core) ---------- */
+/* No reference counterpart: the reference proves one call at a time.  A worker
+ * thread drains the request queue in waves: each wave takes queued requests
+ * oldest first while it holds fewer than max_batch proofs and their device
+ * scratch fits mem_budget_bytes (0: no memory limit), and runs them as one
+ * mixed-k proof-core call (max_batch = 1 is the plain one-at-a-time prover).
+ * Witness buffers referenced by a job must stay valid until its wait returns. */
+typedef struct mzk_server mzk_server;
+int mzk_server_create(mzk_ctx *ctx, uint32_t max_batch, uint64_t mem_budget_bytes, mzk_server **out);
+/* register the domain and proving key of one k (all keys share one SRS buffer) */
+int mzk_server_add_key(mzk_server *s, mzk_domain *d, const mzk_proving_key_desc *pk);
+int mzk_server_submit(mzk_server *s, uint32_t k, const mzk_proof_job *job, uint64_t *ticket);
+/* blocks until the request is done: out 11 x 18 u64 as mzk_prove_core_device,
+ * latency from submit to completion */
+int mzk_server_wait(mzk_server *s, uint64_t ticket, uint64_t *out, double *latency_ms);
+int mzk_server_stats(mzk_server *s, uint64_t *waves, uint64_t *proofs, double *busy_ms);
+int mzk_server_destroy(mzk_server *s);
+
 /* ---- seeded synthetic inputs (benchmarks and tests) -------------------- */
 /* n uniform Fr elements (Montgomery) of stream `seed`, elements first..first+n-1 */
 int mzk_gen_rand_fr_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);

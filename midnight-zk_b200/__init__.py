@@ -65,6 +65,13 @@ SIGNATURES = {
     "mzk_domain_op_device": (_i32, [_vp, _vp, _i32, _vp, _vp]),
     "mzk_quotient_eval_device": (_i32, [_vp, _vp, ctypes.c_void_p, _i32, _vp]),
     "mzk_compute_h_poly_device": (_i32, [_vp, _vp, ctypes.c_void_p, _vp, _sz, _u64p, _u64p, _vp]),
+    "mzk_prove_core_device": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u64p]),
+    "mzk_server_create": (_i32, [_vp, _u32, _u64, ctypes.POINTER(_vp)]),
+    "mzk_server_add_key": (_i32, [_vp, _vp, ctypes.c_void_p]),
+    "mzk_server_submit": (_i32, [_vp, _u32, ctypes.c_void_p, _u64p]),
+    "mzk_server_wait": (_i32, [_vp, _u64, _u64p, ctypes.POINTER(ctypes.c_double)]),
+    "mzk_server_stats": (_i32, [_vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_double)]),
+    "mzk_server_destroy": (_i32, [_vp]),
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
     "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
 }
@@ -72,6 +79,26 @@ SIGNATURES = {
 class MsmBatchItem(ctypes.Structure):
     """mzk_msm_batch_item (include/mzk.h)."""
     _fields_ = [("d_scalars", ctypes.c_void_p), ("base_offset", ctypes.c_uint64), ("n", ctypes.c_uint64)]
+
+
+class ProvingKeyDesc(ctypes.Structure):
+    """mzk_proving_key_desc (include/mzk.h)."""
+    _fields_ = [("k", ctypes.c_uint32), ("fixed_ext", ctypes.c_void_p * 7), ("sigma_ext", ctypes.c_void_p * 3),
+                ("l0_ext", ctypes.c_void_p), ("l_last_ext", ctypes.c_void_p), ("l_active_ext", ctypes.c_void_p),
+                ("srs", ctypes.c_void_p), ("srs_len", ctypes.c_uint64), ("off_g", ctypes.c_uint64),
+                ("off_lagrange", ctypes.c_uint64), ("off_lagrange_delta", ctypes.c_uint64),
+                ("off_lagrange_double_delta", ctypes.c_uint64), ("blinding_factors", ctypes.c_uint32)]
+
+
+class ProofJob(ctypes.Structure):
+    """mzk_proof_job (include/mzk.h)."""
+    _fields_ = [("advice", ctypes.c_void_p * 3), ("perm_z", ctypes.c_void_p), ("lookup_m", ctypes.c_void_p),
+                ("lookup_h", ctypes.c_void_p), ("lookup_Z", ctypes.c_void_p), ("y", ctypes.c_uint64 * 4),
+                ("beta", ctypes.c_uint64 * 4), ("gamma", ctypes.c_uint64 * 4), ("theta", ctypes.c_uint64 * 4),
+                ("quotient_blinds", (ctypes.c_uint64 * 4) * 3)]
+
+
+PROOF_CORE_COMMITMENTS = ["a", "b", "c", "m_delta", "z_delta", "Z_double_delta", "h", "H0", "H1", "H2", "H3"]
 
 
 class QuotientDesc(ctypes.Structure):
@@ -408,11 +435,62 @@ class EvaluationDomain:
                                                _ptr(blinds), _ptr(out), dl or None))
         return out
 
+    def prove_core_device(self, pk_desc, jobs):
+        """Device part of create_proof for a list of ProofJob: (len, 11, 18) commitments."""
+        arr = (ProofJob * max(1, len(jobs)))(*jobs)
+        out = np.zeros((max(1, len(jobs)), len(PROOF_CORE_COMMITMENTS), 18), np.uint64)
+        _check(lib().mzk_prove_core_device(self.ctx.h, self.h, ctypes.byref(pk_desc), ctypes.addressof(arr),
+                                           len(jobs), _ptr(out)))
+        return out[:len(jobs)]
+
     def op_device(self, name, d_in, d_out):
         """Operation on device buffers (pointers or DeviceBuffers)."""
         di = d_in.ptr if isinstance(d_in, DeviceBuffer) else int(d_in)
         do = d_out.ptr if isinstance(d_out, DeviceBuffer) else int(d_out)
         _check(lib().mzk_domain_op_device(self.ctx.h, self.h, self.OPS[name], di, do))
+
+
+class ProvingServer:
+    """Proving service with continuous batching (mzk_server_*)."""
+
+    def __init__(self, ctx, max_batch=16, mem_budget_bytes=0):
+        self.ctx = ctx
+        h = _vp()
+        _check(lib().mzk_server_create(ctx.h, int(max_batch), int(mem_budget_bytes), ctypes.byref(h)))
+        self.h = h.value
+        self._keys = []
+
+    def add_key(self, domain, pk_desc):
+        self._keys.append((domain, pk_desc))
+        _check(lib().mzk_server_add_key(self.h, domain.h, ctypes.byref(pk_desc)))
+
+    def submit(self, k, job):
+        t = np.zeros(1, np.uint64)
+        _check(lib().mzk_server_submit(self.h, int(k), ctypes.byref(job), _ptr(t)))
+        return int(t[0])
+
+    def wait(self, ticket):
+        out = np.zeros((len(PROOF_CORE_COMMITMENTS), 18), np.uint64)
+        lat = ctypes.c_double()
+        _check(lib().mzk_server_wait(self.h, ticket, _ptr(out), ctypes.byref(lat)))
+        return out, lat.value
+
+    def stats(self):
+        w, p = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
+        busy = ctypes.c_double()
+        _check(lib().mzk_server_stats(self.h, _ptr(w), _ptr(p), ctypes.byref(busy)))
+        return {"waves": int(w[0]), "proofs": int(p[0]), "busy_ms": busy.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mzk_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def msm_pick_window(n):

@@ -117,6 +117,12 @@ Context::~Context() {
 
 }  // namespace mzk
 
+namespace mzk {
+Context* context_of(mzk_ctx* ctx) { return &ctx->impl; }
+std::recursive_mutex* context_mutex(mzk_ctx* ctx) { return &ctx->impl.mu; }
+const Domain* domain_of(mzk_domain* d) { return d->impl; }
+}  // namespace mzk
+
 using mzk::Status;
 
 namespace {
@@ -466,6 +472,19 @@ int mzk_compute_h_poly_device(mzk_ctx* ctx, mzk_domain* d, const mzk_quotient_de
     Guard g(ctx);
     return mzk::compute_h_poly_device(&ctx->impl, d->impl, desc, d_srs_g, srs_len, blinds, out_commitments,
                                       d_limbs_out, ctx->impl.stream);
+}
+
+int mzk_prove_core_device(mzk_ctx* ctx, mzk_domain* d, const mzk_proving_key_desc* pk, const mzk_proof_job* jobs,
+                          size_t count, uint64_t* out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || !pk || !out || (count && !jobs)) {
+        mzk::set_error("prove_core: null argument");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    MZK_TRY(mzk::prove_core_device(&ctx->impl, d->impl, pk, jobs, count, out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,204 @@
+// prover.cu — the device part of create_proof for the single-proof circuit.
+//
+// For the circuit shape of the single-proof configuration (three advice
+// columns a, b, c under the standard gate, one permutation set over a, b, c,
+// one logup lookup of a into a fixed table) this runs every data-parallel step
+// of proofs/src/plonk/prover.rs on the GPU, for one or many proofs at once:
+//
+//   1. witness commitments in the reference's bases (prover.rs:619-623,
+//      logup/prover.rs:168, :299, permutation/prover.rs:241): a, b, c and the
+//      logup helper h against the Lagrange basis, the multiplicities m and the
+//      permutation product z in delta form against the delta basis, the logup
+//      aggregator Z in double-delta form against the double-delta basis
+//      (Polynomial::to_delta / to_double_delta, proofs/src/poly/mod.rs:297-336);
+//   2. lagrange_to_coeff of the seven witness polynomials (prover.rs:231-280);
+//   3. coeff_to_extended of the seven (prover.rs:652-659, evaluation.rs:868-960);
+//   4. compute_h_poly (prover.rs:701-771): fused quotient, division by t(X),
+//      extended_to_coeff, blinded limbs;
+//   5. the limb commitments.
+// The MSMs of all proofs in a call run as two batched MSMs (step 1 for all
+// proofs, step 5 for all proofs), so small proofs share the GPU's chunks.
+// Witness generation, the permutation and logup running products, the
+// transcript, evaluations and the multi-open argument stay with the caller.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mzk.h"
+#include "field.cuh"
+#include "ntt.hpp"
+#include "quotient.hpp"
+#include "runtime.hpp"
+
+namespace mzk {
+
+namespace {
+
+// order 1: b_0 = a_0, b_i = a_i - a_{i-1}; order 2: c_0 = a_0,
+// c_1 = a_1 - 2 a_0, c_i = a_i - 2 a_{i-1} + a_{i-2}
+__global__ void k_delta(const Fr* __restrict__ a, Fr* __restrict__ out, uint32_t n, int order) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Fr v = a[i];
+        if (i >= 1) {
+            const Fr p = a[i - 1];
+            v = fr_sub(v, order == 2 ? fr_add(p, p) : p);
+        }
+        if (order == 2 && i >= 2) v = fr_add(v, a[i - 2]);
+        out[i] = v;
+    }
+}
+
+constexpr int kPolys = 7;  // a, b, c, z, m, h, Z
+
+}  // namespace
+
+Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_proving_key_desc* const* pks,
+                        const mzk_proof_job* jobs, size_t count, uint64_t* out, cudaStream_t st) {
+    std::memset(out, 0, count * kProofCoreCommitments * 18 * 8);
+    if (count == 0) return OK;
+    if (pks[0]->srs == nullptr) {
+        set_error("prove_core: null SRS");
+        return ERR_ARG;
+    }
+    const void* srs = pks[0]->srs;
+    const uint64_t srs_len = pks[0]->srs_len;
+    std::vector<BatchItem> items;
+    std::vector<Fr*> coeff(count * kPolys), ext(count * kPolys), limbs(count);
+    size_t max_en = 0;
+    for (size_t j = 0; j < count; j++) {
+        const Domain* d = doms[j];
+        const mzk_proving_key_desc* pk = pks[j];
+        const uint32_t n = 1u << d->k, en = 1u << d->ext_k, qdeg = d->quotient_poly_degree;
+        const std::string tag = std::to_string(j);
+        if (pk->k != d->k || qdeg + 7 != kProofCoreCommitments) {
+            set_error("prove_core: job " + tag + ": the key's k must match the domain and the domain must have j = 5");
+            return ERR_ARG;
+        }
+        if (pk->srs != srs || pk->srs_len != srs_len) {
+            set_error("prove_core: all keys of one call must share one SRS buffer");
+            return ERR_ARG;
+        }
+        if (pk->off_g + n > srs_len || pk->off_lagrange + n > srs_len || pk->off_lagrange_delta + n > srs_len ||
+            pk->off_lagrange_double_delta + n > srs_len) {
+            set_error("prove_core: job " + tag + ": SRS bases out of range");
+            return ERR_ARG;
+        }
+        max_en = std::max<size_t>(max_en, en);
+        void *pc, *pe, *pd, *pl;
+        MZK_TRY(ctx->ensure(("core_coeff_" + tag).c_str(), (size_t)kPolys * n * sizeof(Fr), &pc));
+        MZK_TRY(ctx->ensure(("core_ext_" + tag).c_str(), (size_t)kPolys * en * sizeof(Fr), &pe));
+        MZK_TRY(ctx->ensure(("core_delta_" + tag).c_str(), (size_t)3 * n * sizeof(Fr), &pd));
+        MZK_TRY(ctx->ensure(("core_limbs_" + tag).c_str(), (size_t)qdeg * n * sizeof(Fr), &pl));
+        for (int p = 0; p < kPolys; p++) {
+            coeff[j * kPolys + p] = static_cast<Fr*>(pc) + (size_t)p * n;
+            ext[j * kPolys + p] = static_cast<Fr*>(pe) + (size_t)p * en;
+        }
+        limbs[j] = static_cast<Fr*>(pl);
+        const mzk_proof_job& jb = jobs[j];
+        const void* lag[kPolys] = {jb.advice[0], jb.advice[1], jb.advice[2], jb.perm_z, jb.lookup_m, jb.lookup_h,
+                                   jb.lookup_Z};
+        for (int p = 0; p < kPolys; p++)
+            if (!lag[p]) {
+                set_error("prove_core: null witness polynomial in job " + tag);
+                return ERR_ARG;
+            }
+        const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 8);
+        Fr* dm = static_cast<Fr*>(pd);
+        Fr* dz = dm + n;
+        Fr* dZ = dz + n;
+        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(jb.lookup_m), dm, n, 1);
+        MZK_LAUNCH_CHECK(ctx);
+        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(jb.perm_z), dz, n, 1);
+        MZK_LAUNCH_CHECK(ctx);
+        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(jb.lookup_Z), dZ, n, 2);
+        MZK_LAUNCH_CHECK(ctx);
+        const BatchItem its[7] = {{jb.advice[0], pk->off_lagrange, n},  {jb.advice[1], pk->off_lagrange, n},
+                                  {jb.advice[2], pk->off_lagrange, n},  {dm, pk->off_lagrange_delta, n},
+                                  {dz, pk->off_lagrange_delta, n},      {dZ, pk->off_lagrange_double_delta, n},
+                                  {jb.lookup_h, pk->off_lagrange, n}};
+        items.insert(items.end(), its, its + 7);
+    }
+    // 1. witness commitments of every proof in one batch
+    std::vector<uint64_t> res1(items.size() * 18);
+    MZK_TRY(msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res1.data(), st));
+    for (size_t j = 0; j < count; j++)
+        std::memcpy(out + (j * kProofCoreCommitments) * 18, res1.data() + j * 7 * 18, 7 * 18 * 8);
+    // 2-4. per proof: coefficient and extended forms, quotient limbs
+    void *hbuf, *dbl;
+    MZK_TRY(ctx->ensure("core_hbuf", max_en * sizeof(Fr), &hbuf));
+    MZK_TRY(ctx->ensure("core_blinds", 8 * sizeof(Fr), &dbl));
+    for (size_t j = 0; j < count; j++) {
+        const Domain* d = doms[j];
+        const mzk_proving_key_desc* pk = pks[j];
+        const mzk_proof_job& jb = jobs[j];
+        const void* lag[kPolys] = {jb.advice[0], jb.advice[1], jb.advice[2], jb.perm_z, jb.lookup_m, jb.lookup_h,
+                                   jb.lookup_Z};
+        for (int p = 0; p < kPolys; p++) {
+            MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, lag[p], coeff[j * kPolys + p], st));
+            MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, coeff[j * kPolys + p], ext[j * kPolys + p], st));
+        }
+        Fr* const* e = &ext[j * kPolys];
+        const uint64_t* adv[3] = {(const uint64_t*)e[0], (const uint64_t*)e[1], (const uint64_t*)e[2]};
+        const uint64_t* sig[3] = {pk->sigma_ext[0], pk->sigma_ext[1], pk->sigma_ext[2]};
+        const uint64_t* zs[1] = {(const uint64_t*)e[3]};
+        const uint32_t kinds[3] = {0, 0, 0}, idxs[3] = {0, 1, 2};
+        mzk_quotient_desc q;
+        std::memset(&q, 0, sizeof(q));
+        q.k = d->k;
+        q.extended_k = d->ext_k;
+        q.advice = adv;
+        q.n_advice = 3;
+        q.fixed = pk->fixed_ext;
+        q.n_fixed = 7;
+        for (int i = 0; i < 5; i++) q.gate_fixed[i] = (uint32_t)i;
+        for (int i = 0; i < 3; i++) q.gate_advice[i] = (uint32_t)i;
+        q.n_perm_cols = 3;
+        q.perm_col_kind = kinds;
+        q.perm_col_index = idxs;
+        q.perm_sigma = sig;
+        q.n_perm_sets = 1;
+        q.perm_z = zs;
+        q.chunk_len = 3;  // cs.degree() - 2 with degree 5
+        q.blinding_factors = pk->blinding_factors;
+        q.has_lookup = 1;
+        q.lookup_input_advice = 0;
+        q.lookup_table_fixed = 5;
+        q.lookup_selector_fixed = 6;
+        q.lookup_m = (const uint64_t*)e[4];
+        q.lookup_h = (const uint64_t*)e[5];
+        q.lookup_z = (const uint64_t*)e[6];
+        q.l0 = pk->l0_ext;
+        q.l_last = pk->l_last_ext;
+        q.l_active = pk->l_active_ext;
+        std::memcpy(q.y, jb.y, 32);
+        std::memcpy(q.beta, jb.beta, 32);
+        std::memcpy(q.gamma, jb.gamma, 32);
+        std::memcpy(q.theta, jb.theta, 32);
+        MZK_TRY(compute_h_limbs_device(ctx, d, &q, &jb.quotient_blinds[0][0], limbs[j], hbuf, dbl, st));
+    }
+    // 5. limb commitments of every proof in one batch
+    items.clear();
+    for (size_t j = 0; j < count; j++) {
+        const uint32_t n = 1u << doms[j]->k;
+        for (uint32_t i = 0; i < doms[j]->quotient_poly_degree; i++)
+            items.push_back({limbs[j] + (size_t)i * n, pks[j]->off_g, n});
+    }
+    std::vector<uint64_t> res2(items.size() * 18);
+    MZK_TRY(msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res2.data(), st));
+    for (size_t j = 0; j < count; j++)
+        std::memcpy(out + (j * kProofCoreCommitments + 7) * 18, res2.data() + j * 4 * 18, 4 * 18 * 8);
+    return OK;
+}
+
+Status prove_core_device(Context* ctx, const Domain* d, const mzk_proving_key_desc* pk, const mzk_proof_job* jobs,
+                         size_t count, uint64_t* out, cudaStream_t st) {
+    std::vector<const Domain*> doms(count, d);
+    std::vector<const mzk_proving_key_desc*> pks(count, pk);
+    return prove_core_multi(ctx, doms.data(), pks.data(), jobs, count, out, st);
+}
+
+}  // namespace mzk

@@ -233,34 +233,41 @@ __global__ void k_split_limbs(const Fr* __restrict__ h, uint32_t n, uint32_t lim
 
 }  // namespace
 
-Status compute_h_poly_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, const void* d_srs_g,
-                             size_t srs_len, const uint64_t* blinds, uint64_t* commitments, void* d_limbs_out,
-                             cudaStream_t st) {
+Status compute_h_limbs_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, const uint64_t* blinds,
+                              void* d_limbs_out, void* d_hbuf, void* d_blinds, cudaStream_t st) {
     const uint32_t n = 1u << d->k, en = 1u << d->ext_k, limbs = d->quotient_poly_degree;
     if (limbs < 2) {
         set_error("compute_h_poly: quotient degree below 2 has no limbs to blind");
-        return ERR_ARG;
-    }
-    if (srs_len < n) {
-        set_error("compute_h_poly: monomial SRS shorter than n");
         return ERR_ARG;
     }
     if ((uint64_t)(n - 1) * limbs > en) {
         set_error("compute_h_poly: extended domain too small for the quotient degree");
         return ERR_ARG;
     }
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_blinds, blinds, (size_t)(limbs - 1) * sizeof(Fr), cudaMemcpyHostToDevice, st));
+    MZK_TRY(quotient_eval_device(ctx, d, desc, 1, d_hbuf, st));
+    MZK_TRY(domain_op_device(ctx, d, OP_EXTENDED_TO_COEFF, d_hbuf, d_hbuf, st));
+    const uint32_t total = n * limbs;
+    k_split_limbs<<<(uint32_t)std::min<uint64_t>((total + 255) / 256, (uint64_t)ctx->num_sms * 8), 256, 0, st>>>(
+        static_cast<const Fr*>(d_hbuf), n, limbs, static_cast<const Fr*>(d_blinds), static_cast<Fr*>(d_limbs_out));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+Status compute_h_poly_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, const void* d_srs_g,
+                             size_t srs_len, const uint64_t* blinds, uint64_t* commitments, void* d_limbs_out,
+                             cudaStream_t st) {
+    const uint32_t n = 1u << d->k, en = 1u << d->ext_k, limbs = d->quotient_poly_degree;
+    if (srs_len < n) {
+        set_error("compute_h_poly: monomial SRS shorter than n");
+        return ERR_ARG;
+    }
     void *hbuf, *limbs_buf, *dblinds;
     MZK_TRY(ctx->ensure("hpoly_ext", (size_t)en * sizeof(Fr), &hbuf));
     if (d_limbs_out) limbs_buf = d_limbs_out;
-    else MZK_TRY(ctx->ensure("hpoly_limbs", (size_t)limbs * n * sizeof(Fr), &limbs_buf));
-    MZK_TRY(ctx->ensure("hpoly_blinds", (size_t)limbs * sizeof(Fr), &dblinds));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(dblinds, blinds, (size_t)(limbs - 1) * sizeof(Fr), cudaMemcpyHostToDevice, st));
-    MZK_TRY(quotient_eval_device(ctx, d, desc, 1, hbuf, st));
-    MZK_TRY(domain_op_device(ctx, d, OP_EXTENDED_TO_COEFF, hbuf, hbuf, st));
-    const uint32_t total = n * limbs;
-    k_split_limbs<<<(uint32_t)std::min<uint64_t>((total + 255) / 256, (uint64_t)ctx->num_sms * 8), 256, 0, st>>>(
-        static_cast<const Fr*>(hbuf), n, limbs, static_cast<const Fr*>(dblinds), static_cast<Fr*>(limbs_buf));
-    MZK_LAUNCH_CHECK(ctx);
+    else MZK_TRY(ctx->ensure("hpoly_limbs", (size_t)std::max<uint32_t>(limbs, 1) * n * sizeof(Fr), &limbs_buf));
+    MZK_TRY(ctx->ensure("hpoly_blinds", (size_t)std::max<uint32_t>(limbs, 1) * sizeof(Fr), &dblinds));
+    MZK_TRY(compute_h_limbs_device(ctx, d, desc, blinds, limbs_buf, hbuf, dblinds, st));
     std::vector<BatchItem> items(limbs);
     for (uint32_t i = 0; i < limbs; i++) {
         items[i].d_scalars = static_cast<const Fr*>(limbs_buf) + (size_t)i * n;

@@ -37,6 +37,17 @@ struct QuotientParams {
 Status compute_h_poly_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, const void* d_srs_g,
                              size_t srs_len, const uint64_t* blinds, uint64_t* commitments, void* d_limbs_out,
                              cudaStream_t st);
+// the limb stage of compute_h_poly into caller buffers (d_hbuf: 2^ext_k Fr,
+// d_blinds: qdeg Fr, both device scratch); blinds on the host
+Status compute_h_limbs_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, const uint64_t* blinds,
+                              void* d_limbs_out, void* d_hbuf, void* d_blinds, cudaStream_t st);
+// device part of create_proof for the single-proof circuit (prover.cu)
+constexpr int kProofCoreCommitments = 11;  // a, b, c, m, z, Z, h, 4 quotient limbs
+Status prove_core_device(Context* ctx, const Domain* d, const mzk_proving_key_desc* pk, const mzk_proof_job* jobs,
+                         size_t count, uint64_t* out, cudaStream_t st);
+// jobs of different k: job j uses doms[j] and pks[j] (all keys share one SRS buffer)
+Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_proving_key_desc* const* pks,
+                        const mzk_proof_job* jobs, size_t count, uint64_t* out, cudaStream_t st);
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st);
 
