@@ -18,6 +18,7 @@ The directory name is not a Python identifier; ``_loader.load()`` at the
 repository root imports it as ``mzk_b200``.
 """
 import ctypes
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -212,9 +213,10 @@ class DeviceBuffer:
         p = _vp()
         _check(lib().mzk_device_alloc(ctx.h, self.nbytes, ctypes.byref(p)))
         self.ptr = p.value
+        ctx._buffers.add(self)
 
     def free(self):
-        if self.ptr:
+        if self.ptr and self.ctx.h:
             _check(lib().mzk_device_free(self.ctx.h, self.ptr))
             self.ptr = None
 
@@ -244,9 +246,20 @@ class Context:
         _check(lib().mzk_ctx_create(device, ctypes.byref(h)))
         self.h = h.value
         self.device = device
+        # objects that hold library handles tied to this context: closed
+        # (servers first, then domains, then buffers) before the context goes
+        self._servers, self._domains, self._buffers = weakref.WeakSet(), weakref.WeakSet(), weakref.WeakSet()
 
     def close(self):
         if getattr(self, "h", None):
+            for group in (self._servers, self._domains):
+                for obj in list(group):
+                    obj.close()
+            for buf in list(self._buffers):
+                try:
+                    buf.free()
+                except MzkError:
+                    pass
             lib().mzk_ctx_destroy(self.h)
             self.h = None
 
@@ -363,6 +376,7 @@ class EvaluationDomain:
         h = _vp()
         _check(lib().mzk_domain_create(ctx.h, j, k, ctypes.byref(h)))
         self.h = h.value
+        ctx._domains.add(self)
         kk, ek = _u32(), _u32()
         _check(lib().mzk_domain_shape(self.h, ctypes.byref(kk), ctypes.byref(ek)))
         self.k, self.extended_k = kk.value, ek.value
@@ -458,6 +472,7 @@ class ProvingServer:
         h = _vp()
         _check(lib().mzk_server_create(ctx.h, int(max_batch), int(mem_budget_bytes), ctypes.byref(h)))
         self.h = h.value
+        ctx._servers.add(self)
         self._keys = []
 
     def add_key(self, domain, pk_desc):
