@@ -49,6 +49,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the NTT and quotient lines")
     p.add_argument("--ntt-log-n", type=int, default=24)
+    p.add_argument("--no-prover", action="store_true", help="skip the proof-core, batched-MSM and serving lines")
+    p.add_argument("--serve-requests", type=int, default=80)
     return p.parse_args()
 
 
@@ -188,6 +190,191 @@ def measure_quotient(mzk, ctx, stream, k, reps):
     return {"rows": E, "ms": round(ms, 3), "rows_per_s": round(E / (ms / 1e3), 1),
             "hbm_gbs_algorithmic": round((ncols + 1) * 32 * E / (ms / 1e3) / 1e9, 1),
             "columns_read": ncols}
+
+
+FR_ONE_MONT = [0x00000001fffffffe, 0x5884b7fa00034802, 0x998c4fefecbc4ff5, 0x1824b159acc5056f]  # R mod r
+SERVE_KS = (14, 16, 18, 20)
+SERVE_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
+
+
+class ProverKeys:
+    """Synthetic proving keys of the single-proof circuit for several k, resident
+    on the device: one SRS buffer [g (2^max k) | per k: lagrange, delta, double
+    delta] of seeded points, and per k the 13 extended fixed/permutation/
+    Lagrange-selector columns of seeded Fr values.  Timing depends only on
+    sizes and scalar distributions, not on the bases' discrete logs."""
+
+    def __init__(self, mzk, ctx, ks):
+        self.mzk, self.ctx, self.ks = mzk, ctx, tuple(ks)
+        gmax = 1 << max(ks)
+        self.srs_len = gmax + sum(3 << k for k in ks)
+        self.srs = ctx.gen_bases(0x5125, self.srs_len)
+        self.doms, self.pks, self.cols = {}, {}, {}
+        off = gmax
+        for k in ks:
+            dom = mzk.EvaluationDomain(ctx, 5, k)
+            E = dom.extended_len
+            cols = ctx.gen_rand_fr(0xC0150000 + k, 13 * E)
+            pk = mzk.ProvingKeyDesc()
+            pk.k = k
+            for i in range(7):
+                pk.fixed_ext[i] = cols.ptr + i * E * 32
+            for i in range(3):
+                pk.sigma_ext[i] = cols.ptr + (7 + i) * E * 32
+            pk.l0_ext, pk.l_last_ext, pk.l_active_ext = (cols.ptr + (10 + i) * E * 32 for i in range(3))
+            pk.srs, pk.srs_len = self.srs.ptr, self.srs_len
+            n = 1 << k
+            pk.off_g, pk.off_lagrange, pk.off_lagrange_delta, pk.off_lagrange_double_delta = 0, off, off + n, off + 2 * n
+            off += 3 * n
+            pk.blinding_factors = 7
+            self.doms[k], self.pks[k], self.cols[k] = dom, pk, cols
+
+    def job(self, k, seed):
+        """A proof job with fresh seeded witness columns (a, b, c, z, m, h, Z) on the device."""
+        n = 1 << k
+        w = self.ctx.gen_rand_fr(seed, 7 * n)
+        j = self.mzk.ProofJob()
+        ptr = [w.ptr + i * n * 32 for i in range(7)]
+        j.advice[0], j.advice[1], j.advice[2] = ptr[0], ptr[1], ptr[2]
+        j.perm_z, j.lookup_m, j.lookup_h, j.lookup_Z = ptr[3], ptr[4], ptr[5], ptr[6]
+        for i, name in enumerate(("y", "beta", "gamma", "theta")):
+            getattr(j, name)[:] = [seed % 1000 + 3 + i, 0, 0, 0]
+        for i in range(3):
+            j.quotient_blinds[i][:] = [seed % 977 + 11 + i, 0, 0, 0]
+        return j, w
+
+    def close(self):
+        for d in self.doms.values():
+            d.close()
+
+
+def measure_proof_core(mzk, ctx, keys, k, reps, batch):
+    """Device part of one proof at 2^k rows: plain (one proof per call, every
+    MSM its own call), one proof with its MSMs batched, and `batch` proofs in
+    one call; wall-clock per call, results on the host."""
+    dom, pk = keys.doms[k], keys.pks[k]
+    jobs = [keys.job(k, 0x9000 + i) for i in range(batch)]
+    dom.prove_core_device(pk, [jobs[0][0]])  # warm-up (scratch allocation)
+    dom.prove_core_device(pk, [jobs[0][0]], per_call=True)
+    dom.prove_core_device(pk, [j for j, _ in jobs])
+    t0 = time.perf_counter()
+    for i in range(reps):
+        dom.prove_core_device(pk, [jobs[i % batch][0]], per_call=True)
+    per_call_ms = (time.perf_counter() - t0) / reps * 1e3
+    t0 = time.perf_counter()
+    for i in range(reps):
+        dom.prove_core_device(pk, [jobs[i % batch][0]])
+    plain_ms = (time.perf_counter() - t0) / reps * 1e3
+    t0 = time.perf_counter()
+    for _ in range(max(1, reps // batch)):
+        dom.prove_core_device(pk, [j for j, _ in jobs])
+    batch_ms = (time.perf_counter() - t0) / max(1, reps // batch) * 1e3
+    return {"k": k, "rows": 1 << k, "per_call_ms_per_proof": round(per_call_ms, 2),
+            "one_proof_batched_msms_ms": round(plain_ms, 2), "batch": batch,
+            "batched_ms_per_call": round(batch_ms, 2), "batched_proofs_per_s": round(batch * 1e3 / batch_ms, 2),
+            "msms_per_proof": 11, "scalars": "uniform Fr in every witness column (conservative)"}
+
+
+def measure_batched_msm(mzk, ctx, reps):
+    """64 MSMs, sizes 2^U(12,22) log-uniform, over one shared 2^22-point SRS;
+    one in four sparse (90% of scalars in {0, 1}).  One batched call versus
+    the same MSMs one call each."""
+    import numpy as np
+    rng = np.random.default_rng(0xBA7C4)
+    sizes = [int(2 ** rng.uniform(12, 22)) for _ in range(64)]
+    srs = ctx.gen_bases(0x5125, 1 << 22)
+    bufs, items = [], []
+    one = np.array(FR_ONE_MONT, np.uint64)
+    for i, n in enumerate(sizes):
+        b = ctx.gen_rand_fr(0xB000 + i, n)
+        if i % 4 == 3:
+            s = b.download((n, 4))
+            u = rng.random(n)
+            s[u < 0.45] = 0
+            s[(u >= 0.45) & (u < 0.9)] = one
+            b.upload(s)
+        bufs.append(b)
+        items.append((b, 0, n))
+    total = sum(sizes)
+    together = ctx.msm_batch_device(srs, 1 << 22, items)
+    single = np.stack([ctx.msm_device(b, srs, n) for b, _, n in items])
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ctx.msm_batch_device(srs, 1 << 22, items)
+    t_batch = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for b, _, n in items:
+            ctx.msm_device(b, srs, n)
+    t_seq = (time.perf_counter() - t0) / reps
+    return {"msms": 64, "points": total, "sparse_msms": 16, "batched_ms": round(t_batch * 1e3, 2),
+            "batched_mpts_per_s": round(total / t_batch / 1e6, 2), "one_call_each_ms": round(t_seq * 1e3, 2),
+            "one_call_each_mpts_per_s": round(total / t_seq / 1e6, 2),
+            "batched_equals_one_call_each": bool(np.array_equal(together, single))}
+
+
+def measure_serving(mzk, ctx, keys, n_requests, max_batch, lanes, mem_budget):
+    """Poisson stream of proof requests, k drawn from SERVE_KS with SERVE_WEIGHTS.
+    The plain prover (one proof at a time, every MSM its own call) is measured
+    closed-loop for its throughput; every mode then takes open-loop Poisson
+    streams at 0.8x and 1.5x that rate.  Latency = submit to results on the host."""
+    import threading
+
+    import numpy as np
+    rng = np.random.default_rng(0x5E7E)
+    ks = [int(k) for k in rng.choice(SERVE_KS, size=n_requests, p=SERVE_WEIGHTS)]
+    reqs = [keys.job(k, 0x20000 + i) for i, k in enumerate(ks)]
+
+    def run(server_args, arrivals):
+        srv = mzk.ProvingServer(ctx, **server_args)
+        for k in keys.ks:
+            srv.add_key(keys.doms[k], keys.pks[k])
+        # warm-up: the whole request list once, closed loop (the lanes' scratch
+        # arenas reach their working size here, not in the timed pass)
+        for t in [srv.submit(k, j, keep=w) for k, (j, w) in zip(ks, reqs)]:
+            srv.wait(t)
+        warm_waves = srv.stats()["waves"]
+        lat = [None] * len(ks)
+        tickets = [None] * len(ks)
+        ready = threading.Semaphore(0)
+
+        def collector():
+            for i in range(len(ks)):
+                ready.acquire()
+                lat[i] = srv.wait(tickets[i])[1]
+
+        th = threading.Thread(target=collector)
+        th.start()
+        t0 = time.perf_counter()
+        for i, (k, (job, _)) in enumerate(zip(ks, reqs)):
+            if arrivals is not None:
+                d = t0 + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            tickets[i] = srv.submit(k, job, keep=reqs[i][1])
+            ready.release()
+        th.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        lat = np.array(lat)
+        return {"proofs_per_s": round(len(ks) / wall, 2), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                "p99_ms": round(float(np.percentile(lat, 99)), 2), "waves": st["waves"] - warm_waves,
+                "wall_s": round(wall, 2)}
+
+    modes = {
+        "plain": {"max_batch": 1, "lanes": 1, "per_call": True},           # one proof, one MSM per call
+        "one_proof_batched_msms": {"max_batch": 1, "lanes": 1},            # one proof, its MSMs batched
+        "served": {"max_batch": max_batch, "lanes": lanes, "mem_budget_bytes": mem_budget},
+    }
+    out = {"requests": n_requests, "k_mix": dict(zip(map(str, SERVE_KS), SERVE_WEIGHTS)), "modes": modes}
+    out["closed_loop"] = {name: run(a, None) for name, a in modes.items()}
+    rate = out["closed_loop"]["plain"]["proofs_per_s"]
+    for f in (0.8, 1.5):
+        arr = np.cumsum(rng.exponential(1.0 / (f * rate), size=n_requests))
+        out[f"poisson_{f}x_plain"] = {"rate_per_s": round(f * rate, 2),
+                                      **{name: run(a, arr) for name, a in modes.items()}}
+    return out
 
 
 def dist_init(backend):
@@ -351,10 +538,20 @@ def run_ours(args):
                "api": "mzk_msm_g1 (host pointers, pinned)"}
 
     extra_ntt = extra_q = None
+    extra_prover = {}
     if not args.no_extras:
         del ds, db
         extra_ntt = measure_ntt(mzk, ctx, stream, args.ntt_log_n, 5)
         extra_q = measure_quotient(mzk, ctx, stream, 18, 5)
+        if not args.no_prover:
+            extra_prover["batched_msm"] = measure_batched_msm(mzk, ctx, 3)
+            keys = ProverKeys(mzk, ctx, SERVE_KS)
+            extra_prover["proof_core_k18"] = measure_proof_core(mzk, ctx, keys, 18, 8, 8)
+            extra_prover["proof_core_by_k"] = {str(k): measure_proof_core(mzk, ctx, keys, k, reps, b)
+                                               for k, reps, b in ((14, 32, 16), (16, 32, 16), (20, 4, 2))}
+            extra_prover["serving"] = measure_serving(mzk, ctx, keys, args.serve_requests, 16, 2, 8 << 30)
+            keys.close()
+            del keys
         ds = ctx.gen_rand_fr(0xC0FFEE + rank, n)
         db = ctx.gen_bases(0xBA5E + rank, n)
 
@@ -387,7 +584,7 @@ def run_ours(args):
             "fp_mul_rate_g_per_s": round(fp_mul_rate / 1e9, 2),
             "imad_probe_t_per_s": {k: round(v / 1e12, 3) for k, v in imad_variants.items()},
             "madd_in_registers_g_per_s": round(madd_rate / 1e9, 3),
-            "ntt": extra_ntt, "quotient_k18": extra_q,
+            "ntt": extra_ntt, "quotient_k18": extra_q, **extra_prover,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -205,19 +205,28 @@ typedef struct {
 /* For each job: commitments (out: count x 11 x 18 u64 G1Projective, in the
  * order a, b, c, m (delta), z (delta), Z (double delta), h, quotient limbs
  * 0..3), lagrange_to_coeff and coeff_to_extended of the seven witness
- * polynomials, compute_h_poly.  All jobs' MSMs run as two batched MSMs. */
+ * polynomials, compute_h_poly.  All jobs' MSMs run as two batched MSMs, or,
+ * with MZK_PROVE_MSM_PER_CALL in flags, each as its own call (the plain
+ * one-call-at-a-time form; same results). */
+#define MZK_PROVE_MSM_PER_CALL 1u
 int mzk_prove_core_device(mzk_ctx *ctx, mzk_domain *d, const mzk_proving_key_desc *pk, const mzk_proof_job *jobs,
-                          size_t count, uint64_t *out);
+                          size_t count, uint32_t flags, uint64_t *out);
 
 /* ---- proving service (continuous batching over the proof core) ---------- */
-/* No reference counterpart: the reference proves one call at a time.  A worker
- * thread drains the request queue in waves: each wave takes queued requests
- * oldest first while it holds fewer than max_batch proofs and their device
- * scratch fits mem_budget_bytes (0: no memory limit), and runs them as one
- * mixed-k proof-core call (max_batch = 1 is the plain one-at-a-time prover).
- * Witness buffers referenced by a job must stay valid until its wait returns. */
+/* No reference counterpart: the reference proves one call at a time.
+ * `lanes` worker threads (1..8), each with its own device context, serve one
+ * request queue.  An idle lane takes a wave: queued requests oldest first
+ * while the wave holds fewer than max_batch proofs, its device scratch stays
+ * within mem_budget_bytes / lanes and that of all proofs in flight within
+ * mem_budget_bytes (0: no limit; a proof larger than that runs alone when
+ * nothing else is in flight), run as one mixed-k proof-core call, so
+ * requests arriving while a wave runs start beside it on the device.
+ * max_batch = 1 with one lane and MZK_PROVE_MSM_PER_CALL is the plain
+ * one-call-at-a-time prover.  Witness
+ * buffers referenced by a job must stay valid until its wait returns. */
 typedef struct mzk_server mzk_server;
-int mzk_server_create(mzk_ctx *ctx, uint32_t max_batch, uint64_t mem_budget_bytes, mzk_server **out);
+int mzk_server_create(mzk_ctx *ctx, uint32_t max_batch, uint32_t lanes, uint64_t mem_budget_bytes,
+                      uint32_t flags /* MZK_PROVE_* of every wave */, mzk_server **out);
 /* register the domain and proving key of one k (all keys share one SRS buffer) */
 int mzk_server_add_key(mzk_server *s, mzk_domain *d, const mzk_proving_key_desc *pk);
 int mzk_server_submit(mzk_server *s, uint32_t k, const mzk_proof_job *job, uint64_t *ticket);

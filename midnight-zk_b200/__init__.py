@@ -66,8 +66,8 @@ SIGNATURES = {
     "mzk_domain_op_device": (_i32, [_vp, _vp, _i32, _vp, _vp]),
     "mzk_quotient_eval_device": (_i32, [_vp, _vp, ctypes.c_void_p, _i32, _vp]),
     "mzk_compute_h_poly_device": (_i32, [_vp, _vp, ctypes.c_void_p, _vp, _sz, _u64p, _u64p, _vp]),
-    "mzk_prove_core_device": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u64p]),
-    "mzk_server_create": (_i32, [_vp, _u32, _u64, ctypes.POINTER(_vp)]),
+    "mzk_prove_core_device": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u32, _u64p]),
+    "mzk_server_create": (_i32, [_vp, _u32, _u32, _u64, _u32, ctypes.POINTER(_vp)]),
     "mzk_server_add_key": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_submit": (_i32, [_vp, _u32, ctypes.c_void_p, _u64p]),
     "mzk_server_wait": (_i32, [_vp, _u64, _u64p, ctypes.POINTER(ctypes.c_double)]),
@@ -99,6 +99,7 @@ class ProofJob(ctypes.Structure):
                 ("quotient_blinds", (ctypes.c_uint64 * 4) * 3)]
 
 
+PROVE_MSM_PER_CALL = 1  # MZK_PROVE_MSM_PER_CALL
 PROOF_CORE_COMMITMENTS = ["a", "b", "c", "m_delta", "z_delta", "Z_double_delta", "h", "H0", "H1", "H2", "H3"]
 
 
@@ -449,12 +450,13 @@ class EvaluationDomain:
                                                _ptr(blinds), _ptr(out), dl or None))
         return out
 
-    def prove_core_device(self, pk_desc, jobs):
-        """Device part of create_proof for a list of ProofJob: (len, 11, 18) commitments."""
+    def prove_core_device(self, pk_desc, jobs, per_call=False):
+        """Device part of create_proof for a list of ProofJob: (len, 11, 18) commitments.
+        per_call: every MSM as its own call instead of two batched MSMs."""
         arr = (ProofJob * max(1, len(jobs)))(*jobs)
         out = np.zeros((max(1, len(jobs)), len(PROOF_CORE_COMMITMENTS), 18), np.uint64)
         _check(lib().mzk_prove_core_device(self.ctx.h, self.h, ctypes.byref(pk_desc), ctypes.addressof(arr),
-                                           len(jobs), _ptr(out)))
+                                           len(jobs), PROVE_MSM_PER_CALL if per_call else 0, _ptr(out)))
         return out[:len(jobs)]
 
     def op_device(self, name, d_in, d_out):
@@ -467,27 +469,35 @@ class EvaluationDomain:
 class ProvingServer:
     """Proving service with continuous batching (mzk_server_*)."""
 
-    def __init__(self, ctx, max_batch=16, mem_budget_bytes=0):
+    def __init__(self, ctx, max_batch=16, lanes=2, mem_budget_bytes=0, per_call=False):
         self.ctx = ctx
         h = _vp()
-        _check(lib().mzk_server_create(ctx.h, int(max_batch), int(mem_budget_bytes), ctypes.byref(h)))
+        _check(lib().mzk_server_create(ctx.h, int(max_batch), int(lanes), int(mem_budget_bytes),
+                                       PROVE_MSM_PER_CALL if per_call else 0, ctypes.byref(h)))
         self.h = h.value
         ctx._servers.add(self)
         self._keys = []
+        self._held = {}
 
     def add_key(self, domain, pk_desc):
         self._keys.append((domain, pk_desc))
         _check(lib().mzk_server_add_key(self.h, domain.h, ctypes.byref(pk_desc)))
 
-    def submit(self, k, job):
+    def submit(self, k, job, keep=None):
+        """Queue one proof; `keep` (e.g. the job's witness DeviceBuffers) stays
+        referenced until the request's wait returns."""
         t = np.zeros(1, np.uint64)
         _check(lib().mzk_server_submit(self.h, int(k), ctypes.byref(job), _ptr(t)))
+        self._held[int(t[0])] = keep
         return int(t[0])
 
     def wait(self, ticket):
         out = np.zeros((len(PROOF_CORE_COMMITMENTS), 18), np.uint64)
         lat = ctypes.c_double()
-        _check(lib().mzk_server_wait(self.h, ticket, _ptr(out), ctypes.byref(lat)))
+        try:
+            _check(lib().mzk_server_wait(self.h, ticket, _ptr(out), ctypes.byref(lat)))
+        finally:
+            self._held.pop(int(ticket), None)
         return out, lat.value
 
     def stats(self):

@@ -39,7 +39,11 @@ Status Context::ensure(const char* name, size_t bytes, void** out) {
         cudaFree(b.p);
         b.p = nullptr;
         b.bytes = 0;
+        // a buffer that had to grow once tends to grow again (mixed sizes):
+        // take 25 % headroom so repeated growth reallocates rarely
+        bytes += bytes / 4;
     }
+    bytes = (bytes + 255) & ~(size_t)255;
     cudaError_t e = cudaMalloc(&b.p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -119,7 +123,6 @@ Context::~Context() {
 
 namespace mzk {
 Context* context_of(mzk_ctx* ctx) { return &ctx->impl; }
-std::recursive_mutex* context_mutex(mzk_ctx* ctx) { return &ctx->impl.mu; }
 const Domain* domain_of(mzk_domain* d) { return d->impl; }
 }  // namespace mzk
 
@@ -475,14 +478,14 @@ int mzk_compute_h_poly_device(mzk_ctx* ctx, mzk_domain* d, const mzk_quotient_de
 }
 
 int mzk_prove_core_device(mzk_ctx* ctx, mzk_domain* d, const mzk_proving_key_desc* pk, const mzk_proof_job* jobs,
-                          size_t count, uint64_t* out) {
+                          size_t count, uint32_t flags, uint64_t* out) {
     if (int s = check_ctx(ctx)) return s;
     if (!d || !pk || !out || (count && !jobs)) {
         mzk::set_error("prove_core: null argument");
         return mzk::ERR_ARG;
     }
     Guard g(ctx);
-    MZK_TRY(mzk::prove_core_device(&ctx->impl, d->impl, pk, jobs, count, out, ctx->impl.stream));
+    MZK_TRY(mzk::prove_core_device(&ctx->impl, d->impl, pk, jobs, count, out, flags, ctx->impl.stream));
     MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
     return mzk::OK;
 }

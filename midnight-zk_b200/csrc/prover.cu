@@ -17,7 +17,8 @@
 //      extended_to_coeff, blinded limbs;
 //   5. the limb commitments.
 // The MSMs of all proofs in a call run as two batched MSMs (step 1 for all
-// proofs, step 5 for all proofs), so small proofs share the GPU's chunks.
+// proofs, step 5 for all proofs), so small proofs share the GPU's chunks; with
+// MZK_PROVE_MSM_PER_CALL each MSM is its own call instead (the plain form).
 // Witness generation, the permutation and logup running products, the
 // transcript, evaluations and the multi-open argument stay with the caller.
 #include <cuda_runtime.h>
@@ -56,8 +57,20 @@ constexpr int kPolys = 7;  // a, b, c, z, m, h, Z
 
 }  // namespace
 
+// the MSMs of `items` against the SRS: one batched MSM, or one call each
+static Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const std::vector<BatchItem>& items,
+                       uint64_t* res, uint32_t flags, cudaStream_t st) {
+    if (!(flags & MZK_PROVE_MSM_PER_CALL))
+        return msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res, st);
+    for (size_t i = 0; i < items.size(); i++) {
+        const void* bases = static_cast<const uint8_t*>(srs) + items[i].base_offset * 96;
+        MZK_TRY(msm_g1_device(ctx, items[i].d_scalars, bases, items[i].n, res + i * 18, st, nullptr));
+    }
+    return OK;
+}
+
 Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_proving_key_desc* const* pks,
-                        const mzk_proof_job* jobs, size_t count, uint64_t* out, cudaStream_t st) {
+                        const mzk_proof_job* jobs, size_t count, uint64_t* out, uint32_t flags, cudaStream_t st) {
     std::memset(out, 0, count * kProofCoreCommitments * 18 * 8);
     if (count == 0) return OK;
     if (pks[0]->srs == nullptr) {
@@ -69,6 +82,16 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
     std::vector<BatchItem> items;
     std::vector<Fr*> coeff(count * kPolys), ext(count * kPolys), limbs(count);
     size_t max_en = 0;
+    // all per-proof scratch of the call in one buffer, carved in job order, so
+    // a call's scratch grows (and is reallocated) only when its total grows
+    size_t wave_elems = 0;
+    for (size_t j = 0; j < count; j++) {
+        const size_t n = (size_t)1 << doms[j]->k, en = (size_t)1 << doms[j]->ext_k;
+        wave_elems += kPolys * n + kPolys * en + 3 * n + (size_t)doms[j]->quotient_poly_degree * n;
+    }
+    void* wave;
+    MZK_TRY(ctx->ensure("core_wave", wave_elems * sizeof(Fr), &wave));
+    Fr* carve = static_cast<Fr*>(wave);
     for (size_t j = 0; j < count; j++) {
         const Domain* d = doms[j];
         const mzk_proving_key_desc* pk = pks[j];
@@ -88,16 +111,16 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
             return ERR_ARG;
         }
         max_en = std::max<size_t>(max_en, en);
-        void *pc, *pe, *pd, *pl;
-        MZK_TRY(ctx->ensure(("core_coeff_" + tag).c_str(), (size_t)kPolys * n * sizeof(Fr), &pc));
-        MZK_TRY(ctx->ensure(("core_ext_" + tag).c_str(), (size_t)kPolys * en * sizeof(Fr), &pe));
-        MZK_TRY(ctx->ensure(("core_delta_" + tag).c_str(), (size_t)3 * n * sizeof(Fr), &pd));
-        MZK_TRY(ctx->ensure(("core_limbs_" + tag).c_str(), (size_t)qdeg * n * sizeof(Fr), &pl));
+        Fr* pc = carve;
+        Fr* pe = pc + (size_t)kPolys * n;
+        Fr* pd = pe + (size_t)kPolys * en;
+        Fr* pl = pd + (size_t)3 * n;
+        carve = pl + (size_t)qdeg * n;
         for (int p = 0; p < kPolys; p++) {
-            coeff[j * kPolys + p] = static_cast<Fr*>(pc) + (size_t)p * n;
-            ext[j * kPolys + p] = static_cast<Fr*>(pe) + (size_t)p * en;
+            coeff[j * kPolys + p] = pc + (size_t)p * n;
+            ext[j * kPolys + p] = pe + (size_t)p * en;
         }
-        limbs[j] = static_cast<Fr*>(pl);
+        limbs[j] = pl;
         const mzk_proof_job& jb = jobs[j];
         const void* lag[kPolys] = {jb.advice[0], jb.advice[1], jb.advice[2], jb.perm_z, jb.lookup_m, jb.lookup_h,
                                    jb.lookup_Z};
@@ -107,7 +130,7 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
                 return ERR_ARG;
             }
         const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 8);
-        Fr* dm = static_cast<Fr*>(pd);
+        Fr* dm = pd;
         Fr* dz = dm + n;
         Fr* dZ = dz + n;
         k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(jb.lookup_m), dm, n, 1);
@@ -124,7 +147,7 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
     }
     // 1. witness commitments of every proof in one batch
     std::vector<uint64_t> res1(items.size() * 18);
-    MZK_TRY(msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res1.data(), st));
+    MZK_TRY(run_msms(ctx, srs, srs_len, items, res1.data(), flags, st));
     for (size_t j = 0; j < count; j++)
         std::memcpy(out + (j * kProofCoreCommitments) * 18, res1.data() + j * 7 * 18, 7 * 18 * 8);
     // 2-4. per proof: coefficient and extended forms, quotient limbs
@@ -188,17 +211,17 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
             items.push_back({limbs[j] + (size_t)i * n, pks[j]->off_g, n});
     }
     std::vector<uint64_t> res2(items.size() * 18);
-    MZK_TRY(msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res2.data(), st));
+    MZK_TRY(run_msms(ctx, srs, srs_len, items, res2.data(), flags, st));
     for (size_t j = 0; j < count; j++)
         std::memcpy(out + (j * kProofCoreCommitments + 7) * 18, res2.data() + j * 4 * 18, 4 * 18 * 8);
     return OK;
 }
 
 Status prove_core_device(Context* ctx, const Domain* d, const mzk_proving_key_desc* pk, const mzk_proof_job* jobs,
-                         size_t count, uint64_t* out, cudaStream_t st) {
+                         size_t count, uint64_t* out, uint32_t flags, cudaStream_t st) {
     std::vector<const Domain*> doms(count, d);
     std::vector<const mzk_proving_key_desc*> pks(count, pk);
-    return prove_core_multi(ctx, doms.data(), pks.data(), jobs, count, out, st);
+    return prove_core_multi(ctx, doms.data(), pks.data(), jobs, count, out, flags, st);
 }
 
 }  // namespace mzk

@@ -43,11 +43,13 @@ Status compute_h_limbs_device(Context* ctx, const Domain* d, const mzk_quotient_
                               void* d_limbs_out, void* d_hbuf, void* d_blinds, cudaStream_t st);
 // device part of create_proof for the single-proof circuit (prover.cu)
 constexpr int kProofCoreCommitments = 11;  // a, b, c, m, z, Z, h, 4 quotient limbs
+// flags: MZK_PROVE_MSM_PER_CALL runs every MSM as its own call (the plain
+// one-call-at-a-time form) instead of the two batched MSMs
 Status prove_core_device(Context* ctx, const Domain* d, const mzk_proving_key_desc* pk, const mzk_proof_job* jobs,
-                         size_t count, uint64_t* out, cudaStream_t st);
+                         size_t count, uint64_t* out, uint32_t flags, cudaStream_t st);
 // jobs of different k: job j uses doms[j] and pks[j] (all keys share one SRS buffer)
 Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_proving_key_desc* const* pks,
-                        const mzk_proof_job* jobs, size_t count, uint64_t* out, cudaStream_t st);
+                        const mzk_proof_job* jobs, size_t count, uint64_t* out, uint32_t flags, cudaStream_t st);
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st);
 

@@ -1,16 +1,19 @@
 // server.cu — a proving service over the device proof core.
 //
 // Requests (one proof each, any registered k) are queued by any number of
-// host threads; one worker thread drains the queue in waves.  A wave takes
-// every queued request, oldest first, while the wave has fewer than
-// `max_batch` proofs and their device scratch fits the memory budget, and runs
-// them as ONE mixed-k call of the proof core: the witness commitments of all
-// of them form one batched MSM, the quotient-limb commitments another, so
-// requests that arrive while a wave runs are admitted into the next wave
-// (continuous batching) instead of waiting for one another one by one.  With
-// max_batch = 1 the same service is the plain one-proof-at-a-time prover.
-// Latency is measured from submit to the moment the wave that holds the
-// request has its results on the host.
+// host threads and served by `lanes` worker threads, each with its own device
+// context (stream and scratch arena).  An idle lane takes a wave: queued
+// requests, oldest first, while the wave holds fewer than `max_batch` proofs
+// and the device scratch of every proof in flight (all lanes) stays within
+// the memory budget; it runs the wave as ONE mixed-k call of the proof core,
+// in which the witness commitments of all its proofs form one batched MSM and
+// the quotient-limb commitments another.  Requests that arrive while a wave is
+// on the GPU are taken by the next free lane at once, so their kernels run
+// beside the running wave's on the device and fill what one wave leaves idle
+// (the host-side tails of a wave included): continuous batching.  With
+// max_batch = 1 and one lane the same service is the plain
+// one-proof-at-a-time prover.  Latency is measured from submit to the moment
+// the wave that holds the request has its results on the host.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -30,6 +33,10 @@
 
 namespace mzk {
 
+// access to the context internals of capi.cu
+Context* context_of(mzk_ctx* ctx);
+const Domain* domain_of(mzk_domain* d);
+
 namespace {
 
 double now_ms() {
@@ -40,7 +47,7 @@ double now_ms() {
 struct ServerKey {
     const Domain* dom;
     mzk_proving_key_desc pk;
-    size_t job_bytes;  // device scratch of one proof of this k
+    uint64_t job_bytes;  // device scratch of one proof of this k
 };
 
 struct Request {
@@ -56,41 +63,68 @@ struct Request {
 }  // namespace
 
 struct Server {
-    Context* ctx = nullptr;
-    std::recursive_mutex* ctx_mu = nullptr;
-    int device = 0;
+    std::vector<mzk_ctx*> lanes;  // one device context per worker
     uint32_t max_batch = 1;
-    uint64_t mem_budget = 0;
+    uint32_t flags = 0;       // MZK_PROVE_* flags of every wave
+    uint64_t mem_budget = 0;  // 0: no limit
     std::map<uint32_t, ServerKey> keys;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<uint64_t> queue;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
     uint64_t next_ticket = 1;
+    uint64_t in_flight_bytes = 0;
     bool stop = false;
     uint64_t waves = 0, proofs = 0;
     double busy_ms = 0;
-    std::thread worker;
+    std::vector<std::thread> workers;
 
-    void run() {
-        cudaSetDevice(device);
+    // the next wave for an idle lane; called with mu held.  Empty when the
+    // head of the queue does not fit in the memory left by the waves in flight.
+    std::vector<uint64_t> take_wave(uint64_t* bytes) {
+        std::vector<uint64_t> batch;
+        *bytes = 0;
+        // one wave takes at most its lane's share of the budget, so the other
+        // lanes can admit requests beside it
+        const uint64_t lane_cap = mem_budget / lanes.size();
+        while (!queue.empty() && batch.size() < max_batch) {
+            const ServerKey& key = keys[reqs[queue.front()]->k];
+            const uint64_t wave_after = *bytes + key.job_bytes;
+            // the first proof of a wave is admitted when nothing else is in flight,
+            // so a proof larger than the budget still runs (alone)
+            const bool fits = mem_budget == 0 ||
+                              (in_flight_bytes + wave_after <= mem_budget && wave_after <= lane_cap) ||
+                              (in_flight_bytes == 0 && batch.empty());
+            if (!fits) break;
+            *bytes += key.job_bytes;
+            batch.push_back(queue.front());
+            queue.pop_front();
+        }
+        return batch;
+    }
+
+    void run(mzk_ctx* lane) {
+        Context* ctx = context_of(lane);
+        cudaSetDevice(ctx->device);
         for (;;) {
             std::vector<uint64_t> batch;
             std::vector<mzk_proof_job> jobs;
             std::vector<const Domain*> doms;
             std::vector<const mzk_proving_key_desc*> pks;
+            uint64_t bytes = 0;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] { return stop || !queue.empty(); });
-                if (queue.empty()) return;  // stop requested and nothing left
-                uint64_t bytes = 0;
-                while (!queue.empty() && batch.size() < max_batch) {
-                    Request& r = *reqs[queue.front()];
+                cv_work.wait(lk, [&] {
+                    if (stop && queue.empty()) return true;
+                    if (queue.empty()) return false;
+                    batch = take_wave(&bytes);
+                    return !batch.empty();
+                });
+                if (batch.empty()) return;  // stop requested and nothing left
+                in_flight_bytes += bytes;
+                for (uint64_t t : batch) {
+                    const Request& r = *reqs[t];
                     const ServerKey& key = keys[r.k];
-                    if (!batch.empty() && mem_budget && bytes + key.job_bytes > mem_budget) break;
-                    bytes += key.job_bytes;
-                    batch.push_back(queue.front());
-                    queue.pop_front();
                     jobs.push_back(r.job);
                     doms.push_back(key.dom);
                     pks.push_back(&key.pk);
@@ -101,9 +135,9 @@ struct Server {
             Status st;
             std::string err;
             {
-                std::lock_guard<std::recursive_mutex> g(*ctx_mu);
-                cudaSetDevice(device);
-                st = prove_core_multi(ctx, doms.data(), pks.data(), jobs.data(), jobs.size(), out.data(), ctx->stream);
+                std::lock_guard<std::recursive_mutex> g(ctx->mu);
+                st = prove_core_multi(ctx, doms.data(), pks.data(), jobs.data(), jobs.size(), out.data(), flags,
+                                      ctx->stream);
                 if (st == OK) {
                     cudaError_t e = cudaStreamSynchronize(ctx->stream);
                     if (e != cudaSuccess) {
@@ -116,6 +150,7 @@ struct Server {
             const double t1 = now_ms();
             {
                 std::lock_guard<std::mutex> lk(mu);
+                in_flight_bytes -= bytes;
                 waves++;
                 proofs += batch.size();
                 busy_ms += t1 - t0;
@@ -129,6 +164,7 @@ struct Server {
                 }
             }
             cv_done.notify_all();
+            cv_work.notify_all();  // memory came free: another lane may admit now
         }
     }
 };
@@ -143,7 +179,8 @@ namespace {
 
 // device scratch of one proof of size 2^k in the proof core: coefficient and
 // extended forms of seven polynomials, three delta forms, four limbs, plus the
-// MSM entries and buckets it contributes to the two batched MSMs
+// sorted MSM entries it contributes to the batched witness MSM (the largest
+// of the two batched MSMs)
 uint64_t job_scratch_bytes(const mzk::Domain* d) {
     const uint64_t n = 1ull << d->k, en = 1ull << d->ext_k;
     const uint64_t fr = 32;
@@ -157,7 +194,8 @@ uint64_t job_scratch_bytes(const mzk::Domain* d) {
 // these entry points are declared in include/mzk.h
 extern "C" {
 
-int mzk_server_create(mzk_ctx* ctx, uint32_t max_batch, uint64_t mem_budget_bytes, mzk_server** out);
+int mzk_server_create(mzk_ctx* ctx, uint32_t max_batch, uint32_t lanes, uint64_t mem_budget_bytes,
+                      uint32_t flags, mzk_server** out);
 int mzk_server_add_key(mzk_server* s, mzk_domain* d, const mzk_proving_key_desc* pk);
 int mzk_server_submit(mzk_server* s, uint32_t k, const mzk_proof_job* job, uint64_t* ticket);
 int mzk_server_wait(mzk_server* s, uint64_t ticket, uint64_t* out, double* latency_ms);
@@ -166,25 +204,28 @@ int mzk_server_destroy(mzk_server* s);
 
 }  // extern "C"
 
-// access to the context internals of capi.cu
-namespace mzk {
-Context* context_of(mzk_ctx* ctx);
-std::recursive_mutex* context_mutex(mzk_ctx* ctx);
-const Domain* domain_of(mzk_domain* d);
-}  // namespace mzk
-
-extern "C" int mzk_server_create(mzk_ctx* ctx, uint32_t max_batch, uint64_t mem_budget_bytes, mzk_server** out) {
-    if (!ctx || !out || max_batch == 0) {
-        mzk::set_error("server: need a context and max_batch >= 1");
+extern "C" int mzk_server_create(mzk_ctx* ctx, uint32_t max_batch, uint32_t lanes, uint64_t mem_budget_bytes,
+                                 uint32_t flags, mzk_server** out) {
+    if (!ctx || !out || max_batch == 0 || lanes == 0 || lanes > 8) {
+        mzk::set_error("server: need a context, max_batch >= 1 and 1..8 lanes");
         return mzk::ERR_ARG;
     }
+    *out = nullptr;
     mzk_server* s = new mzk_server;
-    s->impl.ctx = mzk::context_of(ctx);
-    s->impl.ctx_mu = mzk::context_mutex(ctx);
-    s->impl.device = s->impl.ctx->device;
     s->impl.max_batch = max_batch;
     s->impl.mem_budget = mem_budget_bytes;
-    s->impl.worker = std::thread([s] { s->impl.run(); });
+    s->impl.flags = flags;
+    const int device = mzk::context_of(ctx)->device;
+    for (uint32_t i = 0; i < lanes; i++) {
+        mzk_ctx* lane = nullptr;
+        if (int st = mzk_ctx_create(device, &lane)) {
+            for (mzk_ctx* c : s->impl.lanes) mzk_ctx_destroy(c);
+            delete s;
+            return st;
+        }
+        s->impl.lanes.push_back(lane);
+    }
+    for (mzk_ctx* lane : s->impl.lanes) s->impl.workers.emplace_back([s, lane] { s->impl.run(lane); });
     *out = s;
     return mzk::OK;
 }
@@ -256,7 +297,9 @@ extern "C" int mzk_server_destroy(mzk_server* s) {
         s->impl.stop = true;
     }
     s->impl.cv_work.notify_all();
-    if (s->impl.worker.joinable()) s->impl.worker.join();
+    for (std::thread& w : s->impl.workers)
+        if (w.joinable()) w.join();
+    for (mzk_ctx* c : s->impl.lanes) mzk_ctx_destroy(c);
     delete s;
     return mzk::OK;
 }

@@ -33,3 +33,5 @@ def test_prove_core_batch_equals_single(ctx):
     together = st.g.prove_core_device(st.pk, jobs)
     for i, j in enumerate(jobs):
         assert np.array_equal(st.g.prove_core_device(st.pk, [j])[0], together[i])
+    # the plain form (every MSM its own call) gives the same commitments
+    assert np.array_equal(st.g.prove_core_device(st.pk, jobs[:2], per_call=True), together[:2])

@@ -71,7 +71,7 @@ def test_mixed_waves_equal_alone_and_oracle(ctx, keys):
 
 @pytest.mark.parametrize("mode", ["plain", "budget"])
 def test_one_proof_per_wave(ctx, keys, mode):
-    srv = (mzk.ProvingServer(ctx, max_batch=1) if mode == "plain"
+    srv = (mzk.ProvingServer(ctx, max_batch=1, lanes=1, per_call=True) if mode == "plain"
            else mzk.ProvingServer(ctx, max_batch=16, mem_budget_bytes=1))
     srv.add_key(keys[7].g, keys[7].pk)
     jobs = [keys[7].job(200 + i)[0] for i in range(4)]
