@@ -44,6 +44,7 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--log-n", type=int, default=24)
+    p.add_argument("--window", type=int, default=0, help="force the MSM window width c (0: cost model)")
     p.add_argument("--cpu-sample-log-n", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -437,6 +438,8 @@ def run_ours(args):
     mzk = load()
     ctx = mzk.Context(local)
     n = 1 << args.log_n
+    if args.window:
+        ctx.set_msm_window(args.window)
     ds = ctx.gen_rand_fr(0xC0FFEE + rank, n)
     db = ctx.gen_bases(0xBA5E + rank, n)
     imad_peak, fp_mul_rate, imad_variants = ctx.probe_imad_peak()

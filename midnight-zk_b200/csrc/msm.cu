@@ -47,7 +47,7 @@ namespace mzk {
 
 namespace {
 
-constexpr int kGroupLen = 16;      // buckets per running-sum group
+constexpr int kGroupLog = 5;       // log2 of the buckets per running-sum group (fewer when nb is smaller)
 constexpr int kAccThreads = 128;   // threads per block of the accumulate kernel
 constexpr int kReduceThreads = 128;
 constexpr uint32_t kNoKey = 0xffffffffu;
@@ -57,7 +57,8 @@ struct MsmShape {
     int windows;    // number of windows
     uint32_t nb;    // buckets per window = 2^(c-1)
     uint32_t keys;  // windows * nb
-    uint32_t groups;  // running-sum groups per window = nb / kGroupLen
+    int glen_log;   // log2 of the buckets per running-sum group
+    uint32_t groups;  // running-sum groups per window = nb >> glen_log
     int planes;     // log2(groups)
 };
 
@@ -67,7 +68,8 @@ MsmShape make_shape(int c) {
     s.windows = (256 + c - 1) / c;
     s.nb = 1u << (c - 1);
     s.keys = s.nb * (uint32_t)s.windows;
-    s.groups = s.nb / kGroupLen;
+    s.glen_log = c - 1 < kGroupLog ? c - 1 : kGroupLog;
+    s.groups = s.nb >> s.glen_log;
     s.planes = 0;
     while ((1u << s.planes) < s.groups) s.planes++;
     return s;
@@ -132,30 +134,55 @@ __global__ void k_histogram(const Fr* __restrict__ scalars, size_t n, int c, int
     }
 }
 
+// Windows whose cursor atomics a warp keeps in flight at once: the scatter is
+// bound by the latency of the atomics' round trips, not by bandwidth.
+constexpr int kScatterWindows = 8;
+
+// The cursor of bucket `key` is cursor[key] (= offsets + 1 of the caller):
+// it starts at the bucket's first slot (the exclusive scan written one place
+// to the right) and each atomic returns absolute positions.  After the
+// scatter cursor[key] = end of bucket key = start of bucket key + 1, so the
+// array from offsets[0] = 0 is exactly the bucket offset table.
+__device__ __forceinline__ void scatter_group(const uint32_t (&key)[kScatterWindows],
+                                              const bool (&neg)[kScatterWindows], uint32_t value, int lane,
+                                              uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint32_t peers[kScatterWindows], slot[kScatterWindows];
+#pragma unroll
+    for (int j = 0; j < kScatterWindows; j++) {
+        peers[j] = __match_any_sync(0xffffffffu, key[j]);
+        slot[j] = 0;
+        if (key[j] != kNoKey && lane == __ffs(peers[j]) - 1) slot[j] = atomicAdd(&cursor[key[j]], (uint32_t)__popc(peers[j]));
+    }
+#pragma unroll
+    for (int j = 0; j < kScatterWindows; j++) {
+        const uint32_t first = __shfl_sync(0xffffffffu, slot[j], __ffs(peers[j]) - 1);
+        if (key[j] != kNoKey) sorted[first + (uint32_t)__popc(peers[j] & lt_mask)] = value | (neg[j] ? 0x80000000u : 0u);
+    }
+}
+
 __global__ void k_scatter(const Fr* __restrict__ scalars, size_t n, int c, int windows, uint32_t nb,
-                          const uint32_t* __restrict__ offsets, uint32_t* __restrict__ fill,
-                          uint32_t* __restrict__ sorted) {
+                          uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
-    const uint32_t lt_mask = (1u << lane) - 1u;
     for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
         const size_t i = base + threadIdx.x;
         const bool valid = i < n;
         Fr s = valid ? fr_from_mont(load_fr(scalars, i)) : fr_zero();
         uint32_t carry = 0;
-        for (int w = 0; w < windows; w++) {
-            bool neg;
-            uint32_t key = next_digit(s, w, c, nb, carry, neg);
-            if (!valid) key = kNoKey;
-            const uint32_t peers = __match_any_sync(0xffffffffu, key);
-            const int leader = __ffs(peers) - 1;
-            uint32_t slot = 0;
-            if (key != kNoKey && lane == leader) slot = atomicAdd(&fill[key], (uint32_t)__popc(peers));
-            slot = __shfl_sync(peers, slot, leader);
-            if (key != kNoKey) {
-                const uint32_t pos = offsets[key] + slot + (uint32_t)__popc(peers & lt_mask);
-                sorted[pos] = (uint32_t)i | (neg ? 0x80000000u : 0u);
+        for (int w0 = 0; w0 < windows; w0 += kScatterWindows) {
+            uint32_t key[kScatterWindows];
+            bool neg[kScatterWindows];
+#pragma unroll
+            for (int j = 0; j < kScatterWindows; j++) {
+                key[j] = kNoKey;
+                neg[j] = false;
+                if (w0 + j < windows) {
+                    key[j] = next_digit(s, w0 + j, c, nb, carry, neg[j]);
+                    if (!valid) key[j] = kNoKey;
+                }
             }
+            scatter_group(key, neg, (uint32_t)i, lane, cursor, sorted);
         }
     }
 }
@@ -386,19 +413,47 @@ __global__ void __launch_bounds__(kReduceThreads) k_fixup_long(const int* __rest
     }
 }
 
-// per (window, group): running sum over kGroupLen buckets, top first
+// ---- bucket reduction over a table of windows ----
+//
+// A window's sum S = sum_{b=1}^{nb} b * B_b is reduced in three steps:
+//   1. running sums over groups of L = 2^glen_log consecutive buckets, top
+//      first: R_g = sum of the group's buckets, T_g = sum_i (i+1) B_{gL+i};
+//   2. plane sums: Q_j = sum of R_g over the groups g with bit j set, and
+//      T = sum_g T_g (each plane split over `split` blocks, then merged);
+//   3. S = T + L * sum_j 2^j Q_j (Horner, one thread per window).
+// One table row per window serves a single MSM and a batch of MSMs alike.
+struct WinDev {
+    uint32_t key_start;    // first bucket key of the window
+    uint32_t nb;           // buckets in the window
+    uint32_t group_start;  // first running-sum group of the window
+    uint32_t plane_start;  // first of its planes + 1 plane slots
+    uint32_t glen_log;     // log2 of the buckets per group
+    int planes;            // log2 of the groups per window
+};
+
+__device__ __forceinline__ uint32_t find_win(const WinDev* wins, uint32_t n_wins, uint32_t v, bool by_plane) {
+    uint32_t lo = 0, hi = n_wins;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((by_plane ? wins[mid].plane_start : wins[mid].group_start) <= v) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 __global__ void __launch_bounds__(kReduceThreads) k_group_sums(const Xyzz* __restrict__ buckets,
-                                                               const uint32_t* __restrict__ offsets, uint32_t nb,
-                                                               uint32_t groups, uint32_t total_groups,
-                                                               Xyzz* __restrict__ run_out, Xyzz* __restrict__ tot_out) {
+                                                               const uint32_t* __restrict__ offsets,
+                                                               const WinDev* __restrict__ wins, uint32_t n_wins,
+                                                               uint32_t total_groups, Xyzz* __restrict__ run_out,
+                                                               Xyzz* __restrict__ tot_out) {
     const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= total_groups) return;
-    const uint32_t w = gid / groups, g = gid % groups;
-    const uint32_t key0 = w * nb + g * kGroupLen;
+    const WinDev wd = wins[find_win(wins, n_wins, gid, false)];
+    const uint32_t key0 = wd.key_start + ((gid - wd.group_start) << wd.glen_log);
     Xyzz run, tot;
     xyzz_set_inf(run);
     xyzz_set_inf(tot);
-    for (int b = kGroupLen - 1; b >= 0; b--) {
+    for (int b = (1 << wd.glen_log) - 1; b >= 0; b--) {
         const uint32_t key = key0 + (uint32_t)b;
         if (offsets[key + 1] > offsets[key]) run = xyzz_add(run, load_xyzz(&buckets[key]));
         tot = xyzz_add(tot, run);
@@ -407,43 +462,106 @@ __global__ void __launch_bounds__(kReduceThreads) k_group_sums(const Xyzz* __res
     store_xyzz(&tot_out[gid], tot);
 }
 
-// one block per (window, plane): plane < planes sums R_g over g with bit
-// `plane` set; plane == planes sums T_g over all g.
-__global__ void __launch_bounds__(kReduceThreads) k_plane_sums(const Xyzz* __restrict__ run, const Xyzz* __restrict__ tot,
-                                                               uint32_t groups, int planes, Xyzz* __restrict__ plane_out) {
+// block b: plane slot b / split, part b % split of the window's groups.
+// Slot plane < planes sums R_g over the g with bit `plane` set; slot plane ==
+// planes sums T_g over all g.
+__global__ void __launch_bounds__(kReduceThreads) k_plane_sums(const Xyzz* __restrict__ run,
+                                                               const Xyzz* __restrict__ tot,
+                                                               const WinDev* __restrict__ wins, uint32_t n_wins,
+                                                               uint32_t split, Xyzz* __restrict__ partial) {
     extern __shared__ uint4 smem_raw[];
     Xyzz* sm = reinterpret_cast<Xyzz*>(smem_raw);
-    const int plane = blockIdx.x % (planes + 1);
-    const uint32_t w = blockIdx.x / (planes + 1);
-    const Xyzz* src = (plane == planes ? tot : run) + (size_t)w * groups;
+    const uint32_t slot = blockIdx.x / split, part = blockIdx.x % split;
+    const WinDev wd = wins[find_win(wins, n_wins, slot, true)];
+    const int plane = (int)(slot - wd.plane_start);
+    const uint32_t groups = wd.nb >> wd.glen_log;
+    const uint32_t chunk = (groups + split - 1) / split;
+    const uint32_t g_end = min(groups, (part + 1) * chunk);
+    const Xyzz* src = (plane == wd.planes ? tot : run) + wd.group_start;
     Xyzz acc;
     xyzz_set_inf(acc);
-    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
-        if (plane == planes || ((g >> plane) & 1u)) acc = xyzz_add(acc, load_xyzz(&src[g]));
-    }
+    for (uint32_t g = part * chunk + threadIdx.x; g < g_end; g += blockDim.x)
+        if (plane == wd.planes || ((g >> plane) & 1u)) acc = xyzz_add(acc, load_xyzz(&src[g]));
     sm[threadIdx.x] = acc;
     __syncthreads();
     for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
         if ((int)threadIdx.x < off) sm[threadIdx.x] = xyzz_add(sm[threadIdx.x], sm[threadIdx.x + off]);
         __syncthreads();
     }
-    if (threadIdx.x == 0) store_xyzz(&plane_out[blockIdx.x], sm[0]);
+    if (threadIdx.x == 0) store_xyzz(&partial[blockIdx.x], sm[0]);
 }
 
-// window sum S_w = T + kGroupLen * sum_j 2^j Q_j
-__global__ void k_window_finish(const Xyzz* __restrict__ planes_in, int planes, int windows, Xyzz* __restrict__ out) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= windows) return;
-    const Xyzz* q = planes_in + (size_t)w * (planes + 1);
+// q[slot] = sum of the slot's `split` partial plane sums
+__global__ void k_plane_merge(const Xyzz* __restrict__ partial, uint32_t slots, uint32_t split,
+                              Xyzz* __restrict__ q) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= slots) return;
+    Xyzz acc = load_xyzz(&partial[(size_t)slot * split]);
+    for (uint32_t p = 1; p < split; p++) acc = xyzz_add(acc, load_xyzz(&partial[(size_t)slot * split + p]));
+    store_xyzz(&q[slot], acc);
+}
+
+// S = T + L * sum_j 2^j Q_j, one thread per window
+__global__ void k_window_finish(const Xyzz* __restrict__ q_all, const WinDev* __restrict__ wins, uint32_t n_wins,
+                                Xyzz* __restrict__ out) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n_wins) return;
+    const WinDev wd = wins[w];
+    const Xyzz* q = q_all + wd.plane_start;
     Xyzz acc;
     xyzz_set_inf(acc);
-    for (int j = planes - 1; j >= 0; j--) {
+    for (int j = wd.planes - 1; j >= 0; j--) {
         acc = xyzz_dbl(acc);
         acc = xyzz_add(acc, load_xyzz(&q[j]));
     }
-    for (int b = 1; b < kGroupLen; b <<= 1) acc = xyzz_dbl(acc);
-    acc = xyzz_add(acc, load_xyzz(&q[planes]));
+    for (uint32_t b = 0; b < wd.glen_log; b++) acc = xyzz_dbl(acc);
+    acc = xyzz_add(acc, load_xyzz(&q[wd.planes]));
     store_xyzz(&out[w], acc);
+}
+
+// the table rows of one MSM's windows, appended to `wins`
+void append_windows(const MsmShape& sh, uint64_t key_base, std::vector<WinDev>& wins, uint64_t& groups,
+                    uint64_t& slots) {
+    for (int w = 0; w < sh.windows; w++) {
+        WinDev wd;
+        wd.key_start = (uint32_t)(key_base + (uint64_t)w * sh.nb);
+        wd.nb = sh.nb;
+        wd.group_start = (uint32_t)groups;
+        wd.plane_start = (uint32_t)slots;
+        wd.glen_log = (uint32_t)sh.glen_log;
+        wd.planes = sh.planes;
+        wins.push_back(wd);
+        groups += sh.groups;
+        slots += (uint64_t)sh.planes + 1;
+    }
+}
+
+// blocks per plane slot: enough blocks to fill the GPU, at most one per
+// kReduceThreads groups of the largest window, at most 16
+uint32_t plane_split(uint64_t slots, uint32_t max_groups, int num_sms) {
+    const uint64_t want = ((uint64_t)num_sms * 8 + slots - 1) / slots;
+    const uint64_t cap = std::max<uint64_t>(1, max_groups / kReduceThreads);
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>({want, cap, 16}));
+}
+
+// steps 1-3 on `st`.  partial holds slots * split plane partials and may be
+// q itself when split == 1; q holds slots plane sums.  Returns the launch
+// error, if any; adds the launches to *launches when given.
+cudaError_t launch_reduce(const Xyzz* buckets, const uint32_t* offsets, const WinDev* d_wins, uint32_t n_wins,
+                          uint64_t groups, uint64_t slots, uint32_t split, Xyzz* run, Xyzz* tot, Xyzz* partial,
+                          Xyzz* q, Xyzz* wsum, uint64_t* launches, cudaStream_t st) {
+    k_group_sums<<<(uint32_t)((groups + kReduceThreads - 1) / kReduceThreads), kReduceThreads, 0, st>>>(
+        buckets, offsets, d_wins, n_wins, (uint32_t)groups, run, tot);
+    k_plane_sums<<<(uint32_t)(slots * split), kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
+        run, tot, d_wins, n_wins, split, split == 1 ? q : partial);
+    uint64_t n = 3;
+    if (split > 1) {
+        k_plane_merge<<<(uint32_t)((slots + 63) / 64), 64, 0, st>>>(partial, (uint32_t)slots, split, q);
+        n++;
+    }
+    k_window_finish<<<(n_wins + 31) / 32, 32, 0, st>>>(q, d_wins, n_wins, wsum);
+    if (launches) *launches += n;
+    return cudaGetLastError();
 }
 
 Status scan_u32(Context* ctx, const uint32_t* in, uint32_t* out, uint32_t len, cudaStream_t st) {
@@ -505,7 +623,7 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
 
     void *counts, *offsets, *sorted, *buckets, *partials, *owner, *run, *tot, *planes, *wsum;
     MZK_TRY(ctx->ensure("msm_counts", ((size_t)sh.keys + 1) * 4, &counts));
-    MZK_TRY(ctx->ensure("msm_offsets", ((size_t)sh.keys + 1) * 4, &offsets));
+    MZK_TRY(ctx->ensure("msm_offsets", ((size_t)sh.keys + 2) * 4, &offsets));
     MZK_TRY(ctx->ensure("msm_sorted", entries_cap * 4, &sorted));
     MZK_TRY(ctx->ensure("msm_buckets", (size_t)sh.keys * sizeof(Xyzz), &buckets));
     MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
@@ -513,11 +631,16 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     void *long_count, *long_list;
     MZK_TRY(ctx->ensure("msm_long_count", 64, &long_count));
     MZK_TRY(ctx->ensure("msm_long_list", (size_t)acc_threads * sizeof(uint2), &long_list));
-    const size_t total_groups = (size_t)sh.groups * sh.windows;
+    std::vector<WinDev> wins;
+    uint64_t total_groups = 0, slots = 0;
+    append_windows(sh, 0, wins, total_groups, slots);
+    const uint32_t split = plane_split(slots, sh.groups, ctx->num_sms);
+    void *d_wins, *q;
+    MZK_TRY(ctx->ensure("msm_wins", wins.size() * sizeof(WinDev), &d_wins));
     MZK_TRY(ctx->ensure("msm_run", total_groups * sizeof(Xyzz), &run));
     MZK_TRY(ctx->ensure("msm_tot", total_groups * sizeof(Xyzz), &tot));
-    const size_t nplanes = (size_t)sh.windows * (sh.planes + 1);
-    MZK_TRY(ctx->ensure("msm_planes", nplanes * sizeof(Xyzz), &planes));
+    MZK_TRY(ctx->ensure("msm_planes", slots * split * sizeof(Xyzz), &planes));
+    MZK_TRY(ctx->ensure("msm_q", slots * sizeof(Xyzz), &q));
     MZK_TRY(ctx->ensure("msm_wsum", (size_t)sh.windows * sizeof(Xyzz), &wsum));
     void* host_wsum;
     MZK_TRY(ctx->ensure_pinned((size_t)sh.windows * sizeof(Xyzz) + 64, &host_wsum));
@@ -527,18 +650,20 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     const int pt_threads = 256;
     const uint32_t pt_blocks = (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)ctx->num_sms * 16);
 
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, wins.data(), wins.size() * sizeof(WinDev), cudaMemcpyHostToDevice, st));
     MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
     k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)counts);
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCAN, st));
-    MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets, sh.keys + 1, st));
+    // exclusive scan one place to the right: offsets[key + 1] = start of key
+    MZK_CUDA_CHECK(cudaMemsetAsync(offsets, 0, 4, st));
+    MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets + 1, sh.keys + 1, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
-    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
-    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (const uint32_t*)offsets,
-                                                (uint32_t*)counts, (uint32_t*)sorted);
+    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)offsets + 1,
+                                                (uint32_t*)sorted);
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     if (bases_ready) MZK_CUDA_CHECK(cudaStreamWaitEvent(st, bases_ready, 0));
@@ -559,15 +684,9 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
-    const uint32_t gblocks = (uint32_t)((total_groups + kReduceThreads - 1) / kReduceThreads);
-    k_group_sums<<<gblocks, kReduceThreads, 0, st>>>((const Xyzz*)buckets, (const uint32_t*)offsets, sh.nb, sh.groups,
-                                                    (uint32_t)total_groups, (Xyzz*)run, (Xyzz*)tot);
-    MZK_LAUNCH_CHECK(ctx);
-    k_plane_sums<<<(uint32_t)nplanes, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
-        (const Xyzz*)run, (const Xyzz*)tot, sh.groups, sh.planes, (Xyzz*)planes);
-    MZK_LAUNCH_CHECK(ctx);
-    k_window_finish<<<(sh.windows + 31) / 32, 32, 0, st>>>((const Xyzz*)planes, sh.planes, sh.windows, (Xyzz*)wsum);
-    MZK_LAUNCH_CHECK(ctx);
+    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets, (const uint32_t*)offsets, (const WinDev*)d_wins,
+                                 (uint32_t)wins.size(), total_groups, slots, split, (Xyzz*)run, (Xyzz*)tot,
+                                 (Xyzz*)planes, (Xyzz*)q, (Xyzz*)wsum, &ctx->launches, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_CUDA_CHECK(cudaMemcpyAsync(host_wsum, wsum, (size_t)sh.windows * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
     uint32_t* host_entries = reinterpret_cast<uint32_t*>(static_cast<char*>(host_wsum) + (size_t)sh.windows * sizeof(Xyzz));
@@ -613,11 +732,6 @@ struct BatchItemDev {
     uint32_t c, windows, nb, key_start;
 };
 
-struct BatchWinDev {
-    uint32_t key_start, nb, group_start, plane_block_start;
-    int planes;
-};
-
 __device__ __forceinline__ uint32_t find_item(const BatchItemDev* items, uint32_t n_items, uint32_t p) {
     uint32_t lo = 0, hi = n_items;
     while (hi - lo > 1) {
@@ -630,11 +744,10 @@ __device__ __forceinline__ uint32_t find_item(const BatchItemDev* items, uint32_
 
 template <bool kScatter>
 __global__ void k_digits_batch(const BatchItemDev* __restrict__ items, uint32_t n_items, uint32_t total_points,
-                               int max_windows, uint32_t* __restrict__ counts_or_fill,
-                               const uint32_t* __restrict__ offsets, uint32_t* __restrict__ sorted) {
+                               int max_windows, uint32_t* __restrict__ counts_or_cursor,
+                               uint32_t* __restrict__ sorted) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
-    const uint32_t lt_mask = (1u << lane) - 1u;
     for (uint32_t base = blockIdx.x * blockDim.x; base < total_points; base += stride) {
         const uint32_t p = base + threadIdx.x;
         const bool valid = p < total_points;
@@ -642,107 +755,30 @@ __global__ void k_digits_batch(const BatchItemDev* __restrict__ items, uint32_t 
         const uint32_t local = p - it.point_start;
         Fr s = valid ? fr_from_mont(load_fr(it.scalars, local)) : fr_zero();
         uint32_t carry = 0;
-        for (int w = 0; w < max_windows; w++) {
-            bool neg = false;
-            uint32_t key = kNoKey;
-            if (valid && w < (int)it.windows) {
-                key = next_digit(s, w, (int)it.c, it.nb, carry, neg);
-                if (key != kNoKey) key += it.key_start;
-            }
-            const uint32_t peers = __match_any_sync(0xffffffffu, key);
-            const int leader = __ffs(peers) - 1;
-            if (!kScatter) {
-                if (key != kNoKey && lane == leader) atomicAdd(&counts_or_fill[key], (uint32_t)__popc(peers));
-            } else {
-                uint32_t slot = 0;
-                if (key != kNoKey && lane == leader) slot = atomicAdd(&counts_or_fill[key], (uint32_t)__popc(peers));
-                slot = __shfl_sync(peers, slot, leader);
-                if (key != kNoKey) {
-                    const uint32_t pos = offsets[key] + slot + (uint32_t)__popc(peers & lt_mask);
-                    sorted[pos] = (it.base_offset + local) | (neg ? 0x80000000u : 0u);
+        for (int w0 = 0; w0 < max_windows; w0 += kScatterWindows) {
+            uint32_t key[kScatterWindows];
+            bool neg[kScatterWindows];
+#pragma unroll
+            for (int j = 0; j < kScatterWindows; j++) {
+                const int w = w0 + j;
+                key[j] = kNoKey;
+                neg[j] = false;
+                if (valid && w < (int)it.windows) {
+                    key[j] = next_digit(s, w, (int)it.c, it.nb, carry, neg[j]);
+                    if (key[j] != kNoKey) key[j] += it.key_start;
                 }
+            }
+            if (!kScatter) {
+#pragma unroll
+                for (int j = 0; j < kScatterWindows; j++) {
+                    const uint32_t peers = __match_any_sync(0xffffffffu, key[j]);
+                    if (key[j] != kNoKey && lane == __ffs(peers) - 1) atomicAdd(&counts_or_cursor[key[j]], (uint32_t)__popc(peers));
+                }
+            } else {
+                scatter_group(key, neg, it.base_offset + local, lane, counts_or_cursor, sorted);
             }
         }
     }
-}
-
-__device__ __forceinline__ uint32_t find_win_by_group(const BatchWinDev* wins, uint32_t n_wins, uint32_t g) {
-    uint32_t lo = 0, hi = n_wins;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (wins[mid].group_start <= g) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-__global__ void __launch_bounds__(kReduceThreads) k_group_sums_batch(const Xyzz* __restrict__ buckets,
-                                                                     const uint32_t* __restrict__ offsets,
-                                                                     const BatchWinDev* __restrict__ wins,
-                                                                     uint32_t n_wins, uint32_t total_groups,
-                                                                     Xyzz* __restrict__ run_out,
-                                                                     Xyzz* __restrict__ tot_out) {
-    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= total_groups) return;
-    const BatchWinDev wd = wins[find_win_by_group(wins, n_wins, gid)];
-    const uint32_t key0 = wd.key_start + (gid - wd.group_start) * kGroupLen;
-    Xyzz run, tot;
-    xyzz_set_inf(run);
-    xyzz_set_inf(tot);
-    for (int b = kGroupLen - 1; b >= 0; b--) {
-        const uint32_t key = key0 + (uint32_t)b;
-        if (offsets[key + 1] > offsets[key]) run = xyzz_add(run, load_xyzz(&buckets[key]));
-        tot = xyzz_add(tot, run);
-    }
-    store_xyzz(&run_out[gid], run);
-    store_xyzz(&tot_out[gid], tot);
-}
-
-__global__ void __launch_bounds__(kReduceThreads) k_plane_sums_batch(const Xyzz* __restrict__ run,
-                                                                     const Xyzz* __restrict__ tot,
-                                                                     const BatchWinDev* __restrict__ wins,
-                                                                     uint32_t n_wins, Xyzz* __restrict__ plane_out) {
-    extern __shared__ uint4 smem_raw[];
-    Xyzz* sm = reinterpret_cast<Xyzz*>(smem_raw);
-    // block -> (window, plane)
-    uint32_t lo = 0, hi = n_wins;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (wins[mid].plane_block_start <= blockIdx.x) lo = mid;
-        else hi = mid;
-    }
-    const BatchWinDev wd = wins[lo];
-    const int plane = (int)(blockIdx.x - wd.plane_block_start);
-    const uint32_t groups = wd.nb / kGroupLen;
-    const Xyzz* src = (plane == wd.planes ? tot : run) + wd.group_start;
-    Xyzz acc;
-    xyzz_set_inf(acc);
-    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x)
-        if (plane == wd.planes || ((g >> plane) & 1u)) acc = xyzz_add(acc, load_xyzz(&src[g]));
-    sm[threadIdx.x] = acc;
-    __syncthreads();
-    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
-        if ((int)threadIdx.x < off) sm[threadIdx.x] = xyzz_add(sm[threadIdx.x], sm[threadIdx.x + off]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) store_xyzz(&plane_out[blockIdx.x], sm[0]);
-}
-
-__global__ void k_window_finish_batch(const Xyzz* __restrict__ planes_in, const BatchWinDev* __restrict__ wins,
-                                      uint32_t n_wins, Xyzz* __restrict__ out) {
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= n_wins) return;
-    const BatchWinDev wd = wins[w];
-    const Xyzz* q = planes_in + wd.plane_block_start;
-    Xyzz acc;
-    xyzz_set_inf(acc);
-    for (int j = wd.planes - 1; j >= 0; j--) {
-        acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, load_xyzz(&q[j]));
-    }
-    for (int b = 1; b < kGroupLen; b <<= 1) acc = xyzz_dbl(acc);
-    acc = xyzz_add(acc, load_xyzz(&q[wd.planes]));
-    store_xyzz(&out[w], acc);
 }
 
 }  // namespace
@@ -751,9 +787,10 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
                            uint64_t* out, cudaStream_t st) {
     std::memset(out, 0, count * 18 * 8);
     std::vector<BatchItemDev> hi;
-    std::vector<BatchWinDev> hw;
+    std::vector<WinDev> hw;
     std::vector<size_t> item_of;  // position in `items` of every device item
-    uint64_t points = 0, keys = 0, entries = 0, groups = 0, plane_blocks = 0;
+    uint64_t points = 0, keys = 0, entries = 0, groups = 0, slots = 0;
+    uint32_t max_groups = 1;
     int max_windows = 0;
     for (size_t m = 0; m < count; m++) {
         const BatchItem& it = items[m];
@@ -777,17 +814,8 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
         d.windows = (uint32_t)sh.windows;
         d.nb = sh.nb;
         d.key_start = (uint32_t)keys;
-        for (int w = 0; w < sh.windows; w++) {
-            BatchWinDev wd;
-            wd.key_start = (uint32_t)(keys + (uint64_t)w * sh.nb);
-            wd.nb = sh.nb;
-            wd.group_start = (uint32_t)groups;
-            wd.plane_block_start = (uint32_t)plane_blocks;
-            wd.planes = sh.planes;
-            hw.push_back(wd);
-            groups += sh.groups;
-            plane_blocks += (uint64_t)sh.planes + 1;
-        }
+        append_windows(sh, keys, hw, groups, slots);
+        max_groups = std::max(max_groups, sh.groups);
         points += it.n;
         keys += sh.keys;
         entries += (uint64_t)sh.windows * it.n;
@@ -809,9 +837,9 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     void *d_items, *d_wins, *counts, *offsets, *sorted, *buckets, *partials, *owner, *long_count, *long_list, *run, *tot,
         *planes, *wsum;
     MZK_TRY(ctx->ensure("batch_items", hi.size() * sizeof(BatchItemDev), &d_items));
-    MZK_TRY(ctx->ensure("batch_wins", n_wins * sizeof(BatchWinDev), &d_wins));
+    MZK_TRY(ctx->ensure("batch_wins", n_wins * sizeof(WinDev), &d_wins));
     MZK_TRY(ctx->ensure("msm_counts", (keys + 1) * 4, &counts));
-    MZK_TRY(ctx->ensure("msm_offsets", (keys + 1) * 4, &offsets));
+    MZK_TRY(ctx->ensure("msm_offsets", (keys + 2) * 4, &offsets));
     MZK_TRY(ctx->ensure("msm_sorted", entries * 4, &sorted));
     MZK_TRY(ctx->ensure("msm_buckets", keys * sizeof(Xyzz), &buckets));
     MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
@@ -820,12 +848,15 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_TRY(ctx->ensure("msm_long_list", (size_t)acc_threads * sizeof(uint2), &long_list));
     MZK_TRY(ctx->ensure("msm_run", groups * sizeof(Xyzz), &run));
     MZK_TRY(ctx->ensure("msm_tot", groups * sizeof(Xyzz), &tot));
-    MZK_TRY(ctx->ensure("msm_planes", plane_blocks * sizeof(Xyzz), &planes));
+    const uint32_t split = plane_split(slots, max_groups, ctx->num_sms);
+    void* q;
+    MZK_TRY(ctx->ensure("msm_planes", slots * split * sizeof(Xyzz), &planes));
+    MZK_TRY(ctx->ensure("msm_q", slots * sizeof(Xyzz), &q));
     MZK_TRY(ctx->ensure("msm_wsum", n_wins * sizeof(Xyzz), &wsum));
     void* host_wsum;
     MZK_TRY(ctx->ensure_pinned(n_wins * sizeof(Xyzz) + 64, &host_wsum));
     MZK_CUDA_CHECK(cudaMemcpyAsync(d_items, hi.data(), hi.size() * sizeof(BatchItemDev), cudaMemcpyHostToDevice, st));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, hw.data(), n_wins * sizeof(BatchWinDev), cudaMemcpyHostToDevice, st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, hw.data(), n_wins * sizeof(WinDev), cudaMemcpyHostToDevice, st));
 
     const uint32_t n_items = (uint32_t)hi.size();
     const int pt_threads = 256;
@@ -834,17 +865,16 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, (keys + 1) * 4, st));
     k_digits_batch<false><<<pt_blocks, pt_threads, 0, st>>>((const BatchItemDev*)d_items, n_items, (uint32_t)points,
-                                                           max_windows, (uint32_t*)counts, nullptr, nullptr);
+                                                           max_windows, (uint32_t*)counts, nullptr);
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCAN, st));
-    MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets, (uint32_t)keys + 1, st));
+    MZK_CUDA_CHECK(cudaMemsetAsync(offsets, 0, 4, st));
+    MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets + 1, (uint32_t)keys + 1, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
-    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, (keys + 1) * 4, st));
     k_digits_batch<true><<<pt_blocks, pt_threads, 0, st>>>((const BatchItemDev*)d_items, n_items, (uint32_t)points,
-                                                          max_windows, (uint32_t*)counts, (const uint32_t*)offsets,
-                                                          (uint32_t*)sorted);
+                                                          max_windows, (uint32_t*)offsets + 1, (uint32_t*)sorted);
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
@@ -865,17 +895,9 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
-    k_group_sums_batch<<<(uint32_t)((groups + kReduceThreads - 1) / kReduceThreads), kReduceThreads, 0, st>>>(
-        (const Xyzz*)buckets, (const uint32_t*)offsets, (const BatchWinDev*)d_wins, (uint32_t)n_wins,
-        (uint32_t)groups, (Xyzz*)run, (Xyzz*)tot);
-    MZK_LAUNCH_CHECK(ctx);
-    k_plane_sums_batch<<<(uint32_t)plane_blocks, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
-        (const Xyzz*)run, (const Xyzz*)tot, (const BatchWinDev*)d_wins, (uint32_t)n_wins, (Xyzz*)planes);
-    MZK_LAUNCH_CHECK(ctx);
-    k_window_finish_batch<<<(uint32_t)((n_wins + 31) / 32), 32, 0, st>>>((const Xyzz*)planes,
-                                                                        (const BatchWinDev*)d_wins, (uint32_t)n_wins,
-                                                                        (Xyzz*)wsum);
-    MZK_LAUNCH_CHECK(ctx);
+    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets, (const uint32_t*)offsets, (const WinDev*)d_wins,
+                                 (uint32_t)n_wins, groups, slots, split, (Xyzz*)run, (Xyzz*)tot, (Xyzz*)planes,
+                                 (Xyzz*)q, (Xyzz*)wsum, &ctx->launches, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_CUDA_CHECK(cudaMemcpyAsync(host_wsum, wsum, n_wins * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
     MZK_CUDA_CHECK(cudaStreamSynchronize(st));
@@ -942,16 +964,18 @@ constexpr size_t kNaMaxWindows = 32;  // c = 8
 constexpr size_t kNaAccThreads = (size_t)kNoAllocAccBlocks * kAccThreads;
 constexpr size_t kNaCountsOff = 0;
 constexpr size_t kNaOffsetsOff = kNaCountsOff + align256((kNaKeys + 1) * 4);
-constexpr size_t kNaSortedOff = kNaOffsetsOff + align256((kNaKeys + 1) * 4);
+constexpr size_t kNaSortedOff = kNaOffsetsOff + align256((kNaKeys + 2) * 4);
 constexpr size_t kNaBucketsOff = kNaSortedOff + align256(kNaMaxWindows * kNoAllocMaxN * 4);
 constexpr size_t kNaPartialsOff = kNaBucketsOff + align256(kNaKeys * sizeof(Xyzz));
 constexpr size_t kNaOwnerOff = kNaPartialsOff + align256(kNaAccThreads * 2 * sizeof(Xyzz));
 constexpr size_t kNaRunOff = kNaOwnerOff + align256(kNaAccThreads * 4);
-constexpr size_t kNaTotOff = kNaRunOff + align256(kNaKeys / kGroupLen * sizeof(Xyzz));
-constexpr size_t kNaPlanesOff = kNaTotOff + align256(kNaKeys / kGroupLen * sizeof(Xyzz));
+// running-sum groups: kNaKeys >> kGroupLog for c >= 8
+constexpr size_t kNaTotOff = kNaRunOff + align256((kNaKeys >> kGroupLog) * sizeof(Xyzz));
+constexpr size_t kNaPlanesOff = kNaTotOff + align256((kNaKeys >> kGroupLog) * sizeof(Xyzz));
 constexpr size_t kNaWsumOff = kNaPlanesOff + align256(kNaMaxWindows * 8 * sizeof(Xyzz));
 constexpr size_t kNaScanOff = kNaWsumOff + align256(kNaMaxWindows * sizeof(Xyzz));
-constexpr size_t kNaLongOff = kNaScanOff + align256(64 * 4);
+constexpr size_t kNaWinsOff = kNaScanOff + align256(64 * 4);
+constexpr size_t kNaLongOff = kNaWinsOff + align256(kNaMaxWindows * sizeof(WinDev));
 constexpr size_t kNaBytes = kNaLongOff + align256(16 + kNaAccThreads * sizeof(uint2));
 
 // The scratch itself.  Host code must not use this name as a device address:
@@ -1029,9 +1053,9 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
     k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, counts);
     MZK_CUDA_CHECK(cudaGetLastError());
-    MZK_TRY(scan_u32_noalloc(counts, offsets, sh.keys + 1, scan_sums, st));
-    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
-    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, offsets, counts, sorted);
+    MZK_CUDA_CHECK(cudaMemsetAsync(offsets, 0, 4, st));
+    MZK_TRY(scan_u32_noalloc(counts, offsets + 1, sh.keys + 1, scan_sums, st));
+    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, offsets + 1, sorted);
     MZK_CUDA_CHECK(cudaGetLastError());
     k_accumulate<<<kNoAllocAccBlocks, kAccThreads, 0, st>>>(ba, sorted, offsets, sh.keys, buckets, partials, owner);
     MZK_CUDA_CHECK(cudaGetLastError());
@@ -1045,17 +1069,14 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
                                                                                           long_count, long_list,
                                                                                           buckets);
     MZK_CUDA_CHECK(cudaGetLastError());
-    const size_t total_groups = (size_t)sh.groups * sh.windows;
-    const uint32_t gblocks = (uint32_t)((total_groups + kReduceThreads - 1) / kReduceThreads);
-    k_group_sums<<<gblocks, kReduceThreads, 0, st>>>(buckets, offsets, sh.nb, sh.groups, (uint32_t)total_groups, run,
-                                                    tot);
-    MZK_CUDA_CHECK(cudaGetLastError());
-    const size_t nplanes = (size_t)sh.windows * (sh.planes + 1);
-    k_plane_sums<<<(uint32_t)nplanes, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(run, tot, sh.groups,
-                                                                                          sh.planes, planes);
-    MZK_CUDA_CHECK(cudaGetLastError());
-    k_window_finish<<<(sh.windows + 31) / 32, 32, 0, st>>>(planes, sh.planes, sh.windows, wsum);
-    MZK_CUDA_CHECK(cudaGetLastError());
+    // window table (a copy from pageable memory is staged before the call returns)
+    std::vector<WinDev> wins;
+    uint64_t total_groups = 0, slots = 0;
+    append_windows(sh, 0, wins, total_groups, slots);
+    WinDev* d_wins = reinterpret_cast<WinDev*>(base + kNaWinsOff);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, wins.data(), wins.size() * sizeof(WinDev), cudaMemcpyHostToDevice, st));
+    MZK_CUDA_CHECK(launch_reduce(buckets, offsets, d_wins, (uint32_t)wins.size(), total_groups, slots, 1, run, tot,
+                                 planes, planes, wsum, nullptr, st));
     // window sums to host memory owned by this function (no pinned allocation)
     host::Xyzz6 hs[kNaMaxWindows];
     MZK_CUDA_CHECK(cudaMemcpyAsync(hs, wsum, (size_t)sh.windows * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
