@@ -58,6 +58,12 @@ struct PassArgs {
     int use_pre;       // multiply input element i by pre[i % 3] (coset scaling)
     int twiddle_after; // inter-pass twiddle (all passes but the last)
     Fr pre[3];
+    // last pass only: write element idx to out[bitrev(idx)] (natural order),
+    // times post[bitrev(idx) % 3] when use_post, and only when bitrev(idx) < m_out
+    int bitrev_out;
+    int use_post;
+    uint32_t m_out;
+    Fr post[3];
 };
 
 // Shared-memory tiles hold Fr elements as two planes of 16-byte halves, so a
@@ -79,7 +85,51 @@ struct FrPlanes {
     }
 };
 
-__global__ void __launch_bounds__(kNttThreads) k_ntt_dif_pass(PassArgs a) {
+// Shared-memory slot of tile element e: the low 3 bits XORed with bits 3..5.
+// A quarter-warp's 16-byte accesses then hit 8 different 16-byte bank
+// groups for the strided patterns of the last rounds (row strides of 8, 16
+// and 32 elements) as well as for contiguous runs.
+__device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 3) & 7u); }
+
+// K consecutive DIF stages s .. s+K-1 of the tile in registers: each thread
+// takes groups of 2^K elements of one column at rows m0 + i q (q = 2^log_q,
+// the last stage's half-size), runs the K radix-2 stages on them and stores
+// them back.  Stage s+t pairs rows r and r + q 2^(K-1-t); its twiddle is
+// w_R^(pos << (s+t)) with pos = r mod (q 2^(K-t)).
+template <int K>
+__device__ __forceinline__ void dif_round(const FrPlanes& sx, const FrPlanes& sw, uint32_t s, uint32_t log_r,
+                                          uint32_t log_b, uint32_t tile) {
+    const uint32_t log_q = log_r - s - K;
+    const uint32_t B = 1u << log_b;
+    for (uint32_t g = threadIdx.x; g < (tile >> K); g += blockDim.x) {
+        const uint32_t b = g & (B - 1);
+        const uint32_t rest = g >> log_b;
+        const uint32_t j = rest & ((1u << log_q) - 1);
+        const uint32_t m0 = ((rest >> log_q) << (log_q + K)) + j;
+        Fr x[1 << K];
+#pragma unroll
+        for (int i = 0; i < (1 << K); i++) x[i] = sx.get(swz(((m0 + ((uint32_t)i << log_q)) << log_b) + b));
+#pragma unroll
+        for (int t = 0; t < K; t++) {
+            const int d = 1 << (K - 1 - t);
+#pragma unroll
+            for (int i = 0; i < (1 << K); i++) {
+                if ((i & (2 * d - 1)) < d) {
+                    const Fr x0 = x[i], x1 = x[i + d];
+                    x[i] = fr_add(x0, x1);
+                    Fr v = fr_sub(x0, x1);
+                    const uint32_t pos = j + ((uint32_t)(i & (2 * d - 1)) << log_q);
+                    if (pos) v = fr_mul(v, sw.get(pos << (s + (uint32_t)t)));
+                    x[i + d] = v;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < (1 << K); i++) sx.set(swz(((m0 + ((uint32_t)i << log_q)) << log_b) + b), x[i]);
+    }
+}
+
+__global__ void __launch_bounds__(kNttThreads, 2) k_ntt_dif_pass(PassArgs a) {
     extern __shared__ uint4 smem_raw[];
     const uint32_t N = 1u << a.log_n;
     const uint32_t R = 1u << a.log_r;
@@ -89,12 +139,17 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_dif_pass(PassArgs a) {
     const uint32_t B = 1u << log_b;
     const FrPlanes sx{smem_raw, smem_raw + tile};
     const FrPlanes sw{smem_raw + 2 * tile, smem_raw + 2 * tile + R / 2};  // w_R^u for u < R/2
-    const uint32_t c0 = blockIdx.x << log_b;
+    // columns of this block: B consecutive columns, or, in the last pass, the
+    // columns blockIdx.x + b * 2^(log_ncol - log_b), whose bit-reversed
+    // output positions are B consecutive elements (256-byte runs for B = 8)
+    const uint32_t log_ncol = a.log_n - a.log_r;
+    const uint32_t c0 = a.bitrev_out ? blockIdx.x : blockIdx.x << log_b;
+    const uint32_t cstep_log = a.bitrev_out ? log_ncol - log_b : 0u;
 
     for (uint32_t u = threadIdx.x; u < R / 2; u += blockDim.x) sw.set(u, root_pow(a.tlo, a.thi, u << (a.log_n - a.log_r)));
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         const uint32_t m = e >> log_b, b = e & (B - 1);
-        const uint32_t c = c0 + b;
+        const uint32_t c = c0 + (b << cstep_log);
         const uint32_t idx = ((c >> log_m) << a.log_s) + (m << log_m) + (c & ((1u << log_m) - 1));
         Fr v = fr_zero();
         if (idx < a.n_real) {
@@ -104,69 +159,43 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_dif_pass(PassArgs a) {
                 if (r3) v = fr_mul(v, a.pre[r3]);
             }
         }
-        sx.set(e, v);
+        sx.set(swz(e), v);
     }
     __syncthreads();
-    for (uint32_t s = 0; s < a.log_r; s++) {
-        const uint32_t log_h = a.log_r - 1 - s;
-        const uint32_t h = 1u << log_h;
-        for (uint32_t q = threadIdx.x; q < tile / 2; q += blockDim.x) {
-            const uint32_t b = q & (B - 1), p = q >> log_b;
-            const uint32_t pos = p & (h - 1);
-            const uint32_t m0 = ((p >> log_h) << (log_h + 1)) + pos;
-            const uint32_t i0 = (m0 << log_b) + b, i1 = ((m0 + h) << log_b) + b;
-            const Fr x0 = sx.get(i0), x1 = sx.get(i1);
-            sx.set(i0, fr_add(x0, x1));
-            Fr v = fr_sub(x0, x1);
-            if (pos) v = fr_mul(v, sw.get(pos << s));
-            sx.set(i1, v);
-        }
+    // stages in rounds of three (radix 8), the last round of one or two
+    for (uint32_t s = 0; s < a.log_r;) {
+        const uint32_t k = min(3u, a.log_r - s);
+        if (k == 3) dif_round<3>(sx, sw, s, a.log_r, log_b, tile);
+        else if (k == 2) dif_round<2>(sx, sw, s, a.log_r, log_b, tile);
+        else dif_round<1>(sx, sw, s, a.log_r, log_b, tile);
         __syncthreads();
+        s += k;
     }
+    // unrolled so that the twiddle-table loads of several elements are in flight
+#pragma unroll 4
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         const uint32_t m = e >> log_b, b = e & (B - 1);
-        const uint32_t c = c0 + b;
+        const uint32_t c = c0 + (b << cstep_log);
         const uint32_t j = c & ((1u << log_m) - 1);
         const uint32_t idx = ((c >> log_m) << a.log_s) + (m << log_m) + j;
-        Fr v = sx.get(e);
+        Fr v = sx.get(swz(e));
         if (a.twiddle_after && j) {
             const uint32_t k1 = __brev(m) >> (32 - a.log_r);
             const uint32_t ex = (j * k1) << (a.log_n - a.log_s);  // (N/S) j k1 < N
             v = fr_mul(v, root_pow(a.tlo, a.thi, ex & (N - 1)));
         }
-        a.out[idx] = v;
-    }
-}
-
-// in place: a[i] <-> a[bitrev(i)], each output multiplied by scale[i % 3]
-__global__ void k_bitrev_scale(Fr* __restrict__ a, uint32_t log_n, int use_scale, Fr s0, Fr s1, Fr s2) {
-    const uint32_t N = 1u << log_n;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-        const uint32_t j = log_n ? (__brev(i) >> (32 - log_n)) : 0u;
-        if (j < i) continue;
-        const Fr x = a[i];
-        const Fr y = a[j];
-        Fr oi = y, oj = x;
-        if (use_scale) {
-            const uint32_t ri = i % 3, rj = j % 3;
-            oi = fr_mul(oi, ri == 0 ? s0 : (ri == 1 ? s1 : s2));
-            oj = fr_mul(oj, rj == 0 ? s0 : (rj == 1 ? s1 : s2));
+        if (a.bitrev_out) {
+            const uint32_t o = a.log_n ? (__brev(idx) >> (32 - a.log_n)) : 0u;
+            if (o < a.m_out) {
+                if (a.use_post) {
+                    const uint32_t r = o % 3;
+                    v = fr_mul(v, a.post[r]);
+                }
+                a.out[o] = v;
+            }
+        } else {
+            a.out[idx] = v;
         }
-        a[i] = oi;
-        if (j != i) a[j] = oj;
-    }
-}
-
-// out[i] = in[bitrev(i)] * scale[i % 3] for i < m (gathers a prefix of the
-// natural-order result out of a bit-reversed vector of length 2^log_n)
-__global__ void k_bitrev_gather(const Fr* __restrict__ in, Fr* __restrict__ out, uint32_t log_n, uint32_t m, Fr s0,
-                                Fr s1, Fr s2) {
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-        const uint32_t j = log_n ? (__brev(i) >> (32 - log_n)) : 0u;
-        const uint32_t r = i % 3;
-        out[i] = fr_mul(in[j], r == 0 ? s0 : (r == 1 ? s1 : s2));
     }
 }
 
@@ -296,21 +325,34 @@ Status domain_create(Context* ctx, uint32_t j, uint32_t k, Domain** out) {
 // Forward DIF passes over 2^log_n elements with root table `root` (0..3),
 // first pass reading `in` (n_real elements, optional coset scaling) and
 // writing `out`; later passes in place on `out`.  Output bit-reversed.
+// The DIF passes of one transform, ending in natural order: the last pass
+// writes every element to its bit-reversed position (times post[i % 3] when
+// post is given, only positions < m_out).  Since that pass's writes cross
+// blocks, it reads from the scratch buffer the earlier passes wrote, so `in`
+// and `out` may be the same buffer.  A transform of one tile (log_n <= 11) is
+// one block, which reads all before it writes.
 static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n, const Fr* in, Fr* out,
-                         uint32_t n_real, bool coset, cudaStream_t st) {
+                         uint32_t n_real, bool coset, const host::Fr4* post, uint32_t m_out, cudaStream_t st) {
     const uint32_t N = 1u << log_n;
     const uint32_t tile = std::min(kTile, N);
     const uint32_t tile_log = std::min(kTileLog, log_n);
     const uint32_t passes = (log_n + tile_log - 1) / tile_log;
     MZK_CUDA_CHECK(cudaFuncSetAttribute(k_ntt_dif_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)(kTile * sizeof(Fr) + kTile / 2 * sizeof(Fr))));
+    Fr* tmp = nullptr;
+    if (passes > 1) {
+        void* p;
+        MZK_TRY(ctx->ensure("ntt_tmp", (size_t)N * sizeof(Fr), &p));
+        tmp = static_cast<Fr*>(p);
+    }
     uint32_t log_s = log_n;
     for (uint32_t p = 0; p < passes; p++) {
         const uint32_t rem = passes - p;
         const uint32_t log_r = (log_s + rem - 1) / rem;  // even split, larger passes first
+        const bool last = p + 1 == passes;
         PassArgs a;
-        a.in = p == 0 ? in : out;
-        a.out = out;
+        a.in = p == 0 ? in : tmp;
+        a.out = last ? out : tmp;
         a.tlo = d->lo[root];
         a.thi = d->hi[root];
         a.log_n = log_n;
@@ -318,10 +360,14 @@ static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n
         a.log_r = log_r;
         a.n_real = p == 0 ? n_real : N;
         a.use_pre = (p == 0 && coset) ? 1 : 0;
-        a.twiddle_after = p + 1 < passes ? 1 : 0;
+        a.twiddle_after = last ? 0 : 1;
         a.pre[0] = to_dev(host::fr_one());
         a.pre[1] = to_dev(d->zeta);
         a.pre[2] = to_dev(d->zeta2);
+        a.bitrev_out = last ? 1 : 0;
+        a.use_post = post ? 1 : 0;
+        a.m_out = m_out;
+        for (int i = 0; i < 3; i++) a.post[i] = to_dev(post ? post[i] : host::fr_one());
         const size_t smem = (size_t)tile * sizeof(Fr) + (size_t)(1u << log_r) / 2 * sizeof(Fr);
         k_ntt_dif_pass<<<N / tile, kNttThreads, smem, st>>>(a);
         MZK_LAUNCH_CHECK(ctx);
@@ -330,13 +376,6 @@ static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n
     return OK;
 }
 
-static Status bitrev(Context* ctx, Fr* a, uint32_t log_n, bool scale, const host::Fr4& s0, const host::Fr4& s1,
-                     const host::Fr4& s2, cudaStream_t st) {
-    const uint32_t N = 1u << log_n;
-    k_bitrev_scale<<<grid_for(ctx, N, 256), 256, 0, st>>>(a, log_n, scale ? 1 : 0, to_dev(s0), to_dev(s1), to_dev(s2));
-    MZK_LAUNCH_CHECK(ctx);
-    return OK;
-}
 
 Status domain_op_device(Context* ctx, const Domain* d, int op, const void* d_in, void* d_out, cudaStream_t st) {
     const uint32_t k = d->k, ek = d->ext_k;
@@ -346,28 +385,23 @@ Status domain_op_device(Context* ctx, const Domain* d, int op, const void* d_in,
     const Fr* in = static_cast<const Fr*>(d_in);
     switch (op) {
         case OP_COEFF_TO_LAGRANGE:  // best_fft(a, omega)
-            MZK_TRY(dif_passes(ctx, d, 0, k, in, out, n, false, st));
-            return bitrev(ctx, out, k, false, one, one, one, st);
-        case OP_LAGRANGE_TO_COEFF:  // ifft: best_fft(a, omega_inv), * n^-1
-            MZK_TRY(dif_passes(ctx, d, 1, k, in, out, n, false, st));
-            return bitrev(ctx, out, k, true, d->ifft_div, d->ifft_div, d->ifft_div, st);
-        case OP_COEFF_TO_EXTENDED:  // zeta^(i mod 3) scaling, pad to 2^ext_k, fft(ext_omega)
-            MZK_TRY(dif_passes(ctx, d, 2, ek, in, out, n, true, st));
-            return bitrev(ctx, out, ek, false, one, one, one, st);
-        case OP_EXTENDED_TO_COEFF: {  // ifft(ext_omega_inv), * (2^ext_k)^-1, zeta unscaling
-            MZK_TRY(dif_passes(ctx, d, 3, ek, in, out, en, false, st));
-            const host::Fr4 s1 = host::fr_mul(d->ext_ifft_div, d->zeta2), s2 = host::fr_mul(d->ext_ifft_div, d->zeta);
-            return bitrev(ctx, out, ek, true, d->ext_ifft_div, s1, s2, st);
+            return dif_passes(ctx, d, 0, k, in, out, n, false, nullptr, n, st);
+        case OP_LAGRANGE_TO_COEFF: {  // ifft: best_fft(a, omega_inv), * n^-1
+            const host::Fr4 post[3] = {d->ifft_div, d->ifft_div, d->ifft_div};
+            return dif_passes(ctx, d, 1, k, in, out, n, false, post, n, st);
         }
-        case OP_EXTENDED_TO_LAGRANGE: {  // in (2^ext_k, consumed) -> out (n)
-            Fr* work = const_cast<Fr*>(in);
-            MZK_TRY(dif_passes(ctx, d, 3, ek, in, work, en, false, st));
-            const host::Fr4 s1 = host::fr_mul(d->ext_ifft_div, d->zeta2), s2 = host::fr_mul(d->ext_ifft_div, d->zeta);
-            k_bitrev_gather<<<grid_for(ctx, n, 256), 256, 0, st>>>(work, out, ek, n, to_dev(d->ext_ifft_div), to_dev(s1),
-                                                                 to_dev(s2));
-            MZK_LAUNCH_CHECK(ctx);
-            MZK_TRY(dif_passes(ctx, d, 0, k, out, out, n, false, st));
-            return bitrev(ctx, out, k, false, one, one, one, st);
+        case OP_COEFF_TO_EXTENDED:  // zeta^(i mod 3) scaling, pad to 2^ext_k, fft(ext_omega)
+            return dif_passes(ctx, d, 2, ek, in, out, n, true, nullptr, en, st);
+        case OP_EXTENDED_TO_COEFF: {  // ifft(ext_omega_inv), * (2^ext_k)^-1, zeta unscaling
+            const host::Fr4 post[3] = {d->ext_ifft_div, host::fr_mul(d->ext_ifft_div, d->zeta2),
+                                       host::fr_mul(d->ext_ifft_div, d->zeta)};
+            return dif_passes(ctx, d, 3, ek, in, out, en, false, post, en, st);
+        }
+        case OP_EXTENDED_TO_LAGRANGE: {  // in (2^ext_k) -> out (n): E2C truncated to n, then C2L
+            const host::Fr4 post[3] = {d->ext_ifft_div, host::fr_mul(d->ext_ifft_div, d->zeta2),
+                                       host::fr_mul(d->ext_ifft_div, d->zeta)};
+            MZK_TRY(dif_passes(ctx, d, 3, ek, in, out, en, false, post, n, st));
+            return dif_passes(ctx, d, 0, k, out, out, n, false, nullptr, n, st);
         }
         case OP_DIVIDE_BY_VANISHING: {
             if (in != out) MZK_CUDA_CHECK(cudaMemcpyAsync(out, in, (size_t)en * sizeof(Fr), cudaMemcpyDeviceToDevice, st));
