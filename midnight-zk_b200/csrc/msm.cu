@@ -47,7 +47,7 @@ namespace mzk {
 
 namespace {
 
-constexpr int kGroupLog = 5;       // log2 of the buckets per running-sum group (fewer when nb is smaller)
+constexpr int kGroupLog = 6;       // log2 of the buckets per running-sum group (fewer when nb is smaller)
 constexpr int kAccThreads = 128;   // threads per block of the accumulate kernel
 constexpr int kReduceThreads = 128;
 constexpr uint32_t kNoKey = 0xffffffffu;
@@ -62,17 +62,28 @@ struct MsmShape {
     int planes;     // log2(groups)
 };
 
-MsmShape make_shape(int c) {
+// glen_log: log2 of the buckets per running-sum group, at most c - 1
+MsmShape make_shape(int c, int glen_log = kGroupLog) {
     MsmShape s;
     s.c = c;
     s.windows = (256 + c - 1) / c;
     s.nb = 1u << (c - 1);
     s.keys = s.nb * (uint32_t)s.windows;
-    s.glen_log = c - 1 < kGroupLog ? c - 1 : kGroupLog;
+    s.glen_log = c - 1 < glen_log ? c - 1 : glen_log;
     s.groups = s.nb >> s.glen_log;
     s.planes = 0;
     while ((1u << s.planes) < s.groups) s.planes++;
     return s;
+}
+
+// Running-sum group length for a call whose windows hold `keys` buckets in
+// all: long groups (fewer plane sums) while there are still >= 32768 groups
+// to fill the GPU, shorter ones for small MSMs, whose group chains would
+// otherwise be latency-bound (a group is one thread's chain of 2L additions).
+int group_log_for(uint64_t keys) {
+    int g = 2;
+    while (g < kGroupLog && (keys >> (g + 1)) >= 32768) g++;
+    return g;
 }
 
 __device__ __forceinline__ uint32_t fr_limb(const Fr& s, int i) {
@@ -608,7 +619,7 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
         set_error("msm: window width must be in [5, 24]");
         return ERR_ARG;
     }
-    const MsmShape sh = make_shape(c);
+    const MsmShape sh = make_shape(c, group_log_for(make_shape(c).keys));
     const size_t entries_cap = (size_t)sh.windows * n;
     if (entries_cap >= 0xffffffffull) {
         set_error("msm: n * windows exceeds 2^32 entries");
@@ -642,15 +653,20 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     MZK_TRY(ctx->ensure("msm_planes", slots * split * sizeof(Xyzz), &planes));
     MZK_TRY(ctx->ensure("msm_q", slots * sizeof(Xyzz), &q));
     MZK_TRY(ctx->ensure("msm_wsum", (size_t)sh.windows * sizeof(Xyzz), &wsum));
+    // pinned staging: window sums and the entry count (read back), then the
+    // window table (uploaded without the sync a pageable copy implies)
     void* host_wsum;
-    MZK_TRY(ctx->ensure_pinned((size_t)sh.windows * sizeof(Xyzz) + 64, &host_wsum));
+    const size_t tab_off = (size_t)sh.windows * sizeof(Xyzz) + 64;
+    MZK_TRY(ctx->ensure_pinned(tab_off + wins.size() * sizeof(WinDev), &host_wsum));
+    WinDev* host_tab = reinterpret_cast<WinDev*>(static_cast<char*>(host_wsum) + tab_off);
+    std::memcpy(host_tab, wins.data(), wins.size() * sizeof(WinDev));
 
     const Fr* sc = static_cast<const Fr*>(d_scalars);
     const Affine* ba = static_cast<const Affine*>(d_bases);
     const int pt_threads = 256;
     const uint32_t pt_blocks = (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)ctx->num_sms * 16);
 
-    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, wins.data(), wins.size() * sizeof(WinDev), cudaMemcpyHostToDevice, st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, host_tab, wins.size() * sizeof(WinDev), cudaMemcpyHostToDevice, st));
     MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
     k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)counts);
@@ -792,6 +808,13 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     uint64_t points = 0, keys = 0, entries = 0, groups = 0, slots = 0;
     uint32_t max_groups = 1;
     int max_windows = 0;
+    // the group length follows the buckets of the whole batch
+    uint64_t all_keys = 0;
+    for (size_t m = 0; m < count; m++)
+        if (items[m].n)
+            all_keys += make_shape(ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(items[m].n))
+                            .keys;
+    const int glen_log = group_log_for(all_keys);
     for (size_t m = 0; m < count; m++) {
         const BatchItem& it = items[m];
         if (it.n == 0) continue;
@@ -804,7 +827,7 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
             return ERR_ARG;
         }
         const int c = ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(it.n);
-        const MsmShape sh = make_shape(c);
+        const MsmShape sh = make_shape(c, glen_log);
         BatchItemDev d;
         d.scalars = static_cast<const Fr*>(it.d_scalars);
         d.n = (uint32_t)it.n;
@@ -853,10 +876,17 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_TRY(ctx->ensure("msm_planes", slots * split * sizeof(Xyzz), &planes));
     MZK_TRY(ctx->ensure("msm_q", slots * sizeof(Xyzz), &q));
     MZK_TRY(ctx->ensure("msm_wsum", n_wins * sizeof(Xyzz), &wsum));
+    // pinned staging: window sums (read back), then the item and window tables
     void* host_wsum;
-    MZK_TRY(ctx->ensure_pinned(n_wins * sizeof(Xyzz) + 64, &host_wsum));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(d_items, hi.data(), hi.size() * sizeof(BatchItemDev), cudaMemcpyHostToDevice, st));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, hw.data(), n_wins * sizeof(WinDev), cudaMemcpyHostToDevice, st));
+    const size_t items_off = n_wins * sizeof(Xyzz) + 64;
+    const size_t wins_off = items_off + ((hi.size() * sizeof(BatchItemDev) + 255) & ~(size_t)255);
+    MZK_TRY(ctx->ensure_pinned(wins_off + n_wins * sizeof(WinDev), &host_wsum));
+    char* staging = static_cast<char*>(host_wsum);
+    std::memcpy(staging + items_off, hi.data(), hi.size() * sizeof(BatchItemDev));
+    std::memcpy(staging + wins_off, hw.data(), n_wins * sizeof(WinDev));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_items, staging + items_off, hi.size() * sizeof(BatchItemDev),
+                                   cudaMemcpyHostToDevice, st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, staging + wins_off, n_wins * sizeof(WinDev), cudaMemcpyHostToDevice, st));
 
     const uint32_t n_items = (uint32_t)hi.size();
     const int pt_threads = 256;
@@ -969,9 +999,10 @@ constexpr size_t kNaBucketsOff = kNaSortedOff + align256(kNaMaxWindows * kNoAllo
 constexpr size_t kNaPartialsOff = kNaBucketsOff + align256(kNaKeys * sizeof(Xyzz));
 constexpr size_t kNaOwnerOff = kNaPartialsOff + align256(kNaAccThreads * 2 * sizeof(Xyzz));
 constexpr size_t kNaRunOff = kNaOwnerOff + align256(kNaAccThreads * 4);
-// running-sum groups: kNaKeys >> kGroupLog for c >= 8
-constexpr size_t kNaTotOff = kNaRunOff + align256((kNaKeys >> kGroupLog) * sizeof(Xyzz));
-constexpr size_t kNaPlanesOff = kNaTotOff + align256((kNaKeys >> kGroupLog) * sizeof(Xyzz));
+// running-sum groups of 2^kNoAllocGroupLog buckets (c >= 8)
+constexpr int kNoAllocGroupLog = 4;
+constexpr size_t kNaTotOff = kNaRunOff + align256((kNaKeys >> kNoAllocGroupLog) * sizeof(Xyzz));
+constexpr size_t kNaPlanesOff = kNaTotOff + align256((kNaKeys >> kNoAllocGroupLog) * sizeof(Xyzz));
 constexpr size_t kNaWsumOff = kNaPlanesOff + align256(kNaMaxWindows * 8 * sizeof(Xyzz));
 constexpr size_t kNaScanOff = kNaWsumOff + align256(kNaMaxWindows * sizeof(Xyzz));
 constexpr size_t kNaWinsOff = kNaScanOff + align256(64 * 4);
@@ -1031,7 +1062,7 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
     unsigned char* base = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
     int c = msm_pick_window(n);
     c = c < kNoAllocMinC ? kNoAllocMinC : (c > kNoAllocMaxC ? kNoAllocMaxC : c);
-    const MsmShape sh = make_shape(c);
+    const MsmShape sh = make_shape(c, kNoAllocGroupLog);
     uint32_t* counts = reinterpret_cast<uint32_t*>(base + kNaCountsOff);
     uint32_t* offsets = reinterpret_cast<uint32_t*>(base + kNaOffsetsOff);
     uint32_t* sorted = reinterpret_cast<uint32_t*>(base + kNaSortedOff);

@@ -91,6 +91,12 @@ struct FrPlanes {
 // and 32 elements) as well as for contiguous runs.
 __device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 3) & 7u); }
 
+// Shared-memory slot of twiddle w_R^u (u < 1024): the low 3 bits XORed with
+// the XOR of the 3-bit chunks above them.  A stage reads u = j << sigma for
+// consecutive j (sigma = 0..9); for every sigma the 8 lanes of a
+// quarter-warp then land in 8 different 16-byte bank groups.
+__device__ __forceinline__ uint32_t tw_swz(uint32_t u) { return u ^ (((u >> 3) ^ (u >> 6) ^ (u >> 9)) & 7u); }
+
 // K consecutive DIF stages s .. s+K-1 of the tile in registers: each thread
 // takes groups of 2^K elements of one column at rows m0 + i q (q = 2^log_q,
 // the last stage's half-size), runs the K radix-2 stages on them and stores
@@ -119,7 +125,7 @@ __device__ __forceinline__ void dif_round(const FrPlanes& sx, const FrPlanes& sw
                     x[i] = fr_add(x0, x1);
                     Fr v = fr_sub(x0, x1);
                     const uint32_t pos = j + ((uint32_t)(i & (2 * d - 1)) << log_q);
-                    if (pos) v = fr_mul(v, sw.get(pos << (s + (uint32_t)t)));
+                    if (pos) v = fr_mul(v, sw.get(tw_swz(pos << (s + (uint32_t)t))));
                     x[i + d] = v;
                 }
             }
@@ -146,7 +152,8 @@ __global__ void __launch_bounds__(kNttThreads, 2) k_ntt_dif_pass(PassArgs a) {
     const uint32_t c0 = a.bitrev_out ? blockIdx.x : blockIdx.x << log_b;
     const uint32_t cstep_log = a.bitrev_out ? log_ncol - log_b : 0u;
 
-    for (uint32_t u = threadIdx.x; u < R / 2; u += blockDim.x) sw.set(u, root_pow(a.tlo, a.thi, u << (a.log_n - a.log_r)));
+    for (uint32_t u = threadIdx.x; u < R / 2; u += blockDim.x)
+        sw.set(tw_swz(u), root_pow(a.tlo, a.thi, u << (a.log_n - a.log_r)));
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         const uint32_t m = e >> log_b, b = e & (B - 1);
         const uint32_t c = c0 + (b << cstep_log);
