@@ -212,6 +212,54 @@ typedef struct {
 int mzk_prove_core_device(mzk_ctx *ctx, mzk_domain *d, const mzk_proving_key_desc *pk, const mzk_proof_job *jobs,
                           size_t count, uint32_t flags, uint64_t *out);
 
+/* ---- column scans: grand products, running sums, evaluations ------------- */
+/* All arrays are DEVICE arrays of Fr (4 x u64 Montgomery) unless marked host. */
+
+/* ff 0.13 BatchInvert (used by permutation/prover.rs:139, logup/prover.rs:221,
+ * 232): every non-zero element of a[0..n) replaced by its inverse, zeros kept. */
+int mzk_batch_invert_device(mzk_ctx *ctx, uint64_t *a, size_t n);
+/* eval_polynomial (proofs/src/utils/arithmetic.rs:59-87): out (host) =
+ * sum_i poly[i] point^i. */
+int mzk_eval_polynomial_device(mzk_ctx *ctx, const uint64_t *poly, size_t n, const uint64_t point[4],
+                               uint64_t out[4]);
+/* kate_division (utils/arithmetic.rs:106-125): q[0..n-1) = a(X) / (X - b). */
+int mzk_kate_division_device(mzk_ctx *ctx, const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q);
+
+/* Permutation argument, permutation/prover.rs:81-255: the z polynomial of each
+ * set of chunk_len columns (Lagrange form, n = 2^k values each), blinding rows
+ * from blinds (host, n_sets x blinding_factors Fr), sets chained as in the
+ * reference.  values[j], sigmas[j]: column j and its permutation polynomial. */
+typedef struct {
+    uint32_t n_cols;
+    const uint64_t *const *values;  /* n_cols device arrays */
+    const uint64_t *const *sigmas;  /* n_cols device arrays */
+    uint32_t chunk_len;             /* cs.degree() - 2, at most 8 */
+    uint32_t blinding_factors;
+    const uint64_t *blinds;         /* host */
+    uint64_t beta[4], gamma[4];
+    uint64_t *const *z_out;         /* ceil(n_cols / chunk_len) device arrays */
+} mzk_permutation_desc;
+int mzk_permutation_z_device(mzk_ctx *ctx, mzk_domain *d, const mzk_permutation_desc *desc);
+
+/* Logup argument, logup/prover.rs:195-300: helper h_c = sum over the chunk's
+ * compressed input columns of 1/(f + beta), and the aggregator (running sum of
+ * selector * sum_c h_c - m / (t + beta), n - blinding_factors rows, then the
+ * blinding values). */
+typedef struct {
+    uint32_t n_chunks;               /* at most 8 */
+    const uint32_t *chunk_cols;      /* host: columns per chunk */
+    const uint64_t *const *inputs;   /* compressed input columns, chunk by chunk */
+    const uint64_t *table;           /* compressed table expression */
+    const uint64_t *selector;
+    const uint64_t *multiplicities;
+    uint32_t blinding_factors;
+    const uint64_t *blinds;          /* host, blinding_factors Fr */
+    uint64_t beta[4];
+    uint64_t *const *helpers_out;    /* n_chunks device arrays */
+    uint64_t *aggregator_out;
+} mzk_logup_desc;
+int mzk_logup_device(mzk_ctx *ctx, mzk_domain *d, const mzk_logup_desc *desc);
+
 /* ---- proving service (continuous batching over the proof core) ---------- */
 /* No reference counterpart: the reference proves one call at a time.
  * `lanes` worker threads (1..8), each with its own device context, serve one

@@ -67,6 +67,11 @@ SIGNATURES = {
     "mzk_quotient_eval_device": (_i32, [_vp, _vp, ctypes.c_void_p, _i32, _vp]),
     "mzk_compute_h_poly_device": (_i32, [_vp, _vp, ctypes.c_void_p, _vp, _sz, _u64p, _u64p, _vp]),
     "mzk_prove_core_device": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u32, _u64p]),
+    "mzk_batch_invert_device": (_i32, [_vp, ctypes.c_void_p, _sz]),
+    "mzk_eval_polynomial_device": (_i32, [_vp, ctypes.c_void_p, _sz, _u64p, _u64p]),
+    "mzk_kate_division_device": (_i32, [_vp, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p]),
+    "mzk_permutation_z_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
+    "mzk_logup_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_create": (_i32, [_vp, _u32, _u32, _u64, _u32, ctypes.POINTER(_vp)]),
     "mzk_server_add_key": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_submit": (_i32, [_vp, _u32, ctypes.c_void_p, _u64p]),
@@ -239,6 +244,29 @@ class DeviceBuffer:
         return out
 
 
+class PermutationDesc(ctypes.Structure):
+    """mzk_permutation_desc (include/mzk.h)."""
+    _fields_ = [("n_cols", ctypes.c_uint32), ("values", ctypes.c_void_p), ("sigmas", ctypes.c_void_p),
+                ("chunk_len", ctypes.c_uint32), ("blinding_factors", ctypes.c_uint32), ("blinds", ctypes.c_void_p),
+                ("beta", ctypes.c_uint64 * 4), ("gamma", ctypes.c_uint64 * 4), ("z_out", ctypes.c_void_p)]
+
+
+class LogupDesc(ctypes.Structure):
+    """mzk_logup_desc (include/mzk.h)."""
+    _fields_ = [("n_chunks", ctypes.c_uint32), ("chunk_cols", ctypes.c_void_p), ("inputs", ctypes.c_void_p),
+                ("table", ctypes.c_void_p), ("selector", ctypes.c_void_p), ("multiplicities", ctypes.c_void_p),
+                ("blinding_factors", ctypes.c_uint32), ("blinds", ctypes.c_void_p), ("beta", ctypes.c_uint64 * 4),
+                ("helpers_out", ctypes.c_void_p), ("aggregator_out", ctypes.c_void_p)]
+
+
+def _dptr(x):
+    return x.ptr if isinstance(x, DeviceBuffer) else int(x)
+
+
+def _ptrs(xs):
+    return (ctypes.c_void_p * max(1, len(xs)))(*[_dptr(x) for x in xs])
+
+
 class Context:
     """One device context (streams, scratch arena) on GPU `device`."""
 
@@ -350,6 +378,21 @@ class Context:
         _check(lib().mzk_msm_g1_batch_device(self.h, db, int(bases_len), ctypes.addressof(arr), len(items), _ptr(out)))
         return out[:len(items)]
 
+    # ---- column scans ----
+    def batch_invert_device(self, buf, n):
+        """ff BatchInvert in place on n device Fr (zeros stay zero)."""
+        _check(lib().mzk_batch_invert_device(self.h, _dptr(buf), int(n)))
+
+    def eval_polynomial_device(self, buf, n, point):
+        out = np.zeros(4, np.uint64)
+        _check(lib().mzk_eval_polynomial_device(self.h, _dptr(buf), int(n), _ptr(np.ascontiguousarray(point, np.uint64)),
+                                                _ptr(out)))
+        return out
+
+    def kate_division_device(self, a, n, b, q):
+        _check(lib().mzk_kate_division_device(self.h, _dptr(a), int(n), _ptr(np.ascontiguousarray(b, np.uint64)),
+                                              _dptr(q)))
+
     # ---- synthetic inputs ----
     def gen_rand_fr(self, seed, n, first=0, out=None):
         buf = out or self.alloc(n * 32)
@@ -458,6 +501,37 @@ class EvaluationDomain:
         _check(lib().mzk_prove_core_device(self.ctx.h, self.h, ctypes.byref(pk_desc), ctypes.addressof(arr),
                                            len(jobs), PROVE_MSM_PER_CALL if per_call else 0, _ptr(out)))
         return out[:len(jobs)]
+
+    def permutation_z_device(self, values, sigmas, chunk_len, blinding_factors, blinds, beta, gamma, z_out):
+        """z of every permutation set (permutation/prover.rs:81-255) into the
+        device buffers z_out; blinds: host (n_sets, blinding_factors, 4)."""
+        d = PermutationDesc()
+        vp, sp, zp = _ptrs(values), _ptrs(sigmas), _ptrs(z_out)
+        bl = np.ascontiguousarray(blinds, np.uint64).reshape(-1)
+        d.n_cols, d.values, d.sigmas = len(values), ctypes.addressof(vp), ctypes.addressof(sp)
+        d.chunk_len, d.blinding_factors = chunk_len, blinding_factors
+        d.blinds = bl.ctypes.data if bl.size else None
+        d.beta[:] = [int(v) for v in beta]
+        d.gamma[:] = [int(v) for v in gamma]
+        d.z_out = ctypes.addressof(zp)
+        _check(lib().mzk_permutation_z_device(self.ctx.h, self.h, ctypes.byref(d)))
+
+    def logup_device(self, chunks, table, selector, multiplicities, blinding_factors, blinds, beta, helpers_out,
+                     aggregator_out):
+        """helpers and aggregator of one logup argument (logup/prover.rs:195-300);
+        chunks: list of lists of device columns; blinds: host (blinding_factors, 4)."""
+        d = LogupDesc()
+        cols = [c for ch in chunks for c in ch]
+        counts = (ctypes.c_uint32 * max(1, len(chunks)))(*[len(ch) for ch in chunks])
+        ip, hp = _ptrs(cols), _ptrs(helpers_out)
+        bl = np.ascontiguousarray(blinds, np.uint64).reshape(-1)
+        d.n_chunks, d.chunk_cols, d.inputs = len(chunks), ctypes.addressof(counts), ctypes.addressof(ip)
+        d.table, d.selector, d.multiplicities = _dptr(table), _dptr(selector), _dptr(multiplicities)
+        d.blinding_factors = blinding_factors
+        d.blinds = bl.ctypes.data if bl.size else None
+        d.beta[:] = [int(v) for v in beta]
+        d.helpers_out, d.aggregator_out = ctypes.addressof(hp), _dptr(aggregator_out)
+        _check(lib().mzk_logup_device(self.ctx.h, self.h, ctypes.byref(d)))
 
     def op_device(self, name, d_in, d_out):
         """Operation on device buffers (pointers or DeviceBuffers)."""

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "../../include/mzk.h"
+#include "grand.hpp"
 #include "ntt.hpp"
 #include "quotient.hpp"
 #include "runtime.hpp"
@@ -475,6 +476,49 @@ int mzk_compute_h_poly_device(mzk_ctx* ctx, mzk_domain* d, const mzk_quotient_de
     Guard g(ctx);
     return mzk::compute_h_poly_device(&ctx->impl, d->impl, desc, d_srs_g, srs_len, blinds, out_commitments,
                                       d_limbs_out, ctx->impl.stream);
+}
+
+int mzk_batch_invert_device(mzk_ctx* ctx, uint64_t* a, size_t n) {
+    if (int s = check_ctx(ctx)) return s;
+    if (n && !a) return mzk::ERR_ARG;
+    Guard g(ctx);
+    MZK_TRY(mzk::batch_invert_device(&ctx->impl, a, n, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_eval_polynomial_device(mzk_ctx* ctx, const uint64_t* poly, size_t n, const uint64_t point[4], uint64_t out[4]) {
+    if (int s = check_ctx(ctx)) return s;
+    if ((n && !poly) || !point || !out) return mzk::ERR_ARG;
+    Guard g(ctx);
+    return mzk::eval_polynomial_device(&ctx->impl, poly, n, point, out, ctx->impl.stream);
+}
+
+int mzk_kate_division_device(mzk_ctx* ctx, const uint64_t* a, size_t n, const uint64_t b[4], uint64_t* q) {
+    if (int s = check_ctx(ctx)) return s;
+    if ((n > 1 && (!a || !q)) || !b) return mzk::ERR_ARG;
+    Guard g(ctx);
+    MZK_TRY(mzk::kate_division_device(&ctx->impl, a, n, b, q, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_permutation_z_device(mzk_ctx* ctx, mzk_domain* d, const mzk_permutation_desc* desc) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || !desc) return mzk::ERR_ARG;
+    Guard g(ctx);
+    MZK_TRY(mzk::permutation_z_device(&ctx->impl, d->impl, desc, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_logup_device(mzk_ctx* ctx, mzk_domain* d, const mzk_logup_desc* desc) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || !desc) return mzk::ERR_ARG;
+    Guard g(ctx);
+    MZK_TRY(mzk::logup_device(&ctx->impl, d->impl, desc, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
 }
 
 int mzk_prove_core_device(mzk_ctx* ctx, mzk_domain* d, const mzk_proving_key_desc* pk, const mzk_proof_job* jobs,

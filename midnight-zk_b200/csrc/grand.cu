@@ -1,0 +1,466 @@
+// grand.cu — the prover stages around the commitments that are scans over a
+// column rather than MSMs or NTTs:
+//
+//   * batch inversion with ff 0.13 BatchInvert semantics (zeros stay zero),
+//     used by both arguments below;
+//   * the permutation argument's grand products z of every set
+//     (proofs/src/plonk/permutation/prover.rs:81-255);
+//   * the logup argument's helper polynomials and running-sum aggregator
+//     (proofs/src/plonk/logup/prover.rs:195-300);
+//   * eval_polynomial (proofs/src/utils/arithmetic.rs:59-87) and
+//     kate_division (arithmetic.rs:106-125), both first-order linear
+//     recurrences y_i = c_i + k y_{i+1} solved by one chunked primitive.
+//
+// Every result is an exact field value, so the parallel orders here give the
+// reference's bytes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mzk.h"
+#include "field.cuh"
+#include "host_ec.hpp"
+#include "grand.hpp"
+#include "ntt.hpp"
+#include "runtime.hpp"
+
+namespace mzk {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kInvChunk = 64;  // elements per thread of a batch inversion
+constexpr uint32_t kRecChunk = 64;  // elements per thread of a linear recurrence
+constexpr uint32_t kScanItems = 8;  // elements per thread of a block scan
+constexpr uint32_t kMaxPermSetCols = 8;
+constexpr uint32_t kMaxLogupChunks = 8;
+// DELTA (GENERATOR^(2^S)), curves/src/bls12_381/fq.rs:501-508
+const uint64_t kDeltaU64[4] = {0x70e310d3d146f96aULL, 0x4b64c08919e299e6ULL, 0x51e114186a8b970dULL,
+                               0x6185d06627c067cbULL};
+
+__device__ __forceinline__ bool fr_is_zero(const Fr& a) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc |= a.l[j];
+    return acc == 0;
+}
+
+// a^(r-2) (Fermat); r = 1 mod 2^32, so r - 2 has limbs (2^32 - 1, r_1 - 1, r_2..r_7)
+static_assert(FrP::mod(0) == 1u, "Fr modulus limb 0 is 1");
+__device__ __noinline__ Fr fr_inv(const Fr& a) {
+    Fr acc = fr_one();
+    for (int limb = 7; limb >= 0; limb--) {
+        const uint32_t e = limb == 0 ? 0xffffffffu : (limb == 1 ? FrP::mod(1) - 1u : FrP::mod(limb));
+        for (int bit = 31; bit >= 0; bit--) {
+            acc = fr_mul(acc, acc);
+            if ((e >> bit) & 1u) acc = fr_mul(acc, a);
+        }
+    }
+    return acc;
+}
+
+Fr to_dev(const host::Fr4& h) {
+    Fr r;
+    std::memcpy(r.l, h.l, 32);
+    return r;
+}
+host::Fr4 to_host(const uint64_t* p) {
+    host::Fr4 r;
+    std::memcpy(r.l, p, 32);
+    return r;
+}
+
+uint32_t grid_for(const Context* ctx, uint64_t items, uint32_t threads) {
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((items + threads - 1) / threads, (uint64_t)ctx->num_sms * 16));
+}
+
+// ---- batch inversion: thread t takes the elements t, t + T, t + 2T, ... (T
+// threads), Montgomery's trick over them with one Fermat inversion.  Loads
+// and stores are coalesced; pre holds the forward prefix products.
+__global__ void __launch_bounds__(kThreads) k_batch_invert(Fr* __restrict__ a, Fr* __restrict__ pre, uint64_t n) {
+    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    Fr acc = fr_one();
+    for (uint64_t i = t; i < n; i += T) {
+        pre[i] = acc;
+        const Fr v = a[i];
+        if (!fr_is_zero(v)) acc = fr_mul(acc, v);
+    }
+    acc = fr_inv(acc);
+    const uint64_t last = t + ((n - 1 - t) / T) * T;
+    for (uint64_t i = last;; i -= T) {
+        const Fr v = a[i];
+        if (!fr_is_zero(v)) {
+            a[i] = fr_mul(pre[i], acc);
+            acc = fr_mul(acc, v);
+        }
+        if (i < T) break;
+    }
+}
+
+Status batch_invert(Context* ctx, Fr* a, uint64_t n, cudaStream_t st) {
+    if (n == 0) return OK;
+    void* pre;
+    MZK_TRY(ctx->ensure("grand_pre", n * sizeof(Fr), &pre));
+    const uint64_t threads = std::max<uint64_t>(1, (n + kInvChunk - 1) / kInvChunk);
+    k_batch_invert<<<(uint32_t)((threads + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, (Fr*)pre, n);
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+// ---- exclusive scans (product or sum) of Fr values ----
+template <bool kMul>
+__device__ __forceinline__ Fr op(const Fr& a, const Fr& b) {
+    return kMul ? fr_mul(a, b) : fr_add(a, b);
+}
+template <bool kMul>
+__device__ __forceinline__ Fr identity() {
+    return kMul ? fr_one() : fr_zero();
+}
+
+// block-wide exclusive scan of one value per thread (Hillis-Steele in shared
+// memory); returns the exclusive prefix, *total the block's total
+template <bool kMul>
+__device__ Fr block_exclusive(Fr v, Fr* sm, Fr* total) {
+    sm[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+        Fr o = identity<kMul>();
+        if (threadIdx.x >= off) o = sm[threadIdx.x - off];
+        __syncthreads();
+        if (threadIdx.x >= off) sm[threadIdx.x] = op<kMul>(o, sm[threadIdx.x]);
+        __syncthreads();
+    }
+    *total = sm[blockDim.x - 1];
+    const Fr ex = threadIdx.x ? sm[threadIdx.x - 1] : identity<kMul>();
+    __syncthreads();
+    return ex;
+}
+
+// pass 1: out = exclusive scan within each tile of kThreads * kScanItems, sums[tile] = tile total
+template <bool kMul>
+__global__ void __launch_bounds__(kThreads) k_scan_tile(const Fr* in, Fr* out, uint64_t n, Fr* __restrict__ sums) {
+    __shared__ Fr sm[kThreads];
+    const uint64_t base = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) * kScanItems;
+    Fr v[kScanItems];
+    Fr acc = identity<kMul>();
+#pragma unroll
+    for (uint32_t j = 0; j < kScanItems; j++) {
+        v[j] = base + j < n ? in[base + j] : identity<kMul>();
+        acc = op<kMul>(acc, v[j]);
+    }
+    Fr total;
+    Fr pre = block_exclusive<kMul>(acc, sm, &total);
+#pragma unroll
+    for (uint32_t j = 0; j < kScanItems; j++) {
+        if (base + j < n) out[base + j] = pre;
+        pre = op<kMul>(pre, v[j]);
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// pass 3: out[i] = prefix[tile] (op) out[i]
+template <bool kMul>
+__global__ void k_scan_apply(Fr* __restrict__ out, uint64_t n, const Fr* __restrict__ prefix) {
+    const uint64_t tile = (uint64_t)kThreads * kScanItems;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t t = i / tile;
+        if (t) out[i] = op<kMul>(prefix[t], out[i]);
+    }
+}
+
+// out[i] = in[0] (op) ... (op) in[i-1] (the identity for i = 0); in and out may alias
+template <bool kMul>
+Status scan_exclusive(Context* ctx, const Fr* in, Fr* out, uint64_t n, cudaStream_t st, int depth = 0) {
+    if (n == 0) return OK;
+    const uint64_t tile = (uint64_t)kThreads * kScanItems;
+    const uint64_t tiles = (n + tile - 1) / tile;
+    void* sums;
+    MZK_TRY(ctx->ensure(("grand_scan_" + std::to_string(depth)).c_str(), (tiles + 1) * sizeof(Fr), &sums));
+    k_scan_tile<kMul><<<(uint32_t)tiles, kThreads, 0, st>>>(in, out, n, (Fr*)sums);
+    MZK_LAUNCH_CHECK(ctx);
+    if (tiles > 1) {
+        // exclusive scan of the tile totals (recursively), then fold it in
+        MZK_TRY(scan_exclusive<kMul>(ctx, (const Fr*)sums, (Fr*)sums, tiles, st, depth + 1));
+        k_scan_apply<kMul><<<grid_for(ctx, n, kThreads), kThreads, 0, st>>>(out, n, (const Fr*)sums);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    return OK;
+}
+
+// ---- first-order linear recurrence from the top: y_i = c_i + k y_{i+1},
+// y_n = 0.  Thread t solves its chunk [tK, tK+K) with a zero carry-in and
+// records L_t = its local y at tK; the true values at the chunk starts solve
+// the same recurrence over the L_t with k^K; a last pass adds k^(hi-i) Y_{t+1}.
+__global__ void __launch_bounds__(kThreads) k_rec_local(const Fr* __restrict__ c, Fr* __restrict__ y, uint64_t n,
+                                                        Fr k, Fr* __restrict__ lows) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t lo = t * kRecChunk;
+    if (lo >= n) return;
+    const uint64_t hi = min(n, lo + kRecChunk);
+    Fr acc = fr_zero();
+    for (uint64_t i = hi; i-- > lo;) {
+        acc = fr_add(c[i], fr_mul(k, acc));
+        y[i] = acc;
+    }
+    lows[t] = acc;
+}
+__global__ void __launch_bounds__(kThreads) k_rec_fix(Fr* __restrict__ y, uint64_t n, Fr k,
+                                                      const Fr* __restrict__ starts, uint64_t chunks) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t + 1 >= chunks) return;  // the top chunk has a zero carry-in
+    const uint64_t lo = t * kRecChunk, hi = lo + kRecChunk;
+    const Fr carry = starts[t + 1];
+    Fr pw = k;  // k^(hi - i) for i = hi - 1
+    for (uint64_t i = hi; i-- > lo;) {
+        y[i] = fr_add(y[i], fr_mul(pw, carry));
+        pw = fr_mul(pw, k);
+    }
+}
+
+// y (n) from c (n), in and out may not alias
+Status linrec_suffix(Context* ctx, const Fr* c, Fr* y, uint64_t n, const host::Fr4& k, cudaStream_t st, int depth = 0) {
+    if (n == 0) return OK;
+    const uint64_t chunks = (n + kRecChunk - 1) / kRecChunk;
+    void* lows;
+    MZK_TRY(ctx->ensure(("grand_rec_" + std::to_string(depth)).c_str(), 2 * chunks * sizeof(Fr), &lows));
+    Fr* L = (Fr*)lows;
+    Fr* Y = L + chunks;
+    k_rec_local<<<(uint32_t)((chunks + kThreads - 1) / kThreads), kThreads, 0, st>>>(c, y, n, to_dev(k), L);
+    MZK_LAUNCH_CHECK(ctx);
+    if (chunks > 1) {
+        host::Fr4 kk = k;  // k^kRecChunk
+        for (uint32_t b = 1; b < kRecChunk; b <<= 1) kk = host::fr_mul(kk, kk);
+        MZK_TRY(linrec_suffix(ctx, L, Y, chunks, kk, st, depth + 1));
+        k_rec_fix<<<(uint32_t)((chunks + kThreads - 1) / kThreads), kThreads, 0, st>>>(y, n, to_dev(k), Y, chunks);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    return OK;
+}
+
+// ---- permutation argument ----
+struct PermCols {
+    const Fr* values[kMaxPermSetCols];
+    const Fr* sigmas[kMaxPermSetCols];
+    Fr delta_pow[kMaxPermSetCols];  // delta^(set chunk_len + j)
+    uint32_t cols;
+};
+
+// den[i] = prod_j (beta s_j[i] + gamma + p_j[i])
+__global__ void k_perm_den(PermCols pc, Fr beta, Fr gamma, Fr* __restrict__ den, uint32_t n) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Fr acc = fr_one();
+        for (uint32_t j = 0; j < pc.cols; j++)
+            acc = fr_mul(acc, fr_add(fr_add(fr_mul(beta, pc.sigmas[j][i]), gamma), pc.values[j][i]));
+        den[i] = acc;
+    }
+}
+// mv[i] *= prod_j (delta^(..+j) w^i beta + gamma + p_j[i]); w^i from the split tables
+__global__ void k_perm_num(PermCols pc, Fr beta, Fr gamma, const Fr* __restrict__ wlo, const Fr* __restrict__ whi,
+                           Fr* __restrict__ mv, uint32_t n) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const Fr wb = fr_mul(fr_mul(wlo[i & 4095u], whi[i >> 12]), beta);
+        Fr acc = mv[i];
+        for (uint32_t j = 0; j < pc.cols; j++)
+            acc = fr_mul(acc, fr_add(fr_add(fr_mul(pc.delta_pow[j], wb), gamma), pc.values[j][i]));
+        mv[i] = acc;
+    }
+}
+// z[i] = (i < n - bf ? z[i] : blinds[i - (n - bf)]) * corr
+__global__ void k_perm_finish(Fr* __restrict__ z, uint32_t n, uint32_t bf, const Fr* __restrict__ blinds, Fr corr,
+                              int scale) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Fr v = i < n - bf ? z[i] : blinds[i - (n - bf)];
+        if (scale) v = fr_mul(v, corr);
+        z[i] = v;
+    }
+}
+
+// ---- logup argument ----
+// out[i] = beta + v[i]
+__global__ void k_add_const(const Fr* __restrict__ v, Fr beta, Fr* __restrict__ out, uint32_t n) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = fr_add(beta, v[i]);
+}
+// h[i] = sum of the chunk's inverted columns (cols consecutive arrays of n)
+__global__ void k_sum_cols(const Fr* __restrict__ inv, uint32_t cols, Fr* __restrict__ h, uint32_t n) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Fr acc = fr_zero();
+        for (uint32_t j = 0; j < cols; j++) acc = fr_add(acc, inv[(size_t)j * n + i]);
+        h[i] = acc;
+    }
+}
+// ld[i] = sel[i] * sum_c h_c[i] - m[i] * tden[i]
+struct HelperPtrs {
+    Fr* h[kMaxLogupChunks];
+    uint32_t chunks;
+};
+__global__ void k_logderivative(HelperPtrs hp, const Fr* __restrict__ sel, const Fr* __restrict__ m,
+                                const Fr* __restrict__ tden, Fr* __restrict__ ld, uint32_t n) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Fr s = fr_zero();
+        for (uint32_t c = 0; c < hp.chunks; c++) s = fr_add(s, hp.h[c][i]);
+        ld[i] = fr_sub(fr_mul(sel[i], s), fr_mul(m[i], tden[i]));
+    }
+}
+// z[n - bf + b] = blinds[b]
+__global__ void k_set_tail(Fr* __restrict__ z, uint32_t n, uint32_t bf, const Fr* __restrict__ blinds) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < bf) z[n - bf + b] = blinds[b];
+}
+
+}  // namespace
+
+Status permutation_z_device(Context* ctx, const Domain* d, const mzk_permutation_desc* desc, cudaStream_t st) {
+    const uint32_t n = 1u << d->k, bf = desc->blinding_factors;
+    if (desc->chunk_len == 0 || desc->chunk_len > kMaxPermSetCols || bf + 1 >= n || desc->n_cols == 0 ||
+        !desc->values || !desc->sigmas || !desc->z_out || (bf && !desc->blinds)) {
+        set_error("permutation_z: need 1..8 columns per set, blinding_factors < n - 1 and non-null arrays");
+        return ERR_ARG;
+    }
+    const uint32_t sets = (desc->n_cols + desc->chunk_len - 1) / desc->chunk_len;
+    void *mv_buf, *dbl;
+    MZK_TRY(ctx->ensure("perm_mv", (size_t)n * sizeof(Fr), &mv_buf));
+    MZK_TRY(ctx->ensure("perm_blinds", ((size_t)sets * bf + 1) * sizeof(Fr), &dbl));
+    if (bf)
+        MZK_CUDA_CHECK(cudaMemcpyAsync(dbl, desc->blinds, (size_t)sets * bf * sizeof(Fr), cudaMemcpyHostToDevice, st));
+    Fr* mv = (Fr*)mv_buf;
+    const Fr beta = to_dev(to_host(desc->beta)), gamma = to_dev(to_host(desc->gamma));
+    const host::Fr4 delta = to_host(kDeltaU64);
+    const uint32_t grid = grid_for(ctx, n, kThreads);
+    for (uint32_t s = 0; s < sets; s++) {
+        PermCols pc;
+        pc.cols = std::min(desc->chunk_len, desc->n_cols - s * desc->chunk_len);
+        const uint64_t e0 = (uint64_t)s * desc->chunk_len;
+        host::Fr4 dp = host::fr_pow(delta, &e0, 1);
+        for (uint32_t j = 0; j < pc.cols; j++) {
+            const uint32_t c = s * desc->chunk_len + j;
+            if (!desc->values[c] || !desc->sigmas[c] || !desc->z_out[s]) {
+                set_error("permutation_z: null column");
+                return ERR_ARG;
+            }
+            pc.values[j] = reinterpret_cast<const Fr*>(desc->values[c]);
+            pc.sigmas[j] = reinterpret_cast<const Fr*>(desc->sigmas[c]);
+            pc.delta_pow[j] = to_dev(dp);
+            dp = host::fr_mul(dp, delta);
+        }
+        k_perm_den<<<grid, kThreads, 0, st>>>(pc, beta, gamma, mv, n);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_TRY(batch_invert(ctx, mv, n, st));
+        k_perm_num<<<grid, kThreads, 0, st>>>(pc, beta, gamma, d->lo[0], d->hi[0], mv, n);
+        MZK_LAUNCH_CHECK(ctx);
+        Fr* z = reinterpret_cast<Fr*>(desc->z_out[s]);
+        MZK_TRY(scan_exclusive<true>(ctx, mv, z, n, st));
+    }
+    // the uncorrected last products z_s[n - bf - 1] (before the blinds) -> corrections
+    void* host_last;
+    MZK_TRY(ctx->ensure_pinned((size_t)sets * 32, &host_last));
+    for (uint32_t s = 0; s < sets; s++)
+        MZK_CUDA_CHECK(cudaMemcpyAsync(static_cast<char*>(host_last) + 32 * s,
+                                       reinterpret_cast<const Fr*>(desc->z_out[s]) + (n - bf - 1), 32,
+                                       cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    std::vector<host::Fr4> last(sets);
+    for (uint32_t s = 0; s < sets; s++) last[s] = to_host(static_cast<const uint64_t*>(host_last) + 4 * s);
+    host::Fr4 corr = host::fr_one();
+    for (uint32_t s = 0; s < sets; s++) {
+        const bool scale = std::memcmp(corr.l, host::fr_one().l, 32) != 0;
+        k_perm_finish<<<grid, kThreads, 0, st>>>(reinterpret_cast<Fr*>(desc->z_out[s]), n, bf,
+                                                 (const Fr*)dbl + (size_t)s * bf, to_dev(corr), scale ? 1 : 0);
+        MZK_LAUNCH_CHECK(ctx);
+        corr = host::fr_mul(corr, last[s]);
+    }
+    return OK;
+}
+
+Status logup_device(Context* ctx, const Domain* d, const mzk_logup_desc* desc, cudaStream_t st) {
+    const uint32_t n = 1u << d->k, bf = desc->blinding_factors;
+    if (desc->n_chunks == 0 || desc->n_chunks > kMaxLogupChunks || bf + 1 >= n || !desc->chunk_cols ||
+        !desc->inputs || !desc->table || !desc->selector || !desc->multiplicities || !desc->helpers_out ||
+        !desc->aggregator_out || (bf && !desc->blinds)) {
+        set_error("logup: need 1..8 chunks, blinding_factors < n - 1 and non-null arrays");
+        return ERR_ARG;
+    }
+    uint32_t total_cols = 0;
+    for (uint32_t c = 0; c < desc->n_chunks; c++) total_cols += desc->chunk_cols[c];
+    void *tden_buf, *cols_buf, *ld_buf, *dbl;
+    MZK_TRY(ctx->ensure("logup_tden", (size_t)n * sizeof(Fr), &tden_buf));
+    MZK_TRY(ctx->ensure("logup_cols", (size_t)std::max(1u, total_cols) * n * sizeof(Fr), &cols_buf));
+    MZK_TRY(ctx->ensure("logup_ld", (size_t)n * sizeof(Fr), &ld_buf));
+    MZK_TRY(ctx->ensure("logup_blinds", ((size_t)bf + 1) * sizeof(Fr), &dbl));
+    if (bf) MZK_CUDA_CHECK(cudaMemcpyAsync(dbl, desc->blinds, (size_t)bf * sizeof(Fr), cudaMemcpyHostToDevice, st));
+    Fr *tden = (Fr*)tden_buf, *cols = (Fr*)cols_buf, *ld = (Fr*)ld_buf;
+    const Fr beta = to_dev(to_host(desc->beta));
+    const uint32_t grid = grid_for(ctx, n, kThreads);
+    // T = 1 / (t + beta)
+    k_add_const<<<grid, kThreads, 0, st>>>(reinterpret_cast<const Fr*>(desc->table), beta, tden, n);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(batch_invert(ctx, tden, n, st));
+    // every input column: 1 / (f + beta) (inverting them together gives the same field values)
+    for (uint32_t j = 0; j < total_cols; j++) {
+        if (!desc->inputs[j]) {
+            set_error("logup: null input column");
+            return ERR_ARG;
+        }
+        k_add_const<<<grid, kThreads, 0, st>>>(reinterpret_cast<const Fr*>(desc->inputs[j]), beta,
+                                               cols + (size_t)j * n, n);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    MZK_TRY(batch_invert(ctx, cols, (uint64_t)total_cols * n, st));
+    HelperPtrs hp;
+    hp.chunks = desc->n_chunks;
+    for (uint32_t c = 0, j = 0; c < desc->n_chunks; j += desc->chunk_cols[c], c++) {
+        if (!desc->helpers_out[c]) {
+            set_error("logup: null helper output");
+            return ERR_ARG;
+        }
+        hp.h[c] = reinterpret_cast<Fr*>(desc->helpers_out[c]);
+        k_sum_cols<<<grid, kThreads, 0, st>>>(cols + (size_t)j * n, desc->chunk_cols[c], hp.h[c], n);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    k_logderivative<<<grid, kThreads, 0, st>>>(hp, reinterpret_cast<const Fr*>(desc->selector),
+                                               reinterpret_cast<const Fr*>(desc->multiplicities), tden, ld, n);
+    MZK_LAUNCH_CHECK(ctx);
+    // aggregator: exclusive running sum over the first n - bf rows, then the blinds
+    Fr* agg = reinterpret_cast<Fr*>(desc->aggregator_out);
+    MZK_TRY(scan_exclusive<false>(ctx, ld, agg, n - bf, st));
+    if (bf) {
+        k_set_tail<<<1, 64, 0, st>>>(agg, n, bf, (const Fr*)dbl);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    return OK;
+}
+
+Status batch_invert_device(Context* ctx, void* a, uint64_t n, cudaStream_t st) {
+    return batch_invert(ctx, static_cast<Fr*>(a), n, st);
+}
+
+Status eval_polynomial_device(Context* ctx, const void* poly, uint64_t n, const uint64_t point[4], uint64_t out[4],
+                              cudaStream_t st) {
+    std::memset(out, 0, 32);
+    if (n == 0) return OK;
+    void* y;
+    MZK_TRY(ctx->ensure("grand_eval", n * sizeof(Fr), &y));
+    MZK_TRY(linrec_suffix(ctx, static_cast<const Fr*>(poly), (Fr*)y, n, to_host(point), st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(out, y, 32, cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    return OK;
+}
+
+Status kate_division_device(Context* ctx, const void* a, uint64_t n, const uint64_t b[4], void* q, cudaStream_t st) {
+    if (n < 2) return OK;
+    // q_i = a_{i+1} + b q_{i+1}, q_{n-1} = 0
+    return linrec_suffix(ctx, static_cast<const Fr*>(a) + 1, static_cast<Fr*>(q), n - 1, to_host(b), st);
+}
+
+}  // namespace mzk

@@ -1173,6 +1173,141 @@ void or_eval_polynomial(uint64_t out[4], const uint64_t *poly, size_t n, const u
 }
 
 /* ------------------------------------------------------------------------- */
+/* Grand products and running sums of the permutation and logup arguments    */
+/* ------------------------------------------------------------------------- */
+
+static int fr_is_zero(const u64 *a) { return (a[0] | a[1] | a[2] | a[3]) == 0; }
+
+/* ff 0.13 BatchInvert (crate `ff`, a dependency of the reference that is not
+ * vendored; used at permutation/prover.rs:139 and logup/prover.rs:221,232):
+ * Montgomery's simultaneous inversion, forward products skipping zeros, one
+ * inversion, backward pass; zero elements are left unchanged. */
+void or_fr_batch_invert(uint64_t *a, size_t n) {
+    u64 *pre = (u64 *)malloc((n ? n : 1) * 32);
+    u64 acc[4];
+    memcpy(acc, FR_R, 32);
+    for (size_t i = 0; i < n; i++) {
+        memcpy(pre + 4 * i, acc, 32);
+        if (!fr_is_zero(a + 4 * i)) fr_mul(acc, acc, a + 4 * i);
+    }
+    fr_inv(acc, acc);
+    for (size_t i = n; i-- > 0;) {
+        if (fr_is_zero(a + 4 * i)) continue;
+        u64 t[4], inv[4];
+        fr_mul(inv, pre + 4 * i, acc); /* 1 / a_i */
+        fr_mul(t, acc, a + 4 * i);     /* drop a_i from the running inverse */
+        memcpy(acc, t, 32);
+        memcpy(a + 4 * i, inv, 32);
+    }
+    free(pre);
+}
+
+/* permutation/prover.rs:81-255 (Stages 1, 2 A-C): per set of chunk_len
+ * columns, modified_values[i] = prod_j (p_j(w^i) + delta^(s chunk_len + j) w^i
+ * beta + gamma) / prod_j (p_j(w^i) + beta s_j(w^i) + gamma); z[0] = 1,
+ * z[r] = z[r-1] modified[r-1]; the last blinding_factors rows are the blinds;
+ * set s is then multiplied (every row, blinds included) by the product of the
+ * earlier sets' z[n - blinding_factors - 1]. */
+void or_permutation_z(const uint64_t *const *values, const uint64_t *const *sigmas, uint32_t n_cols,
+                      uint32_t chunk_len, uint32_t k, const uint64_t omega[4], const uint64_t beta[4],
+                      const uint64_t gamma[4], uint32_t blinding_factors, const uint64_t *blinds,
+                      uint64_t *const *z_out) {
+    const size_t n = (size_t)1 << k;
+    const uint32_t n_sets = (n_cols + chunk_len - 1) / chunk_len;
+    u64 *mv = (u64 *)malloc(n * 32);
+    u64 correction[4];
+    memcpy(correction, FR_R, 32);
+    for (uint32_t s = 0; s < n_sets; s++) {
+        const uint32_t c0 = s * chunk_len, c1 = c0 + chunk_len < n_cols ? c0 + chunk_len : n_cols;
+        for (size_t i = 0; i < n; i++) memcpy(mv + 4 * i, FR_R, 32);
+        for (uint32_t c = c0; c < c1; c++)
+            for (size_t i = 0; i < n; i++) {
+                u64 t[4];
+                fr_mul(t, beta, sigmas[c] + 4 * i);
+                fr_add(t, t, gamma);
+                fr_add(t, t, values[c] + 4 * i);
+                fr_mul(mv + 4 * i, mv + 4 * i, t);
+            }
+        or_fr_batch_invert(mv, n);
+        u64 deltaomega[4], e[1] = {(u64)c0};
+        fr_pow(deltaomega, FR_DELTA, e, 1);
+        for (uint32_t c = c0; c < c1; c++) {
+            u64 dw[4];
+            memcpy(dw, deltaomega, 32);
+            for (size_t i = 0; i < n; i++) {
+                u64 t[4];
+                fr_mul(t, dw, beta);
+                fr_add(t, t, gamma);
+                fr_add(t, t, values[c] + 4 * i);
+                fr_mul(mv + 4 * i, mv + 4 * i, t);
+                fr_mul(dw, dw, omega);
+            }
+            fr_mul(deltaomega, deltaomega, FR_DELTA);
+        }
+        u64 *z = z_out[s];
+        memcpy(z, FR_R, 32);
+        for (size_t r = 1; r < n; r++) fr_mul(z + 4 * r, z + 4 * (r - 1), mv + 4 * (r - 1));
+        for (uint32_t b = 0; b < blinding_factors; b++) memcpy(z + 4 * (n - blinding_factors + b), blinds + 4 * ((size_t)s * blinding_factors + b), 32);
+        u64 last[4];
+        memcpy(last, z + 4 * (n - blinding_factors - 1), 32);
+        for (size_t i = 0; i < n; i++) fr_mul(z + 4 * i, z + 4 * i, correction);
+        fr_mul(correction, correction, last); /* the next set's correction */
+    }
+    free(mv);
+}
+
+/* logup/prover.rs:195-300: T = 1/(t + beta) and per chunk of compressed input
+ * columns h = sum_j 1/(f_j + beta) (each column batch-inverted on its own);
+ * logderivative[i] = selector[i] (sum over chunks of h[i]) - m[i] T[i];
+ * aggregator = [0, running sums of logderivative] taken to n - blinding_factors
+ * rows, then the blinding values. */
+void or_logup(const uint64_t *const *inputs, const uint32_t *chunk_cols, uint32_t n_chunks, const uint64_t *table,
+              const uint64_t *selector, const uint64_t *multiplicities, size_t n, const uint64_t beta[4],
+              uint32_t blinding_factors, const uint64_t *blinds, uint64_t *const *helpers_out,
+              uint64_t *aggregator_out) {
+    u64 *tden = (u64 *)malloc(n * 32), *col = (u64 *)malloc(n * 32);
+    for (size_t i = 0; i < n; i++) fr_add(tden + 4 * i, beta, table + 4 * i);
+    or_fr_batch_invert(tden, n);
+    uint32_t ci = 0;
+    for (uint32_t c = 0; c < n_chunks; c++) {
+        u64 *h = helpers_out[c];
+        memset(h, 0, n * 32);
+        for (uint32_t j = 0; j < chunk_cols[c]; j++, ci++) {
+            for (size_t i = 0; i < n; i++) fr_add(col + 4 * i, beta, inputs[ci] + 4 * i);
+            or_fr_batch_invert(col, n);
+            for (size_t i = 0; i < n; i++) fr_add(h + 4 * i, h + 4 * i, col + 4 * i);
+        }
+    }
+    u64 state[4] = {0, 0, 0, 0};
+    memset(aggregator_out, 0, 32);
+    for (size_t i = 0; i + 1 < n - blinding_factors; i++) {
+        u64 sum[4] = {0, 0, 0, 0}, t[4], u[4];
+        for (uint32_t c = 0; c < n_chunks; c++) fr_add(sum, sum, helpers_out[c] + 4 * i);
+        fr_mul(t, selector + 4 * i, sum);
+        fr_mul(u, multiplicities + 4 * i, tden + 4 * i);
+        fr_sub(t, t, u);
+        fr_add(state, state, t);
+        memcpy(aggregator_out + 4 * (i + 1), state, 32);
+    }
+    for (uint32_t b = 0; b < blinding_factors; b++) memcpy(aggregator_out + 4 * (n - blinding_factors + b), blinds + 4 * b, 32);
+    free(tden);
+    free(col);
+}
+
+/* utils/arithmetic.rs:106-125: quotient of a(X) by (X - b), n - 1 coefficients:
+ * from the top, q = a_{i+1} - tmp, tmp = q * (-b). */
+void or_kate_division(const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q) {
+    u64 nb[4], tmp[4] = {0, 0, 0, 0}, zero[4] = {0, 0, 0, 0};
+    fr_sub(nb, zero, b);
+    for (size_t i = n - 1; i-- > 0;) {
+        u64 lead[4];
+        fr_sub(lead, a + 4 * (i + 1), tmp);
+        memcpy(q + 4 * i, lead, 32);
+        fr_mul(tmp, lead, nb);
+    }
+}
+
+/* ------------------------------------------------------------------------- */
 /* Quotient numerator, proofs/src/plonk/evaluation.rs:818-1114               */
 /* ------------------------------------------------------------------------- */
 /* get_rotation_idx, evaluation.rs:13-16 */

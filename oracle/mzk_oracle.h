@@ -111,6 +111,18 @@ void or_domain_divide_by_vanishing_poly(const or_domain *d, uint64_t *a, int thr
  * advice/fixed columns, at most one logup lookup with one input column and one
  * helper, no trashcans.  All columns are extended-domain (coset) evaluations
  * of length 2^extended_k, Fr Montgomery. */
+/* grand products and running sums (permutation and logup arguments) */
+void or_fr_batch_invert(uint64_t *a, size_t n); /* ff BatchInvert: zeros stay zero */
+void or_permutation_z(const uint64_t *const *values, const uint64_t *const *sigmas, uint32_t n_cols,
+                      uint32_t chunk_len, uint32_t k, const uint64_t omega[4], const uint64_t beta[4],
+                      const uint64_t gamma[4], uint32_t blinding_factors, const uint64_t *blinds,
+                      uint64_t *const *z_out);
+void or_logup(const uint64_t *const *inputs, const uint32_t *chunk_cols, uint32_t n_chunks, const uint64_t *table,
+              const uint64_t *selector, const uint64_t *multiplicities, size_t n, const uint64_t beta[4],
+              uint32_t blinding_factors, const uint64_t *blinds, uint64_t *const *helpers_out,
+              uint64_t *aggregator_out);
+void or_kate_division(const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q);
+
 typedef struct {
     uint32_t k, extended_k;
     const uint64_t *const *advice; uint32_t n_advice;

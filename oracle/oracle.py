@@ -37,6 +37,12 @@ def _load():
     u64 = ctypes.c_uint64
     sigs = {
         "or_fr_mul": (None, [_u64p, _u64p, _u64p]),
+        "or_fr_batch_invert": (None, [_u64p, sz]),
+        "or_permutation_z": (None, [ctypes.c_void_p, ctypes.c_void_p, u32, u32, u32, _u64p, _u64p, _u64p, u32,
+                                    _u64p, ctypes.c_void_p]),
+        "or_logup": (None, [ctypes.c_void_p, ctypes.POINTER(u32), u32, _u64p, _u64p, _u64p, sz, _u64p, u32, _u64p,
+                            ctypes.c_void_p, _u64p]),
+        "or_kate_division": (None, [_u64p, sz, _u64p, _u64p]),
         "or_fr_add": (None, [_u64p, _u64p, _u64p]),
         "or_fr_sub": (None, [_u64p, _u64p, _u64p]),
         "or_fr_neg": (None, [_u64p, _u64p]),
@@ -287,6 +293,56 @@ def eval_polynomial(poly, point, threads=None):
     lib.or_eval_polynomial(P(o), P(poly), poly.shape[0], P(np.ascontiguousarray(point, np.uint64)),
                            threads or threads_default())
     return o
+
+
+def _ptr_array(arrays):
+    arr = (ctypes.c_void_p * max(1, len(arrays)))(*[a.ctypes.data for a in arrays])
+    return arr
+
+
+def batch_invert(a):
+    """ff BatchInvert: every non-zero element inverted, zeros left as zero."""
+    o = np.ascontiguousarray(a, np.uint64).copy()
+    lib.or_fr_batch_invert(P(o), o.shape[0])
+    return o
+
+
+def permutation_z(values, sigmas, chunk_len, k, omega, beta, gamma, blinding_factors, blinds):
+    """permutation/prover.rs:81-255: z of every set (Lagrange form).  blinds:
+    (n_sets, blinding_factors, 4)."""
+    n = 1 << k
+    values = [np.ascontiguousarray(v, np.uint64) for v in values]
+    sigmas = [np.ascontiguousarray(v, np.uint64) for v in sigmas]
+    n_sets = (len(values) + chunk_len - 1) // chunk_len
+    zs = [np.zeros((n, 4), np.uint64) for _ in range(n_sets)]
+    bl = np.ascontiguousarray(blinds, np.uint64).reshape(-1, 4)
+    lib.or_permutation_z(_ptr_array(values), _ptr_array(sigmas), len(values), chunk_len, k,
+                         P(np.ascontiguousarray(omega, np.uint64)), P(np.ascontiguousarray(beta, np.uint64)),
+                         P(np.ascontiguousarray(gamma, np.uint64)), blinding_factors, P(bl), _ptr_array(zs))
+    return zs
+
+
+def logup(chunks, table, selector, multiplicities, beta, blinding_factors, blinds):
+    """logup/prover.rs:195-300: (helper per chunk, aggregator).  chunks: list
+    of lists of compressed input columns."""
+    n = table.shape[0]
+    cols = [np.ascontiguousarray(c, np.uint64) for ch in chunks for c in ch]
+    counts = (ctypes.c_uint32 * max(1, len(chunks)))(*[len(ch) for ch in chunks])
+    helpers = [np.zeros((n, 4), np.uint64) for _ in chunks]
+    agg = np.zeros((n, 4), np.uint64)
+    lib.or_logup(_ptr_array(cols), counts, len(chunks), P(np.ascontiguousarray(table, np.uint64)),
+                 P(np.ascontiguousarray(selector, np.uint64)), P(np.ascontiguousarray(multiplicities, np.uint64)),
+                 n, P(np.ascontiguousarray(beta, np.uint64)), blinding_factors,
+                 P(np.ascontiguousarray(blinds, np.uint64).reshape(-1, 4)), _ptr_array(helpers), P(agg))
+    return helpers, agg
+
+
+def kate_division(a, b):
+    """utils/arithmetic.rs:106-125: coefficients of a(X) / (X - b), n - 1 of them."""
+    a = np.ascontiguousarray(a, np.uint64)
+    q = np.zeros((max(0, a.shape[0] - 1), 4), np.uint64)
+    lib.or_kate_division(P(a), a.shape[0], P(np.ascontiguousarray(b, np.uint64)), P(q))
+    return q
 
 
 def fr_pow(x, e):
