@@ -215,7 +215,7 @@ class ProverKeys:
         for k in ks:
             dom = mzk.EvaluationDomain(ctx, 5, k)
             E = dom.extended_len
-            cols = ctx.gen_rand_fr(0xC0150000 + k, 13 * E)
+            cols = ctx.gen_rand_fr(0xC0150000 + k, 13 * E + 5 * (1 << k))
             pk = mzk.ProvingKeyDesc()
             pk.k = k
             for i in range(7):
@@ -223,6 +223,10 @@ class ProverKeys:
             for i in range(3):
                 pk.sigma_ext[i] = cols.ptr + (7 + i) * E * 32
             pk.l0_ext, pk.l_last_ext, pk.l_active_ext = (cols.ptr + (10 + i) * E * 32 for i in range(3))
+            lag0 = cols.ptr + 13 * E * 32  # Lagrange sigma a, b, c, table, selector (n each)
+            for i in range(3):
+                pk.sigma_lagrange[i] = lag0 + i * (1 << k) * 32
+            pk.table_lagrange, pk.selector_lagrange = lag0 + 3 * (1 << k) * 32, lag0 + 4 * (1 << k) * 32
             pk.srs, pk.srs_len = self.srs.ptr, self.srs_len
             n = 1 << k
             pk.off_g, pk.off_lagrange, pk.off_lagrange_delta, pk.off_lagrange_double_delta = 0, off, off + n, off + 2 * n
@@ -231,13 +235,19 @@ class ProverKeys:
             self.doms[k], self.pks[k], self.cols[k] = dom, pk, cols
 
     def job(self, k, seed):
-        """A proof job with fresh seeded witness columns (a, b, c, z, m, h, Z) on the device."""
+        """A proof job with fresh seeded witness columns a, b, c and lookup
+        multiplicities m on the device; the permutation product z and the
+        logup helper h and aggregator Z are derived by the device."""
         n = 1 << k
-        w = self.ctx.gen_rand_fr(seed, 7 * n)
+        w = self.ctx.gen_rand_fr(seed, 4 * n)
         j = self.mzk.ProofJob()
-        ptr = [w.ptr + i * n * 32 for i in range(7)]
+        ptr = [w.ptr + i * n * 32 for i in range(4)]
         j.advice[0], j.advice[1], j.advice[2] = ptr[0], ptr[1], ptr[2]
-        j.perm_z, j.lookup_m, j.lookup_h, j.lookup_Z = ptr[3], ptr[4], ptr[5], ptr[6]
+        j.lookup_m = ptr[3]
+        j.perm_z = j.lookup_h = j.lookup_Z = None
+        for i in range(8):
+            j.perm_blinds[i][:] = [seed % 991 + 20 + i, 0, 0, 0]
+            j.lookup_blinds[i][:] = [seed % 983 + 40 + i, 0, 0, 0]
         for i, name in enumerate(("y", "beta", "gamma", "theta")):
             getattr(j, name)[:] = [seed % 1000 + 3 + i, 0, 0, 0]
         for i in range(3):
@@ -273,7 +283,7 @@ def measure_proof_core(mzk, ctx, keys, k, reps, batch):
     return {"k": k, "rows": 1 << k, "per_call_ms_per_proof": round(per_call_ms, 2),
             "one_proof_batched_msms_ms": round(plain_ms, 2), "batch": batch,
             "batched_ms_per_call": round(batch_ms, 2), "batched_proofs_per_s": round(batch * 1e3 / batch_ms, 2),
-            "msms_per_proof": 11, "scalars": "uniform Fr in every witness column (conservative)"}
+            "msms_per_proof": 11, "witness": "a, b, c, m uniform Fr; z, h, Z derived on the device"}
 
 
 def measure_batched_msm(mzk, ctx, reps):

@@ -192,15 +192,26 @@ typedef struct {
     const uint64_t *srs;           /* DEVICE G1Affine array holding the four bases below */
     uint64_t srs_len;              /* points in srs */
     uint64_t off_g, off_lagrange, off_lagrange_delta, off_lagrange_double_delta; /* ParamsKZG::bases, params.rs:83-93 */
-    uint32_t blinding_factors;
+    uint32_t blinding_factors;     /* at most 8 */
+    /* Lagrange forms (DEVICE, n each), read only for jobs whose z / h / Z the
+     * device derives (null perm_z, lookup_h, lookup_Z): */
+    const uint64_t *sigma_lagrange[3];  /* permutation polynomials of a, b, c */
+    const uint64_t *table_lagrange;     /* lookup table column */
+    const uint64_t *selector_lagrange;  /* lookup selector column */
 } mzk_proving_key_desc;
-/* One proof's witness (Lagrange form, DEVICE, n Fr each) and challenges. */
+/* One proof's witness (Lagrange form, DEVICE, n Fr each) and challenges.
+ * perm_z null: the device derives z (permutation/prover.rs:81-255) from a, b,
+ * c and the key's sigma_lagrange with perm_blinds; lookup_h and lookup_Z both
+ * null: it derives them (logup/prover.rs:195-300; the compressed input of the
+ * single input expression is a itself) with lookup_blinds. */
 typedef struct {
     const uint64_t *advice[3];     /* a, b, c */
-    const uint64_t *perm_z;        /* permutation product */
-    const uint64_t *lookup_m, *lookup_h, *lookup_Z; /* logup multiplicities, helper, aggregator */
+    const uint64_t *perm_z;        /* permutation product, or null */
+    const uint64_t *lookup_m, *lookup_h, *lookup_Z; /* logup multiplicities, helper, aggregator (h, Z or null) */
     uint64_t y[4], beta[4], gamma[4], theta[4];
     uint64_t quotient_blinds[3][4];
+    uint64_t perm_blinds[8][4];    /* blinding rows of a derived z */
+    uint64_t lookup_blinds[8][4];  /* blinding rows of a derived Z */
 } mzk_proof_job;
 /* For each job: commitments (out: count x 11 x 18 u64 G1Projective, in the
  * order a, b, c, m (delta), z (delta), Z (double delta), h, quotient limbs

@@ -93,7 +93,9 @@ class ProvingKeyDesc(ctypes.Structure):
                 ("l0_ext", ctypes.c_void_p), ("l_last_ext", ctypes.c_void_p), ("l_active_ext", ctypes.c_void_p),
                 ("srs", ctypes.c_void_p), ("srs_len", ctypes.c_uint64), ("off_g", ctypes.c_uint64),
                 ("off_lagrange", ctypes.c_uint64), ("off_lagrange_delta", ctypes.c_uint64),
-                ("off_lagrange_double_delta", ctypes.c_uint64), ("blinding_factors", ctypes.c_uint32)]
+                ("off_lagrange_double_delta", ctypes.c_uint64), ("blinding_factors", ctypes.c_uint32),
+                ("sigma_lagrange", ctypes.c_void_p * 3), ("table_lagrange", ctypes.c_void_p),
+                ("selector_lagrange", ctypes.c_void_p)]
 
 
 class ProofJob(ctypes.Structure):
@@ -101,7 +103,8 @@ class ProofJob(ctypes.Structure):
     _fields_ = [("advice", ctypes.c_void_p * 3), ("perm_z", ctypes.c_void_p), ("lookup_m", ctypes.c_void_p),
                 ("lookup_h", ctypes.c_void_p), ("lookup_Z", ctypes.c_void_p), ("y", ctypes.c_uint64 * 4),
                 ("beta", ctypes.c_uint64 * 4), ("gamma", ctypes.c_uint64 * 4), ("theta", ctypes.c_uint64 * 4),
-                ("quotient_blinds", (ctypes.c_uint64 * 4) * 3)]
+                ("quotient_blinds", (ctypes.c_uint64 * 4) * 3), ("perm_blinds", (ctypes.c_uint64 * 4) * 8),
+                ("lookup_blinds", (ctypes.c_uint64 * 4) * 8)]
 
 
 PROVE_MSM_PER_CALL = 1  # MZK_PROVE_MSM_PER_CALL

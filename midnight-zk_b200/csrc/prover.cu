@@ -19,8 +19,10 @@
 // The MSMs of all proofs in a call run as two batched MSMs (step 1 for all
 // proofs, step 5 for all proofs), so small proofs share the GPU's chunks; with
 // MZK_PROVE_MSM_PER_CALL each MSM is its own call instead (the plain form).
-// Witness generation, the permutation and logup running products, the
-// transcript, evaluations and the multi-open argument stay with the caller.
+// The permutation product z and the logup helper h and aggregator Z are taken
+// from the job or, when it leaves them null, derived on the device first
+// (grand.cu).  Witness generation, the lookup multiplicities, the transcript,
+// evaluations and the multi-open argument stay with the caller.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,6 +32,7 @@
 
 #include "../../include/mzk.h"
 #include "field.cuh"
+#include "grand.hpp"
 #include "ntt.hpp"
 #include "quotient.hpp"
 #include "runtime.hpp"
@@ -81,13 +84,15 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
     const uint64_t srs_len = pks[0]->srs_len;
     std::vector<BatchItem> items;
     std::vector<Fr*> coeff(count * kPolys), ext(count * kPolys), limbs(count);
+    std::vector<const void*> lagrange(count * kPolys);  // a, b, c, z, m, h, Z of every job
     size_t max_en = 0;
     // all per-proof scratch of the call in one buffer, carved in job order, so
     // a call's scratch grows (and is reallocated) only when its total grows
     size_t wave_elems = 0;
     for (size_t j = 0; j < count; j++) {
         const size_t n = (size_t)1 << doms[j]->k, en = (size_t)1 << doms[j]->ext_k;
-        wave_elems += kPolys * n + kPolys * en + 3 * n + (size_t)doms[j]->quotient_poly_degree * n;
+        // coefficient and extended forms, delta forms, limbs, derived z / h / Z
+        wave_elems += kPolys * n + kPolys * en + 3 * n + (size_t)doms[j]->quotient_poly_degree * n + 3 * n;
     }
     void* wave;
     MZK_TRY(ctx->ensure("core_wave", wave_elems * sizeof(Fr), &wave));
@@ -115,34 +120,89 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
         Fr* pe = pc + (size_t)kPolys * n;
         Fr* pd = pe + (size_t)kPolys * en;
         Fr* pl = pd + (size_t)3 * n;
-        carve = pl + (size_t)qdeg * n;
+        Fr* pg = pl + (size_t)qdeg * n;  // derived z, h, Z
+        carve = pg + (size_t)3 * n;
         for (int p = 0; p < kPolys; p++) {
             coeff[j * kPolys + p] = pc + (size_t)p * n;
             ext[j * kPolys + p] = pe + (size_t)p * en;
         }
         limbs[j] = pl;
         const mzk_proof_job& jb = jobs[j];
-        const void* lag[kPolys] = {jb.advice[0], jb.advice[1], jb.advice[2], jb.perm_z, jb.lookup_m, jb.lookup_h,
-                                   jb.lookup_Z};
-        for (int p = 0; p < kPolys; p++)
-            if (!lag[p]) {
-                set_error("prove_core: null witness polynomial in job " + tag);
+        const void** lag = &lagrange[j * kPolys];
+        const void* given[kPolys] = {jb.advice[0], jb.advice[1], jb.advice[2], jb.perm_z, jb.lookup_m, jb.lookup_h,
+                                     jb.lookup_Z};
+        for (int p = 0; p < kPolys; p++) lag[p] = given[p];
+        if (pk->blinding_factors > 8 || pk->blinding_factors + 1 >= n) {
+            set_error("prove_core: blinding_factors must be at most 8 and below n - 1");
+            return ERR_ARG;
+        }
+        if ((jb.lookup_h == nullptr) != (jb.lookup_Z == nullptr)) {
+            set_error("prove_core: job " + tag + ": give both or neither of lookup_h and lookup_Z");
+            return ERR_ARG;
+        }
+        if (!jb.advice[0] || !jb.advice[1] || !jb.advice[2] || !jb.lookup_m) {
+            set_error("prove_core: null witness polynomial in job " + tag);
+            return ERR_ARG;
+        }
+        if (!jb.lookup_h) {  // logup helper and aggregator on the device
+            if (!pk->table_lagrange || !pk->selector_lagrange) {
+                set_error("prove_core: deriving h and Z needs the key's table and selector in Lagrange form");
                 return ERR_ARG;
             }
+            uint64_t* hz[1] = {reinterpret_cast<uint64_t*>(pg + n)};
+            const uint64_t* in[1] = {static_cast<const uint64_t*>(jb.advice[0])};
+            const uint32_t cols[1] = {1};
+            mzk_logup_desc ld;
+            std::memset(&ld, 0, sizeof(ld));
+            ld.n_chunks = 1;
+            ld.chunk_cols = cols;
+            ld.inputs = in;
+            ld.table = pk->table_lagrange;
+            ld.selector = pk->selector_lagrange;
+            ld.multiplicities = jb.lookup_m;
+            ld.blinding_factors = pk->blinding_factors;
+            ld.blinds = &jb.lookup_blinds[0][0];
+            std::memcpy(ld.beta, jb.beta, 32);
+            ld.helpers_out = hz;
+            ld.aggregator_out = reinterpret_cast<uint64_t*>(pg + 2 * (size_t)n);
+            MZK_TRY(logup_device(ctx, d, &ld, st));
+            lag[5] = pg + n;
+            lag[6] = pg + 2 * (size_t)n;
+        }
+        if (!jb.perm_z) {  // permutation product on the device
+            if (!pk->sigma_lagrange[0] || !pk->sigma_lagrange[1] || !pk->sigma_lagrange[2]) {
+                set_error("prove_core: deriving z needs the key's permutation polynomials in Lagrange form");
+                return ERR_ARG;
+            }
+            uint64_t* zo[1] = {reinterpret_cast<uint64_t*>(pg)};
+            mzk_permutation_desc pd_;
+            std::memset(&pd_, 0, sizeof(pd_));
+            pd_.n_cols = 3;
+            pd_.values = reinterpret_cast<const uint64_t* const*>(jb.advice);
+            pd_.sigmas = pk->sigma_lagrange;
+            pd_.chunk_len = 3;  // cs.degree() - 2 with degree 5
+            pd_.blinding_factors = pk->blinding_factors;
+            pd_.blinds = &jb.perm_blinds[0][0];
+            std::memcpy(pd_.beta, jb.beta, 32);
+            std::memcpy(pd_.gamma, jb.gamma, 32);
+            pd_.z_out = zo;
+            MZK_TRY(permutation_z_device(ctx, d, &pd_, st));
+            lag[3] = pg;
+        }
         const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 8);
         Fr* dm = pd;
         Fr* dz = dm + n;
         Fr* dZ = dz + n;
-        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(jb.lookup_m), dm, n, 1);
+        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(lag[4]), dm, n, 1);
         MZK_LAUNCH_CHECK(ctx);
-        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(jb.perm_z), dz, n, 1);
+        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(lag[3]), dz, n, 1);
         MZK_LAUNCH_CHECK(ctx);
-        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(jb.lookup_Z), dZ, n, 2);
+        k_delta<<<grid, 256, 0, st>>>(reinterpret_cast<const Fr*>(lag[6]), dZ, n, 2);
         MZK_LAUNCH_CHECK(ctx);
         const BatchItem its[7] = {{jb.advice[0], pk->off_lagrange, n},  {jb.advice[1], pk->off_lagrange, n},
                                   {jb.advice[2], pk->off_lagrange, n},  {dm, pk->off_lagrange_delta, n},
                                   {dz, pk->off_lagrange_delta, n},      {dZ, pk->off_lagrange_double_delta, n},
-                                  {jb.lookup_h, pk->off_lagrange, n}};
+                                  {lag[5], pk->off_lagrange, n}};
         items.insert(items.end(), its, its + 7);
     }
     // 1. witness commitments of every proof in one batch
@@ -158,8 +218,7 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
         const Domain* d = doms[j];
         const mzk_proving_key_desc* pk = pks[j];
         const mzk_proof_job& jb = jobs[j];
-        const void* lag[kPolys] = {jb.advice[0], jb.advice[1], jb.advice[2], jb.perm_z, jb.lookup_m, jb.lookup_h,
-                                   jb.lookup_Z};
+        const void* const* lag = &lagrange[j * kPolys];
         for (int p = 0; p < kPolys; p++) {
             MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, lag[p], coeff[j * kPolys + p], st));
             MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, coeff[j * kPolys + p], ext[j * kPolys + p], st));

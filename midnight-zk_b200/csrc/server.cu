@@ -178,13 +178,14 @@ struct mzk_server {
 namespace {
 
 // device scratch of one proof of size 2^k in the proof core: coefficient and
-// extended forms of seven polynomials, three delta forms, four limbs, plus the
+// extended forms of seven polynomials, three delta forms, four limbs, three
+// device-derived columns (z, h, Z), plus the
 // sorted MSM entries it contributes to the batched witness MSM (the largest
 // of the two batched MSMs)
 uint64_t job_scratch_bytes(const mzk::Domain* d) {
     const uint64_t n = 1ull << d->k, en = 1ull << d->ext_k;
     const uint64_t fr = 32;
-    const uint64_t polys = (7 * n + 7 * en + 3 * n + 4 * n) * fr;
+    const uint64_t polys = (7 * n + 7 * en + 3 * n + 4 * n + 3 * n) * fr;
     const uint64_t msm = 7 * n * 20 * 4;  // sorted entries of 7 MSMs (<= 20 windows)
     return polys + msm;
 }

@@ -52,6 +52,12 @@ class Setup:
         pk.srs, pk.srs_len = (dev(self.srs) if srs_ptr is None else srs_ptr), self.srs.shape[0]
         pk.off_g, pk.off_lagrange, pk.off_lagrange_delta, pk.off_lagrange_double_delta = self.offs
         pk.blinding_factors = 7
+        # Lagrange forms for device-derived z / h / Z
+        self.sigma_lag = [col(n) for _ in range(3)]
+        self.table_lag, self.sel_lag = col(n), col(n)
+        for i in range(3):
+            pk.sigma_lagrange[i] = dev(self.sigma_lag[i])
+        pk.table_lagrange, pk.selector_lagrange = dev(self.table_lag), dev(self.sel_lag)
         self.pk = pk
         self.rnd = rnd
 

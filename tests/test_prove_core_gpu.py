@@ -35,3 +35,39 @@ def test_prove_core_batch_equals_single(ctx):
         assert np.array_equal(st.g.prove_core_device(st.pk, [j])[0], together[i])
     # the plain form (every MSM its own call) gives the same commitments
     assert np.array_equal(st.g.prove_core_device(st.pk, jobs[:2], per_call=True), together[:2])
+
+
+def test_device_derives_z_h_Z(ctx):
+    """Jobs that leave z, h and Z null: the device derives them (permutation
+    and logup arguments) and the commitments equal those of the same proof
+    with the oracle's z, h and Z passed in."""
+    from oracle import oracle as O
+    st = Setup(ctx, 9, seed=9)
+    n, bf = st.n, 7
+    for seed in (21, 22):
+        job, w, ch, blinds = st.job(seed)
+        pblinds = O.rand_fr(seed * 50 + 40, bf)
+        lblinds = O.rand_fr(seed * 50 + 41, bf)
+        for i in range(bf):
+            job.perm_blinds[i][:] = [int(v) for v in pblinds[i]]
+            job.lookup_blinds[i][:] = [int(v) for v in lblinds[i]]
+        z = O.permutation_z([w["a"], w["b"], w["c"]], st.sigma_lag, 3, 9, st.o.get(0), ch["beta"], ch["gamma"], bf,
+                            pblinds.reshape(1, bf, 4))[0]
+        (h,), Z = O.logup([[w["a"]]], st.table_lag, st.sel_lag, w["m"], ch["beta"], bf, lblinds)
+        given = mzk.ProofJob()
+        ctypes_copy(given, job)
+        given.perm_z, given.lookup_h, given.lookup_Z = st.dev(z), st.dev(h), st.dev(Z)
+        job.perm_z = job.lookup_h = job.lookup_Z = None
+        derived = st.g.prove_core_device(st.pk, [job])[0]
+        expect = st.g.prove_core_device(st.pk, [given])[0]
+        assert np.array_equal(derived, expect)
+        # and z alone derived, h and Z given
+        mixed = mzk.ProofJob()
+        ctypes_copy(mixed, given)
+        mixed.perm_z = None
+        assert np.array_equal(st.g.prove_core_device(st.pk, [mixed])[0], expect)
+
+
+def ctypes_copy(dst, src):
+    import ctypes
+    ctypes.memmove(ctypes.byref(dst), ctypes.byref(src), ctypes.sizeof(src))
