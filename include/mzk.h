@@ -235,6 +235,12 @@ int mzk_eval_polynomial_device(mzk_ctx *ctx, const uint64_t *poly, size_t n, con
                                uint64_t out[4]);
 /* kate_division (utils/arithmetic.rs:106-125): q[0..n-1) = a(X) / (X - b). */
 int mzk_kate_division_device(mzk_ctx *ctx, const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q);
+/* poly_inner_product of multi_open (proofs/src/poly/kzg/mod.rs:125-147):
+ * out[i] = sum_p scalars[p] * polys[p][i], each polynomial zero-extended to
+ * out_len = the longest length.  polys: m device pointers (host array), lens:
+ * their lengths (host), scalars: m Fr (host). */
+int mzk_poly_inner_product_device(mzk_ctx *ctx, const uint64_t *const *polys, const size_t *lens, size_t m,
+                                  const uint64_t *scalars, uint64_t *out, size_t out_len);
 
 /* Permutation argument, permutation/prover.rs:81-255: the z polynomial of each
  * set of chunk_len columns (Lagrange form, n = 2^k values each), blinding rows

@@ -71,6 +71,7 @@ SIGNATURES = {
     "mzk_eval_polynomial_device": (_i32, [_vp, ctypes.c_void_p, _sz, _u64p, _u64p]),
     "mzk_kate_division_device": (_i32, [_vp, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p]),
     "mzk_permutation_z_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
+    "mzk_poly_inner_product_device": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p, _sz]),
     "mzk_logup_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_create": (_i32, [_vp, _u32, _u32, _u64, _u32, ctypes.POINTER(_vp)]),
     "mzk_server_add_key": (_i32, [_vp, _vp, ctypes.c_void_p]),
@@ -391,6 +392,14 @@ class Context:
         _check(lib().mzk_eval_polynomial_device(self.h, _dptr(buf), int(n), _ptr(np.ascontiguousarray(point, np.uint64)),
                                                 _ptr(out)))
         return out
+
+    def poly_inner_product_device(self, polys, lens, scalars, out, out_len):
+        """out = sum_p scalars[p] polys[p] (kzg/mod.rs:125-147)."""
+        pp = _ptrs(polys)
+        ll = (ctypes.c_size_t * max(1, len(lens)))(*[int(x) for x in lens])
+        sc = np.ascontiguousarray(scalars, np.uint64).reshape(-1)
+        _check(lib().mzk_poly_inner_product_device(self.h, ctypes.addressof(pp), ctypes.addressof(ll), len(polys),
+                                                   _ptr(sc) if sc.size else None, _dptr(out), int(out_len)))
 
     def kate_division_device(self, a, n, b, q):
         _check(lib().mzk_kate_division_device(self.h, _dptr(a), int(n), _ptr(np.ascontiguousarray(b, np.uint64)),

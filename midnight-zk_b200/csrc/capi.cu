@@ -4,6 +4,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/mzk.h"
 #include "grand.hpp"
@@ -501,6 +502,25 @@ int mzk_kate_division_device(mzk_ctx* ctx, const uint64_t* a, size_t n, const ui
     MZK_TRY(mzk::kate_division_device(&ctx->impl, a, n, b, q, ctx->impl.stream));
     MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
     return mzk::OK;
+}
+
+int mzk_poly_inner_product_device(mzk_ctx* ctx, const uint64_t* const* polys, const size_t* lens, size_t m,
+                                  const uint64_t* scalars, uint64_t* out, size_t out_len) {
+    if (int s = check_ctx(ctx)) return s;
+    if ((m && (!polys || !lens || !scalars)) || (out_len && !out) || m >= (1u << 20)) return mzk::ERR_ARG;
+    size_t longest = 0;
+    for (size_t p = 0; p < m; p++) {
+        if (lens[p] && !polys[p]) return mzk::ERR_ARG;
+        longest = lens[p] > longest ? lens[p] : longest;
+    }
+    if (longest > out_len) {
+        mzk::set_error("poly_inner_product: out_len shorter than the longest polynomial");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    std::vector<uint64_t> l64(lens, lens + m);
+    return mzk::poly_inner_product_device(&ctx->impl, polys, l64.data(), (uint32_t)m, scalars, out, out_len,
+                                          ctx->impl.stream);
 }
 
 int mzk_permutation_z_device(mzk_ctx* ctx, mzk_domain* d, const mzk_permutation_desc* desc) {

@@ -441,6 +441,43 @@ Status logup_device(Context* ctx, const Domain* d, const mzk_logup_desc* desc, c
     return OK;
 }
 
+namespace {
+// out[i] = sum_p s_p polys[p][i] (i < len_p), polys and lengths in device tables
+__global__ void k_inner_product(const Fr* const* __restrict__ polys, const uint64_t* __restrict__ lens,
+                                const Fr* __restrict__ scalars, uint32_t m, Fr* __restrict__ out, uint64_t out_len) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < out_len; i += stride) {
+        Fr acc = fr_zero();
+        for (uint32_t p = 0; p < m; p++)
+            if (i < lens[p]) acc = fr_add(acc, fr_mul(polys[p][i], scalars[p]));
+        out[i] = acc;
+    }
+}
+}  // namespace
+
+Status poly_inner_product_device(Context* ctx, const uint64_t* const* polys, const uint64_t* lens, uint32_t m,
+                                 const uint64_t* scalars, void* out, uint64_t out_len, cudaStream_t st) {
+    if (out_len == 0) return OK;
+    // one device table: m pointers, m lengths, m scalars (staged through pinned memory)
+    const size_t bytes = (size_t)m * (8 + 8 + 32);
+    void *d_tab, *h_tab;
+    MZK_TRY(ctx->ensure("grand_ip_tab", bytes + 64, &d_tab));
+    MZK_TRY(ctx->ensure_pinned(bytes + 64, &h_tab));
+    char* h = static_cast<char*>(h_tab);
+    std::memcpy(h, polys, (size_t)m * 8);
+    std::memcpy(h + (size_t)m * 8, lens, (size_t)m * 8);
+    std::memcpy(h + (size_t)m * 16, scalars, (size_t)m * 32);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_tab, h_tab, bytes, cudaMemcpyHostToDevice, st));
+    const char* d = static_cast<const char*>(d_tab);
+    k_inner_product<<<grid_for(ctx, out_len, kThreads), kThreads, 0, st>>>(
+        reinterpret_cast<const Fr* const*>(d), reinterpret_cast<const uint64_t*>(d + (size_t)m * 8),
+        reinterpret_cast<const Fr*>(d + (size_t)m * 16), m, static_cast<Fr*>(out), out_len);
+    MZK_LAUNCH_CHECK(ctx);
+    // the pinned table is reused by the next call: finish this one first
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    return OK;
+}
+
 Status batch_invert_device(Context* ctx, void* a, uint64_t n, cudaStream_t st) {
     return batch_invert(ctx, static_cast<Fr*>(a), n, st);
 }

@@ -15,6 +15,10 @@ Status eval_polynomial_device(Context* ctx, const void* poly, uint64_t n, const 
                               cudaStream_t st);
 // q (n - 1) = a (n) / (X - b) (utils/arithmetic.rs:106-125)
 Status kate_division_device(Context* ctx, const void* a, uint64_t n, const uint64_t b[4], void* q, cudaStream_t st);
+// kzg/mod.rs:125-147 poly_inner_product over m device polynomials (host
+// tables of pointers, lengths and scalars)
+Status poly_inner_product_device(Context* ctx, const uint64_t* const* polys, const uint64_t* lens, uint32_t m,
+                                 const uint64_t* scalars, void* out, uint64_t out_len, cudaStream_t st);
 // permutation/prover.rs:81-255
 Status permutation_z_device(Context* ctx, const Domain* d, const mzk_permutation_desc* desc, cudaStream_t st);
 // logup/prover.rs:195-300

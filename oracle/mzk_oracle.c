@@ -1294,6 +1294,19 @@ void or_logup(const uint64_t *const *inputs, const uint32_t *chunk_cols, uint32_
     free(col);
 }
 
+/* kzg/mod.rs:125-147 poly_inner_product: out[i] = sum_p scalars[p] polys[p][i],
+ * shorter polynomials zero-extended to the longest (out_len). */
+void or_poly_inner_product(const uint64_t *const *polys, const size_t *lens, size_t m, const uint64_t *scalars,
+                           uint64_t *out, size_t out_len) {
+    memset(out, 0, out_len * 32);
+    for (size_t p = 0; p < m; p++)
+        for (size_t i = 0; i < lens[p] && i < out_len; i++) {
+            u64 t[4];
+            fr_mul(t, polys[p] + 4 * i, scalars + 4 * p);
+            fr_add(out + 4 * i, out + 4 * i, t);
+        }
+}
+
 /* utils/arithmetic.rs:106-125: quotient of a(X) by (X - b), n - 1 coefficients:
  * from the top, q = a_{i+1} - tmp, tmp = q * (-b). */
 void or_kate_division(const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q) {

@@ -43,6 +43,7 @@ def _load():
         "or_logup": (None, [ctypes.c_void_p, ctypes.POINTER(u32), u32, _u64p, _u64p, _u64p, sz, _u64p, u32, _u64p,
                             ctypes.c_void_p, _u64p]),
         "or_kate_division": (None, [_u64p, sz, _u64p, _u64p]),
+        "or_poly_inner_product": (None, [ctypes.c_void_p, ctypes.POINTER(sz), sz, _u64p, _u64p, sz]),
         "or_fr_add": (None, [_u64p, _u64p, _u64p]),
         "or_fr_sub": (None, [_u64p, _u64p, _u64p]),
         "or_fr_neg": (None, [_u64p, _u64p]),
@@ -335,6 +336,17 @@ def logup(chunks, table, selector, multiplicities, beta, blinding_factors, blind
                  n, P(np.ascontiguousarray(beta, np.uint64)), blinding_factors,
                  P(np.ascontiguousarray(blinds, np.uint64).reshape(-1, 4)), _ptr_array(helpers), P(agg))
     return helpers, agg
+
+
+def poly_inner_product(polys, scalars):
+    """kzg/mod.rs:125-147: sum_p scalars[p] polys[p], zero-extended."""
+    polys = [np.ascontiguousarray(p, np.uint64) for p in polys]
+    out_len = max((p.shape[0] for p in polys), default=0)
+    lens = (ctypes.c_size_t * max(1, len(polys)))(*[p.shape[0] for p in polys])
+    out = np.zeros((out_len, 4), np.uint64)
+    sc = np.ascontiguousarray(scalars, np.uint64).reshape(-1, 4)
+    lib.or_poly_inner_product(_ptr_array(polys), lens, len(polys), P(sc), P(out), out_len)
+    return out
 
 
 def kate_division(a, b):

@@ -179,3 +179,34 @@ def test_bad_descriptors_raise(ctx):
         dom.permutation_z_device([v], [v], 0, 3, np.zeros((1, 3, 4), np.uint64), ZERO, ZERO, [v])  # chunk_len 0
     with pytest.raises(mzk.MzkError):
         dom.permutation_z_device([v], [v], 1, 16, np.zeros((1, 16, 4), np.uint64), ZERO, ZERO, [v])  # bf >= n - 1
+
+
+@pytest.mark.parametrize("lens", [[5], [64, 17, 64], [1000, 3, 777, 1000, 1], [1 << 16, 1 << 14]])
+def test_poly_inner_product(ctx, lens):
+    polys = [O.rand_fr(6000 + i + len(lens), n) for i, n in enumerate(lens)]
+    scalars = O.rand_fr(6100 + len(lens), len(lens))
+    out_len = max(lens)
+    out = ctx.alloc(out_len * 32)
+    ctx.poly_inner_product_device([dev(ctx, p) for p in polys], lens, scalars, out, out_len)
+    assert np.array_equal(out.download((out_len, 4)), O.poly_inner_product(polys, scalars))
+
+
+def test_multi_open_final_step(ctx):
+    """The last step of multi_open (kzg/mod.rs:268-283) through the device
+    entry points: final = sum_p x4^p q_p, v = final(x3), pi = (final - v)/(X - x3);
+    checked against the oracle's primitives."""
+    qs = [O.rand_fr(6200 + i, n) for i, n in enumerate([300, 250, 300])]
+    x3, x4 = O.rand_fr(6300, 2)
+    pw = [ONE, x4, O.fr_op("mul", x4, x4)]
+    final = ctx.alloc(300 * 32)
+    ctx.poly_inner_product_device([dev(ctx, q) for q in qs], [300, 250, 300], np.stack(pw), final, 300)
+    v = ctx.eval_polynomial_device(final, 300, x3)
+    f = final.download((300, 4))
+    f[0] = O.fr_op("sub", f[0], v)
+    pi = ctx.alloc(299 * 32)
+    ctx.kate_division_device(dev(ctx, f), 300, x3, pi)
+    ref_final = O.poly_inner_product(qs, np.stack(pw))
+    ref_v = O.eval_polynomial(ref_final, x3)
+    assert np.array_equal(v, ref_v)
+    ref_final[0] = O.fr_op("sub", ref_final[0], ref_v)
+    assert np.array_equal(pi.download((299, 4)), O.kate_division(ref_final, x3))

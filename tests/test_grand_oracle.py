@@ -207,3 +207,17 @@ def test_logup_running_sum_is_zero_when_lookup_holds():
     assert not agg[0].any()
     assert not agg[u].any()
     assert np.array_equal(agg[n - bf:], blinds)
+
+
+def test_poly_inner_product_matches_python():
+    polys = [O.rand_fr(800, 7), O.rand_fr(801, 3), O.rand_fr(802, 5)]
+    sc = O.rand_fr(803, 3)
+    got = O.poly_inner_product(polys, sc)
+    want = []
+    for i in range(7):
+        acc = ZERO.copy()
+        for p, s in zip(polys, sc):
+            if i < p.shape[0]:
+                acc = add(acc, mul(p[i], s))
+        want.append(acc)
+    assert np.array_equal(got, np.array(want))
