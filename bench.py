@@ -401,6 +401,18 @@ def dist_init(backend):
     return world, rank, local
 
 
+def max_over_ranks_of(x, world, device):
+    """The maximum of x over the ranks of the job (the step time of a replica
+    run is its slowest rank's)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args):
     world, rank, _ = dist_init("gloo")
     if rank != 0:
@@ -466,12 +478,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, world, "cuda")
 
     for _ in range(args.warmup):
         ctx.msm_device(ds, db, n)
