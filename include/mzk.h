@@ -277,6 +277,19 @@ typedef struct {
 } mzk_logup_desc;
 int mzk_logup_device(mzk_ctx *ctx, mzk_domain *d, const mzk_logup_desc *desc);
 
+/* ---- KZG setup on the device ------------------------------------------- */
+/* ParamsKZG::unsafe_setup (proofs/src/poly/kzg/params.rs:160-209), G1 part,
+ * for the secret s (host Fr, Montgomery; the reference draws it from its rng)
+ * and the domain's n = 2^k: g[i] = [s^i]G, g_lagrange[i] = [L_i(s)]G with
+ * L_i(s) = (s^n - 1)/n * w^i/(s - w^i), g_lagrange_delta = suffix sums of
+ * g_lagrange and g_lagrange_double_delta = suffix sums of those
+ * (suffix_sum, params.rs:47-57).  Outputs: DEVICE G1Affine arrays of n points,
+ * any of them null when not wanted.  The G2 elements are not produced. */
+int mzk_srs_setup_device(mzk_ctx *ctx, mzk_domain *d, const uint64_t s[4], uint64_t *g, uint64_t *g_lagrange,
+                         uint64_t *g_lagrange_delta, uint64_t *g_lagrange_double_delta);
+/* suffix_sum (params.rs:47-57): out[i] = sum_{j >= i} in[j], n DEVICE G1Affine. */
+int mzk_g1_suffix_sum_device(mzk_ctx *ctx, const uint64_t *in, size_t n, uint64_t *out);
+
 /* ---- proving service (continuous batching over the proof core) ---------- */
 /* No reference counterpart: the reference proves one call at a time.
  * `lanes` worker threads (1..8), each with its own device context, serve one

@@ -71,6 +71,9 @@ SIGNATURES = {
     "mzk_eval_polynomial_device": (_i32, [_vp, ctypes.c_void_p, _sz, _u64p, _u64p]),
     "mzk_kate_division_device": (_i32, [_vp, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p]),
     "mzk_permutation_z_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
+    "mzk_srs_setup_device": (_i32, [_vp, _vp, _u64p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p]),
+    "mzk_g1_suffix_sum_device": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.c_void_p]),
     "mzk_poly_inner_product_device": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p, _sz]),
     "mzk_logup_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_create": (_i32, [_vp, _u32, _u32, _u64, _u32, ctypes.POINTER(_vp)]),
@@ -393,6 +396,10 @@ class Context:
                                                 _ptr(out)))
         return out
 
+    def g1_suffix_sum_device(self, d_in, n, d_out):
+        """suffix_sum (params.rs:47-57) of n device affine points."""
+        _check(lib().mzk_g1_suffix_sum_device(self.h, _dptr(d_in), int(n), _dptr(d_out)))
+
     def poly_inner_product_device(self, polys, lens, scalars, out, out_len):
         """out = sum_p scalars[p] polys[p] (kzg/mod.rs:125-147)."""
         pp = _ptrs(polys)
@@ -513,6 +520,13 @@ class EvaluationDomain:
         _check(lib().mzk_prove_core_device(self.ctx.h, self.h, ctypes.byref(pk_desc), ctypes.addressof(arr),
                                            len(jobs), PROVE_MSM_PER_CALL if per_call else 0, _ptr(out)))
         return out[:len(jobs)]
+
+    def srs_setup_device(self, s, g=None, g_lagrange=None, g_lagrange_delta=None, g_lagrange_double_delta=None):
+        """G1 part of ParamsKZG::unsafe_setup (params.rs:160-209) for secret s
+        into device buffers of n affine points (any may be None)."""
+        opt = lambda b: None if b is None else _dptr(b)
+        _check(lib().mzk_srs_setup_device(self.ctx.h, self.h, _ptr(np.ascontiguousarray(s, np.uint64)), opt(g),
+                                          opt(g_lagrange), opt(g_lagrange_delta), opt(g_lagrange_double_delta)))
 
     def permutation_z_device(self, values, sigmas, chunk_len, blinding_factors, blinds, beta, gamma, z_out):
         """z of every permutation set (permutation/prover.rs:81-255) into the

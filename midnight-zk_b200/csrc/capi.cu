@@ -11,6 +11,7 @@
 #include "ntt.hpp"
 #include "quotient.hpp"
 #include "runtime.hpp"
+#include "srs.hpp"
 
 struct mzk_ctx {
     mzk::Context impl;
@@ -521,6 +522,26 @@ int mzk_poly_inner_product_device(mzk_ctx* ctx, const uint64_t* const* polys, co
     std::vector<uint64_t> l64(lens, lens + m);
     return mzk::poly_inner_product_device(&ctx->impl, polys, l64.data(), (uint32_t)m, scalars, out, out_len,
                                           ctx->impl.stream);
+}
+
+int mzk_srs_setup_device(mzk_ctx* ctx, mzk_domain* d, const uint64_t s[4], uint64_t* g, uint64_t* g_lagrange,
+                         uint64_t* g_lagrange_delta, uint64_t* g_lagrange_double_delta) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!d || !s) return mzk::ERR_ARG;
+    Guard gd(ctx);
+    MZK_TRY(mzk::srs_setup_device(&ctx->impl, d->impl, s, g, g_lagrange, g_lagrange_delta, g_lagrange_double_delta,
+                                  ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_g1_suffix_sum_device(mzk_ctx* ctx, const uint64_t* in, size_t n, uint64_t* out) {
+    if (int st = check_ctx(ctx)) return st;
+    if (n && (!in || !out)) return mzk::ERR_ARG;
+    Guard gd(ctx);
+    MZK_TRY(mzk::g1_suffix_sum_device(&ctx->impl, in, n, out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
 }
 
 int mzk_permutation_z_device(mzk_ctx* ctx, mzk_domain* d, const mzk_permutation_desc* desc) {

@@ -77,6 +77,22 @@ __global__ void __launch_bounds__(128) k_gen_bases(uint64_t seed, uint64_t first
     }
 }
 
+// [s_i]G for scalars s_i (Montgomery) by the same fixed-base table
+__global__ void __launch_bounds__(128) k_fixed_base(const Fr* __restrict__ scalars, size_t n,
+                                                    const Affine* __restrict__ table, Affine* __restrict__ out) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const Fr r = fr_from_mont(scalars[i]);
+        Xyzz acc;
+        xyzz_set_inf(acc);
+        for (int j = 0; j < 32; j++) {
+            const uint32_t v = (r.l[j >> 2] >> (8 * (j & 3))) & 0xffu;
+            if (v) xyzz_add_affine(acc, load_affine(table, (uint32_t)(j * 256) + v));
+        }
+        out[i] = xyzz_to_affine(acc);
+    }
+}
+
 // G1 generator, canonical coordinates (curves/README.md:96-101)
 const uint64_t kGenX[6] = {0xfb3af00adb22c6bbULL, 0x6c55e83ff97a1aefULL, 0xa14e3a3f171bac58ULL,
                            0xc3688c4f9774b905ULL, 0x2695638c4fa9ac0fULL, 0x17f1d3a73197d794ULL};
@@ -116,6 +132,16 @@ Status gen_rand_fr(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* 
     if (n == 0) return OK;
     const uint32_t blocks = (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 32);
     k_rand_fr<<<blocks, 256, 0, st>>>(seed, first, n, static_cast<Fr*>(d_out));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+Status fixed_base_g1(Context* ctx, const void* d_scalars, size_t n, void* d_out, cudaStream_t st) {
+    if (n == 0) return OK;
+    MZK_TRY(ensure_gen_table(ctx));
+    const uint32_t blocks = (uint32_t)std::min<size_t>((n + 127) / 128, (size_t)ctx->num_sms * 16);
+    k_fixed_base<<<blocks, 128, 0, st>>>(static_cast<const Fr*>(d_scalars), n,
+                                         static_cast<const Affine*>(ctx->gen_table), static_cast<Affine*>(d_out));
     MZK_LAUNCH_CHECK(ctx);
     return OK;
 }

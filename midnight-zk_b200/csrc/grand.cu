@@ -478,6 +478,20 @@ Status poly_inner_product_device(Context* ctx, const uint64_t* const* polys, con
     return OK;
 }
 
+namespace {
+__global__ void k_fill(Fr* __restrict__ out, uint64_t n, Fr v) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = v;
+}
+}  // namespace
+
+Status fr_powers_device(Context* ctx, const uint64_t s[4], uint64_t n, void* out, cudaStream_t st) {
+    if (n == 0) return OK;
+    k_fill<<<grid_for(ctx, n, kThreads), kThreads, 0, st>>>(static_cast<Fr*>(out), n, to_dev(to_host(s)));
+    MZK_LAUNCH_CHECK(ctx);
+    return scan_exclusive<true>(ctx, static_cast<const Fr*>(out), static_cast<Fr*>(out), n, st);
+}
+
 Status batch_invert_device(Context* ctx, void* a, uint64_t n, cudaStream_t st) {
     return batch_invert(ctx, static_cast<Fr*>(a), n, st);
 }

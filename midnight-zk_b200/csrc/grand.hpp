@@ -8,6 +8,8 @@
 
 namespace mzk {
 
+// out[i] = s^i, i < n
+Status fr_powers_device(Context* ctx, const uint64_t s[4], uint64_t n, void* out, cudaStream_t st);
 // ff BatchInvert on n device Fr values in place (zeros stay zero)
 Status batch_invert_device(Context* ctx, void* a, uint64_t n, cudaStream_t st);
 // sum_i poly[i] point^i (utils/arithmetic.rs:59-87), result on the host

@@ -122,6 +122,8 @@ Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s, double
 
 // ---- synthetic inputs (gen.cu) ----
 Status gen_rand_fr(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t stream);
+// [s_i]G for n device scalars (Montgomery) into n device affine points
+Status fixed_base_g1(Context* ctx, const void* d_scalars, size_t n, void* d_out, cudaStream_t st);
 Status gen_bases_g1(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t stream);
 
 }  // namespace mzk

@@ -1294,6 +1294,49 @@ void or_logup(const uint64_t *const *inputs, const uint32_t *chunk_cols, uint32_
     free(col);
 }
 
+/* params.rs:47-57 suffix_sum: out[i] = sum_{j >= i} in[j] (affine in and out) */
+void or_g1_suffix_sum(const uint64_t *in, size_t n, uint64_t *out) {
+    u64 acc[18] = {0}, p[18], t[18];
+    for (size_t i = n; i-- > 0;) {
+        or_g1_from_affine(p, in + 12 * i);
+        or_g1_add(t, acc, p);
+        memcpy(acc, t, sizeof(acc));
+        or_g1_to_affine(out + 12 * i, acc);
+    }
+}
+
+/* params.rs:160-209 unsafe_setup, G1 part, for secret s and n = 2^k with the
+ * domain's root omega: g[i] = [s^i]G, lag[i] = [(s^n - 1)/n w^i/(s - w^i)]G,
+ * then the two suffix sums. */
+void or_srs_setup(const uint64_t s[4], uint32_t k, const uint64_t omega[4], uint64_t *g, uint64_t *lag,
+                  uint64_t *delta, uint64_t *ddelta) {
+    const size_t n = (size_t)1 << k;
+    u64 gen[12], sp[4], w[4], sn[4], e[1] = {(u64)n}, ninv[4], nn[4], mult[4], t[4], u[4];
+    or_g1_generator(gen);
+    memcpy(sp, FR_R, 32);
+    for (size_t i = 0; i < n; i++) {
+        or_g1_mul(g + 12 * i, gen, sp);
+        fr_mul(sp, sp, s);
+    }
+    fr_pow(sn, s, e, 1);
+    fr_sub(sn, sn, FR_R);
+    u64 nc[4] = {(u64)n, 0, 0, 0};
+    fr_mul(nn, nc, FR_R2);
+    fr_inv(ninv, nn);
+    fr_mul(mult, sn, ninv);
+    memcpy(w, FR_R, 32);
+    for (size_t i = 0; i < n; i++) {
+        fr_sub(t, s, w);
+        fr_inv(t, t);
+        fr_mul(u, mult, w);
+        fr_mul(u, u, t);
+        or_g1_mul(lag + 12 * i, gen, u);
+        fr_mul(w, w, omega);
+    }
+    or_g1_suffix_sum(lag, n, delta);
+    or_g1_suffix_sum(delta, n, ddelta);
+}
+
 /* kzg/mod.rs:125-147 poly_inner_product: out[i] = sum_p scalars[p] polys[p][i],
  * shorter polynomials zero-extended to the longest (out_len). */
 void or_poly_inner_product(const uint64_t *const *polys, const size_t *lens, size_t m, const uint64_t *scalars,

@@ -122,6 +122,9 @@ void or_logup(const uint64_t *const *inputs, const uint32_t *chunk_cols, uint32_
               uint32_t blinding_factors, const uint64_t *blinds, uint64_t *const *helpers_out,
               uint64_t *aggregator_out);
 void or_kate_division(const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q);
+void or_g1_suffix_sum(const uint64_t *in, size_t n, uint64_t *out);
+void or_srs_setup(const uint64_t s[4], uint32_t k, const uint64_t omega[4], uint64_t *g, uint64_t *lag,
+                  uint64_t *delta, uint64_t *ddelta);
 void or_poly_inner_product(const uint64_t *const *polys, const size_t *lens, size_t m, const uint64_t *scalars,
                            uint64_t *out, size_t out_len);
 

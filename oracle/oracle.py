@@ -43,6 +43,8 @@ def _load():
         "or_logup": (None, [ctypes.c_void_p, ctypes.POINTER(u32), u32, _u64p, _u64p, _u64p, sz, _u64p, u32, _u64p,
                             ctypes.c_void_p, _u64p]),
         "or_kate_division": (None, [_u64p, sz, _u64p, _u64p]),
+        "or_g1_suffix_sum": (None, [_u64p, sz, _u64p]),
+        "or_srs_setup": (None, [_u64p, u32, _u64p, _u64p, _u64p, _u64p, _u64p]),
         "or_poly_inner_product": (None, [ctypes.c_void_p, ctypes.POINTER(sz), sz, _u64p, _u64p, sz]),
         "or_fr_add": (None, [_u64p, _u64p, _u64p]),
         "or_fr_sub": (None, [_u64p, _u64p, _u64p]),
@@ -347,6 +349,23 @@ def poly_inner_product(polys, scalars):
     sc = np.ascontiguousarray(scalars, np.uint64).reshape(-1, 4)
     lib.or_poly_inner_product(_ptr_array(polys), lens, len(polys), P(sc), P(out), out_len)
     return out
+
+
+def g1_suffix_sum(points):
+    """params.rs:47-57: out[i] = sum_{j >= i} points[j] (affine)."""
+    p = np.ascontiguousarray(points, np.uint64)
+    out = np.zeros_like(p)
+    lib.or_g1_suffix_sum(P(p), p.shape[0], P(out))
+    return out
+
+
+def srs_setup(s, k):
+    """params.rs:160-209 (G1 part): (g, g_lagrange, g_lagrange_delta, g_lagrange_double_delta)."""
+    n = 1 << k
+    omega = Domain(5, k).get(0) if k >= 1 else fr_const(0)
+    outs = [np.zeros((n, 12), np.uint64) for _ in range(4)]
+    lib.or_srs_setup(P(np.ascontiguousarray(s, np.uint64)), k, P(omega), *[P(o) for o in outs])
+    return outs
 
 
 def kate_division(a, b):
