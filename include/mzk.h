@@ -289,6 +289,23 @@ int mzk_srs_setup_device(mzk_ctx *ctx, mzk_domain *d, const uint64_t s[4], uint6
                          uint64_t *g_lagrange_delta, uint64_t *g_lagrange_double_delta);
 /* suffix_sum (params.rs:47-57): out[i] = sum_{j >= i} in[j], n DEVICE G1Affine. */
 int mzk_g1_suffix_sum_device(mzk_ctx *ctx, const uint64_t *in, size_t n, uint64_t *out);
+/* G1Affine::from_compressed (curves/src/bls12_381/g1.rs:367-376) of n 48-byte
+ * ZCash encodings (DEVICE, contiguous) into n DEVICE G1Affine; status
+ * (optional DEVICE n bytes): 0 ok, 1 bad encoding, 2 not on the curve, 3 not
+ * in G1 (checked when check_subgroup != 0); invalid points are written as the
+ * identity and counted in *n_invalid (host, optional). */
+int mzk_g1_decompress_device(mzk_ctx *ctx, const uint8_t *in, size_t n, int check_subgroup, uint64_t *out,
+                             uint8_t *status, uint64_t *n_invalid);
+/* ParamsKZG::read_custom with SerdeFormat::Processed (params.rs:283-350), G1
+ * part: bytes (host) = k as u32 LE, 2^k compressed g, 2^k compressed
+ * g_lagrange (the G2 elements that follow are not read).  Points are
+ * decompressed and checked on the device; the delta bases are derived as the
+ * reference does after reading.  Outputs: DEVICE arrays of capacity points
+ * (any may be null); returns MZK_ERR_ARG on a short buffer, 2^k > capacity or
+ * an invalid point encoding. */
+int mzk_srs_read_processed(mzk_ctx *ctx, const uint8_t *bytes, size_t len, size_t capacity, uint32_t *k_out,
+                           uint64_t *g, uint64_t *g_lagrange, uint64_t *g_lagrange_delta,
+                           uint64_t *g_lagrange_double_delta);
 
 /* ---- proving service (continuous batching over the proof core) ---------- */
 /* No reference counterpart: the reference proves one call at a time.

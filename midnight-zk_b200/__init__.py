@@ -74,6 +74,10 @@ SIGNATURES = {
     "mzk_srs_setup_device": (_i32, [_vp, _vp, _u64p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p]),
     "mzk_g1_suffix_sum_device": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.c_void_p]),
+    "mzk_g1_decompress_device": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                        _u64p]),
+    "mzk_srs_read_processed": (_i32, [_vp, ctypes.c_void_p, _sz, _sz, ctypes.POINTER(_u32), ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "mzk_poly_inner_product_device": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p, _sz]),
     "mzk_logup_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_create": (_i32, [_vp, _u32, _u32, _u64, _u32, ctypes.POINTER(_vp)]),
@@ -395,6 +399,23 @@ class Context:
         _check(lib().mzk_eval_polynomial_device(self.h, _dptr(buf), int(n), _ptr(np.ascontiguousarray(point, np.uint64)),
                                                 _ptr(out)))
         return out
+
+    def g1_decompress_device(self, d_in, n, d_out, d_status=None, check_subgroup=True):
+        """G1Affine::from_compressed of n device encodings; returns the invalid count."""
+        bad = np.zeros(1, np.uint64)
+        _check(lib().mzk_g1_decompress_device(self.h, _dptr(d_in), int(n), 1 if check_subgroup else 0, _dptr(d_out),
+                                              None if d_status is None else _dptr(d_status), _ptr(bad)))
+        return int(bad[0])
+
+    def srs_read_processed(self, data, capacity, g=None, g_lagrange=None, g_lagrange_delta=None,
+                           g_lagrange_double_delta=None):
+        """ParamsKZG::read_custom (Processed) from host bytes into device buffers; returns k."""
+        buf = np.frombuffer(bytes(data), np.uint8)
+        k = _u32()
+        opt = lambda b: None if b is None else _dptr(b)
+        _check(lib().mzk_srs_read_processed(self.h, buf.ctypes.data, buf.size, int(capacity), ctypes.byref(k), opt(g),
+                                            opt(g_lagrange), opt(g_lagrange_delta), opt(g_lagrange_double_delta)))
+        return k.value
 
     def g1_suffix_sum_device(self, d_in, n, d_out):
         """suffix_sum (params.rs:47-57) of n device affine points."""

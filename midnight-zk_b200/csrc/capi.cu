@@ -544,6 +544,28 @@ int mzk_g1_suffix_sum_device(mzk_ctx* ctx, const uint64_t* in, size_t n, uint64_
     return mzk::OK;
 }
 
+int mzk_g1_decompress_device(mzk_ctx* ctx, const uint8_t* in, size_t n, int check_subgroup, uint64_t* out,
+                             uint8_t* status, uint64_t* n_invalid) {
+    if (int st = check_ctx(ctx)) return st;
+    if (n && (!in || !out)) return mzk::ERR_ARG;
+    Guard gd(ctx);
+    MZK_TRY(mzk::g1_decompress_device(&ctx->impl, in, n, check_subgroup, out, status, n_invalid, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_srs_read_processed(mzk_ctx* ctx, const uint8_t* bytes, size_t len, size_t capacity, uint32_t* k_out,
+                           uint64_t* g, uint64_t* g_lagrange, uint64_t* g_lagrange_delta,
+                           uint64_t* g_lagrange_double_delta) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!bytes || !k_out) return mzk::ERR_ARG;
+    Guard gd(ctx);
+    MZK_TRY(mzk::srs_read_processed(&ctx->impl, bytes, len, capacity, k_out, g, g_lagrange, g_lagrange_delta,
+                                    g_lagrange_double_delta, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
 int mzk_permutation_z_device(mzk_ctx* ctx, mzk_domain* d, const mzk_permutation_desc* desc) {
     if (int s = check_ctx(ctx)) return s;
     if (!d || !desc) return mzk::ERR_ARG;

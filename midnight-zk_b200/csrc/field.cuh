@@ -49,6 +49,12 @@ struct FpP {
              : i == 4 ? 0x53c758bau : i == 5 ? 0x5f489857u : i == 6 ? 0x70525745u : i == 7 ? 0x77ce5853u
              : i == 8 ? 0xa256ec6du : i == 9 ? 0x5c071a97u : i == 10 ? 0xfa80e493u : 0x15f65ec3u;
     }
+    // R^2 mod p (R = 2^384): canonical -> Montgomery by one multiplication
+    __host__ __device__ static constexpr uint32_t r2(int i) {
+        return i == 0 ? 0x1c341746u : i == 1 ? 0xf4df1f34u : i == 2 ? 0x09d104f1u : i == 3 ? 0x0a76e6a6u
+             : i == 4 ? 0x4c95b6d5u : i == 5 ? 0x8de5476cu : i == 6 ? 0x939d83c0u : i == 7 ? 0x67eb88a9u
+             : i == 8 ? 0xb519952du : i == 9 ? 0x9a793e85u : i == 10 ? 0x92cae3aau : 0x11988fe5u;
+    }
 };
 
 struct FrP {

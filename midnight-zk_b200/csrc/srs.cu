@@ -103,6 +103,135 @@ __global__ void k_lag_scal(const Fr* __restrict__ wlo, const Fr* __restrict__ wh
         scal[i] = fr_mul(fr_mul(mult, fr_mul(wlo[i & 4095u], whi[i >> 12])), scal[i]);
 }
 
+// ---- compressed G1 points (ZCash format, G1Affine::from_compressed,
+// curves/src/bls12_381/g1.rs:367-376) ----
+struct Exp12 {
+    uint32_t l[12];
+};
+struct FrOrder {
+    uint32_t l[8];
+};
+
+// (p + 1) / 4 and the group order r as 32-bit limbs, from the moduli
+Exp12 sqrt_exponent() {
+    Exp12 e;
+    uint64_t carry = 1;
+    for (int i = 0; i < 12; i++) {
+        const uint64_t v = (uint64_t)FpP::mod(i) + carry;
+        e.l[i] = (uint32_t)v;
+        carry = v >> 32;
+    }
+    for (int i = 0; i < 12; i++) e.l[i] = (e.l[i] >> 2) | (i < 11 ? e.l[i + 1] << 30 : 0u);
+    return e;
+}
+FrOrder group_order() {
+    FrOrder r;
+    for (int i = 0; i < 8; i++) r.l[i] = FrP::mod(i);
+    return r;
+}
+
+__device__ __forceinline__ Fp fp_pow_limbs(const Fp& a, const uint32_t* e, int limbs) {
+    Fp acc = fp_one();
+    for (int i = limbs - 1; i >= 0; i--)
+        for (int bit = 31; bit >= 0; bit--) {
+            acc = fp_sqr(acc);
+            if ((e[i] >> bit) & 1u) acc = fp_mul(acc, a);
+        }
+    return acc;
+}
+
+// status: 0 ok, 1 bad encoding, 2 not on the curve, 3 not in G1
+__global__ void __launch_bounds__(kThreads) k_g1_decompress(const uint8_t* __restrict__ in, uint64_t n, int check,
+                                                            Exp12 sqrt_e, FrOrder order, Affine* __restrict__ out,
+                                                            uint8_t* __restrict__ status,
+                                                            unsigned long long* __restrict__ invalid) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint8_t* b = in + 48 * i;
+        uint32_t w[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) {  // limb k little-endian from big-endian bytes
+            const uint8_t* q = b + 44 - 4 * k;
+            w[k] = ((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) | q[3];
+        }
+        const uint32_t flags = b[0] & 0xe0u;
+        w[11] &= 0x1fffffffu;
+        uint8_t st = 0;
+        Affine p;
+        p.x = fp_zero();
+        p.y = fp_zero();
+        if (!(flags & 0x80u)) {
+            st = 1;
+        } else if (flags & 0x40u) {
+            uint32_t rest = b[0] & 0x3fu;
+#pragma unroll
+            for (int k = 0; k < 11; k++) rest |= w[k];
+            rest |= w[11];
+            if (rest) st = 1;
+        } else {
+            // x < p
+            bool less = false, decided = false;
+            for (int k = 11; k >= 0 && !decided; k--)
+                if (w[k] != FpP::mod(k)) {
+                    less = w[k] < FpP::mod(k);
+                    decided = true;
+                }
+            if (!less) {
+                st = 1;
+            } else {
+                Fp x, r2;
+#pragma unroll
+                for (int k = 0; k < 12; k++) {
+                    x.l[k] = w[k];
+                    r2.l[k] = FpP::r2(k);
+                }
+                x = fp_canonical(fp_mul(x, r2));
+                Fp four_m = fp_add(fp_add(fp_one(), fp_one()), fp_add(fp_one(), fp_one()));
+                const Fp rhs = fp_add(fp_mul(fp_sqr(x), x), four_m);
+                Fp y = fp_canonical(fp_pow_limbs(rhs, sqrt_e.l, 12));
+                if (!fp_is_zero(fp_sub(fp_sqr(y), rhs))) {
+                    st = 2;
+                } else {
+                    // the sign flag marks the larger root: y > p - y as integers,
+                    // so compare the canonical (non-Montgomery) values
+                    const Fp ny = fp_canonical(fp_sub(fp_zero(), y));
+                    Fp one_raw;
+#pragma unroll
+                    for (int k = 0; k < 12; k++) one_raw.l[k] = k == 0 ? 1u : 0u;
+                    const Fp yi = fp_canonical(fp_mul(y, one_raw)), nyi = fp_canonical(fp_mul(ny, one_raw));
+                    bool y_larger = false;
+                    decided = false;
+                    for (int k = 11; k >= 0 && !decided; k--)
+                        if (yi.l[k] != nyi.l[k]) {
+                            y_larger = yi.l[k] > nyi.l[k];
+                            decided = true;
+                        }
+                    if (y_larger != ((flags & 0x20u) != 0)) y = ny;
+                    p.x = x;
+                    p.y = y;
+                    if (check) {  // [r] P must be the identity
+                        Xyzz acc;
+                        xyzz_set_inf(acc);
+                        for (int k = 7; k >= 0; k--)
+                            for (int bit = 31; bit >= 0; bit--) {
+                                acc = xyzz_dbl(acc);
+                                if ((order.l[k] >> bit) & 1u) xyzz_add_affine(acc, p);
+                            }
+                        if (!xyzz_is_inf(acc)) st = 3;
+                    }
+                }
+            }
+        }
+        if (st) {
+            p.x = fp_zero();
+            p.y = fp_zero();
+            atomicAdd(invalid, 1ull);
+        }
+        out[i] = p;
+        if (status) status[i] = st;
+    }
+}
+
 Fr to_dev_fr(const host::Fr4& h) {
     Fr r;
     std::memcpy(r.l, h.l, 32);
@@ -118,6 +247,66 @@ Status g1_suffix_sum_device(Context* ctx, const void* in, uint64_t n, void* out,
     MZK_TRY(suffix_scan<Affine>(ctx, static_cast<const Affine*>(in), static_cast<Xyzz*>(x), n, st));
     k_to_affine<<<blocks_for(ctx, n), kThreads, 0, st>>>(static_cast<const Xyzz*>(x), n, static_cast<Affine*>(out));
     MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+Status g1_decompress_device(Context* ctx, const void* in, uint64_t n, int check_subgroup, void* out,
+                            uint8_t* status, uint64_t* invalid, cudaStream_t st) {
+    if (invalid) *invalid = 0;
+    if (n == 0) return OK;
+    void* cnt;
+    MZK_TRY(ctx->ensure("srs_invalid", 16, &cnt));
+    MZK_CUDA_CHECK(cudaMemsetAsync(cnt, 0, 8, st));
+    k_g1_decompress<<<blocks_for(ctx, n), kThreads, 0, st>>>(static_cast<const uint8_t*>(in), n, check_subgroup,
+                                                             sqrt_exponent(), group_order(), static_cast<Affine*>(out),
+                                                             status, static_cast<unsigned long long*>(cnt));
+    MZK_LAUNCH_CHECK(ctx);
+    if (invalid) {
+        void* h;
+        MZK_TRY(ctx->ensure_pinned(16, &h));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(h, cnt, 8, cudaMemcpyDeviceToHost, st));
+        MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+        *invalid = *static_cast<const uint64_t*>(h);
+    }
+    return OK;
+}
+
+Status srs_read_processed(Context* ctx, const uint8_t* bytes, size_t len, uint64_t capacity, uint32_t* k_out,
+                          void* g, void* lag, void* delta, void* ddelta, cudaStream_t st) {
+    if (len < 4) {
+        set_error("srs_read: buffer shorter than the k field");
+        return ERR_ARG;
+    }
+    uint32_t k;
+    std::memcpy(&k, bytes, 4);  // u32 little-endian (params.rs:265)
+    if (k > 31 || (1ull << k) > capacity) {
+        set_error("srs_read: k = " + std::to_string(k) + " exceeds the output capacity");
+        return ERR_ARG;
+    }
+    const uint64_t n = 1ull << k;
+    if (len < 4 + 2 * n * 48) {
+        set_error("srs_read: buffer shorter than 2^k compressed g and g_lagrange points");
+        return ERR_ARG;
+    }
+    *k_out = k;
+    void* comp;
+    MZK_TRY(ctx->ensure("srs_comp", 2 * n * 48, &comp));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(comp, bytes + 4, 2 * n * 48, cudaMemcpyHostToDevice, st));
+    void* lag_out = lag;
+    if (!lag_out) MZK_TRY(ctx->ensure("srs_lag", n * sizeof(Affine), &lag_out));
+    uint64_t bad_g = 0, bad_l = 0;
+    if (g) MZK_TRY(g1_decompress_device(ctx, comp, n, 1, g, nullptr, &bad_g, st));
+    MZK_TRY(g1_decompress_device(ctx, static_cast<const uint8_t*>(comp) + n * 48, n, 1, lag_out, nullptr, &bad_l, st));
+    if (bad_g || bad_l) {
+        set_error("srs_read: invalid point encoding (" + std::to_string(bad_g + bad_l) + " points)");
+        return ERR_ARG;
+    }
+    // the delta bases are derived after reading (params.rs:340-341)
+    if (!delta && !ddelta) return OK;
+    void* delta_out = delta;
+    if (!delta_out) MZK_TRY(ctx->ensure("srs_delta", n * sizeof(Affine), &delta_out));
+    MZK_TRY(g1_suffix_sum_device(ctx, lag_out, n, delta_out, st));
+    if (ddelta) MZK_TRY(g1_suffix_sum_device(ctx, delta_out, n, ddelta, st));
     return OK;
 }
 

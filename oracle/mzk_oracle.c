@@ -404,6 +404,59 @@ void or_g1_compress(uint8_t out[48], const uint64_t aff[12]) {
     if (!geq_n(ny, y, 6)) out[0] |= 0x20;
 }
 
+/* The reverse of or_g1_compress, as G1Affine::from_compressed (g1.rs:367-376:
+ * blst_p1_uncompress, then the G1 membership check): compression flag set;
+ * the infinity flag with every other bit zero is the identity; otherwise
+ * x < p, y = (x^3 + 4)^((p+1)/4) must square back (p = 3 mod 4), the sign
+ * flag picks y > (p-1)/2, and with check_subgroup [r]P must be the identity.
+ * Returns 0 ok, 1 bad encoding, 2 not on the curve, 3 not in G1. */
+int or_g1_decompress(uint64_t out[12], const uint8_t in[48], int check_subgroup) {
+    aff_t *p = (aff_t *)out;
+    memset(out, 0, 96);
+    const uint8_t flags = in[0] & 0xe0;
+    if (!(flags & 0x80)) return 1;
+    if (flags & 0x40) {
+        if (in[0] & 0x3f) return 1;
+        for (int i = 1; i < 48; i++)
+            if (in[i]) return 1;
+        return 0;
+    }
+    u64 x[6] = {0};
+    for (int i = 0; i < 48; i++) x[i / 8] |= (u64)(i == 47 ? (in[0] & 0x1f) : in[47 - i]) << (8 * (i % 8));
+    if (geq_n(x, FP_MOD, 6)) return 1;
+    u64 xm[6], rhs[6], y[6], t[6], e[6], one[6] = {1, 0, 0, 0, 0, 0};
+    fp_mul(xm, x, FP_R2);
+    fp_mul(t, xm, xm);
+    fp_mul(t, t, xm);
+    fp_add(rhs, t, FP_B);
+    /* e = (p + 1) / 4 */
+    add_n(e, FP_MOD, one, 6);
+    for (int i = 0; i < 6; i++) e[i] = (e[i] >> 2) | (i < 5 ? e[i + 1] << 62 : 0);
+    memcpy(y, FP_R, 48);
+    for (int i = 6 * 64 - 1; i >= 0; i--) {
+        fp_mul(y, y, y);
+        if ((e[i / 64] >> (i % 64)) & 1) fp_mul(y, y, rhs);
+    }
+    fp_mul(t, y, y);
+    if (!fp_eq(t, rhs)) return 2;
+    u64 yc[6], nyc[6], z[6] = {0}, ny[6];
+    or_fp_to_canonical(yc, y);
+    fp_sub(ny, z, y);
+    or_fp_to_canonical(nyc, ny);
+    const int larger = !geq_n(nyc, yc, 6); /* y > p - y */
+    if (larger != !!(flags & 0x20)) memcpy(y, ny, 48);
+    memcpy(p->x, xm, 48);
+    memcpy(p->y, y, 48);
+    if (check_subgroup) {
+        jac_t r;
+        u64 order[4];
+        memcpy(order, FR_MOD, 32);
+        jac_mul_canonical(&r, p, order);
+        if (!fp_is_zero(r.z)) return 3;
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------------- */
 /* MSM                                                                       */
 /* ------------------------------------------------------------------------- */

@@ -60,6 +60,8 @@ int  or_g1_is_on_curve_affine(const uint64_t aff[12]);
 void or_g1_mul(uint64_t out_affine[12], const uint64_t aff[12], const uint64_t scalar_mont[4]);
 /* 48-byte compressed encoding (ZCash BLS12-381 format) */
 void or_g1_compress(uint8_t out[48], const uint64_t aff[12]);
+/* from_compressed: 0 ok, 1 bad encoding, 2 not on the curve, 3 not in G1 */
+int or_g1_decompress(uint64_t out[12], const uint8_t in[48], int check_subgroup);
 
 /* ---- MSM ---------------------------------------------------------------- */
 /* naive sum of double-and-add products, result affine */

@@ -44,6 +44,7 @@ def _load():
                             ctypes.c_void_p, _u64p]),
         "or_kate_division": (None, [_u64p, sz, _u64p, _u64p]),
         "or_g1_suffix_sum": (None, [_u64p, sz, _u64p]),
+        "or_g1_decompress": (i32, [_u64p, _u8p, i32]),
         "or_srs_setup": (None, [_u64p, u32, _u64p, _u64p, _u64p, _u64p, _u64p]),
         "or_poly_inner_product": (None, [ctypes.c_void_p, ctypes.POINTER(sz), sz, _u64p, _u64p, sz]),
         "or_fr_add": (None, [_u64p, _u64p, _u64p]),
@@ -349,6 +350,14 @@ def poly_inner_product(polys, scalars):
     sc = np.ascontiguousarray(scalars, np.uint64).reshape(-1, 4)
     lib.or_poly_inner_product(_ptr_array(polys), lens, len(polys), P(sc), P(out), out_len)
     return out
+
+
+def g1_decompress(b48, check_subgroup=True):
+    """(status, affine point): 0 ok, 1 bad encoding, 2 not on the curve, 3 not in G1."""
+    buf = np.frombuffer(bytes(b48), np.uint8).copy()
+    out = np.zeros(12, np.uint64)
+    st = lib.or_g1_decompress(P(out), buf.ctypes.data_as(_u8p), 1 if check_subgroup else 0)
+    return st, out
 
 
 def g1_suffix_sum(points):

@@ -328,3 +328,26 @@ def test_eval_polynomial_matches_horner_and_dft():
     b = O.rand_fr(93, 64)
     lag = d.coeff_to_lagrange(b)
     assert np.array_equal(lag[5], O.eval_polynomial(b, O.fr_pow(d.get(0), 5)))
+
+
+def test_g1_decompress_inverts_compress():
+    """from_compressed of to_compressed: the generator (the reference's README
+    coordinates), random points and the identity; a cleared compression flag,
+    x >= p and set padding bits of the identity are rejected."""
+    pts = O.gen_bases(31, 16)
+    pts[2] = 0
+    pts = np.concatenate([pts, O.g1_generator().reshape(1, 12)])
+    for p in pts:
+        st, q = O.g1_decompress(O.g1_compress(p))
+        assert st == 0 and np.array_equal(q, p)
+    c = bytearray(O.g1_compress(O.g1_generator()))
+    c[0] &= 0x7f
+    assert O.g1_decompress(c)[0] == 1
+    p_bytes = bytearray((0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab).to_bytes(48, "big"))
+    p_bytes[0] |= 0x80
+    assert O.g1_decompress(p_bytes)[0] == 1
+    ident = bytearray(48)
+    ident[0] = 0xc0
+    assert O.g1_decompress(ident)[0] == 0
+    ident[47] = 1
+    assert O.g1_decompress(ident)[0] == 1

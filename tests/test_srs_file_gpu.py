@@ -1,0 +1,90 @@
+"""SRS file reading on the B200 (ParamsKZG::read_custom, SerdeFormat::
+Processed, params.rs:283-350) and G1Affine::from_compressed on the device,
+against the oracle: valid points, the identity, bad encodings, points off
+the curve and points on the curve outside G1."""
+import numpy as np
+import pytest
+
+from _loader import load
+from oracle import oracle as O
+
+mzk = load()
+pytestmark = pytest.mark.gpu
+
+P_MOD = 0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = mzk.Context(0)
+    yield c
+    c.close()
+
+
+def encodings():
+    pts = O.gen_bases(41, 40)
+    pts[7] = 0
+    enc = [bytes(O.g1_compress(p)) for p in pts]
+    bad = bytearray(enc[0])
+    bad[0] &= 0x7f                                   # compression flag cleared
+    enc.append(bytes(bad))
+    over = bytearray((P_MOD + 5).to_bytes(48, "big"))
+    over[0] |= 0x80                                  # x >= p
+    enc.append(bytes(over))
+    ident_pad = bytearray(48)
+    ident_pad[0], ident_pad[20] = 0xc0, 1            # identity with a stray bit
+    enc.append(bytes(ident_pad))
+    for x in range(1, 40):                           # small x: off the curve or outside G1
+        b = bytearray(48)
+        b[47], b[0] = x, 0x80 | (0x20 if x % 2 else 0)
+        enc.append(bytes(b))
+    return enc
+
+
+@pytest.mark.parametrize("check", [True, False])
+def test_decompress_matches_oracle(ctx, check):
+    enc = encodings()
+    n = len(enc)
+    raw = np.frombuffer(b"".join(enc), np.uint8)
+    d_in, d_out, d_st = ctx.alloc(raw.nbytes), ctx.alloc(n * 96), ctx.alloc(n)
+    d_in.upload(raw)
+    bad = ctx.g1_decompress_device(d_in, n, d_out, d_st, check_subgroup=check)
+    got = d_out.download((n, 12))
+    st = d_st.download((n,), np.uint8)
+    want = [O.g1_decompress(e, check) for e in enc]
+    assert [int(s) for s in st] == [w[0] for w in want]
+    assert bad == sum(1 for w in want if w[0])
+    for i, (s, p) in enumerate(want):
+        assert np.array_equal(got[i], p if s == 0 else np.zeros(12, np.uint64)), i
+    assert {int(s) for s in st} >= ({0, 1, 2, 3} if check else {0, 1, 2})
+
+
+def srs_file(k, s):
+    g, lag, _, _ = O.srs_setup(s, k)
+    body = b"".join(bytes(O.g1_compress(p)) for p in g) + b"".join(bytes(O.g1_compress(p)) for p in lag)
+    return k.to_bytes(4, "little") + body + bytes(192)  # the G2 elements are not read
+
+
+def test_read_processed_matches_setup(ctx):
+    k = 7
+    s = O.rand_fr(99, 1)[0]
+    data = srs_file(k, s)
+    n = 1 << k
+    bufs = [ctx.alloc(n * 96) for _ in range(4)]
+    assert ctx.srs_read_processed(data, n, *bufs) == k
+    for b, w in zip(bufs, O.srs_setup(s, k)):
+        assert np.array_equal(b.download((n, 12)), w)
+
+
+def test_read_processed_rejects(ctx):
+    k = 4
+    n = 1 << k
+    data = bytearray(srs_file(k, O.rand_fr(98, 1)[0]))
+    bufs = [ctx.alloc(n * 96) for _ in range(4)]
+    with pytest.raises(mzk.MzkError):
+        ctx.srs_read_processed(bytes(data[:100]), n, *bufs)          # short buffer
+    with pytest.raises(mzk.MzkError):
+        ctx.srs_read_processed(bytes(data), n // 2, *bufs)           # capacity below 2^k
+    data[4 + 3 * 48 + 47] ^= 1                                       # corrupt one point of g
+    with pytest.raises(mzk.MzkError):
+        ctx.srs_read_processed(bytes(data), n, *bufs)
