@@ -273,14 +273,28 @@ __global__ void k_perm_num(PermCols pc, Fr beta, Fr gamma, const Fr* __restrict_
         mv[i] = acc;
     }
 }
-// z[i] = (i < n - bf ? z[i] : blinds[i - (n - bf)]) * corr
-__global__ void k_perm_finish(Fr* __restrict__ z, uint32_t n, uint32_t bf, const Fr* __restrict__ blinds, Fr corr,
-                              int scale) {
+constexpr uint32_t kMaxPermSets = 16;
+struct SetPtrs {
+    Fr* z[kMaxPermSets];
+};
+// corr[0] = 1, corr[s] = corr[s-1] * z_{s-1}[n - bf - 1] (the uncorrected last
+// products, read before any set is corrected); one thread, sets in order
+__global__ void k_perm_corrections(SetPtrs sp, uint32_t sets, uint32_t last, Fr* __restrict__ corr) {
+    Fr c = fr_one();
+    for (uint32_t s = 0; s < sets; s++) {
+        corr[s] = c;
+        c = fr_mul(c, sp.z[s][last]);
+    }
+}
+// z[i] = (i < n - bf ? z[i] : blinds[i - (n - bf)]) * corr (multiplying by
+// one where the reference skips the product leaves the value unchanged)
+__global__ void k_perm_finish(Fr* __restrict__ z, uint32_t n, uint32_t bf, const Fr* __restrict__ blinds,
+                              const Fr* __restrict__ corr) {
+    const Fr c = *corr;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        Fr v = i < n - bf ? z[i] : blinds[i - (n - bf)];
-        if (scale) v = fr_mul(v, corr);
-        z[i] = v;
+        const Fr v = i < n - bf ? z[i] : blinds[i - (n - bf)];
+        z[i] = fr_mul(v, c);
     }
 }
 
@@ -329,9 +343,14 @@ Status permutation_z_device(Context* ctx, const Domain* d, const mzk_permutation
         return ERR_ARG;
     }
     const uint32_t sets = (desc->n_cols + desc->chunk_len - 1) / desc->chunk_len;
-    void *mv_buf, *dbl;
+    if (sets > kMaxPermSets) {
+        set_error("permutation_z: at most 16 sets");
+        return ERR_ARG;
+    }
+    void *mv_buf, *dbl, *corr;
     MZK_TRY(ctx->ensure("perm_mv", (size_t)n * sizeof(Fr), &mv_buf));
     MZK_TRY(ctx->ensure("perm_blinds", ((size_t)sets * bf + 1) * sizeof(Fr), &dbl));
+    MZK_TRY(ctx->ensure("perm_corr", (size_t)sets * sizeof(Fr), &corr));
     if (bf)
         MZK_CUDA_CHECK(cudaMemcpyAsync(dbl, desc->blinds, (size_t)sets * bf * sizeof(Fr), cudaMemcpyHostToDevice, st));
     Fr* mv = (Fr*)mv_buf;
@@ -362,23 +381,15 @@ Status permutation_z_device(Context* ctx, const Domain* d, const mzk_permutation
         Fr* z = reinterpret_cast<Fr*>(desc->z_out[s]);
         MZK_TRY(scan_exclusive<true>(ctx, mv, z, n, st));
     }
-    // the uncorrected last products z_s[n - bf - 1] (before the blinds) -> corrections
-    void* host_last;
-    MZK_TRY(ctx->ensure_pinned((size_t)sets * 32, &host_last));
-    for (uint32_t s = 0; s < sets; s++)
-        MZK_CUDA_CHECK(cudaMemcpyAsync(static_cast<char*>(host_last) + 32 * s,
-                                       reinterpret_cast<const Fr*>(desc->z_out[s]) + (n - bf - 1), 32,
-                                       cudaMemcpyDeviceToHost, st));
-    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
-    std::vector<host::Fr4> last(sets);
-    for (uint32_t s = 0; s < sets; s++) last[s] = to_host(static_cast<const uint64_t*>(host_last) + 4 * s);
-    host::Fr4 corr = host::fr_one();
+    // corrections from the uncorrected last products z_s[n - bf - 1], on the
+    // device (no host round trip), then blinds and corrections per set
+    SetPtrs sp;
+    for (uint32_t s = 0; s < sets; s++) sp.z[s] = reinterpret_cast<Fr*>(desc->z_out[s]);
+    k_perm_corrections<<<1, 1, 0, st>>>(sp, sets, n - bf - 1, (Fr*)corr);
+    MZK_LAUNCH_CHECK(ctx);
     for (uint32_t s = 0; s < sets; s++) {
-        const bool scale = std::memcmp(corr.l, host::fr_one().l, 32) != 0;
-        k_perm_finish<<<grid, kThreads, 0, st>>>(reinterpret_cast<Fr*>(desc->z_out[s]), n, bf,
-                                                 (const Fr*)dbl + (size_t)s * bf, to_dev(corr), scale ? 1 : 0);
+        k_perm_finish<<<grid, kThreads, 0, st>>>(sp.z[s], n, bf, (const Fr*)dbl + (size_t)s * bf, (const Fr*)corr + s);
         MZK_LAUNCH_CHECK(ctx);
-        corr = host::fr_mul(corr, last[s]);
     }
     return OK;
 }

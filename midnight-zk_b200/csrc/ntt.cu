@@ -39,6 +39,7 @@ namespace {
 constexpr uint32_t kTileLog = 11;
 constexpr uint32_t kTile = 1u << kTileLog;  // elements per block
 constexpr int kNttThreads = 256;
+static_assert(kTile % kNttThreads == 0, "a tile is a whole number of elements per thread");
 constexpr uint32_t kLoBits = 12;            // low table: w^i for i < 4096
 
 // w^e from the split tables (e < N)
@@ -154,19 +155,28 @@ __global__ void __launch_bounds__(kNttThreads, 2) k_ntt_dif_pass(PassArgs a) {
 
     for (uint32_t u = threadIdx.x; u < R / 2; u += blockDim.x)
         sw.set(tw_swz(u), root_pow(a.tlo, a.thi, u << (a.log_n - a.log_r)));
-    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
+    // all of a thread's global loads are issued before the first is used
+    constexpr int kPer = kTile / kNttThreads;
+    Fr v[kPer];
+    uint32_t vidx[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+        const uint32_t e = threadIdx.x + (uint32_t)q * kNttThreads;
         const uint32_t m = e >> log_b, b = e & (B - 1);
         const uint32_t c = c0 + (b << cstep_log);
-        const uint32_t idx = ((c >> log_m) << a.log_s) + (m << log_m) + (c & ((1u << log_m) - 1));
-        Fr v = fr_zero();
-        if (idx < a.n_real) {
-            v = a.in[idx];
-            if (a.use_pre) {
-                const uint32_t r3 = idx % 3;
-                if (r3) v = fr_mul(v, a.pre[r3]);
-            }
+        vidx[q] = ((c >> log_m) << a.log_s) + (m << log_m) + (c & ((1u << log_m) - 1));
+        v[q] = fr_zero();
+        if (e < tile && vidx[q] < a.n_real) v[q] = a.in[vidx[q]];
+    }
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+        const uint32_t e = threadIdx.x + (uint32_t)q * kNttThreads;
+        if (e >= tile) continue;
+        if (a.use_pre && vidx[q] < a.n_real) {
+            const uint32_t r3 = vidx[q] % 3;
+            if (r3) v[q] = fr_mul(v[q], a.pre[r3]);
         }
-        sx.set(swz(e), v);
+        sx.set(swz(e), v[q]);
     }
     __syncthreads();
     // stages in rounds of three (radix 8), the last round of one or two
