@@ -287,6 +287,13 @@ int mzk_logup_device(mzk_ctx *ctx, mzk_domain *d, const mzk_logup_desc *desc);
  * any of them null when not wanted.  The G2 elements are not produced. */
 int mzk_srs_setup_device(mzk_ctx *ctx, mzk_domain *d, const uint64_t s[4], uint64_t *g, uint64_t *g_lagrange,
                          uint64_t *g_lagrange_delta, uint64_t *g_lagrange_double_delta);
+/* g_to_lagrange (proofs/src/utils/arithmetic.rs:34-54): out[i] = (1/n)
+ * sum_j w^(-ij) g[j] for the domain's n = 2^k (DEVICE G1Affine arrays). */
+int mzk_g1_to_lagrange_device(mzk_ctx *ctx, mzk_domain *d, const uint64_t *g, uint64_t *out);
+/* ParamsKZG::downsize (params.rs:96-107) for the domain's k: g_lagrange =
+ * g_to_lagrange(g[0..n)), then its two suffix sums (outputs may be null). */
+int mzk_srs_downsize_device(mzk_ctx *ctx, mzk_domain *d, const uint64_t *g, uint64_t *g_lagrange,
+                            uint64_t *g_lagrange_delta, uint64_t *g_lagrange_double_delta);
 /* suffix_sum (params.rs:47-57): out[i] = sum_{j >= i} in[j], n DEVICE G1Affine. */
 int mzk_g1_suffix_sum_device(mzk_ctx *ctx, const uint64_t *in, size_t n, uint64_t *out);
 /* G1Affine::from_compressed (curves/src/bls12_381/g1.rs:367-376) of n 48-byte

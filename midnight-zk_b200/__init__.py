@@ -74,6 +74,8 @@ SIGNATURES = {
     "mzk_srs_setup_device": (_i32, [_vp, _vp, _u64p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p]),
     "mzk_g1_suffix_sum_device": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.c_void_p]),
+    "mzk_g1_to_lagrange_device": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p]),
+    "mzk_srs_downsize_device": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "mzk_g1_decompress_device": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                         _u64p]),
     "mzk_srs_read_processed": (_i32, [_vp, ctypes.c_void_p, _sz, _sz, ctypes.POINTER(_u32), ctypes.c_void_p,
@@ -548,6 +550,16 @@ class EvaluationDomain:
         opt = lambda b: None if b is None else _dptr(b)
         _check(lib().mzk_srs_setup_device(self.ctx.h, self.h, _ptr(np.ascontiguousarray(s, np.uint64)), opt(g),
                                           opt(g_lagrange), opt(g_lagrange_delta), opt(g_lagrange_double_delta)))
+
+    def g1_to_lagrange_device(self, g, out):
+        """g_to_lagrange (utils/arithmetic.rs:34-54) of the first n device points of g."""
+        _check(lib().mzk_g1_to_lagrange_device(self.ctx.h, self.h, _dptr(g), _dptr(out)))
+
+    def srs_downsize_device(self, g, g_lagrange=None, g_lagrange_delta=None, g_lagrange_double_delta=None):
+        """ParamsKZG::downsize (params.rs:96-107) to this domain's k."""
+        opt = lambda b: None if b is None else _dptr(b)
+        _check(lib().mzk_srs_downsize_device(self.ctx.h, self.h, _dptr(g), opt(g_lagrange), opt(g_lagrange_delta),
+                                             opt(g_lagrange_double_delta)))
 
     def permutation_z_device(self, values, sigmas, chunk_len, blinding_factors, blinds, beta, gamma, z_out):
         """z of every permutation set (permutation/prover.rs:81-255) into the

@@ -535,6 +535,26 @@ int mzk_srs_setup_device(mzk_ctx* ctx, mzk_domain* d, const uint64_t s[4], uint6
     return mzk::OK;
 }
 
+int mzk_g1_to_lagrange_device(mzk_ctx* ctx, mzk_domain* d, const uint64_t* g, uint64_t* out) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!d || !g || !out) return mzk::ERR_ARG;
+    Guard gd(ctx);
+    MZK_TRY(mzk::g1_to_lagrange_device(&ctx->impl, d->impl, g, out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_srs_downsize_device(mzk_ctx* ctx, mzk_domain* d, const uint64_t* g, uint64_t* g_lagrange,
+                            uint64_t* g_lagrange_delta, uint64_t* g_lagrange_double_delta) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!d || !g) return mzk::ERR_ARG;
+    Guard gd(ctx);
+    MZK_TRY(mzk::srs_downsize_device(&ctx->impl, d->impl, g, g_lagrange, g_lagrange_delta, g_lagrange_double_delta,
+                                     ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
 int mzk_g1_suffix_sum_device(mzk_ctx* ctx, const uint64_t* in, size_t n, uint64_t* out) {
     if (int st = check_ctx(ctx)) return st;
     if (n && (!in || !out)) return mzk::ERR_ARG;

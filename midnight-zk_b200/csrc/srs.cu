@@ -232,6 +232,65 @@ __global__ void __launch_bounds__(kThreads) k_g1_decompress(const uint8_t* __res
     }
 }
 
+// ---- g_to_lagrange (proofs/src/utils/arithmetic.rs:34-54): inverse FFT over
+// G1 points.  Decimation-in-frequency radix-2 stages in global memory (the
+// butterflies are compute-bound: one variable-base scalar multiplication
+// each), then bit reversal, the 1/n scaling and normalisation in one pass.
+
+// [k] P for a canonical scalar k (8 x 32-bit), MSB-first double-and-add
+__device__ Xyzz xyzz_mul_scalar(const Xyzz& p, const Fr& k) {
+    Xyzz acc;
+    xyzz_set_inf(acc);
+    int top = 7;
+    while (top >= 0 && k.l[top] == 0) top--;
+    for (int limb = top; limb >= 0; limb--)
+        for (int bit = 31; bit >= 0; bit--) {
+            acc = xyzz_dbl(acc);
+            if ((k.l[limb] >> bit) & 1u) acc = xyzz_add(acc, p);
+        }
+    return acc;
+}
+__device__ __forceinline__ Xyzz xyzz_neg(const Xyzz& p) {
+    Xyzz r = p;
+    r.y = fp_sub(fp_zero(), p.y);
+    return r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_aff_to_xyzz(const Affine* __restrict__ in, uint64_t n,
+                                                          Xyzz* __restrict__ out) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = xyzz_from_affine(in[i]);
+}
+// one DIF stage of half-size h = 2^log_h: (a, b) -> (a + b, (a - b) w^(pos n / 2h))
+__global__ void __launch_bounds__(kThreads) k_ec_dif_stage(Xyzz* __restrict__ a, uint32_t log_n, uint32_t log_h,
+                                                           const Fr* __restrict__ wlo, const Fr* __restrict__ whi) {
+    const uint32_t half = 1u << (log_n - 1);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < half; q += stride) {
+        const uint32_t pos = q & ((1u << log_h) - 1);
+        const uint32_t i0 = ((q >> log_h) << (log_h + 1)) + pos, i1 = i0 + (1u << log_h);
+        const Xyzz x0 = a[i0], x1 = a[i1];
+        a[i0] = xyzz_add(x0, x1);
+        Xyzz d = xyzz_add(x0, xyzz_neg(x1));
+        if (pos) {
+            const uint32_t e = pos << (log_n - 1 - log_h);  // w_n^(pos n / 2h)
+            d = xyzz_mul_scalar(d, fr_from_mont(fr_mul(wlo[e & 4095u], whi[e >> 12])));
+        }
+        a[i1] = d;
+    }
+}
+// out[bitrev(i)] = affine([n_inv] a[i])
+__global__ void __launch_bounds__(kThreads) k_ec_finish(const Xyzz* __restrict__ a, uint32_t log_n, Fr n_inv_canon,
+                                                        Affine* __restrict__ out) {
+    const uint32_t n = 1u << log_n;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t o = log_n ? (__brev(i) >> (32 - log_n)) : 0u;
+        out[o] = xyzz_to_affine(xyzz_mul_scalar(a[i], n_inv_canon));
+    }
+}
+
 Fr to_dev_fr(const host::Fr4& h) {
     Fr r;
     std::memcpy(r.l, h.l, 32);
@@ -302,6 +361,40 @@ Status srs_read_processed(Context* ctx, const uint8_t* bytes, size_t len, uint64
         return ERR_ARG;
     }
     // the delta bases are derived after reading (params.rs:340-341)
+    if (!delta && !ddelta) return OK;
+    void* delta_out = delta;
+    if (!delta_out) MZK_TRY(ctx->ensure("srs_delta", n * sizeof(Affine), &delta_out));
+    MZK_TRY(g1_suffix_sum_device(ctx, lag_out, n, delta_out, st));
+    if (ddelta) MZK_TRY(g1_suffix_sum_device(ctx, delta_out, n, ddelta, st));
+    return OK;
+}
+
+Status g1_to_lagrange_device(Context* ctx, const Domain* d, const void* g, void* out, cudaStream_t st) {
+    const uint32_t k = d->k, n = 1u << k;
+    void* x;
+    MZK_TRY(ctx->ensure("srs_ecfft", (size_t)n * sizeof(Xyzz), &x));
+    Xyzz* a = static_cast<Xyzz*>(x);
+    k_aff_to_xyzz<<<blocks_for(ctx, n), kThreads, 0, st>>>(static_cast<const Affine*>(g), n, a);
+    MZK_LAUNCH_CHECK(ctx);
+    for (int log_h = (int)k - 1; log_h >= 0; log_h--) {
+        k_ec_dif_stage<<<blocks_for(ctx, n / 2), kThreads, 0, st>>>(a, k, (uint32_t)log_h, d->lo[1], d->hi[1]);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    // 1/n as a canonical scalar (the domain's ifft divisor is n^-1 in Montgomery form)
+    host::Fr4 one_raw = {};
+    one_raw.l[0] = 1;
+    const host::Fr4 n_inv_canon = host::fr_mul(d->ifft_div, one_raw);
+    k_ec_finish<<<blocks_for(ctx, n), kThreads, 0, st>>>(a, k, to_dev_fr(n_inv_canon), static_cast<Affine*>(out));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+Status srs_downsize_device(Context* ctx, const Domain* d, const void* g, void* lag, void* delta, void* ddelta,
+                           cudaStream_t st) {
+    const uint64_t n = 1ull << d->k;
+    void* lag_out = lag;
+    if (!lag_out) MZK_TRY(ctx->ensure("srs_lag", n * sizeof(Affine), &lag_out));
+    MZK_TRY(g1_to_lagrange_device(ctx, d, g, lag_out, st));
     if (!delta && !ddelta) return OK;
     void* delta_out = delta;
     if (!delta_out) MZK_TRY(ctx->ensure("srs_delta", n * sizeof(Affine), &delta_out));

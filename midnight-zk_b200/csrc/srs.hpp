@@ -17,6 +17,13 @@ Status g1_decompress_device(Context* ctx, const void* in, uint64_t n, int check_
 // ParamsKZG::read_custom, SerdeFormat::Processed (params.rs:283-350), G1 part
 Status srs_read_processed(Context* ctx, const uint8_t* bytes, size_t len, uint64_t capacity, uint32_t* k_out,
                           void* g, void* lag, void* delta, void* ddelta, cudaStream_t st);
+// g_to_lagrange (utils/arithmetic.rs:34-54): out = inverse FFT of the n = 2^k
+// points g over the domain, scaled by 1/n, affine
+Status g1_to_lagrange_device(Context* ctx, const Domain* d, const void* g, void* out, cudaStream_t st);
+// ParamsKZG::downsize (params.rs:96-107): Lagrange and delta bases of a
+// smaller domain from the first 2^k points of g
+Status srs_downsize_device(Context* ctx, const Domain* d, const void* g, void* lag, void* delta, void* ddelta,
+                           cudaStream_t st);
 // params.rs:47-57: out[i] = sum_{j >= i} in[j] (affine, n points)
 Status g1_suffix_sum_device(Context* ctx, const void* in, uint64_t n, void* out, cudaStream_t st);
 

@@ -73,3 +73,50 @@ def test_commitments_agree_across_bases(ctx):
     trapdoor = O.g1_mul(O.g1_generator(), O.eval_polynomial(coeff, s))
     for c in commits:
         assert np.array_equal(c, trapdoor)
+
+
+@pytest.mark.parametrize("k", [1, 4, 6])
+def test_g_to_lagrange_matches_dft(ctx, k):
+    """g_to_lagrange (utils/arithmetic.rs:34-54) against the inverse DFT by
+    definition: out[i] = sum_j (n^-1 w^-ij) g[j], one oracle MSM per row."""
+    n = 1 << k
+    pts = O.gen_bases(120 + k, n)
+    dom = mzk.EvaluationDomain(ctx, 5, k)
+    d_in, d_out = ctx.alloc(n * 96), ctx.alloc(n * 96)
+    d_in.upload(pts)
+    dom.g1_to_lagrange_device(d_in, d_out)
+    got = d_out.download((n, 12))
+    od = O.Domain(5, k)
+    w_inv, n_inv = od.get(1), od.get(5)
+    for i in range(n):
+        wi = O.fr_pow(w_inv, i)
+        c = [n_inv]
+        for _ in range(n - 1):
+            c.append(O.fr_op("mul", c[-1], wi))
+        assert np.array_equal(got[i], O.msm_naive(np.stack(c), pts)), i
+
+
+def test_g_to_lagrange_of_setup_is_setup_lagrange(ctx):
+    """Two algorithms, one answer: the inverse FFT of [s^i]G equals the
+    Lagrange bases computed from s directly."""
+    k = 10
+    n = 1 << k
+    s = O.rand_fr(130, 1)[0]
+    dom, bufs, setup_pts = setup(ctx, k, s)
+    out = ctx.alloc(n * 96)
+    dom.g1_to_lagrange_device(bufs[0], out)
+    assert np.array_equal(out.download((n, 12)), setup_pts[1])
+
+
+def test_downsize(ctx):
+    """ParamsKZG::downsize (params.rs:96-107): the k = 7 bases rebuilt from
+    the k = 10 monomial bases equal the k = 7 setup with the same secret."""
+    s = O.rand_fr(131, 1)[0]
+    _, big, _ = setup(ctx, 10, s)
+    small = mzk.EvaluationDomain(ctx, 5, 7)
+    n = 1 << 7
+    outs = [ctx.alloc(n * 96) for _ in range(3)]
+    small.srs_downsize_device(big[0], *outs)
+    want = O.srs_setup(s, 7)
+    for o, w in zip(outs, want[1:]):
+        assert np.array_equal(o.download((n, 12)), w)
