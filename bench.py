@@ -388,6 +388,85 @@ def measure_serving(mzk, ctx, keys, n_requests, max_batch, lanes, mem_budget):
     return out
 
 
+P_FP = 0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab
+R_INV_FP = pow(1 << 384, -1, P_FP)
+
+
+def compress_g1(p):
+    """ZCash compressed encoding of an affine point (12 x u64 Montgomery),
+    as G1Affine::to_compressed writes it (input preparation for the bench)."""
+    if not any(int(v) for v in p):
+        return bytes([0xC0]) + bytes(47)
+    x = sum(int(v) << (64 * i) for i, v in enumerate(p[:6])) * R_INV_FP % P_FP
+    y = sum(int(v) << (64 * i) for i, v in enumerate(p[6:])) * R_INV_FP % P_FP
+    b = bytearray(x.to_bytes(48, "big"))
+    b[0] |= 0x80 | (0x20 if y > P_FP - y else 0)
+    return bytes(b)
+
+
+def measure_setup_and_scans(mzk, ctx, stream):
+    """The prover's column scans and the KZG setup path at production sizes,
+    device time (CUDA events on the library's stream); inputs resident."""
+    import numpy as np
+    import torch
+
+    def timed(fn, reps=3):
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    n24 = 1 << 24
+    a = ctx.gen_rand_fr(0xA1, n24)
+    x = np.array([12345, 0, 0, 0], np.uint64)
+    ms = timed(lambda: ctx.batch_invert_device(a, n24))
+    out["batch_invert_2^24"] = {"ms": round(ms, 3), "elements_per_s": round(n24 / ms * 1e3, 1)}
+    ms = timed(lambda: ctx.eval_polynomial_device(a, n24, x))
+    out["eval_polynomial_2^24"] = {"ms": round(ms, 3), "elements_per_s": round(n24 / ms * 1e3, 1)}
+    q = ctx.alloc(n24 * 32)
+    ms = timed(lambda: ctx.kate_division_device(a, n24, x, q))
+    out["kate_division_2^24"] = {"ms": round(ms, 3), "elements_per_s": round(n24 / ms * 1e3, 1)}
+    del q
+    k = 20
+    n = 1 << k
+    dom = mzk.EvaluationDomain(ctx, 5, k)
+    cols = [ctx.gen_rand_fr(0xB0 + i, n) for i in range(9)]
+    z = ctx.alloc(n * 32)
+    beta, gamma = np.array([7, 0, 0, 0], np.uint64), np.array([11, 0, 0, 0], np.uint64)
+    blinds = np.zeros((1, 7, 4), np.uint64)
+    ms = timed(lambda: dom.permutation_z_device(cols[:3], cols[3:6], 3, 7, blinds, beta, gamma, [z]))
+    out["permutation_z_k20_3cols"] = {"ms": round(ms, 3), "rows_per_s": round(n / ms * 1e3, 1)}
+    h, agg = ctx.alloc(n * 32), ctx.alloc(n * 32)
+    ms = timed(lambda: dom.logup_device([[cols[0]]], cols[6], cols[7], cols[8], 7, blinds[0], beta, [h], agg))
+    out["logup_k20_1input"] = {"ms": round(ms, 3), "rows_per_s": round(n / ms * 1e3, 1)}
+    bufs = [ctx.alloc(n * 96) for _ in range(4)]
+    s = np.array([0x1234567, 0x89, 0, 0], np.uint64)
+    ms = timed(lambda: dom.srs_setup_device(s, *bufs), reps=1)
+    out["srs_setup_k20"] = {"ms": round(ms, 2), "points_per_s": round(4 * n / ms * 1e3, 1),
+                            "note": "g, g_lagrange, delta, double delta (4 x 2^20 points)"}
+    small = mzk.EvaluationDomain(ctx, 5, 16)
+    ms = timed(lambda: small.g1_to_lagrange_device(bufs[0], bufs[1]), reps=1)
+    out["g_to_lagrange_k16"] = {"ms": round(ms, 2), "points_per_s": round((1 << 16) / ms * 1e3, 1),
+                                "note": "inverse FFT over G1, one scalar multiplication per butterfly"}
+    # compressed points: 2^12 of the setup's g, compressed on the host, repeated
+    m = 1 << 12
+    pts = bufs[0].download((m, 12))
+    comp = np.frombuffer(b"".join(compress_g1(p) for p in pts) * (n // m), np.uint8)
+    d_comp = ctx.alloc(comp.nbytes)
+    d_comp.upload(comp)
+    ms = timed(lambda: ctx.g1_decompress_device(d_comp, n, bufs[2]), reps=1)
+    out["g1_decompress_2^20"] = {"ms": round(ms, 2), "points_per_s": round(n / ms * 1e3, 1),
+                                 "note": "square root, sign and the [r]P subgroup check per point"}
+    small.close()
+    dom.close()
+    return out
+
+
 def dist_init(backend):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -572,6 +651,7 @@ def run_ours(args):
             extra_prover["serving"] = measure_serving(mzk, ctx, keys, args.serve_requests, 16, 2, 8 << 30)
             keys.close()
             del keys
+            extra_prover["setup_and_scans"] = measure_setup_and_scans(mzk, ctx, stream)
         ds = ctx.gen_rand_fr(0xC0FFEE + rank, n)
         db = ctx.gen_bases(0xBA5E + rank, n)
 
