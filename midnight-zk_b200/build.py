@@ -33,15 +33,23 @@ def build(force=False, verbose=False, extra=()):
     OBJ.mkdir(exist_ok=True)
     LIB.parent.mkdir(exist_ok=True)
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list((PKG.parent / "include").glob("*.h"))
-    objs = []
+    objs, jobs = [], []
     for src in sorted(CSRC.glob("*.cu")):
         obj = OBJ / (src.stem + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            jobs.append([NVCC, *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)])
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(run, cmd) for cmd in jobs]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
         if verbose:
