@@ -132,7 +132,11 @@ FrOrder group_order() {
 
 __device__ __forceinline__ Fp fp_pow_limbs(const Fp& a, const uint32_t* e, int limbs) {
     Fp acc = fp_one();
+    // kept rolled: a full unroll of 384 square-and-multiply steps only
+    // inflates the code and the compile time
+#pragma unroll 1
     for (int i = limbs - 1; i >= 0; i--)
+#pragma unroll 1
         for (int bit = 31; bit >= 0; bit--) {
             acc = fp_sqr(acc);
             if ((e[i] >> bit) & 1u) acc = fp_mul(acc, a);
@@ -212,7 +216,9 @@ __global__ void __launch_bounds__(kThreads) k_g1_decompress(const uint8_t* __res
                     if (check) {  // [r] P must be the identity
                         Xyzz acc;
                         xyzz_set_inf(acc);
+#pragma unroll 1
                         for (int k = 7; k >= 0; k--)
+#pragma unroll 1
                             for (int bit = 31; bit >= 0; bit--) {
                                 acc = xyzz_dbl(acc);
                                 if ((order.l[k] >> bit) & 1u) xyzz_add_affine(acc, p);
@@ -243,7 +249,9 @@ __device__ Xyzz xyzz_mul_scalar(const Xyzz& p, const Fr& k) {
     xyzz_set_inf(acc);
     int top = 7;
     while (top >= 0 && k.l[top] == 0) top--;
+#pragma unroll 1
     for (int limb = top; limb >= 0; limb--)
+#pragma unroll 1
         for (int bit = 31; bit >= 0; bit--) {
             acc = xyzz_dbl(acc);
             if ((k.l[limb] >> bit) & 1u) acc = xyzz_add(acc, p);
