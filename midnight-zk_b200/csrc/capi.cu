@@ -116,6 +116,7 @@ Context::~Context() {
     if (pinned) cudaFreeHost(pinned);
     if (gen_table) cudaFree(gen_table);
     if (ev_copy) cudaEventDestroy(ev_copy);
+    if (ev_copy2) cudaEventDestroy(ev_copy2);
     for (int i = 0; i < kMaxEvents; i++)
         if (prof_ev[i]) cudaEventDestroy(prof_ev[i]);
     if (stream) cudaStreamDestroy(stream);
@@ -178,6 +179,7 @@ int mzk_ctx_create(int device, mzk_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->impl.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->impl.copy_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->impl.ev_copy, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->impl.ev_copy2, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         mzk::set_error(std::string("context setup: ") + cudaGetErrorString(e));
         delete c;
@@ -306,6 +308,9 @@ int mzk_msm_g1_device(mzk_ctx* ctx, const uint64_t* d_scalars, const uint64_t* d
     return mzk::msm_g1_device(&ctx->impl, d_scalars, d_bases, n, out, ctx->impl.stream, nullptr);
 }
 
+// host-buffer MSMs of at least this many points upload and compute in two parts
+constexpr size_t kPipelineMinPoints = size_t(1) << 20;
+
 int mzk_msm_g1(mzk_ctx* ctx, const uint64_t* scalars, const uint64_t* bases, size_t n, uint64_t out[18]) {
     if (int s = check_ctx(ctx)) return s;
     if (!out || (n && (!scalars || !bases))) {
@@ -321,12 +326,27 @@ int mzk_msm_g1(mzk_ctx* ctx, const uint64_t* scalars, const uint64_t* bases, siz
     void *ds, *db;
     MZK_TRY(c->ensure("in_scalars", n * 32, &ds));
     MZK_TRY(c->ensure("in_bases", n * 96, &db));
-    // scalars first on the compute stream (the digit passes need only them),
-    // bases on the copy stream, overlapping the sort
-    MZK_CUDA_CHECK(cudaMemcpyAsync(ds, scalars, n * 32, cudaMemcpyHostToDevice, c->stream));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(db, bases, n * 96, cudaMemcpyHostToDevice, c->copy_stream));
+    char* dsc = static_cast<char*>(ds);
+    char* dba = static_cast<char*>(db);
+    const char* hsc = reinterpret_cast<const char*>(scalars);
+    const char* hba = reinterpret_cast<const char*>(bases);
+    // Scalars first on the compute stream (the digit passes need only them),
+    // bases on the copy stream, overlapping the sort.  Large MSMs go in two
+    // parts: the first ~30 % of the points is sorted and accumulated while the
+    // rest is still uploading (the accumulation of 30 % of the points takes
+    // about as long as the upload of the other 70 %).
+    const size_t first = n >= kPipelineMinPoints ? (n * 3 / 10) & ~(size_t)1023 : n;
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dsc, hsc, first * 32, cudaMemcpyHostToDevice, c->stream));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dba, hba, first * 96, cudaMemcpyHostToDevice, c->copy_stream));
     MZK_CUDA_CHECK(cudaEventRecord(c->ev_copy, c->copy_stream));
-    return mzk::msm_g1_device(c, ds, db, n, out, c->stream, c->ev_copy);
+    if (first == n) return mzk::msm_g1_device(c, ds, db, n, out, c->stream, c->ev_copy);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dsc + first * 32, hsc + first * 32, (n - first) * 32, cudaMemcpyHostToDevice,
+                                   c->copy_stream));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dba + first * 96, hba + first * 96, (n - first) * 96, cudaMemcpyHostToDevice,
+                                   c->copy_stream));
+    MZK_CUDA_CHECK(cudaEventRecord(c->ev_copy2, c->copy_stream));
+    const mzk::MsmPart parts[2] = {{0, first, nullptr, c->ev_copy}, {first, n, c->ev_copy2, c->ev_copy2}};
+    return mzk::msm_g1_parts(c, ds, db, n, out, c->stream, parts, 2);
 }
 
 int mzk_gen_rand_fr_device(mzk_ctx* ctx, uint64_t seed, uint64_t first, size_t n, uint64_t* d_out) {

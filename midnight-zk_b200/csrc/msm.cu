@@ -452,8 +452,12 @@ __device__ __forceinline__ uint32_t find_win(const WinDev* wins, uint32_t n_wins
     return lo;
 }
 
+// buckets2/offsets2 (optional): a second bucket set over the same keys (the
+// second part of a pipelined MSM), added bucket by bucket
 __global__ void __launch_bounds__(kReduceThreads) k_group_sums(const Xyzz* __restrict__ buckets,
                                                                const uint32_t* __restrict__ offsets,
+                                                               const Xyzz* __restrict__ buckets2,
+                                                               const uint32_t* __restrict__ offsets2,
                                                                const WinDev* __restrict__ wins, uint32_t n_wins,
                                                                uint32_t total_groups, Xyzz* __restrict__ run_out,
                                                                Xyzz* __restrict__ tot_out) {
@@ -467,6 +471,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_group_sums(const Xyzz* __res
     for (int b = (1 << wd.glen_log) - 1; b >= 0; b--) {
         const uint32_t key = key0 + (uint32_t)b;
         if (offsets[key + 1] > offsets[key]) run = xyzz_add(run, load_xyzz(&buckets[key]));
+        if (buckets2 && offsets2[key + 1] > offsets2[key]) run = xyzz_add(run, load_xyzz(&buckets2[key]));
         tot = xyzz_add(tot, run);
     }
     store_xyzz(&run_out[gid], run);
@@ -558,11 +563,12 @@ uint32_t plane_split(uint64_t slots, uint32_t max_groups, int num_sms) {
 // steps 1-3 on `st`.  partial holds slots * split plane partials and may be
 // q itself when split == 1; q holds slots plane sums.  Returns the launch
 // error, if any; adds the launches to *launches when given.
-cudaError_t launch_reduce(const Xyzz* buckets, const uint32_t* offsets, const WinDev* d_wins, uint32_t n_wins,
-                          uint64_t groups, uint64_t slots, uint32_t split, Xyzz* run, Xyzz* tot, Xyzz* partial,
-                          Xyzz* q, Xyzz* wsum, uint64_t* launches, cudaStream_t st) {
+cudaError_t launch_reduce(const Xyzz* buckets, const uint32_t* offsets, const Xyzz* buckets2,
+                          const uint32_t* offsets2, const WinDev* d_wins, uint32_t n_wins, uint64_t groups,
+                          uint64_t slots, uint32_t split, Xyzz* run, Xyzz* tot, Xyzz* partial, Xyzz* q, Xyzz* wsum,
+                          uint64_t* launches, cudaStream_t st) {
     k_group_sums<<<(uint32_t)((groups + kReduceThreads - 1) / kReduceThreads), kReduceThreads, 0, st>>>(
-        buckets, offsets, d_wins, n_wins, (uint32_t)groups, run, tot);
+        buckets, offsets, buckets2, offsets2, d_wins, n_wins, (uint32_t)groups, run, tot);
     k_plane_sums<<<(uint32_t)(slots * split), kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
         run, tot, d_wins, n_wins, split, split == 1 ? q : partial);
     uint64_t n = 3;
@@ -608,11 +614,33 @@ int msm_pick_window(size_t n) {
 
 Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
                      cudaStream_t st, cudaEvent_t bases_ready) {
+    const MsmPart whole{0, n, nullptr, bases_ready};
+    return msm_g1_parts(ctx, d_scalars, d_bases, n, out18, st, &whole, 1);
+}
+
+// Each part is sorted and accumulated into its own bucket set, in order on
+// `st`; the running-sum groups then add the bucket sets key by key.  The sort
+// and accumulation scratch (counts, sorted entries, chunk partials) is shared:
+// stream order finishes one part's use before the next part's writes.
+Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
+                    cudaStream_t st, const MsmPart* parts, int n_parts) {
     std::memset(out18, 0, 18 * 8);
     if (n == 0) return OK;
     if (n >= 0x80000000ull) {
         set_error("msm: n must be < 2^31");
         return ERR_ARG;
+    }
+    if (n_parts < 1 || n_parts > kMaxMsmParts || parts[0].begin != 0 || parts[n_parts - 1].end != n) {
+        set_error("msm: parts must cover [0, n) in 1.." + std::to_string(kMaxMsmParts) + " pieces");
+        return ERR_ARG;
+    }
+    size_t max_part = 0;
+    for (int p = 0; p < n_parts; p++) {
+        if (parts[p].end <= parts[p].begin || (p > 0 && parts[p].begin != parts[p - 1].end)) {
+            set_error("msm: parts must be non-empty and contiguous");
+            return ERR_ARG;
+        }
+        max_part = std::max(max_part, parts[p].end - parts[p].begin);
     }
     const int c = ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(n);
     if (c < 5 || c > 24) {
@@ -620,7 +648,7 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
         return ERR_ARG;
     }
     const MsmShape sh = make_shape(c, group_log_for(make_shape(c).keys));
-    const size_t entries_cap = (size_t)sh.windows * n;
+    const size_t entries_cap = (size_t)sh.windows * max_part;
     if (entries_cap >= 0xffffffffull) {
         set_error("msm: n * windows exceeds 2^32 entries");
         return ERR_ARG;
@@ -632,11 +660,16 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     const uint32_t acc_blocks = (uint32_t)(ctx->num_sms * acc_blocks_per_sm);
     const uint32_t acc_threads = acc_blocks * kAccThreads;
 
-    void *counts, *offsets, *sorted, *buckets, *partials, *owner, *run, *tot, *planes, *wsum;
+    void *counts, *sorted, *partials, *owner, *run, *tot, *planes, *wsum;
+    void *offsets[kMaxMsmParts] = {}, *buckets[kMaxMsmParts] = {};
+    static const char* const kOffsetNames[kMaxMsmParts] = {"msm_offsets", "msm_offsets2"};
+    static const char* const kBucketNames[kMaxMsmParts] = {"msm_buckets", "msm_buckets2"};
     MZK_TRY(ctx->ensure("msm_counts", ((size_t)sh.keys + 1) * 4, &counts));
-    MZK_TRY(ctx->ensure("msm_offsets", ((size_t)sh.keys + 2) * 4, &offsets));
+    for (int p = 0; p < n_parts; p++) {
+        MZK_TRY(ctx->ensure(kOffsetNames[p], ((size_t)sh.keys + 2) * 4, &offsets[p]));
+        MZK_TRY(ctx->ensure(kBucketNames[p], (size_t)sh.keys * sizeof(Xyzz), &buckets[p]));
+    }
     MZK_TRY(ctx->ensure("msm_sorted", entries_cap * 4, &sorted));
-    MZK_TRY(ctx->ensure("msm_buckets", (size_t)sh.keys * sizeof(Xyzz), &buckets));
     MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
     MZK_TRY(ctx->ensure("msm_owner", (size_t)acc_threads * 4, &owner));
     void *long_count, *long_list;
@@ -653,65 +686,75 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
     MZK_TRY(ctx->ensure("msm_planes", slots * split * sizeof(Xyzz), &planes));
     MZK_TRY(ctx->ensure("msm_q", slots * sizeof(Xyzz), &q));
     MZK_TRY(ctx->ensure("msm_wsum", (size_t)sh.windows * sizeof(Xyzz), &wsum));
-    // pinned staging: window sums and the entry count (read back), then the
-    // window table (uploaded without the sync a pageable copy implies)
+    // pinned staging: window sums and the parts' entry counts (read back),
+    // then the window table (uploaded without the sync a pageable copy implies)
     void* host_wsum;
     const size_t tab_off = (size_t)sh.windows * sizeof(Xyzz) + 64;
     MZK_TRY(ctx->ensure_pinned(tab_off + wins.size() * sizeof(WinDev), &host_wsum));
     WinDev* host_tab = reinterpret_cast<WinDev*>(static_cast<char*>(host_wsum) + tab_off);
     std::memcpy(host_tab, wins.data(), wins.size() * sizeof(WinDev));
+    uint32_t* host_entries =
+        reinterpret_cast<uint32_t*>(static_cast<char*>(host_wsum) + (size_t)sh.windows * sizeof(Xyzz));
 
     const Fr* sc = static_cast<const Fr*>(d_scalars);
     const Affine* ba = static_cast<const Affine*>(d_bases);
     const int pt_threads = 256;
-    const uint32_t pt_blocks = (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)ctx->num_sms * 16);
 
     MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, host_tab, wins.size() * sizeof(WinDev), cudaMemcpyHostToDevice, st));
-    MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
-    MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
-    k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)counts);
-    MZK_LAUNCH_CHECK(ctx);
-    MZK_TRY(ctx->phase_end(st));
-    MZK_TRY(ctx->phase_begin(PH_SCAN, st));
-    // exclusive scan one place to the right: offsets[key + 1] = start of key
-    MZK_CUDA_CHECK(cudaMemsetAsync(offsets, 0, 4, st));
-    MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets + 1, sh.keys + 1, st));
-    MZK_TRY(ctx->phase_end(st));
-    MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
-    k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, (uint32_t*)offsets + 1,
-                                                (uint32_t*)sorted);
-    MZK_LAUNCH_CHECK(ctx);
-    MZK_TRY(ctx->phase_end(st));
-    if (bases_ready) MZK_CUDA_CHECK(cudaStreamWaitEvent(st, bases_ready, 0));
-    MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
-    k_accumulate<<<acc_blocks, kAccThreads, 0, st>>>(ba, (const uint32_t*)sorted, (const uint32_t*)offsets, sh.keys,
-                                                    (Xyzz*)buckets, (Xyzz*)partials, (int*)owner);
-    MZK_LAUNCH_CHECK(ctx);
-    MZK_TRY(ctx->phase_end(st));
-    MZK_TRY(ctx->phase_begin(PH_FIXUP, st));
-    MZK_CUDA_CHECK(cudaMemsetAsync(long_count, 0, 4, st));
-    k_fixup<<<acc_blocks, kAccThreads, 0, st>>>((const uint32_t*)offsets, sh.keys, (const Xyzz*)partials,
-                                               (const int*)owner, (Xyzz*)buckets, (uint32_t*)long_count,
-                                               (uint2*)long_list);
-    MZK_LAUNCH_CHECK(ctx);
-    k_fixup_long<<<ctx->num_sms * 2, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
-        (const int*)owner, (const Xyzz*)partials, (const uint32_t*)long_count, (const uint2*)long_list,
-        (Xyzz*)buckets);
-    MZK_LAUNCH_CHECK(ctx);
-    MZK_TRY(ctx->phase_end(st));
+    for (int p = 0; p < n_parts; p++) {
+        const MsmPart& part = parts[p];
+        const size_t np = part.end - part.begin;
+        uint32_t* off = static_cast<uint32_t*>(offsets[p]);
+        const uint32_t pt_blocks =
+            (uint32_t)std::min<size_t>((np + pt_threads - 1) / pt_threads, (size_t)ctx->num_sms * 16);
+        if (part.scalars_ready) MZK_CUDA_CHECK(cudaStreamWaitEvent(st, part.scalars_ready, 0));
+        MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
+        MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
+        k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc + part.begin, np, sh.c, sh.windows, sh.nb,
+                                                      (uint32_t*)counts);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_TRY(ctx->phase_end(st));
+        MZK_TRY(ctx->phase_begin(PH_SCAN, st));
+        // exclusive scan one place to the right: off[key + 1] = start of key
+        MZK_CUDA_CHECK(cudaMemsetAsync(off, 0, 4, st));
+        MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, off + 1, sh.keys + 1, st));
+        MZK_TRY(ctx->phase_end(st));
+        MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
+        k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc + part.begin, np, sh.c, sh.windows, sh.nb, off + 1,
+                                                    (uint32_t*)sorted);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_TRY(ctx->phase_end(st));
+        if (part.bases_ready) MZK_CUDA_CHECK(cudaStreamWaitEvent(st, part.bases_ready, 0));
+        MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
+        k_accumulate<<<acc_blocks, kAccThreads, 0, st>>>(ba + part.begin, (const uint32_t*)sorted, off, sh.keys,
+                                                        (Xyzz*)buckets[p], (Xyzz*)partials, (int*)owner);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_TRY(ctx->phase_end(st));
+        MZK_TRY(ctx->phase_begin(PH_FIXUP, st));
+        MZK_CUDA_CHECK(cudaMemsetAsync(long_count, 0, 4, st));
+        k_fixup<<<acc_blocks, kAccThreads, 0, st>>>(off, sh.keys, (const Xyzz*)partials, (const int*)owner,
+                                                   (Xyzz*)buckets[p], (uint32_t*)long_count, (uint2*)long_list);
+        MZK_LAUNCH_CHECK(ctx);
+        k_fixup_long<<<ctx->num_sms * 2, kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
+            (const int*)owner, (const Xyzz*)partials, (const uint32_t*)long_count, (const uint2*)long_list,
+            (Xyzz*)buckets[p]);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_TRY(ctx->phase_end(st));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(host_entries + p, off + sh.keys, 4, cudaMemcpyDeviceToHost, st));
+    }
     MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
-    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets, (const uint32_t*)offsets, (const WinDev*)d_wins,
-                                 (uint32_t)wins.size(), total_groups, slots, split, (Xyzz*)run, (Xyzz*)tot,
-                                 (Xyzz*)planes, (Xyzz*)q, (Xyzz*)wsum, &ctx->launches, st));
+    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets[0], (const uint32_t*)offsets[0], (const Xyzz*)buckets[1],
+                                 (const uint32_t*)offsets[1], (const WinDev*)d_wins, (uint32_t)wins.size(),
+                                 total_groups, slots, split, (Xyzz*)run, (Xyzz*)tot, (Xyzz*)planes, (Xyzz*)q,
+                                 (Xyzz*)wsum, &ctx->launches, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_CUDA_CHECK(cudaMemcpyAsync(host_wsum, wsum, (size_t)sh.windows * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
-    uint32_t* host_entries = reinterpret_cast<uint32_t*>(static_cast<char*>(host_wsum) + (size_t)sh.windows * sizeof(Xyzz));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(host_entries, (const uint32_t*)offsets + sh.keys, 4, cudaMemcpyDeviceToHost, st));
     MZK_CUDA_CHECK(cudaStreamSynchronize(st));
     ctx->phase_collect();
     ctx->last_c = sh.c;
     ctx->last_windows = sh.windows;
-    ctx->last_entries = *host_entries;
+    ctx->last_entries = 0;
+    for (int p = 0; p < n_parts; p++) ctx->last_entries += host_entries[p];
 
     // host: sum_w 2^(c w) S_w by Horner, then normalise
     const host::Xyzz6* hs = static_cast<const host::Xyzz6*>(host_wsum);
@@ -925,8 +968,8 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
-    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets, (const uint32_t*)offsets, (const WinDev*)d_wins,
-                                 (uint32_t)n_wins, groups, slots, split, (Xyzz*)run, (Xyzz*)tot, (Xyzz*)planes,
+    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets, (const uint32_t*)offsets, nullptr, nullptr,
+                                 (const WinDev*)d_wins, (uint32_t)n_wins, groups, slots, split, (Xyzz*)run, (Xyzz*)tot, (Xyzz*)planes,
                                  (Xyzz*)q, (Xyzz*)wsum, &ctx->launches, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_CUDA_CHECK(cudaMemcpyAsync(host_wsum, wsum, n_wins * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
@@ -1106,8 +1149,8 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
     append_windows(sh, 0, wins, total_groups, slots);
     WinDev* d_wins = reinterpret_cast<WinDev*>(base + kNaWinsOff);
     MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, wins.data(), wins.size() * sizeof(WinDev), cudaMemcpyHostToDevice, st));
-    MZK_CUDA_CHECK(launch_reduce(buckets, offsets, d_wins, (uint32_t)wins.size(), total_groups, slots, 1, run, tot,
-                                 planes, planes, wsum, nullptr, st));
+    MZK_CUDA_CHECK(launch_reduce(buckets, offsets, nullptr, nullptr, d_wins, (uint32_t)wins.size(), total_groups,
+                                 slots, 1, run, tot, planes, planes, wsum, nullptr, st));
     // window sums to host memory owned by this function (no pinned allocation)
     host::Xyzz6 hs[kNaMaxWindows];
     MZK_CUDA_CHECK(cudaMemcpyAsync(hs, wsum, (size_t)sh.windows * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));

@@ -36,7 +36,7 @@ struct Context {
     int num_sms = 0;
     cudaStream_t stream = nullptr;       // compute stream
     cudaStream_t copy_stream = nullptr;  // host->device copies overlapped with compute
-    cudaEvent_t ev_copy = nullptr;
+    cudaEvent_t ev_copy = nullptr, ev_copy2 = nullptr;  // uploads of the first and second part
     std::recursive_mutex mu;
     std::map<std::string, DevBuf> bufs;
     void* pinned = nullptr;
@@ -103,6 +103,17 @@ struct Context {
 // first kernel that reads the bases (their upload overlaps the digit sort)
 Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
                      cudaStream_t stream, cudaEvent_t bases_ready);
+// A pipelined MSM over contiguous point ranges [begin, end): the compute
+// stream waits on a part's scalars_ready before sorting its digits and on its
+// bases_ready before accumulating, so the upload of later parts overlaps the
+// accumulation of earlier ones.  Same result as one part.
+constexpr int kMaxMsmParts = 2;
+struct MsmPart {
+    size_t begin, end;
+    cudaEvent_t scalars_ready, bases_ready;  // optional
+};
+Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
+                    cudaStream_t stream, const MsmPart* parts, int n_parts);
 int msm_pick_window(size_t n);
 // one MSM of a batch: scalars (device) against bases[base_offset, base_offset + n)
 struct BatchItem {

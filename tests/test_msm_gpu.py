@@ -170,3 +170,28 @@ def test_full_size_closed_form(ctx, log_n):
     r = O.rand_fr(seed_r, n)
     t = O.fr_inner_product(s, r)
     assert np.array_equal(mzk.affine(got), O.g1_mul(O.g1_generator(), t))
+
+
+@pytest.mark.parametrize("log_n,extra", [(20, 0), (20, 777), (24, 0)])
+def test_host_buffers_two_part_upload(ctx, log_n, extra):
+    """Host-buffer MSMs of 2^20 points and more upload and compute in two
+    parts (the first ~30 % of the points, then the rest): the result equals
+    the device-resident call on the same data and the closed form, with
+    zero scalars and one repeated bucket straddling the part boundary."""
+    n = (1 << log_n) + extra
+    seed_s, seed_r = 0xC0DE + log_n + extra, 0xFACE + log_n + extra
+    hs = ctx.gen_rand_fr(seed_s, n).download((n, 4))
+    db = ctx.gen_bases(seed_r, n)
+    hb = db.download((n, 12))
+    first = (n * 3 // 10) & ~1023
+    hs[first - 300:first + 300] = 0
+    hs[first - 2000:first - 1000] = O.fr_const(0)  # scalar one: all in bucket 1 of window 0
+    hs[first + 1000:first + 2000] = O.fr_const(0)
+    hs[-5:] = 0
+    ds = ctx.alloc(hs.nbytes)
+    ds.upload(hs)
+    got = ctx.msm_best(hs, hb)
+    assert np.array_equal(got, ctx.msm_device(ds, db, n))
+    del db, hb
+    r = O.rand_fr(seed_r, n)
+    assert np.array_equal(mzk.affine(got), O.g1_mul(O.g1_generator(), O.fr_inner_product(hs, r)))
