@@ -461,7 +461,7 @@ def measure_setup_and_scans(mzk, ctx, stream):
     d_comp.upload(comp)
     ms = timed(lambda: ctx.g1_decompress_device(d_comp, n, bufs[2]), reps=1)
     out["g1_decompress_2^20"] = {"ms": round(ms, 2), "points_per_s": round(n / ms * 1e3, 1),
-                                 "note": "square root, sign and the [r]P subgroup check per point"}
+                                 "note": "square root, sign and the G1 membership test phi(P) = -[u^2]P per point"}
     small.close()
     dom.close()
     return out

@@ -55,6 +55,12 @@ int mzk_ctx_phase_stats(mzk_ctx *ctx, double *ms_out, uint64_t *count_out, int m
  * second with operands in registers. */
 int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s, double variants[4]);
 
+/* Self-check of the field code: squares n device Fp values (12 x u32
+ * Montgomery, lazily reduced in [0, 2p)) with the dedicated squaring and with
+ * the general multiplication, and counts the values whose results differ in
+ * any limb (expected 0). */
+int mzk_probe_fp_sqr_check(mzk_ctx *ctx, const uint64_t *d_values, size_t n, uint64_t *mismatches);
+
 /* ---- device memory helpers (for callers without a CUDA runtime) ---------- */
 int mzk_device_alloc(mzk_ctx *ctx, size_t bytes, void **out);
 int mzk_device_free(mzk_ctx *ctx, void *ptr);

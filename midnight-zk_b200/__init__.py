@@ -52,6 +52,7 @@ SIGNATURES = {
     "mzk_device_free": (_i32, [_vp, _vp]),
     "mzk_memcpy_h2d": (_i32, [_vp, _vp, _vp, _sz]),
     "mzk_memcpy_d2h": (_i32, [_vp, _vp, _vp, _sz]),
+    "mzk_probe_fp_sqr_check": (_i32, [_vp, _vp, _sz, _u64p]),
     "mzk_msm_g1": (_i32, [_vp, _u64p, _u64p, _sz, _u64p]),
     "mzk_msm_g1_device": (_i32, [_vp, _vp, _vp, _sz, _u64p]),
     "mzk_msm_g1_noalloc": (_i32, [_vp, _vp, _sz, _u64p, _vp]),
@@ -349,6 +350,13 @@ class Context:
         v = (ctypes.c_double * 4)()
         _check(lib().mzk_probe_imad_peak(self.h, ctypes.byref(a), ctypes.byref(b), v))
         return a.value, b.value, {"mad_lo_hi": v[0], "mad_cc_chain": v[1], "mad_lo": v[2], "madd_regs": v[3]}
+
+    def probe_fp_sqr_check(self, d_values, n):
+        """Values among n device Fp elements whose dedicated square differs from a*a."""
+        out = np.zeros(1, np.uint64)
+        ptr = d_values.ptr if isinstance(d_values, DeviceBuffer) else int(d_values)
+        _check(lib().mzk_probe_fp_sqr_check(self.h, ptr, int(n), _ptr(out)))
+        return int(out[0])
 
     def msm_last_shape(self):
         c, w, e = _i32(), _i32(), np.zeros(1, np.uint64)

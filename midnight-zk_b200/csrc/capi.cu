@@ -298,6 +298,16 @@ int mzk_probe_imad_peak(mzk_ctx* ctx, double* imad_per_s, double* fp_mul_per_s, 
     return mzk::probe_imad(&ctx->impl, imad_per_s, fp_mul_per_s, variants);
 }
 
+int mzk_probe_fp_sqr_check(mzk_ctx* ctx, const uint64_t* d_values, size_t n, uint64_t* mismatches) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!mismatches || (n && !d_values)) {
+        mzk::set_error("probe: null pointer");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    return mzk::check_fp_sqr(&ctx->impl, d_values, n, mismatches);
+}
+
 int mzk_msm_g1_device(mzk_ctx* ctx, const uint64_t* d_scalars, const uint64_t* d_bases, size_t n, uint64_t out[18]) {
     if (int s = check_ctx(ctx)) return s;
     if (!out || (n && (!d_scalars || !d_bases))) {

@@ -112,6 +112,8 @@ __device__ __forceinline__ void xyzz_add_affine_fast(Xyzz& acc, const Affine& q)
         return;
     }
     Fp pp, rr;
+    // squares as general products: measured faster here than the dedicated
+    // squaring (fewer registers in the bucket loop)
     fp_mul2(pp, p, p, rr, r, r);
     Fp ppp, q1;
     fp_mul2(ppp, p, pp, q1, acc.x, pp);
@@ -139,11 +141,11 @@ __device__ __forceinline__ Xyzz xyzz_add(const Xyzz& a, const Xyzz& b) {
         xyzz_set_inf(z);
         return z;
     }
-    Fp pp = fp_sqr(p);
+    Fp pp = fp_mul(p, p);  // general products: the dedicated squaring spills in the bucket reduction
     Fp ppp = fp_mul(p, pp);
     Fp q1 = fp_mul(u1, pp);
     Xyzz o;
-    o.x = fp_sub(fp_sub(fp_sqr(r), ppp), fp_dbl(q1));
+    o.x = fp_sub(fp_sub(fp_mul(r, r), ppp), fp_dbl(q1));
     o.y = fp_sub(fp_mul(r, fp_sub(q1, o.x)), fp_mul(s1, ppp));
     o.zz = fp_mul(fp_mul(a.zz, b.zz), pp);
     o.zzz = fp_mul(fp_mul(a.zzz, b.zzz), ppp);

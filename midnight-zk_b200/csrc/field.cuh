@@ -187,6 +187,91 @@ __device__ __forceinline__ void add_masked(uint32_t* r, const uint32_t* t, uint3
     MZK_ASM("addc.u32 %0, %1, %2;" : "=r"(r[N - 1]) : "r"(t[N - 1]), "r"(modf(N - 1) & mask));
 }
 
+// Montgomery square r = a^2 * 2^(-32N) mod m, the same value as
+// mont_mul_raw(r, a, a) with ~N^2/2 fewer wide multiply-adds:
+//  1. T = sum_{i<j} a_i a_j 2^(32(i+j)) (2N words).  Row i's products are
+//     split by the parity of j - i into two chains of aligned word pairs; the
+//     chain reaching word i+N runs first, and the row's last carries land in
+//     word i+N+1, which no earlier row has reached.
+//  2. T = 2T + sum_i a_i^2 2^(64i): a funnel shift, then one chain of the
+//     diagonal products.
+//  3. Montgomery reduction of the low half on an N+1-word window X (N rows
+//     of X = (X + m m_mod) / 2^32, X < R throughout), then + the high half:
+//     (T_lo + M m_mod)/R + T_hi = (T + M m_mod)/R, where M = -T m_mod^-1 mod R
+//     is the unique multiplier word-serial Montgomery uses as well.  With
+//     a < 2m and 4m < R the result is < m + 1 + m/2 < 2m.
+template <class P>
+__device__ __forceinline__ void mont_sqr_raw(uint32_t* r, const uint32_t* a) {
+    constexpr int N = P::N;
+    uint32_t t[2 * N];
+#pragma unroll
+    for (int k = 0; k < 2 * N; k++) t[k] = 0;
+#pragma unroll
+    for (int i = 0; i < N - 1; i++) {
+        // chain reaching the top product a_i a_{N-1}: j = N-1, N-3, ... > i
+        const int j_top0 = ((N - 1 - i) & 1) ? i + 1 : i + 2;  // first j of that parity
+        MZK_ASM("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                : "+r"(t[i + j_top0]), "+r"(t[i + j_top0 + 1]) : "r"(a[i]), "r"(a[j_top0]));
+#pragma unroll
+        for (int j = j_top0 + 2; j < N; j += 2)
+            MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                    : "+r"(t[i + j]), "+r"(t[i + j + 1]) : "r"(a[i]), "r"(a[j]));
+        MZK_ASM("addc.u32 %0, 0, 0;" : "=r"(t[i + N + 1]));
+        // the other parity: j = N-2, N-4, ... > i, ending at word i+N-1
+        const int j_oth0 = j_top0 == i + 1 ? i + 2 : i + 1;
+        if (j_oth0 <= N - 2) {
+            MZK_ASM("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                    : "+r"(t[i + j_oth0]), "+r"(t[i + j_oth0 + 1]) : "r"(a[i]), "r"(a[j_oth0]));
+#pragma unroll
+            for (int j = j_oth0 + 2; j < N - 1; j += 2)
+                MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                        : "+r"(t[i + j]), "+r"(t[i + j + 1]) : "r"(a[i]), "r"(a[j]));
+            MZK_ASM("addc.cc.u32 %0, %0, 0;\n\taddc.u32 %1, %1, 0;" : "+r"(t[i + N]), "+r"(t[i + N + 1]));
+        }
+    }
+    // doubling (the off-diagonal sum is < 2^(64N-1)), then the diagonal
+#pragma unroll
+    for (int k = 2 * N - 1; k > 0; k--)
+        MZK_ASM("shf.l.clamp.b32 %0, %1, %0, 1;" : "+r"(t[k]) : "r"(t[k - 1]));
+    t[0] <<= 1;
+    MZK_ASM("mad.lo.cc.u32 %0, %2, %2, %0;\n\tmadc.hi.cc.u32 %1, %2, %2, %1;" : "+r"(t[0]), "+r"(t[1]) : "r"(a[0]));
+#pragma unroll
+    for (int i = 1; i < N - 1; i++)
+        MZK_ASM("madc.lo.cc.u32 %0, %2, %2, %0;\n\tmadc.hi.cc.u32 %1, %2, %2, %1;"
+                : "+r"(t[2 * i]), "+r"(t[2 * i + 1]) : "r"(a[i]));
+    MZK_ASM("madc.lo.cc.u32 %0, %2, %2, %0;\n\tmadc.hi.u32 %1, %2, %2, %1;"
+            : "+r"(t[2 * N - 2]), "+r"(t[2 * N - 1]) : "r"(a[N - 1]));
+    // reduction of the low half
+    uint32_t x[N + 1];
+#pragma unroll
+    for (int k = 0; k < N; k++) x[k] = t[k];
+    x[N] = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const uint32_t m = x[0] * P::N0;
+        MZK_ASM("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                : "+r"(x[0]), "+r"(x[1]) : "r"(m), "r"(P::mod(0)));
+#pragma unroll
+        for (int j = 2; j < N; j += 2)
+            MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                    : "+r"(x[j]), "+r"(x[j + 1]) : "r"(m), "r"(P::mod(j)));
+        MZK_ASM("addc.u32 %0, %0, 0;" : "+r"(x[N]));
+        MZK_ASM("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                : "+r"(x[1]), "+r"(x[2]) : "r"(m), "r"(P::mod(1)));
+#pragma unroll
+        for (int j = 3; j < N - 1; j += 2)
+            MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.cc.u32 %1, %2, %3, %1;"
+                    : "+r"(x[j]), "+r"(x[j + 1]) : "r"(m), "r"(P::mod(j)));
+        MZK_ASM("madc.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.u32 %1, %2, %3, %1;"
+                : "+r"(x[N - 1]), "+r"(x[N]) : "r"(m), "r"(P::mod(N - 1)));
+        // x[0] is zero: divide by 2^32
+#pragma unroll
+        for (int k = 0; k < N; k++) x[k] = x[k + 1];
+        x[N] = 0;
+    }
+    add_n<N>(r, x, t + N);
+}
+
 // -------------------------------------------------------------------- Fp ----
 struct FpMod { __device__ __forceinline__ uint32_t operator()(int i) const { return FpP::mod(i); } };
 struct FpMod2 { __device__ __forceinline__ uint32_t operator()(int i) const { return FpP::mod2(i); } };
@@ -205,7 +290,11 @@ __device__ __forceinline__ void fp_mul2(Fp& r1, const Fp& a1, const Fp& b1, Fp& 
     r1 = t1;
     r2 = t2;
 }
-__device__ __forceinline__ Fp fp_sqr(const Fp& a) { return fp_mul(a, a); }
+__device__ __forceinline__ Fp fp_sqr(const Fp& a) {
+    Fp r;
+    mont_sqr_raw<FpP>(r.l, a.l);
+    return r;
+}
 __device__ __forceinline__ Fp fp_add(const Fp& a, const Fp& b) {
     Fp t, r;
     add_n<12>(t.l, a.l, b.l);

@@ -3,6 +3,8 @@
 // 12-limb Montgomery multiplication of field.cuh reaches on it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "ec.cuh"
 #include "field.cuh"
 #include "runtime.hpp"
@@ -120,7 +122,36 @@ __global__ void __launch_bounds__(128, 1) k_probe_madd(uint32_t seed, uint32_t* 
     if (r == 0x12345678u) sink[0] = r;
 }
 
+// Self-check of the dedicated squaring: fp_sqr(a) and fp_mul(a, a) must agree
+// limb for limb (both are (a^2 + M p) / R with the same unique M).
+__global__ void k_check_fp_sqr(const Fp* __restrict__ in, size_t n, unsigned long long* __restrict__ mismatches) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const Fp a = in[i];
+        const Fp s = fp_sqr(a), m = fp_mul(a, a);
+        uint32_t diff = 0;
+#pragma unroll
+        for (int j = 0; j < 12; j++) diff |= s.l[j] ^ m.l[j];
+        if (diff) atomicAdd(mismatches, 1ull);
+    }
+}
+
 }  // namespace
+
+Status check_fp_sqr(Context* ctx, const void* d_values, size_t n, uint64_t* mismatches) {
+    void* cnt;
+    MZK_TRY(ctx->ensure("probe_count", 64, &cnt));
+    MZK_CUDA_CHECK(cudaMemsetAsync(cnt, 0, 8, ctx->stream));
+    if (n) {
+        const uint32_t blocks = (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8);
+        k_check_fp_sqr<<<blocks, 256, 0, ctx->stream>>>(static_cast<const Fp*>(d_values), n,
+                                                        static_cast<unsigned long long*>(cnt));
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    MZK_CUDA_CHECK(cudaMemcpyAsync(mismatches, cnt, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    return OK;
+}
 
 Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s, double* variants) {
     void* sink;

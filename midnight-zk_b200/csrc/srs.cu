@@ -108,9 +108,6 @@ __global__ void k_lag_scal(const Fr* __restrict__ wlo, const Fr* __restrict__ wh
 struct Exp12 {
     uint32_t l[12];
 };
-struct FrOrder {
-    uint32_t l[8];
-};
 
 // (p + 1) / 4 and the group order r as 32-bit limbs, from the moduli
 Exp12 sqrt_exponent() {
@@ -124,10 +121,40 @@ Exp12 sqrt_exponent() {
     for (int i = 0; i < 12; i++) e.l[i] = (e.l[i] >> 2) | (i < 11 ? e.l[i + 1] << 30 : 0u);
     return e;
 }
-FrOrder group_order() {
-    FrOrder r;
-    for (int i = 0; i < 8; i++) r.l[i] = FrP::mod(i);
-    return r;
+// The G1 membership test of Scott (ePrint 2021/1130, section 6; its proof
+// for BLS12-381 completed in ePrint 2022/352): a point P of E(Fp) lies in G1
+// iff phi(P) = -[u^2] P, where u = 0xd201000000010000 is |x| of the curve
+// parameter x = -u and phi(x, y) = (beta x, y) with beta the cube root of
+// unity on which phi acts on G1 as -u^2 (the other root acts as u^2 - 1).
+// Same decision as [r] P = O (blst_p1_affine_in_g1, which G1Affine::
+// is_torsion_free calls, g1.rs:398-400) for ~1/3 of the group operations.
+// beta in Montgomery form (beta * 2^384 mod p); beta = 0x5f19672fdf76ce51
+// ba69c6076a0f77eaddb3a93be6f89688de17d813620a00022e01fffffffefffe.
+__device__ __forceinline__ uint32_t g1_beta_mont(int i) {
+    return i == 0 ? 0x798a64e8u : i == 1 ? 0x30f1361bu : i == 2 ? 0x7ece5a2au : i == 3 ? 0xf3b8ddabu
+         : i == 4 ? 0xc61577f7u : i == 5 ? 0x16a8ca3au : i == 6 ? 0x74fd029bu : i == 7 ? 0xc26a2ff8u
+         : i == 8 ? 0x60701c6eu : i == 9 ? 0x3636b766u : i == 10 ? 0x241b6160u : 0x051ba4abu;
+}
+// [u] q, MSB-first double-and-add over the 64-bit u (63 doublings, 5 additions)
+__device__ Xyzz xyzz_mul_bls_u(const Xyzz& q) {
+    constexpr uint64_t kU = 0xd201000000010000ull;
+    Xyzz acc = q;
+#pragma unroll 1
+    for (int bit = 62; bit >= 0; bit--) {
+        acc = xyzz_dbl(acc);
+        if ((kU >> bit) & 1u) acc = xyzz_add(acc, q);
+    }
+    return acc;
+}
+__device__ bool g1_in_subgroup(const Affine& p) {
+    const Xyzz q = xyzz_mul_bls_u(xyzz_mul_bls_u(xyzz_from_affine(p)));
+    if (xyzz_is_inf(q)) return false;  // p is not the identity, so phi(p) is not either
+    Fp beta;
+#pragma unroll
+    for (int k = 0; k < 12; k++) beta.l[k] = g1_beta_mont(k);
+    // phi(p) = -q  <=>  beta x ZZ = X  and  y ZZZ = -Y
+    const Fp bx = fp_mul(beta, p.x);
+    return fp_is_zero(fp_sub(q.x, fp_mul(bx, q.zz))) && fp_is_zero(fp_add(q.y, fp_mul(p.y, q.zzz)));
 }
 
 __device__ __forceinline__ Fp fp_pow_limbs(const Fp& a, const uint32_t* e, int limbs) {
@@ -146,7 +173,7 @@ __device__ __forceinline__ Fp fp_pow_limbs(const Fp& a, const uint32_t* e, int l
 
 // status: 0 ok, 1 bad encoding, 2 not on the curve, 3 not in G1
 __global__ void __launch_bounds__(kThreads) k_g1_decompress(const uint8_t* __restrict__ in, uint64_t n, int check,
-                                                            Exp12 sqrt_e, FrOrder order, Affine* __restrict__ out,
+                                                            Exp12 sqrt_e, Affine* __restrict__ out,
                                                             uint8_t* __restrict__ status,
                                                             unsigned long long* __restrict__ invalid) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -213,18 +240,7 @@ __global__ void __launch_bounds__(kThreads) k_g1_decompress(const uint8_t* __res
                     if (y_larger != ((flags & 0x20u) != 0)) y = ny;
                     p.x = x;
                     p.y = y;
-                    if (check) {  // [r] P must be the identity
-                        Xyzz acc;
-                        xyzz_set_inf(acc);
-#pragma unroll 1
-                        for (int k = 7; k >= 0; k--)
-#pragma unroll 1
-                            for (int bit = 31; bit >= 0; bit--) {
-                                acc = xyzz_dbl(acc);
-                                if ((order.l[k] >> bit) & 1u) xyzz_add_affine(acc, p);
-                            }
-                        if (!xyzz_is_inf(acc)) st = 3;
-                    }
+                    if (check && !g1_in_subgroup(p)) st = 3;
                 }
             }
         }
@@ -325,7 +341,7 @@ Status g1_decompress_device(Context* ctx, const void* in, uint64_t n, int check_
     MZK_TRY(ctx->ensure("srs_invalid", 16, &cnt));
     MZK_CUDA_CHECK(cudaMemsetAsync(cnt, 0, 8, st));
     k_g1_decompress<<<blocks_for(ctx, n), kThreads, 0, st>>>(static_cast<const uint8_t*>(in), n, check_subgroup,
-                                                             sqrt_exponent(), group_order(), static_cast<Affine*>(out),
+                                                             sqrt_exponent(), static_cast<Affine*>(out),
                                                              status, static_cast<unsigned long long*>(cnt));
     MZK_LAUNCH_CHECK(ctx);
     if (invalid) {

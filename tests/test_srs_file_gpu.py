@@ -88,3 +88,83 @@ def test_read_processed_rejects(ctx):
     data[4 + 3 * 48 + 47] ^= 1                                       # corrupt one point of g
     with pytest.raises(mzk.MzkError):
         ctx.srs_read_processed(bytes(data), n, *bufs)
+
+
+# ---- the subgroup check against points with a torsion component of every
+# prime-power order dividing the G1 cofactor (plain Python curve arithmetic) ----
+R_ORDER = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
+COFACTOR_PRIMES = [(3, 1), (11, 2), (10177, 2), (859267, 2), (52437899, 2)]  # (l, e): l^e | h
+COFACTOR = 3 * 11 ** 2 * 10177 ** 2 * 859267 ** 2 * 52437899 ** 2
+GEN = (0x17F1D3A73197D7942695638C4FA9AC0FC3688C4F9774B905A14E3A3F171BAC586C55E83FF97A1AEFFB3AF00ADB22C6BB,
+       0x08B3F481E3AAA0F1A09E30ED741D8AE4FCF5E095D5D00AF600DB18CB2C04B3EDD03CC744A2888AE40CAA232946C5E7E1)
+
+
+def ec_add(a, b):
+    if a is None:
+        return b
+    if b is None:
+        return a
+    (x1, y1), (x2, y2) = a, b
+    if x1 == x2:
+        if (y1 + y2) % P_MOD == 0:
+            return None
+        lam = 3 * x1 * x1 * pow(2 * y1, -1, P_MOD) % P_MOD
+    else:
+        lam = (y2 - y1) * pow(x2 - x1, -1, P_MOD) % P_MOD
+    x3 = (lam * lam - x1 - x2) % P_MOD
+    return x3, (lam * (x1 - x3) - y1) % P_MOD
+
+
+def ec_mul(a, k):
+    acc = None
+    for bit in bin(k)[2:]:
+        acc = ec_add(acc, acc)
+        if bit == "1":
+            acc = ec_add(acc, a)
+    return acc
+
+
+def curve_point(x):
+    rhs = (x ** 3 + 4) % P_MOD
+    y = pow(rhs, (P_MOD + 1) // 4, P_MOD)
+    return (x, y) if y * y % P_MOD == rhs else None
+
+
+def compress(pt):
+    x, y = pt
+    b = bytearray(x.to_bytes(48, "big"))
+    b[0] |= 0x80 | (0x20 if y > P_MOD - y else 0)
+    return bytes(b)
+
+
+def torsion_cases():
+    """(encoding, in G1) pairs: for every prime l | h, a point T of the
+    l-Sylow subgroup (order l or l^2), T plus a G1 point, [l] T when that is
+    not the identity, and G1 points."""
+    assert COFACTOR * R_ORDER == P_MOD + 1 - (1 - 0xD201000000010000)  # #E(Fp) = p + 1 - t
+    raw = [pt for pt in (curve_point(x) for x in range(2, 60)) if pt]
+    cases = []
+    for i, (l, e) in enumerate(COFACTOR_PRIMES):
+        t = next(t for t in (ec_mul(pt, COFACTOR * R_ORDER // l ** e) for pt in raw) if t is not None)
+        assert ec_mul(t, l ** e) is None
+        g = ec_mul(GEN, 7 + 1000 * i)
+        cases += [(compress(t), False), (compress(ec_add(g, t)), False), (compress(g), True)]
+        lt = ec_mul(t, l)
+        if lt is not None:
+            cases += [(compress(lt), False), (compress(ec_add(g, lt)), False)]
+    return cases
+
+
+def test_subgroup_check_on_torsion_components(ctx):
+    cases = torsion_cases()
+    enc = [c for c, _ in cases]
+    n = len(enc)
+    raw = np.frombuffer(b"".join(enc), np.uint8)
+    d_in, d_out, d_st = ctx.alloc(raw.nbytes), ctx.alloc(n * 96), ctx.alloc(n)
+    d_in.upload(raw)
+    bad = ctx.g1_decompress_device(d_in, n, d_out, d_st, check_subgroup=True)
+    st = [int(s) for s in d_st.download((n,), np.uint8)]
+    want = [O.g1_decompress(e, True)[0] for e in enc]
+    assert want == [0 if ok else 3 for _, ok in cases]
+    assert st == want
+    assert bad == sum(1 for _, ok in cases if not ok)
