@@ -44,7 +44,8 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--log-n", type=int, default=24)
-    p.add_argument("--window", type=int, default=0, help="force the MSM window width c (0: cost model)")
+    p.add_argument("--window", type=int, default=0, help="force the MSM window width c (0: autotuned / cost model)")
+    p.add_argument("--no-tune", action="store_true", help="skip the autotuner (cost-model window, even NTT split)")
     p.add_argument("--cpu-sample-log-n", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -549,6 +550,17 @@ def run_ours(args):
     # x 600 half-products is the denominator unless a plain IMAD probe beats it
     madd_rate = imad_variants.pop("madd_regs")
     imad_peak = max(imad_peak, max(imad_variants.values()), fp_mul_rate * IMAD_PER_FP_MUL)
+    # the autotuner, before anything is timed: MSM window widths for every
+    # log2 size the bench runs (the headline and the prover's MSMs) on the
+    # headline inputs, NTT pass splits for 2^12 .. 2^26
+    tune = None
+    if not args.window and not args.no_tune:
+        t0 = time.perf_counter()
+        res = ctx.autotune(ds, db, msm_log_n=list(range(12, args.log_n + 1)), ntt_log_n=list(range(12, 27)), reps=2)
+        tune = {"msm_c": {str(L): v[0] for L, v in res["msm"].items()},
+                "ntt_split": {str(L): v[0] for L, v in res["ntt"].items()},
+                "ntt_split_modes": "1 even, 2 largest passes first, 3 largest passes last",
+                "seconds": round(time.perf_counter() - t0, 2)}
     stream = torch.cuda.ExternalStream(ctx.stream)
 
     def barrier():
@@ -679,7 +691,7 @@ def run_ours(args):
                        "bucket_entries": entries, "l2": "inputs 2.1 GB > 126 MB L2 (no flush)",
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "roofline_msm": msm_roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches, "clocks": clocks,
+            "gpu_launches": launches, "clocks": clocks, "autotune": tune,
             "phases_ms": {k: round(v[0] / max(v[1], 1), 3) for k, v in phases.items()},
             "fp_mul_rate_g_per_s": round(fp_mul_rate / 1e9, 2),
             "imad_probe_t_per_s": {k: round(v / 1e12, 3) for k, v in imad_variants.items()},

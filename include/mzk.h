@@ -61,6 +61,35 @@ int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s, 
  * any limb (expected 0). */
 int mzk_probe_fp_sqr_check(mzk_ctx *ctx, const uint64_t *d_values, size_t n, uint64_t *mismatches);
 
+/* Captured CUDA graphs of this context: captures made and replays run (the
+ * proof core's per-proof NTT sequences). */
+int mzk_ctx_graph_stats(mzk_ctx *ctx, uint64_t *captures, uint64_t *replays);
+
+/* ---- autotuner -------------------------------------------------------------
+ * The reference fixes its choices in code: the window width c = ceil(ln n)
+ * (curves/src/msm.rs:464-470) and the blst/msm_best cut-over at 2^19 points
+ * (proofs/src/poly/kzg/msm.rs:187-190).  Here the MSM window width and the
+ * NTT pass split are chosen per log2 size by timing the candidates on the
+ * device; every choice gives the same results, only the speed differs.
+ * Without a tuned entry the cost model / even split apply; mzk_msm_set_window
+ * overrides everything.  A context created with the environment variable
+ * MZK_TUNE_FILE set loads that table (a malformed file fails the creation). */
+#define MZK_TUNE_MSM_WINDOW 0 /* value: window width c in [5, 24] */
+#define MZK_TUNE_NTT_SPLIT 1  /* value: 1 even, 2 largest passes first, 3 largest passes last */
+/* Time the window widths c_model-2 .. c_model+2 for each log2 size in
+ * msm_log_n on the first 2^L device scalars and bases (both holding at least
+ * 2^max(L) elements), and the three NTT splits for each log2 size in ntt_log_n
+ * (a forward transform of random data); keep the fastest.  reps: timed runs
+ * per candidate after one warm-up.  msm_ms / ntt_ms (may be NULL): the best
+ * time per size. */
+int mzk_autotune(mzk_ctx *ctx, const uint64_t *d_scalars, const uint64_t *d_bases, const uint32_t *msm_log_n,
+                 size_t n_msm, const uint32_t *ntt_log_n, size_t n_ntt, int reps, double *msm_ms, double *ntt_ms);
+int mzk_autotune_get(mzk_ctx *ctx, int kind, uint32_t log_n, int *value); /* 0 = not tuned */
+int mzk_autotune_set(mzk_ctx *ctx, int kind, uint32_t log_n, int value);  /* 0 clears the entry */
+/* the table as text lines "msm_c <log_n> <c>" / "ntt_split <log_n> <mode>" */
+int mzk_autotune_save(mzk_ctx *ctx, const char *path);
+int mzk_autotune_load(mzk_ctx *ctx, const char *path);
+
 /* ---- device memory helpers (for callers without a CUDA runtime) ---------- */
 int mzk_device_alloc(mzk_ctx *ctx, size_t bytes, void **out);
 int mzk_device_free(mzk_ctx *ctx, void *ptr);
@@ -226,6 +255,9 @@ typedef struct {
  * with MZK_PROVE_MSM_PER_CALL in flags, each as its own call (the plain
  * one-call-at-a-time form; same results). */
 #define MZK_PROVE_MSM_PER_CALL 1u
+/* launch each proof's NTT sequence kernel by kernel instead of replaying a
+ * captured CUDA graph (same kernels, same results) */
+#define MZK_PROVE_NO_GRAPHS 2u
 int mzk_prove_core_device(mzk_ctx *ctx, mzk_domain *d, const mzk_proving_key_desc *pk, const mzk_proof_job *jobs,
                           size_t count, uint32_t flags, uint64_t *out);
 

@@ -53,6 +53,13 @@ SIGNATURES = {
     "mzk_memcpy_h2d": (_i32, [_vp, _vp, _vp, _sz]),
     "mzk_memcpy_d2h": (_i32, [_vp, _vp, _vp, _sz]),
     "mzk_probe_fp_sqr_check": (_i32, [_vp, _vp, _sz, _u64p]),
+    "mzk_autotune": (_i32, [_vp, _vp, _vp, ctypes.POINTER(_u32), _sz, ctypes.POINTER(_u32), _sz, _i32,
+                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "mzk_autotune_get": (_i32, [_vp, _i32, _u32, ctypes.POINTER(_i32)]),
+    "mzk_ctx_graph_stats": (_i32, [_vp, _u64p, _u64p]),
+    "mzk_autotune_set": (_i32, [_vp, _i32, _u32, _i32]),
+    "mzk_autotune_save": (_i32, [_vp, ctypes.c_char_p]),
+    "mzk_autotune_load": (_i32, [_vp, ctypes.c_char_p]),
     "mzk_msm_g1": (_i32, [_vp, _u64p, _u64p, _sz, _u64p]),
     "mzk_msm_g1_device": (_i32, [_vp, _vp, _vp, _sz, _u64p]),
     "mzk_msm_g1_noalloc": (_i32, [_vp, _vp, _sz, _u64p, _vp]),
@@ -119,6 +126,9 @@ class ProofJob(ctypes.Structure):
 
 
 PROVE_MSM_PER_CALL = 1  # MZK_PROVE_MSM_PER_CALL
+PROVE_NO_GRAPHS = 2  # MZK_PROVE_NO_GRAPHS
+# the plain one-call-at-a-time form: every MSM its own call, every kernel its own launch
+PROVE_PLAIN = PROVE_MSM_PER_CALL | PROVE_NO_GRAPHS
 PROOF_CORE_COMMITMENTS = ["a", "b", "c", "m_delta", "z_delta", "Z_double_delta", "h", "H0", "H1", "H2", "H3"]
 
 
@@ -351,6 +361,43 @@ class Context:
         _check(lib().mzk_probe_imad_peak(self.h, ctypes.byref(a), ctypes.byref(b), v))
         return a.value, b.value, {"mad_lo_hi": v[0], "mad_cc_chain": v[1], "mad_lo": v[2], "madd_regs": v[3]}
 
+    def graph_stats(self):
+        """(captures, replays) of the context's CUDA graphs."""
+        c, r = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
+        _check(lib().mzk_ctx_graph_stats(self.h, _ptr(c), _ptr(r)))
+        return int(c[0]), int(r[0])
+
+    TUNE_MSM_WINDOW, TUNE_NTT_SPLIT = 0, 1
+
+    def autotune(self, d_scalars=None, d_bases=None, msm_log_n=(), ntt_log_n=(), reps=2):
+        """Time the MSM window widths (on the first 2^L device scalars/bases) and
+        the NTT pass splits per log2 size and keep the fastest.  Returns
+        {"msm": {L: (c, ms)}, "ntt": {L: (split, ms)}}."""
+        ml = (_u32 * max(1, len(msm_log_n)))(*msm_log_n)
+        nl = (_u32 * max(1, len(ntt_log_n)))(*ntt_log_n)
+        mms = (ctypes.c_double * max(1, len(msm_log_n)))()
+        nms = (ctypes.c_double * max(1, len(ntt_log_n)))()
+        ds = 0 if d_scalars is None else (d_scalars.ptr if isinstance(d_scalars, DeviceBuffer) else int(d_scalars))
+        db = 0 if d_bases is None else (d_bases.ptr if isinstance(d_bases, DeviceBuffer) else int(d_bases))
+        _check(lib().mzk_autotune(self.h, ds or None, db or None, ml, len(msm_log_n), nl, len(ntt_log_n), int(reps),
+                                  mms, nms))
+        return {"msm": {int(L): (self.tuned(self.TUNE_MSM_WINDOW, L), mms[i]) for i, L in enumerate(msm_log_n)},
+                "ntt": {int(L): (self.tuned(self.TUNE_NTT_SPLIT, L), nms[i]) for i, L in enumerate(ntt_log_n)}}
+
+    def tuned(self, kind, log_n):
+        v = _i32()
+        _check(lib().mzk_autotune_get(self.h, int(kind), int(log_n), ctypes.byref(v)))
+        return v.value
+
+    def set_tuned(self, kind, log_n, value):
+        _check(lib().mzk_autotune_set(self.h, int(kind), int(log_n), int(value)))
+
+    def save_tuning(self, path):
+        _check(lib().mzk_autotune_save(self.h, str(path).encode()))
+
+    def load_tuning(self, path):
+        _check(lib().mzk_autotune_load(self.h, str(path).encode()))
+
     def probe_fp_sqr_check(self, d_values, n):
         """Values among n device Fp elements whose dedicated square differs from a*a."""
         out = np.zeros(1, np.uint64)
@@ -543,13 +590,18 @@ class EvaluationDomain:
                                                _ptr(blinds), _ptr(out), dl or None))
         return out
 
-    def prove_core_device(self, pk_desc, jobs, per_call=False):
+    def prove_core_device(self, pk_desc, jobs, per_call=False, graphs=None):
         """Device part of create_proof for a list of ProofJob: (len, 11, 18) commitments.
-        per_call: every MSM as its own call instead of two batched MSMs."""
+        per_call: the plain form (every MSM its own call, the NTT sequence launched
+        kernel by kernel) instead of batched MSMs and a replayed CUDA graph;
+        graphs: override the graph choice."""
         arr = (ProofJob * max(1, len(jobs)))(*jobs)
         out = np.zeros((max(1, len(jobs)), len(PROOF_CORE_COMMITMENTS), 18), np.uint64)
+        flags = PROVE_PLAIN if per_call else 0
+        if graphs is not None:
+            flags = (flags & ~PROVE_NO_GRAPHS) | (0 if graphs else PROVE_NO_GRAPHS)
         _check(lib().mzk_prove_core_device(self.ctx.h, self.h, ctypes.byref(pk_desc), ctypes.addressof(arr),
-                                           len(jobs), PROVE_MSM_PER_CALL if per_call else 0, _ptr(out)))
+                                           len(jobs), flags, _ptr(out)))
         return out[:len(jobs)]
 
     def srs_setup_device(self, s, g=None, g_lagrange=None, g_lagrange_delta=None, g_lagrange_double_delta=None):
@@ -614,7 +666,7 @@ class ProvingServer:
         self.ctx = ctx
         h = _vp()
         _check(lib().mzk_server_create(ctx.h, int(max_batch), int(lanes), int(mem_budget_bytes),
-                                       PROVE_MSM_PER_CALL if per_call else 0, ctypes.byref(h)))
+                                       PROVE_PLAIN if per_call else 0, ctypes.byref(h)))
         self.h = h.value
         ctx._servers.add(self)
         self._keys = []

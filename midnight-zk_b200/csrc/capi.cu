@@ -1,6 +1,7 @@
 // capi.cu — the extern "C" boundary (include/mzk.h) and the device context.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -40,6 +41,7 @@ Status Context::ensure(const char* name, size_t bytes, void** out) {
         cudaStreamSynchronize(stream);
         cudaStreamSynchronize(copy_stream);
         cudaFree(b.p);
+        buf_generation++;  // captured graphs may hold the old address
         b.p = nullptr;
         b.bytes = 0;
         // a buffer that had to grow once tends to grow again (mixed sizes):
@@ -111,6 +113,8 @@ void Context::phase_collect() {
 Context::~Context() {
     if (stream) cudaStreamSynchronize(stream);
     if (copy_stream) cudaStreamSynchronize(copy_stream);
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
     for (auto& kv : bufs)
         if (kv.second.p) cudaFree(kv.second.p);
     if (pinned) cudaFreeHost(pinned);
@@ -192,6 +196,15 @@ int mzk_ctx_create(int device, mzk_ctx** out) {
         return mzk::ERR_STATE;
     }
     c->impl.num_sms = prop.multiProcessorCount;
+    if (const char* tf = std::getenv("MZK_TUNE_FILE")) {
+        if (*tf) {
+            const mzk::Status s = mzk::tune_load(&c->impl, tf);
+            if (s != mzk::OK) {
+                delete c;
+                return s;
+            }
+        }
+    }
     *out = c;
     return mzk::OK;
 }
@@ -298,6 +311,72 @@ int mzk_probe_imad_peak(mzk_ctx* ctx, double* imad_per_s, double* fp_mul_per_s, 
     return mzk::probe_imad(&ctx->impl, imad_per_s, fp_mul_per_s, variants);
 }
 
+int mzk_ctx_graph_stats(mzk_ctx* ctx, uint64_t* captures, uint64_t* replays) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    if (captures) *captures = ctx->impl.graph_captures;
+    if (replays) *replays = ctx->impl.graph_replays;
+    return mzk::OK;
+}
+
+int mzk_autotune(mzk_ctx* ctx, const uint64_t* d_scalars, const uint64_t* d_bases, const uint32_t* msm_log_n,
+                 size_t n_msm, const uint32_t* ntt_log_n, size_t n_ntt, int reps, double* msm_ms, double* ntt_ms) {
+    if (int s = check_ctx(ctx)) return s;
+    if ((n_msm && !msm_log_n) || (n_ntt && !ntt_log_n)) {
+        mzk::set_error("autotune: null size list");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    return mzk::autotune(&ctx->impl, d_scalars, d_bases, msm_log_n, n_msm, ntt_log_n, n_ntt, reps, msm_ms, ntt_ms);
+}
+
+static int* tune_slot(mzk_ctx* ctx, int kind, uint32_t log_n) {
+    if (log_n >= (uint32_t)mzk::kTuneSlots) return nullptr;
+    if (kind == MZK_TUNE_MSM_WINDOW) return &ctx->impl.tuned_msm_c[log_n];
+    if (kind == MZK_TUNE_NTT_SPLIT) return &ctx->impl.tuned_ntt_split[log_n];
+    return nullptr;
+}
+
+int mzk_autotune_get(mzk_ctx* ctx, int kind, uint32_t log_n, int* value) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    int* slot = tune_slot(ctx, kind, log_n);
+    if (!slot || !value) {
+        mzk::set_error("autotune: unknown kind or size, or null output");
+        return mzk::ERR_ARG;
+    }
+    *value = *slot;
+    return mzk::OK;
+}
+
+int mzk_autotune_set(mzk_ctx* ctx, int kind, uint32_t log_n, int value) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    int* slot = tune_slot(ctx, kind, log_n);
+    const bool ok = value == 0 || (kind == MZK_TUNE_MSM_WINDOW && value >= 5 && value <= 24) ||
+                    (kind == MZK_TUNE_NTT_SPLIT && value >= mzk::kSplitEven && value <= mzk::kSplitBack);
+    if (!slot || !ok) {
+        mzk::set_error("autotune: unknown kind or size, or value out of range");
+        return mzk::ERR_ARG;
+    }
+    *slot = value;
+    return mzk::OK;
+}
+
+int mzk_autotune_save(mzk_ctx* ctx, const char* path) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!path) return mzk::ERR_ARG;
+    Guard g(ctx);
+    return mzk::tune_save(&ctx->impl, path);
+}
+
+int mzk_autotune_load(mzk_ctx* ctx, const char* path) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!path) return mzk::ERR_ARG;
+    Guard g(ctx);
+    return mzk::tune_load(&ctx->impl, path);
+}
+
 int mzk_probe_fp_sqr_check(mzk_ctx* ctx, const uint64_t* d_values, size_t n, uint64_t* mismatches) {
     if (int s = check_ctx(ctx)) return s;
     if (!mismatches || (n && !d_values)) {
@@ -399,6 +478,7 @@ int mzk_domain_destroy(mzk_domain* d) {
     if (!d) return mzk::OK;
     Guard g(d->ctx);
     cudaStreamSynchronize(d->ctx->impl.stream);
+    d->ctx->impl.buf_generation++;  // captured graphs may hold its tables
     delete d->impl;
     delete d;
     return mzk::OK;

@@ -642,7 +642,7 @@ Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, si
         }
         max_part = std::max(max_part, parts[p].end - parts[p].begin);
     }
-    const int c = ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(n);
+    const int c = msm_window_for(ctx, n);
     if (c < 5 || c > 24) {
         set_error("msm: window width must be in [5, 24]");
         return ERR_ARG;
@@ -855,7 +855,7 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     uint64_t all_keys = 0;
     for (size_t m = 0; m < count; m++)
         if (items[m].n)
-            all_keys += make_shape(ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(items[m].n))
+            all_keys += make_shape(msm_window_for(ctx, items[m].n))
                             .keys;
     const int glen_log = group_log_for(all_keys);
     for (size_t m = 0; m < count; m++) {
@@ -869,7 +869,7 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
             set_error("msm batch: item " + std::to_string(m) + " reads past the bases");
             return ERR_ARG;
         }
-        const int c = ctx->msm_window_override > 0 ? ctx->msm_window_override : msm_pick_window(it.n);
+        const int c = msm_window_for(ctx, it.n);
         const MsmShape sh = make_shape(c, glen_log);
         BatchItemDev d;
         d.scalars = static_cast<const Fr*>(it.d_scalars);

@@ -262,6 +262,10 @@ Domain::~Domain() {
 
 // EvaluationDomain::new (proofs/src/poly/domain.rs:54-167)
 Status domain_create(Context* ctx, uint32_t j, uint32_t k, Domain** out) {
+    // the pass kernel's shared memory limit, set here once rather than per
+    // transform: transforms may be captured into CUDA graphs
+    MZK_CUDA_CHECK(cudaFuncSetAttribute(k_ntt_dif_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(kTile * sizeof(Fr) + kTile / 2 * sizeof(Fr))));
     *out = nullptr;
     if (j < 2 || k < 1 || k > 28) {
         set_error("domain: need j >= 2 and 1 <= k <= 28");
@@ -354,18 +358,21 @@ static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n
     const uint32_t tile = std::min(kTile, N);
     const uint32_t tile_log = std::min(kTileLog, log_n);
     const uint32_t passes = (log_n + tile_log - 1) / tile_log;
-    MZK_CUDA_CHECK(cudaFuncSetAttribute(k_ntt_dif_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(kTile * sizeof(Fr) + kTile / 2 * sizeof(Fr))));
     Fr* tmp = nullptr;
     if (passes > 1) {
         void* p;
         MZK_TRY(ctx->ensure("ntt_tmp", (size_t)N * sizeof(Fr), &p));
         tmp = static_cast<Fr*>(p);
     }
+    const int split = log_n < (uint32_t)kTuneSlots ? ctx->tuned_ntt_split[log_n] : 0;
     uint32_t log_s = log_n;
     for (uint32_t p = 0; p < passes; p++) {
         const uint32_t rem = passes - p;
-        const uint32_t log_r = (log_s + rem - 1) / rem;  // even split, larger passes first
+        // every pass keeps at least one stage and at most tile_log; the
+        // remaining passes can always take what is left
+        uint32_t log_r = (log_s + rem - 1) / rem;  // even split, larger passes first
+        if (split == kSplitFront) log_r = std::min(tile_log, log_s - (rem - 1));
+        if (split == kSplitBack) log_r = std::max(1u, log_s - (rem - 1) * tile_log);
         const bool last = p + 1 == passes;
         PassArgs a;
         a.in = p == 0 ? in : tmp;

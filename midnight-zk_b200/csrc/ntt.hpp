@@ -19,6 +19,11 @@ enum DomainOp : int {
     OP_DIVIDE_BY_VANISHING = 5,
 };
 
+// pass split of a multi-pass transform (the autotuner's NTT choice):
+// even (larger passes first when uneven), the largest passes (2^11 elements
+// per tile) first, or the largest passes last
+enum NttSplit : int { kSplitEven = 1, kSplitFront = 2, kSplitBack = 3 };
+
 struct Domain {
     uint32_t k = 0, ext_k = 0;
     uint32_t quotient_poly_degree = 0;  // j - 1

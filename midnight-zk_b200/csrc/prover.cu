@@ -72,6 +72,81 @@ static Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const st
     return OK;
 }
 
+// One proof's NTT sequence: lagrange_to_coeff then coeff_to_extended of each
+// of its seven polynomials (2-3 pass kernels per transform).  With use_graph
+// the sequence is captured once into a CUDA graph per key (the domain, its
+// tables, the NTT scratch, the pass splits and the 21 column pointers: all
+// that the kernels read) and replayed afterwards; the graph holds the same
+// launches with the same arguments, so the results are the same.
+static Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag, Fr* const* coeff, Fr* const* ext,
+                           bool use_graph, cudaStream_t st) {
+    auto eager = [&]() -> Status {
+        for (int p = 0; p < kPolys; p++) {
+            MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, lag[p], coeff[p], st));
+            MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, coeff[p], ext[p], st));
+        }
+        return OK;
+    };
+    if (!use_graph || ctx->profiling || ctx->graphs_unsupported) return eager();
+    // the scratch of the largest transform exists before capture: nothing
+    // may be allocated while the stream is capturing
+    void* tmp;
+    MZK_TRY(ctx->ensure("ntt_tmp", ((size_t)1 << d->ext_k) * sizeof(Fr), &tmp));
+    std::vector<uintptr_t> key = {(uintptr_t)d, d->k, d->ext_k, (uintptr_t)tmp,
+                                  (uintptr_t)ctx->tuned_ntt_split[d->k], (uintptr_t)ctx->tuned_ntt_split[d->ext_k]};
+    for (int r = 0; r < 4; r++) key.push_back((uintptr_t)d->tables[r]);
+    for (int p = 0; p < kPolys; p++) {
+        key.push_back((uintptr_t)lag[p]);
+        key.push_back((uintptr_t)coeff[p]);
+        key.push_back((uintptr_t)ext[p]);
+    }
+    auto& gs = ctx->graphs;
+    for (size_t i = 0; i < gs.size();) {  // drop graphs that may hold freed addresses
+        if (gs[i].generation != ctx->buf_generation) {
+            cudaGraphExecDestroy(gs[i].exec);
+            gs.erase(gs.begin() + (ptrdiff_t)i);
+        } else {
+            i++;
+        }
+    }
+    for (auto& g : gs)
+        if (g.key == key) {
+            g.last_use = ++ctx->graph_clock;
+            MZK_CUDA_CHECK(cudaGraphLaunch(g.exec, st));
+            ctx->launches += g.launches;
+            ctx->graph_replays++;
+            return OK;
+        }
+    const uint64_t launches0 = ctx->launches, gen0 = ctx->buf_generation;
+    MZK_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const Status s = eager();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ei = cudaErrorUnknown;
+    if (s == OK && e == cudaSuccess && graph && ctx->buf_generation == gen0)
+        ei = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {  // not captured: the same launches, issued one by one
+        cudaGetLastError();
+        ctx->launches = launches0;
+        const Status se = eager();
+        if (se == OK) ctx->graphs_unsupported = true;  // the capture itself was refused
+        return se;
+    }
+    if (gs.size() >= Context::kMaxGraphs) {  // least recently used out
+        size_t lru = 0;
+        for (size_t i = 1; i < gs.size(); i++)
+            if (gs[i].last_use < gs[lru].last_use) lru = i;
+        cudaGraphExecDestroy(gs[lru].exec);
+        gs.erase(gs.begin() + (ptrdiff_t)lru);
+    }
+    gs.push_back({key, exec, ctx->launches - launches0, gen0, ++ctx->graph_clock});
+    ctx->graph_captures++;
+    MZK_CUDA_CHECK(cudaGraphLaunch(exec, st));
+    return OK;
+}
+
 Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_proving_key_desc* const* pks,
                         const mzk_proof_job* jobs, size_t count, uint64_t* out, uint32_t flags, cudaStream_t st) {
     std::memset(out, 0, count * kProofCoreCommitments * 18 * 8);
@@ -219,10 +294,7 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
         const mzk_proving_key_desc* pk = pks[j];
         const mzk_proof_job& jb = jobs[j];
         const void* const* lag = &lagrange[j * kPolys];
-        for (int p = 0; p < kPolys; p++) {
-            MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, lag[p], coeff[j * kPolys + p], st));
-            MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, coeff[j * kPolys + p], ext[j * kPolys + p], st));
-        }
+        MZK_TRY(ntt_sequence(ctx, d, lag, &coeff[j * kPolys], &ext[j * kPolys], !(flags & MZK_PROVE_NO_GRAPHS), st));
         Fr* const* e = &ext[j * kPolys];
         const uint64_t* adv[3] = {(const uint64_t*)e[0], (const uint64_t*)e[1], (const uint64_t*)e[2]};
         const uint64_t* sig[3] = {pk->sigma_ext[0], pk->sigma_ext[1], pk->sigma_ext[2]};

@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace mzk {
 
@@ -42,6 +43,11 @@ struct Context {
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
     int msm_window_override = 0;
+    // autotuned choices by floor(log2 size), 0 = not tuned (tune.cu): MSM
+    // window width, NTT pass split (NttSplit, ntt.hpp)
+    static constexpr int kTuneSlotsN = 33;
+    int tuned_msm_c[kTuneSlotsN] = {};
+    int tuned_ntt_split[kTuneSlotsN] = {};
     // fixed-base table of the G1 generator for synthetic inputs (device)
     void* gen_table = nullptr;
     // kernels launched by the library since context creation (for reporting)
@@ -55,6 +61,20 @@ struct Context {
     int prof_used = 0;
     double phase_ms[kPhases] = {};
     uint64_t phase_count[kPhases] = {};
+    // Captured CUDA graphs (a proof's NTT sequence), keyed by every pointer and
+    // setting their kernels use.  buf_generation is bumped whenever ensure()
+    // replaces a buffer or a domain is destroyed: graphs of an older generation
+    // are dropped before any lookup, so a freed address is never replayed.
+    struct GraphEntry {
+        std::vector<uintptr_t> key;
+        cudaGraphExec_t exec;
+        uint64_t launches, generation, last_use;
+    };
+    static constexpr size_t kMaxGraphs = 64;
+    std::vector<GraphEntry> graphs;
+    uint64_t buf_generation = 0, graph_clock = 0, graph_captures = 0, graph_replays = 0;
+    bool graphs_unsupported = false;  // a capture failed once: launch eagerly from then on
+
     // shape of the last MSM: window width, windows, bucket entries processed
     int last_c = 0, last_windows = 0;
     uint64_t last_entries = 0;
@@ -115,6 +135,16 @@ struct MsmPart {
 Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18,
                     cudaStream_t stream, const MsmPart* parts, int n_parts);
 int msm_pick_window(size_t n);
+// window width for an MSM of n points: the explicit override, else the
+// autotuned width for floor(log2 n), else the cost model
+constexpr int kTuneSlots = Context::kTuneSlotsN;
+int msm_window_for(const Context* ctx, size_t n);
+// tune.cu: time the MSM window widths and NTT pass splits of the given log2
+// sizes on this device and keep the fastest; save / load the table as text
+Status autotune(Context* ctx, const void* d_scalars, const void* d_bases, const uint32_t* msm_log_n, size_t n_msm,
+                const uint32_t* ntt_log_n, size_t n_ntt, int reps, double* msm_ms_out, double* ntt_ms_out);
+Status tune_save(const Context* ctx, const char* path);
+Status tune_load(Context* ctx, const char* path);
 // one MSM of a batch: scalars (device) against bases[base_offset, base_offset + n)
 struct BatchItem {
     const void* d_scalars;

@@ -71,3 +71,28 @@ def test_device_derives_z_h_Z(ctx):
 def ctypes_copy(dst, src):
     import ctypes
     ctypes.memmove(ctypes.byref(dst), ctypes.byref(src), ctypes.sizeof(src))
+
+
+def test_ntt_sequence_graph_replays_equal_launches(ctx):
+    """Each proof's NTT sequence is captured into a CUDA graph once per key
+    and replayed afterwards: the commitments equal those of the kernel-by-
+    kernel launches, replays happen on repeated calls, and destroying a domain
+    drops the graphs (a new domain at the same address is captured afresh)."""
+    c = mzk.Context(0)
+    try:
+        st = Setup(c, 8, seed=31)
+        jobs = [st.job(s)[0] for s in (41, 42)]
+        eager = st.g.prove_core_device(st.pk, jobs, graphs=False)
+        assert c.graph_stats() == (0, 0)
+        first = st.g.prove_core_device(st.pk, jobs)
+        caps, reps = c.graph_stats()
+        assert caps == 2 and reps == 0                 # one graph per proof slot of the wave
+        again = st.g.prove_core_device(st.pk, jobs)
+        assert c.graph_stats() == (2, 2)
+        assert np.array_equal(first, eager) and np.array_equal(again, eager)
+        st2 = Setup(c, 8, seed=31)                     # same circuit, fresh domain and key buffers
+        st.g.close()
+        assert np.array_equal(st2.g.prove_core_device(st2.pk, jobs), eager)
+        assert c.graph_stats()[0] >= 3                 # recaptured after the domain went away
+    finally:
+        c.close()
