@@ -8,12 +8,16 @@
 //  1. histogram   one thread per scalar: Montgomery -> canonical (one Fr
 //                 multiplication by 1, the reference's `to_repr`), signed
 //                 c-bit window digits d_w in [-2^(c-1), 2^(c-1)], count of
-//                 entries per key (window, |d|-1) with warp-aggregated atomics.
+//                 entries per key (window, |d|-1) with warp-aggregated atomics;
+//                 the digits are also stored, window-major.
 //  2. scan        exclusive prefix sum of the counts = start of every bucket
 //                 in the sorted entry array (a counting sort).
-//  3. scatter     digits recomputed, each (point index | sign) written to its
-//                 bucket's slice.  Zero digits produce no entry, so zero and
-//                 sparse scalars cost nothing (msm_specific drops zero scalars).
+//  3. scatter     one window at a time from the stored digits: each
+//                 (point index | sign) goes to its bucket's slice; a window's
+//                 slices (4n bytes) stay in L2 while it is scattered, so the
+//                 random 4-byte writes leave L2 as whole sectors.  Zero digits
+//                 produce no entry, so zero and sparse scalars cost nothing
+//                 (msm_specific drops zero scalars).
 //  4. accumulate  the sorted entries split into equal chunks, one per thread:
 //                 every thread walks its chunk adding points into an XYZZ
 //                 accumulator (mixed addition, affine bases gathered from HBM).
@@ -126,8 +130,11 @@ __device__ __forceinline__ uint32_t next_digit(const Fr& s, int w, int c, uint32
     return mag == 0 ? kNoKey : (uint32_t)w * nb + (mag - 1);
 }
 
+// digits (optional): every point's signed digit per window, window-major
+// (digits[w * n + i] = key | sign << 31, kNoKey for a zero digit), for the
+// window-by-window scatter
 __global__ void k_histogram(const Fr* __restrict__ scalars, size_t n, int c, int windows, uint32_t nb,
-                            uint32_t* __restrict__ counts) {
+                            uint32_t* __restrict__ counts, uint32_t* __restrict__ digits) {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
     for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -139,14 +146,15 @@ __global__ void k_histogram(const Fr* __restrict__ scalars, size_t n, int c, int
             bool neg;
             uint32_t key = next_digit(s, w, c, nb, carry, neg);
             if (!valid) key = kNoKey;
+            if (digits && valid) digits[(size_t)w * n + i] = key == kNoKey ? kNoKey : key | (neg ? 0x80000000u : 0u);
             const uint32_t peers = __match_any_sync(0xffffffffu, key);
             if (key != kNoKey && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
         }
     }
 }
 
-// Windows whose cursor atomics a warp keeps in flight at once: the scatter is
-// bound by the latency of the atomics' round trips, not by bandwidth.
+// All-windows scatter of the fixed-scratch path (n <= 2^16, whose sorted
+// array fits in L2): windows whose cursor atomics a warp keeps in flight.
 constexpr int kScatterWindows = 8;
 
 // The cursor of bucket `key` is cursor[key] (= offsets + 1 of the caller):
@@ -169,6 +177,28 @@ __device__ __forceinline__ void scatter_group(const uint32_t (&key)[kScatterWind
     for (int j = 0; j < kScatterWindows; j++) {
         const uint32_t first = __shfl_sync(0xffffffffu, slot[j], __ffs(peers[j]) - 1);
         if (key[j] != kNoKey) sorted[first + (uint32_t)__popc(peers[j] & lt_mask)] = value | (neg[j] ? 0x80000000u : 0u);
+    }
+}
+
+// The scatter of one window from the stored digits.  Its entries go to that
+// window's slice of the sorted array (4n bytes: 67 MB at 2^24, inside the
+// 126 MB L2), so the scattered 4-byte writes merge into whole sectors in L2
+// instead of each costing a DRAM sector read and write.
+__global__ void k_scatter_window(const uint32_t* __restrict__ digits_w, size_t n, uint32_t* __restrict__ cursor,
+                                 uint32_t* __restrict__ sorted) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const size_t i = base + threadIdx.x;
+        const uint32_t d = i < n ? __ldg(digits_w + i) : kNoKey;
+        const uint32_t key = d == kNoKey ? kNoKey : d & 0x7fffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        uint32_t slot = 0;
+        if (key != kNoKey && lane == leader) slot = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
+        slot = __shfl_sync(0xffffffffu, slot, leader);
+        if (key != kNoKey) sorted[slot + (uint32_t)__popc(peers & lt_mask)] = (uint32_t)i | (d & 0x80000000u);
     }
 }
 
@@ -670,6 +700,8 @@ Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, si
         MZK_TRY(ctx->ensure(kBucketNames[p], (size_t)sh.keys * sizeof(Xyzz), &buckets[p]));
     }
     MZK_TRY(ctx->ensure("msm_sorted", entries_cap * 4, &sorted));
+    void* digits;
+    MZK_TRY(ctx->ensure("msm_digits", entries_cap * 4, &digits));
     MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
     MZK_TRY(ctx->ensure("msm_owner", (size_t)acc_threads * 4, &owner));
     void *long_count, *long_list;
@@ -711,7 +743,7 @@ Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, si
         MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
         MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
         k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc + part.begin, np, sh.c, sh.windows, sh.nb,
-                                                      (uint32_t*)counts);
+                                                      (uint32_t*)counts, (uint32_t*)digits);
         MZK_LAUNCH_CHECK(ctx);
         MZK_TRY(ctx->phase_end(st));
         MZK_TRY(ctx->phase_begin(PH_SCAN, st));
@@ -720,9 +752,11 @@ Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, si
         MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, off + 1, sh.keys + 1, st));
         MZK_TRY(ctx->phase_end(st));
         MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
-        k_scatter<<<pt_blocks, pt_threads, 0, st>>>(sc + part.begin, np, sh.c, sh.windows, sh.nb, off + 1,
-                                                    (uint32_t*)sorted);
-        MZK_LAUNCH_CHECK(ctx);
+        for (int w = 0; w < sh.windows; w++) {
+            k_scatter_window<<<pt_blocks, pt_threads, 0, st>>>((const uint32_t*)digits + (size_t)w * np, np,
+                                                               off + 1, (uint32_t*)sorted);
+            MZK_LAUNCH_CHECK(ctx);
+        }
         MZK_TRY(ctx->phase_end(st));
         if (part.bases_ready) MZK_CUDA_CHECK(cudaStreamWaitEvent(st, part.bases_ready, 0));
         MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
@@ -801,10 +835,11 @@ __device__ __forceinline__ uint32_t find_item(const BatchItemDev* items, uint32_
     return lo;
 }
 
-template <bool kScatter>
+// Counts per key of every item's digits, and every point's digit per window,
+// window-major (digits[w * total_points + p] = key | sign << 31, kNoKey for a
+// zero digit or a window past the item's), for the window-by-window scatter.
 __global__ void k_digits_batch(const BatchItemDev* __restrict__ items, uint32_t n_items, uint32_t total_points,
-                               int max_windows, uint32_t* __restrict__ counts_or_cursor,
-                               uint32_t* __restrict__ sorted) {
+                               int max_windows, uint32_t* __restrict__ counts, uint32_t* __restrict__ digits) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
     for (uint32_t base = blockIdx.x * blockDim.x; base < total_points; base += stride) {
@@ -814,32 +849,45 @@ __global__ void k_digits_batch(const BatchItemDev* __restrict__ items, uint32_t 
         const uint32_t local = p - it.point_start;
         Fr s = valid ? fr_from_mont(load_fr(it.scalars, local)) : fr_zero();
         uint32_t carry = 0;
-        for (int w0 = 0; w0 < max_windows; w0 += kScatterWindows) {
-            uint32_t key[kScatterWindows];
-            bool neg[kScatterWindows];
-#pragma unroll
-            for (int j = 0; j < kScatterWindows; j++) {
-                const int w = w0 + j;
-                key[j] = kNoKey;
-                neg[j] = false;
-                if (valid && w < (int)it.windows) {
-                    key[j] = next_digit(s, w, (int)it.c, it.nb, carry, neg[j]);
-                    if (key[j] != kNoKey) key[j] += it.key_start;
-                }
+        for (int w = 0; w < max_windows; w++) {
+            bool neg = false;
+            uint32_t key = kNoKey;
+            if (valid && w < (int)it.windows) {
+                key = next_digit(s, w, (int)it.c, it.nb, carry, neg);
+                if (key != kNoKey) key += it.key_start;
             }
-            if (!kScatter) {
-#pragma unroll
-                for (int j = 0; j < kScatterWindows; j++) {
-                    const uint32_t peers = __match_any_sync(0xffffffffu, key[j]);
-                    if (key[j] != kNoKey && lane == __ffs(peers) - 1) atomicAdd(&counts_or_cursor[key[j]], (uint32_t)__popc(peers));
-                }
-            } else {
-                scatter_group(key, neg, it.base_offset + local, lane, counts_or_cursor, sorted);
-            }
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            if (key != kNoKey && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
+            if (valid) digits[(size_t)w * total_points + p] = key == kNoKey ? kNoKey : key | (neg ? 0x80000000u : 0u);
         }
     }
 }
 
+
+// The batch scatter of window w of every item from the stored digits: the
+// entries land in the items' window-w slices (4 bytes per point of the batch),
+// which stay in L2 while the window is scattered.
+__global__ void k_scatter_window_batch(const uint32_t* __restrict__ digits_w, const BatchItemDev* __restrict__ items,
+                                       uint32_t n_items, uint32_t total_points, uint32_t* __restrict__ cursor,
+                                       uint32_t* __restrict__ sorted) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total_points; base += stride) {
+        const uint32_t p = base + threadIdx.x;
+        const uint32_t d = p < total_points ? __ldg(digits_w + p) : kNoKey;
+        const uint32_t key = d == kNoKey ? kNoKey : d & 0x7fffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        uint32_t slot = 0;
+        if (key != kNoKey && lane == leader) slot = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
+        slot = __shfl_sync(0xffffffffu, slot, leader);
+        if (key != kNoKey) {
+            const BatchItemDev& it = items[find_item(items, n_items, p)];
+            sorted[slot + (uint32_t)__popc(peers & lt_mask)] = (it.base_offset + (p - it.point_start)) | (d & 0x80000000u);
+        }
+    }
+}
 }  // namespace
 
 Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, const BatchItem* items, size_t count,
@@ -907,6 +955,8 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_TRY(ctx->ensure("msm_counts", (keys + 1) * 4, &counts));
     MZK_TRY(ctx->ensure("msm_offsets", (keys + 2) * 4, &offsets));
     MZK_TRY(ctx->ensure("msm_sorted", entries * 4, &sorted));
+    void* digits;
+    MZK_TRY(ctx->ensure("msm_digits", (size_t)max_windows * points * 4, &digits));
     MZK_TRY(ctx->ensure("msm_buckets", keys * sizeof(Xyzz), &buckets));
     MZK_TRY(ctx->ensure("msm_partials", (size_t)acc_threads * 2 * sizeof(Xyzz), &partials));
     MZK_TRY(ctx->ensure("msm_owner", (size_t)acc_threads * 4, &owner));
@@ -937,8 +987,8 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
         (uint32_t)std::min<uint64_t>((points + pt_threads - 1) / pt_threads, (uint64_t)ctx->num_sms * 16);
     MZK_TRY(ctx->phase_begin(PH_HISTOGRAM, st));
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, (keys + 1) * 4, st));
-    k_digits_batch<false><<<pt_blocks, pt_threads, 0, st>>>((const BatchItemDev*)d_items, n_items, (uint32_t)points,
-                                                           max_windows, (uint32_t*)counts, nullptr);
+    k_digits_batch<<<pt_blocks, pt_threads, 0, st>>>((const BatchItemDev*)d_items, n_items, (uint32_t)points,
+                                                    max_windows, (uint32_t*)counts, (uint32_t*)digits);
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCAN, st));
@@ -946,9 +996,13 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_TRY(scan_u32(ctx, (const uint32_t*)counts, (uint32_t*)offsets + 1, (uint32_t)keys + 1, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
-    k_digits_batch<true><<<pt_blocks, pt_threads, 0, st>>>((const BatchItemDev*)d_items, n_items, (uint32_t)points,
-                                                          max_windows, (uint32_t*)offsets + 1, (uint32_t*)sorted);
-    MZK_LAUNCH_CHECK(ctx);
+    for (int w = 0; w < max_windows; w++) {
+        k_scatter_window_batch<<<pt_blocks, pt_threads, 0, st>>>((const uint32_t*)digits + (size_t)w * points,
+                                                                 (const BatchItemDev*)d_items, n_items,
+                                                                 (uint32_t)points, (uint32_t*)offsets + 1,
+                                                                 (uint32_t*)sorted);
+        MZK_LAUNCH_CHECK(ctx);
+    }
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_ACCUMULATE, st));
     k_accumulate<<<acc_blocks, kAccThreads, 0, st>>>(static_cast<const Affine*>(d_bases), (const uint32_t*)sorted,
@@ -1125,7 +1179,7 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
         (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)g_noalloc_sms[dev] * 16);
     // the array keeps the previous call's contents: zero the counters
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
-    k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, counts);
+    k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, counts, nullptr);
     MZK_CUDA_CHECK(cudaGetLastError());
     MZK_CUDA_CHECK(cudaMemsetAsync(offsets, 0, 4, st));
     MZK_TRY(scan_u32_noalloc(counts, offsets + 1, sh.keys + 1, scan_sums, st));
