@@ -168,12 +168,41 @@ int mzk_domain_op(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *in, uint6
 int mzk_domain_op_device(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *d_in, uint64_t *d_out);
 
 /* ---- quotient evaluation (proofs/src/plonk/evaluation.rs:818-1114) ------ */
+/* Custom gates of any circuit as the reference flattens them
+ * (FlatGraphEvaluator, proofs/src/plonk/evaluation.rs:148-213; evaluated per
+ * row as evaluate_chunk, :530-651).  Each row has one values buffer: the
+ * constants, the challenge slots (beta, theta, trash_challenge, y) and the
+ * previous value (zero: the gates come first), the column reads, then the
+ * intermediates; result_idx holds the Horner-in-y combination of every gate
+ * polynomial.  Column types as ColumnRead (:163-181): 0 fixed, 1 advice,
+ * 2 instance.  Ops in FlatOpKind order (:134-143), operand indices into the
+ * values buffer: dst = a+b, a-b, a*b, a^2, 2a, -a, a*b+c.  At most 256 values
+ * and 32 rotations; every index is checked before anything runs. */
+#define MZK_FLAT_ADD 0
+#define MZK_FLAT_SUB 1
+#define MZK_FLAT_MUL 2
+#define MZK_FLAT_SQUARE 3
+#define MZK_FLAT_DOUBLE 4
+#define MZK_FLAT_NEGATE 5
+#define MZK_FLAT_MULADD 6
+typedef struct { uint32_t col_type, col_idx, rot_idx, dst; } mzk_column_read;
+typedef struct { uint32_t kind, dst, a, b, c; } mzk_flat_op;
+typedef struct {
+    const uint64_t *constants; uint32_t n_constants; /* HOST, Montgomery Fr, values [0, n_constants) */
+    const int32_t *rotations; uint32_t n_rotations;  /* row offsets of the original domain */
+    const mzk_column_read *reads; uint32_t n_reads;
+    const mzk_flat_op *ops; uint32_t n_ops;
+    uint32_t values_len;
+    uint32_t beta_idx, theta_idx, trash_challenge_idx, y_idx, previous_value_idx, result_idx;
+} mzk_flat_graph;
+
 /* Columns are extended-domain (coset) evaluations, 2^extended_k Fr each,
  * DEVICE pointers, given through HOST arrays of pointers.  Circuit shape: one
- * standard gate q_l a + q_r b + q_m a b + q_o c + q_c, permutation sets over
- * advice/fixed columns (chunk_len = cs.degree() - 2 columns each), at most one
- * logup lookup with one input column and one helper, no trashcans.  Limits:
- * 16 advice, 16 fixed, 16 permutation columns, 8 sets.  extended_omega and
+ * standard gate q_l a + q_r b + q_m a b + q_o c + q_c, or any custom gates given
+ * as a flattened program (`gates`), permutation sets over advice/fixed columns
+ * (chunk_len = cs.degree() - 2 columns each), at most one logup lookup with
+ * one input column and one helper, no trashcans.  Limits: 16 advice, 16
+ * fixed, 4 instance, 16 permutation columns, 8 sets.  extended_omega and
  * g_coset are taken from the domain (the fields exist for layout parity with
  * the CPU restatement). */
 typedef struct {
@@ -197,6 +226,12 @@ typedef struct {
     const uint64_t *l0, *l_last, *l_active;
     uint64_t y[4], beta[4], gamma[4], theta[4];
     uint64_t extended_omega[4], g_coset[4];
+    /* custom gates as a flattened program (null: the standard gate above);
+     * instance columns (extended coset, DEVICE) and the trash challenge are
+     * read by programs only */
+    const mzk_flat_graph *gates;
+    const uint64_t *const *instance; uint32_t n_instance;
+    uint64_t trash_challenge[4];
 } mzk_quotient_desc;
 /* d_out (2^extended_k Fr) = nu(X) on the extended coset; with divide != 0,
  * h(X) = nu(X) / (X^n - 1) (evaluate_numerator + divide_by_vanishing_poly,

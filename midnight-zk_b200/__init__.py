@@ -150,7 +150,58 @@ class QuotientDesc(ctypes.Structure):
     ("l0", ctypes.c_void_p), ("l_last", ctypes.c_void_p), ("l_active", ctypes.c_void_p),
     ("y", ctypes.c_uint64 * 4), ("beta", ctypes.c_uint64 * 4), ("gamma", ctypes.c_uint64 * 4),
     ("theta", ctypes.c_uint64 * 4), ("extended_omega", ctypes.c_uint64 * 4), ("g_coset", ctypes.c_uint64 * 4),
+    ("gates", ctypes.c_void_p), ("instance", ctypes.POINTER(ctypes.c_void_p)), ("n_instance", ctypes.c_uint32),
+    ("trash_challenge", ctypes.c_uint64 * 4),
 ]
+
+# FlatOpKind (proofs/src/plonk/evaluation.rs:134-143), MZK_FLAT_* in include/mzk.h
+FLAT_ADD, FLAT_SUB, FLAT_MUL, FLAT_SQUARE, FLAT_DOUBLE, FLAT_NEGATE, FLAT_MULADD = range(7)
+COL_FIXED, COL_ADVICE, COL_INSTANCE = 0, 1, 2
+
+
+class ColumnRead(ctypes.Structure):
+    _fields_ = [("col_type", ctypes.c_uint32), ("col_idx", ctypes.c_uint32), ("rot_idx", ctypes.c_uint32),
+                ("dst", ctypes.c_uint32)]
+
+
+class FlatOp(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("dst", ctypes.c_uint32), ("a", ctypes.c_uint32), ("b", ctypes.c_uint32),
+                ("c", ctypes.c_uint32)]
+
+
+class FlatGraph(ctypes.Structure):
+    """mzk_flat_graph: the custom gates as the reference's FlatGraphEvaluator
+    (proofs/src/plonk/evaluation.rs:148-213)."""
+    _fields_ = [
+        ("constants", ctypes.c_void_p), ("n_constants", ctypes.c_uint32),
+        ("rotations", ctypes.POINTER(ctypes.c_int32)), ("n_rotations", ctypes.c_uint32),
+        ("reads", ctypes.POINTER(ColumnRead)), ("n_reads", ctypes.c_uint32),
+        ("ops", ctypes.POINTER(FlatOp)), ("n_ops", ctypes.c_uint32),
+        ("values_len", ctypes.c_uint32),
+        ("beta_idx", ctypes.c_uint32), ("theta_idx", ctypes.c_uint32), ("trash_challenge_idx", ctypes.c_uint32),
+        ("y_idx", ctypes.c_uint32), ("previous_value_idx", ctypes.c_uint32), ("result_idx", ctypes.c_uint32),
+    ]
+
+
+def build_flat_graph(constants, rotations, reads, ops, values_len, beta_idx, theta_idx, trash_challenge_idx, y_idx,
+                     previous_value_idx, result_idx):
+    """A FlatGraph from plain Python data: constants (m, 4) uint64 Montgomery,
+    rotations [int], reads [(col_type, col_idx, rot_idx, dst)], ops
+    [(kind, dst, a, b, c)].  Keeps its arrays alive on the returned object."""
+    g = FlatGraph()
+    consts = np.ascontiguousarray(np.asarray(constants, np.uint64).reshape(-1, 4))
+    rots = (ctypes.c_int32 * max(1, len(rotations)))(*rotations)
+    rd = (ColumnRead * max(1, len(reads)))(*[ColumnRead(*r) for r in reads])
+    op = (FlatOp * max(1, len(ops)))(*[FlatOp(*(tuple(o) + (0,) * (5 - len(o)))) for o in ops])
+    g.constants, g.n_constants = consts.ctypes.data, consts.shape[0]
+    g.rotations, g.n_rotations = ctypes.cast(rots, ctypes.POINTER(ctypes.c_int32)), len(rotations)
+    g.reads, g.n_reads = ctypes.cast(rd, ctypes.POINTER(ColumnRead)), len(reads)
+    g.ops, g.n_ops = ctypes.cast(op, ctypes.POINTER(FlatOp)), len(ops)
+    g.values_len = values_len
+    g.beta_idx, g.theta_idx, g.trash_challenge_idx = beta_idx, theta_idx, trash_challenge_idx
+    g.y_idx, g.previous_value_idx, g.result_idx = y_idx, previous_value_idx, result_idx
+    g._keep = (consts, rots, rd, op)
+    return g
 
 
 def build_quotient_desc(cols, k, extended_k, addr):
@@ -173,8 +224,8 @@ def build_quotient_desc(cols, k, extended_k, addr):
     d.k, d.extended_k = k, extended_k
     d.advice, d.n_advice = ptr_array(cols["advice"]), len(cols["advice"])
     d.fixed, d.n_fixed = ptr_array(cols["fixed"]), len(cols["fixed"])
-    d.gate_fixed[:] = cols["gate_fixed"]
-    d.gate_advice[:] = cols["gate_advice"]
+    d.gate_fixed[:] = cols.get("gate_fixed", [0] * 5)
+    d.gate_advice[:] = cols.get("gate_advice", [0] * 3)
     pc = cols.get("perm_cols", [])
     d.n_perm_cols = len(pc)
     d.perm_col_kind = u32_array([kind for kind, _ in pc])
@@ -190,9 +241,14 @@ def build_quotient_desc(cols, k, extended_k, addr):
         d.lookup_input_advice, d.lookup_table_fixed, d.lookup_selector_fixed = lk["input"], lk["table"], lk["selector"]
         d.lookup_h, d.lookup_z, d.lookup_m = addr(lk["h"]), addr(lk["z"]), addr(lk["m"])
     d.l0, d.l_last, d.l_active = addr(cols["l0"]), addr(cols["l_last"]), addr(cols["l_active"])
-    for name in ("y", "beta", "gamma", "theta", "extended_omega", "g_coset"):
+    for name in ("y", "beta", "gamma", "theta", "extended_omega", "g_coset", "trash_challenge"):
         if name in cols:
             getattr(d, name)[:] = [int(v) for v in cols[name]]
+    if cols.get("gates") is not None:
+        keep.append(cols["gates"])
+        d.gates = ctypes.addressof(cols["gates"])
+    inst = cols.get("instance", [])
+    d.instance, d.n_instance = ptr_array(inst), len(inst)
     d._keep = keep
     return d
 

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/mzk.h"
@@ -46,15 +47,19 @@ __global__ void __launch_bounds__(256) k_quotient(QuotientParams q) {
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < E; idx += stride) {
         const uint32_t r_next = (idx + (1u << q.log_scale)) & mask;
         const uint32_t r_last = (idx + (uint32_t)(q.last_rot * (int32_t)(1u << q.log_scale))) & mask;
-        // custom gate (Horner from zero over the single gate polynomial)
-        const Fr a = ldfr(q.advice[q.gate_advice[0]], idx);
-        const Fr b = ldfr(q.advice[q.gate_advice[1]], idx);
-        const Fr c = ldfr(q.advice[q.gate_advice[2]], idx);
-        Fr v = fr_mul(ldfr(q.fixed[q.gate_fixed[0]], idx), a);
-        v = fr_add(v, fr_mul(ldfr(q.fixed[q.gate_fixed[1]], idx), b));
-        v = fr_add(v, fr_mul(fr_mul(a, b), ldfr(q.fixed[q.gate_fixed[2]], idx)));
-        v = fr_add(v, fr_mul(ldfr(q.fixed[q.gate_fixed[3]], idx), c));
-        v = fr_add(v, ldfr(q.fixed[q.gate_fixed[4]], idx));
+        Fr v;
+        if (q.gate_from_out) {  // custom gates evaluated by k_gates_flat
+            v = q.out[idx];
+        } else {  // the standard gate (Horner from zero over its single polynomial)
+            const Fr a = ldfr(q.advice[q.gate_advice[0]], idx);
+            const Fr b = ldfr(q.advice[q.gate_advice[1]], idx);
+            const Fr c = ldfr(q.advice[q.gate_advice[2]], idx);
+            v = fr_mul(ldfr(q.fixed[q.gate_fixed[0]], idx), a);
+            v = fr_add(v, fr_mul(ldfr(q.fixed[q.gate_fixed[1]], idx), b));
+            v = fr_add(v, fr_mul(fr_mul(a, b), ldfr(q.fixed[q.gate_fixed[2]], idx)));
+            v = fr_add(v, fr_mul(ldfr(q.fixed[q.gate_fixed[3]], idx), c));
+            v = fr_add(v, ldfr(q.fixed[q.gate_fixed[4]], idx));
+        }
         Fr l0 = fr_zero(), la = fr_zero();
         if (q.n_sets || q.has_lookup) {
             l0 = ldfr(q.l0, idx);
@@ -108,6 +113,42 @@ __global__ void __launch_bounds__(256) k_quotient(QuotientParams q) {
     }
 }
 
+// The custom gates of any circuit, one thread per row, as the reference's
+// FlatGraphEvaluator::evaluate_chunk (evaluation.rs:530-651): the values buffer
+// lives in the thread's local memory; its constants and challenge slots are
+// loaded once, the previous value (zero) and the column reads per row, then
+// the ops run in order.  Every index was checked on the host against
+// kFlatMaxValues and the column counts.
+__global__ void __launch_bounds__(128) k_gates_flat(FlatParams f) {
+    Fr vals[kFlatMaxValues];
+    for (uint32_t i = 0; i < f.static_len; i++) vals[i] = f.statics[i];
+    const uint32_t E = 1u << f.log_n, mask = E - 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < E; idx += stride) {
+        vals[f.pv_idx] = fr_zero();
+        for (uint32_t r = 0; r < f.n_reads; r++) {
+            const uint32_t* rd = f.reads + 4 * r;
+            vals[rd[3]] = ldfr(f.cols[rd[0]][rd[1]], (idx + f.rot_off[rd[2]]) & mask);
+        }
+        for (uint32_t o = 0; o < f.n_ops; o++) {
+            const uint32_t* op = f.ops + 5 * o;
+            const Fr& a = vals[op[2]];
+            Fr r;
+            switch (op[0]) {
+                case MZK_FLAT_ADD: r = fr_add(a, vals[op[3]]); break;
+                case MZK_FLAT_SUB: r = fr_sub(a, vals[op[3]]); break;
+                case MZK_FLAT_MUL: r = fr_mul(a, vals[op[3]]); break;
+                case MZK_FLAT_SQUARE: r = fr_mul(a, a); break;
+                case MZK_FLAT_DOUBLE: r = fr_add(a, a); break;
+                case MZK_FLAT_NEGATE: r = fr_sub(fr_zero(), a); break;
+                default: r = fr_add(fr_mul(a, vals[op[3]]), vals[op[4]]); break;  // MZK_FLAT_MULADD
+            }
+            vals[op[1]] = r;
+        }
+        f.out[idx] = vals[f.result_idx];
+    }
+}
+
 Fr fr_from_u64s(const uint64_t* p) {
     Fr r;
     std::memcpy(r.l, p, 32);
@@ -117,6 +158,92 @@ Fr fr_from_u64s(const uint64_t* p) {
 // DELTA (GENERATOR^(2^S)), curves/src/bls12_381/fq.rs:501-508
 const uint64_t kDelta[4] = {0x70e310d3d146f96aULL, 0x4b64c08919e299e6ULL, 0x51e114186a8b970dULL,
                             0x6185d06627c067cbULL};
+
+// Checks every index of a flattened gate program, packs it into one device
+// buffer and runs k_gates_flat into d_out.
+Status launch_gates_flat(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, void* d_out, cudaStream_t st) {
+    const mzk_flat_graph& g = *desc->gates;
+    auto fail = [](const std::string& m) {
+        set_error("quotient gates: " + m);
+        return ERR_ARG;
+    };
+    if (desc->n_instance > kQMaxInstance || (desc->n_instance && !desc->instance))
+        return fail("at most 4 instance columns");
+    if (g.values_len == 0 || g.values_len > kFlatMaxValues) return fail("values_len must be in [1, 256]");
+    if (g.n_rotations > kFlatMaxRotations || (g.n_rotations && !g.rotations)) return fail("at most 32 rotations");
+    if ((g.n_constants && !g.constants) || (g.n_reads && !g.reads) || (g.n_ops && !g.ops)) return fail("null array");
+    const uint32_t slots[6] = {g.beta_idx, g.theta_idx, g.trash_challenge_idx, g.y_idx, g.previous_value_idx,
+                               g.result_idx};
+    for (uint32_t v : slots)
+        if (v >= g.values_len) return fail("slot index past values_len");
+    if (g.n_constants > g.values_len) return fail("more constants than values");
+    const uint32_t n_cols[3] = {desc->n_fixed, desc->n_advice, desc->n_instance};
+    for (uint32_t r = 0; r < g.n_reads; r++) {
+        const mzk_column_read& rd = g.reads[r];
+        if (rd.col_type > 2 || rd.col_idx >= n_cols[rd.col_type] || rd.rot_idx >= g.n_rotations ||
+            rd.dst >= g.values_len)
+            return fail("column read " + std::to_string(r) + " out of range");
+    }
+    for (uint32_t o = 0; o < g.n_ops; o++) {
+        const mzk_flat_op& op = g.ops[o];
+        const bool uses_b = op.kind == MZK_FLAT_ADD || op.kind == MZK_FLAT_SUB || op.kind == MZK_FLAT_MUL ||
+                            op.kind == MZK_FLAT_MULADD;
+        if (op.kind > MZK_FLAT_MULADD || op.dst >= g.values_len || op.a >= g.values_len ||
+            (uses_b && op.b >= g.values_len) || (op.kind == MZK_FLAT_MULADD && op.c >= g.values_len))
+            return fail("op " + std::to_string(o) + " out of range");
+    }
+    // statics: constants, then the challenge slots
+    uint32_t static_len = g.n_constants;
+    for (int i = 0; i < 4; i++) static_len = std::max(static_len, slots[i] + 1);
+    std::vector<Fr> statics(static_len, Fr{});
+    for (uint32_t i = 0; i < g.n_constants; i++) statics[i] = fr_from_u64s(g.constants + 4 * i);
+    statics[g.beta_idx] = fr_from_u64s(desc->beta);
+    statics[g.theta_idx] = fr_from_u64s(desc->theta);
+    statics[g.trash_challenge_idx] = fr_from_u64s(desc->trash_challenge);
+    statics[g.y_idx] = fr_from_u64s(desc->y);
+    const uint32_t E = 1u << d->ext_k, log_scale = d->ext_k - d->k;
+    std::vector<uint32_t> words;  // reads | ops | rot_off, then the statics (16-byte aligned)
+    for (uint32_t r = 0; r < g.n_reads; r++)
+        words.insert(words.end(), {g.reads[r].col_type, g.reads[r].col_idx, g.reads[r].rot_idx, g.reads[r].dst});
+    const size_t ops_at = words.size();
+    for (uint32_t o = 0; o < g.n_ops; o++)
+        words.insert(words.end(), {g.ops[o].kind, g.ops[o].dst, g.ops[o].a, g.ops[o].b, g.ops[o].c});
+    const size_t rot_at = words.size();
+    for (uint32_t r = 0; r < g.n_rotations; r++)
+        words.push_back((uint32_t)(((int64_t)g.rotations[r] << log_scale) & (int64_t)(E - 1)));
+    while (words.size() % 4) words.push_back(0);
+    const size_t statics_at = words.size();
+    const size_t bytes = words.size() * 4 + statics.size() * sizeof(Fr);
+    void *dev, *host;
+    MZK_TRY(ctx->ensure("quotient_flat", bytes, &dev));
+    MZK_TRY(ctx->ensure_pinned(bytes, &host));
+    std::memcpy(host, words.data(), words.size() * 4);
+    std::memcpy(static_cast<char*>(host) + statics_at * 4, statics.data(), statics.size() * sizeof(Fr));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, st));
+    FlatParams f;
+    std::memset(&f, 0, sizeof(f));
+    for (uint32_t i = 0; i < desc->n_fixed; i++) f.cols[0][i] = reinterpret_cast<const Fr*>(desc->fixed[i]);
+    for (uint32_t i = 0; i < desc->n_advice; i++) f.cols[1][i] = reinterpret_cast<const Fr*>(desc->advice[i]);
+    for (uint32_t i = 0; i < desc->n_instance; i++) f.cols[2][i] = reinterpret_cast<const Fr*>(desc->instance[i]);
+    const uint32_t* w = static_cast<const uint32_t*>(dev);
+    f.reads = w;
+    f.ops = w + ops_at;
+    f.rot_off = w + rot_at;
+    f.statics = reinterpret_cast<const Fr*>(w + statics_at);
+    f.n_reads = g.n_reads;
+    f.n_ops = g.n_ops;
+    f.static_len = static_len;
+    f.pv_idx = g.previous_value_idx;
+    f.result_idx = g.result_idx;
+    f.log_n = d->ext_k;
+    f.out = static_cast<Fr*>(d_out);
+    const uint32_t blocks = (uint32_t)std::min<uint64_t>((E + 127) / 128, (uint64_t)ctx->num_sms * 16);
+    k_gates_flat<<<blocks, 128, 0, st>>>(f);
+    MZK_LAUNCH_CHECK(ctx);
+    // the pinned staging may be reused by the next call: let this copy finish
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    return OK;
+}
 
 }  // namespace
 
@@ -141,14 +268,18 @@ Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_de
     std::memset(&q, 0, sizeof(q));
     for (uint32_t i = 0; i < desc->n_advice; i++) q.advice[i] = reinterpret_cast<const Fr*>(desc->advice[i]);
     for (uint32_t i = 0; i < desc->n_fixed; i++) q.fixed[i] = reinterpret_cast<const Fr*>(desc->fixed[i]);
-    for (int i = 0; i < 5; i++) {
+    if (desc->gates) {
+        MZK_TRY(launch_gates_flat(ctx, d, desc, d_out, st));
+        q.gate_from_out = 1;
+    }
+    for (int i = 0; i < 5 && !desc->gates; i++) {
         if (desc->gate_fixed[i] >= desc->n_fixed) {
             set_error("quotient: gate fixed column out of range");
             return ERR_ARG;
         }
         q.gate_fixed[i] = desc->gate_fixed[i];
     }
-    for (int i = 0; i < 3; i++) {
+    for (int i = 0; i < 3 && !desc->gates; i++) {
         if (desc->gate_advice[i] >= desc->n_advice) {
             set_error("quotient: gate advice column out of range");
             return ERR_ARG;

@@ -29,6 +29,19 @@ struct QuotientParams {
     uint32_t lookup_input, lookup_table;
     uint32_t tlen, log_n, log_scale;
     int32_t divide;
+    int32_t gate_from_out;  // the custom-gate value of each row is already in out (k_gates_flat)
+};
+
+// custom gates as the reference's flattened program (mzk_flat_graph)
+constexpr uint32_t kQMaxInstance = 4, kFlatMaxValues = 256, kFlatMaxRotations = 32;
+struct FlatParams {
+    const Fr* cols[3][kQMaxFixed > kQMaxAdvice ? kQMaxFixed : kQMaxAdvice];  // fixed, advice, instance
+    const uint32_t* reads;   // n_reads x (col_type, col_idx, rot_idx, dst)
+    const uint32_t* ops;     // n_ops x (kind, dst, a, b, c)
+    const Fr* statics;       // values [0, static_len): constants and challenge slots
+    const uint32_t* rot_off; // per rotation: (rot << log_scale) mod 2^log_n
+    uint32_t n_reads, n_ops, static_len, pv_idx, result_idx, log_n;
+    Fr* out;
 };
 
 // compute_h_poly (proofs/src/plonk/prover.rs:701-771) without the transcript:

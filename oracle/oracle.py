@@ -126,6 +126,51 @@ class QuotientDesc(ctypes.Structure):
 ]
 
 
+def flat_gates_eval(graph, fixed, advice, instance, k, extended_k, beta, theta, trash_challenge, y):
+    """The custom-gate values of every row of the extended coset, restating
+    FlatGraphEvaluator::evaluate_chunk (proofs/src/plonk/evaluation.rs:530-651)
+    with the previous value zero (the gates are the first pass of
+    evaluate_numerator, :846-856).  `graph` is a dict with the FlatGraph fields:
+    constants, rotations, reads [(col_type, col_idx, rot_idx, dst)], ops
+    [(kind, dst, a, b, c)], values_len and the slot indices; kinds in
+    FlatOpKind order (:134-143).  Pure Python over single-element oracle field
+    operations: small domains only."""
+    E, scale = 1 << extended_k, extended_k - k
+    zero = np.zeros(4, np.uint64)
+    template = [zero] * graph["values_len"]
+    for i, c in enumerate(graph["constants"]):
+        template[i] = np.asarray(c, np.uint64)
+    template[graph["beta_idx"]] = np.asarray(beta, np.uint64)
+    template[graph["theta_idx"]] = np.asarray(theta, np.uint64)
+    template[graph["trash_challenge_idx"]] = np.asarray(trash_challenge, np.uint64)
+    template[graph["y_idx"]] = np.asarray(y, np.uint64)
+    cols = (fixed, advice, instance)
+    out = np.zeros((E, 4), np.uint64)
+    for idx in range(E):
+        vals = list(template)
+        vals[graph["previous_value_idx"]] = zero
+        for t, c, r, dst in graph["reads"]:
+            vals[dst] = cols[t][c][(idx + (graph["rotations"][r] << scale)) % E]
+        for kind, dst, a, b, c in graph["ops"]:
+            if kind == 0:
+                v = fr_op("add", vals[a], vals[b])
+            elif kind == 1:
+                v = fr_op("sub", vals[a], vals[b])
+            elif kind == 2:
+                v = fr_op("mul", vals[a], vals[b])
+            elif kind == 3:
+                v = fr_op("mul", vals[a], vals[a])
+            elif kind == 4:
+                v = fr_op("add", vals[a], vals[a])
+            elif kind == 5:
+                v = fr_op("neg", vals[a])
+            else:
+                v = fr_op("add", fr_op("mul", vals[a], vals[b]), vals[c])
+            vals[dst] = v
+        out[idx] = vals[graph["result_idx"]]
+    return out
+
+
 def threads_default():
     return int(os.environ.get("MZK_ORACLE_THREADS", os.cpu_count() or 1))
 

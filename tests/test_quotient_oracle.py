@@ -130,3 +130,27 @@ def test_oracle_quotient_matches_python(n_perm, n_sets, sel):
         want = python_numerator(cols, k, ek, val(cols["y"]), val(cols["beta"]), val(cols["gamma"]),
                                 val(d.get(3)), val(d.get(2)), divide, tinv)
         assert [val(x) for x in got] == want
+
+
+def test_flat_gates_restatement_matches_direct_evaluation():
+    """The oracle's restatement of FlatGraphEvaluator::evaluate_chunk on the
+    sample program equals the three gates evaluated directly with Python
+    integers (rotations in the extended domain scaled by 2^(ek - k))."""
+    from _gates import sample_graph
+    k, ek = 3, 5
+    E, scale = 1 << ek, ek - k
+    fixed = [column(900 + i, E) for i in range(3)]
+    advice = [column(910 + i, E) for i in range(3)]
+    instance = [column(920, E)]
+    c0, y, beta, theta, trash = (O.rand_fr(930 + i, 1)[0] for i in range(5))
+    got = O.flat_gates_eval(sample_graph(c0), fixed, advice, instance, k, ek, beta, theta, trash, y)
+    F = [[val(c[i]) for i in range(E)] for c in fixed]
+    A = [[val(c[i]) for i in range(E)] for c in advice]
+    I0 = [val(instance[0][i]) for i in range(E)]
+    yv, th, cv = val(y), val(theta), val(c0)
+    for idx in range(E):
+        nxt, prv = (idx + (1 << scale)) % E, (idx - (1 << scale)) % E
+        g1 = F[0][idx] * A[0][idx] * A[1][nxt] + A[2][idx] - cv
+        g2 = A[1][idx] ** 2 - 2 * A[0][prv] * F[1][idx]
+        g3 = -(A[2][idx] * F[2][idx]) + A[0][nxt] * th + I0[idx]
+        assert val(got[idx]) == ((g1 * yv + g2) * yv + g3) % R, idx
