@@ -195,14 +195,39 @@ typedef struct {
     uint32_t values_len;
     uint32_t beta_idx, theta_idx, trash_challenge_idx, y_idx, previous_value_idx, result_idx;
 } mzk_flat_graph;
+/* A logup argument of any shape (Evaluator::lookups_flat, evaluation.rs:
+ * 686-767; its constraint terms :1034-1090): one program per helper column
+ * (per chunk of input expressions) computing, in its values buffer, the sum of
+ * the partial products sum_j prod_{k!=j} (f_k + beta), the product
+ * prod_j (f_j + beta), the compressed table + beta and the selector; outputs
+ * holds those four value indices per helper (the table and selector are read
+ * from the first helper's program, as the reference does). */
+typedef struct {
+    uint32_t n_helpers;
+    const mzk_flat_graph *programs;   /* n_helpers */
+    const uint32_t *outputs;          /* n_helpers x 4: sum_partial_products, product, table, selector */
+    const uint64_t *const *helpers;   /* n_helpers extended cosets, DEVICE */
+    const uint64_t *aggregator;       /* Z, extended coset, DEVICE */
+    const uint64_t *multiplicities;   /* m, extended coset, DEVICE */
+} mzk_lookup_arg;
+/* A trash argument (trash/prover.rs; its constraint term evaluation.rs:
+ * 1093-1109): the program compresses the constraint expressions with the
+ * trash challenge (result_idx), the term is compressed - (1 - q) trash. */
+typedef struct {
+    mzk_flat_graph program;
+    uint32_t selector_fixed;          /* fixed column q */
+    const uint64_t *trash;            /* trash polynomial, extended coset, DEVICE */
+} mzk_trash_arg;
 
 /* Columns are extended-domain (coset) evaluations, 2^extended_k Fr each,
  * DEVICE pointers, given through HOST arrays of pointers.  Circuit shape: one
  * standard gate q_l a + q_r b + q_m a b + q_o c + q_c, or any custom gates given
  * as a flattened program (`gates`), permutation sets over advice/fixed columns
- * (chunk_len = cs.degree() - 2 columns each), at most one logup lookup with
- * one input column and one helper, no trashcans.  Limits: 16 advice, 16
- * fixed, 4 instance, 16 permutation columns, 8 sets.  extended_omega and
+ * (chunk_len = cs.degree() - 2 columns each), then either the built-in logup
+ * lookup (one input column, one helper: has_lookup) or lookups and trashcans
+ * of any shape as programs (`lookups`, `trash`).  Limits: 16 advice, 16 fixed,
+ * 4 instance, 16 permutation columns, 8 sets, 8 lookups of 8 helpers each,
+ * 8 trashcans.  extended_omega and
  * g_coset are taken from the domain (the fields exist for layout parity with
  * the CPU restatement). */
 typedef struct {
@@ -232,6 +257,10 @@ typedef struct {
     const mzk_flat_graph *gates;
     const uint64_t *const *instance; uint32_t n_instance;
     uint64_t trash_challenge[4];
+    /* lookups and trashcans of any shape as programs (used when has_lookup
+     * is 0): their terms follow the permutation terms in the reference's order */
+    uint32_t n_lookups; const mzk_lookup_arg *lookups;
+    uint32_t n_trash; const mzk_trash_arg *trash;
 } mzk_quotient_desc;
 /* d_out (2^extended_k Fr) = nu(X) on the extended coset; with divide != 0,
  * h(X) = nu(X) / (X^n - 1) (evaluate_numerator + divide_by_vanishing_poly,

@@ -152,6 +152,8 @@ class QuotientDesc(ctypes.Structure):
     ("theta", ctypes.c_uint64 * 4), ("extended_omega", ctypes.c_uint64 * 4), ("g_coset", ctypes.c_uint64 * 4),
     ("gates", ctypes.c_void_p), ("instance", ctypes.POINTER(ctypes.c_void_p)), ("n_instance", ctypes.c_uint32),
     ("trash_challenge", ctypes.c_uint64 * 4),
+    ("n_lookups", ctypes.c_uint32), ("lookups", ctypes.c_void_p), ("n_trash", ctypes.c_uint32),
+    ("trash", ctypes.c_void_p),
 ]
 
 # FlatOpKind (proofs/src/plonk/evaluation.rs:134-143), MZK_FLAT_* in include/mzk.h
@@ -204,6 +206,18 @@ def build_flat_graph(constants, rotations, reads, ops, values_len, beta_idx, the
     return g
 
 
+class LookupArg(ctypes.Structure):
+    """mzk_lookup_arg: a logup argument of any shape as one program per helper."""
+    _fields_ = [("n_helpers", ctypes.c_uint32), ("programs", ctypes.POINTER(FlatGraph)),
+                ("outputs", ctypes.POINTER(ctypes.c_uint32)), ("helpers", ctypes.POINTER(ctypes.c_void_p)),
+                ("aggregator", ctypes.c_void_p), ("multiplicities", ctypes.c_void_p)]
+
+
+class TrashArg(ctypes.Structure):
+    """mzk_trash_arg: a trash argument (program, selector column, trash polynomial)."""
+    _fields_ = [("program", FlatGraph), ("selector_fixed", ctypes.c_uint32), ("trash", ctypes.c_void_p)]
+
+
 def build_quotient_desc(cols, k, extended_k, addr):
     """Fill a QuotientDesc from `cols` (a dict of column objects and parameters);
     addr(x) turns each column object into an address (device pointer or host
@@ -249,6 +263,32 @@ def build_quotient_desc(cols, k, extended_k, addr):
         d.gates = ctypes.addressof(cols["gates"])
     inst = cols.get("instance", [])
     d.instance, d.n_instance = ptr_array(inst), len(inst)
+    # lookups / trashcans as programs: [{"programs": [FlatGraph], "outputs": [(spp, prod, table, sel)],
+    # "helpers": [col], "aggregator": col, "multiplicities": col}], [{"program": FlatGraph, "selector": i,
+    # "trash": col}]
+    lps = cols.get("lookup_programs", [])
+    if lps:
+        arr = (LookupArg * len(lps))()
+        for n, lp in enumerate(lps):
+            progs = (FlatGraph * len(lp["programs"]))(*lp["programs"])
+            outs = (ctypes.c_uint32 * (4 * len(lp["outputs"])))(*[v for o in lp["outputs"] for v in o])
+            keep.extend([progs, outs] + list(lp["programs"]))
+            arr[n].n_helpers = len(lp["programs"])
+            arr[n].programs = ctypes.cast(progs, ctypes.POINTER(FlatGraph))
+            arr[n].outputs = ctypes.cast(outs, ctypes.POINTER(ctypes.c_uint32))
+            arr[n].helpers = ptr_array(lp["helpers"])
+            arr[n].aggregator, arr[n].multiplicities = addr(lp["aggregator"]), addr(lp["multiplicities"])
+        keep.append(arr)
+        d.n_lookups, d.lookups = len(lps), ctypes.addressof(arr)
+    tcs = cols.get("trash", [])
+    if tcs:
+        arr = (TrashArg * len(tcs))()
+        for n, tc in enumerate(tcs):
+            arr[n].program = tc["program"]
+            arr[n].selector_fixed, arr[n].trash = tc["selector"], addr(tc["trash"])
+            keep.append(tc["program"])
+        keep.append(arr)
+        d.n_trash, d.trash = len(tcs), ctypes.addressof(arr)
     d._keep = keep
     return d
 

@@ -113,39 +113,94 @@ __global__ void __launch_bounds__(256) k_quotient(QuotientParams q) {
     }
 }
 
-// The custom gates of any circuit, one thread per row, as the reference's
-// FlatGraphEvaluator::evaluate_chunk (evaluation.rs:530-651): the values buffer
-// lives in the thread's local memory; its constants and challenge slots are
-// loaded once, the previous value (zero) and the column reads per row, then
-// the ops run in order.  Every index was checked on the host against
-// kFlatMaxValues and the column counts.
-__global__ void __launch_bounds__(128) k_gates_flat(FlatParams f) {
+// One row of a packed program, as FlatGraphEvaluator::evaluate
+// (evaluation.rs:530-651): statics, the previous value (zero: every program
+// here starts from zero), the column reads at their rotations, then the ops.
+// Every index was checked on the host against kFlatMaxValues and the column
+// counts.
+__device__ void run_program(const uint32_t* __restrict__ W, uint32_t h, const FlatCols& cols, uint32_t idx,
+                            uint32_t mask, Fr* vals) {
+    const uint32_t n_reads = W[h], n_ops = W[h + 1], static_len = W[h + 2], pv = W[h + 3];
+    const uint32_t* reads = W + W[h + 5];
+    const uint32_t* ops = W + W[h + 6];
+    const uint32_t* rot_off = W + W[h + 7];
+    const Fr* statics = reinterpret_cast<const Fr*>(W + W[h + 8]);
+    for (uint32_t i = 0; i < static_len; i++) vals[i] = statics[i];
+    vals[pv] = fr_zero();
+    for (uint32_t r = 0; r < n_reads; r++) {
+        const uint32_t* rd = reads + 4 * r;
+        vals[rd[3]] = ldfr(cols.c[rd[0]][rd[1]], (idx + rot_off[rd[2]]) & mask);
+    }
+    for (uint32_t o = 0; o < n_ops; o++) {
+        const uint32_t* op = ops + 5 * o;
+        const Fr& a = vals[op[2]];
+        Fr r;
+        switch (op[0]) {
+            case MZK_FLAT_ADD: r = fr_add(a, vals[op[3]]); break;
+            case MZK_FLAT_SUB: r = fr_sub(a, vals[op[3]]); break;
+            case MZK_FLAT_MUL: r = fr_mul(a, vals[op[3]]); break;
+            case MZK_FLAT_SQUARE: r = fr_mul(a, a); break;
+            case MZK_FLAT_DOUBLE: r = fr_add(a, a); break;
+            case MZK_FLAT_NEGATE: r = fr_sub(fr_zero(), a); break;
+            default: r = fr_add(fr_mul(a, vals[op[3]]), vals[op[4]]); break;  // MZK_FLAT_MULADD
+        }
+        vals[op[1]] = r;
+    }
+}
+
+// The custom gates of any circuit, one thread per row (the first pass of
+// evaluate_numerator, evaluation.rs:846-856); the values buffer lives in the
+// thread's local memory.
+__global__ void __launch_bounds__(128) k_gates_flat(GatesParams g) {
     Fr vals[kFlatMaxValues];
-    for (uint32_t i = 0; i < f.static_len; i++) vals[i] = f.statics[i];
-    const uint32_t E = 1u << f.log_n, mask = E - 1;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t E = 1u << g.log_n, mask = E - 1, stride = gridDim.x * blockDim.x;
+    const uint32_t result = g.words[g.prog + 4];
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < E; idx += stride) {
-        vals[f.pv_idx] = fr_zero();
-        for (uint32_t r = 0; r < f.n_reads; r++) {
-            const uint32_t* rd = f.reads + 4 * r;
-            vals[rd[3]] = ldfr(f.cols[rd[0]][rd[1]], (idx + f.rot_off[rd[2]]) & mask);
-        }
-        for (uint32_t o = 0; o < f.n_ops; o++) {
-            const uint32_t* op = f.ops + 5 * o;
-            const Fr& a = vals[op[2]];
-            Fr r;
-            switch (op[0]) {
-                case MZK_FLAT_ADD: r = fr_add(a, vals[op[3]]); break;
-                case MZK_FLAT_SUB: r = fr_sub(a, vals[op[3]]); break;
-                case MZK_FLAT_MUL: r = fr_mul(a, vals[op[3]]); break;
-                case MZK_FLAT_SQUARE: r = fr_mul(a, a); break;
-                case MZK_FLAT_DOUBLE: r = fr_add(a, a); break;
-                case MZK_FLAT_NEGATE: r = fr_sub(fr_zero(), a); break;
-                default: r = fr_add(fr_mul(a, vals[op[3]]), vals[op[4]]); break;  // MZK_FLAT_MULADD
+        run_program(g.words, g.prog, g.cols, idx, mask, vals);
+        g.out[idx] = vals[result];
+    }
+}
+
+// The lookup terms (evaluation.rs:1034-1090) and trash terms (:1093-1109) of
+// any shape, continuing each row's y-Horner accumulator from out (custom
+// gates and permutation terms), then the division by t(X).
+__global__ void __launch_bounds__(128) k_tail_flat(TailParams t) {
+    Fr vals[kFlatMaxValues];
+    const uint32_t E = 1u << t.log_n, mask = E - 1, stride = gridDim.x * blockDim.x;
+    const Fr one = fr_one();
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < E; idx += stride) {
+        const uint32_t r_next = (idx + (1u << t.log_scale)) & mask;
+        Fr v = t.out[idx];
+        if (t.n_lookups) {
+            const Fr l0 = ldfr(t.l0, idx), ll = ldfr(t.l_last, idx), la = ldfr(t.l_active, idx);
+            for (uint32_t n = 0; n < t.n_lookups; n++) {
+                const Fr Z = ldfr(t.agg[n], idx);
+                v = fr_add(fr_mul(v, t.y), fr_mul(Z, fr_add(l0, ll)));
+                Fr sum_h = fr_zero(), table = fr_zero(), sel = fr_zero();
+                for (uint32_t fi = 0; fi < t.n_helpers[n]; fi++) {
+                    run_program(t.words, t.prog[n][fi], t.cols, idx, mask, vals);
+                    const uint32_t* o = t.outputs[n][fi];
+                    if (fi == 0) {
+                        table = vals[o[2]];
+                        sel = vals[o[3]];
+                    }
+                    const Fr h = ldfr(t.helper[n][fi], idx);
+                    v = fr_sub(fr_add(fr_mul(v, t.y), fr_mul(h, vals[o[1]])), vals[o[0]]);
+                    sum_h = fr_add(sum_h, h);
+                }
+                Fr u = fr_sub(fr_sub(ldfr(t.agg[n], r_next), Z), fr_mul(sel, sum_h));
+                u = fr_add(fr_mul(u, table), ldfr(t.mult[n], idx));
+                v = fr_add(fr_mul(v, t.y), fr_mul(la, u));
             }
-            vals[op[1]] = r;
         }
-        f.out[idx] = vals[f.result_idx];
+        for (uint32_t n = 0; n < t.n_trash; n++) {
+            run_program(t.words, t.trash_prog[n], t.cols, idx, mask, vals);
+            const Fr q = ldfr(t.cols.c[0][t.trash_sel[n]], idx);
+            const Fr compressed = vals[t.words[t.trash_prog[n] + 4]];
+            v = fr_add(fr_mul(v, t.y), fr_sub(compressed, fr_mul(fr_sub(one, q), ldfr(t.trash[n], idx))));
+        }
+        if (t.divide) v = fr_mul(v, t.tinv[idx & (t.tlen - 1)]);
+        t.out[idx] = v;
     }
 }
 
@@ -159,30 +214,23 @@ Fr fr_from_u64s(const uint64_t* p) {
 const uint64_t kDelta[4] = {0x70e310d3d146f96aULL, 0x4b64c08919e299e6ULL, 0x51e114186a8b970dULL,
                             0x6185d06627c067cbULL};
 
-// Checks every index of a flattened gate program, packs it into one device
-// buffer and runs k_gates_flat into d_out.
-Status launch_gates_flat(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, void* d_out, cudaStream_t st) {
-    const mzk_flat_graph& g = *desc->gates;
-    auto fail = [](const std::string& m) {
-        set_error("quotient gates: " + m);
-        return ERR_ARG;
-    };
-    if (desc->n_instance > kQMaxInstance || (desc->n_instance && !desc->instance))
-        return fail("at most 4 instance columns");
-    if (g.values_len == 0 || g.values_len > kFlatMaxValues) return fail("values_len must be in [1, 256]");
-    if (g.n_rotations > kFlatMaxRotations || (g.n_rotations && !g.rotations)) return fail("at most 32 rotations");
-    if ((g.n_constants && !g.constants) || (g.n_reads && !g.reads) || (g.n_ops && !g.ops)) return fail("null array");
+// Appends a flattened program to W after checking every index; returns its
+// header offset, or sets `err`.
+uint32_t pack_program(std::vector<uint32_t>& W, const mzk_flat_graph& g, const uint32_t n_cols[3],
+                      const mzk_quotient_desc* desc, uint32_t log_scale, uint32_t E, std::string& err) {
+    if (g.values_len == 0 || g.values_len > kFlatMaxValues) return err = "values_len must be in [1, 256]", 0;
+    if (g.n_rotations > kFlatMaxRotations || (g.n_rotations && !g.rotations)) return err = "at most 32 rotations", 0;
+    if ((g.n_constants && !g.constants) || (g.n_reads && !g.reads) || (g.n_ops && !g.ops)) return err = "null array", 0;
     const uint32_t slots[6] = {g.beta_idx, g.theta_idx, g.trash_challenge_idx, g.y_idx, g.previous_value_idx,
                                g.result_idx};
     for (uint32_t v : slots)
-        if (v >= g.values_len) return fail("slot index past values_len");
-    if (g.n_constants > g.values_len) return fail("more constants than values");
-    const uint32_t n_cols[3] = {desc->n_fixed, desc->n_advice, desc->n_instance};
+        if (v >= g.values_len) return err = "slot index past values_len", 0;
+    if (g.n_constants > g.values_len) return err = "more constants than values", 0;
     for (uint32_t r = 0; r < g.n_reads; r++) {
         const mzk_column_read& rd = g.reads[r];
         if (rd.col_type > 2 || rd.col_idx >= n_cols[rd.col_type] || rd.rot_idx >= g.n_rotations ||
             rd.dst >= g.values_len)
-            return fail("column read " + std::to_string(r) + " out of range");
+            return err = "column read " + std::to_string(r) + " out of range", 0;
     }
     for (uint32_t o = 0; o < g.n_ops; o++) {
         const mzk_flat_op& op = g.ops[o];
@@ -190,9 +238,8 @@ Status launch_gates_flat(Context* ctx, const Domain* d, const mzk_quotient_desc*
                             op.kind == MZK_FLAT_MULADD;
         if (op.kind > MZK_FLAT_MULADD || op.dst >= g.values_len || op.a >= g.values_len ||
             (uses_b && op.b >= g.values_len) || (op.kind == MZK_FLAT_MULADD && op.c >= g.values_len))
-            return fail("op " + std::to_string(o) + " out of range");
+            return err = "op " + std::to_string(o) + " out of range", 0;
     }
-    // statics: constants, then the challenge slots
     uint32_t static_len = g.n_constants;
     for (int i = 0; i < 4; i++) static_len = std::max(static_len, slots[i] + 1);
     std::vector<Fr> statics(static_len, Fr{});
@@ -201,47 +248,98 @@ Status launch_gates_flat(Context* ctx, const Domain* d, const mzk_quotient_desc*
     statics[g.theta_idx] = fr_from_u64s(desc->theta);
     statics[g.trash_challenge_idx] = fr_from_u64s(desc->trash_challenge);
     statics[g.y_idx] = fr_from_u64s(desc->y);
-    const uint32_t E = 1u << d->ext_k, log_scale = d->ext_k - d->k;
-    std::vector<uint32_t> words;  // reads | ops | rot_off, then the statics (16-byte aligned)
+    const uint32_t h = (uint32_t)W.size();
+    W.resize(h + kFlatHeaderWords);
+    W[h] = g.n_reads;
+    W[h + 1] = g.n_ops;
+    W[h + 2] = static_len;
+    W[h + 3] = g.previous_value_idx;
+    W[h + 4] = g.result_idx;
+    W[h + 5] = (uint32_t)W.size();
     for (uint32_t r = 0; r < g.n_reads; r++)
-        words.insert(words.end(), {g.reads[r].col_type, g.reads[r].col_idx, g.reads[r].rot_idx, g.reads[r].dst});
-    const size_t ops_at = words.size();
+        W.insert(W.end(), {g.reads[r].col_type, g.reads[r].col_idx, g.reads[r].rot_idx, g.reads[r].dst});
+    W[h + 6] = (uint32_t)W.size();
     for (uint32_t o = 0; o < g.n_ops; o++)
-        words.insert(words.end(), {g.ops[o].kind, g.ops[o].dst, g.ops[o].a, g.ops[o].b, g.ops[o].c});
-    const size_t rot_at = words.size();
+        W.insert(W.end(), {g.ops[o].kind, g.ops[o].dst, g.ops[o].a, g.ops[o].b, g.ops[o].c});
+    W[h + 7] = (uint32_t)W.size();
     for (uint32_t r = 0; r < g.n_rotations; r++)
-        words.push_back((uint32_t)(((int64_t)g.rotations[r] << log_scale) & (int64_t)(E - 1)));
-    while (words.size() % 4) words.push_back(0);
-    const size_t statics_at = words.size();
-    const size_t bytes = words.size() * 4 + statics.size() * sizeof(Fr);
+        W.push_back((uint32_t)(((int64_t)g.rotations[r] << log_scale) & (int64_t)(E - 1)));
+    while (W.size() % 4) W.push_back(0);
+    W[h + 8] = (uint32_t)W.size();
+    const size_t at = W.size();
+    W.resize(at + statics.size() * 8);
+    std::memcpy(W.data() + at, statics.data(), statics.size() * sizeof(Fr));
+    return h;
+}
+
+// Checks and packs every program of the descriptor (gates, lookup helpers,
+// trashcans) into one device buffer and fills the parameters of the two
+// program kernels.
+Status pack_programs(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, GatesParams& gp, TailParams& tp,
+                     cudaStream_t st) {
+    std::string err;
+    auto fail = [&](const std::string& m) {
+        set_error("quotient programs: " + m);
+        return ERR_ARG;
+    };
+    if (desc->n_instance > kQMaxInstance || (desc->n_instance && !desc->instance))
+        return fail("at most 4 instance columns");
+    if (desc->n_lookups > kQMaxLookups || (desc->n_lookups && !desc->lookups)) return fail("at most 8 lookups");
+    if (desc->n_trash > kQMaxTrash || (desc->n_trash && !desc->trash)) return fail("at most 8 trashcans");
+    const uint32_t n_cols[3] = {desc->n_fixed, desc->n_advice, desc->n_instance};
+    const uint32_t E = 1u << d->ext_k, log_scale = d->ext_k - d->k;
+    FlatCols cols;
+    std::memset(&cols, 0, sizeof(cols));
+    for (uint32_t i = 0; i < desc->n_fixed; i++) cols.c[0][i] = reinterpret_cast<const Fr*>(desc->fixed[i]);
+    for (uint32_t i = 0; i < desc->n_advice; i++) cols.c[1][i] = reinterpret_cast<const Fr*>(desc->advice[i]);
+    for (uint32_t i = 0; i < desc->n_instance; i++) cols.c[2][i] = reinterpret_cast<const Fr*>(desc->instance[i]);
+    std::vector<uint32_t> W;
+    if (desc->gates) {
+        gp.prog = pack_program(W, *desc->gates, n_cols, desc, log_scale, E, err);
+        if (!err.empty()) return fail("gates: " + err);
+    }
+    for (uint32_t n = 0; n < desc->n_lookups; n++) {
+        const mzk_lookup_arg& L = desc->lookups[n];
+        if (L.n_helpers == 0 || L.n_helpers > kQMaxHelpers || !L.programs || !L.outputs || !L.helpers ||
+            !L.aggregator || !L.multiplicities)
+            return fail("lookup " + std::to_string(n) + ": 1..8 helpers and every column needed");
+        tp.agg[n] = reinterpret_cast<const Fr*>(L.aggregator);
+        tp.mult[n] = reinterpret_cast<const Fr*>(L.multiplicities);
+        tp.n_helpers[n] = L.n_helpers;
+        for (uint32_t fi = 0; fi < L.n_helpers; fi++) {
+            tp.prog[n][fi] = pack_program(W, L.programs[fi], n_cols, desc, log_scale, E, err);
+            if (!err.empty()) return fail("lookup " + std::to_string(n) + " helper " + std::to_string(fi) + ": " + err);
+            for (int q = 0; q < 4; q++) {
+                if (L.outputs[4 * fi + q] >= L.programs[fi].values_len)
+                    return fail("lookup " + std::to_string(n) + ": output index past values_len");
+                tp.outputs[n][fi][q] = L.outputs[4 * fi + q];
+            }
+            tp.helper[n][fi] = reinterpret_cast<const Fr*>(L.helpers[fi]);
+        }
+    }
+    tp.n_lookups = desc->n_lookups;
+    for (uint32_t n = 0; n < desc->n_trash; n++) {
+        const mzk_trash_arg& T = desc->trash[n];
+        if (T.selector_fixed >= desc->n_fixed || !T.trash) return fail("trashcan " + std::to_string(n) + " columns");
+        tp.trash_prog[n] = pack_program(W, T.program, n_cols, desc, log_scale, E, err);
+        if (!err.empty()) return fail("trashcan " + std::to_string(n) + ": " + err);
+        tp.trash_sel[n] = T.selector_fixed;
+        tp.trash[n] = reinterpret_cast<const Fr*>(T.trash);
+    }
+    tp.n_trash = desc->n_trash;
+    const size_t bytes = W.size() * 4;
     void *dev, *host;
     MZK_TRY(ctx->ensure("quotient_flat", bytes, &dev));
     MZK_TRY(ctx->ensure_pinned(bytes, &host));
-    std::memcpy(host, words.data(), words.size() * 4);
-    std::memcpy(static_cast<char*>(host) + statics_at * 4, statics.data(), statics.size() * sizeof(Fr));
+    std::memcpy(host, W.data(), bytes);
     MZK_CUDA_CHECK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, st));
-    FlatParams f;
-    std::memset(&f, 0, sizeof(f));
-    for (uint32_t i = 0; i < desc->n_fixed; i++) f.cols[0][i] = reinterpret_cast<const Fr*>(desc->fixed[i]);
-    for (uint32_t i = 0; i < desc->n_advice; i++) f.cols[1][i] = reinterpret_cast<const Fr*>(desc->advice[i]);
-    for (uint32_t i = 0; i < desc->n_instance; i++) f.cols[2][i] = reinterpret_cast<const Fr*>(desc->instance[i]);
-    const uint32_t* w = static_cast<const uint32_t*>(dev);
-    f.reads = w;
-    f.ops = w + ops_at;
-    f.rot_off = w + rot_at;
-    f.statics = reinterpret_cast<const Fr*>(w + statics_at);
-    f.n_reads = g.n_reads;
-    f.n_ops = g.n_ops;
-    f.static_len = static_len;
-    f.pv_idx = g.previous_value_idx;
-    f.result_idx = g.result_idx;
-    f.log_n = d->ext_k;
-    f.out = static_cast<Fr*>(d_out);
-    const uint32_t blocks = (uint32_t)std::min<uint64_t>((E + 127) / 128, (uint64_t)ctx->num_sms * 16);
-    k_gates_flat<<<blocks, 128, 0, st>>>(f);
-    MZK_LAUNCH_CHECK(ctx);
-    // the pinned staging may be reused by the next call: let this copy finish
+    // the pinned staging may be reused by the next call: let the copy finish
     MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    gp.cols = cols;
+    tp.cols = cols;
+    gp.words = tp.words = static_cast<const uint32_t*>(dev);
+    gp.log_n = tp.log_n = d->ext_k;
+    tp.log_scale = log_scale;
     return OK;
 }
 
@@ -268,8 +366,22 @@ Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_de
     std::memset(&q, 0, sizeof(q));
     for (uint32_t i = 0; i < desc->n_advice; i++) q.advice[i] = reinterpret_cast<const Fr*>(desc->advice[i]);
     for (uint32_t i = 0; i < desc->n_fixed; i++) q.fixed[i] = reinterpret_cast<const Fr*>(desc->fixed[i]);
+    const bool tail = desc->n_lookups || desc->n_trash;
+    if (tail && desc->has_lookup) {
+        set_error("quotient: give either the built-in lookup (has_lookup) or lookup / trash programs");
+        return ERR_ARG;
+    }
+    GatesParams gp;
+    TailParams tp;
+    std::memset(&gp, 0, sizeof(gp));
+    std::memset(&tp, 0, sizeof(tp));
+    if (desc->gates || tail) MZK_TRY(pack_programs(ctx, d, desc, gp, tp, st));
+    const uint32_t E_rows = 1u << d->ext_k;
+    const uint32_t prog_blocks = (uint32_t)std::min<uint64_t>((E_rows + 127) / 128, (uint64_t)ctx->num_sms * 16);
     if (desc->gates) {
-        MZK_TRY(launch_gates_flat(ctx, d, desc, d_out, st));
+        gp.out = static_cast<Fr*>(d_out);
+        k_gates_flat<<<prog_blocks, 128, 0, st>>>(gp);
+        MZK_LAUNCH_CHECK(ctx);
         q.gate_from_out = 1;
     }
     for (int i = 0; i < 5 && !desc->gates; i++) {
@@ -336,10 +448,27 @@ Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_de
     q.log_n = d->ext_k;
     q.log_scale = d->ext_k - d->k;
     q.out = static_cast<Fr*>(d_out);
+    if (tail) q.divide = 0;  // the division comes after the lookup and trash terms
     const uint32_t E = 1u << d->ext_k;
     const uint32_t blocks = (uint32_t)std::min<uint64_t>((E + 255) / 256, (uint64_t)ctx->num_sms * 8);
     k_quotient<<<blocks, 256, 0, st>>>(q);
     MZK_LAUNCH_CHECK(ctx);
+    if (tail) {
+        if (desc->n_lookups && (!desc->l0 || !desc->l_last || !desc->l_active)) {
+            set_error("quotient: lookups need l0, l_last and l_active");
+            return ERR_ARG;
+        }
+        tp.l0 = reinterpret_cast<const Fr*>(desc->l0);
+        tp.l_last = reinterpret_cast<const Fr*>(desc->l_last);
+        tp.l_active = reinterpret_cast<const Fr*>(desc->l_active);
+        tp.tinv = static_cast<const Fr*>(d->d_tinv);
+        tp.tlen = (uint32_t)d->t_inv.size();
+        tp.y = q.y;
+        tp.divide = divide ? 1 : 0;
+        tp.out = static_cast<Fr*>(d_out);
+        k_tail_flat<<<prog_blocks, 128, 0, st>>>(tp);
+        MZK_LAUNCH_CHECK(ctx);
+    }
     return OK;
 }
 

@@ -32,15 +32,41 @@ struct QuotientParams {
     int32_t gate_from_out;  // the custom-gate value of each row is already in out (k_gates_flat)
 };
 
-// custom gates as the reference's flattened program (mzk_flat_graph)
+// Flattened programs (mzk_flat_graph: custom gates, lookup helpers,
+// trashcans), packed into one device word buffer.  A program's header at word
+// h: n_reads, n_ops, static_len, previous_value_idx, result_idx, then the word
+// offsets of its reads (4 words each: col_type, col_idx, rot_idx, dst), ops (5
+// words: kind, dst, a, b, c), rotation offsets ((rot << log_scale) mod 2^log_n)
+// and statics (Fr values [0, static_len): constants and challenge slots,
+// 16-byte aligned).
 constexpr uint32_t kQMaxInstance = 4, kFlatMaxValues = 256, kFlatMaxRotations = 32;
-struct FlatParams {
-    const Fr* cols[3][kQMaxFixed > kQMaxAdvice ? kQMaxFixed : kQMaxAdvice];  // fixed, advice, instance
-    const uint32_t* reads;   // n_reads x (col_type, col_idx, rot_idx, dst)
-    const uint32_t* ops;     // n_ops x (kind, dst, a, b, c)
-    const Fr* statics;       // values [0, static_len): constants and challenge slots
-    const uint32_t* rot_off; // per rotation: (rot << log_scale) mod 2^log_n
-    uint32_t n_reads, n_ops, static_len, pv_idx, result_idx, log_n;
+constexpr uint32_t kQMaxLookups = 8, kQMaxHelpers = 8, kQMaxTrash = 8;
+constexpr uint32_t kFlatHeaderWords = 9;
+struct FlatCols {
+    const Fr* c[3][kQMaxFixed > kQMaxAdvice ? kQMaxFixed : kQMaxAdvice];  // fixed, advice, instance
+};
+struct GatesParams {  // k_gates_flat: the custom gates
+    FlatCols cols;
+    const uint32_t* words;
+    uint32_t prog, log_n;
+    Fr* out;
+};
+struct TailParams {  // k_tail_flat: lookup and trash terms after the permutations
+    FlatCols cols;
+    const uint32_t* words;
+    const Fr *l0, *l_last, *l_active, *tinv;
+    const Fr* agg[kQMaxLookups];
+    const Fr* mult[kQMaxLookups];
+    const Fr* helper[kQMaxLookups][kQMaxHelpers];
+    uint32_t prog[kQMaxLookups][kQMaxHelpers];
+    uint32_t outputs[kQMaxLookups][kQMaxHelpers][4];  // sum_partial_products, product, table, selector
+    uint32_t n_helpers[kQMaxLookups];
+    uint32_t n_lookups;
+    const Fr* trash[kQMaxTrash];
+    uint32_t trash_sel[kQMaxTrash], trash_prog[kQMaxTrash], n_trash;
+    Fr y;
+    uint32_t tlen, log_n, log_scale;
+    int32_t divide;
     Fr* out;
 };
 

@@ -126,6 +126,38 @@ class QuotientDesc(ctypes.Structure):
 ]
 
 
+def _run_program(graph, cols, idx, E, scale, challenges):
+    """One row of a flattened program (FlatGraphEvaluator::evaluate,
+    proofs/src/plonk/evaluation.rs:530-651) with the previous value zero;
+    returns the whole values buffer.  challenges = (beta, theta, trash, y)."""
+    zero = np.zeros(4, np.uint64)
+    vals = [zero] * graph["values_len"]
+    for i, c in enumerate(graph["constants"]):
+        vals[i] = np.asarray(c, np.uint64)
+    for slot, v in zip(("beta_idx", "theta_idx", "trash_challenge_idx", "y_idx"), challenges):
+        vals[graph[slot]] = np.asarray(v, np.uint64)
+    vals[graph["previous_value_idx"]] = zero
+    for t, c, r, dst in graph["reads"]:
+        vals[dst] = cols[t][c][(idx + (graph["rotations"][r] << scale)) % E]
+    for kind, dst, a, b, c in graph["ops"]:
+        if kind == 0:
+            v = fr_op("add", vals[a], vals[b])
+        elif kind == 1:
+            v = fr_op("sub", vals[a], vals[b])
+        elif kind == 2:
+            v = fr_op("mul", vals[a], vals[b])
+        elif kind == 3:
+            v = fr_op("mul", vals[a], vals[a])
+        elif kind == 4:
+            v = fr_op("add", vals[a], vals[a])
+        elif kind == 5:
+            v = fr_op("neg", vals[a])
+        else:
+            v = fr_op("add", fr_op("mul", vals[a], vals[b]), vals[c])
+        vals[dst] = v
+    return vals
+
+
 def flat_gates_eval(graph, fixed, advice, instance, k, extended_k, beta, theta, trash_challenge, y):
     """The custom-gate values of every row of the extended coset, restating
     FlatGraphEvaluator::evaluate_chunk (proofs/src/plonk/evaluation.rs:530-651)
@@ -136,38 +168,49 @@ def flat_gates_eval(graph, fixed, advice, instance, k, extended_k, beta, theta, 
     FlatOpKind order (:134-143).  Pure Python over single-element oracle field
     operations: small domains only."""
     E, scale = 1 << extended_k, extended_k - k
-    zero = np.zeros(4, np.uint64)
-    template = [zero] * graph["values_len"]
-    for i, c in enumerate(graph["constants"]):
-        template[i] = np.asarray(c, np.uint64)
-    template[graph["beta_idx"]] = np.asarray(beta, np.uint64)
-    template[graph["theta_idx"]] = np.asarray(theta, np.uint64)
-    template[graph["trash_challenge_idx"]] = np.asarray(trash_challenge, np.uint64)
-    template[graph["y_idx"]] = np.asarray(y, np.uint64)
-    cols = (fixed, advice, instance)
+    cols, ch = (fixed, advice, instance), (beta, theta, trash_challenge, y)
     out = np.zeros((E, 4), np.uint64)
     for idx in range(E):
-        vals = list(template)
-        vals[graph["previous_value_idx"]] = zero
-        for t, c, r, dst in graph["reads"]:
-            vals[dst] = cols[t][c][(idx + (graph["rotations"][r] << scale)) % E]
-        for kind, dst, a, b, c in graph["ops"]:
-            if kind == 0:
-                v = fr_op("add", vals[a], vals[b])
-            elif kind == 1:
-                v = fr_op("sub", vals[a], vals[b])
-            elif kind == 2:
-                v = fr_op("mul", vals[a], vals[b])
-            elif kind == 3:
-                v = fr_op("mul", vals[a], vals[a])
-            elif kind == 4:
-                v = fr_op("add", vals[a], vals[a])
-            elif kind == 5:
-                v = fr_op("neg", vals[a])
-            else:
-                v = fr_op("add", fr_op("mul", vals[a], vals[b]), vals[c])
-            vals[dst] = v
-        out[idx] = vals[graph["result_idx"]]
+        out[idx] = _run_program(graph, cols, idx, E, scale, ch)[graph["result_idx"]]
+    return out
+
+
+def flat_tail_eval(v_in, fixed, advice, instance, k, extended_k, beta, theta, trash_challenge, y, l0, l_last,
+                   l_active, lookups=(), trashcans=()):
+    """The lookup terms (evaluation.rs:1034-1090) and trash terms (:1093-1109)
+    of any shape continuing each row's y-Horner accumulator v_in (the gate and
+    permutation terms).  lookups: [{"programs": [graph], "outputs":
+    [(sum_partial_products, product, table, selector)], "helpers": [col],
+    "aggregator": col, "multiplicities": col}]; trashcans: [{"program": graph,
+    "selector": fixed index, "trash": col}].  Pure Python, small domains."""
+    E, scale = 1 << extended_k, extended_k - k
+    cols, ch = (fixed, advice, instance), (beta, theta, trash_challenge, y)
+    one = fr_const(0)
+    out = np.zeros((E, 4), np.uint64)
+    for idx in range(E):
+        r_next = (idx + (1 << scale)) % E
+        v = v_in[idx]
+        for lk in lookups:
+            Z = lk["aggregator"][idx]
+            v = fr_op("add", fr_op("mul", v, y), fr_op("mul", Z, fr_op("add", l0[idx], l_last[idx])))
+            sum_h = np.zeros(4, np.uint64)
+            table = sel = None
+            for fi, prog in enumerate(lk["programs"]):
+                vals = _run_program(prog, cols, idx, E, scale, ch)
+                spp, prod, tbl, sl = lk["outputs"][fi]
+                if fi == 0:
+                    table, sel = vals[tbl], vals[sl]
+                h = lk["helpers"][fi][idx]
+                v = fr_op("sub", fr_op("add", fr_op("mul", v, y), fr_op("mul", h, vals[prod])), vals[spp])
+                sum_h = fr_op("add", sum_h, h)
+            u = fr_op("sub", fr_op("sub", lk["aggregator"][r_next], Z), fr_op("mul", sel, sum_h))
+            u = fr_op("add", fr_op("mul", u, table), lk["multiplicities"][idx])
+            v = fr_op("add", fr_op("mul", v, y), fr_op("mul", l_active[idx], u))
+        for tc in trashcans:
+            comp = _run_program(tc["program"], cols, idx, E, scale, ch)[tc["program"]["result_idx"]]
+            q = fixed[tc["selector"]][idx]
+            v = fr_op("add", fr_op("mul", v, y), fr_op("sub", comp, fr_op("mul", fr_op("sub", one, q), tc["trash"][idx])))
+        out[idx] = v
     return out
 
 

@@ -44,3 +44,63 @@ def standard_gate_graph():
     return {"constants": [], "rotations": [0], "reads": reads, "ops": [o + (0,) * (5 - len(o)) for o in ops],
             "values_len": 24, "beta_idx": BETA, "theta_idx": THETA, "trash_challenge_idx": TRASH, "y_idx": Y,
             "previous_value_idx": PREV, "result_idx": 23}
+
+
+def single_lookup_graph(input_advice, table_fixed, selector_fixed):
+    """The built-in lookup of the fused kernel as a helper program: one input
+    expression (a single advice column) compressed with theta, so
+    product = a + beta, sum of partial products = 1 (Store(Constant(1)) of
+    the reference for one input, evaluation.rs:730-740), table = t + beta,
+    selector = s.  Constants [0, 1] as GraphEvaluator's first constants.
+    Returns (graph, outputs)."""
+    reads = [(ADVICE, input_advice, 0, 7), (FIXED, table_fixed, 0, 8), (FIXED, selector_fixed, 0, 9)]
+    ops = [(MULADD, 10, 0, 3, 7), (ADD, 11, 10, 2, 0), (MULADD, 12, 0, 3, 8), (ADD, 13, 12, 2, 0)]
+    graph = {"constants": None, "rotations": [0], "reads": reads, "ops": ops, "values_len": 14, "beta_idx": 2,
+             "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5, "previous_value_idx": 6, "result_idx": 13}
+    return graph, (1, 11, 13, 9)
+
+
+def multi_lookup_graphs():
+    """A lookup of three input expressions in two helper chunks, the table the
+    theta-compression of (f3, f4) at rotations 0 and +1, selector f5 * a2:
+      chunk 0: f_0 = (a0, a1(+1)) compressed, f_1 = a2 f0      -> product, sum of partial products
+      chunk 1: f_2 = a1 - a0(-1)
+    Returns [(graph, outputs)] per chunk; every chunk computes table and selector."""
+    def common(reads, ops, first_free):
+        t = first_free
+        reads = reads + [(FIXED, 3, 0, t), (FIXED, 4, 1, t + 1), (FIXED, 5, 0, t + 2), (ADVICE, 2, 0, t + 3)]
+        ops = ops + [(MULADD, t + 4, 0, 3, t), (MULADD, t + 5, t + 4, 3, t + 1), (ADD, t + 6, t + 5, 2, 0),
+                     (MUL, t + 7, t + 2, t + 3, 0)]
+        return reads, ops, t + 6, t + 7, t + 8
+    # chunk 0: inputs f_0 = theta-compression of (a0, a1(+1)) + beta, f_1 = a2 f0 + beta
+    r0 = [(ADVICE, 0, 0, 7), (ADVICE, 1, 1, 8), (ADVICE, 2, 0, 9), (FIXED, 0, 0, 10)]
+    o0 = [(MULADD, 11, 0, 3, 7), (MULADD, 12, 11, 3, 8), (ADD, 13, 12, 2, 0),      # f_0 + beta
+          (MUL, 14, 9, 10, 0), (MULADD, 15, 0, 3, 14), (ADD, 16, 15, 2, 0),        # f_1 + beta
+          (MUL, 17, 13, 16, 0),                                                    # product
+          (ADD, 18, 16, 13, 0)]                                                    # sum of partial products
+    r0, o0, tbl0, sel0, n0 = common(r0, o0, 19)
+    g0 = {"constants": None, "rotations": [0, 1, -1], "reads": r0, "ops": o0, "values_len": n0, "beta_idx": 2,
+          "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5, "previous_value_idx": 6, "result_idx": 17}
+    # chunk 1: f_2 = a1 - a0(-1), + beta; one input: sum of partial products = 1
+    r1 = [(ADVICE, 1, 0, 7), (ADVICE, 0, 2, 8)]
+    o1 = [(SUB, 9, 7, 8, 0), (MULADD, 10, 0, 3, 9), (ADD, 11, 10, 2, 0)]
+    r1, o1, tbl1, sel1, n1 = common(r1, o1, 12)
+    g1 = {"constants": None, "rotations": [0, 1, -1], "reads": r1, "ops": o1, "values_len": n1, "beta_idx": 2,
+          "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5, "previous_value_idx": 6, "result_idx": 11}
+    return [(g0, (18, 17, tbl0, sel0)), (g1, (1, 11, tbl1, sel1))]
+
+
+def trash_graph():
+    """A trash argument's compression of (a0 - f1, a1 a2(+1)) with the trash
+    challenge (Horner from zero, evaluation.rs:776-785)."""
+    reads = [(ADVICE, 0, 0, 7), (FIXED, 1, 0, 8), (ADVICE, 1, 0, 9), (ADVICE, 2, 1, 10)]
+    ops = [(SUB, 11, 7, 8, 0), (MUL, 12, 9, 10, 0), (MULADD, 13, 0, 4, 11), (MULADD, 14, 13, 4, 12)]
+    return {"constants": None, "rotations": [0, 1], "reads": reads, "ops": ops, "values_len": 15, "beta_idx": 2,
+            "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5, "previous_value_idx": 6, "result_idx": 14}
+
+
+def with_constants(graph, zero, one):
+    """The graph with GraphEvaluator's first constants [0, 1] filled in."""
+    g = dict(graph)
+    g["constants"] = [zero, one]
+    return g

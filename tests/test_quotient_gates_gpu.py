@@ -110,3 +110,79 @@ def test_malformed_programs_are_refused(ctx):
     c["gates"] = as_flat(base)
     with pytest.raises(mzk.MzkError):
         device_quotient(ctx, k, c, False)
+
+
+def program_lookup(graphs_outs, helpers, agg, mult):
+    zero, one = np.zeros(4, np.uint64), O.fr_const(0)
+    from _gates import with_constants
+    gs = [with_constants(g, zero, one) for g, _ in graphs_outs]
+    return gs, {"programs": [as_flat(g) for g in gs], "outputs": [o for _, o in graphs_outs], "helpers": helpers,
+                "aggregator": agg, "multiplicities": mult}
+
+
+@pytest.mark.parametrize("k", [4, 8])
+def test_lookup_program_equals_builtin_lookup(ctx, k):
+    """The built-in single-input lookup and the same lookup as a helper
+    program give the same quotient (with the division), equal to the C oracle."""
+    from _gates import single_lookup_graph
+    E = 1 << (k + 2)
+    cols = make_columns(80 + k, E, 5, 2, lookup_selector=6)
+    got_builtin, expect = run_both(ctx, k, cols, True)
+    prog = dict(cols)
+    lk = prog.pop("lookup")
+    _, lp = program_lookup([single_lookup_graph(lk["input"], lk["table"], lk["selector"])], [lk["h"]], lk["z"],
+                           lk["m"])
+    prog["lookup_programs"] = [lp]
+    assert np.array_equal(got_builtin, expect)
+    assert np.array_equal(device_quotient(ctx, k, prog, True), expect)
+
+
+@pytest.mark.parametrize("k", [3, 6])
+def test_lookups_and_trash_of_any_shape_match_oracle(ctx, k):
+    """Two lookups (one of three inputs in two helper chunks, one
+    single-input) and a trashcan after a gate program and two permutation
+    sets, against the oracle: the C oracle's gates + permutations (here
+    the same gate as a program) continued by the restated lookup and trash
+    terms, then divided by t(X)."""
+    from _gates import multi_lookup_graphs, single_lookup_graph, standard_gate_graph, trash_graph, with_constants
+    ek = k + 2
+    E = 1 << ek
+    cols = make_columns(90 + k, E, 5, 2, lookup_selector=None)
+    cols["trash_challenge"] = O.rand_fr(95 + k, 1)[0]
+    col = lambda i: O.rand_fr(9000 + 10 * k + i, E)
+    g_multi, lp0 = program_lookup(multi_lookup_graphs(), [col(0), col(1)], col(2), col(3))
+    g_single, lp1 = program_lookup([single_lookup_graph(1, 5, 6)], [col(4)], col(5), col(6))
+    tg = with_constants(trash_graph(), np.zeros(4, np.uint64), O.fr_const(0))
+    trash = {"program": as_flat(tg), "selector": 2, "trash": col(7)}
+    base = run_both(ctx, k, cols, False)[1]                      # C oracle: standard gate + permutations
+    want = O.flat_tail_eval(base, cols["fixed"], cols["advice"], [], k, ek, cols["beta"], cols["theta"],
+                            cols["trash_challenge"], cols["y"], cols["l0"], cols["l_last"], cols["l_active"],
+                            lookups=[dict(lp0, programs=g_multi), dict(lp1, programs=g_single)],
+                            trashcans=[dict(trash, program=tg)])
+    dev_cols = dict(cols)
+    dev_cols["gates"] = as_flat(standard_gate_graph())
+    dev_cols["lookup_programs"] = [lp0, lp1]
+    dev_cols["trash"] = [trash]
+    assert np.array_equal(device_quotient(ctx, k, dev_cols, False), want)
+    assert np.array_equal(device_quotient(ctx, k, dev_cols, True), O.Domain(5, k).divide_by_vanishing_poly(want))
+
+
+def test_bad_lookup_and_trash_programs_are_refused(ctx):
+    from _gates import single_lookup_graph
+    k, E = 3, 1 << 5
+    cols = make_columns(7, E, 3, 1, lookup_selector=6)
+    lk = cols["lookup"]
+    g, outs = single_lookup_graph(0, 5, 6)
+    _, lp = program_lookup([(g, outs)], [lk["h"]], lk["z"], lk["m"])
+    both = dict(cols, lookup_programs=[lp])                          # built-in lookup and a program
+    with pytest.raises(mzk.MzkError):
+        device_quotient(ctx, k, both, False)
+    c = dict(cols)
+    c.pop("lookup")
+    _, lp_bad = program_lookup([(g, (1, 11, 13, 14))], [lk["h"]], lk["z"], lk["m"])   # output past values_len
+    with pytest.raises(mzk.MzkError):
+        device_quotient(ctx, k, dict(c, lookup_programs=[lp_bad]), False)
+    from _gates import trash_graph, with_constants
+    tg = as_flat(with_constants(trash_graph(), np.zeros(4, np.uint64), O.fr_const(0)))
+    with pytest.raises(mzk.MzkError):                                 # selector column 9 of 7
+        device_quotient(ctx, k, dict(c, trash=[{"program": tg, "selector": 9, "trash": lk["h"]}]), False)

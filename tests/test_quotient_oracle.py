@@ -154,3 +154,40 @@ def test_flat_gates_restatement_matches_direct_evaluation():
         g2 = A[1][idx] ** 2 - 2 * A[0][prv] * F[1][idx]
         g3 = -(A[2][idx] * F[2][idx]) + A[0][nxt] * th + I0[idx]
         assert val(got[idx]) == ((g1 * yv + g2) * yv + g3) % R, idx
+
+
+def oracle_quotient(cols, k, divide=False):
+    """The C oracle's quotient (built-in gate and lookup) for make_columns data."""
+    from _loader import load
+    mzk = load()
+    o = O.Domain(5, k)
+    cols = dict(cols)
+    cols["extended_omega"], cols["g_coset"] = o.get(2), o.get(3)
+    host = mzk.build_quotient_desc(cols, k, o.extended_k, lambda a: a.ctypes.data)
+    od = O.QuotientDesc()
+    ctypes.memmove(ctypes.byref(od), ctypes.byref(host), ctypes.sizeof(od))
+    od._keep = host._keep
+    return o.quotient_eval(od, divide)
+
+
+def test_lookup_program_restatement_matches_builtin_lookup():
+    """The oracle's restatement of the lookup terms of any shape
+    (evaluation.rs:1034-1090), run on the single-input lookup written as a
+    helper program, continues the gate + permutation value of the C oracle to
+    exactly the C oracle's value with its built-in lookup."""
+    from _gates import single_lookup_graph, with_constants
+    from test_quotient_gpu import make_columns
+    k = 3
+    E = 1 << (k + 2)
+    cols = make_columns(61, E, 5, 2, lookup_selector=6)
+    full = oracle_quotient(cols, k)
+    base_cols = dict(cols)
+    lk = base_cols.pop("lookup")
+    base = oracle_quotient(base_cols, k)
+    graph, outs = single_lookup_graph(lk["input"], lk["table"], lk["selector"])
+    graph = with_constants(graph, np.zeros(4, np.uint64), O.fr_const(0))
+    tail = O.flat_tail_eval(base, cols["fixed"], cols["advice"], [], k, k + 2, cols["beta"], cols["theta"],
+                            np.zeros(4, np.uint64), cols["y"], cols["l0"], cols["l_last"], cols["l_active"],
+                            lookups=[{"programs": [graph], "outputs": [outs], "helpers": [lk["h"]],
+                                      "aggregator": lk["z"], "multiplicities": lk["m"]}])
+    assert np.array_equal(tail, full)
