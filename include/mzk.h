@@ -405,6 +405,16 @@ int mzk_g1_suffix_sum_device(mzk_ctx *ctx, const uint64_t *in, size_t n, uint64_
  * identity and counted in *n_invalid (host, optional). */
 int mzk_g1_decompress_device(mzk_ctx *ctx, const uint8_t *in, size_t n, int check_subgroup, uint64_t *out,
                              uint8_t *status, uint64_t *n_invalid);
+/* G1Affine::to_compressed (curves/src/bls12_381/g1.rs:326-334; ZCash format:
+ * x big-endian, 0x80 compressed, 0x40 identity, 0x20 the larger y) of n
+ * DEVICE points into n x 48 DEVICE bytes. */
+int mzk_g1_compress_device(mzk_ctx *ctx, const uint64_t *points, size_t n, uint8_t *out);
+/* ParamsKZG::write_custom(.., SerdeFormat::Processed) (proofs/src/poly/kzg/
+ * params.rs:260-281), G1 part: out (host, at least 4 + 96 n bytes) = k as u32
+ * little-endian, n compressed g, n compressed g_lagrange (n = 2^k, DEVICE
+ * inputs); the caller appends the two G2 elements. */
+int mzk_srs_write_processed(mzk_ctx *ctx, const uint64_t *g, const uint64_t *g_lagrange, size_t n, uint8_t *out,
+                            size_t out_len);
 /* ParamsKZG::read_custom with SerdeFormat::Processed (params.rs:283-350), G1
  * part: bytes (host) = k as u32 LE, 2^k compressed g, 2^k compressed
  * g_lagrange (the G2 elements that follow are not read).  Points are

@@ -56,6 +56,8 @@ SIGNATURES = {
     "mzk_autotune": (_i32, [_vp, _vp, _vp, ctypes.POINTER(_u32), _sz, ctypes.POINTER(_u32), _sz, _i32,
                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "mzk_autotune_get": (_i32, [_vp, _i32, _u32, ctypes.POINTER(_i32)]),
+    "mzk_g1_compress_device": (_i32, [_vp, _vp, _sz, _vp]),
+    "mzk_srs_write_processed": (_i32, [_vp, _vp, _vp, _sz, _vp, _sz]),
     "mzk_ctx_graph_stats": (_i32, [_vp, _u64p, _u64p]),
     "mzk_autotune_set": (_i32, [_vp, _i32, _u32, _i32]),
     "mzk_autotune_save": (_i32, [_vp, ctypes.c_char_p]),
@@ -552,6 +554,17 @@ class Context:
         _check(lib().mzk_eval_polynomial_device(self.h, _dptr(buf), int(n), _ptr(np.ascontiguousarray(point, np.uint64)),
                                                 _ptr(out)))
         return out
+
+    def g1_compress_device(self, d_points, n, d_out):
+        """G1Affine::to_compressed of n device points into n x 48 device bytes."""
+        _check(lib().mzk_g1_compress_device(self.h, _dptr(d_points), int(n), _dptr(d_out)))
+
+    def srs_write_processed(self, d_g, d_g_lagrange, n):
+        """write_custom (Processed), G1 part: bytes k | g | g_lagrange (the caller adds G2)."""
+        out = np.zeros(4 + 96 * int(n), np.uint8)
+        _check(lib().mzk_srs_write_processed(self.h, _dptr(d_g), _dptr(d_g_lagrange), int(n),
+                                             ctypes.c_void_p(out.ctypes.data), out.size))
+        return out.tobytes()
 
     def g1_decompress_device(self, d_in, n, d_out, d_status=None, check_subgroup=True):
         """G1Affine::from_compressed of n device encodings; returns the invalid count."""

@@ -684,6 +684,29 @@ int mzk_g1_decompress_device(mzk_ctx* ctx, const uint8_t* in, size_t n, int chec
     return mzk::OK;
 }
 
+int mzk_g1_compress_device(mzk_ctx* ctx, const uint64_t* points, size_t n, uint8_t* out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (n && (!points || !out)) {
+        mzk::set_error("g1_compress: null pointer");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    MZK_TRY(mzk::g1_compress_device(&ctx->impl, points, n, out, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_srs_write_processed(mzk_ctx* ctx, const uint64_t* g, const uint64_t* g_lagrange, size_t n, uint8_t* out,
+                            size_t out_len) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!g || !g_lagrange || !out) {
+        mzk::set_error("srs_write: null pointer");
+        return mzk::ERR_ARG;
+    }
+    Guard gd(ctx);
+    return mzk::srs_write_processed(&ctx->impl, g, g_lagrange, n, out, out_len, ctx->impl.stream);
+}
+
 int mzk_srs_read_processed(mzk_ctx* ctx, const uint8_t* bytes, size_t len, size_t capacity, uint32_t* k_out,
                            uint64_t* g, uint64_t* g_lagrange, uint64_t* g_lagrange_delta,
                            uint64_t* g_lagrange_double_delta) {

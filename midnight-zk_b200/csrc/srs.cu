@@ -254,6 +254,45 @@ __global__ void __launch_bounds__(kThreads) k_g1_decompress(const uint8_t* __res
     }
 }
 
+// ZCash-format compression (G1Affine::to_compressed, g1.rs:326-334, blst's
+// p1_affine_compress): x as 48 big-endian bytes of its canonical value,
+// flags in the top bits of byte 0: 0x80 compressed, 0x40 the identity (every
+// other bit zero), 0x20 y is the larger of y and p - y.
+__global__ void __launch_bounds__(kThreads) k_g1_compress(const Affine* __restrict__ in, uint64_t n,
+                                                          uint8_t* __restrict__ out) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const Affine p = in[i];
+        uint8_t* o = out + 48 * i;
+        if (aff_is_inf(p)) {
+            o[0] = 0xc0u;
+            for (int k = 1; k < 48; k++) o[k] = 0;
+            continue;
+        }
+        Fp one_raw;
+#pragma unroll
+        for (int k = 0; k < 12; k++) one_raw.l[k] = k == 0 ? 1u : 0u;
+        const Fp x = fp_canonical(fp_mul(p.x, one_raw));
+        const Fp y = fp_canonical(fp_mul(p.y, one_raw));
+        const Fp ny = fp_canonical(fp_sub(fp_zero(), y));  // p - y (0 when y = 0)
+        bool y_larger = false, decided = false;
+        for (int k = 11; k >= 0 && !decided; k--)
+            if (y.l[k] != ny.l[k]) {
+                y_larger = y.l[k] > ny.l[k];
+                decided = true;
+            }
+#pragma unroll
+        for (int k = 0; k < 12; k++) {  // limb k little-endian -> bytes 44 - 4k .. 47 - 4k big-endian
+            const uint32_t w = x.l[k];
+            o[44 - 4 * k] = (uint8_t)(w >> 24);
+            o[45 - 4 * k] = (uint8_t)(w >> 16);
+            o[46 - 4 * k] = (uint8_t)(w >> 8);
+            o[47 - 4 * k] = (uint8_t)w;
+        }
+        o[0] |= 0x80u | (y_larger ? 0x20u : 0u);
+    }
+}
+
 // ---- g_to_lagrange (proofs/src/utils/arithmetic.rs:34-54): inverse FFT over
 // G1 points.  Decimation-in-frequency radix-2 stages in global memory (the
 // butterflies are compute-bound: one variable-base scalar multiplication
@@ -351,6 +390,37 @@ Status g1_decompress_device(Context* ctx, const void* in, uint64_t n, int check_
         MZK_CUDA_CHECK(cudaStreamSynchronize(st));
         *invalid = *static_cast<const uint64_t*>(h);
     }
+    return OK;
+}
+
+Status g1_compress_device(Context* ctx, const void* in, uint64_t n, void* out, cudaStream_t st) {
+    if (n == 0) return OK;
+    k_g1_compress<<<blocks_for(ctx, n), kThreads, 0, st>>>(static_cast<const Affine*>(in), n,
+                                                           static_cast<uint8_t*>(out));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+// ParamsKZG::write_custom(.., SerdeFormat::Processed) (params.rs:260-281), G1
+// part: k as u32 little-endian, then g and g_lagrange compressed.
+Status srs_write_processed(Context* ctx, const void* g, const void* lag, uint64_t n, uint8_t* out, size_t out_len,
+                           cudaStream_t st) {
+    if (n == 0 || (n & (n - 1)) || n > (1ull << 31)) {
+        set_error("srs_write: n must be a power of two (2^k points)");
+        return ERR_ARG;
+    }
+    if (out_len < 4 + 2 * n * 48) {
+        set_error("srs_write: output shorter than 4 + 96 n bytes");
+        return ERR_ARG;
+    }
+    const uint32_t k = (uint32_t)__builtin_ctzll(n);
+    std::memcpy(out, &k, 4);
+    void* comp;
+    MZK_TRY(ctx->ensure("srs_comp", 2 * n * 48, &comp));
+    MZK_TRY(g1_compress_device(ctx, g, n, comp, st));
+    MZK_TRY(g1_compress_device(ctx, lag, n, static_cast<uint8_t*>(comp) + n * 48, st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(out + 4, comp, 2 * n * 48, cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
     return OK;
 }
 

@@ -15,6 +15,11 @@ Status srs_setup_device(Context* ctx, const Domain* d, const uint64_t s[4], void
 Status g1_decompress_device(Context* ctx, const void* in, uint64_t n, int check_subgroup, void* out,
                             uint8_t* status, uint64_t* invalid, cudaStream_t st);
 // ParamsKZG::read_custom, SerdeFormat::Processed (params.rs:283-350), G1 part
+// G1Affine::to_compressed of n device points into n x 48 device bytes
+Status g1_compress_device(Context* ctx, const void* in, uint64_t n, void* out, cudaStream_t st);
+// write_custom (Processed), G1 part, into a host buffer of 4 + 96 n bytes
+Status srs_write_processed(Context* ctx, const void* g, const void* lag, uint64_t n, uint8_t* out, size_t out_len,
+                           cudaStream_t st);
 Status srs_read_processed(Context* ctx, const uint8_t* bytes, size_t len, uint64_t capacity, uint32_t* k_out,
                           void* g, void* lag, void* delta, void* ddelta, cudaStream_t st);
 // g_to_lagrange (utils/arithmetic.rs:34-54): out = inverse FFT of the n = 2^k

@@ -168,3 +168,40 @@ def test_subgroup_check_on_torsion_components(ctx):
     assert want == [0 if ok else 3 for _, ok in cases]
     assert st == want
     assert bad == sum(1 for _, ok in cases if not ok)
+
+
+def test_compress_matches_oracle_and_round_trips(ctx):
+    """G1Affine::to_compressed on the device: the oracle's encoding for
+    random points, the identity and a point with y and p - y swapped, and
+    decompression of the result gives the points back."""
+    pts = O.gen_bases(71, 300)
+    pts[5] = 0                                        # the identity
+    pts[6, 6:] = O.fp_op("sub", np.zeros(6, np.uint64), pts[6, 6:])  # -P: the other sign
+    n = pts.shape[0]
+    d_pts, d_out = ctx.alloc(pts.nbytes), ctx.alloc(n * 48)
+    d_pts.upload(pts)
+    ctx.g1_compress_device(d_pts, n, d_out)
+    enc = d_out.download((n * 48,), np.uint8)
+    want = b"".join(bytes(O.g1_compress(p)) for p in pts)
+    assert enc.tobytes() == want
+    d_back, d_st = ctx.alloc(n * 96), ctx.alloc(n)
+    assert ctx.g1_decompress_device(d_out, n, d_back, d_st, check_subgroup=True) == 0
+    assert np.array_equal(d_back.download((n, 12)), pts)
+
+
+def test_write_then_read_processed(ctx):
+    k = 6
+    n = 1 << k
+    s = O.rand_fr(123, 1)[0]
+    g, lag, delta, ddelta = O.srs_setup(s, k)
+    d_g, d_l = ctx.alloc(g.nbytes), ctx.alloc(lag.nbytes)
+    d_g.upload(g)
+    d_l.upload(lag)
+    data = ctx.srs_write_processed(d_g, d_l, n)
+    assert data == srs_file(k, s)[:4 + 96 * n]      # the oracle-built file, G1 part
+    bufs = [ctx.alloc(n * 96) for _ in range(4)]
+    assert ctx.srs_read_processed(data + bytes(192), n, *bufs) == k
+    for b, w in zip(bufs, (g, lag, delta, ddelta)):
+        assert np.array_equal(b.download((n, 12)), w)
+    with pytest.raises(mzk.MzkError):
+        ctx.srs_write_processed(d_g, d_l, 48)           # not a power of two
