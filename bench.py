@@ -188,10 +188,41 @@ def measure_quotient(mzk, ctx, stream, k, reps):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / reps
     ncols = 3 + 7 + 3 + 1 + 3 + 3
+    # the same circuit (its lookup selector read from a fixed column) with the
+    # gate and the lookup given as flattened programs
+    # (FlatGraphEvaluator layout: constants [0, 1], slots beta 2, theta 3,
+    # trash 4, y 5, previous value 6), run by the program interpreters
+    zero, one = np.zeros(4, np.uint64), np.array(FR_ONE_MONT, np.uint64)
+    gate = mzk.build_flat_graph(
+        [zero, one], [0], [(0, i, 0, 7 + i) for i in range(5)] + [(1, i, 0, 12 + i) for i in range(3)],
+        [(2, 15, 7, 12, 0), (2, 16, 8, 13, 0), (0, 17, 15, 16, 0), (2, 18, 12, 13, 0), (2, 19, 18, 9, 0),
+         (0, 20, 17, 19, 0), (2, 21, 10, 14, 0), (0, 22, 20, 21, 0), (0, 23, 22, 11, 0), (6, 24, 6, 5, 23)],
+        25, 2, 3, 4, 5, 6, 24)
+    lookup = mzk.build_flat_graph(
+        [zero, one], [0], [(1, 0, 0, 7), (0, 5, 0, 8), (0, 6, 0, 9)],
+        [(6, 10, 0, 3, 7), (0, 11, 10, 2, 0), (6, 12, 0, 3, 8), (0, 13, 12, 2, 0)], 14, 2, 3, 4, 5, 6, 13)
+    lk = cols["lookup"]
+    pcols = dict(cols)
+    del pcols["lookup"]
+    pcols["fixed"] = cols["fixed"][:6] + [ctx.gen_rand_fr(1999, E)]  # the program reads selector column 6
+    pcols["gates"] = gate
+    pcols["lookup_programs"] = [{"programs": [lookup], "outputs": [(1, 11, 13, 9)], "helpers": [lk["h"]],
+                                 "aggregator": lk["z"], "multiplicities": lk["m"]}]
+    pdesc = mzk.build_quotient_desc(pcols, k, k + 2, lambda b: b.ptr)
+    dom.quotient_eval_device(pdesc, out)
+    e0.record(stream)
+    for _ in range(reps):
+        dom.quotient_eval_device(pdesc, out)
+    e1.record(stream)
+    e1.synchronize()
+    ms_prog = e0.elapsed_time(e1) / reps
     dom.close()
     return {"rows": E, "ms": round(ms, 3), "rows_per_s": round(E / (ms / 1e3), 1),
             "hbm_gbs_algorithmic": round((ncols + 1) * 32 * E / (ms / 1e3) / 1e9, 1),
-            "columns_read": ncols}
+            "columns_read": ncols,
+            "as_programs_ms": round(ms_prog, 3),
+            "as_programs": "the gate and the lookup as flattened programs (interpreted per row) instead of "
+                           "the built-in fast path"}
 
 
 FR_ONE_MONT = [0x00000001fffffffe, 0x5884b7fa00034802, 0x998c4fefecbc4ff5, 0x1824b159acc5056f]  # R mod r
