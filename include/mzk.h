@@ -137,6 +137,22 @@ typedef struct {
 } mzk_msm_batch_item;
 int mzk_msm_g1_batch_device(mzk_ctx *ctx, const uint64_t *d_bases, size_t bases_len, const mzk_msm_batch_item *items,
                             size_t count, uint64_t *out);
+
+/* Fixed-base window tables for a resident SRS.  Row j of a table of width c
+ * holds [2^(c j)] of every base (row 0 the bases, len points per row); an MSM
+ * of width c over such bases needs no per-window bucket sets: window w of
+ * point i reads row w, every window's digits go to one bucket set, and the
+ * window sums need no doublings.  Same results as without the table.
+ * mzk_msm_table_rows(c): rows a table of width c needs.
+ * mzk_msm_window_table: fills rows 1 .. rows-1 of d_table (DEVICE, rows x len
+ * affine points) from row 0, which the caller has written.
+ * mzk_msm_g1_batch_table_device: mzk_msm_g1_batch_device over a table (items
+ * index row 0); items of at least min_n points use the table at width c,
+ * smaller ones run as usual on row 0. */
+int mzk_msm_table_rows(int c);
+int mzk_msm_window_table(mzk_ctx *ctx, uint64_t *d_table, size_t len, int c, size_t rows);
+int mzk_msm_g1_batch_table_device(mzk_ctx *ctx, const uint64_t *d_table, size_t len, int c, size_t rows,
+                                  size_t min_n, const mzk_msm_batch_item *items, size_t count, uint64_t *out);
 /* Window width override (0 = automatic), for tuning and tests. */
 int mzk_msm_set_window(mzk_ctx *ctx, int c);
 int mzk_msm_pick_window(size_t n);
@@ -297,6 +313,12 @@ typedef struct {
     const uint64_t *sigma_lagrange[3];  /* permutation polynomials of a, b, c */
     const uint64_t *table_lagrange;     /* lookup table column */
     const uint64_t *selector_lagrange;  /* lookup selector column */
+    /* srs_table_c > 0: srs is row 0 of a window table of that width with
+     * srs_table_rows rows of srs_len points (mzk_msm_window_table); MSMs of
+     * at least srs_table_min_n points use it */
+    int32_t srs_table_c;
+    uint32_t srs_table_rows;
+    uint64_t srs_table_min_n;
 } mzk_proving_key_desc;
 /* One proof's witness (Lagrange form, DEVICE, n Fr each) and challenges.
  * perm_z null: the device derives z (permutation/prover.rs:81-255) from a, b,

@@ -57,6 +57,9 @@ SIGNATURES = {
                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "mzk_autotune_get": (_i32, [_vp, _i32, _u32, ctypes.POINTER(_i32)]),
     "mzk_g1_compress_device": (_i32, [_vp, _vp, _sz, _vp]),
+    "mzk_msm_table_rows": (_i32, [_i32]),
+    "mzk_msm_window_table": (_i32, [_vp, _vp, _sz, _i32, _sz]),
+    "mzk_msm_g1_batch_table_device": (_i32, [_vp, _vp, _sz, _i32, _sz, _sz, _vp, _sz, _u64p]),
     "mzk_srs_write_processed": (_i32, [_vp, _vp, _vp, _sz, _vp, _sz]),
     "mzk_ctx_graph_stats": (_i32, [_vp, _u64p, _u64p]),
     "mzk_autotune_set": (_i32, [_vp, _i32, _u32, _i32]),
@@ -115,7 +118,8 @@ class ProvingKeyDesc(ctypes.Structure):
                 ("off_lagrange", ctypes.c_uint64), ("off_lagrange_delta", ctypes.c_uint64),
                 ("off_lagrange_double_delta", ctypes.c_uint64), ("blinding_factors", ctypes.c_uint32),
                 ("sigma_lagrange", ctypes.c_void_p * 3), ("table_lagrange", ctypes.c_void_p),
-                ("selector_lagrange", ctypes.c_void_p)]
+                ("selector_lagrange", ctypes.c_void_p), ("srs_table_c", ctypes.c_int32),
+                ("srs_table_rows", ctypes.c_uint32), ("srs_table_min_n", ctypes.c_uint64)]
 
 
 class ProofJob(ctypes.Structure):
@@ -542,6 +546,26 @@ class Context:
         db = d_bases.ptr if isinstance(d_bases, DeviceBuffer) else int(d_bases)
         out = np.zeros((max(1, len(items)), 18), np.uint64)
         _check(lib().mzk_msm_g1_batch_device(self.h, db, int(bases_len), ctypes.addressof(arr), len(items), _ptr(out)))
+        return out[:len(items)]
+
+    # ---- fixed-base window tables ----
+    @staticmethod
+    def msm_table_rows(c):
+        return int(lib().mzk_msm_table_rows(int(c)))
+
+    def msm_window_table(self, d_table, length, c, rows):
+        """Fill rows 1 .. rows-1 of a window table whose row 0 (length points) is in place."""
+        _check(lib().mzk_msm_window_table(self.h, _dptr(d_table), int(length), int(c), int(rows)))
+
+    def msm_batch_table_device(self, d_table, length, c, rows, min_n, items):
+        """msm_batch_device over a window table: items of at least min_n points use it."""
+        arr = (MsmBatchItem * max(1, len(items)))()
+        for i, (ds, off, n) in enumerate(items):
+            arr[i].d_scalars = ds.ptr if isinstance(ds, DeviceBuffer) else int(ds)
+            arr[i].base_offset, arr[i].n = int(off), int(n)
+        out = np.zeros((max(1, len(items)), 18), np.uint64)
+        _check(lib().mzk_msm_g1_batch_table_device(self.h, _dptr(d_table), int(length), int(c), int(rows), int(min_n),
+                                                   ctypes.addressof(arr), len(items), _ptr(out)))
         return out[:len(items)]
 
     # ---- column scans ----

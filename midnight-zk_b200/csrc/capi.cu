@@ -1,6 +1,7 @@
 // capi.cu — the extern "C" boundary (include/mzk.h) and the device context.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -575,6 +576,35 @@ int mzk_msm_g1_batch_device(mzk_ctx* ctx, const uint64_t* d_bases, size_t bases_
     Guard g(ctx);
     return mzk::msm_g1_batch_device(&ctx->impl, d_bases, bases_len, reinterpret_cast<const mzk::BatchItem*>(items),
                                     count, out, ctx->impl.stream);
+}
+
+int mzk_msm_table_rows(int c) { return (c < 5 || c > 24) ? 0 : (int)mzk::msm_table_rows(c); }
+
+int mzk_msm_window_table(mzk_ctx* ctx, uint64_t* d_table, size_t len, int c, size_t rows) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d_table) {
+        mzk::set_error("window table: null table");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    MZK_TRY(mzk::msm_window_table(&ctx->impl, d_table, len, c, (uint32_t)std::min<size_t>(rows, 0xffffffffu),
+                                  ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_msm_g1_batch_table_device(mzk_ctx* ctx, const uint64_t* d_table, size_t len, int c, size_t rows,
+                                  size_t min_n, const mzk_msm_batch_item* items, size_t count, uint64_t* out) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!out || !d_table || (count && !items) || c < 5 || c > 24) {
+        mzk::set_error("msm batch table: null pointer or width outside [5, 24]");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    std::vector<mzk::BatchItem> its(count);
+    for (size_t i = 0; i < count; i++) its[i] = {items[i].d_scalars, items[i].base_offset, items[i].n};
+    const mzk::MsmTable table{d_table, len, c, (uint32_t)std::min<size_t>(rows, 0xffffffffu), min_n};
+    return mzk::msm_g1_batch_device(&ctx->impl, d_table, len, its.data(), count, out, ctx->impl.stream, &table);
 }
 
 int mzk_compute_h_poly_device(mzk_ctx* ctx, mzk_domain* d, const mzk_quotient_desc* desc, const uint64_t* d_srs_g,

@@ -823,6 +823,7 @@ struct BatchItemDev {
     const Fr* scalars;
     uint32_t n, point_start, base_offset;
     uint32_t c, windows, nb, key_start;
+    uint32_t fixed;  // 1: the windows share one bucket set, window w reads table row w
 };
 
 __device__ __forceinline__ uint32_t find_item(const BatchItemDev* items, uint32_t n_items, uint32_t p) {
@@ -854,7 +855,7 @@ __global__ void k_digits_batch(const BatchItemDev* __restrict__ items, uint32_t 
             uint32_t key = kNoKey;
             if (valid && w < (int)it.windows) {
                 key = next_digit(s, w, (int)it.c, it.nb, carry, neg);
-                if (key != kNoKey) key += it.key_start;
+                if (key != kNoKey) key += it.key_start - (it.fixed ? (uint32_t)w * it.nb : 0u);
             }
             const uint32_t peers = __match_any_sync(0xffffffffu, key);
             if (key != kNoKey && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
@@ -867,9 +868,10 @@ __global__ void k_digits_batch(const BatchItemDev* __restrict__ items, uint32_t 
 // The batch scatter of window w of every item from the stored digits: the
 // entries land in the items' window-w slices (4 bytes per point of the batch),
 // which stay in L2 while the window is scattered.
+// row_off: w x the table stride (fixed items read window w from table row w)
 __global__ void k_scatter_window_batch(const uint32_t* __restrict__ digits_w, const BatchItemDev* __restrict__ items,
-                                       uint32_t n_items, uint32_t total_points, uint32_t* __restrict__ cursor,
-                                       uint32_t* __restrict__ sorted) {
+                                       uint32_t n_items, uint32_t total_points, uint32_t row_off,
+                                       uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -884,14 +886,51 @@ __global__ void k_scatter_window_batch(const uint32_t* __restrict__ digits_w, co
         slot = __shfl_sync(0xffffffffu, slot, leader);
         if (key != kNoKey) {
             const BatchItemDev& it = items[find_item(items, n_items, p)];
-            sorted[slot + (uint32_t)__popc(peers & lt_mask)] = (it.base_offset + (p - it.point_start)) | (d & 0x80000000u);
+            const uint32_t point = it.base_offset + (p - it.point_start) + (it.fixed ? row_off : 0u);
+            sorted[slot + (uint32_t)__popc(peers & lt_mask)] = point | (d & 0x80000000u);
         }
     }
 }
 }  // namespace
 
+namespace {
+// row j+1 of a window table from row j: [2^c] P, normalised
+__global__ void __launch_bounds__(256) k_window_row(const Affine* __restrict__ prev, Affine* __restrict__ next,
+                                                    uint64_t n, int c) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Xyzz p = xyzz_from_affine(prev[i]);
+        for (int b = 0; b < c; b++) p = xyzz_dbl(p);
+        next[i] = xyzz_to_affine(p);
+    }
+}
+}  // namespace
+
+uint32_t msm_table_rows(int c) { return (uint32_t)make_shape(c).windows; }
+
+Status msm_window_table(Context* ctx, void* d_table, uint64_t len, int c, uint32_t rows, cudaStream_t st) {
+    if (c < 5 || c > 24 || rows < msm_table_rows(c) || len == 0 || (uint64_t)rows * len >= 0x80000000ull) {
+        set_error("window table: c in [5, 24], at least msm_table_rows(c) rows, rows x len < 2^31");
+        return ERR_ARG;
+    }
+    Affine* t = static_cast<Affine*>(d_table);
+    const uint32_t blocks = (uint32_t)std::min<uint64_t>((len + 255) / 256, (uint64_t)ctx->num_sms * 8);
+    for (uint32_t j = 1; j < rows; j++) {
+        k_window_row<<<blocks, 256, 0, st>>>(t + (j - 1) * len, t + j * len, len, c);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    return OK;
+}
+
 Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, const BatchItem* items, size_t count,
-                           uint64_t* out, cudaStream_t st) {
+                           uint64_t* out, cudaStream_t st, const MsmTable* table) {
+    if (table) {
+        if (table->d_table != d_bases || table->stride != bases_len || table->rows < msm_table_rows(table->c) ||
+            table->rows * table->stride >= 0x80000000ull) {
+            set_error("msm batch: the window table must start at the bases and cover the windows of its width");
+            return ERR_ARG;
+        }
+    }
     std::memset(out, 0, count * 18 * 8);
     std::vector<BatchItemDev> hi;
     std::vector<WinDev> hw;
@@ -900,11 +939,12 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     uint32_t max_groups = 1;
     int max_windows = 0;
     // the group length follows the buckets of the whole batch
+    auto uses_table = [&](uint64_t n) { return table && n >= table->min_n; };
     uint64_t all_keys = 0;
     for (size_t m = 0; m < count; m++)
         if (items[m].n)
-            all_keys += make_shape(msm_window_for(ctx, items[m].n))
-                            .keys;
+            all_keys += uses_table(items[m].n) ? make_shape(table->c).nb
+                                                : make_shape(msm_window_for(ctx, items[m].n)).keys;
     const int glen_log = group_log_for(all_keys);
     for (size_t m = 0; m < count; m++) {
         const BatchItem& it = items[m];
@@ -917,7 +957,8 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
             set_error("msm batch: item " + std::to_string(m) + " reads past the bases");
             return ERR_ARG;
         }
-        const int c = msm_window_for(ctx, it.n);
+        const bool fixed = uses_table(it.n);
+        const int c = fixed ? table->c : msm_window_for(ctx, it.n);
         const MsmShape sh = make_shape(c, glen_log);
         BatchItemDev d;
         d.scalars = static_cast<const Fr*>(it.d_scalars);
@@ -928,10 +969,18 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
         d.windows = (uint32_t)sh.windows;
         d.nb = sh.nb;
         d.key_start = (uint32_t)keys;
-        append_windows(sh, keys, hw, groups, slots);
+        d.fixed = fixed ? 1u : 0u;
+        if (fixed) {  // one window row: every window's digits land in the same buckets
+            MsmShape one = sh;
+            one.windows = 1;
+            append_windows(one, keys, hw, groups, slots);
+            keys += sh.nb;
+        } else {
+            append_windows(sh, keys, hw, groups, slots);
+            keys += sh.keys;
+        }
         max_groups = std::max(max_groups, sh.groups);
         points += it.n;
-        keys += sh.keys;
         entries += (uint64_t)sh.windows * it.n;
         max_windows = std::max(max_windows, sh.windows);
         hi.push_back(d);
@@ -997,10 +1046,11 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_SCATTER, st));
     for (int w = 0; w < max_windows; w++) {
+        const uint32_t row_off = table ? (uint32_t)((uint64_t)w * table->stride) : 0u;
         k_scatter_window_batch<<<pt_blocks, pt_threads, 0, st>>>((const uint32_t*)digits + (size_t)w * points,
                                                                  (const BatchItemDev*)d_items, n_items,
-                                                                 (uint32_t)points, (uint32_t*)offsets + 1,
-                                                                 (uint32_t*)sorted);
+                                                                 (uint32_t)points, row_off,
+                                                                 (uint32_t*)offsets + 1, (uint32_t*)sorted);
         MZK_LAUNCH_CHECK(ctx);
     }
     MZK_TRY(ctx->phase_end(st));
@@ -1034,12 +1084,16 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     // batch spreads them over host threads
     const host::Xyzz6* hs = static_cast<const host::Xyzz6*>(host_wsum);
     std::vector<size_t> first_win(hi.size());
-    for (size_t i = 0, w0 = 0; i < hi.size(); w0 += hi[i].windows, i++) first_win[i] = w0;
+    for (size_t i = 0, w0 = 0; i < hi.size(); w0 += hi[i].fixed ? 1 : hi[i].windows, i++) first_win[i] = w0;
     auto tail = [&](size_t i) {
         host::Xyzz6 acc = host::infinity();
-        for (int w = (int)hi[i].windows - 1; w >= 0; w--) {
-            for (uint32_t b = 0; b < hi[i].c; b++) acc = host::dbl(acc);
-            acc = host::add(acc, host::canon(hs[first_win[i] + w]));
+        if (hi[i].fixed) {  // the table rows already carry the 2^(c w) factors
+            acc = host::canon(hs[first_win[i]]);
+        } else {
+            for (int w = (int)hi[i].windows - 1; w >= 0; w--) {
+                for (uint32_t b = 0; b < hi[i].c; b++) acc = host::dbl(acc);
+                acc = host::add(acc, host::canon(hs[first_win[i] + w]));
+            }
         }
         host::to_jacobian_normalised(acc, out + 18 * item_of[i]);
     };

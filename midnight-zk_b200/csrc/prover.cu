@@ -60,12 +60,17 @@ constexpr int kPolys = 7;  // a, b, c, z, m, h, Z
 
 }  // namespace
 
-// the MSMs of `items` against the SRS: one batched MSM, or one call each
+// the MSMs of `items` against the SRS: one batched MSM, or one call each;
+// with a window table (table non-null) the large ones use it either way
 static Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const std::vector<BatchItem>& items,
-                       uint64_t* res, uint32_t flags, cudaStream_t st) {
+                       uint64_t* res, uint32_t flags, const MsmTable* table, cudaStream_t st) {
     if (!(flags & MZK_PROVE_MSM_PER_CALL))
-        return msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res, st);
+        return msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res, st, table);
     for (size_t i = 0; i < items.size(); i++) {
+        if (table && items[i].n >= table->min_n) {
+            MZK_TRY(msm_g1_batch_device(ctx, srs, srs_len, &items[i], 1, res + i * 18, st, table));
+            continue;
+        }
         const void* bases = static_cast<const uint8_t*>(srs) + items[i].base_offset * 96;
         MZK_TRY(msm_g1_device(ctx, items[i].d_scalars, bases, items[i].n, res + i * 18, st, nullptr));
     }
@@ -157,6 +162,9 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
     }
     const void* srs = pks[0]->srs;
     const uint64_t srs_len = pks[0]->srs_len;
+    // a window table over the shared SRS buffer (every key of the call shares it)
+    MsmTable table_desc{srs, srs_len, pks[0]->srs_table_c, pks[0]->srs_table_rows, pks[0]->srs_table_min_n};
+    const MsmTable* table = pks[0]->srs_table_c > 0 ? &table_desc : nullptr;
     std::vector<BatchItem> items;
     std::vector<Fr*> coeff(count * kPolys), ext(count * kPolys), limbs(count);
     std::vector<const void*> lagrange(count * kPolys);  // a, b, c, z, m, h, Z of every job
@@ -282,7 +290,7 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
     }
     // 1. witness commitments of every proof in one batch
     std::vector<uint64_t> res1(items.size() * 18);
-    MZK_TRY(run_msms(ctx, srs, srs_len, items, res1.data(), flags, st));
+    MZK_TRY(run_msms(ctx, srs, srs_len, items, res1.data(), flags, table, st));
     for (size_t j = 0; j < count; j++)
         std::memcpy(out + (j * kProofCoreCommitments) * 18, res1.data() + j * 7 * 18, 7 * 18 * 8);
     // 2-4. per proof: coefficient and extended forms, quotient limbs
@@ -342,7 +350,7 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
             items.push_back({limbs[j] + (size_t)i * n, pks[j]->off_g, n});
     }
     std::vector<uint64_t> res2(items.size() * 18);
-    MZK_TRY(run_msms(ctx, srs, srs_len, items, res2.data(), flags, st));
+    MZK_TRY(run_msms(ctx, srs, srs_len, items, res2.data(), flags, table, st));
     for (size_t j = 0; j < count; j++)
         std::memcpy(out + (j * kProofCoreCommitments + 7) * 18, res2.data() + j * 4 * 18, 4 * 18 * 8);
     return OK;

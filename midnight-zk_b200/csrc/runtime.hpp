@@ -151,9 +151,25 @@ struct BatchItem {
     uint64_t base_offset;
     uint64_t n;
 };
-// out: count x 18 u64 (host), results in item order
+// A window table of fixed bases: row j (j < rows) holds [2^(c j)] of every
+// base, `stride` points per row, row 0 the bases themselves.  Items of at
+// least min_n points use it: their windows share one bucket set of width c
+// and window w reads row w (no per-window reduction, no doublings).
+struct MsmTable {
+    const void* d_table;
+    uint64_t stride;
+    int c;
+    uint32_t rows;
+    uint64_t min_n;
+};
+// rows a window table of width c needs (the windows of a width-c MSM)
+uint32_t msm_table_rows(int c);
+// out: count x 18 u64 (host), results in item order.  With a table, d_bases
+// must be its row 0 (bases_len = its stride).
 Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, const BatchItem* items, size_t count,
-                           uint64_t* out, cudaStream_t stream);
+                           uint64_t* out, cudaStream_t stream, const MsmTable* table = nullptr);
+// rows 1 .. rows-1 of a window table whose row 0 (len points) is in place
+Status msm_window_table(Context* ctx, void* d_table, uint64_t len, int c, uint32_t rows, cudaStream_t stream);
 enum MsmPhase { PH_HISTOGRAM = 0, PH_SCAN, PH_SCATTER, PH_ACCUMULATE, PH_FIXUP, PH_REDUCE, PH_TAIL, PH_COPY };
 
 // ---- microbenchmarks (probe.cu) ----
