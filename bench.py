@@ -225,6 +225,9 @@ def measure_quotient(mzk, ctx, stream, k, reps):
                            "the built-in fast path"}
 
 
+# fixed-base window tables of the resident SRS (prover keys, batched MSMs):
+# width 20, used by MSMs of 2^18 points and more
+TABLE_C, TABLE_MIN_N = 20, 1 << 18
 FR_ONE_MONT = [0x00000001fffffffe, 0x5884b7fa00034802, 0x998c4fefecbc4ff5, 0x1824b159acc5056f]  # R mod r
 SERVE_KS = (14, 16, 18, 20)
 SERVE_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
@@ -237,11 +240,20 @@ class ProverKeys:
     Lagrange-selector columns of seeded Fr values.  Timing depends only on
     sizes and scalar distributions, not on the bases' discrete logs."""
 
-    def __init__(self, mzk, ctx, ks):
+    def __init__(self, mzk, ctx, ks, table_c=TABLE_C, table_min_n=TABLE_MIN_N):
         self.mzk, self.ctx, self.ks = mzk, ctx, tuple(ks)
         gmax = 1 << max(ks)
         self.srs_len = gmax + sum(3 << k for k in ks)
-        self.srs = ctx.gen_bases(0x5125, self.srs_len)
+        # the SRS as row 0 of a fixed-base window table (rows [2^(c j)] bases),
+        # built once like the SRS itself
+        self.table_rows = mzk.Context.msm_table_rows(table_c) if table_c else 1
+        self.srs = ctx.alloc(self.table_rows * self.srs_len * 96)
+        ctx.gen_bases(0x5125, self.srs_len, out=self.srs)
+        t0 = time.perf_counter()
+        if table_c:
+            ctx.msm_window_table(self.srs, self.srs_len, table_c, self.table_rows)
+        self.table = {"c": table_c, "rows": self.table_rows, "min_n": table_min_n,
+                      "bytes": self.table_rows * self.srs_len * 96, "build_s": round(time.perf_counter() - t0, 2)}
         self.doms, self.pks, self.cols = {}, {}, {}
         off = gmax
         for k in ks:
@@ -264,6 +276,7 @@ class ProverKeys:
             pk.off_g, pk.off_lagrange, pk.off_lagrange_delta, pk.off_lagrange_double_delta = 0, off, off + n, off + 2 * n
             off += 3 * n
             pk.blinding_factors = 7
+            pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n = table_c, self.table_rows, table_min_n
             self.doms[k], self.pks[k], self.cols[k] = dom, pk, cols
 
     def job(self, k, seed):
@@ -350,10 +363,30 @@ def measure_batched_msm(mzk, ctx, reps):
         for b, _, n in items:
             ctx.msm_device(b, srs, n)
     t_seq = (time.perf_counter() - t0) / reps
+    # the same batch over a fixed-base window table of the SRS (built once,
+    # untimed, like the SRS itself): items of 2^18 points and more use it
+    c, min_n = TABLE_C, TABLE_MIN_N
+    rows = mzk.Context.msm_table_rows(c)
+    del srs
+    table = ctx.alloc(rows * (1 << 22) * 96)
+    ctx.gen_bases(0x5125, 1 << 22, out=table)
+    t0 = time.perf_counter()
+    ctx.msm_window_table(table, 1 << 22, c, rows)
+    t_build = time.perf_counter() - t0
+    tabled = ctx.msm_batch_table_device(table, 1 << 22, c, rows, min_n, items)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ctx.msm_batch_table_device(table, 1 << 22, c, rows, min_n, items)
+    t_table = (time.perf_counter() - t0) / reps
+    del table
     return {"msms": 64, "points": total, "sparse_msms": 16, "batched_ms": round(t_batch * 1e3, 2),
             "batched_mpts_per_s": round(total / t_batch / 1e6, 2), "one_call_each_ms": round(t_seq * 1e3, 2),
             "one_call_each_mpts_per_s": round(total / t_seq / 1e6, 2),
-            "batched_equals_one_call_each": bool(np.array_equal(together, single))}
+            "batched_equals_one_call_each": bool(np.array_equal(together, single)),
+            "window_table": {"c": c, "rows": rows, "min_n": min_n, "bytes": rows * (1 << 22) * 96,
+                             "build_s": round(t_build, 2), "batched_ms": round(t_table * 1e3, 2),
+                             "batched_mpts_per_s": round(total / t_table / 1e6, 2),
+                             "equals_batched": bool(np.array_equal(tabled, together))}}
 
 
 def measure_serving(mzk, ctx, keys, n_requests, max_batch, lanes, mem_budget):
@@ -692,6 +725,7 @@ def run_ours(args):
             extra_prover["proof_core_by_k"] = {str(k): measure_proof_core(mzk, ctx, keys, k, reps, b)
                                                for k, reps, b in ((14, 32, 16), (16, 32, 16), (20, 4, 2))}
             extra_prover["serving"] = measure_serving(mzk, ctx, keys, args.serve_requests, 16, 2, 8 << 30)
+            extra_prover["prover_srs_window_table"] = keys.table
             keys.close()
             del keys
             extra_prover["setup_and_scans"] = measure_setup_and_scans(mzk, ctx, stream)
