@@ -517,7 +517,7 @@ def measure_setup_and_scans(mzk, ctx, stream):
     small = mzk.EvaluationDomain(ctx, 5, 16)
     ms = timed(lambda: small.g1_to_lagrange_device(bufs[0], bufs[1]), reps=1)
     out["g_to_lagrange_k16"] = {"ms": round(ms, 2), "points_per_s": round((1 << 16) / ms * 1e3, 1),
-                                "note": "inverse FFT over G1, one scalar multiplication per butterfly"}
+                                "note": "inverse FFT over G1, one GLV scalar multiplication per butterfly"}
     # compressed points: 2^12 of the setup's g, compressed on the host, repeated
     m = 1 << 12
     pts = bufs[0].download((m, 12))
