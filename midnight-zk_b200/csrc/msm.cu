@@ -367,6 +367,9 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumulate(const Affine* __r
     if (s >= e) return;
     uint32_t k = find_key(offsets, keys, s);
     uint32_t seg_lo = offsets[k], seg_hi = offsets[k + 1];
+    // the end of the following bucket, loaded one bucket ahead (offsets has
+    // keys + 2 entries, so k + 2 <= keys + 1 is in range)
+    uint32_t nxt_hi = __ldg(offsets + k + 2);
     Xyzz acc;
     xyzz_set_inf(acc);
     // the next entry's base is loaded one iteration ahead to hide the gather latency
@@ -376,11 +379,15 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumulate(const Affine* __r
         if (j == seg_hi) {
             flush_bucket(acc, k, seg_lo, seg_hi, s, e, t, buckets, partials, owner_key);
             xyzz_set_inf(acc);
-            do {
+            k++;
+            seg_lo = seg_hi;
+            seg_hi = nxt_hi;
+            while (seg_hi <= j) {  // empty buckets
                 k++;
                 seg_lo = seg_hi;
                 seg_hi = offsets[k + 1];
-            } while (seg_hi <= j);
+            }
+            nxt_hi = __ldg(offsets + k + 2);
         }
         Affine p = nxt;
         const uint32_t cur = ent;
