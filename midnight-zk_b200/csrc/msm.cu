@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumulate(const Affine* __r
             nxt = load_affine(bases, ent & 0x7fffffffu);
         }
         if (aff_is_inf(p)) continue;
-        if (cur >> 31) p.y = fp_neg(p.y);
+        p.y = fp_select((cur >> 31) != 0, fp_neg(p.y), p.y);
         if (xyzz_is_inf(acc)) {
             acc.x = p.x;
             acc.y = p.y;
