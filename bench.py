@@ -13,6 +13,14 @@ inside the timed region).  With N > 1 (torchrun) every rank runs its own MSM
 on its own GPU (replicas, weak scaling; the MSM has no exchange step) and the
 step time is the max over ranks.
 
+Before anything is timed, the autotuner picks the MSM window widths and NTT
+pass splits for the sizes the run uses (`--no-tune` keeps the cost model).
+The same JSON line then carries the other configurations: the NTT sweep, the
+k = 18 quotient (built-in and as flattened programs), 64 batched MSMs over a
+2^22 SRS (plain and over a fixed-base window table), the proof core per k,
+serving (plain / batched / served, closed loop and Poisson), and the column
+scans and SRS set-up path (`--no-extras`, `--no-prover` skip them).
+
 `--impl reference` times the CPU restatement of the reference's msm_best
 (curves/src/msm.rs:460-532; the reference is Rust whose arithmetic lives in the
 un-vendored blst crate, so it cannot be built here) on the host cores.
