@@ -104,3 +104,26 @@ def test_bad_tables_are_refused(ctx):
         ctx.msm_window_table(t, 64, 16, 3)                                 # fewer rows than the windows
     with pytest.raises(mzk.MzkError):
         ctx.msm_window_table(t, 64, 30, rows)                              # width outside [5, 24]
+
+
+def test_served_proofs_over_a_table_equal_the_untabled_proof(ctx):
+    """The proving service with a key whose SRS is a window table: every
+    result equals the same proof run alone without the table."""
+    st = Setup(ctx, 8, seed=91)
+    jobs = [st.job(s)[0] for s in (92, 93, 94)]
+    want = [st.g.prove_core_device(st.pk, [j])[0] for j in jobs]
+    c = 16
+    t, rows = make_table(ctx, st.srs, c)
+    pk = st.pk
+    saved = (pk.srs, pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n)
+    pk.srs, pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n = t.ptr, c, rows, 1
+    try:
+        srv = mzk.ProvingServer(ctx, max_batch=4)
+        srv.add_key(st.g, pk)
+        tickets = [srv.submit(8, j) for j in jobs]
+        outs = [srv.wait(tk)[0] for tk in tickets]
+        srv.close()
+    finally:
+        pk.srs, pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n = saved
+    for o, w in zip(outs, want):
+        assert np.array_equal(o, w)
