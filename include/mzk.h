@@ -347,6 +347,120 @@ typedef struct {
 int mzk_prove_core_device(mzk_ctx *ctx, mzk_domain *d, const mzk_proving_key_desc *pk, const mzk_proof_job *jobs,
                           size_t count, uint32_t flags, uint64_t *out);
 
+/* ---- Fiat-Shamir transcript (proofs/src/transcript) --------------------- */
+/* CircuitTranscript<Blake2bState> (transcript/mod.rs:83-150,
+ * implementors.rs:13-30, 138-185): keyed BLAKE2b-512; points are absorbed and
+ * written compressed (48 bytes), scalars as 32 little-endian canonical bytes;
+ * a squeezed challenge is the digest reduced mod r.  Points use the MSM
+ * result layout (18 u64: x, y, z with z = 1 in Montgomery form, or all zero
+ * for the identity); scalars are Fr (4 u64 Montgomery).  Host only. */
+typedef struct mzk_transcript mzk_transcript;
+int mzk_transcript_create(mzk_transcript **out);
+int mzk_transcript_destroy(mzk_transcript *t);
+int mzk_transcript_common_fr(mzk_transcript *t, const uint64_t v[4]);    /* Transcript::common */
+int mzk_transcript_write_fr(mzk_transcript *t, const uint64_t v[4]);     /* Transcript::write */
+int mzk_transcript_write_point(mzk_transcript *t, const uint64_t p[18]); /* Transcript::write */
+int mzk_transcript_squeeze(mzk_transcript *t, uint64_t out[4]);          /* squeeze_challenge */
+/* the proof bytes written so far (Transcript::finalize); *len = their count */
+int mzk_transcript_proof(const mzk_transcript *t, uint8_t *out, size_t cap, size_t *len);
+/* VerifyingKey::from_parts's transcript_repr (proofs/src/plonk/mod.rs:227-284):
+ * Blake2b-512 personalised "Halo2-Verify-Key" over the version byte, k, the
+ * fixed and permutation commitments (uncompressed, each list after its u32
+ * length) and `pinned` = format!("{:?}", domain.pinned()) followed by
+ * format!("{:?}", cs.pinned()) as the caller renders them, then
+ * from_uniform_bytes.  Commitments in the 18-u64 point layout. */
+int mzk_vk_transcript_repr(uint32_t k, const uint64_t *fixed_coms, size_t n_fixed, const uint64_t *perm_coms,
+                           size_t n_perm, const uint8_t *pinned, size_t pinned_len, uint64_t out[4]);
+
+/* ---- keygen and create_proof (proofs/src/plonk/{keygen,prover}.rs) ------- */
+/* A column query of ConstraintSystem::advice_queries / fixed_queries. */
+typedef struct { uint32_t column; int32_t rotation; } mzk_query;
+/* A logup lookup whose input expression is one advice column (queried at
+ * rotation 0) and whose table expression is one fixed column, with a fixed
+ * selector column or none (selector_fixed = -1: the constant one). */
+typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } mzk_lookup_shape;
+/* The constraint system a key is built for.  Gates: the standard gate
+ * q_l a + q_r b + q_m a b + q_o c + q_c over fixed columns gate_fixed and
+ * advice columns gate_advice (every column it reads queried at rotation 0).
+ * Permutation columns: kind 0 advice, 1 fixed; sets of degree - 2 columns.
+ * The query lists and their order are the reference's (they fix the order
+ * of the evaluations in the proof).  Limits: 16 advice, 16 fixed, 16
+ * permutation columns (8 sets), at most one lookup, no instance columns,
+ * trashcans or simple selectors. */
+typedef struct {
+    uint32_t degree;                   /* cs.degree() (plonk/circuit.rs:2174-2199), 3..9 */
+    uint32_t blinding_factors;         /* cs.blinding_factors() (circuit.rs:2203-2245) */
+    uint32_t n_advice, n_fixed;
+    const mzk_query *advice_queries; uint32_t n_advice_queries;
+    const mzk_query *fixed_queries; uint32_t n_fixed_queries;
+    uint32_t gate_fixed[5], gate_advice[3];
+    uint32_t n_perm_cols;
+    const uint32_t *perm_col_kind, *perm_col_index;
+    uint32_t n_lookups;
+    const mzk_lookup_shape *lookups;
+} mzk_circuit_desc;
+/* ParamsKZG's bases (params.rs:83-93) inside one DEVICE G1Affine buffer;
+ * table_c > 0: srs is row 0 of a window table of that width and table_rows
+ * rows of srs_len points (mzk_msm_window_table), used by MSMs of at least
+ * table_min_n points. */
+typedef struct {
+    const uint64_t *srs;
+    uint64_t srs_len;
+    uint64_t off_g, off_lagrange, off_lagrange_delta, off_lagrange_double_delta;
+    int32_t table_c;
+    uint32_t table_rows;
+    uint64_t table_min_n;
+} mzk_srs_desc;
+typedef struct mzk_plonk_key mzk_plonk_key;
+/* keygen_vk + keygen_pk (plonk/keygen.rs:227-359) on the device for domain d
+ * (2^k rows, created with j = degree): the fixed columns' polynomials and
+ * extended cosets, the permutation polynomials of build_pk
+ * (permutation/keygen.rs:138-185; cell (c, r) holds delta^c' omega^r' of the
+ * cell (c', r') it maps to), their polynomials and cosets, l0, l_last and
+ * l_active_row (keygen.rs:361-404), the fixed and permutation commitments
+ * (Lagrange basis) and the VK's transcript_repr (mzk_vk_transcript_repr).
+ * fixed_values: n_fixed HOST columns of 2^k Fr (Lagrange form); perm_mapping:
+ * HOST n_perm_cols x 2^k x 2 u32 (column, row) pairs (Assembly::mapping), or
+ * null for the identity.  The key keeps pointers to d and to the SRS buffer:
+ * both must outlive it. */
+int mzk_keygen(mzk_ctx *ctx, mzk_domain *d, const mzk_circuit_desc *cs, const mzk_srs_desc *srs,
+               const uint64_t *const *fixed_values, const uint32_t *perm_mapping, const uint8_t *pinned,
+               size_t pinned_len, mzk_plonk_key **out);
+int mzk_plonk_key_destroy(mzk_plonk_key *key);
+/* repr (optional): transcript_repr; proof_len: bytes of one proof;
+ * n_blinds: the rng draws one proof takes (the order under
+ * mzk_create_proofs) */
+int mzk_plonk_key_info(const mzk_plonk_key *key, uint64_t repr[4], size_t *proof_len, size_t *n_blinds);
+/* the VK commitments: fixed n_fixed x 18 u64, permutation n_perm_cols x 18 u64 */
+int mzk_plonk_key_commitments(const mzk_plonk_key *key, uint64_t *fixed, uint64_t *perm);
+/* One proof: the advice columns (2^k Fr each in Lagrange form; rows from
+ * 2^k - blinding_factors - 1 on are replaced by blinding values), HOST or
+ * DEVICE pointers, and the rng draws in the reference's order: the blinding
+ * rows of every advice column (prover.rs:606-617, bf + 1 each), the
+ * multiplicity blinds of every lookup (prover.rs:122-123, bf + 1 each), the
+ * permutation blinds of every set (:165-167, bf each), the logup blinds of
+ * every lookup (:168, bf each), then the degree - 2 quotient-limb blinds
+ * (blind_quotient_limbs draws those from OsRng, prover.rs:774-785; taking them
+ * from the caller makes proofs reproducible).  proof_out receives the
+ * transcript bytes (Transcript::finalize). */
+typedef struct {
+    const mzk_plonk_key *key;
+    const uint64_t *const *advice;
+    int advice_on_device;
+    const uint64_t *blinds;  /* HOST, n_blinds Fr */
+    uint8_t *proof_out;      /* HOST, at least proof_len bytes */
+} mzk_proof_request;
+/* create_proof (plonk/prover.rs:432-473) for `count` proofs, any keys over
+ * one SRS buffer: each phase of the reference's Fiat-Shamir order (advice
+ * commitments, theta; multiplicities, beta, gamma; permutation products and
+ * logup helper / aggregator, trash challenge, y; quotient limbs, x;
+ * evaluations; multi_open with f, x3, the q evaluations, x4 and pi,
+ * kzg/mod.rs:110-289) runs for every proof before the next, its MSMs as one
+ * batched MSM (or, with MZK_PROVE_MSM_PER_CALL, one call each).  Flags:
+ * MZK_PROVE_MSM_PER_CALL, MZK_PROVE_NO_GRAPHS (above) and: */
+#define MZK_PROVE_SELF_CHECK 4u /* also check L'(x) = -C (prover.rs:404-408): an unsatisfied witness fails */
+int mzk_create_proofs(mzk_ctx *ctx, const mzk_proof_request *reqs, size_t count, uint32_t flags);
+
 /* ---- column scans: grand products, running sums, evaluations ------------- */
 /* All arrays are DEVICE arrays of Fr (4 x u64 Montgomery) unless marked host. */
 

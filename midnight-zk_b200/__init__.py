@@ -101,6 +101,20 @@ SIGNATURES = {
     "mzk_server_wait": (_i32, [_vp, _u64, _u64p, ctypes.POINTER(ctypes.c_double)]),
     "mzk_server_stats": (_i32, [_vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_double)]),
     "mzk_server_destroy": (_i32, [_vp]),
+    "mzk_transcript_create": (_i32, [ctypes.POINTER(_vp)]),
+    "mzk_transcript_destroy": (_i32, [_vp]),
+    "mzk_transcript_common_fr": (_i32, [_vp, _u64p]),
+    "mzk_transcript_write_fr": (_i32, [_vp, _u64p]),
+    "mzk_transcript_write_point": (_i32, [_vp, _u64p]),
+    "mzk_transcript_squeeze": (_i32, [_vp, _u64p]),
+    "mzk_transcript_proof": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.POINTER(_sz)]),
+    "mzk_vk_transcript_repr": (_i32, [_u32, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, _u64p]),
+    "mzk_keygen": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                          ctypes.c_void_p, _sz, ctypes.POINTER(_vp)]),
+    "mzk_plonk_key_destroy": (_i32, [_vp]),
+    "mzk_plonk_key_info": (_i32, [_vp, _u64p, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
+    "mzk_plonk_key_commitments": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p]),
+    "mzk_create_proofs": (_i32, [_vp, ctypes.c_void_p, _sz, _u32]),
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
     "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
 }
@@ -842,6 +856,191 @@ class ProvingServer:
             self.close()
         except Exception:
             pass
+
+
+class Query(ctypes.Structure):
+    """mzk_query (include/mzk.h)."""
+    _fields_ = [("column", ctypes.c_uint32), ("rotation", ctypes.c_int32)]
+
+
+class LookupShape(ctypes.Structure):
+    """mzk_lookup_shape (include/mzk.h)."""
+    _fields_ = [("input_advice", ctypes.c_uint32), ("table_fixed", ctypes.c_uint32),
+                ("selector_fixed", ctypes.c_int32)]
+
+
+class CircuitDesc(ctypes.Structure):
+    """mzk_circuit_desc (include/mzk.h)."""
+    _fields_ = [("degree", ctypes.c_uint32), ("blinding_factors", ctypes.c_uint32),
+                ("n_advice", ctypes.c_uint32), ("n_fixed", ctypes.c_uint32),
+                ("advice_queries", ctypes.c_void_p), ("n_advice_queries", ctypes.c_uint32),
+                ("fixed_queries", ctypes.c_void_p), ("n_fixed_queries", ctypes.c_uint32),
+                ("gate_fixed", ctypes.c_uint32 * 5), ("gate_advice", ctypes.c_uint32 * 3),
+                ("n_perm_cols", ctypes.c_uint32), ("perm_col_kind", ctypes.c_void_p),
+                ("perm_col_index", ctypes.c_void_p), ("n_lookups", ctypes.c_uint32), ("lookups", ctypes.c_void_p)]
+
+
+class SrsDesc(ctypes.Structure):
+    """mzk_srs_desc (include/mzk.h)."""
+    _fields_ = [("srs", ctypes.c_void_p), ("srs_len", ctypes.c_uint64), ("off_g", ctypes.c_uint64),
+                ("off_lagrange", ctypes.c_uint64), ("off_lagrange_delta", ctypes.c_uint64),
+                ("off_lagrange_double_delta", ctypes.c_uint64), ("table_c", ctypes.c_int32),
+                ("table_rows", ctypes.c_uint32), ("table_min_n", ctypes.c_uint64)]
+
+
+class ProofRequest(ctypes.Structure):
+    """mzk_proof_request (include/mzk.h)."""
+    _fields_ = [("key", ctypes.c_void_p), ("advice", ctypes.c_void_p), ("advice_on_device", ctypes.c_int),
+                ("blinds", ctypes.c_void_p), ("proof_out", ctypes.c_void_p)]
+
+
+PROVE_MSM_PER_CALL, PROVE_NO_GRAPHS, PROVE_SELF_CHECK = 1, 2, 4
+
+
+class Transcript:
+    """CircuitTranscript<Blake2bState> (proofs/src/transcript/mod.rs:83-150)
+    as the library implements it: common / write of Fr (4 u64 Montgomery) and
+    G1 points (18 u64, z = 1 or all zero), squeeze_challenge, finalize."""
+
+    def __init__(self):
+        h = _vp()
+        _check(lib().mzk_transcript_create(ctypes.byref(h)))
+        self.h = h.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mzk_transcript_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def common_fr(self, v):
+        _check(lib().mzk_transcript_common_fr(self.h, _ptr(np.ascontiguousarray(v, np.uint64))))
+
+    def write_fr(self, v):
+        _check(lib().mzk_transcript_write_fr(self.h, _ptr(np.ascontiguousarray(v, np.uint64))))
+
+    def write_point(self, p18):
+        _check(lib().mzk_transcript_write_point(self.h, _ptr(np.ascontiguousarray(p18, np.uint64))))
+
+    def squeeze_challenge(self):
+        out = np.zeros(4, np.uint64)
+        _check(lib().mzk_transcript_squeeze(self.h, _ptr(out)))
+        return out
+
+    def finalize(self):
+        n = _sz()
+        _check(lib().mzk_transcript_proof(self.h, None, 0, ctypes.byref(n)))
+        buf = (ctypes.c_uint8 * max(1, n.value))()
+        _check(lib().mzk_transcript_proof(self.h, buf, n.value, ctypes.byref(n)))
+        return bytes(buf[:n.value])
+
+
+def vk_transcript_repr(k, fixed_coms, perm_coms, pinned=b""):
+    """VerifyingKey::from_parts's transcript_repr (proofs/src/plonk/mod.rs:227-284)
+    over commitments in the 18-u64 point layout."""
+    f = np.ascontiguousarray(fixed_coms, np.uint64).reshape(-1, 18)
+    pm = np.ascontiguousarray(perm_coms, np.uint64).reshape(-1, 18)
+    out = np.zeros(4, np.uint64)
+    pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
+    _check(lib().mzk_vk_transcript_repr(k, f.ctypes.data if f.size else None, f.shape[0],
+                                        pm.ctypes.data if pm.size else None, pm.shape[0], pin, len(pinned),
+                                        _ptr(out)))
+    return out
+
+
+class PlonkKey:
+    """keygen_vk + keygen_pk (proofs/src/plonk/keygen.rs:227-359) on the device.
+
+    circuit: dict with degree, blinding_factors, n_advice, n_fixed,
+    advice_queries / fixed_queries [(column, rotation)], gate_fixed (5),
+    gate_advice (3), perm_cols [(kind 0 advice | 1 fixed, column)], lookups
+    [{"input", "table", "selector" (None: constant one)}].  fixed_values:
+    host (n, 4) arrays; mapping: (n_perm_cols, n, 2) uint32 or None; srs:
+    an SrsDesc.  The domain and the SRS buffer must outlive the key."""
+
+    def __init__(self, ctx, domain, circuit, srs, fixed_values, mapping=None, pinned=b""):
+        self.ctx, self.domain, self.circuit = ctx, domain, circuit
+        keep = []
+
+        def arr(ctype, items):
+            a = (ctype * max(1, len(items)))(*items)
+            keep.append(a)
+            return ctypes.addressof(a)
+
+        cs = CircuitDesc()
+        cs.degree, cs.blinding_factors = circuit["degree"], circuit["blinding_factors"]
+        cs.n_advice, cs.n_fixed = circuit["n_advice"], circuit["n_fixed"]
+        cs.advice_queries = arr(Query, [Query(c, r) for c, r in circuit["advice_queries"]])
+        cs.n_advice_queries = len(circuit["advice_queries"])
+        cs.fixed_queries = arr(Query, [Query(c, r) for c, r in circuit["fixed_queries"]])
+        cs.n_fixed_queries = len(circuit["fixed_queries"])
+        cs.gate_fixed[:] = circuit["gate_fixed"]
+        cs.gate_advice[:] = circuit["gate_advice"]
+        pc = circuit["perm_cols"]
+        cs.n_perm_cols = len(pc)
+        cs.perm_col_kind = arr(ctypes.c_uint32, [kd for kd, _ in pc])
+        cs.perm_col_index = arr(ctypes.c_uint32, [ci for _, ci in pc])
+        lks = circuit["lookups"]
+        cs.n_lookups = len(lks)
+        cs.lookups = arr(LookupShape, [LookupShape(lk["input"], lk["table"],
+                                                   -1 if lk["selector"] is None else lk["selector"]) for lk in lks])
+        cols = [np.ascontiguousarray(v, np.uint64) for v in fixed_values]
+        if any(c.shape != (domain.n, 4) for c in cols):
+            raise MzkError(1, "keygen: every fixed column needs n Fr values")
+        fptrs = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+        mp = None if mapping is None else np.ascontiguousarray(mapping, np.uint32)
+        pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
+        h = _vp()
+        _check(lib().mzk_keygen(ctx.h, domain.h, ctypes.byref(cs), ctypes.byref(srs), fptrs,
+                                None if mp is None else mp.ctypes.data, pin, len(pinned), ctypes.byref(h)))
+        self.h = h.value
+        repr_, plen, nbl = np.zeros(4, np.uint64), _sz(), _sz()
+        _check(lib().mzk_plonk_key_info(self.h, _ptr(repr_), ctypes.byref(plen), ctypes.byref(nbl)))
+        self.repr, self.proof_len, self.n_blinds = repr_, plen.value, nbl.value
+        self.fixed_coms = np.zeros((circuit["n_fixed"], 18), np.uint64)
+        self.perm_coms = np.zeros((len(pc), 18), np.uint64)
+        _check(lib().mzk_plonk_key_commitments(self.h, self.fixed_coms.ctypes.data, self.perm_coms.ctypes.data))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mzk_plonk_key_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def create_proofs(ctx, jobs, flags=0):
+    """create_proof (proofs/src/plonk/prover.rs:432-473) for many proofs in
+    one call.  jobs: [(PlonkKey, advice columns, blinds)] where the advice
+    columns are host (n, 4) arrays or DeviceBuffers and blinds an (n_blinds, 4)
+    host array in the reference's draw order (include/mzk.h).  Returns the
+    proofs as bytes."""
+    reqs = (ProofRequest * max(1, len(jobs)))()
+    keep, outs = [], []
+    for i, (key, advice, blinds) in enumerate(jobs):
+        on_dev = isinstance(advice[0], DeviceBuffer)
+        if on_dev:
+            ptrs = (ctypes.c_void_p * len(advice))(*[a.ptr for a in advice])
+        else:
+            cols = [np.ascontiguousarray(a, np.uint64) for a in advice]
+            keep.extend(cols)
+            ptrs = (ctypes.c_void_p * len(cols))(*[c.ctypes.data for c in cols])
+        bl = np.ascontiguousarray(blinds, np.uint64).reshape(-1, 4)
+        if bl.shape[0] != key.n_blinds:
+            raise MzkError(1, f"create_proof: {key.n_blinds} blinding values expected, got {bl.shape[0]}")
+        out = (ctypes.c_uint8 * key.proof_len)()
+        keep.extend([ptrs, bl])
+        outs.append(out)
+        reqs[i].key, reqs[i].advice, reqs[i].advice_on_device = key.h, ctypes.addressof(ptrs), 1 if on_dev else 0
+        reqs[i].blinds, reqs[i].proof_out = bl.ctypes.data, ctypes.addressof(out)
+    _check(lib().mzk_create_proofs(ctx.h, reqs, len(jobs), flags))
+    return [bytes(o) for o in outs]
 
 
 def msm_pick_window(n):

@@ -37,9 +37,6 @@ constexpr uint32_t kRecChunk = 64;  // elements per thread of a linear recurrenc
 constexpr uint32_t kScanItems = 8;  // elements per thread of a block scan
 constexpr uint32_t kMaxPermSetCols = 8;
 constexpr uint32_t kMaxLogupChunks = 8;
-// DELTA (GENERATOR^(2^S)), curves/src/bls12_381/fq.rs:501-508
-const uint64_t kDeltaU64[4] = {0x70e310d3d146f96aULL, 0x4b64c08919e299e6ULL, 0x51e114186a8b970dULL,
-                               0x6185d06627c067cbULL};
 
 __device__ __forceinline__ bool fr_is_zero(const Fr& a) {
     uint32_t acc = 0;
@@ -355,7 +352,7 @@ Status permutation_z_device(Context* ctx, const Domain* d, const mzk_permutation
         MZK_CUDA_CHECK(cudaMemcpyAsync(dbl, desc->blinds, (size_t)sets * bf * sizeof(Fr), cudaMemcpyHostToDevice, st));
     Fr* mv = (Fr*)mv_buf;
     const Fr beta = to_dev(to_host(desc->beta)), gamma = to_dev(to_host(desc->gamma));
-    const host::Fr4 delta = to_host(kDeltaU64);
+    const host::Fr4 delta = to_host(host::FR_DELTA4);
     const uint32_t grid = grid_for(ctx, n, kThreads);
     for (uint32_t s = 0; s < sets; s++) {
         PermCols pc;

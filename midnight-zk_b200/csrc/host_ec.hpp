@@ -183,6 +183,10 @@ static const uint64_t FR_ONE4[4] = {0x00000001fffffffeULL, 0x5884b7fa00034802ULL
 static const uint64_t FR_R2_4[4] = {0xc999e990f3f29c6dULL, 0x2b6cedcb87925c23ULL, 0x05d314967254398fULL,
                                     0x0748d9d99f59ff11ULL};
 
+// DELTA = GENERATOR^(2^S) in Montgomery form (curves/src/bls12_381/fq.rs:501-508)
+static const uint64_t FR_DELTA4[4] = {0x70e310d3d146f96aULL, 0x4b64c08919e299e6ULL, 0x51e114186a8b970dULL,
+                                      0x6185d06627c067cbULL};
+
 inline bool fr_geq(const uint64_t* a, const uint64_t* b) {
     for (int i = 3; i >= 0; i--)
         if (a[i] != b[i]) return a[i] > b[i];

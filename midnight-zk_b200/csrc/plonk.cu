@@ -1,0 +1,1433 @@
+// plonk.cu — keygen and create_proof with the Fiat-Shamir transcript.
+//
+// keygen (proofs/src/plonk/keygen.rs:227-404, permutation/keygen.rs:138-287)
+// builds a device-resident proving key: the fixed columns in Lagrange,
+// coefficient and extended-coset form, the permutation polynomials from the
+// caller's copy mapping in the same three forms, l0 / l_last / l_active_row,
+// the VK commitments and the VK's transcript_repr, the lookup table index of
+// the multiplicity kernels, and the point-set layout of the multi-open
+// argument (which polynomial is opened at which rotations of x).
+//
+// create_proof (proofs/src/plonk/prover.rs:66-473) runs in the reference's
+// Fiat-Shamir order, each phase for every proof of the call before the next,
+// so the MSMs of a phase form one batched MSM over the shared SRS:
+//   1. advice commitments (Lagrange basis), then theta;
+//   2. lookup multiplicities m (logup/prover.rs:95-184, 412-477) committed in
+//      delta form, then beta and gamma;
+//   3. permutation products z (permutation/prover.rs:81-255, delta form),
+//      logup helper h (Lagrange) and aggregator Z (double delta), then the
+//      trash challenge and y;
+//   4. lagrange_to_coeff / coeff_to_extended of every witness polynomial,
+//      the fused quotient, extended_to_coeff and the blinded limbs
+//      (compute_h_poly, prover.rs:701-785), the limb commitments, then x;
+//   5. the evaluations at x and its rotations (prover.rs:798-868,
+//      permutation/prover.rs:270-335, logup/prover.rs:318-352) and the
+//      linearization polynomial (linearization/prover.rs:41-86);
+//   6-8. multi_open (kzg/mod.rs:110-289): x1, x2, the q polynomials of each
+//      point set, f = sum x2^s q_s / prod (X - p), its commitment, x3, the q
+//      evaluations at x3, x4, the final polynomial and pi.
+// The transcript, the identities at x and the point-set bookkeeping run on
+// the host (transcript.hpp); everything proportional to n runs on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mzk.h"
+#include "field.cuh"
+#include "grand.hpp"
+#include "ntt.hpp"
+#include "quotient.hpp"
+#include "runtime.hpp"
+#include "transcript.hpp"
+
+namespace mzk {
+
+Context* context_of(mzk_ctx* ctx);
+const Domain* domain_of(mzk_domain* d);
+
+using host::Fr4;
+
+namespace {
+
+constexpr uint32_t kThreads = 256;
+
+inline Fr to_dev(const Fr4& a) {
+    Fr r;
+    std::memcpy(r.l, a.l, 32);
+    return r;
+}
+
+uint32_t grid_of(const Context* ctx, uint64_t n) {
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n + kThreads - 1) / kThreads, (uint64_t)ctx->num_sms * 8));
+}
+
+// ------------------------------------------------------------- kernels ----
+// out[c n + r] = delta^c' omega^r' for (c', r') = mapping of cell (c, r)
+// (identity when mapping is null); omega^e = lo[e & 4095] hi[e >> 12]
+__global__ void k_perm_values(Fr* __restrict__ out, const uint32_t* __restrict__ mapping, const Fr* __restrict__ deltas,
+                              const Fr* __restrict__ wlo, const Fr* __restrict__ whi, uint32_t n, uint32_t cols) {
+    const uint64_t total = (uint64_t)n * cols, stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        uint32_t mc = (uint32_t)(i / n), mr = (uint32_t)(i % n);
+        if (mapping) {
+            mc = mapping[2 * i];
+            mr = mapping[2 * i + 1];
+        }
+        Fr w = wlo[mr & 4095u];
+        if (mr >> 12) w = fr_mul(whi[mr >> 12], w);
+        out[i] = fr_mul(deltas[mc], w);
+    }
+}
+
+// out[i] = one for lo <= i < hi, else zero
+__global__ void k_unit(Fr* __restrict__ out, uint64_t n, uint64_t lo, uint64_t hi) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = (i >= lo && i < hi) ? fr_one() : fr_zero();
+}
+
+// l_active_row = 1 - (l_last + l_blind) (keygen.rs:393-401)
+__global__ void k_active(Fr* __restrict__ out, const Fr* __restrict__ l_last, const Fr* __restrict__ l_blind,
+                         uint64_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = fr_sub(fr_one(), fr_add(l_last[i], l_blind[i]));
+}
+
+__device__ __forceinline__ bool fr_is_zero_dev(const Fr& a) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc |= a.l[j];
+    return acc == 0;
+}
+
+// -1, 0, 1 as a < b, a == b, a > b in the order of the table index (the
+// four 64-bit words compared from the lowest)
+__device__ __forceinline__ int cmp_words(const Fr& a, const Fr& b) {
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        const uint64_t x = (uint64_t)a.l[2 * w + 1] << 32 | a.l[2 * w];
+        const uint64_t y = (uint64_t)b.l[2 * w + 1] << 32 | b.l[2 * w];
+        if (x != y) return x < y ? -1 : 1;
+    }
+    return 0;
+}
+
+// compute_multiplicities, counting half (logup/prover.rs:432-445): every
+// selected input row of the usable rows adds one to its table value's count;
+// a value not in the table sets *missing (the reference panics)
+__global__ void k_lookup_count(const Fr* __restrict__ input, const Fr* __restrict__ selector, uint32_t usable,
+                               const Fr* __restrict__ uniq, uint32_t n_uniq, uint32_t* __restrict__ counts,
+                               uint32_t* __restrict__ missing) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < usable; i += stride) {
+        if (selector && fr_is_zero_dev(selector[i])) continue;
+        const Fr v = input[i];
+        uint32_t lo = 0, hi = n_uniq;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (cmp_words(uniq[mid], v) < 0) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < n_uniq && cmp_words(uniq[lo], v) == 0) atomicAdd(&counts[lo], 1u);
+        else atomicOr(missing, 1u);
+    }
+}
+
+// compute_multiplicities, normalising half (:447-476): m_i = count(t_i) /
+// (copies of t_i in the table) on the usable rows
+__global__ void k_lookup_m(Fr* __restrict__ m, const uint32_t* __restrict__ uid, const uint32_t* __restrict__ counts,
+                           const Fr* __restrict__ tinv, uint32_t usable) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < usable; i += stride) {
+        const uint32_t u = uid[i];
+        Fr c = fr_zero();
+        c.l[0] = counts[u];
+        m[i] = fr_mul(fr_to_mont(c), tinv[u]);
+    }
+}
+
+// Batched polynomial evaluation.  A block sums 2048 coefficients of one
+// task: each thread runs Horner over 8 consecutive coefficients, then the
+// block combines its threads' values pairwise with the powers point^(8 2^l)
+// (a tree of 8 levels).  Segment sums land in seg_out; a later level
+// evaluates them as a polynomial in point^2048.
+struct EvalTask {
+    const Fr* poly;
+    uint64_t len;
+    Fr* seg_out;
+    Fr pw[9];  // point, point^8, point^16, ..., point^1024
+};
+constexpr uint32_t kEvalSeg = 2048;
+
+__global__ void __launch_bounds__(kThreads) k_eval_segments(const EvalTask* __restrict__ tasks) {
+    __shared__ Fr part[kThreads];
+    const EvalTask& t = tasks[blockIdx.y];
+    const uint64_t base = (uint64_t)blockIdx.x * kEvalSeg;
+    if (base >= t.len) return;  // uniform across the block
+    const uint32_t tid = threadIdx.x;
+    const Fr x = t.pw[0];
+    Fr acc = fr_zero();
+    for (int j = 7; j >= 0; j--) {
+        const uint64_t idx = base + 8ull * tid + (uint64_t)j;
+        acc = fr_mul(acc, x);
+        if (idx < t.len) acc = fr_add(acc, t.poly[idx]);
+    }
+    part[tid] = acc;
+    __syncthreads();
+    for (int l = 0; l < 8; l++) {
+        const uint32_t s = 1u << l;
+        if ((tid & (2 * s - 1)) == 0) part[tid] = fr_add(part[tid], fr_mul(part[tid + s], t.pw[1 + l]));
+        __syncthreads();
+    }
+    if (tid == 0) t.seg_out[blockIdx.x] = part[0];
+}
+
+// Batched linear combinations: out_o[i] = sum_t s_t p_t[i] (i < len_t), zero
+// past a term's length (poly_inner_product, kzg/mod.rs:125-147)
+struct LinTerm {
+    const Fr* p;
+    uint64_t len;
+    Fr s;
+};
+struct LinOut {
+    Fr* out;
+    uint64_t len;
+    uint32_t t0, nt;
+};
+__global__ void k_lincomb(const LinOut* __restrict__ outs, const LinTerm* __restrict__ terms) {
+    const LinOut o = outs[blockIdx.y];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < o.len; i += stride) {
+        Fr acc = fr_zero();
+        for (uint32_t t = o.t0; t < o.t0 + o.nt; t++)
+            if (i < terms[t].len) acc = fr_add(acc, fr_mul(terms[t].p[i], terms[t].s));
+        o.out[i] = acc;
+    }
+}
+
+// ------------------------------------------------------- host scalar math --
+Fr4 fr_rot(const Domain* d, const Fr4& x, int32_t rot) {
+    return rot >= 0 ? host::fr_mul(x, host::fr_pow_u64(d->omega, (uint64_t)rot))
+                    : host::fr_mul(x, host::fr_pow_u64(d->omega_inv, (uint64_t)(-(int64_t)rot)));
+}
+
+// EvaluationDomain::l_i_range (domain.rs:487-512) at one rotation
+Fr4 l_i(const Domain* d, const Fr4& x, const Fr4& xn, int32_t i) {
+    const Fr4 wi = fr_rot(d, host::fr_one(), i);
+    const Fr4 num = host::fr_mul(host::fr_mul(wi, host::fr_sub(xn, host::fr_one())), d->ifft_div);
+    return host::fr_mul(num, host::fr_inv(host::fr_sub(x, wi)));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- the key ----
+struct PlonkKey {
+    const Domain* dom = nullptr;
+    uint32_t k = 0, n = 0, u = 0, bf = 0, degree = 0, qdeg = 0, chunk = 0, n_sets = 0;
+    uint32_t n_advice = 0, n_fixed = 0, n_perm = 0;
+    std::vector<mzk_query> advice_queries, fixed_queries;
+    uint32_t gate_fixed[5] = {}, gate_advice[3] = {};
+    std::vector<uint32_t> perm_kind, perm_index;
+    bool has_lookup = false;
+    mzk_lookup_shape lookup = {};
+    uint32_t n_uniq = 0;
+    // device
+    void* mem = nullptr;
+    std::vector<Fr*> fixed_lag, fixed_coeff, fixed_ext, perm_lag, perm_coeff, perm_ext;
+    Fr *l0 = nullptr, *l_last = nullptr, *l_active = nullptr, *ones = nullptr;
+    Fr* uniq = nullptr;     // distinct table values of the usable rows, in the index order
+    uint32_t* uid = nullptr;  // per usable row: its value's index in uniq
+    Fr* tinv = nullptr;     // per distinct value: 1 / (its copies in the table)
+    mzk_srs_desc srs = {};
+    // verifying key
+    std::vector<std::array<uint64_t, 18>> fixed_coms, perm_coms;
+    Fr4 repr = {};
+    // multi-open layout: polynomials (kind, index) and point sets sorted by
+    // (size, first appearance), each with its polynomials and rotations
+    enum PolyKind { P_ADVICE = 0, P_PERM_Z, P_M, P_H, P_AGG, P_FIXED, P_PERM_FIXED, P_LIN };
+    struct OpenSet {
+        std::vector<std::pair<int, uint32_t>> polys;
+        std::vector<int32_t> rots;
+    };
+    std::vector<OpenSet> open_sets;
+    size_t proof_len = 0, n_blinds = 0;
+    int32_t last_rot() const { return -(int32_t)(bf + 1); }
+    ~PlonkKey() {
+        if (mem) cudaFree(mem);
+    }
+};
+
+namespace {
+
+Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
+    auto fail = [](const std::string& m) {
+        set_error("keygen: " + m);
+        return ERR_ARG;
+    };
+    if (cs->degree < 3 || cs->degree > 9) return fail("degree must be in 3..9");
+    if (d->quotient_poly_degree != cs->degree - 1) return fail("the domain must be created with j = degree");
+    const uint64_t n = 1ull << d->k;
+    if ((uint64_t)cs->blinding_factors + 2 >= n) return fail("blinding_factors too large for the domain");
+    if (cs->n_advice == 0 || cs->n_advice > kQMaxAdvice || cs->n_fixed > kQMaxFixed)
+        return fail("1..16 advice and at most 16 fixed columns");
+    if (cs->n_perm_cols > kQMaxPermCols || (cs->n_perm_cols + cs->degree - 3) / (cs->degree - 2) > kQMaxSets)
+        return fail("at most 16 permutation columns in at most 8 sets");
+    if (cs->n_lookups > 1) return fail("at most one lookup");
+    if ((cs->n_advice_queries && !cs->advice_queries) || (cs->n_fixed_queries && !cs->fixed_queries))
+        return fail("null query list");
+    if ((cs->n_perm_cols && (!cs->perm_col_kind || !cs->perm_col_index)) || (cs->n_lookups && !cs->lookups))
+        return fail("null column list");
+    auto queried = [&](const mzk_query* q, uint32_t nq, uint32_t col) {
+        for (uint32_t i = 0; i < nq; i++)
+            if (q[i].column == col && q[i].rotation == 0) return true;
+        return false;
+    };
+    for (uint32_t i = 0; i < cs->n_advice_queries; i++) {
+        const mzk_query q = cs->advice_queries[i];
+        if (q.column >= cs->n_advice) return fail("advice query column out of range");
+        if (q.rotation <= -(int32_t)n || q.rotation >= (int32_t)n) return fail("rotation out of range");
+        for (uint32_t j = 0; j < i; j++)
+            if (cs->advice_queries[j].column == q.column && cs->advice_queries[j].rotation == q.rotation)
+                return fail("duplicated advice query");
+    }
+    for (uint32_t i = 0; i < cs->n_fixed_queries; i++) {
+        const mzk_query q = cs->fixed_queries[i];
+        if (q.column >= cs->n_fixed) return fail("fixed query column out of range");
+        if (q.rotation <= -(int32_t)n || q.rotation >= (int32_t)n) return fail("rotation out of range");
+        for (uint32_t j = 0; j < i; j++)
+            if (cs->fixed_queries[j].column == q.column && cs->fixed_queries[j].rotation == q.rotation)
+                return fail("duplicated fixed query");
+    }
+    for (int i = 0; i < 5; i++)
+        if (!queried(cs->fixed_queries, cs->n_fixed_queries, cs->gate_fixed[i]))
+            return fail("a gate fixed column is not queried at rotation 0");
+    for (int i = 0; i < 3; i++)
+        if (!queried(cs->advice_queries, cs->n_advice_queries, cs->gate_advice[i]))
+            return fail("a gate advice column is not queried at rotation 0");
+    for (uint32_t i = 0; i < cs->n_perm_cols; i++) {
+        const uint32_t kind = cs->perm_col_kind[i], col = cs->perm_col_index[i];
+        if (kind > 1) return fail("permutation column kind must be 0 (advice) or 1 (fixed)");
+        if (kind == 0 ? !queried(cs->advice_queries, cs->n_advice_queries, col)
+                      : !queried(cs->fixed_queries, cs->n_fixed_queries, col))
+            return fail("a permutation column is not queried at rotation 0");
+    }
+    for (uint32_t i = 0; i < cs->n_lookups; i++) {
+        const mzk_lookup_shape& l = cs->lookups[i];
+        if (!queried(cs->advice_queries, cs->n_advice_queries, l.input_advice) ||
+            !queried(cs->fixed_queries, cs->n_fixed_queries, l.table_fixed) ||
+            (l.selector_fixed >= 0 && !queried(cs->fixed_queries, cs->n_fixed_queries, (uint32_t)l.selector_fixed)))
+            return fail("a lookup column is not queried at rotation 0");
+    }
+    return OK;
+}
+
+// construct_intermediate_sets (kzg/utils.rs:46-140) over the symbolic
+// queries (polynomial, rotation of x), then the sort by (size, index) of
+// multi_open (kzg/mod.rs:207-221).  Distinct rotations are distinct points
+// for any x outside the n-th roots of unity.
+void build_open_sets(PlonkKey* key, const std::vector<std::pair<std::pair<int, uint32_t>, int32_t>>& queries) {
+    std::map<int32_t, uint32_t> point_index;
+    std::vector<std::pair<std::pair<int, uint32_t>, std::vector<uint32_t>>> com;
+    for (const auto& q : queries) {
+        auto it = point_index.find(q.second);
+        if (it == point_index.end()) it = point_index.emplace(q.second, (uint32_t)point_index.size()).first;
+        bool found = false;
+        for (auto& c : com)
+            if (c.first == q.first) {
+                c.second.push_back(it->second);
+                found = true;
+                break;
+            }
+        if (!found) com.push_back({q.first, {it->second}});
+    }
+    std::map<std::vector<uint32_t>, uint32_t> set_index;
+    std::vector<std::pair<std::pair<int, uint32_t>, uint32_t>> labels;
+    for (auto& c : com) {
+        std::vector<uint32_t> s = c.second;
+        std::sort(s.begin(), s.end());
+        auto it = set_index.find(s);
+        if (it == set_index.end()) it = set_index.emplace(s, (uint32_t)set_index.size()).first;
+        labels.push_back({c.first, it->second});
+    }
+    std::vector<int32_t> rot_of(point_index.size());
+    for (auto& kv : point_index) rot_of[kv.second] = kv.first;
+    std::vector<PlonkKey::OpenSet> sets(set_index.size());
+    for (auto& kv : set_index)
+        for (uint32_t pi : kv.first) sets[kv.second].rots.push_back(rot_of[pi]);
+    for (auto& l : labels) sets[l.second].polys.push_back(l.first);
+    std::vector<uint32_t> order(sets.size());
+    for (uint32_t i = 0; i < order.size(); i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return sets[a].rots.size() < sets[b].rots.size(); });
+    key->open_sets.clear();
+    for (uint32_t i : order) key->open_sets.push_back(sets[i]);
+}
+
+}  // namespace
+
+Status vk_transcript_repr(uint32_t k, const uint64_t* fixed, size_t n_fixed, const uint64_t* perm, size_t n_perm,
+                          const uint8_t* pinned, size_t pinned_len, Fr4* out) {
+    static const char kPersonal[] = "Halo2-Verify-Key";
+    host::Blake2b h(64, nullptr, 0, reinterpret_cast<const uint8_t*>(kPersonal), 16);
+    uint8_t head[6] = {0x03, (uint8_t)k, 0, 0, 0, 0};  // VERSION (plonk/mod.rs:74), k, u32 count
+    for (int b = 0; b < 4; b++) head[2 + b] = (uint8_t)(n_fixed >> (8 * b));
+    h.update(head, 6);
+    uint8_t enc[96];
+    for (size_t i = 0; i < n_fixed; i++) {
+        host::g1_uncompressed(fixed + 18 * i, enc);
+        h.update(enc, 96);
+    }
+    uint8_t cnt[4];
+    for (int b = 0; b < 4; b++) cnt[b] = (uint8_t)(n_perm >> (8 * b));
+    h.update(cnt, 4);
+    for (size_t i = 0; i < n_perm; i++) {
+        host::g1_uncompressed(perm + 18 * i, enc);
+        h.update(enc, 96);
+    }
+    if (pinned_len) h.update(pinned, pinned_len);
+    uint8_t d[64];
+    h.digest(d);
+    *out = host::fr_from_uniform(d);
+    return OK;
+}
+
+Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const mzk_srs_desc* srs,
+              const uint64_t* const* fixed_values, const uint32_t* mapping, const uint8_t* pinned, size_t pinned_len,
+              PlonkKey** out) {
+    MZK_TRY(check_circuit(d, cs));
+    const uint32_t n = 1u << d->k, E = 1u << d->ext_k;
+    if (!srs || !srs->srs) {
+        set_error("keygen: null SRS");
+        return ERR_ARG;
+    }
+    for (uint64_t off : {srs->off_g, srs->off_lagrange, srs->off_lagrange_delta, srs->off_lagrange_double_delta})
+        if (off + n > srs->srs_len) {
+            set_error("keygen: SRS bases out of range");
+            return ERR_ARG;
+        }
+    if (cs->n_fixed && !fixed_values) {
+        set_error("keygen: null fixed columns");
+        return ERR_ARG;
+    }
+    for (uint32_t i = 0; i < cs->n_fixed; i++)
+        if (!fixed_values[i]) {
+            set_error("keygen: null fixed column");
+            return ERR_ARG;
+        }
+    const uint32_t P = cs->n_perm_cols;
+    if (mapping)
+        for (uint64_t i = 0; i < (uint64_t)P * n; i++)
+            if (mapping[2 * i] >= P || mapping[2 * i + 1] >= n) {
+                set_error("keygen: permutation mapping out of range");
+                return ERR_ARG;
+            }
+    auto key = std::unique_ptr<PlonkKey>(new PlonkKey);
+    key->dom = d;
+    key->k = d->k;
+    key->n = n;
+    key->bf = cs->blinding_factors;
+    key->u = n - cs->blinding_factors - 1;
+    key->degree = cs->degree;
+    key->qdeg = cs->degree - 1;
+    key->chunk = cs->degree - 2;
+    key->n_perm = P;
+    key->n_sets = (P + key->chunk - 1) / key->chunk;
+    key->n_advice = cs->n_advice;
+    key->n_fixed = cs->n_fixed;
+    key->advice_queries.assign(cs->advice_queries, cs->advice_queries + cs->n_advice_queries);
+    key->fixed_queries.assign(cs->fixed_queries, cs->fixed_queries + cs->n_fixed_queries);
+    std::memcpy(key->gate_fixed, cs->gate_fixed, sizeof(key->gate_fixed));
+    std::memcpy(key->gate_advice, cs->gate_advice, sizeof(key->gate_advice));
+    key->perm_kind.assign(cs->perm_col_kind, cs->perm_col_kind + P);
+    key->perm_index.assign(cs->perm_col_index, cs->perm_col_index + P);
+    key->has_lookup = cs->n_lookups == 1;
+    if (key->has_lookup) key->lookup = cs->lookups[0];
+    key->srs = *srs;
+    const uint32_t F = cs->n_fixed, u = key->u;
+    // lookup table index (host): the distinct values of the table's usable
+    // rows in the order of the device search, each row's index, 1 / copies
+    std::vector<std::array<uint64_t, 4>> uniq;
+    std::vector<uint32_t> uid;
+    std::vector<Fr4> tinv;
+    if (key->has_lookup) {
+        const uint64_t* t = fixed_values[key->lookup.table_fixed];
+        std::map<std::array<uint64_t, 4>, uint32_t> count;
+        for (uint32_t i = 0; i < u; i++) count[{t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]}]++;
+        std::map<std::array<uint64_t, 4>, uint32_t> index;
+        for (auto& kv : count) {
+            // the device compares the 64-bit words from the lowest: the map's order
+            index[kv.first] = (uint32_t)uniq.size();
+            uniq.push_back(kv.first);
+            tinv.push_back(host::fr_inv(host::fr_from_u64(kv.second)));
+        }
+        uid.resize(u);
+        for (uint32_t i = 0; i < u; i++) uid[i] = index[{t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]}];
+        key->n_uniq = (uint32_t)uniq.size();
+    }
+    const bool need_ones = key->has_lookup && key->lookup.selector_fixed < 0;
+    // one device allocation for the whole key
+    const size_t fr_elems = (size_t)F * (2 * n + E) + (size_t)P * (2 * n + E) + 3 * (size_t)E + (need_ones ? n : 0) +
+                            2 * (size_t)key->n_uniq;
+    const size_t bytes = fr_elems * sizeof(Fr) + (size_t)u * 4 * key->has_lookup + 256;
+    cudaError_t e = cudaMalloc(&key->mem, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("keygen: device allocation of " + std::to_string(bytes) + " bytes failed");
+        return ERR_OOM;
+    }
+    cudaStream_t st = ctx->stream;
+    Fr* carve = static_cast<Fr*>(key->mem);
+    auto take = [&](size_t elems) {
+        Fr* p = carve;
+        carve += elems;
+        return p;
+    };
+    for (uint32_t i = 0; i < F; i++) {
+        key->fixed_lag.push_back(take(n));
+        key->fixed_coeff.push_back(take(n));
+        key->fixed_ext.push_back(take(E));
+    }
+    for (uint32_t i = 0; i < P; i++) {
+        key->perm_lag.push_back(take(n));
+        key->perm_coeff.push_back(take(n));
+        key->perm_ext.push_back(take(E));
+    }
+    key->l0 = take(E);
+    key->l_last = take(E);
+    key->l_active = take(E);
+    if (need_ones) key->ones = take(n);
+    if (key->has_lookup) {
+        key->uniq = take(key->n_uniq);
+        key->tinv = take(key->n_uniq);
+        key->uid = reinterpret_cast<uint32_t*>(carve);
+    }
+    // fixed columns
+    for (uint32_t i = 0; i < F; i++) {
+        MZK_CUDA_CHECK(cudaMemcpyAsync(key->fixed_lag[i], fixed_values[i], (size_t)n * sizeof(Fr),
+                                       cudaMemcpyHostToDevice, st));
+        MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, key->fixed_lag[i], key->fixed_coeff[i], st));
+        MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, key->fixed_coeff[i], key->fixed_ext[i], st));
+    }
+    // permutation polynomials (build_pk)
+    if (P) {
+        std::vector<Fr4> deltas(P);
+        Fr4 delta;
+        std::memcpy(delta.l, host::FR_DELTA4, 32);
+        deltas[0] = host::fr_one();
+        for (uint32_t c = 1; c < P; c++) deltas[c] = host::fr_mul(deltas[c - 1], delta);
+        void *d_tab, *d_map = nullptr;
+        MZK_TRY(ctx->ensure("kg_deltas", (size_t)P * sizeof(Fr), &d_tab));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(d_tab, deltas.data(), (size_t)P * 32, cudaMemcpyHostToDevice, st));
+        if (mapping) {
+            MZK_TRY(ctx->ensure("kg_mapping", (size_t)P * n * 8, &d_map));
+            MZK_CUDA_CHECK(cudaMemcpyAsync(d_map, mapping, (size_t)P * n * 8, cudaMemcpyHostToDevice, st));
+        }
+        k_perm_values<<<grid_of(ctx, (uint64_t)P * n), kThreads, 0, st>>>(
+            key->perm_lag[0], static_cast<const uint32_t*>(d_map), static_cast<const Fr*>(d_tab), d->lo[0], d->hi[0],
+            n, P);
+        MZK_LAUNCH_CHECK(ctx);
+        for (uint32_t i = 0; i < P; i++) {
+            MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, key->perm_lag[i], key->perm_coeff[i], st));
+            MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, key->perm_coeff[i], key->perm_ext[i], st));
+        }
+    }
+    // l0, l_last, l_active_row (compute_lagrange_polys)
+    {
+        void* tmp;
+        MZK_TRY(ctx->ensure("kg_lagrange", (size_t)(2 * n + E) * sizeof(Fr), &tmp));
+        Fr* lag = static_cast<Fr*>(tmp);
+        Fr* coeff = lag + n;
+        Fr* blind_ext = coeff + n;
+        const uint64_t bf = key->bf;
+        struct {
+            uint64_t lo, hi;
+            Fr* ext;
+        } polys[3] = {{0, 1, key->l0}, {n - bf - 1, n - bf, key->l_last}, {n - bf, n, blind_ext}};
+        for (auto& p : polys) {
+            k_unit<<<grid_of(ctx, n), kThreads, 0, st>>>(lag, n, p.lo, p.hi);
+            MZK_LAUNCH_CHECK(ctx);
+            MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, lag, coeff, st));
+            MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, coeff, p.ext, st));
+        }
+        k_active<<<grid_of(ctx, E), kThreads, 0, st>>>(key->l_active, key->l_last, blind_ext, E);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    if (need_ones) {
+        k_unit<<<grid_of(ctx, n), kThreads, 0, st>>>(key->ones, n, 0, n);
+        MZK_LAUNCH_CHECK(ctx);
+    }
+    if (key->has_lookup) {
+        MZK_CUDA_CHECK(cudaMemcpyAsync(key->uniq, uniq.data(), uniq.size() * 32, cudaMemcpyHostToDevice, st));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(key->tinv, tinv.data(), tinv.size() * 32, cudaMemcpyHostToDevice, st));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(key->uid, uid.data(), uid.size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    // VK commitments (Lagrange basis) as one batch
+    std::vector<BatchItem> items;
+    for (uint32_t i = 0; i < F; i++) items.push_back({key->fixed_lag[i], srs->off_lagrange, n});
+    for (uint32_t i = 0; i < P; i++) items.push_back({key->perm_lag[i], srs->off_lagrange, n});
+    std::vector<uint64_t> res(items.size() * 18);
+    MsmTable table{srs->srs, srs->srs_len, srs->table_c, srs->table_rows, srs->table_min_n};
+    if (!items.empty())
+        MZK_TRY(run_msms(ctx, srs->srs, srs->srs_len, items, res.data(), 0, srs->table_c > 0 ? &table : nullptr, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    key->fixed_coms.resize(F);
+    key->perm_coms.resize(P);
+    for (uint32_t i = 0; i < F; i++) std::memcpy(key->fixed_coms[i].data(), &res[18 * i], 144);
+    for (uint32_t i = 0; i < P; i++) std::memcpy(key->perm_coms[i].data(), &res[18 * (F + i)], 144);
+    MZK_TRY(vk_transcript_repr(d->k, F ? key->fixed_coms[0].data() : nullptr, F,
+                               P ? key->perm_coms[0].data() : nullptr, P, pinned, pinned_len, &key->repr));
+    // the multi-open layout (prover.rs:871-933 query order)
+    std::vector<std::pair<std::pair<int, uint32_t>, int32_t>> qs;
+    for (auto& q : key->advice_queries) qs.push_back({{PlonkKey::P_ADVICE, q.column}, q.rotation});
+    for (uint32_t s = 0; s < key->n_sets; s++) {
+        qs.push_back({{PlonkKey::P_PERM_Z, s}, 0});
+        qs.push_back({{PlonkKey::P_PERM_Z, s}, 1});
+    }
+    for (uint32_t s = key->n_sets; s-- > 1;) qs.push_back({{PlonkKey::P_PERM_Z, s - 1}, key->last_rot()});
+    if (key->has_lookup) {
+        qs.push_back({{PlonkKey::P_M, 0}, 0});
+        qs.push_back({{PlonkKey::P_H, 0}, 0});
+        qs.push_back({{PlonkKey::P_AGG, 0}, 0});
+        qs.push_back({{PlonkKey::P_AGG, 0}, 1});
+    }
+    for (auto& q : key->fixed_queries) qs.push_back({{PlonkKey::P_FIXED, q.column}, q.rotation});
+    for (uint32_t i = 0; i < P; i++) qs.push_back({{PlonkKey::P_PERM_FIXED, i}, 0});
+    qs.push_back({{PlonkKey::P_LIN, 0}, 0});
+    build_open_sets(key.get(), qs);
+    const uint32_t L = key->has_lookup ? 1 : 0, S = key->n_sets;
+    const size_t points = cs->n_advice + L + S + 2 * L + key->qdeg + 2;
+    const size_t scalars = key->advice_queries.size() + key->fixed_queries.size() + P + (S ? 3 * S - 1 : 0) + 4 * L +
+                           key->open_sets.size();
+    key->proof_len = 48 * points + 32 * scalars;
+    key->n_blinds = (size_t)cs->n_advice * (key->bf + 1) + L * (key->bf + 1) + (size_t)S * key->bf + L * key->bf +
+                    (key->qdeg - 1);
+    *out = key.release();
+    return OK;
+}
+
+// --------------------------------------------------------------- prover ----
+namespace {
+
+struct FsProof {
+    const PlonkKey* key = nullptr;
+    const mzk_proof_request* req = nullptr;
+    host::Transcript tr;
+    Fr4 theta, beta, gamma, trash, y, x, xn, x1, x2, x3, x4;
+    std::vector<Fr*> adv_lag, adv_coeff, adv_ext, z_lag, z_delta, z_coeff, z_ext, q, fdiv;
+    Fr *m_lag = nullptr, *m_delta = nullptr, *m_coeff = nullptr, *m_ext = nullptr;
+    Fr *h_lag = nullptr, *h_coeff = nullptr, *h_ext = nullptr;
+    Fr *Z_lag = nullptr, *Z_dd = nullptr, *Z_coeff = nullptr, *Z_ext = nullptr;
+    Fr *limbs = nullptr, *lin = nullptr, *f = nullptr, *fin = nullptr, *pi = nullptr, *tmp_a = nullptr,
+       *tmp_b = nullptr;
+    Fr* d_blinds = nullptr;
+    uint32_t* counts = nullptr;
+    uint64_t f_len = 0;
+    // blinding offsets (elements of req->blinds)
+    size_t off_mult = 0, off_perm = 0, off_logup = 0, off_quot = 0;
+    // evaluations
+    std::vector<Fr4> ev_adv, ev_fix, ev_pc, ev_sets, ev_lk, q_x3;
+};
+
+size_t proof_scratch_elems(const PlonkKey* k) {
+    const size_t n = k->n, E = (size_t)1 << k->dom->ext_k, A = k->n_advice, S = k->n_sets;
+    const size_t L = k->has_lookup ? 1 : 0, O = k->open_sets.size();
+    return A * (2 * n + E) + S * (3 * n + E) + L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) + k->qdeg * n +
+           (4 + 2 * O + 2) * n + k->n_blinds + L * ((k->n_uniq + 7) / 8);
+}
+
+Status eval_many(Context* ctx, const std::vector<EvalTask>& in, std::vector<Fr4>& results, cudaStream_t st) {
+    results.assign(in.size(), host::fr_zero());
+    if (in.empty()) return OK;
+    // level sizes: level l of task t has ceil(len / 2048^l) values; the last
+    // level with more than one value writes into the results slot
+    std::vector<uint64_t> cur_len(in.size());
+    std::vector<Fr4> point(in.size());
+    size_t scratch = 0;
+    for (size_t t = 0; t < in.size(); t++) {
+        cur_len[t] = in[t].len;
+        std::memcpy(point[t].l, in[t].pw[0].l, 32);
+        uint64_t len = in[t].len;
+        while (len > kEvalSeg) {
+            len = (len + kEvalSeg - 1) / kEvalSeg;
+            scratch += len;
+        }
+    }
+    void *d_res, *d_seg, *d_tab;
+    MZK_TRY(ctx->ensure("fs_eval_res", in.size() * sizeof(Fr), &d_res));
+    MZK_TRY(ctx->ensure("fs_eval_seg", std::max<size_t>(scratch, 1) * sizeof(Fr), &d_seg));
+    MZK_TRY(ctx->ensure("fs_eval_tab", in.size() * sizeof(EvalTask), &d_tab));
+    MZK_CUDA_CHECK(cudaMemsetAsync(d_res, 0, in.size() * sizeof(Fr), st));
+    Fr* seg = static_cast<Fr*>(d_seg);
+    std::vector<const Fr*> src(in.size());
+    for (size_t t = 0; t < in.size(); t++) src[t] = in[t].poly;
+    for (;;) {
+        std::vector<EvalTask> lvl;
+        uint32_t max_blocks = 0;
+        for (size_t t = 0; t < in.size(); t++) {
+            if (cur_len[t] == 0) continue;
+            EvalTask e{};
+            e.poly = src[t];
+            e.len = cur_len[t];
+            const uint64_t blocks = (cur_len[t] + kEvalSeg - 1) / kEvalSeg;
+            Fr* dst = blocks == 1 ? static_cast<Fr*>(d_res) + t : seg;
+            if (blocks > 1) seg += blocks;
+            e.seg_out = dst;
+            Fr4 p = point[t];
+            e.pw[0] = to_dev(p);
+            Fr4 p8 = host::fr_pow_u64(p, 8);
+            for (int l = 0; l < 8; l++) {
+                e.pw[1 + l] = to_dev(p8);
+                p8 = host::fr_mul(p8, p8);
+            }
+            lvl.push_back(e);
+            max_blocks = std::max<uint32_t>(max_blocks, (uint32_t)blocks);
+            // the next level evaluates the segment sums at point^2048
+            src[t] = dst;
+            point[t] = host::fr_pow_u64(p, kEvalSeg);
+            cur_len[t] = blocks == 1 ? 0 : blocks;
+        }
+        if (lvl.empty()) break;
+        MZK_TRY(ctx->ensure("fs_eval_tab", lvl.size() * sizeof(EvalTask), &d_tab));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(d_tab, lvl.data(), lvl.size() * sizeof(EvalTask), cudaMemcpyHostToDevice, st));
+        k_eval_segments<<<dim3(max_blocks, (uint32_t)lvl.size()), kThreads, 0, st>>>(
+            static_cast<const EvalTask*>(d_tab));
+        MZK_LAUNCH_CHECK(ctx);
+        // the task table is read by the kernel: the next level's upload waits for it
+        MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
+    MZK_CUDA_CHECK(cudaMemcpyAsync(results.data(), d_res, in.size() * 32, cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    return OK;
+}
+
+EvalTask eval_task(const Fr* p, uint64_t len, const Fr4& point) {
+    EvalTask e{};
+    e.poly = p;
+    e.len = len;
+    e.pw[0] = to_dev(point);
+    return e;
+}
+
+struct LinSpec {
+    Fr* out;
+    uint64_t len;
+    std::vector<LinTerm> terms;
+};
+
+Status lincomb_many(Context* ctx, const std::vector<LinSpec>& specs, cudaStream_t st) {
+    if (specs.empty()) return OK;
+    std::vector<LinOut> outs;
+    std::vector<LinTerm> terms;
+    uint64_t max_len = 0;
+    for (auto& s : specs) {
+        outs.push_back({s.out, s.len, (uint32_t)terms.size(), (uint32_t)s.terms.size()});
+        terms.insert(terms.end(), s.terms.begin(), s.terms.end());
+        max_len = std::max(max_len, s.len);
+    }
+    void* d_tab;
+    const size_t ob = outs.size() * sizeof(LinOut), tb = terms.size() * sizeof(LinTerm);
+    MZK_TRY(ctx->ensure("fs_lin_tab", ob + tb + 16, &d_tab));
+    std::vector<uint8_t> h(ob + tb);
+    std::memcpy(h.data(), outs.data(), ob);
+    std::memcpy(h.data() + ob, terms.data(), tb);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_tab, h.data(), h.size(), cudaMemcpyHostToDevice, st));
+    const uint32_t gx = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>((max_len + kThreads - 1) / kThreads, (uint64_t)ctx->num_sms * 4));
+    k_lincomb<<<dim3(gx, (uint32_t)outs.size()), kThreads, 0, st>>>(
+        static_cast<const LinOut*>(d_tab), reinterpret_cast<const LinTerm*>(static_cast<uint8_t*>(d_tab) + ob));
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));  // the table buffer is reused by the next call
+    return OK;
+}
+
+// the identities of partially_evaluate_identities (plonk/mod.rs:519-608),
+// every one fully evaluated, folded in y by Horner (the linearization's
+// constant term, linearization/prover.rs:52-69)
+Fr4 identities_at_x(const FsProof& p) {
+    using namespace host;
+    const PlonkKey* k = p.key;
+    const Domain* d = k->dom;
+    const Fr4 one = host::fr_one();
+    auto adv = [&](uint32_t col) {
+        for (size_t i = 0; i < k->advice_queries.size(); i++)
+            if (k->advice_queries[i].column == col && k->advice_queries[i].rotation == 0) return p.ev_adv[i];
+        return host::fr_zero();
+    };
+    auto fix = [&](uint32_t col) {
+        for (size_t i = 0; i < k->fixed_queries.size(); i++)
+            if (k->fixed_queries[i].column == col && k->fixed_queries[i].rotation == 0) return p.ev_fix[i];
+        return host::fr_zero();
+    };
+    std::vector<Fr4> ids;
+    // the standard gate
+    const Fr4 a = adv(k->gate_advice[0]), b = adv(k->gate_advice[1]), c = adv(k->gate_advice[2]);
+    Fr4 g = fr_mul(fix(k->gate_fixed[0]), a);
+    g = fr_add(g, fr_mul(fix(k->gate_fixed[1]), b));
+    g = fr_add(g, fr_mul(fr_mul(fix(k->gate_fixed[2]), a), b));
+    g = fr_add(g, fr_mul(fix(k->gate_fixed[3]), c));
+    g = fr_add(g, fix(k->gate_fixed[4]));
+    ids.push_back(g);
+    // l_last, l_blind, l_0 (l_i_range over -(bf + 1) ..= 0)
+    const int32_t bf = (int32_t)k->bf;
+    const Fr4 l_last = l_i(d, p.x, p.xn, -(bf + 1));
+    Fr4 l_blind = host::fr_zero();
+    for (int32_t i = -bf; i <= -1; i++) l_blind = fr_add(l_blind, l_i(d, p.x, p.xn, i));
+    const Fr4 l_0 = l_i(d, p.x, p.xn, 0);
+    const Fr4 active = fr_sub(one, fr_add(l_last, l_blind));
+    // permutation (permutation.rs:195-290)
+    const uint32_t S = k->n_sets;
+    if (S) {
+        auto z = [&](uint32_t s, int which) { return p.ev_sets[3 * s + which]; };
+        ids.push_back(fr_mul(l_0, fr_sub(one, z(0, 0))));
+        ids.push_back(fr_mul(fr_sub(fr_mul(z(S - 1, 0), z(S - 1, 0)), z(S - 1, 0)), l_last));
+        for (uint32_t s = 1; s < S; s++) ids.push_back(fr_mul(fr_sub(z(s, 0), z(s - 1, 2)), l_0));
+        Fr4 delta;
+        std::memcpy(delta.l, host::FR_DELTA4, 32);
+        for (uint32_t s = 0; s < S; s++) {
+            const uint32_t c0 = s * k->chunk, c1 = std::min(k->n_perm, c0 + k->chunk);
+            Fr4 left = z(s, 1), right = z(s, 0);
+            Fr4 cur = fr_mul(fr_mul(p.beta, p.x), fr_pow_u64(delta, c0));
+            for (uint32_t ci = c0; ci < c1; ci++) {
+                const Fr4 e = k->perm_kind[ci] == 0 ? adv(k->perm_index[ci]) : fix(k->perm_index[ci]);
+                left = fr_mul(left, fr_add(fr_add(e, fr_mul(p.beta, p.ev_pc[ci])), p.gamma));
+                right = fr_mul(right, fr_add(fr_add(e, cur), p.gamma));
+                cur = fr_mul(cur, delta);
+            }
+            ids.push_back(fr_mul(fr_sub(left, right), active));
+        }
+    }
+    // the lookup (logup.rs:405-485): one input expression and one helper
+    if (k->has_lookup) {
+        const Fr4 m = p.ev_lk[0], h = p.ev_lk[1], Z = p.ev_lk[2], Zn = p.ev_lk[3];
+        const Fr4 f = adv(k->lookup.input_advice), t = fix(k->lookup.table_fixed);
+        const Fr4 sel = k->lookup.selector_fixed >= 0 ? fix((uint32_t)k->lookup.selector_fixed) : one;
+        ids.push_back(fr_mul(fr_add(l_0, l_last), Z));
+        ids.push_back(fr_sub(fr_mul(h, fr_add(f, p.beta)), one));
+        Fr4 acc = fr_sub(fr_sub(Zn, Z), fr_mul(sel, h));
+        acc = fr_add(fr_mul(acc, fr_add(t, p.beta)), m);
+        ids.push_back(fr_mul(acc, active));
+    }
+    Fr4 acc = host::fr_zero();
+    for (const Fr4& v : ids) acc = fr_add(fr_mul(acc, p.y), v);
+    return acc;
+}
+
+const Fr* open_poly(const FsProof& p, std::pair<int, uint32_t> id) {
+    const PlonkKey* k = p.key;
+    switch (id.first) {
+        case PlonkKey::P_ADVICE: return p.adv_coeff[id.second];
+        case PlonkKey::P_PERM_Z: return p.z_coeff[id.second];
+        case PlonkKey::P_M: return p.m_coeff;
+        case PlonkKey::P_H: return p.h_coeff;
+        case PlonkKey::P_AGG: return p.Z_coeff;
+        case PlonkKey::P_FIXED: return k->fixed_coeff[id.second];
+        case PlonkKey::P_PERM_FIXED: return k->perm_coeff[id.second];
+        default: return p.lin;
+    }
+}
+
+}  // namespace
+
+Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, uint32_t flags, cudaStream_t st) {
+    using namespace host;
+    if (count == 0) return OK;
+    const PlonkKey* k0 = reinterpret_cast<const PlonkKey*>(reqs[0].key);
+    if (!k0) {
+        set_error("create_proof: null key");
+        return ERR_ARG;
+    }
+    const mzk_srs_desc srs = k0->srs;
+    for (size_t j = 0; j < count; j++) {
+        const PlonkKey* k = reinterpret_cast<const PlonkKey*>(reqs[j].key);
+        if (!k || !reqs[j].advice || !reqs[j].blinds || !reqs[j].proof_out) {
+            set_error("create_proof: null argument in request " + std::to_string(j));
+            return ERR_ARG;
+        }
+        if (k->srs.srs != srs.srs || k->srs.srs_len != srs.srs_len || k->srs.table_c != srs.table_c) {
+            set_error("create_proof: all keys of one call must share one SRS buffer");
+            return ERR_ARG;
+        }
+        for (uint32_t i = 0; i < k->n_advice; i++)
+            if (!reqs[j].advice[i]) {
+                set_error("create_proof: null advice column in request " + std::to_string(j));
+                return ERR_ARG;
+            }
+    }
+    MsmTable table{srs.srs, srs.srs_len, srs.table_c, srs.table_rows, srs.table_min_n};
+    const MsmTable* tab = srs.table_c > 0 ? &table : nullptr;
+    // scratch: every proof's buffers carved from one device buffer
+    size_t total = 0, max_E = 0;
+    for (size_t j = 0; j < count; j++) {
+        const PlonkKey* k = reinterpret_cast<const PlonkKey*>(reqs[j].key);
+        total += proof_scratch_elems(k) + 8;
+        max_E = std::max<size_t>(max_E, (size_t)1 << k->dom->ext_k);
+    }
+    void *wave, *hbuf, *dbl, *dmiss;
+    MZK_TRY(ctx->ensure("fs_wave", total * sizeof(Fr), &wave));
+    MZK_TRY(ctx->ensure("fs_hbuf", max_E * sizeof(Fr), &hbuf));
+    MZK_TRY(ctx->ensure("fs_qblinds", 16 * sizeof(Fr), &dbl));
+    MZK_TRY(ctx->ensure("fs_missing", count * 4, &dmiss));
+    std::vector<FsProof> ps(count);
+    Fr* carve = static_cast<Fr*>(wave);
+    auto take = [&](size_t elems) {
+        Fr* p = carve;
+        carve += elems;
+        return p;
+    };
+    for (size_t j = 0; j < count; j++) {
+        FsProof& p = ps[j];
+        p.req = &reqs[j];
+        p.key = reinterpret_cast<const PlonkKey*>(reqs[j].key);
+        const PlonkKey* k = p.key;
+        const size_t n = k->n, E = (size_t)1 << k->dom->ext_k;
+        Fr* start = carve;
+        for (uint32_t i = 0; i < k->n_advice; i++) {
+            p.adv_lag.push_back(take(n));
+            p.adv_coeff.push_back(take(n));
+            p.adv_ext.push_back(take(E));
+        }
+        for (uint32_t s = 0; s < k->n_sets; s++) {
+            p.z_lag.push_back(take(n));
+            p.z_delta.push_back(take(n));
+            p.z_coeff.push_back(take(n));
+            p.z_ext.push_back(take(E));
+        }
+        if (k->has_lookup) {
+            p.m_lag = take(n), p.m_delta = take(n), p.m_coeff = take(n), p.m_ext = take(E);
+            p.h_lag = take(n), p.h_coeff = take(n), p.h_ext = take(E);
+            p.Z_lag = take(n), p.Z_dd = take(n), p.Z_coeff = take(n), p.Z_ext = take(E);
+        }
+        p.limbs = take((size_t)k->qdeg * n);
+        p.lin = take(n), p.f = take(n), p.fin = take(n), p.pi = take(n);
+        for (size_t s = 0; s < k->open_sets.size(); s++) {
+            p.q.push_back(take(n));
+            p.fdiv.push_back(take(n));
+        }
+        p.tmp_a = take(n), p.tmp_b = take(n);
+        p.d_blinds = take(k->n_blinds);
+        if (k->has_lookup) p.counts = reinterpret_cast<uint32_t*>(take((k->n_uniq + 7) / 8));
+        carve = start + proof_scratch_elems(k) + 8;
+        const size_t A = k->n_advice, L = k->has_lookup ? 1 : 0;
+        p.off_mult = A * (k->bf + 1);
+        p.off_perm = p.off_mult + L * (k->bf + 1);
+        p.off_logup = p.off_perm + (size_t)k->n_sets * k->bf;
+        p.off_quot = p.off_logup + L * k->bf;
+        MZK_CUDA_CHECK(cudaMemcpyAsync(p.d_blinds, reqs[j].blinds, k->n_blinds * sizeof(Fr), cudaMemcpyHostToDevice,
+                                       st));
+        p.tr.common_fr(k->repr);  // vk.hash_into (prover.rs:101)
+    }
+    auto write_points = [&](FsProof& p, const uint64_t* res, size_t m) {
+        for (size_t i = 0; i < m; i++) p.tr.write_point(res + 18 * i);
+    };
+    std::vector<BatchItem> items;
+    std::vector<uint64_t> res;
+    auto msm = [&]() -> Status {
+        res.assign(items.size() * 18, 0);
+        if (!items.empty()) MZK_TRY(run_msms(ctx, srs.srs, srs.srs_len, items, res.data(), flags, tab, st));
+        MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+        return OK;
+    };
+    // ---- 1. advice (parse_advices, prover.rs:604-627), theta -------------
+    items.clear();
+    for (auto& p : ps) {
+        const PlonkKey* k = p.key;
+        const size_t n = k->n, u = k->u;
+        for (uint32_t i = 0; i < k->n_advice; i++) {
+            MZK_CUDA_CHECK(cudaMemcpyAsync(p.adv_lag[i], p.req->advice[i], u * sizeof(Fr),
+                                           p.req->advice_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                           st));
+            MZK_CUDA_CHECK(cudaMemcpyAsync(p.adv_lag[i] + u, p.d_blinds + (size_t)i * (k->bf + 1),
+                                           (n - u) * sizeof(Fr), cudaMemcpyDeviceToDevice, st));
+            items.push_back({p.adv_lag[i], k->srs.off_lagrange, n});
+        }
+    }
+    MZK_TRY(msm());
+    for (size_t j = 0, at = 0; j < count; j++) {
+        write_points(ps[j], &res[18 * at], ps[j].key->n_advice);
+        at += ps[j].key->n_advice;
+        ps[j].theta = ps[j].tr.squeeze();
+    }
+    // ---- 2. multiplicities, beta, gamma ---------------------------------
+    items.clear();
+    MZK_CUDA_CHECK(cudaMemsetAsync(dmiss, 0, count * 4, st));
+    for (size_t j = 0; j < count; j++) {
+        FsProof& p = ps[j];
+        const PlonkKey* k = p.key;
+        if (!k->has_lookup) continue;
+        const uint32_t n = k->n, u = k->u;
+        const Fr* sel = k->lookup.selector_fixed >= 0 ? k->fixed_lag[k->lookup.selector_fixed] : nullptr;
+        MZK_CUDA_CHECK(cudaMemsetAsync(p.counts, 0, (size_t)k->n_uniq * 4, st));
+        k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(p.adv_lag[k->lookup.input_advice], sel, u, k->uniq,
+                                                             k->n_uniq, p.counts, static_cast<uint32_t*>(dmiss) + j);
+        MZK_LAUNCH_CHECK(ctx);
+        k_lookup_m<<<grid_of(ctx, u), kThreads, 0, st>>>(p.m_lag, k->uid, p.counts, k->tinv, u);
+        MZK_LAUNCH_CHECK(ctx);
+        MZK_CUDA_CHECK(cudaMemcpyAsync(p.m_lag + u, p.d_blinds + p.off_mult, (size_t)(n - u) * sizeof(Fr),
+                                       cudaMemcpyDeviceToDevice, st));
+        MZK_TRY(delta_device(ctx, p.m_lag, p.m_delta, n, 1, st));
+        items.push_back({p.m_delta, k->srs.off_lagrange_delta, n});
+    }
+    MZK_TRY(msm());
+    {
+        std::vector<uint32_t> miss(count);
+        MZK_CUDA_CHECK(cudaMemcpy(miss.data(), dmiss, count * 4, cudaMemcpyDeviceToHost));
+        for (size_t j = 0; j < count; j++)
+            if (miss[j]) {
+                set_error("create_proof: request " + std::to_string(j) + ": a lookup input value is not in the table");
+                return ERR_ARG;
+            }
+    }
+    for (size_t j = 0, at = 0; j < count; j++) {
+        FsProof& p = ps[j];
+        if (p.key->has_lookup) write_points(p, &res[18 * at++], 1);
+        p.beta = p.tr.squeeze();
+        p.gamma = p.tr.squeeze();
+    }
+    // ---- 3. permutation products, logup helper and aggregator, trash, y --
+    items.clear();
+    for (auto& p : ps) {
+        const PlonkKey* k = p.key;
+        const uint32_t n = k->n;
+        if (k->n_sets) {
+            std::vector<const uint64_t*> vals(k->n_perm), sig(k->n_perm);
+            for (uint32_t c = 0; c < k->n_perm; c++) {
+                vals[c] = reinterpret_cast<const uint64_t*>(k->perm_kind[c] == 0 ? p.adv_lag[k->perm_index[c]]
+                                                                                  : k->fixed_lag[k->perm_index[c]]);
+                sig[c] = reinterpret_cast<const uint64_t*>(k->perm_lag[c]);
+            }
+            std::vector<uint64_t*> zo(k->n_sets);
+            for (uint32_t s = 0; s < k->n_sets; s++) zo[s] = reinterpret_cast<uint64_t*>(p.z_lag[s]);
+            mzk_permutation_desc pd;
+            std::memset(&pd, 0, sizeof(pd));
+            pd.n_cols = k->n_perm;
+            pd.values = vals.data();
+            pd.sigmas = sig.data();
+            pd.chunk_len = k->chunk;
+            pd.blinding_factors = k->bf;
+            pd.blinds = p.req->blinds + 4 * p.off_perm;
+            std::memcpy(pd.beta, p.beta.l, 32);
+            std::memcpy(pd.gamma, p.gamma.l, 32);
+            pd.z_out = zo.data();
+            MZK_TRY(permutation_z_device(ctx, k->dom, &pd, st));
+            for (uint32_t s = 0; s < k->n_sets; s++) {
+                MZK_TRY(delta_device(ctx, p.z_lag[s], p.z_delta[s], n, 1, st));
+                items.push_back({p.z_delta[s], k->srs.off_lagrange_delta, n});
+            }
+        }
+        if (k->has_lookup) {
+            const uint64_t* in[1] = {reinterpret_cast<const uint64_t*>(p.adv_lag[k->lookup.input_advice])};
+            uint64_t* ho[1] = {reinterpret_cast<uint64_t*>(p.h_lag)};
+            const uint32_t cols[1] = {1};
+            mzk_logup_desc ld;
+            std::memset(&ld, 0, sizeof(ld));
+            ld.n_chunks = 1;
+            ld.chunk_cols = cols;
+            ld.inputs = in;
+            ld.table = reinterpret_cast<const uint64_t*>(k->fixed_lag[k->lookup.table_fixed]);
+            ld.selector = reinterpret_cast<const uint64_t*>(
+                k->lookup.selector_fixed >= 0 ? k->fixed_lag[k->lookup.selector_fixed] : k->ones);
+            ld.multiplicities = reinterpret_cast<const uint64_t*>(p.m_lag);
+            ld.blinding_factors = k->bf;
+            ld.blinds = p.req->blinds + 4 * p.off_logup;
+            std::memcpy(ld.beta, p.beta.l, 32);
+            ld.helpers_out = ho;
+            ld.aggregator_out = reinterpret_cast<uint64_t*>(p.Z_lag);
+            MZK_TRY(logup_device(ctx, k->dom, &ld, st));
+            MZK_TRY(delta_device(ctx, p.Z_lag, p.Z_dd, n, 2, st));
+            items.push_back({p.h_lag, k->srs.off_lagrange, n});
+            items.push_back({p.Z_dd, k->srs.off_lagrange_double_delta, n});
+        }
+    }
+    MZK_TRY(msm());
+    for (size_t j = 0, at = 0; j < count; j++) {
+        FsProof& p = ps[j];
+        const size_t m = p.key->n_sets + (p.key->has_lookup ? 2 : 0);
+        write_points(p, &res[18 * at], m);
+        at += m;
+        p.trash = p.tr.squeeze();  // no trashcans: nothing is committed after it
+        p.y = p.tr.squeeze();
+    }
+    // ---- 4. cosets, quotient limbs, x -------------------------------------
+    items.clear();
+    for (auto& p : ps) {
+        const PlonkKey* k = p.key;
+        const Domain* d = k->dom;
+        std::vector<const void*> lag;
+        std::vector<Fr*> co, ex;
+        for (uint32_t i = 0; i < k->n_advice; i++) {
+            lag.push_back(p.adv_lag[i]);
+            co.push_back(p.adv_coeff[i]);
+            ex.push_back(p.adv_ext[i]);
+        }
+        for (uint32_t s = 0; s < k->n_sets; s++) {
+            lag.push_back(p.z_lag[s]);
+            co.push_back(p.z_coeff[s]);
+            ex.push_back(p.z_ext[s]);
+        }
+        if (k->has_lookup) {
+            lag.insert(lag.end(), {p.m_lag, p.h_lag, p.Z_lag});
+            co.insert(co.end(), {p.m_coeff, p.h_coeff, p.Z_coeff});
+            ex.insert(ex.end(), {p.m_ext, p.h_ext, p.Z_ext});
+        }
+        MZK_TRY(ntt_sequence(ctx, d, lag.data(), co.data(), ex.data(), (int)lag.size(),
+                             !(flags & MZK_PROVE_NO_GRAPHS), st));
+        std::vector<const uint64_t*> adv(k->n_advice), fixed(k->n_fixed), sig(k->n_perm), zs(k->n_sets);
+        for (uint32_t i = 0; i < k->n_advice; i++) adv[i] = reinterpret_cast<const uint64_t*>(p.adv_ext[i]);
+        for (uint32_t i = 0; i < k->n_fixed; i++) fixed[i] = reinterpret_cast<const uint64_t*>(k->fixed_ext[i]);
+        for (uint32_t i = 0; i < k->n_perm; i++) sig[i] = reinterpret_cast<const uint64_t*>(k->perm_ext[i]);
+        for (uint32_t s = 0; s < k->n_sets; s++) zs[s] = reinterpret_cast<const uint64_t*>(p.z_ext[s]);
+        mzk_quotient_desc q;
+        std::memset(&q, 0, sizeof(q));
+        q.k = d->k;
+        q.extended_k = d->ext_k;
+        q.advice = adv.data();
+        q.n_advice = k->n_advice;
+        q.fixed = fixed.data();
+        q.n_fixed = k->n_fixed;
+        std::memcpy(q.gate_fixed, k->gate_fixed, sizeof(q.gate_fixed));
+        std::memcpy(q.gate_advice, k->gate_advice, sizeof(q.gate_advice));
+        q.n_perm_cols = k->n_perm;
+        q.perm_col_kind = k->perm_kind.data();
+        q.perm_col_index = k->perm_index.data();
+        q.perm_sigma = sig.data();
+        q.n_perm_sets = k->n_sets;
+        q.perm_z = zs.data();
+        q.chunk_len = k->chunk;
+        q.blinding_factors = k->bf;
+        if (k->has_lookup) {
+            q.has_lookup = 1;
+            q.lookup_input_advice = k->lookup.input_advice;
+            q.lookup_table_fixed = k->lookup.table_fixed;
+            q.lookup_selector_fixed = k->lookup.selector_fixed;
+            q.lookup_h = reinterpret_cast<const uint64_t*>(p.h_ext);
+            q.lookup_z = reinterpret_cast<const uint64_t*>(p.Z_ext);
+            q.lookup_m = reinterpret_cast<const uint64_t*>(p.m_ext);
+        }
+        q.l0 = reinterpret_cast<const uint64_t*>(k->l0);
+        q.l_last = reinterpret_cast<const uint64_t*>(k->l_last);
+        q.l_active = reinterpret_cast<const uint64_t*>(k->l_active);
+        std::memcpy(q.y, p.y.l, 32);
+        std::memcpy(q.beta, p.beta.l, 32);
+        std::memcpy(q.gamma, p.gamma.l, 32);
+        std::memcpy(q.theta, p.theta.l, 32);
+        std::memcpy(q.trash_challenge, p.trash.l, 32);
+        MZK_TRY(compute_h_limbs_device(ctx, d, &q, p.req->blinds + 4 * p.off_quot, p.limbs, hbuf, dbl, st));
+        for (uint32_t i = 0; i < k->qdeg; i++) items.push_back({p.limbs + (size_t)i * k->n, k->srs.off_g, k->n});
+    }
+    MZK_TRY(msm());
+    for (size_t j = 0, at = 0; j < count; j++) {
+        FsProof& p = ps[j];
+        write_points(p, &res[18 * at], p.key->qdeg);
+        at += p.key->qdeg;
+        p.x = p.tr.squeeze();
+        p.xn = fr_pow_u64(p.x, p.key->n);
+    }
+    // ---- 5. evaluations, linearization, x1, x2 ----------------------------
+    {
+        std::vector<EvalTask> tasks;
+        for (auto& p : ps) {
+            const PlonkKey* k = p.key;
+            const Domain* d = k->dom;
+            const uint64_t n = k->n;
+            for (auto& q : k->advice_queries) tasks.push_back(eval_task(p.adv_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
+            for (auto& q : k->fixed_queries) tasks.push_back(eval_task(k->fixed_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
+            for (uint32_t i = 0; i < k->n_perm; i++) tasks.push_back(eval_task(k->perm_coeff[i], n, p.x));
+            for (uint32_t s = 0; s < k->n_sets; s++) {
+                tasks.push_back(eval_task(p.z_coeff[s], n, p.x));
+                tasks.push_back(eval_task(p.z_coeff[s], n, fr_rot(d, p.x, 1)));
+                tasks.push_back(eval_task(p.z_coeff[s], n, fr_rot(d, p.x, k->last_rot())));
+            }
+            if (k->has_lookup) {
+                tasks.push_back(eval_task(p.m_coeff, n, p.x));
+                tasks.push_back(eval_task(p.h_coeff, n, p.x));
+                tasks.push_back(eval_task(p.Z_coeff, n, p.x));
+                tasks.push_back(eval_task(p.Z_coeff, n, fr_rot(d, p.x, 1)));
+            }
+        }
+        std::vector<Fr4> ev;
+        MZK_TRY(eval_many(ctx, tasks, ev, st));
+        size_t at = 0;
+        std::vector<LinSpec> lins;
+        for (auto& p : ps) {
+            const PlonkKey* k = p.key;
+            auto grab = [&](std::vector<Fr4>& dst, size_t m) {
+                dst.assign(ev.begin() + at, ev.begin() + at + m);
+                at += m;
+            };
+            grab(p.ev_adv, k->advice_queries.size());
+            grab(p.ev_fix, k->fixed_queries.size());
+            grab(p.ev_pc, k->n_perm);
+            grab(p.ev_sets, 3 * (size_t)k->n_sets);
+            grab(p.ev_lk, k->has_lookup ? 4 : 0);
+            // transcript order (write_evals_to_transcript, permutation / logup evaluate)
+            for (auto& v : p.ev_adv) p.tr.write_fr(v);
+            for (auto& v : p.ev_fix) p.tr.write_fr(v);
+            for (auto& v : p.ev_pc) p.tr.write_fr(v);
+            for (uint32_t s = 0; s < k->n_sets; s++) {
+                p.tr.write_fr(p.ev_sets[3 * s]);
+                p.tr.write_fr(p.ev_sets[3 * s + 1]);
+                if (s + 1 < k->n_sets) p.tr.write_fr(p.ev_sets[3 * s + 2]);
+            }
+            for (auto& v : p.ev_lk) p.tr.write_fr(v);
+            // L'(X) = -sum_i (x^n - 1) (x^(n-1))^i h_i(X): the identities are
+            // all constants here (no simple selectors)
+            const Fr4 sf = fr_pow_u64(p.x, k->n - 1);
+            Fr4 s = fr_neg(fr_sub(p.xn, host::fr_one()));
+            LinSpec ls{p.lin, k->n, {}};
+            for (uint32_t i = 0; i < k->qdeg; i++) {
+                ls.terms.push_back({p.limbs + (size_t)i * k->n, k->n, to_dev(s)});
+                s = fr_mul(s, sf);
+            }
+            lins.push_back(ls);
+            p.x1 = p.tr.squeeze();
+            p.x2 = p.tr.squeeze();
+        }
+        MZK_TRY(lincomb_many(ctx, lins, st));
+    }
+    // ---- 6. q polynomials, f = sum x2^s q_s / prod (X - p), its commitment, x3
+    {
+        std::vector<LinSpec> qs;
+        for (auto& p : ps) {
+            const PlonkKey* k = p.key;
+            for (size_t s = 0; s < k->open_sets.size(); s++) {
+                LinSpec ls{p.q[s], k->n, {}};
+                Fr4 pw = host::fr_one();
+                for (auto& id : k->open_sets[s].polys) {
+                    ls.terms.push_back({open_poly(p, id), k->n, to_dev(pw)});
+                    pw = fr_mul(pw, p.x1);
+                }
+                qs.push_back(ls);
+            }
+        }
+        MZK_TRY(lincomb_many(ctx, qs, st));
+        std::vector<LinSpec> fs;
+        items.clear();
+        for (auto& p : ps) {
+            const PlonkKey* k = p.key;
+            LinSpec ls{p.f, 0, {}};
+            Fr4 pw = host::fr_one();
+            for (size_t s = 0; s < k->open_sets.size(); s++) {
+                const Fr* src = p.q[s];
+                uint64_t len = k->n;
+                const auto& rots = k->open_sets[s].rots;
+                for (size_t r = 0; r < rots.size(); r++) {
+                    Fr* dst = r + 1 == rots.size() ? p.fdiv[s] : (src == p.tmp_a ? p.tmp_b : p.tmp_a);
+                    const Fr4 pt = fr_rot(k->dom, p.x, rots[r]);
+                    MZK_TRY(kate_division_device(ctx, src, len, pt.l, dst, st));
+                    src = dst;
+                    len -= 1;
+                }
+                ls.terms.push_back({p.fdiv[s], len, to_dev(pw)});
+                ls.len = std::max<uint64_t>(ls.len, len);
+                pw = fr_mul(pw, p.x2);
+            }
+            p.f_len = ls.len;
+            fs.push_back(ls);
+            items.push_back({p.f, k->srs.off_g, p.f_len});
+        }
+        MZK_TRY(lincomb_many(ctx, fs, st));
+        MZK_TRY(msm());
+        for (size_t j = 0; j < count; j++) {
+            write_points(ps[j], &res[18 * j], 1);
+            ps[j].x3 = ps[j].tr.squeeze();
+        }
+    }
+    // ---- 7. q evaluations at x3, x4 ---------------------------------------
+    {
+        const bool check = (flags & MZK_PROVE_SELF_CHECK) != 0;
+        std::vector<EvalTask> tasks;
+        for (auto& p : ps) {
+            for (size_t s = 0; s < p.key->open_sets.size(); s++) tasks.push_back(eval_task(p.q[s], p.key->n, p.x3));
+            if (check) tasks.push_back(eval_task(p.lin, p.key->n, p.x));
+        }
+        std::vector<Fr4> ev;
+        MZK_TRY(eval_many(ctx, tasks, ev, st));
+        size_t at = 0;
+        for (size_t j = 0; j < count; j++) {
+            FsProof& p = ps[j];
+            for (size_t s = 0; s < p.key->open_sets.size(); s++) p.tr.write_fr(ev[at++]);
+            if (check) {
+                // L'(x) = -C holds iff the witness satisfies every identity
+                // (the reference's debug assertion, prover.rs:404-408)
+                const Fr4 lin_x = ev[at++];
+                if (!fr_eq(lin_x, fr_neg(identities_at_x(p)))) {
+                    set_error("create_proof: request " + std::to_string(j) +
+                              ": the witness does not satisfy the circuit (L'(x) != -C)");
+                    return ERR_ARG;
+                }
+            }
+            p.x4 = p.tr.squeeze();
+        }
+    }
+    // ---- 8. final polynomial and pi ---------------------------------------
+    // pi = (final - v) / (X - x3) with v = final(x3); kate_division drops the
+    // remainder, so the quotient of final itself is the same polynomial
+    {
+        std::vector<LinSpec> fins;
+        for (auto& p : ps) {
+            const PlonkKey* k = p.key;
+            LinSpec ls{p.fin, k->n, {}};
+            Fr4 pw = host::fr_one();
+            for (size_t s = 0; s < k->open_sets.size(); s++) {
+                ls.terms.push_back({p.q[s], k->n, to_dev(pw)});
+                pw = fr_mul(pw, p.x4);
+            }
+            ls.terms.push_back({p.f, p.f_len, to_dev(pw)});
+            fins.push_back(ls);
+        }
+        MZK_TRY(lincomb_many(ctx, fins, st));
+        items.clear();
+        for (auto& p : ps) {
+            MZK_TRY(kate_division_device(ctx, p.fin, p.key->n, p.x3.l, p.pi, st));
+            items.push_back({p.pi, p.key->srs.off_g, (uint64_t)p.key->n - 1});
+        }
+        MZK_TRY(msm());
+        for (size_t j = 0; j < count; j++) {
+            write_points(ps[j], &res[18 * j], 1);
+            const auto& pr = ps[j].tr.proof();
+            if (pr.size() != ps[j].key->proof_len) {
+                set_error("create_proof: internal proof length mismatch");
+                return ERR_STATE;
+            }
+            std::memcpy(reqs[j].proof_out, pr.data(), pr.size());
+        }
+    }
+    return OK;
+}
+
+}  // namespace mzk
+
+// ------------------------------------------------------------ the C ABI ----
+struct mzk_transcript {
+    mzk::host::Transcript t;
+};
+
+using mzk::Status;
+
+extern "C" {
+
+int mzk_transcript_create(mzk_transcript** out) {
+    if (!out) {
+        mzk::set_error("null out pointer");
+        return mzk::ERR_ARG;
+    }
+    *out = new (std::nothrow) mzk_transcript;
+    return *out ? mzk::OK : mzk::ERR_OOM;
+}
+int mzk_transcript_destroy(mzk_transcript* t) {
+    delete t;
+    return mzk::OK;
+}
+int mzk_transcript_common_fr(mzk_transcript* t, const uint64_t v[4]) {
+    if (!t || !v) return mzk::ERR_ARG;
+    mzk::host::Fr4 a;
+    std::memcpy(a.l, v, 32);
+    t->t.common_fr(a);
+    return mzk::OK;
+}
+int mzk_transcript_write_fr(mzk_transcript* t, const uint64_t v[4]) {
+    if (!t || !v) return mzk::ERR_ARG;
+    mzk::host::Fr4 a;
+    std::memcpy(a.l, v, 32);
+    t->t.write_fr(a);
+    return mzk::OK;
+}
+int mzk_transcript_write_point(mzk_transcript* t, const uint64_t p[18]) {
+    if (!t || !p) return mzk::ERR_ARG;
+    t->t.write_point(p);
+    return mzk::OK;
+}
+int mzk_transcript_squeeze(mzk_transcript* t, uint64_t out[4]) {
+    if (!t || !out) return mzk::ERR_ARG;
+    const mzk::host::Fr4 c = t->t.squeeze();
+    std::memcpy(out, c.l, 32);
+    return mzk::OK;
+}
+int mzk_transcript_proof(const mzk_transcript* t, uint8_t* out, size_t cap, size_t* len) {
+    if (!t || !len) return mzk::ERR_ARG;
+    const auto& p = t->t.proof();
+    *len = p.size();
+    if (out) {
+        if (cap < p.size()) {
+            mzk::set_error("transcript: output buffer too small");
+            return mzk::ERR_ARG;
+        }
+        std::memcpy(out, p.data(), p.size());
+    }
+    return mzk::OK;
+}
+int mzk_vk_transcript_repr(uint32_t k, const uint64_t* fixed_coms, size_t n_fixed, const uint64_t* perm_coms,
+                           size_t n_perm, const uint8_t* pinned, size_t pinned_len, uint64_t out[4]) {
+    if (!out || (n_fixed && !fixed_coms) || (n_perm && !perm_coms) || (pinned_len && !pinned) || k > 255) {
+        mzk::set_error("vk_transcript_repr: bad argument");
+        return mzk::ERR_ARG;
+    }
+    mzk::host::Fr4 r;
+    MZK_TRY(mzk::vk_transcript_repr(k, fixed_coms, n_fixed, perm_coms, n_perm, pinned, pinned_len, &r));
+    std::memcpy(out, r.l, 32);
+    return mzk::OK;
+}
+
+int mzk_keygen(mzk_ctx* ctx, mzk_domain* d, const mzk_circuit_desc* cs, const mzk_srs_desc* srs,
+               const uint64_t* const* fixed_values, const uint32_t* perm_mapping, const uint8_t* pinned,
+               size_t pinned_len, mzk_plonk_key** out) {
+    if (!ctx || !d || !cs || !out || (pinned_len && !pinned)) {
+        mzk::set_error("keygen: null argument");
+        return mzk::ERR_ARG;
+    }
+    *out = nullptr;
+    mzk::Context* c = mzk::context_of(ctx);
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    mzk::PlonkKey* key = nullptr;
+    MZK_TRY(mzk::keygen(c, mzk::domain_of(d), cs, srs, fixed_values, perm_mapping, pinned, pinned_len, &key));
+    *out = reinterpret_cast<mzk_plonk_key*>(key);
+    return mzk::OK;
+}
+
+int mzk_plonk_key_destroy(mzk_plonk_key* key) {
+    delete reinterpret_cast<mzk::PlonkKey*>(key);
+    return mzk::OK;
+}
+
+int mzk_plonk_key_info(const mzk_plonk_key* key, uint64_t repr[4], size_t* proof_len, size_t* n_blinds) {
+    if (!key) return mzk::ERR_ARG;
+    const mzk::PlonkKey* k = reinterpret_cast<const mzk::PlonkKey*>(key);
+    if (repr) std::memcpy(repr, k->repr.l, 32);
+    if (proof_len) *proof_len = k->proof_len;
+    if (n_blinds) *n_blinds = k->n_blinds;
+    return mzk::OK;
+}
+
+int mzk_plonk_key_commitments(const mzk_plonk_key* key, uint64_t* fixed, uint64_t* perm) {
+    if (!key) return mzk::ERR_ARG;
+    const mzk::PlonkKey* k = reinterpret_cast<const mzk::PlonkKey*>(key);
+    if (fixed)
+        for (size_t i = 0; i < k->fixed_coms.size(); i++) std::memcpy(fixed + 18 * i, k->fixed_coms[i].data(), 144);
+    if (perm)
+        for (size_t i = 0; i < k->perm_coms.size(); i++) std::memcpy(perm + 18 * i, k->perm_coms[i].data(), 144);
+    return mzk::OK;
+}
+
+int mzk_create_proofs(mzk_ctx* ctx, const mzk_proof_request* reqs, size_t count, uint32_t flags) {
+    if (!ctx || (count && !reqs)) {
+        mzk::set_error("create_proof: null argument");
+        return mzk::ERR_ARG;
+    }
+    mzk::Context* c = mzk::context_of(ctx);
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    const Status s = mzk::create_proofs(c, reqs, count, flags, c->stream);
+    if (s != mzk::OK) cudaStreamSynchronize(c->stream);
+    return s;
+}
+
+}  // extern "C"

@@ -60,9 +60,16 @@ constexpr int kPolys = 7;  // a, b, c, z, m, h, Z
 
 }  // namespace
 
+Status delta_device(Context* ctx, const void* a, void* out, uint32_t n, int order, cudaStream_t st) {
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 8);
+    k_delta<<<grid, 256, 0, st>>>(static_cast<const Fr*>(a), static_cast<Fr*>(out), n, order);
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
 // the MSMs of `items` against the SRS: one batched MSM, or one call each;
 // with a window table (table non-null) the large ones use it either way
-static Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const std::vector<BatchItem>& items,
+Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const std::vector<BatchItem>& items,
                        uint64_t* res, uint32_t flags, const MsmTable* table, cudaStream_t st) {
     if (!(flags & MZK_PROVE_MSM_PER_CALL))
         return msm_g1_batch_device(ctx, srs, srs_len, items.data(), items.size(), res, st, table);
@@ -78,15 +85,15 @@ static Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const st
 }
 
 // One proof's NTT sequence: lagrange_to_coeff then coeff_to_extended of each
-// of its seven polynomials (2-3 pass kernels per transform).  With use_graph
+// of its `count` polynomials (2-3 pass kernels per transform).  With use_graph
 // the sequence is captured once into a CUDA graph per key (the domain, its
-// tables, the NTT scratch, the pass splits and the 21 column pointers: all
+// tables, the NTT scratch, the pass splits and the column pointers: all
 // that the kernels read) and replayed afterwards; the graph holds the same
 // launches with the same arguments, so the results are the same.
-static Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag, Fr* const* coeff, Fr* const* ext,
-                           bool use_graph, cudaStream_t st) {
+Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag, Fr* const* coeff, Fr* const* ext,
+                    int count, bool use_graph, cudaStream_t st) {
     auto eager = [&]() -> Status {
-        for (int p = 0; p < kPolys; p++) {
+        for (int p = 0; p < count; p++) {
             MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, lag[p], coeff[p], st));
             MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, coeff[p], ext[p], st));
         }
@@ -98,9 +105,10 @@ static Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag
     void* tmp;
     MZK_TRY(ctx->ensure("ntt_tmp", ((size_t)1 << d->ext_k) * sizeof(Fr), &tmp));
     std::vector<uintptr_t> key = {(uintptr_t)d, d->k, d->ext_k, (uintptr_t)tmp,
-                                  (uintptr_t)ctx->tuned_ntt_split[d->k], (uintptr_t)ctx->tuned_ntt_split[d->ext_k]};
+                                  (uintptr_t)ctx->tuned_ntt_split[d->k], (uintptr_t)ctx->tuned_ntt_split[d->ext_k],
+                                  (uintptr_t)count};
     for (int r = 0; r < 4; r++) key.push_back((uintptr_t)d->tables[r]);
-    for (int p = 0; p < kPolys; p++) {
+    for (int p = 0; p < count; p++) {
         key.push_back((uintptr_t)lag[p]);
         key.push_back((uintptr_t)coeff[p]);
         key.push_back((uintptr_t)ext[p]);
@@ -302,7 +310,8 @@ Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_provi
         const mzk_proving_key_desc* pk = pks[j];
         const mzk_proof_job& jb = jobs[j];
         const void* const* lag = &lagrange[j * kPolys];
-        MZK_TRY(ntt_sequence(ctx, d, lag, &coeff[j * kPolys], &ext[j * kPolys], !(flags & MZK_PROVE_NO_GRAPHS), st));
+        MZK_TRY(ntt_sequence(ctx, d, lag, &coeff[j * kPolys], &ext[j * kPolys], kPolys, !(flags & MZK_PROVE_NO_GRAPHS),
+                             st));
         Fr* const* e = &ext[j * kPolys];
         const uint64_t* adv[3] = {(const uint64_t*)e[0], (const uint64_t*)e[1], (const uint64_t*)e[2]};
         const uint64_t* sig[3] = {pk->sigma_ext[0], pk->sigma_ext[1], pk->sigma_ext[2]};

@@ -210,9 +210,6 @@ Fr fr_from_u64s(const uint64_t* p) {
     return r;
 }
 
-// DELTA (GENERATOR^(2^S)), curves/src/bls12_381/fq.rs:501-508
-const uint64_t kDelta[4] = {0x70e310d3d146f96aULL, 0x4b64c08919e299e6ULL, 0x51e114186a8b970dULL,
-                            0x6185d06627c067cbULL};
 
 // Appends a flattened program to W after checking every index; returns its
 // header offset, or sets `err`.
@@ -439,7 +436,7 @@ Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_de
     std::memcpy(beta4.l, desc->beta, 32);
     const host::Fr4 ds = host::fr_mul(beta4, d->zeta);
     std::memcpy(q.delta_start.l, ds.l, 32);
-    q.delta = fr_from_u64s(kDelta);
+    q.delta = fr_from_u64s(host::FR_DELTA4);
     q.tlo = d->lo[2];
     q.thi = d->hi[2];
     q.tinv = static_cast<const Fr*>(d->d_tinv);

@@ -1,6 +1,7 @@
 // quotient.hpp — kernel parameters of the fused quotient evaluation.
 #pragma once
 #include <cstdint>
+#include <vector>
 
 #include "../../include/mzk.h"
 #include "field.cuh"
@@ -89,6 +90,18 @@ Status prove_core_device(Context* ctx, const Domain* d, const mzk_proving_key_de
 // jobs of different k: job j uses doms[j] and pks[j] (all keys share one SRS buffer)
 Status prove_core_multi(Context* ctx, const Domain* const* doms, const mzk_proving_key_desc* const* pks,
                         const mzk_proof_job* jobs, size_t count, uint64_t* out, uint32_t flags, cudaStream_t st);
+// Polynomial::to_delta (order 1) / to_double_delta (order 2) of n device Fr
+// (proofs/src/poly/mod.rs:297-336); out must not alias a
+Status delta_device(Context* ctx, const void* a, void* out, uint32_t n, int order, cudaStream_t st);
+// the MSMs of `items` against the SRS: one batched MSM, or with
+// MZK_PROVE_MSM_PER_CALL in flags one call each; with a window table
+// (table non-null) the items of at least table->min_n points use it
+Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const std::vector<BatchItem>& items, uint64_t* res,
+                uint32_t flags, const MsmTable* table, cudaStream_t st);
+// lagrange_to_coeff then coeff_to_extended of `count` polynomials, captured
+// once into a CUDA graph per pointer set and replayed when use_graph is set
+Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag, Fr* const* coeff, Fr* const* ext,
+                    int count, bool use_graph, cudaStream_t st);
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st);
 

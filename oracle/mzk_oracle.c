@@ -1403,6 +1403,11 @@ void or_poly_inner_product(const uint64_t *const *polys, const size_t *lens, siz
         }
 }
 
+/* element-wise product out[i] = a[i] * b[i] (test-input construction) */
+void or_fr_mul_vec(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t n) {
+    for (size_t i = 0; i < n; i++) fr_mul(out + 4 * i, a + 4 * i, b + 4 * i);
+}
+
 /* utils/arithmetic.rs:106-125: quotient of a(X) by (X - b), n - 1 coefficients:
  * from the top, q = a_{i+1} - tmp, tmp = q * (-b). */
 void or_kate_division(const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q) {

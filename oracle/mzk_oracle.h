@@ -123,6 +123,7 @@ void or_logup(const uint64_t *const *inputs, const uint32_t *chunk_cols, uint32_
               const uint64_t *selector, const uint64_t *multiplicities, size_t n, const uint64_t beta[4],
               uint32_t blinding_factors, const uint64_t *blinds, uint64_t *const *helpers_out,
               uint64_t *aggregator_out);
+void or_fr_mul_vec(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t n);
 void or_kate_division(const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q);
 void or_g1_suffix_sum(const uint64_t *in, size_t n, uint64_t *out);
 void or_srs_setup(const uint64_t s[4], uint32_t k, const uint64_t omega[4], uint64_t *g, uint64_t *lag,

@@ -43,6 +43,7 @@ def _load():
         "or_logup": (None, [ctypes.c_void_p, ctypes.POINTER(u32), u32, _u64p, _u64p, _u64p, sz, _u64p, u32, _u64p,
                             ctypes.c_void_p, _u64p]),
         "or_kate_division": (None, [_u64p, sz, _u64p, _u64p]),
+        "or_fr_mul_vec": (None, [_u64p, _u64p, _u64p, sz]),
         "or_g1_suffix_sum": (None, [_u64p, sz, _u64p]),
         "or_g1_decompress": (i32, [_u64p, _u8p, i32]),
         "or_srs_setup": (None, [_u64p, u32, _u64p, _u64p, _u64p, _u64p, _u64p]),
@@ -463,6 +464,15 @@ def srs_setup(s, k):
     outs = [np.zeros((n, 12), np.uint64) for _ in range(4)]
     lib.or_srs_setup(P(np.ascontiguousarray(s, np.uint64)), k, P(omega), *[P(o) for o in outs])
     return outs
+
+
+def fr_mul_vec(a, b):
+    """element-wise product of two Fr arrays of the same length"""
+    a = np.ascontiguousarray(a, np.uint64)
+    b = np.ascontiguousarray(b, np.uint64)
+    out = np.zeros_like(a)
+    lib.or_fr_mul_vec(P(a), P(b), P(out), a.shape[0])
+    return out
 
 
 def kate_division(a, b):

@@ -1,0 +1,877 @@
+"""CPU restatement of the reference's PLONK prover and verifier around the hot
+path: keygen, create_proof with its Blake2b Fiat-Shamir transcript, the KZG
+multi-open argument and the verifier's `prepare` with the pairing replaced by
+the G1 trapdoor check.
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA product.  Only tests/,
+__graft_entry__.smoke() and bench.py's cpu_baseline / reference legs import
+this module.
+
+Polynomials are numpy arrays of Montgomery Fr (shape (n, 4)) handled by the C
+oracle (oracle.py); scalars (challenges, evaluations) are Python integers in
+canonical form, so the scalar algebra of the transcript, the identities and
+the verifier is independent of the C field code.  G1 points are affine
+numpy arrays (12 u64, Montgomery, identity all-zero).
+
+Circuit shape (a dict, see `config3_circuit`): advice and fixed columns, the
+reference's query lists (`ConstraintSystem::advice_queries`/`fixed_queries`,
+in their order), one custom gate (the standard gate
+q_l a + q_r b + q_m a b + q_o c + q_c), a permutation over advice/fixed
+columns split into sets of cs.degree() - 2 columns, and at most one logup
+lookup whose input is one advice column and whose table is one fixed column,
+with an optional fixed selector column.  No instance columns, trashcans or
+simple selectors (every identity is fully evaluated at x, so the
+linearization polynomial is the quotient-limb part alone).
+
+Randomness: the reference draws blinding values from the caller's rng in this
+order: the blinding rows of every advice column (proofs/src/plonk/prover.rs:
+606-617, bf + 1 each), the multiplicity blinds of every lookup (:122-123,
+bf + 1 each), the permutation blinds of every set (:165-167, bf each), the
+logup aggregator blinds of every lookup (:168, bf each).  The quotient-limb
+blinds come from OsRng in the reference (prover.rs:774-785); here they are the
+next qdeg - 1 values of the same stream, a documented deviation that makes
+proofs reproducible.
+"""
+import hashlib
+
+import numpy as np
+
+from . import oracle as O
+
+R = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
+P_BASE = 0x1A0111EA397FE69A4B1BA7B6434BACD764774B84F38512BF6730D2A0F6B0F6241EABFFFEB153FFFFB9FEFFFFFFFFAAAB
+MONT = pow(2, 256, R)
+MONT_INV = pow(MONT, -1, R)
+TRANSCRIPT_KEY = b"Domain separator for transcript"   # transcript/implementors.rs:18
+VK_PERSONAL = b"Halo2-Verify-Key"                     # plonk/mod.rs:244-245
+VK_VERSION = 0x03                                     # plonk/mod.rs:74
+
+
+# ------------------------------------------------------------ field helpers --
+def to_int(a):
+    """Montgomery Fr (4 u64) -> canonical integer."""
+    a = np.asarray(a, np.uint64)
+    v = int(a[0]) | int(a[1]) << 64 | int(a[2]) << 128 | int(a[3]) << 192
+    return v * MONT_INV % R
+
+
+def to_mont(v):
+    """canonical integer -> Montgomery Fr (4 u64)."""
+    m = (v % R) * MONT % R
+    return np.array([(m >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(4)], np.uint64)
+
+
+def from_uniform_bytes(b64):
+    """Fq::from_uniform_bytes (curves/src/bls12_381/fq.rs:712-736): a0*R^2 +
+    a1*R^3 in Montgomery form, i.e. the 512-bit little-endian integer mod r."""
+    return int.from_bytes(b64, "little") % R
+
+
+def inv(v):
+    return pow(v, R - 2, R)
+
+
+def powers(base, count):
+    """utils/arithmetic.rs:266-268."""
+    out, p = [], 1
+    for _ in range(count):
+        out.append(p)
+        p = p * base % R
+    return out
+
+
+# ------------------------------------------------------------ G1 encodings --
+def _fp_canon_int(limbs6):
+    return O.to_int(O.fp_op("to_canonical", np.asarray(limbs6, np.uint64)))
+
+
+def is_identity(aff):
+    return not np.any(np.asarray(aff, np.uint64))
+
+
+def compress(aff):
+    """GroupEncoding::to_bytes of G1 (ZCash compressed, g1.rs:326-334)."""
+    return bytes(O.g1_compress(np.asarray(aff, np.uint64)))
+
+
+def uncompressed(aff):
+    """G1Affine::to_uncompressed (SerdeFormat::RawBytesUnchecked writes of the
+    VK hash, plonk/mod.rs:252-262; g1.rs:486-488): x, y big-endian, 0x40 flag
+    for the identity."""
+    if is_identity(aff):
+        return bytes([0x40]) + bytes(95)
+    x, y = _fp_canon_int(aff[:6]), _fp_canon_int(aff[6:])
+    return x.to_bytes(48, "big") + y.to_bytes(48, "big")
+
+
+def pt_mul(aff, s):
+    if is_identity(aff) or s % R == 0:
+        return np.zeros(12, np.uint64)
+    return O.g1_mul(np.asarray(aff, np.uint64), to_mont(s))
+
+
+def pt_add(a, b):
+    return O.g1_to_affine(O.g1_jac_add(O.g1_from_affine(a), O.g1_from_affine(b)))
+
+
+def pt_lincomb(points, scalars):
+    acc = np.zeros(12, np.uint64)
+    for p, s in zip(points, scalars):
+        acc = pt_add(acc, pt_mul(p, s))
+    return acc
+
+
+# ------------------------------------------------------------- transcript --
+class Transcript:
+    """CircuitTranscript<Blake2bState> (transcript/mod.rs:83-150,
+    implementors.rs:13-30): one keyed Blake2b-512 state; absorbing prefixes a
+    1 byte, squeezing absorbs a 0 byte and reads the digest without resetting
+    the state; G1 points go in compressed (48 bytes), scalars as 32-byte
+    little-endian canonical values (implementors.rs:138-175); a challenge is
+    the 64-byte digest reduced mod r (implementors.rs:177-185)."""
+
+    def __init__(self, proof=b""):
+        self.h = hashlib.blake2b(digest_size=64, key=TRANSCRIPT_KEY)
+        self.proof = bytearray()
+        self.buf, self.pos = bytes(proof), 0
+
+    def common_bytes(self, b):
+        self.h.update(b"\x01" + b)
+
+    def common_fr(self, v):
+        self.common_bytes((v % R).to_bytes(32, "little"))
+
+    def write_fr(self, v):
+        b = (v % R).to_bytes(32, "little")
+        self.common_bytes(b)
+        self.proof += b
+
+    def write_point(self, aff):
+        b = compress(aff)
+        self.common_bytes(b)
+        self.proof += b
+
+    def squeeze(self):
+        self.h.update(b"\x00")
+        return from_uniform_bytes(self.h.digest())
+
+    # verifier side (Transcript::read, mod.rs:128-133)
+    def read_fr(self):
+        b = self.buf[self.pos:self.pos + 32]
+        if len(b) != 32:
+            raise ValueError("proof too short")
+        v = int.from_bytes(b, "little")
+        if v >= R:
+            raise ValueError("non-canonical scalar")
+        self.pos += 32
+        self.common_bytes(b)
+        return v
+
+    def read_point(self):
+        b = self.buf[self.pos:self.pos + 48]
+        if len(b) != 48:
+            raise ValueError("proof too short")
+        st, aff = O.g1_decompress(b, True)
+        if st != 0:
+            raise ValueError(f"invalid point encoding ({st})")
+        self.pos += 48
+        self.common_bytes(b)
+        return aff
+
+    def assert_empty(self):
+        if self.pos != len(self.buf):
+            raise ValueError("trailing bytes")
+
+
+# ---------------------------------------------------------------- circuit --
+def blinding_factors(circuit):
+    """ConstraintSystem::blinding_factors (plonk/circuit.rs:2203-2245) for this
+    shape: max(3, max advice queries per column) + helper chunks + 3."""
+    per_col = {}
+    for col, _ in circuit["advice_queries"]:
+        per_col[col] = per_col.get(col, 0) + 1
+    f = max(3, max(per_col.values(), default=1))
+    return f + len(circuit["lookups"]) + 3
+
+
+def n_perm_sets(circuit):
+    chunk = circuit["degree"] - 2
+    return (len(circuit["perm_cols"]) + chunk - 1) // chunk
+
+
+def blind_count(circuit):
+    """Number of rng values one proof draws (the order in the module doc)."""
+    bf = blinding_factors(circuit)
+    qdeg = circuit["degree"] - 1
+    L = len(circuit["lookups"])
+    return circuit["n_advice"] * (bf + 1) + L * (bf + 1) + n_perm_sets(circuit) * bf + L * bf + (qdeg - 1)
+
+
+def query_index(queries, col, rot=0):
+    """ConstraintSystem::get_any_query_index for the column at rotation rot."""
+    for i, (c, r) in enumerate(queries):
+        if c == col and r == rot:
+            return i
+    raise KeyError((col, rot))
+
+
+def config3_circuit(k):
+    """The single-proof configuration: advice a, b, c, fixed q_l, q_r, q_m,
+    q_o, q_c, the lookup table and the lookup selector; the standard gate;
+    the permutation over a, b, c; one lookup of a into the table; degree 5
+    (set_minimum_degree(5), proofs/benches/plonk.rs:191)."""
+    return {
+        "k": k, "degree": 5, "n_advice": 3, "n_fixed": 7,
+        "advice_queries": [(0, 0), (1, 0), (2, 0)],
+        "fixed_queries": [(i, 0) for i in range(7)],
+        "gate_fixed": [0, 1, 2, 3, 4], "gate_advice": [0, 1, 2],
+        "perm_cols": [(0, 0), (0, 1), (0, 2)],          # (0 advice | 1 fixed, column)
+        "lookups": [{"input": 0, "table": 5, "selector": 6}],
+    }
+
+
+def config3_instance(k, seed, table_bits=16, copy_fraction=0.10):
+    """Seeded fixed columns, copy cycles and a satisfying witness for
+    config3_circuit: selectors uniform (q_o non-zero) on the usable rows and
+    zero on the rest; the table holds 0 .. 2^table_bits - 1 (capped at the
+    usable rows) padded with zeros; a is a table value, b uniform, c solves the
+    gate; copy cycles over copy_fraction of the a and b cells of usable rows,
+    each cycle carrying one table value.  Returns (fixed_values, mapping,
+    advice_values) with mapping[c][r] = (column, row) of the next cell of
+    (c, r)'s cycle (identity elsewhere), the permutation build_pk takes
+    (permutation/keygen.rs:138-185)."""
+    c = config3_circuit(k)
+    n = 1 << k
+    bf = blinding_factors(c)
+    u = n - bf - 1
+    rng = np.random.default_rng(seed)
+    rows = min(1 << table_bits, u)
+    col = lambda s: O.rand_fr(seed * 97 + s, n)
+    q = [col(i) for i in range(5)]
+    for qi in q:
+        qi[u:] = 0
+    one = O.fr_const(0)
+    # q_o non-zero on usable rows (a zero draw has negligible probability; replace it anyway)
+    for i in range(u):
+        if not np.any(q[3][i]):
+            q[3][i] = one
+    table = np.zeros((n, 4), np.uint64)
+    table[:rows] = np.stack([to_mont(v) for v in range(rows)]) if rows else table[:0]
+    sel = np.zeros((n, 4), np.uint64)
+    sel[:u] = one
+    fixed = q + [table, sel]
+    a_int = rng.integers(0, rows, size=u)
+    a = np.zeros((n, 4), np.uint64)
+    b = col(10)
+    b[u:] = 0
+    # copy cycles among the a and b cells of usable rows
+    mapping = np.zeros((3, n, 2), np.uint32)
+    for ci in range(3):
+        mapping[ci, :, 0] = ci
+        mapping[ci, :, 1] = np.arange(n, dtype=np.uint32)
+    cells = rng.permutation(2 * u)[: int(copy_fraction * 2 * u)]
+    pos = 0
+    cyc_vals = {}
+    while pos + 1 < len(cells):
+        ln = int(rng.integers(2, 5))
+        cyc = cells[pos:pos + ln]
+        pos += ln
+        if len(cyc) < 2:
+            break
+        v = int(rng.integers(0, rows))
+        for t, cell in enumerate(cyc):
+            nxt = cyc[(t + 1) % len(cyc)]
+            cc, rr = divmod(int(cell), u)
+            mapping[cc, rr] = divmod(int(nxt), u)
+            cyc_vals[(cc, rr)] = v
+    for (cc, rr), v in cyc_vals.items():
+        if cc == 0:
+            a_int[rr] = v
+        else:
+            b[rr] = to_mont(v)
+    a[:u] = np.stack([to_mont(int(v)) for v in a_int])
+    # c = -(q_l a + q_r b + q_m a b + q_c) / q_o on usable rows
+    t = O.poly_inner_product([_hadamard(q[0], a), _hadamard(q[1], b), _hadamard(q[2], _hadamard(a, b)), q[4]],
+                             [one] * 4)
+    cc_col = _hadamard(O.poly_inner_product([t], [to_mont(R - 1)]), O.batch_invert(q[3]))
+    cc_col[u:] = 0
+    return fixed, mapping, [a, b, cc_col]
+
+
+def _hadamard(x, y):
+    """Element-wise product of two Fr arrays (through the C oracle)."""
+    return O.fr_mul_vec(x, y)
+
+
+# ------------------------------------------------------------- polynomials --
+def delta(a, order):
+    """Polynomial::to_delta / to_double_delta (proofs/src/poly/mod.rs:297-336)."""
+    a = np.ascontiguousarray(a, np.uint64)
+    one, m1 = O.fr_const(0), to_mont(R - 1)
+    out = a.copy()
+    shifted = np.zeros_like(a)
+    shifted[1:] = a[:-1]
+    out = O.poly_inner_product([a, shifted], [one, m1])
+    if order == 2:
+        s2 = np.zeros_like(out)
+        s2[1:] = out[:-1]
+        out = O.poly_inner_product([out, s2], [one, m1])
+    return out
+
+
+def commit(scalars, bases):
+    """KZGCommitmentScheme::commit_many's msm_specific over bases[..len]
+    (kzg/mod.rs:82-108)."""
+    scalars = np.ascontiguousarray(scalars, np.uint64)
+    return O.msm_specific(scalars, np.ascontiguousarray(bases[: scalars.shape[0]], np.uint64))
+
+
+def scale(poly, s):
+    return O.poly_inner_product([poly], [to_mont(s)])
+
+
+def eval_at(poly, point):
+    return to_int(O.eval_polynomial(poly, to_mont(point)))
+
+
+def compute_multiplicities(selector, inputs, table, usable_rows, blinds):
+    """logup/prover.rs:412-477: per table row, the number of selected input
+    rows holding its value divided by the value's count in the table (active
+    rows only); blinding rows take the blinding values.  Raises when a
+    selected input value is not in the table."""
+    n = table.shape[0]
+    vt = np.dtype((np.void, 32))
+    tab = np.ascontiguousarray(table[:usable_rows]).view(vt).ravel()
+    uniq, inv_idx, counts = np.unique(tab, return_inverse=True, return_counts=True)
+    incount = np.zeros(len(uniq), np.int64)
+    sel = np.any(selector[:usable_rows] != 0, axis=1)
+    for col in inputs:
+        iv = np.ascontiguousarray(col[:usable_rows][sel]).view(vt).ravel()
+        pos = np.searchsorted(uniq, iv)
+        ok = (pos < len(uniq))
+        ok[ok] = uniq[pos[ok]] == iv[ok]
+        if not np.all(ok):
+            raise ValueError("input value not found in lookup table")
+        incount += np.bincount(pos, minlength=len(uniq))
+    vals = np.stack([to_mont(int(incount[i]) * inv(int(counts[i])) % R) for i in range(len(uniq))])
+    m = np.zeros((n, 4), np.uint64)
+    m[:usable_rows] = vals[inv_idx.ravel()]
+    m[usable_rows:] = np.stack([to_mont(v) for v in blinds])
+    return m
+
+
+# ------------------------------------------------------------------ keygen --
+class Key:
+    pass
+
+
+def keygen(circuit, fixed_values, mapping, srs, pinned_repr):
+    """keygen_vk / keygen_pk for this shape (plonk/keygen.rs:227-359):
+    fixed polynomials and cosets, the permutation polynomials of build_pk
+    (permutation/keygen.rs:138-185: cell (c, r) gets delta^c' omega^r' of the
+    cell it maps to), their polynomials and cosets, l0, l_last and
+    l_active_row (keygen.rs:361-404), the fixed and permutation commitments
+    and the VK's transcript_repr (plonk/mod.rs:227-284).  srs: dict with the
+    affine bases g, lagrange, delta, double_delta (n points each).
+    pinned_repr: the bytes of format!("{:?}", domain.pinned()) followed by
+    format!("{:?}", cs.pinned()), which this restatement cannot produce (they
+    are Rust Debug strings) and takes as given."""
+    key = Key()
+    k = circuit["k"]
+    n = 1 << k
+    dom = O.Domain(circuit["degree"], k)
+    bf = blinding_factors(circuit)
+    key.circuit, key.dom, key.srs, key.n, key.bf = circuit, dom, srs, n, bf
+    key.u = n - bf - 1
+    key.qdeg = circuit["degree"] - 1
+    key.omega, key.omega_inv = to_int(dom.get(0)), to_int(dom.get(1))
+    key.fixed_values = [np.ascontiguousarray(v, np.uint64) for v in fixed_values]
+    key.fixed_polys = [dom.lagrange_to_coeff(v) for v in key.fixed_values]
+    key.fixed_cosets = [dom.coeff_to_extended(p) for p in key.fixed_polys]
+    # permutation polynomials: deltaomega[c][r] = delta^c * omega^r
+    x_poly = np.zeros((n, 4), np.uint64)
+    x_poly[1] = O.fr_const(0)
+    omega_pows = dom.coeff_to_lagrange(x_poly)          # omega^r, r = 0..n-1
+    P = len(circuit["perm_cols"])
+    dlt = to_int(O.fr_const(5))
+    deltaomega = np.stack([scale(omega_pows, pow(dlt, c, R)) for c in range(P)])
+    if mapping is None:
+        mapping = np.zeros((P, n, 2), np.uint32)
+        for c in range(P):
+            mapping[c, :, 0] = c
+            mapping[c, :, 1] = np.arange(n)
+    key.perm_values = [np.ascontiguousarray(deltaomega[mapping[c, :, 0], mapping[c, :, 1]]) for c in range(P)]
+    key.perm_polys = [dom.lagrange_to_coeff(v) for v in key.perm_values]
+    key.perm_cosets = [dom.coeff_to_extended(p) for p in key.perm_polys]
+    # l0, l_last, l_active_row
+    one = O.fr_const(0)
+    unit = lambda rows: _unit(n, rows)
+    l0 = dom.coeff_to_extended(dom.lagrange_to_coeff(unit([0])))
+    l_blind = dom.coeff_to_extended(dom.lagrange_to_coeff(unit(range(n - bf, n))))
+    l_last = dom.coeff_to_extended(dom.lagrange_to_coeff(unit([n - bf - 1])))
+    ones = np.tile(one, (l0.shape[0], 1))
+    l_active = O.poly_inner_product([ones, l_last, l_blind], [one, to_mont(R - 1), to_mont(R - 1)])
+    key.l0, key.l_last, key.l_active = l0, l_last, l_active
+    # commitments and the VK hash
+    key.fixed_coms = [commit(v, srs["lagrange"]) for v in key.fixed_values]
+    key.perm_coms = [commit(v, srs["lagrange"]) for v in key.perm_values]
+    key.repr = vk_transcript_repr(k, key.fixed_coms, key.perm_coms, pinned_repr)
+    # lookup table index of the multiplicities
+    return key
+
+
+def _unit(n, rows):
+    a = np.zeros((n, 4), np.uint64)
+    for r in rows:
+        a[r] = O.fr_const(0)
+    return a
+
+
+def vk_transcript_repr(k, fixed_coms, perm_coms, pinned_repr):
+    """VerifyingKey::from_parts (plonk/mod.rs:227-284): Blake2b-512 with the
+    personalisation "Halo2-Verify-Key" over the version byte, k, the fixed
+    and permutation commitments (uncompressed, each list prefixed by its u32
+    length) and the pinned Debug strings, then from_uniform_bytes."""
+    buf = bytearray([VK_VERSION, k]) + len(fixed_coms).to_bytes(4, "little")
+    for c in fixed_coms:
+        buf += uncompressed(c)
+    buf += len(perm_coms).to_bytes(4, "little")
+    for c in perm_coms:
+        buf += uncompressed(c)
+    buf += pinned_repr
+    return from_uniform_bytes(hashlib.blake2b(bytes(buf), digest_size=64, person=VK_PERSONAL).digest())
+
+
+# ------------------------------------------------------- shared identities --
+def l_i_range(key, x, xn, rotations):
+    """EvaluationDomain::l_i_range (domain.rs:487-512): l_i(x) =
+    omega^i (x^n - 1) / (n (x - omega^i))."""
+    n = key.n
+    out = []
+    for rot in rotations:
+        wi = pow(key.omega, rot, R) if rot >= 0 else pow(key.omega_inv, -rot, R)
+        out.append(wi * (xn - 1) % R * inv(n) % R * inv((x - wi) % R) % R)
+    return out
+
+
+def rotate(key, x, rot):
+    """EvaluationDomain::rotate_omega (domain.rs:449-457)."""
+    return x * (pow(key.omega, rot, R) if rot >= 0 else pow(key.omega_inv, -rot, R)) % R
+
+
+def identities(key, ev, ch):
+    """partially_evaluate_identities (plonk/mod.rs:519-608) with every
+    identity fully evaluated: the gate polynomials, then the permutation
+    expressions (permutation.rs:195-290), then each lookup's boundary, helper
+    and accumulator expressions (logup.rs:405-485).  ev: evaluations by name;
+    ch: challenges.  Returns the list of identity values."""
+    c = key.circuit
+    x, xn, beta, gamma, theta = ch["x"], ch["xn"], ch["beta"], ch["gamma"], ch["theta"]
+    bf = key.bf
+    l_evals = l_i_range(key, x, xn, range(-(bf + 1), 1))
+    l_last, l_blind, l_0 = l_evals[0], sum(l_evals[1:1 + bf]) % R, l_evals[1 + bf]
+    adv, fix = ev["advice"], ev["fixed"]
+    aq = lambda col: adv[query_index(c["advice_queries"], col)]
+    fq = lambda col: fix[query_index(c["fixed_queries"], col)]
+    gf, ga = c["gate_fixed"], c["gate_advice"]
+    ql, qr, qm, qo, qc = (fq(i) for i in gf)
+    a, b, cc = (aq(i) for i in ga)
+    out = [(ql * a + qr * b + qm * a * b + qo * cc + qc) % R]
+    # permutation
+    sets = ev["perm_sets"]
+    chunk = c["degree"] - 2
+    if sets:
+        out.append(l_0 * (1 - sets[0][0]) % R)
+        out.append((sets[-1][0] * sets[-1][0] - sets[-1][0]) * l_last % R)
+        for i in range(1, len(sets)):
+            out.append((sets[i][0] - sets[i - 1][2]) * l_0 % R)
+        dlt = to_int(O.fr_const(5))
+        for si, s in enumerate(sets):
+            cols = c["perm_cols"][si * chunk:(si + 1) * chunk]
+            sig = ev["perm_common"][si * chunk:(si + 1) * chunk]
+            left = s[1]
+            for (kind, ci), se in zip(cols, sig):
+                e = aq(ci) if kind == 0 else fq(ci)
+                left = left * (e + beta * se + gamma) % R
+            right = s[0]
+            cur = beta * x % R * pow(dlt, si * chunk, R) % R
+            for kind, ci in cols:
+                e = aq(ci) if kind == 0 else fq(ci)
+                right = right * (e + cur + gamma) % R
+                cur = cur * dlt % R
+            out.append((left - right) * (1 - (l_last + l_blind)) % R)
+    # lookups
+    for li, lk in enumerate(c["lookups"]):
+        m, h, Z, Zn = ev["lookups"][li]
+        f = aq(lk["input"])
+        table = fq(lk["table"])
+        sel = fq(lk["selector"]) if lk["selector"] is not None else 1
+        out.append((l_0 + l_last) * Z % R)
+        fb = (f + beta) % R
+        out.append((h * fb - 1) % R)              # one input: product f+beta, sum of partial products 1
+        out.append(((Zn - Z - sel * h) * (table + beta) + m) * (1 - (l_last + l_blind)) % R)
+    return [v % R for v in out]
+
+
+def horner(values, y):
+    acc = 0
+    for v in values:
+        acc = (acc * y + v) % R
+    return acc
+
+
+# ---------------------------------------------------------- multi-open sets --
+def intermediate_sets(queries):
+    """construct_intermediate_sets (kzg/utils.rs:46-140): queries
+    [(label, point)] -> (commitment labels in first-seen order with their set
+    index, point sets as lists of points ordered by first-seen point index)."""
+    point_index = {}
+    com = []          # [label, [point indices]]
+    for label, pt in queries:
+        pi = point_index.setdefault(pt, len(point_index))
+        for entry in com:
+            if entry[0] == label:
+                if pi in entry[1]:
+                    raise ValueError("duplicated query")
+                entry[1].append(pi)
+                break
+        else:
+            com.append([label, [pi]])
+    set_index = {}
+    labels = []
+    for label, pis in com:
+        key = tuple(sorted(pis))
+        si = set_index.setdefault(key, len(set_index))
+        labels.append((label, si, key))
+    inv_point = {i: p for p, i in point_index.items()}
+    point_sets = [None] * len(set_index)
+    for key, si in set_index.items():
+        point_sets[si] = [inv_point[i] for i in key]
+    return labels, point_sets, point_index
+
+
+# ---------------------------------------------------------------- prover --
+def create_proof(key, advice, blinds):
+    """create_proof (plonk/prover.rs:432-473): compute_trace, then
+    finalise_proof with the KZG multi_open (kzg/mod.rs:110-289).  advice:
+    Lagrange values of every advice column (rows at and after the usable
+    rows are replaced by blinding values); blinds: integers in the draw order
+    of the module doc.  Returns the proof bytes."""
+    c, dom, srs = key.circuit, key.dom, key.srs
+    n, u, bf, qdeg = key.n, key.u, key.bf, key.qdeg
+    blinds = list(blinds)
+    if len(blinds) != blind_count(c):
+        raise ValueError("wrong number of blinding values")
+    bl = iter(blinds)
+    take = lambda m: [next(bl) for _ in range(m)]
+    tr = Transcript()
+    tr.common_fr(key.repr)                                    # vk.hash_into (prover.rs:101)
+    # parse_advices (prover.rs:541-632)
+    adv = []
+    for col in advice:
+        a = np.ascontiguousarray(col, np.uint64).copy()
+        a[u:] = np.stack([to_mont(v) for v in take(bf + 1)])
+        adv.append(a)
+    for a in adv:
+        tr.write_point(commit(a, srs["lagrange"]))
+    theta = tr.squeeze()
+    # multiplicities (logup/prover.rs:95-184), committed in delta form
+    ms = []
+    for lk in c["lookups"]:
+        sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
+        ms.append(compute_multiplicities(sel, [adv[lk["input"]]], key.fixed_values[lk["table"]], u, take(bf + 1)))
+    for m in ms:
+        tr.write_point(commit(delta(m, 1), srs["delta"]))
+    beta = tr.squeeze()
+    gamma = tr.squeeze()
+    S = n_perm_sets(c)
+    perm_bl = [take(bf) for _ in range(S)]
+    log_bl = [take(bf) for _ in c["lookups"]]
+    # permutation products (permutation/prover.rs:81-255) and logup helper / aggregator
+    pvals = [adv[ci] if kind == 0 else key.fixed_values[ci] for kind, ci in c["perm_cols"]]
+    zs = O.permutation_z(pvals, key.perm_values, c["degree"] - 2, c["k"], to_mont(key.omega), to_mont(beta),
+                         to_mont(gamma), bf, np.stack([np.stack([to_mont(v) for v in b]) for b in perm_bl]))
+    hs, Zs = [], []
+    for li, lk in enumerate(c["lookups"]):
+        sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
+        (h,), Z = O.logup([[adv[lk["input"]]]], key.fixed_values[lk["table"]], sel, ms[li], to_mont(beta), bf,
+                          np.stack([to_mont(v) for v in log_bl[li]]))
+        hs.append(h)
+        Zs.append(Z)
+    for z in zs:
+        tr.write_point(commit(delta(z, 1), srs["delta"]))
+    for h, Z in zip(hs, Zs):
+        tr.write_point(commit(h, srs["lagrange"]))
+        tr.write_point(commit(delta(Z, 2), srs["double_delta"]))
+    trash = tr.squeeze()
+    y = tr.squeeze()
+    # coefficient forms and cosets
+    adv_c = [dom.lagrange_to_coeff(a) for a in adv]
+    z_c = [dom.lagrange_to_coeff(z) for z in zs]
+    m_c = [dom.lagrange_to_coeff(m) for m in ms]
+    h_c = [dom.lagrange_to_coeff(h) for h in hs]
+    Z_c = [dom.lagrange_to_coeff(Z) for Z in Zs]
+    ext = lambda p: dom.coeff_to_extended(p)
+    hpoly = quotient(key, [ext(p) for p in adv_c], [ext(p) for p in z_c], [ext(p) for p in m_c],
+                     [ext(p) for p in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta)
+    hcoeff = dom.extended_to_coeff(hpoly)[: (n - 1) * qdeg]
+    limbs = [np.concatenate([hcoeff[i * (n - 1):(i + 1) * (n - 1)], np.zeros((1, 4), np.uint64)]) for i in range(qdeg)]
+    for i, t in enumerate(take(qdeg - 1), start=1):         # blind_quotient_limbs (prover.rs:774-785)
+        limbs[i - 1][n - 1] = to_mont(t)
+        limbs[i][0] = to_mont(to_int(limbs[i][0]) - t)
+    for lb in limbs:
+        tr.write_point(commit(lb, srs["g"]))
+    x = tr.squeeze()
+    xn = pow(x, n, R)
+    # evaluations (prover.rs:798-868, permutation/prover.rs:270-335, logup/prover.rs:318-352)
+    ev = {"advice": [eval_at(adv_c[col], rotate(key, x, rot)) for col, rot in c["advice_queries"]],
+          "fixed": [eval_at(key.fixed_polys[col], rotate(key, x, rot)) for col, rot in c["fixed_queries"]]}
+    for v in ev["advice"] + ev["fixed"]:
+        tr.write_fr(v)
+    ev["perm_common"] = [eval_at(p, x) for p in key.perm_polys]
+    for v in ev["perm_common"]:
+        tr.write_fr(v)
+    x_next, x_last = rotate(key, x, 1), rotate(key, x, -(bf + 1))
+    sets = []
+    for si, z in enumerate(z_c):
+        s = [eval_at(z, x), eval_at(z, x_next), eval_at(z, x_last) if si < S - 1 else None]
+        sets.append(s)
+        tr.write_fr(s[0])
+        tr.write_fr(s[1])
+        if s[2] is not None:
+            tr.write_fr(s[2])
+    ev["perm_sets"] = sets
+    ev["lookups"] = []
+    for li in range(len(c["lookups"])):
+        e = (eval_at(m_c[li], x), eval_at(h_c[li], x), eval_at(Z_c[li], x), eval_at(Z_c[li], x_next))
+        ev["lookups"].append(e)
+        for v in e:
+            tr.write_fr(v)
+    # linearization (linearization/prover.rs:41-86): every identity is a
+    # constant, so L'(X) = -sum_i (x^n - 1) (x^(n-1))^i h_i(X)
+    sf = pow(x, n - 1, R)
+    lin = O.poly_inner_product(limbs, [to_mont(-(xn - 1) * pow(sf, i, R)) for i in range(qdeg)])
+    # queries (prover.rs:871-933)
+    q = []
+    for col, rot in c["advice_queries"]:
+        q.append((("advice", col), rotate(key, x, rot), adv_c[col]))
+    for si, z in enumerate(z_c):
+        q.append((("perm", si), x, z))
+        q.append((("perm", si), x_next, z))
+    for si in reversed(range(S - 1)):
+        q.append((("perm", si), x_last, z_c[si]))
+    for li in range(len(c["lookups"])):
+        q.append((("m", li), x, m_c[li]))
+        q.append((("h", li, 0), x, h_c[li]))
+        q.append((("Z", li), x, Z_c[li]))
+        q.append((("Z", li), x_next, Z_c[li]))
+    for col, rot in c["fixed_queries"]:
+        q.append((("fixed", col), rotate(key, x, rot), key.fixed_polys[col]))
+    for i, p in enumerate(key.perm_polys):
+        q.append((("perm_fixed", i), x, p))
+    q.append((("lin",), x, lin))
+    multi_open(key, tr, q)
+    return bytes(tr.proof)
+
+
+def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta):
+    """compute_nu_poly + divide_by_vanishing_poly (prover.rs:634-715) through
+    the C oracle's evaluate_numerator restatement."""
+    c, dom = key.circuit, key.dom
+    keep = []
+
+    def parr(items):
+        arr = (O.ctypes.c_void_p * max(1, len(items)))(*[a.ctypes.data for a in items])
+        keep.append(arr)
+        return O.ctypes.cast(arr, O.ctypes.POINTER(O.ctypes.c_void_p))
+
+    def u32(items):
+        arr = (O.ctypes.c_uint32 * max(1, len(items)))(*items)
+        keep.append(arr)
+        return O.ctypes.cast(arr, O.ctypes.POINTER(O.ctypes.c_uint32))
+
+    d = O.QuotientDesc()
+    d.k, d.extended_k = c["k"], dom.extended_k
+    d.advice, d.n_advice = parr(adv_e), len(adv_e)
+    d.fixed, d.n_fixed = parr(key.fixed_cosets), len(key.fixed_cosets)
+    d.gate_fixed[:] = c["gate_fixed"]
+    d.gate_advice[:] = c["gate_advice"]
+    d.n_perm_cols = len(c["perm_cols"])
+    d.perm_col_kind = u32([kind for kind, _ in c["perm_cols"]])
+    d.perm_col_index = u32([ci for _, ci in c["perm_cols"]])
+    d.perm_sigma = parr(key.perm_cosets)
+    d.n_perm_sets, d.perm_z = len(z_e), parr(z_e)
+    d.chunk_len, d.blinding_factors = c["degree"] - 2, key.bf
+    if c["lookups"]:
+        lk = c["lookups"][0]
+        d.has_lookup = 1
+        d.lookup_input_advice, d.lookup_table_fixed = lk["input"], lk["table"]
+        d.lookup_selector_fixed = -1 if lk["selector"] is None else lk["selector"]
+        d.lookup_h, d.lookup_z, d.lookup_m = h_e[0].ctypes.data, Z_e[0].ctypes.data, m_e[0].ctypes.data
+    d.l0, d.l_last, d.l_active = key.l0.ctypes.data, key.l_last.ctypes.data, key.l_active.ctypes.data
+    for name, v in (("y", y), ("beta", beta), ("gamma", gamma), ("theta", theta)):
+        getattr(d, name)[:] = [int(t) for t in to_mont(v)]
+    d.extended_omega[:] = [int(t) for t in dom.get(2)]
+    d.g_coset[:] = [int(t) for t in dom.get(3)]
+    keep.extend([adv_e, z_e, m_e, h_e, Z_e])
+    return dom.quotient_eval(d, True)
+
+
+def multi_open(key, tr, queries):
+    """KZGCommitmentScheme::multi_open (kzg/mod.rs:110-289) without the
+    fewer-point-sets and truncated-challenges features."""
+    srs = key.srs
+    x1 = tr.squeeze()
+    x2 = tr.squeeze()
+    label_poly = {}
+    for label, _, poly in queries:
+        label_poly[label] = poly
+    labels, point_sets, _ = intermediate_sets([(lb, pt) for lb, pt, _ in queries])
+    per_set = [[] for _ in point_sets]
+    for label, si, _ in labels:
+        per_set[si].append(label_poly[label])
+    q_polys = [O.poly_inner_product(ps, [to_mont(v) for v in powers(x1, len(ps))]) for ps in per_set]
+    order = sorted(range(len(point_sets)), key=lambda i: (len(point_sets[i]), i))
+    q_polys = [q_polys[i] for i in order]
+    point_sets = [point_sets[i] for i in order]
+    f_polys = []
+    for pts, qp in zip(point_sets, q_polys):
+        p = qp
+        for pt in pts:
+            p = O.kate_division(p, to_mont(pt))
+        f_polys.append(p)
+    f = O.poly_inner_product(f_polys, [to_mont(v) for v in powers(x2, len(f_polys))])
+    tr.write_point(commit(f, srs["g"]))
+    x3 = tr.squeeze()
+    for qp in q_polys:
+        tr.write_fr(eval_at(qp, x3))
+    x4 = tr.squeeze()
+    final = O.poly_inner_product(q_polys + [f], [to_mont(v) for v in powers(x4, len(q_polys) + 1)])
+    v = eval_at(final, x3)
+    final = final.copy()
+    final[0] = to_mont(to_int(final[0]) - v)
+    tr.write_point(commit(O.kate_division(final, to_mont(x3)), srs["g"]))
+
+
+# --------------------------------------------------------------- verifier --
+def verify(key, proof, s_trapdoor):
+    """prepare (plonk/verifier.rs:371-407: parse_trace, then
+    verify_algebraic_constraints) and KZGCommitmentScheme::multi_prepare
+    (kzg/mod.rs:291-491), finished by DualMSM::check (kzg/msm.rs:294-310)
+    with the pairing e(pi, [s]G2) = e(C - vG + x3 pi, G2) replaced by the
+    equivalent G1 check [s]pi = C - vG + x3 pi for the test setup's known s.
+    Returns True or False; a malformed proof is False."""
+    try:
+        return _verify(key, proof, s_trapdoor)
+    except ValueError:
+        return False
+
+
+def _verify(key, proof, s):
+    c = key.circuit
+    n, bf, qdeg = key.n, key.bf, key.qdeg
+    S = n_perm_sets(c)
+    L = len(c["lookups"])
+    tr = Transcript(proof)
+    tr.common_fr(key.repr)
+    adv_coms = [tr.read_point() for _ in range(c["n_advice"])]
+    theta = tr.squeeze()
+    m_coms = [tr.read_point() for _ in range(L)]
+    beta = tr.squeeze()
+    gamma = tr.squeeze()
+    z_coms = [tr.read_point() for _ in range(S)]
+    hz_coms = [(tr.read_point(), tr.read_point()) for _ in range(L)]
+    tr.squeeze()                                   # trash challenge (no trashcans)
+    y = tr.squeeze()
+    limb_coms = [tr.read_point() for _ in range(qdeg)]
+    x = tr.squeeze()
+    sf = pow(x, n - 1, R)
+    xn = sf * x % R
+    ev = {"advice": [tr.read_fr() for _ in c["advice_queries"]],
+          "fixed": [tr.read_fr() for _ in c["fixed_queries"]]}
+    ev["perm_common"] = [tr.read_fr() for _ in c["perm_cols"]]
+    sets = []
+    for si in range(S):
+        z0, z1 = tr.read_fr(), tr.read_fr()
+        sets.append([z0, z1, tr.read_fr() if si < S - 1 else None])
+    ev["perm_sets"] = sets
+    ev["lookups"] = [tuple(tr.read_fr() for _ in range(4)) for _ in range(L)]
+    ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta}
+    const = horner(identities(key, ev, ch), y)
+    # compute_linearization_commitment (linearization/verifier.rs:27-78)
+    lin_com = pt_lincomb(limb_coms, [(1 - xn) * pow(sf, i, R) for i in range(qdeg)])
+    lin_eval = -const % R
+    x_next, x_last = rotate(key, x, 1), rotate(key, x, -(bf + 1))
+    q = []   # (label, point, commitment, eval)
+    for qi, (col, rot) in enumerate(c["advice_queries"]):
+        q.append((("advice", col), rotate(key, x, rot), adv_coms[col], ev["advice"][qi]))
+    for si in range(S):
+        q.append((("perm", si), x, z_coms[si], sets[si][0]))
+        q.append((("perm", si), x_next, z_coms[si], sets[si][1]))
+    for si in reversed(range(S - 1)):
+        q.append((("perm", si), x_last, z_coms[si], sets[si][2]))
+    for li in range(L):
+        m, h, Z, Zn = ev["lookups"][li]
+        q.append((("m", li), x, m_coms[li], m))
+        q.append((("h", li, 0), x, hz_coms[li][0], h))
+        q.append((("Z", li), x, hz_coms[li][1], Z))
+        q.append((("Z", li), x_next, hz_coms[li][1], Zn))
+    for qi, (col, rot) in enumerate(c["fixed_queries"]):
+        q.append((("fixed", col), rotate(key, x, rot), key.fixed_coms[col], ev["fixed"][qi]))
+    for i, com in enumerate(key.perm_coms):
+        q.append((("perm_fixed", i), x, com, ev["perm_common"][i]))
+    q.append((("lin",), x, lin_com, lin_eval))
+    # multi_prepare
+    x1 = tr.squeeze()
+    x2 = tr.squeeze()
+    label_com = {lb: com for lb, _, com, _ in q}
+    labels, point_sets, point_index = intermediate_sets([(lb, pt) for lb, pt, _, _ in q])
+    evals_of = {}
+    for lb, pt, _, e in q:
+        evals_of.setdefault(lb, {})[pt] = e
+    q_coms = [[] for _ in point_sets]
+    q_evals = [[] for _ in point_sets]
+    for label, si, _ in labels:
+        q_coms[si].append(label_com[label])
+        q_evals[si].append([evals_of[label][pt] for pt in point_sets[si]])
+    nb = max(len(v) for v in q_coms)
+    px1 = powers(x1, nb)
+    q_com = [pt_lincomb(coms, px1) for coms in q_coms]
+    q_ev = [[sum(px1[j] * ev_j[i] for j, ev_j in enumerate(evs)) % R for i in range(len(evs[0]))] for evs in q_evals]
+    order = sorted(range(len(point_sets)), key=lambda i: (len(point_sets[i]), i))
+    q_com = [q_com[i] for i in order]
+    q_ev = [q_ev[i] for i in order]
+    point_sets = [point_sets[i] for i in order]
+    f_com = tr.read_point()
+    x3 = tr.squeeze()
+    q_x3 = [tr.read_fr() for _ in point_sets]
+    f_eval = 0
+    for pts, evs, pe in reversed(list(zip(point_sets, q_ev, q_x3))):
+        r_eval = lagrange_eval(pts, evs, x3)
+        den = 1
+        for p in pts:
+            den = den * (x3 - p) % R
+        f_eval = (f_eval * x2 + (pe - r_eval) * inv(den)) % R
+    x4 = tr.squeeze()
+    p4 = powers(x4, len(q_com) + 1)
+    final_com = pt_lincomb(q_com + [f_com], p4)
+    v = sum(a * b for a, b in zip(q_x3 + [f_eval], p4)) % R
+    pi = tr.read_point()
+    tr.assert_empty()
+    gen = O.g1_generator()
+    right = pt_add(pt_add(final_com, pt_mul(gen, -v % R)), pt_mul(pi, x3))
+    return bool(np.array_equal(pt_mul(pi, s), right))
+
+
+def lagrange_eval(points, evals, at):
+    """The interpolating polynomial of (points, evals) evaluated at `at`
+    (lagrange_interpolate, utils/arithmetic.rs:183-245, then eval_polynomial)."""
+    total = 0
+    for j, (xj, yj) in enumerate(zip(points, evals)):
+        num, den = 1, 1
+        for k2, xk in enumerate(points):
+            if k2 != j:
+                num = num * (at - xk) % R
+                den = den * (xj - xk) % R
+        total = (total + yj * num * inv(den)) % R
+    return total

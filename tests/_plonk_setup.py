@@ -1,0 +1,51 @@
+"""A config-3 circuit (the single-proof configuration) set up on the device
+and in the oracle: seeded fixed columns, copy cycles and witness, the KZG
+test SRS generated on the device (its bases are pinned against the oracle in
+test_srs_gpu.py) and handed to the oracle, and both keys."""
+import numpy as np
+
+from _loader import load
+from oracle import oracle as O
+from oracle import plonk as OP
+
+mzk = load()
+
+
+class Circuit:
+    def __init__(self, ctx, k, seed, pinned=b"config-3 circuit: standard gate, copy cycles, range lookup",
+                 oracle=True, srs=None):
+        """srs = (buffer, offsets) of a shared device SRS whose bases hold this
+        k's g | lagrange | delta | double delta at the offsets; otherwise
+        this circuit gets its own."""
+        self.ctx, self.k, self.seed = ctx, k, seed
+        c = OP.config3_circuit(k)
+        c["blinding_factors"] = OP.blinding_factors(c)
+        self.circuit = c
+        self.fixed, self.mapping, self.advice = OP.config3_instance(k, seed)
+        self.dom = mzk.EvaluationDomain(ctx, c["degree"], k)
+        n = self.n = self.dom.n
+        if srs is None:
+            self.s = O.rand_fr(1000 + seed, 1)[0]
+            self.srs_buf = ctx.alloc(4 * n * 96)
+            p = self.srs_buf.ptr
+            self.dom.srs_setup_device(self.s, p, p + n * 96, p + 2 * n * 96, p + 3 * n * 96)
+            self.offs = (0, n, 2 * n, 3 * n)
+            self.desc = mzk.SrsDesc(p, 4 * n, 0, n, 2 * n, 3 * n, 0, 0, 0)
+        else:
+            self.srs_buf, self.offs, self.desc, self.s = srs
+        self.key = mzk.PlonkKey(ctx, self.dom, c, self.desc, self.fixed, self.mapping, pinned)
+        self.okey = None
+        if oracle:
+            host = self.srs_buf.download((self.desc.srs_len, 12))
+            g, lag, dl, ddl = (host[o:o + n] for o in self.offs)
+            srs_h = {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}
+            self.okey = OP.keygen(OP.config3_circuit(k), self.fixed, self.mapping, srs_h, pinned)
+
+    def blinds(self, seed):
+        return O.rand_fr(5000 + seed, self.key.n_blinds)
+
+    def oracle_proof(self, advice, blinds):
+        return OP.create_proof(self.okey, advice, [OP.to_int(v) for v in blinds])
+
+    def verify(self, proof):
+        return OP.verify(self.okey, proof, OP.to_int(self.s))

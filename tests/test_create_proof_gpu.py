@@ -1,0 +1,144 @@
+"""create_proof on the B200 through the C ABI against the oracle's
+restatement (oracle/plonk.py): device keygen gives the oracle's VK
+commitments and transcript_repr; a proof of the single-proof configuration's
+circuit (standard gate, copy cycles, range lookup) is byte-for-byte the
+oracle's transcript at k = 5, 10 and 18, and the oracle's verifier accepts it
+(with the G1 trapdoor check in place of the pairing) and rejects it once
+tampered; many proofs of mixed k in one call equal each proof alone."""
+import numpy as np
+import pytest
+
+from _plonk_setup import Circuit, mzk
+from oracle import plonk as OP
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = mzk.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def k5(ctx):
+    return Circuit(ctx, 5, seed=1)
+
+
+def test_keygen_matches_oracle(k5):
+    ok = k5.okey
+    assert np.array_equal(k5.key.fixed_coms[:, :12], np.stack(ok.fixed_coms))
+    assert np.array_equal(k5.key.perm_coms[:, :12], np.stack(ok.perm_coms))
+    assert OP.to_int(k5.key.repr) == ok.repr
+    assert k5.key.proof_len == 13 * 48 + 21 * 32
+    assert k5.key.n_blinds == OP.blind_count(OP.config3_circuit(5))
+
+
+@pytest.mark.parametrize("k", [5, 10])
+def test_proof_bytes_equal_oracle_and_verify(ctx, k):
+    c = Circuit(ctx, k, seed=k)
+    for seed in (1, 2):
+        bl = c.blinds(seed)
+        proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)])[0]
+        assert proof == c.oracle_proof(c.advice, bl)
+        assert c.verify(proof)
+
+
+def test_config3_k18_proof_equals_oracle_and_verifies(ctx):
+    c = Circuit(ctx, 18, seed=18)
+    bl = c.blinds(18)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert len(proof) == c.key.proof_len
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+
+
+def test_tampered_proof_is_rejected(k5):
+    bl = k5.blinds(7)
+    proof = mzk.create_proofs(k5.ctx, [(k5.key, k5.advice, bl)])[0]
+    assert k5.verify(proof)
+    for at in (5, 48 * 4 + 9, 13 * 48 - 1, len(proof) - 40):
+        bad = bytearray(proof)
+        bad[at] ^= 0x01
+        assert not k5.verify(bytes(bad)), at
+
+
+def test_batch_of_mixed_k_equals_each_alone(ctx, k5):
+    c7 = Circuit(ctx, 7, seed=3, oracle=False)    # its own SRS buffer: proved in calls of its own
+    jobs = [(k5.key, k5.advice, k5.blinds(1)), (c7.key, c7.advice, c7.blinds(2)), (k5.key, k5.advice, k5.blinds(3))]
+    together = mzk.create_proofs(ctx, [jobs[0], jobs[2]])
+    assert together[0] == mzk.create_proofs(ctx, [jobs[0]])[0]
+    assert together[1] == mzk.create_proofs(ctx, [jobs[2]])[0]
+    assert together[0] != together[1]
+    # the plain form (every MSM its own call, no graphs) gives the same bytes
+    plain = mzk.create_proofs(ctx, [jobs[0], jobs[2]], flags=mzk.PROVE_MSM_PER_CALL | mzk.PROVE_NO_GRAPHS)
+    assert plain == together
+    assert mzk.create_proofs(ctx, [jobs[1]])[0] == mzk.create_proofs(ctx, [jobs[1]], flags=mzk.PROVE_NO_GRAPHS)[0]
+
+
+def test_mixed_k_over_one_srs(ctx):
+    """Keys of k = 6 and k = 8 over one SRS buffer (each k's bases at its own
+    offsets) prove in one call, and each proof equals its proof alone and the
+    oracle's."""
+    from oracle import oracle as O
+    s = O.rand_fr(4242, 1)[0]
+    sizes = {6: 1 << 6, 8: 1 << 8}
+    total = sum(4 * n for n in sizes.values())
+    buf = ctx.alloc(total * 96)
+    offs, at = {}, 0
+    for k, n in sizes.items():
+        dom = mzk.EvaluationDomain(ctx, 5, k)
+        p = buf.ptr + at * 96
+        dom.srs_setup_device(s, p, p + n * 96, p + 2 * n * 96, p + 3 * n * 96)
+        offs[k] = (at, at + n, at + 2 * n, at + 3 * n)
+        at += 4 * n
+        dom.close()
+    cs = {}
+    for k in sizes:
+        d = mzk.SrsDesc(buf.ptr, total, *offs[k], 0, 0, 0)
+        cs[k] = Circuit(ctx, k, seed=k + 30, srs=(buf, offs[k], d, s))
+    jobs = [(cs[6].key, cs[6].advice, cs[6].blinds(1)), (cs[8].key, cs[8].advice, cs[8].blinds(2)),
+            (cs[6].key, cs[6].advice, cs[6].blinds(3))]
+    together = mzk.create_proofs(ctx, jobs)
+    for j, pr in zip(jobs, together):
+        assert pr == mzk.create_proofs(ctx, [j])[0]
+    assert together[1] == cs[8].oracle_proof(cs[8].advice, jobs[1][2])
+    assert cs[8].verify(together[1]) and cs[6].verify(together[0])
+
+
+def test_device_advice_gives_the_same_proof(k5):
+    ctx = k5.ctx
+    bufs = []
+    for col in k5.advice:
+        b = ctx.alloc(col.nbytes)
+        b.upload(col)
+        bufs.append(b)
+    bl = k5.blinds(4)
+    assert mzk.create_proofs(ctx, [(k5.key, bufs, bl)])[0] == mzk.create_proofs(ctx, [(k5.key, k5.advice, bl)])[0]
+
+
+def test_self_check_refuses_unsatisfied_witness(k5):
+    ctx = k5.ctx
+    bl = k5.blinds(5)
+    assert mzk.create_proofs(ctx, [(k5.key, k5.advice, bl)], flags=mzk.PROVE_SELF_CHECK)
+    bad = [a.copy() for a in k5.advice]
+    bad[2][4] = OP.to_mont(OP.to_int(bad[2][4]) + 1)
+    with pytest.raises(mzk.MzkError, match="does not satisfy"):
+        mzk.create_proofs(ctx, [(k5.key, bad, bl)], flags=mzk.PROVE_SELF_CHECK)
+    # without the check the proof is made, and the verifier rejects it
+    assert not k5.verify(mzk.create_proofs(ctx, [(k5.key, bad, bl)])[0])
+
+
+def test_lookup_input_outside_the_table_is_refused(k5):
+    bad = [a.copy() for a in k5.advice]
+    bad[0][1] = OP.to_mont(123456789)
+    with pytest.raises(mzk.MzkError, match="not in the table"):
+        mzk.create_proofs(k5.ctx, [(k5.key, bad, k5.blinds(6))])
+    # the context stays usable
+    assert k5.verify(mzk.create_proofs(k5.ctx, [(k5.key, k5.advice, k5.blinds(6))])[0])
+
+
+def test_wrong_blind_count_is_refused(k5):
+    with pytest.raises(mzk.MzkError):
+        mzk.create_proofs(k5.ctx, [(k5.key, k5.advice, k5.blinds(1)[:-1])])

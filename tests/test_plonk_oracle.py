@@ -1,0 +1,104 @@
+"""The oracle's create_proof and verifier (oracle/plonk.py) on the
+single-proof configuration's circuit: honest proofs are accepted, and the
+verifier rejects every kind of wrong proof it must reject (tampered
+commitments and evaluations, truncated or extended proofs, a wrong trapdoor,
+witnesses that break the gate or a copy constraint).  CPU only."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import plonk as OP
+
+
+def setup(k, seed, pinned=b"config-3 circuit"):
+    c = OP.config3_circuit(k)
+    fixed, mapping, adv = OP.config3_instance(k, seed)
+    s = O.rand_fr(1000 + seed, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    srs = {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}
+    key = OP.keygen(c, fixed, mapping, srs, pinned)
+    return c, key, adv, OP.to_int(s), mapping
+
+
+def blinds(c, seed):
+    return [OP.to_int(v) for v in O.rand_fr(2000 + seed, OP.blind_count(c))]
+
+
+@pytest.fixture(scope="module")
+def k5():
+    c, key, adv, s, mapping = setup(5, 1)
+    proof = OP.create_proof(key, adv, blinds(c, 1))
+    return c, key, adv, s, mapping, proof
+
+
+def test_shape_constants(k5):
+    c, key, _, _, _, proof = k5
+    assert OP.blinding_factors(c) == 7 and key.qdeg == 4 and key.dom.extended_k == 7
+    # 13 commitments (a, b, c, m, z, h, Z, 4 limbs, f, pi) and 21 scalars
+    assert len(proof) == 13 * 48 + 21 * 32
+
+
+def test_honest_proofs_verify(k5):
+    _, key, _, s, _, proof = k5
+    assert OP.verify(key, proof, s)
+    c, key7, adv7, s7, _ = setup(7, 2)
+    assert OP.verify(key7, OP.create_proof(key7, adv7, blinds(c, 2)), s7)
+
+
+def test_proofs_are_deterministic_in_the_blinds(k5):
+    c, key, adv, _, _, proof = k5
+    assert OP.create_proof(key, adv, blinds(c, 1)) == proof
+    assert OP.create_proof(key, adv, blinds(c, 3)) != proof
+
+
+def test_tampered_proofs_are_rejected(k5):
+    _, key, _, s, _, proof = k5
+    gen = bytes(O.g1_compress(O.g1_generator()))
+    for at in (0, 48 * 3, 48 * 7, 48 * 10):            # a, m, h, a quotient limb
+        bad = proof[:at] + gen + proof[at + 48:]
+        assert not OP.verify(key, bad, s), at
+    pts = 11 * 48
+    for i in range(0, 19):                              # every evaluation before the multi-open
+        at = pts + 32 * i
+        v = int.from_bytes(proof[at:at + 32], "little")
+        bad = proof[:at] + ((v + 1) % OP.R).to_bytes(32, "little") + proof[at + 32:]
+        assert not OP.verify(key, bad, s), i
+    assert not OP.verify(key, proof[:-1], s)
+    assert not OP.verify(key, proof + b"\x00", s)
+    assert not OP.verify(key, proof, s + 1)
+
+
+def test_unsatisfied_witnesses_are_rejected(k5):
+    c, key, adv, s, mapping, _ = k5
+    bad = [a.copy() for a in adv]
+    bad[2][3] = OP.to_mont(OP.to_int(bad[2][3]) + 1)    # the gate fails on row 3
+    assert not OP.verify(key, OP.create_proof(key, bad, blinds(c, 1)), s)
+    # a copy constraint fails: a cell of a cycle changes (a b-cell, so the lookup still holds),
+    # its row's c is solved again so the gate still holds
+    cyc = [(cc, r) for cc in range(2) for r in range(key.u) if tuple(mapping[cc, r]) != (cc, r)]
+    cc, r = next((cc, r) for cc, r in cyc if cc == 1)
+    bad = [a.copy() for a in adv]
+    fixed = key.fixed_values
+    bad[1][r] = OP.to_mont(OP.to_int(bad[1][r]) + 5)
+    ql, qr, qm, qo, qcst = (OP.to_int(fixed[i][r]) for i in range(5))
+    a, b = OP.to_int(bad[0][r]), OP.to_int(bad[1][r])
+    bad[2][r] = OP.to_mont(-(ql * a + qr * b + qm * a * b + qcst) * OP.inv(qo))
+    assert not OP.verify(key, OP.create_proof(key, bad, blinds(c, 1)), s)
+
+
+def test_lookup_input_outside_the_table_is_refused(k5):
+    c, key, adv, _, _, _ = k5
+    bad = [a.copy() for a in adv]
+    bad[0][2] = OP.to_mont(10 ** 9)
+    with pytest.raises(ValueError):
+        OP.create_proof(key, bad, blinds(c, 1))
+
+
+def test_intermediate_sets_follow_first_appearance():
+    q = [("a", 1), ("b", 1), ("z", 1), ("z", 7), ("b", 9), ("c", 1), ("Z", 1), ("Z", 7)]
+    labels, sets, _ = OP.intermediate_sets(q)
+    assert [lb for lb, _, _ in labels] == ["a", "b", "z", "c", "Z"]
+    assert sets == [[1], [1, 9], [1, 7]]
+    assert [si for _, si, _ in labels] == [0, 1, 2, 0, 2]
+    with pytest.raises(ValueError):
+        OP.intermediate_sets([("a", 1), ("a", 1)])
