@@ -12,7 +12,7 @@
  * gives the message of the calling thread's last failure.  All entry points
  * are thread-safe; calls on one context are serialised.  The reference panics
  * on length mismatch (curves/src/msm.rs:461, proofs/src/poly/domain.rs:250);
- * the Rust binding turns a non-zero status into that panic (INTEGRATION.md).
+ * the Rust binding turns a non-zero status into that panic.
  */
 #ifndef MZK_H
 #define MZK_H
@@ -119,10 +119,14 @@ int mzk_msm_g1_device(mzk_ctx *ctx, const uint64_t *d_scalars, const uint64_t *d
  * scratch is one fixed device array of about 21 MB inside this library, held
  * by every GPU that loads it until the process exits.  n must not exceed
  * 65536 (larger n returns MZK_ERR_ARG).  The first call on a device looks up
- * that array's device address (make it before any stream capture).  Runs on
- * `stream` (NULL: the default stream) and returns when the result is on the
- * host.  All calls share the array: calls are serialised by a host lock, and
- * GPU work of two calls that overlapped would race on it.
+ * that array's device address (make it before any stream capture); with CUDA's
+ * lazy module loading that first call is also when the module and its array
+ * are loaded onto the device, so make it before the host reserves the rest of
+ * the device's memory.  Runs on `stream` (NULL: the default stream), which
+ * must belong to the current device (whose copy of the array is used), and
+ * returns when the result is on the host.  All calls on one device share its
+ * array: they are serialised by a host lock per device, and GPU work of two
+ * calls that overlapped would race on it.
  */
 int mzk_msm_g1_noalloc(const uint64_t *d_scalars, const uint64_t *d_bases, size_t n, uint64_t out[18], void *stream);
 /* Batched MSMs over one shared device SRS: item m is

@@ -1172,7 +1172,8 @@ constexpr size_t kNaBytes = kNaLongOff + align256(16 + kNaAccThreads * sizeof(ui
 // cudaGetSymbolAddress below.
 __device__ __align__(256) unsigned char g_msm_noalloc_scratch[kNaBytes];
 
-std::mutex g_noalloc_mu;
+// one lock per device: each device has its own copy of the array
+std::mutex g_noalloc_mu[kNoAllocMaxDevices];
 void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 int g_noalloc_sms[kNoAllocMaxDevices] = {};
 
@@ -1188,6 +1189,9 @@ Status scan_u32_noalloc(const uint32_t* in, uint32_t* out, uint32_t len, uint32_
     return OK;
 }
 
+Status msm_g1_noalloc_queued(unsigned char* base, int sms, const void* d_scalars, const void* d_bases, size_t n,
+                             uint64_t* out18, cudaStream_t st);
+
 Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint64_t* out18, cudaStream_t st) {
     std::memset(out18, 0, 18 * 8);
     if (n > kNoAllocMaxN) {
@@ -1202,8 +1206,8 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
         set_error("mzk_msm_g1_noalloc: device index out of range");
         return ERR_ARG;
     }
-    // one lock for the shared array: calls from several host threads take turns
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    // one lock for this device's array: calls from several host threads take turns
+    std::lock_guard<std::mutex> lock(g_noalloc_mu[dev]);
     if (!g_noalloc_ptr[dev]) {
         // set-up, once per device, with that device current
         void* p = nullptr;
@@ -1217,7 +1221,16 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
         g_noalloc_sms[dev] = sms;
         g_noalloc_ptr[dev] = p;
     }
-    unsigned char* base = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+    const Status s = msm_g1_noalloc_queued(static_cast<unsigned char*>(g_noalloc_ptr[dev]), g_noalloc_sms[dev],
+                                           d_scalars, d_bases, n, out18, st);
+    // a failure after work was queued: let that work finish before the lock
+    // is released, so the next call cannot race with it on the array
+    if (s != OK) cudaStreamSynchronize(st);
+    return s;
+}
+
+Status msm_g1_noalloc_queued(unsigned char* base, int sms, const void* d_scalars, const void* d_bases, size_t n,
+                             uint64_t* out18, cudaStream_t st) {
     int c = msm_pick_window(n);
     c = c < kNoAllocMinC ? kNoAllocMinC : (c > kNoAllocMaxC ? kNoAllocMaxC : c);
     const MsmShape sh = make_shape(c, kNoAllocGroupLog);
@@ -1237,7 +1250,7 @@ Status msm_g1_noalloc(const void* d_scalars, const void* d_bases, size_t n, uint
     const Affine* ba = static_cast<const Affine*>(d_bases);
     const int pt_threads = 256;
     const uint32_t pt_blocks =
-        (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)g_noalloc_sms[dev] * 16);
+        (uint32_t)std::min<size_t>((n + pt_threads - 1) / pt_threads, (size_t)sms * 16);
     // the array keeps the previous call's contents: zero the counters
     MZK_CUDA_CHECK(cudaMemsetAsync(counts, 0, ((size_t)sh.keys + 1) * 4, st));
     k_histogram<<<pt_blocks, pt_threads, 0, st>>>(sc, n, sh.c, sh.windows, sh.nb, counts, nullptr);

@@ -495,8 +495,10 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         key->fixed_coeff.push_back(take(n));
         key->fixed_ext.push_back(take(E));
     }
+    // the permutation columns' Lagrange forms are contiguous: k_perm_values
+    // writes them as one P x n array
+    for (uint32_t i = 0; i < P; i++) key->perm_lag.push_back(take(n));
     for (uint32_t i = 0; i < P; i++) {
-        key->perm_lag.push_back(take(n));
         key->perm_coeff.push_back(take(n));
         key->perm_ext.push_back(take(E));
     }

@@ -5,17 +5,24 @@ Reads the midnight-zk sources AS TEXT (nothing of the reference is executed:
 it is Rust, and no Rust toolchain exists in this image).  Every vector records
 the file and line it came from.  Run from the repository root:
 
-    python tests/golden/make_golden.py [/path/to/midnight-zk]
+    python tests/golden/make_golden.py /path/to/midnight-zk
 
+(or set MZK_REFERENCE to the reference tree).
 The generated JSON is committed; the tests only read the JSON, so they run
 where the reference tree is absent.
 """
 import json
+import os
 import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) > 1:
+    REF = Path(sys.argv[1])
+elif os.environ.get("MZK_REFERENCE"):
+    REF = Path(os.environ["MZK_REFERENCE"])
+else:
+    sys.exit("usage: make_golden.py <path to the midnight-zk sources> (or set MZK_REFERENCE)")
 OUT = Path(__file__).resolve().parent / "reference_kats.json"
 
 NUM = r"(?:0x[0-9a-fA-F_]+|\d+)"
