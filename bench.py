@@ -60,7 +60,8 @@ def parse_args():
     p.add_argument("--no-extras", action="store_true", help="skip the NTT and quotient lines")
     p.add_argument("--ntt-log-n", type=int, default=24)
     p.add_argument("--no-prover", action="store_true", help="skip the proof-core, batched-MSM and serving lines")
-    p.add_argument("--serve-requests", type=int, default=80)
+    p.add_argument("--serve-requests", type=int, default=400)
+    p.add_argument("--serve-reps", type=int, default=3)
     return p.parse_args()
 
 
@@ -241,102 +242,86 @@ SERVE_KS = (14, 16, 18, 20)
 SERVE_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
 
 
-class ProverKeys:
-    """Synthetic proving keys of the single-proof circuit for several k, resident
-    on the device: one SRS buffer [g (2^max k) | per k: lagrange, delta, double
-    delta] of seeded points, and per k the 13 extended fixed/permutation/
-    Lagrange-selector columns of seeded Fr values.  Timing depends only on
-    sizes and scalar distributions, not on the bases' discrete logs."""
+class PlonkKeys:
+    """Proving keys of the single-proof configuration's circuit (standard gate,
+    copy cycles over 10 % of the a and b cells, range lookup of a into a 2^16
+    table) for several k over ONE device SRS: the KZG test setup for one seeded
+    secret, g of 2^max k points (a prefix serves every smaller k) then each k's
+    lagrange, delta and double-delta bases, stored as row 0 of a fixed-base
+    window table.  One seeded Config3Instance per k gives the fixed columns,
+    the key (device keygen) and fresh satisfying witnesses per request."""
 
     def __init__(self, mzk, ctx, ks, table_c=TABLE_C, table_min_n=TABLE_MIN_N):
-        self.mzk, self.ctx, self.ks = mzk, ctx, tuple(ks)
-        gmax = 1 << max(ks)
-        self.srs_len = gmax + sum(3 << k for k in ks)
-        # the SRS as row 0 of a fixed-base window table (rows [2^(c j)] bases),
-        # built once like the SRS itself
+        self.mzk, self.ctx, self.ks = mzk, ctx, tuple(sorted(ks))
+        kmax = max(ks)
+        self.srs_len = (1 << kmax) + sum(3 << k for k in ks)
         self.table_rows = mzk.Context.msm_table_rows(table_c) if table_c else 1
         self.srs = ctx.alloc(self.table_rows * self.srs_len * 96)
-        ctx.gen_bases(0x5125, self.srs_len, out=self.srs)
+        secret = ctx.gen_rand_fr(0x5EC2E7, 1).download((1, 4))[0]
+        t0 = time.perf_counter()
+        self.doms, self.inst, off = {}, {}, 1 << kmax
+        offs = {}
+        for k in self.ks:
+            n = 1 << k
+            dom = mzk.EvaluationDomain(ctx, mzk.CONFIG3_DEGREE, k)
+            p = self.srs.ptr
+            dom.srs_setup_device(secret, p if k == kmax else None, p + off * 96, p + (off + n) * 96,
+                                 p + (off + 2 * n) * 96)
+            offs[k] = (0, off, off + n, off + 2 * n)
+            off += 3 * n
+            self.doms[k] = dom
+        setup_s = time.perf_counter() - t0
         t0 = time.perf_counter()
         if table_c:
             ctx.msm_window_table(self.srs, self.srs_len, table_c, self.table_rows)
         self.table = {"c": table_c, "rows": self.table_rows, "min_n": table_min_n,
-                      "bytes": self.table_rows * self.srs_len * 96, "build_s": round(time.perf_counter() - t0, 2)}
-        self.doms, self.pks, self.cols = {}, {}, {}
-        off = gmax
-        for k in ks:
-            dom = mzk.EvaluationDomain(ctx, 5, k)
-            E = dom.extended_len
-            cols = ctx.gen_rand_fr(0xC0150000 + k, 13 * E + 5 * (1 << k))
-            pk = mzk.ProvingKeyDesc()
-            pk.k = k
-            for i in range(7):
-                pk.fixed_ext[i] = cols.ptr + i * E * 32
-            for i in range(3):
-                pk.sigma_ext[i] = cols.ptr + (7 + i) * E * 32
-            pk.l0_ext, pk.l_last_ext, pk.l_active_ext = (cols.ptr + (10 + i) * E * 32 for i in range(3))
-            lag0 = cols.ptr + 13 * E * 32  # Lagrange sigma a, b, c, table, selector (n each)
-            for i in range(3):
-                pk.sigma_lagrange[i] = lag0 + i * (1 << k) * 32
-            pk.table_lagrange, pk.selector_lagrange = lag0 + 3 * (1 << k) * 32, lag0 + 4 * (1 << k) * 32
-            pk.srs, pk.srs_len = self.srs.ptr, self.srs_len
-            n = 1 << k
-            pk.off_g, pk.off_lagrange, pk.off_lagrange_delta, pk.off_lagrange_double_delta = 0, off, off + n, off + 2 * n
-            off += 3 * n
-            pk.blinding_factors = 7
-            pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n = table_c, self.table_rows, table_min_n
-            self.doms[k], self.pks[k], self.cols[k] = dom, pk, cols
+                      "bytes": self.table_rows * self.srs_len * 96, "build_s": round(time.perf_counter() - t0, 2),
+                      "srs_setup_s": round(setup_s, 2)}
+        t0 = time.perf_counter()
+        for k in self.ks:
+            desc = mzk.SrsDesc(self.srs.ptr, self.srs_len, *offs[k], table_c, self.table_rows, table_min_n)
+            self.inst[k] = mzk.Config3Instance(ctx, self.doms[k], desc, seed=0xC0F3 + k)
+        self.keygen_s = round(time.perf_counter() - t0, 2)
 
-    def job(self, k, seed):
-        """A proof job with fresh seeded witness columns a, b, c and lookup
-        multiplicities m on the device; the permutation product z and the
-        logup helper h and aggregator Z are derived by the device."""
-        n = 1 << k
-        w = self.ctx.gen_rand_fr(seed, 4 * n)
-        j = self.mzk.ProofJob()
-        ptr = [w.ptr + i * n * 32 for i in range(4)]
-        j.advice[0], j.advice[1], j.advice[2] = ptr[0], ptr[1], ptr[2]
-        j.lookup_m = ptr[3]
-        j.perm_z = j.lookup_h = j.lookup_Z = None
-        for i in range(8):
-            j.perm_blinds[i][:] = [seed % 991 + 20 + i, 0, 0, 0]
-            j.lookup_blinds[i][:] = [seed % 983 + 40 + i, 0, 0, 0]
-        for i, name in enumerate(("y", "beta", "gamma", "theta")):
-            getattr(j, name)[:] = [seed % 1000 + 3 + i, 0, 0, 0]
-        for i in range(3):
-            j.quotient_blinds[i][:] = [seed % 977 + 11 + i, 0, 0, 0]
-        return j, w
+    def request(self, k, seed):
+        inst = self.inst[k]
+        return inst.key, inst.witness(seed), inst.blinds(seed ^ 0xB11D)
 
     def close(self):
+        self.inst.clear()
         for d in self.doms.values():
             d.close()
 
 
-def measure_proof_core(mzk, ctx, keys, k, reps, batch):
-    """Device part of one proof at 2^k rows: plain (one proof per call, every
-    MSM its own call), one proof with its MSMs batched, and `batch` proofs in
-    one call; wall-clock per call, results on the host."""
-    dom, pk = keys.doms[k], keys.pks[k]
-    jobs = [keys.job(k, 0x9000 + i) for i in range(batch)]
-    dom.prove_core_device(pk, [jobs[0][0]])  # warm-up (scratch allocation)
-    dom.prove_core_device(pk, [jobs[0][0]], per_call=True)
-    dom.prove_core_device(pk, [j for j, _ in jobs])
-    t0 = time.perf_counter()
-    for i in range(reps):
-        dom.prove_core_device(pk, [jobs[i % batch][0]], per_call=True)
-    per_call_ms = (time.perf_counter() - t0) / reps * 1e3
-    t0 = time.perf_counter()
-    for i in range(reps):
-        dom.prove_core_device(pk, [jobs[i % batch][0]])
-    plain_ms = (time.perf_counter() - t0) / reps * 1e3
-    t0 = time.perf_counter()
-    for _ in range(max(1, reps // batch)):
-        dom.prove_core_device(pk, [j for j, _ in jobs])
-    batch_ms = (time.perf_counter() - t0) / max(1, reps // batch) * 1e3
-    return {"k": k, "rows": 1 << k, "per_call_ms_per_proof": round(per_call_ms, 2),
-            "one_proof_batched_msms_ms": round(plain_ms, 2), "batch": batch,
-            "batched_ms_per_call": round(batch_ms, 2), "batched_proofs_per_s": round(batch * 1e3 / batch_ms, 2),
-            "msms_per_proof": 11, "witness": "a, b, c, m uniform Fr; z, h, Z derived on the device"}
+def measure_proofs(mzk, ctx, keys, k, reps, batch):
+    """create_proof of the single-proof configuration at 2^k rows, transcript
+    on the host: plain (one proof per call, every MSM its own call, kernels
+    launched one by one), one proof per call with each phase's MSMs batched,
+    and `batch` proofs in one call.  The first proof runs with the self-check
+    (L'(x) = -C), so the witnesses are known to satisfy the circuit."""
+    reqs = [keys.request(k, 0x9000 + i) for i in range(batch)]
+    mzk.create_proofs(ctx, [reqs[0]], flags=mzk.PROVE_SELF_CHECK)
+    mzk.create_proofs(ctx, [reqs[0]], flags=mzk.PROVE_PLAIN)          # warm-up (scratch allocation)
+    mzk.create_proofs(ctx, [reqs[0]])
+    mzk.create_proofs(ctx, reqs)
+
+    def timed(fn, calls):
+        t0 = time.perf_counter()
+        for i in range(calls):
+            fn(i)
+        return (time.perf_counter() - t0) / calls * 1e3
+
+    plain_ms = timed(lambda i: mzk.create_proofs(ctx, [reqs[i % batch]], flags=mzk.PROVE_PLAIN), reps)
+    one_ms = timed(lambda i: mzk.create_proofs(ctx, [reqs[i % batch]]), reps)
+    calls = max(1, reps // batch)
+    batch_ms = timed(lambda i: mzk.create_proofs(ctx, reqs), calls)
+    key = keys.inst[k].key
+    return {"k": k, "rows": 1 << k, "proof_bytes": key.proof_len, "msms_per_proof": 13,
+            "plain_ms_per_proof": round(plain_ms, 2), "one_proof_batched_msms_ms": round(one_ms, 2),
+            "batch": batch, "batched_ms_per_call": round(batch_ms, 2),
+            "batched_proofs_per_s": round(batch * 1e3 / batch_ms, 2), "plain_proofs_per_s": round(1e3 / plain_ms, 2),
+            "witness": "satisfying (self-checked); a in the 2^16 table, b uniform, c solved; copy cycles",
+            "transcript": "Blake2b Fiat-Shamir, phases in the reference's order"}
 
 
 def measure_batched_msm(mzk, ctx, reps):
@@ -397,52 +382,52 @@ def measure_batched_msm(mzk, ctx, reps):
                              "equals_batched": bool(np.array_equal(tabled, together))}}
 
 
-def measure_serving(mzk, ctx, keys, n_requests, max_batch, lanes, mem_budget):
-    """Poisson stream of proof requests, k drawn from SERVE_KS with SERVE_WEIGHTS.
-    The plain prover (one proof at a time, every MSM its own call) is measured
-    closed-loop for its throughput; every mode then takes open-loop Poisson
-    streams at 0.8x and 1.5x that rate.  Latency = submit to results on the host."""
+def measure_serving(mzk, ctx, keys, n_requests, reps, max_batch, lanes, mem_budget):
+    """A stream of create_proof requests, k drawn from SERVE_KS with
+    SERVE_WEIGHTS, a fresh seeded witness per request.  Closed loop (all
+    requests queued at once): every mode `reps` times, median and spread of
+    proofs/s.  Then open-loop Poisson arrivals at 0.8x and 1.5x the plain
+    prover's closed-loop rate.  Latency = submit to transcript on the host."""
     import threading
 
     import numpy as np
     rng = np.random.default_rng(0x5E7E)
     ks = [int(k) for k in rng.choice(SERVE_KS, size=n_requests, p=SERVE_WEIGHTS)]
-    reqs = [keys.job(k, 0x20000 + i) for i, k in enumerate(ks)]
+    reqs = [keys.request(k, 0x20000 + i) for i, k in enumerate(ks)]
+    warm = [reqs[ks.index(k)] for k in SERVE_KS] * 3
 
     def run(server_args, arrivals):
         srv = mzk.ProvingServer(ctx, **server_args)
-        for k in keys.ks:
-            srv.add_key(keys.doms[k], keys.pks[k])
-        # warm-up: the whole request list once, closed loop (the lanes' scratch
-        # arenas reach their working size here, not in the timed pass)
-        for t in [srv.submit(k, j, keep=w) for k, (j, w) in zip(ks, reqs)]:
+        # warm-up (untimed): a few requests of every k, so the lanes' scratch
+        # arenas reach their working size and the NTT graphs are captured
+        for t in [srv.submit(*r) for r in warm]:
             srv.wait(t)
         warm_waves = srv.stats()["waves"]
-        lat = [None] * len(ks)
-        tickets = [None] * len(ks)
+        lat = [None] * len(reqs)
+        tickets = [None] * len(reqs)
         ready = threading.Semaphore(0)
 
         def collector():
-            for i in range(len(ks)):
+            for i in range(len(reqs)):
                 ready.acquire()
                 lat[i] = srv.wait(tickets[i])[1]
 
         th = threading.Thread(target=collector)
         th.start()
         t0 = time.perf_counter()
-        for i, (k, (job, _)) in enumerate(zip(ks, reqs)):
+        for i, r in enumerate(reqs):
             if arrivals is not None:
                 d = t0 + arrivals[i] - time.perf_counter()
                 if d > 0:
                     time.sleep(d)
-            tickets[i] = srv.submit(k, job, keep=reqs[i][1])
+            tickets[i] = srv.submit(*r)
             ready.release()
         th.join()
         wall = time.perf_counter() - t0
         st = srv.stats()
         srv.close()
         lat = np.array(lat)
-        return {"proofs_per_s": round(len(ks) / wall, 2), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+        return {"proofs_per_s": round(len(reqs) / wall, 2), "p50_ms": round(float(np.percentile(lat, 50)), 2),
                 "p99_ms": round(float(np.percentile(lat, 99)), 2), "waves": st["waves"] - warm_waves,
                 "wall_s": round(wall, 2)}
 
@@ -451,13 +436,24 @@ def measure_serving(mzk, ctx, keys, n_requests, max_batch, lanes, mem_budget):
         "one_proof_batched_msms": {"max_batch": 1, "lanes": 1},            # one proof, its MSMs batched
         "served": {"max_batch": max_batch, "lanes": lanes, "mem_budget_bytes": mem_budget},
     }
-    out = {"requests": n_requests, "k_mix": dict(zip(map(str, SERVE_KS), SERVE_WEIGHTS)), "modes": modes}
-    out["closed_loop"] = {name: run(a, None) for name, a in modes.items()}
-    rate = out["closed_loop"]["plain"]["proofs_per_s"]
+    out = {"requests": n_requests, "k_mix": dict(zip(map(str, SERVE_KS), SERVE_WEIGHTS)), "modes": modes,
+           "repetitions": reps}
+    closed = {}
+    for name, a in modes.items():
+        runs = [run(a, None) for _ in range(reps)]
+        rates = sorted(r["proofs_per_s"] for r in runs)
+        closed[name] = {"proofs_per_s_median": rates[len(rates) // 2], "proofs_per_s_min": rates[0],
+                        "proofs_per_s_max": rates[-1],
+                        "p50_ms_median": sorted(r["p50_ms"] for r in runs)[len(runs) // 2],
+                        "p99_ms_median": sorted(r["p99_ms"] for r in runs)[len(runs) // 2],
+                        "wall_s": [r["wall_s"] for r in runs], "waves": [r["waves"] for r in runs]}
+    out["closed_loop"] = closed
+    rate = closed["plain"]["proofs_per_s_median"]
+    out["served_over_plain_closed_loop"] = round(closed["served"]["proofs_per_s_median"] / rate, 3)
     for f in (0.8, 1.5):
         arr = np.cumsum(rng.exponential(1.0 / (f * rate), size=n_requests))
         out[f"poisson_{f}x_plain"] = {"rate_per_s": round(f * rate, 2),
-                                      **{name: run(a, arr) for name, a in modes.items()}}
+                                      **{name: run(modes[name], arr) for name in ("plain", "served")}}
     return out
 
 
@@ -728,12 +724,14 @@ def run_ours(args):
         extra_q = measure_quotient(mzk, ctx, stream, 18, 5)
         if not args.no_prover:
             extra_prover["batched_msm"] = measure_batched_msm(mzk, ctx, 3)
-            keys = ProverKeys(mzk, ctx, SERVE_KS)
-            extra_prover["proof_core_k18"] = measure_proof_core(mzk, ctx, keys, 18, 8, 8)
-            extra_prover["proof_core_by_k"] = {str(k): measure_proof_core(mzk, ctx, keys, k, reps, b)
-                                               for k, reps, b in ((14, 32, 16), (16, 32, 16), (20, 4, 2))}
-            extra_prover["serving"] = measure_serving(mzk, ctx, keys, args.serve_requests, 16, 2, 8 << 30)
+            keys = PlonkKeys(mzk, ctx, SERVE_KS)
+            extra_prover["create_proof_k18"] = measure_proofs(mzk, ctx, keys, 18, 8, 8)
+            extra_prover["create_proof_by_k"] = {str(k): measure_proofs(mzk, ctx, keys, k, reps, b)
+                                                 for k, reps, b in ((14, 32, 16), (16, 32, 16), (20, 4, 2))}
+            extra_prover["serving"] = measure_serving(mzk, ctx, keys, args.serve_requests, args.serve_reps, 16, 2,
+                                                      48 << 30)
             extra_prover["prover_srs_window_table"] = keys.table
+            extra_prover["prover_keygen_s"] = keys.keygen_s
             keys.close()
             del keys
             extra_prover["setup_and_scans"] = measure_setup_and_scans(mzk, ctx, stream)

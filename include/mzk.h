@@ -437,6 +437,8 @@ int mzk_plonk_key_destroy(mzk_plonk_key *key);
 int mzk_plonk_key_info(const mzk_plonk_key *key, uint64_t repr[4], size_t *proof_len, size_t *n_blinds);
 /* the VK commitments: fixed n_fixed x 18 u64, permutation n_perm_cols x 18 u64 */
 int mzk_plonk_key_commitments(const mzk_plonk_key *key, uint64_t *fixed, uint64_t *perm);
+/* the SRS description the key was built over */
+int mzk_plonk_key_srs(const mzk_plonk_key *key, mzk_srs_desc *out);
 /* One proof: the advice columns (2^k Fr each in Lagrange form; rows from
  * 2^k - blinding_factors - 1 on are replaced by blinding values), HOST or
  * DEVICE pointers, and the rng draws in the reference's order: the blinding
@@ -566,27 +568,27 @@ int mzk_srs_read_processed(mzk_ctx *ctx, const uint8_t *bytes, size_t len, size_
                            uint64_t *g, uint64_t *g_lagrange, uint64_t *g_lagrange_delta,
                            uint64_t *g_lagrange_double_delta);
 
-/* ---- proving service (continuous batching over the proof core) ---------- */
+/* ---- proving service (continuous batching over create_proof) ------------ */
 /* No reference counterpart: the reference proves one call at a time.
  * `lanes` worker threads (1..8), each with its own device context, serve one
- * request queue.  An idle lane takes a wave: queued requests oldest first
- * while the wave holds fewer than max_batch proofs, its device scratch stays
- * within mem_budget_bytes / lanes and that of all proofs in flight within
- * mem_budget_bytes (0: no limit; a proof larger than that runs alone when
- * nothing else is in flight), run as one mixed-k proof-core call, so
- * requests arriving while a wave runs start beside it on the device.
- * max_batch = 1 with one lane and MZK_PROVE_MSM_PER_CALL is the plain
- * one-call-at-a-time prover.  Witness
- * buffers referenced by a job must stay valid until its wait returns. */
+ * request queue of create_proof requests (mzk_proof_request, any keys).  An
+ * idle lane takes a wave: queued requests oldest first whose keys share the
+ * first one's SRS buffer, while the wave holds fewer than max_batch proofs,
+ * its device scratch stays within mem_budget_bytes / lanes and that of all
+ * proofs in flight within mem_budget_bytes (0: no limit; a proof larger than
+ * that runs alone when nothing else is in flight), run as one
+ * mzk_create_proofs call with `flags`; requests arriving while a wave runs
+ * start beside it on the device.  max_batch = 1 with one lane and
+ * MZK_PROVE_MSM_PER_CALL is the plain one-call-at-a-time prover.  A
+ * request's witness, blinds and output buffer must stay valid until its
+ * wait returns. */
 typedef struct mzk_server mzk_server;
 int mzk_server_create(mzk_ctx *ctx, uint32_t max_batch, uint32_t lanes, uint64_t mem_budget_bytes,
                       uint32_t flags /* MZK_PROVE_* of every wave */, mzk_server **out);
-/* register the domain and proving key of one k (all keys share one SRS buffer) */
-int mzk_server_add_key(mzk_server *s, mzk_domain *d, const mzk_proving_key_desc *pk);
-int mzk_server_submit(mzk_server *s, uint32_t k, const mzk_proof_job *job, uint64_t *ticket);
-/* blocks until the request is done: out 11 x 18 u64 as mzk_prove_core_device,
+int mzk_server_submit(mzk_server *s, const mzk_proof_request *req, uint64_t *ticket);
+/* blocks until the request is done (its transcript in req->proof_out);
  * latency from submit to completion */
-int mzk_server_wait(mzk_server *s, uint64_t ticket, uint64_t *out, double *latency_ms);
+int mzk_server_wait(mzk_server *s, uint64_t ticket, double *latency_ms);
 int mzk_server_stats(mzk_server *s, uint64_t *waves, uint64_t *proofs, double *busy_ms);
 int mzk_server_destroy(mzk_server *s);
 
@@ -595,6 +597,22 @@ int mzk_server_destroy(mzk_server *s);
 int mzk_gen_rand_fr_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);
 /* n affine bases [r_i]G with r_i the Fr elements of stream `seed` */
 int mzk_gen_bases_g1_device(mzk_ctx *ctx, uint64_t seed, uint64_t first, size_t n, uint64_t *d_out);
+/* A seeded instance of the single-proof configuration's circuit (standard
+ * gate over a, b, c, copy cycles, range lookup of a), for benchmarks.
+ * gen_config3_fixed: the 7 fixed columns q_l, q_r, q_m, q_o, q_c, table,
+ * selector (one DEVICE buffer of 7 x 2^k Fr): the q uniform on the usable rows
+ * u = 2^k - blinding_factors - 1 (q_o never zero) and zero after them, the
+ * table 0 .. min(table_rows, u) - 1 then zeros, the selector one on the usable
+ * rows.  gen_config3_witness: a, b, c (one DEVICE buffer of 3 x 2^k Fr) for
+ * those columns: a a table value, b uniform, every cell of one copy cycle the
+ * cycle's table value (cycle_of: DEVICE u32 per cell of a then of b, 0xffffffff
+ * outside cycles), c solving the gate with inv_qo = 1 / q_o (DEVICE, 2^k Fr);
+ * rows from u on are zero.  Element values depend only on (seed, row). */
+int mzk_gen_config3_fixed_device(mzk_ctx *ctx, uint32_t k, uint32_t blinding_factors, uint32_t table_rows,
+                                 uint64_t seed, uint64_t *d_fixed);
+int mzk_gen_config3_witness_device(mzk_ctx *ctx, uint32_t k, uint32_t blinding_factors, uint32_t table_rows,
+                                   uint64_t seed, const uint64_t *d_fixed, const uint64_t *d_inv_qo,
+                                   const uint32_t *d_cycle_of, uint64_t *d_advice);
 
 #ifdef __cplusplus
 }

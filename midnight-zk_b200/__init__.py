@@ -96,9 +96,8 @@ SIGNATURES = {
     "mzk_poly_inner_product_device": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p, _sz]),
     "mzk_logup_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_create": (_i32, [_vp, _u32, _u32, _u64, _u32, ctypes.POINTER(_vp)]),
-    "mzk_server_add_key": (_i32, [_vp, _vp, ctypes.c_void_p]),
-    "mzk_server_submit": (_i32, [_vp, _u32, ctypes.c_void_p, _u64p]),
-    "mzk_server_wait": (_i32, [_vp, _u64, _u64p, ctypes.POINTER(ctypes.c_double)]),
+    "mzk_server_submit": (_i32, [_vp, ctypes.c_void_p, _u64p]),
+    "mzk_server_wait": (_i32, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "mzk_server_stats": (_i32, [_vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_double)]),
     "mzk_server_destroy": (_i32, [_vp]),
     "mzk_transcript_create": (_i32, [ctypes.POINTER(_vp)]),
@@ -114,7 +113,10 @@ SIGNATURES = {
     "mzk_plonk_key_destroy": (_i32, [_vp]),
     "mzk_plonk_key_info": (_i32, [_vp, _u64p, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
     "mzk_plonk_key_commitments": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p]),
+    "mzk_plonk_key_srs": (_i32, [_vp, ctypes.c_void_p]),
     "mzk_create_proofs": (_i32, [_vp, ctypes.c_void_p, _sz, _u32]),
+    "mzk_gen_config3_fixed_device": (_i32, [_vp, _u32, _u32, _u32, _u64, _vp]),
+    "mzk_gen_config3_witness_device": (_i32, [_vp, _u32, _u32, _u32, _u64, _vp, _vp, _vp, _vp]),
     "mzk_gen_rand_fr_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
     "mzk_gen_bases_g1_device": (_i32, [_vp, _u64, _u64, _sz, _vp]),
 }
@@ -147,6 +149,7 @@ class ProofJob(ctypes.Structure):
 
 PROVE_MSM_PER_CALL = 1  # MZK_PROVE_MSM_PER_CALL
 PROVE_NO_GRAPHS = 2  # MZK_PROVE_NO_GRAPHS
+PROVE_SELF_CHECK = 4  # MZK_PROVE_SELF_CHECK
 # the plain one-call-at-a-time form: every MSM its own call, every kernel its own launch
 PROVE_PLAIN = PROVE_MSM_PER_CALL | PROVE_NO_GRAPHS
 PROOF_CORE_COMMITMENTS = ["a", "b", "c", "m_delta", "z_delta", "Z_double_delta", "h", "H0", "H1", "H2", "H3"]
@@ -807,38 +810,35 @@ class EvaluationDomain:
 
 
 class ProvingServer:
-    """Proving service with continuous batching (mzk_server_*)."""
+    """Proving service with continuous batching over create_proof (mzk_server_*)."""
 
-    def __init__(self, ctx, max_batch=16, lanes=2, mem_budget_bytes=0, per_call=False):
+    def __init__(self, ctx, max_batch=16, lanes=2, mem_budget_bytes=0, per_call=False, flags=0):
         self.ctx = ctx
         h = _vp()
-        _check(lib().mzk_server_create(ctx.h, int(max_batch), int(lanes), int(mem_budget_bytes),
-                                       PROVE_PLAIN if per_call else 0, ctypes.byref(h)))
+        fl = flags | (PROVE_PLAIN if per_call else 0)
+        _check(lib().mzk_server_create(ctx.h, int(max_batch), int(lanes), int(mem_budget_bytes), fl,
+                                       ctypes.byref(h)))
         self.h = h.value
         ctx._servers.add(self)
-        self._keys = []
         self._held = {}
 
-    def add_key(self, domain, pk_desc):
-        self._keys.append((domain, pk_desc))
-        _check(lib().mzk_server_add_key(self.h, domain.h, ctypes.byref(pk_desc)))
-
-    def submit(self, k, job, keep=None):
-        """Queue one proof; `keep` (e.g. the job's witness DeviceBuffers) stays
-        referenced until the request's wait returns."""
+    def submit(self, key, advice, blinds):
+        """Queue one proof of `key` (a PlonkKey) over the advice columns (host
+        arrays or DeviceBuffers) and the blinding values; wait() returns its
+        transcript."""
+        req, keep, out = _proof_request(key, advice, blinds)
         t = np.zeros(1, np.uint64)
-        _check(lib().mzk_server_submit(self.h, int(k), ctypes.byref(job), _ptr(t)))
-        self._held[int(t[0])] = keep
+        _check(lib().mzk_server_submit(self.h, ctypes.byref(req), _ptr(t)))
+        self._held[int(t[0])] = (req, keep, out)
         return int(t[0])
 
     def wait(self, ticket):
-        out = np.zeros((len(PROOF_CORE_COMMITMENTS), 18), np.uint64)
         lat = ctypes.c_double()
         try:
-            _check(lib().mzk_server_wait(self.h, ticket, _ptr(out), ctypes.byref(lat)))
+            _check(lib().mzk_server_wait(self.h, ticket, ctypes.byref(lat)))
         finally:
-            self._held.pop(int(ticket), None)
-        return out, lat.value
+            held = self._held.pop(int(ticket), None)
+        return bytes(held[2]), lat.value
 
     def stats(self):
         w, p = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
@@ -894,7 +894,6 @@ class ProofRequest(ctypes.Structure):
                 ("blinds", ctypes.c_void_p), ("proof_out", ctypes.c_void_p)]
 
 
-PROVE_MSM_PER_CALL, PROVE_NO_GRAPHS, PROVE_SELF_CHECK = 1, 2, 4
 
 
 class Transcript:
@@ -1015,6 +1014,37 @@ class PlonkKey:
             pass
 
 
+class DevicePtr:
+    """A device address inside a larger DeviceBuffer (kept alive with it)."""
+
+    def __init__(self, buf, offset_bytes=0):
+        self.buf, self.ptr = buf, _dptr(buf) + int(offset_bytes)
+
+
+def _proof_request(key, advice, blinds):
+    """A ProofRequest with the buffers it points to (kept alive by the caller)."""
+    on_dev = isinstance(advice[0], (DeviceBuffer, DevicePtr))
+    keep = [key]
+    if on_dev:
+        ptrs = (ctypes.c_void_p * len(advice))(*[a.ptr for a in advice])
+        keep.extend(advice)
+    else:
+        cols = [np.ascontiguousarray(a, np.uint64) for a in advice]
+        keep.extend(cols)
+        ptrs = (ctypes.c_void_p * len(cols))(*[c.ctypes.data for c in cols])
+    if len(advice) != key.circuit["n_advice"]:
+        raise MzkError(1, f"create_proof: {key.circuit['n_advice']} advice columns expected, got {len(advice)}")
+    bl = np.ascontiguousarray(blinds, np.uint64).reshape(-1, 4)
+    if bl.shape[0] != key.n_blinds:
+        raise MzkError(1, f"create_proof: {key.n_blinds} blinding values expected, got {bl.shape[0]}")
+    out = (ctypes.c_uint8 * key.proof_len)()
+    keep.extend([ptrs, bl])
+    req = ProofRequest()
+    req.key, req.advice, req.advice_on_device = key.h, ctypes.addressof(ptrs), 1 if on_dev else 0
+    req.blinds, req.proof_out = bl.ctypes.data, ctypes.addressof(out)
+    return req, keep, out
+
+
 def create_proofs(ctx, jobs, flags=0):
     """create_proof (proofs/src/plonk/prover.rs:432-473) for many proofs in
     one call.  jobs: [(PlonkKey, advice columns, blinds)] where the advice
@@ -1024,23 +1054,95 @@ def create_proofs(ctx, jobs, flags=0):
     reqs = (ProofRequest * max(1, len(jobs)))()
     keep, outs = [], []
     for i, (key, advice, blinds) in enumerate(jobs):
-        on_dev = isinstance(advice[0], DeviceBuffer)
-        if on_dev:
-            ptrs = (ctypes.c_void_p * len(advice))(*[a.ptr for a in advice])
-        else:
-            cols = [np.ascontiguousarray(a, np.uint64) for a in advice]
-            keep.extend(cols)
-            ptrs = (ctypes.c_void_p * len(cols))(*[c.ctypes.data for c in cols])
-        bl = np.ascontiguousarray(blinds, np.uint64).reshape(-1, 4)
-        if bl.shape[0] != key.n_blinds:
-            raise MzkError(1, f"create_proof: {key.n_blinds} blinding values expected, got {bl.shape[0]}")
-        out = (ctypes.c_uint8 * key.proof_len)()
-        keep.extend([ptrs, bl])
+        req, kp, out = _proof_request(key, advice, blinds)
+        reqs[i] = req
+        keep.append(kp)
         outs.append(out)
-        reqs[i].key, reqs[i].advice, reqs[i].advice_on_device = key.h, ctypes.addressof(ptrs), 1 if on_dev else 0
-        reqs[i].blinds, reqs[i].proof_out = bl.ctypes.data, ctypes.addressof(out)
     _check(lib().mzk_create_proofs(ctx.h, reqs, len(jobs), flags))
     return [bytes(o) for o in outs]
+
+
+CONFIG3_DEGREE = 5
+
+
+def config3_circuit(k):
+    """The single-proof configuration's constraint system (standard gate over
+    advice a, b, c and fixed q_l, q_r, q_m, q_o, q_c; permutation over a, b, c;
+    one lookup of a into the fixed table column 5 with the fixed selector 6;
+    degree 5, set_minimum_degree(5) of proofs/benches/plonk.rs:191) as the
+    dict PlonkKey takes; blinding_factors as ConstraintSystem::blinding_factors
+    (plonk/circuit.rs:2203-2245) gives it: max(3, 1) + 1 helper + 3 = 7."""
+    return {"k": k, "degree": CONFIG3_DEGREE, "blinding_factors": 7, "n_advice": 3, "n_fixed": 7,
+            "advice_queries": [(0, 0), (1, 0), (2, 0)], "fixed_queries": [(i, 0) for i in range(7)],
+            "gate_fixed": [0, 1, 2, 3, 4], "gate_advice": [0, 1, 2],
+            "perm_cols": [(0, 0), (0, 1), (0, 2)], "lookups": [{"input": 0, "table": 5, "selector": 6}]}
+
+
+def copy_cycles(n, usable, seed, fraction=0.10):
+    """Seeded copy cycles of 2 to 4 cells over `fraction` of the a and b cells
+    of the usable rows: (mapping (3, n, 2) uint32, each cell's (column, row)
+    successor in its cycle, identity elsewhere, as Assembly::mapping gives
+    build_pk; cycle_of (2n,) uint32, the cycle of each a then b cell,
+    0xffffffff outside cycles)."""
+    rng = np.random.default_rng(seed)
+    m = int(fraction * 2 * usable)
+    cells = rng.permutation(2 * usable)[:m]
+    lens = rng.integers(2, 5, size=m // 2 + 1)
+    ends = np.cumsum(lens)
+    lens = lens[ends <= m]
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.int64)
+    total = int(lens.sum())
+    cyc = np.repeat(np.arange(len(lens)), lens)
+    first = np.repeat(starts, lens)
+    pos = np.arange(total) - first
+    nxt = cells[first + (pos + 1) % np.repeat(lens, lens)]
+    cur = cells[:total]
+    mapping = np.zeros((3, n, 2), np.uint32)
+    mapping[:, :, 0] = np.arange(3, dtype=np.uint32)[:, None]
+    mapping[:, :, 1] = np.arange(n, dtype=np.uint32)[None, :]
+    mapping[cur // usable, cur % usable, 0] = nxt // usable
+    mapping[cur // usable, cur % usable, 1] = nxt % usable
+    cycle_of = np.full(2 * n, 0xFFFFFFFF, np.uint32)
+    cycle_of[(cur // usable) * n + cur % usable] = cyc
+    return mapping, cycle_of
+
+
+class Config3Instance:
+    """A seeded instance of the single-proof configuration's circuit on the
+    device (benchmarks): the fixed columns (mzk_gen_config3_fixed_device), copy
+    cycles, the proving key over `srs` (an SrsDesc), and fresh satisfying
+    witnesses per request (mzk_gen_config3_witness_device)."""
+
+    def __init__(self, ctx, domain, srs, seed, table_rows=1 << 16, pinned=b"config-3 circuit"):
+        k = domain.k
+        self.ctx, self.domain, self.k, self.n = ctx, domain, k, domain.n
+        self.circuit = config3_circuit(k)
+        bf = self.bf = self.circuit["blinding_factors"]
+        n, self.table_rows = domain.n, table_rows
+        self.fixed = ctx.alloc(7 * n * 32)
+        _check(lib().mzk_gen_config3_fixed_device(ctx.h, k, bf, table_rows, seed, self.fixed.ptr))
+        host = self.fixed.download((7, n, 4))
+        self.inv_qo = ctx.alloc(n * 32)
+        self.inv_qo.upload(host[3])
+        ctx.batch_invert_device(self.inv_qo, n)
+        mapping, cycle_of = copy_cycles(n, n - bf - 1, seed)
+        self.cycle_of = ctx.alloc(cycle_of.nbytes)
+        self.cycle_of.upload(cycle_of)
+        self.key = PlonkKey(ctx, domain, self.circuit, srs, [host[i] for i in range(7)], mapping, pinned)
+
+    def witness(self, seed):
+        """A fresh witness: a DeviceBuffer of a | b | c and the three column pointers."""
+        buf = self.ctx.alloc(3 * self.n * 32)
+        _check(lib().mzk_gen_config3_witness_device(self.ctx.h, self.k, self.bf, self.table_rows, seed,
+                                                    self.fixed.ptr, self.inv_qo.ptr, self.cycle_of.ptr, buf.ptr))
+        return [DevicePtr(buf, i * self.n * 32) for i in range(3)]
+
+    def blinds(self, seed):
+        """n_blinds uniform Fr (Montgomery) from a seeded stream."""
+        out = np.empty((self.key.n_blinds, 4), np.uint64)
+        buf = self.ctx.alloc(out.nbytes)
+        self.ctx.gen_rand_fr(seed, self.key.n_blinds, out=buf)
+        return buf.download(out.shape)
 
 
 def msm_pick_window(n):

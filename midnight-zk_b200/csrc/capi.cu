@@ -455,6 +455,35 @@ int mzk_gen_bases_g1_device(mzk_ctx* ctx, uint64_t seed, uint64_t first, size_t 
     return mzk::OK;
 }
 
+int mzk_gen_config3_fixed_device(mzk_ctx* ctx, uint32_t k, uint32_t blinding_factors, uint32_t table_rows,
+                                 uint64_t seed, uint64_t* d_fixed) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d_fixed || k < 3 || k > 26 || blinding_factors + 2 >= (1u << k) || table_rows == 0) {
+        mzk::set_error("gen_config3_fixed: bad argument");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    MZK_TRY(mzk::gen_config3_fixed(&ctx->impl, k, blinding_factors, table_rows, seed, d_fixed, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
+int mzk_gen_config3_witness_device(mzk_ctx* ctx, uint32_t k, uint32_t blinding_factors, uint32_t table_rows,
+                                   uint64_t seed, const uint64_t* d_fixed, const uint64_t* d_inv_qo,
+                                   const uint32_t* d_cycle_of, uint64_t* d_advice) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d_fixed || !d_inv_qo || !d_cycle_of || !d_advice || k < 3 || k > 26 || blinding_factors + 2 >= (1u << k) ||
+        table_rows == 0) {
+        mzk::set_error("gen_config3_witness: bad argument");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    MZK_TRY(mzk::gen_config3_witness(&ctx->impl, k, blinding_factors, table_rows, seed, d_fixed, d_inv_qo, d_cycle_of,
+                                     d_advice, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
 // ---- EvaluationDomain -----------------------------------------------------
 
 int mzk_domain_create(mzk_ctx* ctx, uint32_t j, uint32_t k, mzk_domain** out) {

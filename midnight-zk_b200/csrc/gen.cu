@@ -8,7 +8,9 @@
 //   uniform Fr: rejection sampling as Fq::random (curves/src/bls12_381/
 //               fq.rs:382-396), attempt a of element i uses words (i*64+a)*4..+3
 //   bases: [r_i]G by an 8-bit fixed-base table of the generator G
-//          (curves/README.md:96-101), normalised to affine per point.
+//          (curves/README.md:96-101), normalised to affine per point;
+//   the fixed columns and witnesses of the single-proof configuration's
+//          circuit (standard gate, copy cycles, range lookup).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -126,7 +128,85 @@ Status ensure_gen_table(Context* ctx) {
     return OK;
 }
 
+// small integer v < 2^32 in Montgomery form
+__device__ __forceinline__ Fr fr_small(uint32_t v) {
+    Fr r = fr_zero();
+    r.l[0] = v;
+    return fr_to_mont(r);
+}
+
+// fixed columns of the single-proof configuration's circuit (one buffer of
+// 7 x n): q_l, q_r, q_m, q_o, q_c uniform on the usable rows (q_o never zero)
+// and zero after, the table 0 .. table_rows - 1 then zeros, the lookup
+// selector one on the usable rows
+__global__ void k_cfg3_fixed(uint64_t seed, uint32_t n, uint32_t u, uint32_t table_rows, Fr* __restrict__ f) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        for (uint32_t j = 0; j < 5; j++) {
+            Fr v = fr_zero();
+            if (i < u) {
+                v = fr_to_mont(rand_fr_canonical(seed + j, i));
+                if (j == 3) {
+                    uint32_t acc = 0;
+                    for (int w = 0; w < 8; w++) acc |= v.l[w];
+                    if (acc == 0) v = fr_one();
+                }
+            }
+            f[(size_t)j * n + i] = v;
+        }
+        f[(size_t)5 * n + i] = i < table_rows ? fr_small(i) : fr_zero();
+        f[(size_t)6 * n + i] = i < u ? fr_one() : fr_zero();
+    }
+}
+
+// a witness of that circuit: a a table value, b uniform, every cell of one
+// copy cycle the cycle's table value, c = -(q_l a + q_r b + q_m a b + q_c) / q_o
+__global__ void k_cfg3_witness(uint64_t seed, uint32_t n, uint32_t u, uint32_t table_rows, const Fr* __restrict__ f,
+                               const Fr* __restrict__ inv_qo, const uint32_t* __restrict__ cycle_of,
+                               Fr* __restrict__ adv) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t kNone = 0xffffffffu;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Fr a = fr_zero(), b = fr_zero(), c = fr_zero();
+        if (i < u) {
+            const uint32_t ca = cycle_of[i], cb = cycle_of[(size_t)n + i];
+            const uint64_t ra = ca != kNone ? rand64(seed, (1ull << 40) + ca) : rand64(seed, i);
+            a = fr_small((uint32_t)(ra % table_rows));
+            b = cb != kNone ? fr_small((uint32_t)(rand64(seed, (1ull << 40) + cb) % table_rows))
+                            : fr_to_mont(rand_fr_canonical(seed ^ 0xB0B0B0B0ull, i));
+            Fr t = fr_mul(f[i], a);
+            t = fr_add(t, fr_mul(f[(size_t)n + i], b));
+            t = fr_add(t, fr_mul(fr_mul(f[(size_t)2 * n + i], a), b));
+            t = fr_add(t, f[(size_t)4 * n + i]);
+            c = fr_sub(fr_zero(), fr_mul(t, inv_qo[i]));
+        }
+        adv[i] = a;
+        adv[(size_t)n + i] = b;
+        adv[(size_t)2 * n + i] = c;
+    }
+}
+
 }  // namespace
+
+Status gen_config3_fixed(Context* ctx, uint32_t k, uint32_t bf, uint32_t table_rows, uint64_t seed, void* d_fixed,
+                         cudaStream_t st) {
+    const uint32_t n = 1u << k, u = n - bf - 1;
+    const uint32_t blocks = (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 32);
+    k_cfg3_fixed<<<blocks, 256, 0, st>>>(seed, n, u, std::min(table_rows, u), static_cast<Fr*>(d_fixed));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
+Status gen_config3_witness(Context* ctx, uint32_t k, uint32_t bf, uint32_t table_rows, uint64_t seed,
+                           const void* d_fixed, const void* d_inv_qo, const uint32_t* d_cycle_of, void* d_advice,
+                           cudaStream_t st) {
+    const uint32_t n = 1u << k, u = n - bf - 1;
+    const uint32_t blocks = (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 32);
+    k_cfg3_witness<<<blocks, 256, 0, st>>>(seed, n, u, std::min(table_rows, u), static_cast<const Fr*>(d_fixed),
+                                           static_cast<const Fr*>(d_inv_qo), d_cycle_of, static_cast<Fr*>(d_advice));
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
 
 Status gen_rand_fr(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t st) {
     if (n == 0) return OK;

@@ -838,6 +838,14 @@ const Fr* open_poly(const FsProof& p, std::pair<int, uint32_t> id) {
 
 }  // namespace
 
+// device bytes one proof of `key` takes in a call: its carved buffers plus
+// the sorted MSM entries it adds to the largest batched MSM of a phase
+uint64_t proof_device_bytes(const mzk_plonk_key* key) {
+    const PlonkKey* k = reinterpret_cast<const PlonkKey*>(key);
+    const uint64_t msm_entries = (uint64_t)std::max<uint32_t>(k->n_advice, k->qdeg) * k->n * 20;
+    return (proof_scratch_elems(k) + 8) * sizeof(Fr) + msm_entries * 4;
+}
+
 Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, uint32_t flags, cudaStream_t st) {
     using namespace host;
     if (count == 0) return OK;
@@ -1416,6 +1424,12 @@ int mzk_plonk_key_commitments(const mzk_plonk_key* key, uint64_t* fixed, uint64_
         for (size_t i = 0; i < k->fixed_coms.size(); i++) std::memcpy(fixed + 18 * i, k->fixed_coms[i].data(), 144);
     if (perm)
         for (size_t i = 0; i < k->perm_coms.size(); i++) std::memcpy(perm + 18 * i, k->perm_coms[i].data(), 144);
+    return mzk::OK;
+}
+
+int mzk_plonk_key_srs(const mzk_plonk_key* key, mzk_srs_desc* out) {
+    if (!key || !out) return mzk::ERR_ARG;
+    *out = reinterpret_cast<const mzk::PlonkKey*>(key)->srs;
     return mzk::OK;
 }
 

@@ -102,6 +102,9 @@ Status run_msms(Context* ctx, const void* srs, uint64_t srs_len, const std::vect
 // once into a CUDA graph per pointer set and replayed when use_graph is set
 Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag, Fr* const* coeff, Fr* const* ext,
                     int count, bool use_graph, cudaStream_t st);
+// create_proof with the Fiat-Shamir transcript (plonk.cu)
+Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, uint32_t flags, cudaStream_t st);
+uint64_t proof_device_bytes(const mzk_plonk_key* key);
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st);
 

@@ -183,5 +183,12 @@ Status gen_rand_fr(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* 
 // [s_i]G for n device scalars (Montgomery) into n device affine points
 Status fixed_base_g1(Context* ctx, const void* d_scalars, size_t n, void* d_out, cudaStream_t st);
 Status gen_bases_g1(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t stream);
+// the single-proof configuration's circuit: 7 fixed columns (one device
+// buffer of 7 x 2^k) and a satisfying witness a, b, c (3 x 2^k)
+Status gen_config3_fixed(Context* ctx, uint32_t k, uint32_t bf, uint32_t table_rows, uint64_t seed, void* d_fixed,
+                         cudaStream_t st);
+Status gen_config3_witness(Context* ctx, uint32_t k, uint32_t bf, uint32_t table_rows, uint64_t seed,
+                           const void* d_fixed, const void* d_inv_qo, const uint32_t* d_cycle_of, void* d_advice,
+                           cudaStream_t st);
 
 }  // namespace mzk

@@ -11,9 +11,12 @@ from oracle import plonk as OP
 mzk = load()
 
 
+# stands for format!("{:?}", domain.pinned()) + format!("{:?}", cs.pinned())
+PINNED = b"config-3 circuit: standard gate, copy cycles, range lookup"
+
+
 class Circuit:
-    def __init__(self, ctx, k, seed, pinned=b"config-3 circuit: standard gate, copy cycles, range lookup",
-                 oracle=True, srs=None):
+    def __init__(self, ctx, k, seed, pinned=PINNED, oracle=True, srs=None):
         """srs = (buffer, offsets) of a shared device SRS whose bases hold this
         k's g | lagrange | delta | double delta at the offsets; otherwise
         this circuit gets its own."""

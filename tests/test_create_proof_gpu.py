@@ -142,3 +142,29 @@ def test_lookup_input_outside_the_table_is_refused(k5):
 def test_wrong_blind_count_is_refused(k5):
     with pytest.raises(mzk.MzkError):
         mzk.create_proofs(k5.ctx, [(k5.key, k5.advice, k5.blinds(1)[:-1])])
+
+
+def test_device_generated_config3_instance_verifies(ctx):
+    """The benchmark's device-generated instances (mzk_gen_config3_*): the
+    fixed columns, copy cycles and a fresh witness satisfy the circuit (the
+    self-check passes), and the proof is the oracle's transcript and verifies."""
+    from oracle import oracle as O
+    k = 10
+    dom = mzk.EvaluationDomain(ctx, 5, k)
+    n = dom.n
+    s = O.rand_fr(99, 1)[0]
+    buf = ctx.alloc(4 * n * 96)
+    dom.srs_setup_device(s, buf.ptr, buf.ptr + n * 96, buf.ptr + 2 * n * 96, buf.ptr + 3 * n * 96)
+    desc = mzk.SrsDesc(buf.ptr, 4 * n, 0, n, 2 * n, 3 * n, 0, 0, 0)
+    inst = mzk.Config3Instance(ctx, dom, desc, seed=3, table_rows=300)
+    wit, bl = inst.witness(5), inst.blinds(6)
+    proof = mzk.create_proofs(ctx, [(inst.key, wit, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    host = buf.download((4 * n, 12))
+    srs = {"g": host[:n], "lagrange": host[n:2 * n], "delta": host[2 * n:3 * n], "double_delta": host[3 * n:]}
+    mapping = mzk.copy_cycles(n, n - 8, 3)[0]
+    okey = OP.keygen(OP.config3_circuit(k), list(inst.fixed.download((7, n, 4))), mapping, srs, b"config-3 circuit")
+    adv = list(wit[0].buf.download((3, n, 4)))
+    assert OP.create_proof(okey, adv, [OP.to_int(v) for v in bl]) == proof
+    assert OP.verify(okey, proof, OP.to_int(s))
+    # a second fresh witness also satisfies the circuit
+    assert mzk.create_proofs(ctx, [(inst.key, inst.witness(7), inst.blinds(8))], flags=mzk.PROVE_SELF_CHECK)

@@ -107,23 +107,22 @@ def test_bad_tables_are_refused(ctx):
 
 
 def test_served_proofs_over_a_table_equal_the_untabled_proof(ctx):
-    """The proving service with a key whose SRS is a window table: every
-    result equals the same proof run alone without the table."""
-    st = Setup(ctx, 8, seed=91)
-    jobs = [st.job(s)[0] for s in (92, 93, 94)]
-    want = [st.g.prove_core_device(st.pk, [j])[0] for j in jobs]
+    """create_proof through the proving service with a key whose SRS is a
+    window table: every transcript equals the same proof with the key over
+    the plain SRS (and the oracle's)."""
+    from _plonk_setup import PINNED, Circuit
+    c8 = Circuit(ctx, 8, seed=91)
+    n = c8.n
+    blinds = [c8.blinds(s) for s in (92, 93, 94)]
+    want = [mzk.create_proofs(ctx, [(c8.key, c8.advice, b)])[0] for b in blinds]
     c = 16
-    t, rows = make_table(ctx, st.srs, c)
-    pk = st.pk
-    saved = (pk.srs, pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n)
-    pk.srs, pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n = t.ptr, c, rows, 1
-    try:
-        srv = mzk.ProvingServer(ctx, max_batch=4)
-        srv.add_key(st.g, pk)
-        tickets = [srv.submit(8, j) for j in jobs]
-        outs = [srv.wait(tk)[0] for tk in tickets]
-        srv.close()
-    finally:
-        pk.srs, pk.srs_table_c, pk.srs_table_rows, pk.srs_table_min_n = saved
-    for o, w in zip(outs, want):
-        assert np.array_equal(o, w)
+    t, rows = make_table(ctx, c8.srs_buf.download((4 * n, 12)), c)
+    desc = mzk.SrsDesc(t.ptr, 4 * n, 0, n, 2 * n, 3 * n, c, rows, 1)
+    key = mzk.PlonkKey(ctx, c8.dom, c8.circuit, desc, c8.fixed, c8.mapping, PINNED)
+    assert np.array_equal(key.fixed_coms, c8.key.fixed_coms) and np.array_equal(key.repr, c8.key.repr)
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    tickets = [srv.submit(key, c8.advice, b) for b in blinds]
+    outs = [srv.wait(tk)[0] for tk in tickets]
+    srv.close()
+    assert outs == want
+    assert outs[0] == c8.oracle_proof(c8.advice, blinds[0])

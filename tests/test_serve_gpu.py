@@ -1,13 +1,13 @@
-"""The proving service (continuous batching over the proof core): every
-result is the one the same proof gets alone, whatever wave it lands in and
-whatever mix of sizes shares that wave; the plain mode and the memory budget
-run one proof per wave; bad requests are refused."""
+"""The proving service (continuous batching over create_proof): every
+transcript is the one the same proof gets alone, whatever wave it lands in and
+whatever mix of sizes shares that wave, and it is the oracle's and verifies;
+the plain mode and the memory budget run one proof per wave; bad requests are
+refused."""
 import threading
 
-import numpy as np
 import pytest
 
-from _proof_setup import Setup, mzk
+from _plonk_setup import Circuit, mzk
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -22,30 +22,38 @@ def ctx():
 
 @pytest.fixture(scope="module")
 def keys(ctx):
-    """Keys for k = 5 and k = 7 whose bases live in ONE SRS buffer:
-    [g (2^7) | lagrange_7 | delta_7 | double_delta_7 | lagrange_5 | delta_5 | double_delta_5]."""
-    n7, n5 = 1 << 7, 1 << 5
-    srs = O.gen_bases(77, 4 * n7 + 3 * n5)
-    buf = ctx.alloc(srs.nbytes)
-    buf.upload(srs)
-    k7 = Setup(ctx, 7, seed=11, shared=(srs, buf.ptr, (0, n7, 2 * n7, 3 * n7)))
-    k5 = Setup(ctx, 5, seed=12, shared=(srs, buf.ptr, (0, 4 * n7, 4 * n7 + n5, 4 * n7 + 2 * n5)))
-    return {5: k5, 7: k7, "buf": buf}
+    """Keys for k = 5 and k = 7 whose bases live in ONE SRS buffer, each k's
+    g | lagrange | delta | double delta at its own offsets."""
+    s = O.rand_fr(777, 1)[0]
+    sizes = {7: 1 << 7, 5: 1 << 5}
+    total = sum(4 * n for n in sizes.values())
+    buf = ctx.alloc(total * 96)
+    out, at = {"buf": buf}, 0
+    for k, n in sizes.items():
+        dom = mzk.EvaluationDomain(ctx, 5, k)
+        p = buf.ptr + at * 96
+        dom.srs_setup_device(s, p, p + n * 96, p + 2 * n * 96, p + 3 * n * 96)
+        dom.close()
+        offs = (at, at + n, at + 2 * n, at + 3 * n)
+        at += 4 * n
+        out[k] = offs
+    for k in sizes:
+        d = mzk.SrsDesc(buf.ptr, total, *out[k], 0, 0, 0)
+        out[k] = Circuit(ctx, k, seed=40 + k, srs=(buf, out[k], d, s))
+    return out
 
 
-def alone(setup, job):
-    return setup.g.prove_core_device(setup.pk, [job])[0]
+def alone(ctx, c, blinds):
+    return mzk.create_proofs(ctx, [(c.key, c.advice, blinds)])[0]
 
 
 def test_mixed_waves_equal_alone_and_oracle(ctx, keys):
     srv = mzk.ProvingServer(ctx, max_batch=8)
-    for k in (5, 7):
-        srv.add_key(keys[k].g, keys[k].pk)
-    jobs = [(k, keys[k].job(100 + i)) for i, k in enumerate([5, 7, 7, 5, 5, 7, 5, 7, 7, 5])]
+    jobs = [(keys[k], keys[k].blinds(100 + i)) for i, k in enumerate([5, 7, 7, 5, 5, 7, 5, 7, 7, 5])]
     results = {}
 
     def client(part):
-        tickets = [(i, srv.submit(k, jb[0])) for i, (k, jb) in part]
+        tickets = [(i, srv.submit(c.key, c.advice, bl)) for i, (c, bl) in part]
         for i, t in tickets:
             results[i] = srv.wait(t)
 
@@ -57,40 +65,43 @@ def test_mixed_waves_equal_alone_and_oracle(ctx, keys):
     stats = srv.stats()
     srv.close()
     assert stats["proofs"] == len(jobs) and 1 <= stats["waves"] <= len(jobs)
-    for i, (k, (job, w, ch, blinds)) in enumerate(jobs):
-        out, lat = results[i]
+    for i, (c, bl) in enumerate(jobs):
+        proof, lat = results[i]
         assert lat > 0
-        assert np.array_equal(out, alone(keys[k], job)), i
-    # one proof of each size against the oracle's step-by-step commitments
-    for i in (0, 1):
-        k, (job, w, ch, blinds) = jobs[i]
-        expect = keys[k].oracle(w, ch, blinds)
-        for ci in range(len(mzk.PROOF_CORE_COMMITMENTS)):
-            assert np.array_equal(mzk.affine(results[i][0][ci]), expect[ci]), (k, ci)
+        assert proof == alone(ctx, c, bl), i
+    for i in (0, 1):                      # one proof of each size: the oracle's transcript, accepted
+        c, bl = jobs[i]
+        assert results[i][0] == c.oracle_proof(c.advice, bl)
+        assert c.verify(results[i][0])
 
 
 @pytest.mark.parametrize("mode", ["plain", "budget"])
 def test_one_proof_per_wave(ctx, keys, mode):
     srv = (mzk.ProvingServer(ctx, max_batch=1, lanes=1, per_call=True) if mode == "plain"
            else mzk.ProvingServer(ctx, max_batch=16, mem_budget_bytes=1))
-    srv.add_key(keys[7].g, keys[7].pk)
-    jobs = [keys[7].job(200 + i)[0] for i in range(4)]
-    tickets = [srv.submit(7, j) for j in jobs]
+    c = keys[7]
+    bls = [c.blinds(200 + i) for i in range(4)]
+    tickets = [srv.submit(c.key, c.advice, bl) for bl in bls]
     outs = [srv.wait(t)[0] for t in tickets]
     stats = srv.stats()
     srv.close()
     assert stats == {"waves": 4, "proofs": 4, "busy_ms": stats["busy_ms"]}
-    for j, o in zip(jobs, outs):
-        assert np.array_equal(o, alone(keys[7], j))
+    for bl, o in zip(bls, outs):
+        assert o == alone(ctx, c, bl)
 
 
 def test_bad_requests_are_refused(ctx, keys):
     srv = mzk.ProvingServer(ctx, max_batch=4)
-    srv.add_key(keys[5].g, keys[5].pk)
+    c = keys[5]
     with pytest.raises(mzk.MzkError):
-        srv.submit(9, keys[5].job(300)[0])  # no key for k = 9
+        srv.submit(c.key, c.advice, c.blinds(1)[:-2])      # wrong number of blinding values
     with pytest.raises(mzk.MzkError):
-        srv.wait(12345)  # unknown ticket
-    with pytest.raises(mzk.MzkError):
-        srv.add_key(keys[7].g, keys[5].pk)  # key and domain sizes differ
+        srv.wait(12345)                                    # unknown ticket
+    # a failing request (a lookup input outside the table) reports its error and the service goes on
+    bad = [a.copy() for a in c.advice]
+    bad[0][0] = O.rand_fr(5, 1)[0]
+    t_bad = srv.submit(c.key, bad, c.blinds(2))
+    with pytest.raises(mzk.MzkError, match="not in the table"):
+        srv.wait(t_bad)
+    assert srv.wait(srv.submit(c.key, c.advice, c.blinds(3)))[0] == alone(ctx, c, c.blinds(3))
     srv.close()
