@@ -169,7 +169,11 @@ def measure_ntt(mzk, ctx, stream, log_n, reps):
     return out
 
 
-def measure_quotient(mzk, ctx, stream, k, reps):
+QUOTIENT_FR_MUL_PER_ROW = 37   # counted on the oracle's evaluate_numerator restatement (tests/test_plonk_oracle.py)
+IMAD_PER_FR_MUL = 272          # CIOS, 8 limbs: 2*8^2+8 = 136 products x (lo, hi)
+
+
+def measure_quotient(mzk, ctx, stream, k, reps, imad_peak):
     """Fused quotient evaluation for the k-row proof circuit (extended 2^(k+2) rows)."""
     import torch
     E = 1 << (k + 2)
@@ -226,7 +230,10 @@ def measure_quotient(mzk, ctx, stream, k, reps):
     e1.synchronize()
     ms_prog = e0.elapsed_time(e1) / reps
     dom.close()
+    imad = QUOTIENT_FR_MUL_PER_ROW * IMAD_PER_FR_MUL * E / (ms / 1e3)
     return {"rows": E, "ms": round(ms, 3), "rows_per_s": round(E / (ms / 1e3), 1),
+            "fr_mul_per_row": QUOTIENT_FR_MUL_PER_ROW, "imad_t_per_s": round(imad / 1e12, 3),
+            "imad_frac": round(imad / imad_peak, 4),
             "hbm_gbs_algorithmic": round((ncols + 1) * 32 * E / (ms / 1e3) / 1e9, 1),
             "columns_read": ncols,
             "as_programs_ms": round(ms_prog, 3),
@@ -721,7 +728,7 @@ def run_ours(args):
     if not args.no_extras:
         del ds, db
         extra_ntt = measure_ntt(mzk, ctx, stream, args.ntt_log_n, 5)
-        extra_q = measure_quotient(mzk, ctx, stream, 18, 5)
+        extra_q = measure_quotient(mzk, ctx, stream, 18, 5, imad_peak)
         if not args.no_prover:
             extra_prover["batched_msm"] = measure_batched_msm(mzk, ctx, 3)
             keys = PlonkKeys(mzk, ctx, SERVE_KS)

@@ -383,9 +383,13 @@ typedef struct { uint32_t column; int32_t rotation; } mzk_query;
  * rotation 0) and whose table expression is one fixed column, with a fixed
  * selector column or none (selector_fixed = -1: the constant one). */
 typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } mzk_lookup_shape;
-/* The constraint system a key is built for.  Gates: the standard gate
- * q_l a + q_r b + q_m a b + q_o c + q_c over fixed columns gate_fixed and
- * advice columns gate_advice (every column it reads queried at rotation 0).
+/* The constraint system a key is built for.  Gates: any custom gates as the
+ * reference flattens them (`gates`, an mzk_flat_graph whose result is the
+ * Horner-in-y combination of every gate polynomial, evaluation.rs:148-213;
+ * every (column, rotation) it reads must be in the query lists), or, with
+ * gates null, the standard gate q_l a + q_r b + q_m a b + q_o c + q_c over
+ * fixed columns gate_fixed and advice columns gate_advice (each queried at
+ * rotation 0).
  * Permutation columns: kind 0 advice, 1 fixed; sets of degree - 2 columns.
  * The query lists and their order are the reference's (they fix the order
  * of the evaluations in the proof).  Limits: 16 advice, 16 fixed, 16
@@ -398,6 +402,7 @@ typedef struct {
     const mzk_query *advice_queries; uint32_t n_advice_queries;
     const mzk_query *fixed_queries; uint32_t n_fixed_queries;
     uint32_t gate_fixed[5], gate_advice[3];
+    const mzk_flat_graph *gates;       /* null: the standard gate above */
     uint32_t n_perm_cols;
     const uint32_t *perm_col_kind, *perm_col_index;
     uint32_t n_lookups;

@@ -876,6 +876,7 @@ class CircuitDesc(ctypes.Structure):
                 ("advice_queries", ctypes.c_void_p), ("n_advice_queries", ctypes.c_uint32),
                 ("fixed_queries", ctypes.c_void_p), ("n_fixed_queries", ctypes.c_uint32),
                 ("gate_fixed", ctypes.c_uint32 * 5), ("gate_advice", ctypes.c_uint32 * 3),
+                ("gates", ctypes.c_void_p),
                 ("n_perm_cols", ctypes.c_uint32), ("perm_col_kind", ctypes.c_void_p),
                 ("perm_col_index", ctypes.c_void_p), ("n_lookups", ctypes.c_uint32), ("lookups", ctypes.c_void_p)]
 
@@ -975,8 +976,15 @@ class PlonkKey:
         cs.n_advice_queries = len(circuit["advice_queries"])
         cs.fixed_queries = arr(Query, [Query(c, r) for c, r in circuit["fixed_queries"]])
         cs.n_fixed_queries = len(circuit["fixed_queries"])
-        cs.gate_fixed[:] = circuit["gate_fixed"]
-        cs.gate_advice[:] = circuit["gate_advice"]
+        cs.gate_fixed[:] = circuit.get("gate_fixed", [0] * 5)
+        cs.gate_advice[:] = circuit.get("gate_advice", [0] * 3)
+        if circuit.get("gates") is not None:
+            g = circuit["gates"]
+            fg = g if isinstance(g, FlatGraph) else build_flat_graph(
+                g["constants"], g["rotations"], g["reads"], g["ops"], g["values_len"], g["beta_idx"],
+                g["theta_idx"], g["trash_challenge_idx"], g["y_idx"], g["previous_value_idx"], g["result_idx"])
+            keep.append(fg)
+            cs.gates = ctypes.addressof(fg)
         pc = circuit["perm_cols"]
         cs.n_perm_cols = len(pc)
         cs.perm_col_kind = arr(ctypes.c_uint32, [kd for kd, _ in pc])

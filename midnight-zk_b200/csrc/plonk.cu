@@ -235,6 +235,13 @@ struct PlonkKey {
     uint32_t n_advice = 0, n_fixed = 0, n_perm = 0;
     std::vector<mzk_query> advice_queries, fixed_queries;
     uint32_t gate_fixed[5] = {}, gate_advice[3] = {};
+    // custom gates as a flattened program (a validated copy), or the standard gate
+    bool has_gates = false;
+    std::vector<uint64_t> g_consts;
+    std::vector<int32_t> g_rots;
+    std::vector<mzk_column_read> g_reads;
+    std::vector<mzk_flat_op> g_ops;
+    mzk_flat_graph gates = {};
     std::vector<uint32_t> perm_kind, perm_index;
     bool has_lookup = false;
     mzk_lookup_shape lookup = {};
@@ -306,12 +313,43 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
             if (cs->fixed_queries[j].column == q.column && cs->fixed_queries[j].rotation == q.rotation)
                 return fail("duplicated fixed query");
     }
-    for (int i = 0; i < 5; i++)
-        if (!queried(cs->fixed_queries, cs->n_fixed_queries, cs->gate_fixed[i]))
-            return fail("a gate fixed column is not queried at rotation 0");
-    for (int i = 0; i < 3; i++)
-        if (!queried(cs->advice_queries, cs->n_advice_queries, cs->gate_advice[i]))
-            return fail("a gate advice column is not queried at rotation 0");
+    if (const mzk_flat_graph* g = cs->gates) {
+        // every index the host evaluation at x uses is checked here; the
+        // quotient checks the program again when it packs it
+        const uint32_t V = g->values_len;
+        if (V == 0 || V > kFlatMaxValues || g->n_constants > V || g->n_rotations > kFlatMaxRotations)
+            return fail("gates: bad values_len, constant count or rotation count");
+        if ((g->n_constants && !g->constants) || (g->n_rotations && !g->rotations) || (g->n_reads && !g->reads) ||
+            (g->n_ops && !g->ops))
+            return fail("gates: null array");
+        for (uint32_t idx : {g->beta_idx, g->theta_idx, g->trash_challenge_idx, g->y_idx, g->previous_value_idx,
+                             g->result_idx})
+            if (idx >= V) return fail("gates: slot index out of range");
+        for (uint32_t i = 0; i < g->n_reads; i++) {
+            const mzk_column_read& r = g->reads[i];
+            if (r.dst >= V || r.rot_idx >= g->n_rotations) return fail("gates: read index out of range");
+            const int32_t rot = g->rotations[r.rot_idx];
+            bool ok = false;
+            if (r.col_type == 0 || r.col_type == 1) {
+                const mzk_query* q = r.col_type == 0 ? cs->fixed_queries : cs->advice_queries;
+                const uint32_t nq = r.col_type == 0 ? cs->n_fixed_queries : cs->n_advice_queries;
+                for (uint32_t j = 0; j < nq; j++) ok = ok || (q[j].column == r.col_idx && q[j].rotation == rot);
+            }
+            if (!ok) return fail("gates: a read is not a fixed or advice query of the circuit");
+        }
+        for (uint32_t i = 0; i < g->n_ops; i++) {
+            const mzk_flat_op& o = g->ops[i];
+            if (o.kind > MZK_FLAT_MULADD || o.dst >= V || o.a >= V || o.b >= V || o.c >= V)
+                return fail("gates: op out of range");
+        }
+    } else {
+        for (int i = 0; i < 5; i++)
+            if (!queried(cs->fixed_queries, cs->n_fixed_queries, cs->gate_fixed[i]))
+                return fail("a gate fixed column is not queried at rotation 0");
+        for (int i = 0; i < 3; i++)
+            if (!queried(cs->advice_queries, cs->n_advice_queries, cs->gate_advice[i]))
+                return fail("a gate advice column is not queried at rotation 0");
+    }
     for (uint32_t i = 0; i < cs->n_perm_cols; i++) {
         const uint32_t kind = cs->perm_col_kind[i], col = cs->perm_col_index[i];
         if (kind > 1) return fail("permutation column kind must be 0 (advice) or 1 (fixed)");
@@ -446,6 +484,18 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     key->fixed_queries.assign(cs->fixed_queries, cs->fixed_queries + cs->n_fixed_queries);
     std::memcpy(key->gate_fixed, cs->gate_fixed, sizeof(key->gate_fixed));
     std::memcpy(key->gate_advice, cs->gate_advice, sizeof(key->gate_advice));
+    if (const mzk_flat_graph* g = cs->gates) {
+        key->has_gates = true;
+        key->g_consts.assign(g->constants, g->constants + 4 * (size_t)g->n_constants);
+        key->g_rots.assign(g->rotations, g->rotations + g->n_rotations);
+        key->g_reads.assign(g->reads, g->reads + g->n_reads);
+        key->g_ops.assign(g->ops, g->ops + g->n_ops);
+        key->gates = *g;
+        key->gates.constants = key->g_consts.data();
+        key->gates.rotations = key->g_rots.data();
+        key->gates.reads = key->g_reads.data();
+        key->gates.ops = key->g_ops.data();
+    }
     key->perm_kind.assign(cs->perm_col_kind, cs->perm_col_kind + P);
     key->perm_index.assign(cs->perm_col_index, cs->perm_col_index + P);
     key->has_lookup = cs->n_lookups == 1;
@@ -769,14 +819,48 @@ Fr4 identities_at_x(const FsProof& p) {
         return host::fr_zero();
     };
     std::vector<Fr4> ids;
-    // the standard gate
-    const Fr4 a = adv(k->gate_advice[0]), b = adv(k->gate_advice[1]), c = adv(k->gate_advice[2]);
-    Fr4 g = fr_mul(fix(k->gate_fixed[0]), a);
-    g = fr_add(g, fr_mul(fix(k->gate_fixed[1]), b));
-    g = fr_add(g, fr_mul(fr_mul(fix(k->gate_fixed[2]), a), b));
-    g = fr_add(g, fr_mul(fix(k->gate_fixed[3]), c));
-    g = fr_add(g, fix(k->gate_fixed[4]));
-    ids.push_back(g);
+    if (k->has_gates) {
+        // the flattened gates at x: each read is the evaluation of its query
+        // (partially_evaluate_identities evaluates the same expressions)
+        const mzk_flat_graph& g = k->gates;
+        std::vector<Fr4> val(g.values_len, host::fr_zero());
+        for (uint32_t i = 0; i < g.n_constants; i++) std::memcpy(val[i].l, g.constants + 4 * (size_t)i, 32);
+        val[g.beta_idx] = p.beta;
+        val[g.theta_idx] = p.theta;
+        val[g.trash_challenge_idx] = p.trash;
+        val[g.y_idx] = p.y;
+        val[g.previous_value_idx] = host::fr_zero();
+        for (uint32_t i = 0; i < g.n_reads; i++) {
+            const mzk_column_read& r = g.reads[i];
+            const auto& qs = r.col_type == 0 ? k->fixed_queries : k->advice_queries;
+            const auto& ev = r.col_type == 0 ? p.ev_fix : p.ev_adv;
+            for (size_t j = 0; j < qs.size(); j++)
+                if (qs[j].column == r.col_idx && qs[j].rotation == g.rotations[r.rot_idx]) val[r.dst] = ev[j];
+        }
+        for (uint32_t i = 0; i < g.n_ops; i++) {
+            const mzk_flat_op& o = g.ops[i];
+            const Fr4 &x = val[o.a], &y2 = val[o.b], &z = val[o.c];
+            switch (o.kind) {
+                case MZK_FLAT_ADD: val[o.dst] = fr_add(x, y2); break;
+                case MZK_FLAT_SUB: val[o.dst] = fr_sub(x, y2); break;
+                case MZK_FLAT_MUL: val[o.dst] = fr_mul(x, y2); break;
+                case MZK_FLAT_SQUARE: val[o.dst] = fr_mul(x, x); break;
+                case MZK_FLAT_DOUBLE: val[o.dst] = fr_add(x, x); break;
+                case MZK_FLAT_NEGATE: val[o.dst] = fr_neg(x); break;
+                default: val[o.dst] = fr_add(fr_mul(x, y2), z); break;
+            }
+        }
+        ids.push_back(val[g.result_idx]);
+    } else {
+        // the standard gate
+        const Fr4 a = adv(k->gate_advice[0]), b = adv(k->gate_advice[1]), c = adv(k->gate_advice[2]);
+        Fr4 g = fr_mul(fix(k->gate_fixed[0]), a);
+        g = fr_add(g, fr_mul(fix(k->gate_fixed[1]), b));
+        g = fr_add(g, fr_mul(fr_mul(fix(k->gate_fixed[2]), a), b));
+        g = fr_add(g, fr_mul(fix(k->gate_fixed[3]), c));
+        g = fr_add(g, fix(k->gate_fixed[4]));
+        ids.push_back(g);
+    }
     // l_last, l_blind, l_0 (l_i_range over -(bf + 1) ..= 0)
     const int32_t bf = (int32_t)k->bf;
     const Fr4 l_last = l_i(d, p.x, p.xn, -(bf + 1));
@@ -1104,6 +1188,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         q.n_fixed = k->n_fixed;
         std::memcpy(q.gate_fixed, k->gate_fixed, sizeof(q.gate_fixed));
         std::memcpy(q.gate_advice, k->gate_advice, sizeof(q.gate_advice));
+        q.gates = k->has_gates ? &k->gates : nullptr;
         q.n_perm_cols = k->n_perm;
         q.perm_col_kind = k->perm_kind.data();
         q.perm_col_index = k->perm_index.data();

@@ -166,7 +166,14 @@ __attribute__((constructor)) static void oracle_ctor(void) { init_consts(); }
 /* ------------------------------------------------------------------------- */
 /* Fr                                                                        */
 /* ------------------------------------------------------------------------- */
-static inline void fr_mul(u64 *o, const u64 *a, const u64 *b) { mont_mul_n(o, a, b, FR_MOD, FR_INV, 4); }
+/* Fr multiplications counted while counting is on (single-threaded runs
+ * only: the work figures of the quotient evaluation come from this count) */
+static int g_fr_count_on;
+static unsigned long long g_fr_mul_count;
+static inline void fr_mul(u64 *o, const u64 *a, const u64 *b) {
+    if (g_fr_count_on) g_fr_mul_count++;
+    mont_mul_n(o, a, b, FR_MOD, FR_INV, 4);
+}
 static inline void fr_add(u64 *o, const u64 *a, const u64 *b) { mod_add_n(o, a, b, FR_MOD, 4); }
 static inline void fr_sub(u64 *o, const u64 *a, const u64 *b) { mod_sub_n(o, a, b, FR_MOD, 4); }
 static void fr_pow(u64 *o, const u64 *a, const u64 *e, int elimbs) {
@@ -1403,6 +1410,14 @@ void or_poly_inner_product(const uint64_t *const *polys, const size_t *lens, siz
         }
 }
 
+/* Fr multiplication counter: on != 0 resets and starts it, on == 0 stops it;
+ * returns the count so far */
+unsigned long long or_fr_mul_counter(int on) {
+    if (on) g_fr_mul_count = 0;
+    g_fr_count_on = on;
+    return g_fr_mul_count;
+}
+
 /* element-wise product out[i] = a[i] * b[i] (test-input construction) */
 void or_fr_mul_vec(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t n) {
     for (size_t i = 0; i < n; i++) fr_mul(out + 4 * i, a + 4 * i, b + 4 * i);
@@ -1430,7 +1445,22 @@ static size_t rot_idx(size_t idx, int rot, uint32_t log_scale, uint32_t log_n) {
     return (idx + (size_t)((intptr_t)rot << log_scale)) & mask;
 }
 
+static void quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divide, const uint64_t *gate_values,
+                          uint64_t *out, int threads);
+
 void or_quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divide, uint64_t *out, int threads) {
+    quotient_eval(d, dom, divide, NULL, out, threads);
+}
+
+/* the same with the custom gates' Horner-in-y value of every row given
+ * (gate_values: 2^extended_k Fr): circuits whose gates are flattened programs */
+void or_quotient_eval_gates(const or_quotient_desc *d, const or_domain *dom, int divide, const uint64_t *gate_values,
+                            uint64_t *out, int threads) {
+    quotient_eval(d, dom, divide, gate_values, out, threads);
+}
+
+static void quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divide, const uint64_t *gate_values,
+                          uint64_t *out, int threads) {
     if (threads < 1) threads = 1;
     const uint32_t log_n = d->extended_k, log_scale = d->extended_k - d->k;
     const size_t E = (size_t)1 << log_n;
@@ -1443,7 +1473,9 @@ void or_quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divid
         const size_t r_next = rot_idx(idx, 1, log_scale, log_n);
         const size_t r_last = rot_idx(idx, last_rotation, log_scale, log_n);
         /* custom gate: Horner(0, [gate], y) = gate (evaluation.rs:849-852, :680-689) */
-        {
+        if (gate_values) {
+            memcpy(v, gate_values + 4 * idx, 32);
+        } else {
             const u64 *ql = d->fixed[d->gate_fixed[0]] + 4 * idx, *qr = d->fixed[d->gate_fixed[1]] + 4 * idx;
             const u64 *qm = d->fixed[d->gate_fixed[2]] + 4 * idx, *qo = d->fixed[d->gate_fixed[3]] + 4 * idx;
             const u64 *qc = d->fixed[d->gate_fixed[4]] + 4 * idx;
@@ -1481,7 +1513,13 @@ void or_quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divid
             /* current_delta = beta * g_coset * omega^idx (omega: extended) */
             u64 cur[4], ew[4];
             u64 e1[1] = {(u64)idx};
+            /* the reference steps omega^idx by one multiplication per row
+             * (beta_term *= omega, evaluation.rs:941); counted as that */
+            const int counting = g_fr_count_on;
+            g_fr_count_on = 0;
             fr_pow(ew, d->extended_omega, e1, 1);
+            g_fr_count_on = counting;
+            if (counting) g_fr_mul_count++;
             fr_mul(cur, delta_start, ew);
             uint32_t col = 0;
             for (uint32_t s = 0; s < d->n_perm_sets; s++) {

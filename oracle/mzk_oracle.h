@@ -123,6 +123,7 @@ void or_logup(const uint64_t *const *inputs, const uint32_t *chunk_cols, uint32_
               const uint64_t *selector, const uint64_t *multiplicities, size_t n, const uint64_t beta[4],
               uint32_t blinding_factors, const uint64_t *blinds, uint64_t *const *helpers_out,
               uint64_t *aggregator_out);
+unsigned long long or_fr_mul_counter(int on); /* count Fr multiplications (single thread) */
 void or_fr_mul_vec(const uint64_t *a, const uint64_t *b, uint64_t *out, size_t n);
 void or_kate_division(const uint64_t *a, size_t n, const uint64_t b[4], uint64_t *q);
 void or_g1_suffix_sum(const uint64_t *in, size_t n, uint64_t *out);
@@ -156,6 +157,9 @@ typedef struct {
 /* out[i] = numerator nu at extended row i; divide != 0 multiplies by the
  * inverted vanishing polynomial (divide_by_vanishing_poly, domain.rs:361). */
 void or_quotient_eval(const or_quotient_desc *d, const or_domain *dom, int divide, uint64_t *out, int threads);
+/* the same with the custom gates' value of every row given (gates as flattened programs) */
+void or_quotient_eval_gates(const or_quotient_desc *d, const or_domain *dom, int divide, const uint64_t *gate_values,
+                            uint64_t *out, int threads);
 
 #ifdef __cplusplus
 }

@@ -44,6 +44,7 @@ def _load():
                             ctypes.c_void_p, _u64p]),
         "or_kate_division": (None, [_u64p, sz, _u64p, _u64p]),
         "or_fr_mul_vec": (None, [_u64p, _u64p, _u64p, sz]),
+        "or_fr_mul_counter": (ctypes.c_ulonglong, [i32]),
         "or_g1_suffix_sum": (None, [_u64p, sz, _u64p]),
         "or_g1_decompress": (i32, [_u64p, _u8p, i32]),
         "or_srs_setup": (None, [_u64p, u32, _u64p, _u64p, _u64p, _u64p, _u64p]),
@@ -95,6 +96,7 @@ def _load():
         "or_domain_extended_to_lagrange": (None, [ctypes.c_void_p, _u64p, _u64p, i32]),
         "or_domain_divide_by_vanishing_poly": (None, [ctypes.c_void_p, _u64p, i32]),
         "or_quotient_eval": (None, [ctypes.c_void_p, ctypes.c_void_p, i32, _u64p, i32]),
+        "or_quotient_eval_gates": (None, [ctypes.c_void_p, ctypes.c_void_p, i32, _u64p, _u64p, i32]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -466,6 +468,17 @@ def srs_setup(s, k):
     return outs
 
 
+def count_fr_muls(fn, *args, **kwargs):
+    """(result of fn, Fr multiplications the C oracle made while it ran);
+    run fn single-threaded for an exact count."""
+    lib.or_fr_mul_counter(1)
+    try:
+        out = fn(*args, **kwargs)
+    finally:
+        count = lib.or_fr_mul_counter(0)
+    return out, int(count)
+
+
 def fr_mul_vec(a, b):
     """element-wise product of two Fr arrays of the same length"""
     a = np.ascontiguousarray(a, np.uint64)
@@ -541,9 +554,14 @@ class Domain:
         lib.or_domain_extended_to_lagrange(self.h, P(a), P(o), threads or threads_default())
         return o
 
-    def quotient_eval(self, desc, divide=True, threads=None):
+    def quotient_eval(self, desc, divide=True, threads=None, gate_values=None):
         o = np.zeros((self.extended_len, 4), np.uint64)
-        lib.or_quotient_eval(ctypes.byref(desc), self.h, 1 if divide else 0, P(o), threads or threads_default())
+        if gate_values is None:
+            lib.or_quotient_eval(ctypes.byref(desc), self.h, 1 if divide else 0, P(o), threads or threads_default())
+        else:
+            g = np.ascontiguousarray(gate_values, np.uint64)
+            lib.or_quotient_eval_gates(ctypes.byref(desc), self.h, 1 if divide else 0, P(g), P(o),
+                                       threads or threads_default())
         return o
 
     def divide_by_vanishing_poly(self, a, threads=None):

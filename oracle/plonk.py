@@ -13,10 +13,11 @@ canonical form, so the scalar algebra of the transcript, the identities and
 the verifier is independent of the C field code.  G1 points are affine
 numpy arrays (12 u64, Montgomery, identity all-zero).
 
-Circuit shape (a dict, see `config3_circuit`): advice and fixed columns, the
-reference's query lists (`ConstraintSystem::advice_queries`/`fixed_queries`,
-in their order), one custom gate (the standard gate
-q_l a + q_r b + q_m a b + q_o c + q_c), a permutation over advice/fixed
+Circuit shape (a dict, see `config3_circuit` and `generic_circuit`): advice
+and fixed columns, the reference's query lists
+(`ConstraintSystem::advice_queries`/`fixed_queries`, in their order), custom
+gates as a flattened program (any gates, rotations included) or the standard
+gate q_l a + q_r b + q_m a b + q_o c + q_c, a permutation over advice/fixed
 columns split into sets of cs.degree() - 2 columns, and at most one logup
 lookup whose input is one advice column and whose table is one fixed column,
 with an optional fixed selector column.  No instance columns, trashcans or
@@ -298,6 +299,101 @@ def config3_instance(k, seed, table_bits=16, copy_fraction=0.10):
     return fixed, mapping, [a, b, cc_col]
 
 
+def generic_circuit(k):
+    """A circuit of another shape: advice a, b, c, d with a queried at rotations
+    0 and 1, fixed q1, q2, q3, q4, the table and the lookup selector; two gates
+    as one flattened program, q1 a b + q2 a(wX) - q4 c and q3 (d - a^2), folded
+    by Horner in y; the permutation over a, b, c, d (two sets of three and one
+    columns); a lookup of a into the table; degree 5."""
+    zero, one = to_mont(0), to_mont(1)
+    gates = {"constants": [zero, one], "rotations": [0, 1],
+             # values: constants 0, 1; slots beta 2, theta 3, trash 4, y 5, previous 6; reads 7..15
+             "reads": [(0, 0, 0, 7), (0, 1, 0, 8), (0, 2, 0, 9), (0, 3, 0, 10), (1, 0, 0, 11), (1, 1, 0, 12),
+                       (1, 2, 0, 13), (1, 3, 0, 14), (1, 0, 1, 15)],
+             "ops": [(2, 16, 11, 12, 0), (2, 17, 7, 16, 0), (2, 18, 8, 15, 0), (0, 19, 17, 18, 0),
+                     (2, 20, 10, 13, 0), (1, 21, 19, 20, 0), (3, 22, 11, 0, 0), (1, 23, 14, 22, 0),
+                     (2, 24, 9, 23, 0), (6, 25, 6, 5, 21), (6, 26, 25, 5, 24)],
+             "values_len": 27, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
+             "previous_value_idx": 6, "result_idx": 26}
+    return {"k": k, "degree": 5, "n_advice": 4, "n_fixed": 6,
+            "advice_queries": [(0, 0), (1, 0), (2, 0), (3, 0), (0, 1)],
+            "fixed_queries": [(i, 0) for i in range(6)],
+            "gates": gates,
+            "perm_cols": [(0, 0), (0, 1), (0, 2), (0, 3)],
+            "lookups": [{"input": 0, "table": 4, "selector": 5}]}
+
+
+def _cycles(rng, n, u, n_cols, cycle_cols, fraction, rows):
+    """Copy cycles of 2 to 4 cells over `fraction` of the cells of columns
+    cycle_cols in rows [0, u): (mapping (n_cols, n, 2), {(col, row): value})
+    with one table value in [0, rows) per cycle."""
+    mapping = np.zeros((n_cols, n, 2), np.uint32)
+    for ci in range(n_cols):
+        mapping[ci, :, 0] = ci
+        mapping[ci, :, 1] = np.arange(n, dtype=np.uint32)
+    ncyc = len(cycle_cols)
+    cells = rng.permutation(ncyc * u)[: int(fraction * ncyc * u)]
+    pos, vals = 0, {}
+    while pos + 1 < len(cells):
+        ln = int(rng.integers(2, 5))
+        cyc = cells[pos:pos + ln]
+        pos += ln
+        if len(cyc) < 2:
+            break
+        v = int(rng.integers(0, rows))
+        for t, cell in enumerate(cyc):
+            nxt = cyc[(t + 1) % len(cyc)]
+            cc, rr = divmod(int(cell), u)
+            nc, nr = divmod(int(nxt), u)
+            mapping[cycle_cols[cc], rr] = (cycle_cols[nc], nr)
+            vals[(cycle_cols[cc], rr)] = v
+    return mapping, vals
+
+
+def generic_instance(k, seed, table_bits=16, copy_fraction=0.10):
+    """Seeded fixed columns, copy cycles (over the a and b cells of rows
+    before the last usable row) and a satisfying witness of generic_circuit:
+    a a table value, b uniform, c = q1 a b + q2 a(wX), d = a^2; the gate
+    selectors q1, q2, q4 are zero from the last usable row on (its a(wX) is a
+    blinding row), q3 from the usable rows on."""
+    c = generic_circuit(k)
+    n = 1 << k
+    bf = blinding_factors(c)
+    u = n - bf - 1
+    rng = np.random.default_rng(seed)
+    rows = min(1 << table_bits, u)
+    one = O.fr_const(0)
+    q = [O.rand_fr(seed * 131 + i, n) for i in range(3)]
+    q1, q2, q3 = q
+    q1[u - 1:] = 0
+    q2[u - 1:] = 0
+    q3[u:] = 0
+    q4 = np.zeros((n, 4), np.uint64)
+    q4[:u - 1] = one
+    table = np.zeros((n, 4), np.uint64)
+    table[:rows] = np.stack([to_mont(v) for v in range(rows)])
+    sel = np.zeros((n, 4), np.uint64)
+    sel[:u] = one
+    mapping, vals = _cycles(rng, n, u - 1, 4, [0, 1], copy_fraction, rows)
+    a_int = rng.integers(0, rows, size=u)
+    b = O.rand_fr(seed * 131 + 7, n)
+    b[u:] = 0
+    for (cc, rr), v in vals.items():
+        if cc == 0:
+            a_int[rr] = v
+        else:
+            b[rr] = to_mont(v)
+    a = np.zeros((n, 4), np.uint64)
+    a[:u] = np.stack([to_mont(int(v)) for v in a_int])
+    a_next = np.zeros_like(a)
+    a_next[:-1] = a[1:]
+    cc_col = O.poly_inner_product([_hadamard(q1, _hadamard(a, b)), _hadamard(q2, a_next)], [one, one])
+    cc_col[u - 1:] = 0
+    d = _hadamard(a, a)
+    d[u:] = 0
+    return [q1, q2, q3, q4, table, sel], mapping, [a, b, cc_col, d]
+
+
 def _hadamard(x, y):
     """Element-wise product of two Fr arrays (through the C oracle)."""
     return O.fr_mul_vec(x, y)
@@ -473,10 +569,17 @@ def identities(key, ev, ch):
     adv, fix = ev["advice"], ev["fixed"]
     aq = lambda col: adv[query_index(c["advice_queries"], col)]
     fq = lambda col: fix[query_index(c["fixed_queries"], col)]
-    gf, ga = c["gate_fixed"], c["gate_advice"]
-    ql, qr, qm, qo, qc = (fq(i) for i in gf)
-    a, b, cc = (aq(i) for i in ga)
-    out = [(ql * a + qr * b + qm * a * b + qo * cc + qc) % R]
+    if c.get("gates") is not None:
+        def read(col_type, col, rot):
+            if col_type == 0:
+                return fix[query_index(c["fixed_queries"], col, rot)]
+            return adv[query_index(c["advice_queries"], col, rot)]
+        out = [program_at(c["gates"], read, ch)]
+    else:
+        gf, ga = c["gate_fixed"], c["gate_advice"]
+        ql, qr, qm, qo, qc = (fq(i) for i in gf)
+        a, b, cc = (aq(i) for i in ga)
+        out = [(ql * a + qr * b + qm * a * b + qo * cc + qc) % R]
     # permutation
     sets = ev["perm_sets"]
     chunk = c["degree"] - 2
@@ -511,6 +614,27 @@ def identities(key, ev, ch):
         out.append((h * fb - 1) % R)              # one input: product f+beta, sum of partial products 1
         out.append(((Zn - Z - sel * h) * (table + beta) + m) * (1 - (l_last + l_blind)) % R)
     return [v % R for v in out]
+
+
+def program_at(graph, read, ch):
+    """A flattened program (FlatGraphEvaluator, evaluation.rs:148-213) at one
+    point with Python integers: each read is read(col_type, column, rotation)
+    (the query's evaluation at x), the previous value zero, the challenge
+    slots from ch; returns the result value.  partially_evaluate_identities
+    evaluates the same gate expressions at x (plonk/mod.rs:537-562)."""
+    vals = [0] * graph["values_len"]
+    for i, cst in enumerate(graph["constants"]):
+        vals[i] = to_int(cst)
+    for slot, name in (("beta_idx", "beta"), ("theta_idx", "theta"), ("trash_challenge_idx", "trash"),
+                       ("y_idx", "y")):
+        vals[graph[slot]] = ch[name]
+    vals[graph["previous_value_idx"]] = 0
+    for t, col, r, dst in graph["reads"]:
+        vals[dst] = read(t, col, graph["rotations"][r])
+    for kind, dst, a, b, c in graph["ops"]:
+        x, y2, z = vals[a], vals[b], vals[c]
+        vals[dst] = [x + y2, x - y2, x * y2, x * x, 2 * x, -x, x * y2 + z][kind] % R
+    return vals[graph["result_idx"]]
 
 
 def horner(values, y):
@@ -613,7 +737,7 @@ def create_proof(key, advice, blinds):
     Z_c = [dom.lagrange_to_coeff(Z) for Z in Zs]
     ext = lambda p: dom.coeff_to_extended(p)
     hpoly = quotient(key, [ext(p) for p in adv_c], [ext(p) for p in z_c], [ext(p) for p in m_c],
-                     [ext(p) for p in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta)
+                     [ext(p) for p in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta, trash=trash)
     hcoeff = dom.extended_to_coeff(hpoly)[: (n - 1) * qdeg]
     limbs = [np.concatenate([hcoeff[i * (n - 1):(i + 1) * (n - 1)], np.zeros((1, 4), np.uint64)]) for i in range(qdeg)]
     for i, t in enumerate(take(qdeg - 1), start=1):         # blind_quotient_limbs (prover.rs:774-785)
@@ -674,7 +798,7 @@ def create_proof(key, advice, blinds):
     return bytes(tr.proof)
 
 
-def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta):
+def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None, trash=0):
     """compute_nu_poly + divide_by_vanishing_poly (prover.rs:634-715) through
     the C oracle's evaluate_numerator restatement."""
     c, dom = key.circuit, key.dom
@@ -694,8 +818,8 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta):
     d.k, d.extended_k = c["k"], dom.extended_k
     d.advice, d.n_advice = parr(adv_e), len(adv_e)
     d.fixed, d.n_fixed = parr(key.fixed_cosets), len(key.fixed_cosets)
-    d.gate_fixed[:] = c["gate_fixed"]
-    d.gate_advice[:] = c["gate_advice"]
+    d.gate_fixed[:] = c.get("gate_fixed", [0] * 5)
+    d.gate_advice[:] = c.get("gate_advice", [0] * 3)
     d.n_perm_cols = len(c["perm_cols"])
     d.perm_col_kind = u32([kind for kind, _ in c["perm_cols"]])
     d.perm_col_index = u32([ci for _, ci in c["perm_cols"]])
@@ -714,7 +838,11 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta):
     d.extended_omega[:] = [int(t) for t in dom.get(2)]
     d.g_coset[:] = [int(t) for t in dom.get(3)]
     keep.extend([adv_e, z_e, m_e, h_e, Z_e])
-    return dom.quotient_eval(d, True)
+    gate_values = None
+    if c.get("gates") is not None:
+        gate_values = O.flat_gates_eval(c["gates"], key.fixed_cosets, adv_e, [], c["k"], dom.extended_k,
+                                        to_mont(beta), to_mont(theta), to_mont(trash), to_mont(y))
+    return dom.quotient_eval(d, True, threads, gate_values)
 
 
 def multi_open(key, tr, queries):
@@ -781,7 +909,7 @@ def _verify(key, proof, s):
     gamma = tr.squeeze()
     z_coms = [tr.read_point() for _ in range(S)]
     hz_coms = [(tr.read_point(), tr.read_point()) for _ in range(L)]
-    tr.squeeze()                                   # trash challenge (no trashcans)
+    trash = tr.squeeze()                           # trash challenge (no trashcans)
     y = tr.squeeze()
     limb_coms = [tr.read_point() for _ in range(qdeg)]
     x = tr.squeeze()
@@ -796,7 +924,7 @@ def _verify(key, proof, s):
         sets.append([z0, z1, tr.read_fr() if si < S - 1 else None])
     ev["perm_sets"] = sets
     ev["lookups"] = [tuple(tr.read_fr() for _ in range(4)) for _ in range(L)]
-    ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta}
+    ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta, "trash": trash, "y": y}
     const = horner(identities(key, ev, ch), y)
     # compute_linearization_commitment (linearization/verifier.rs:27-78)
     lin_com = pt_lincomb(limb_coms, [(1 - xn) * pow(sf, i, R) for i in range(qdeg)])

@@ -15,16 +15,22 @@ mzk = load()
 PINNED = b"config-3 circuit: standard gate, copy cycles, range lookup"
 
 
+SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.generic_circuit, OP.generic_instance)}
+
+
 class Circuit:
-    def __init__(self, ctx, k, seed, pinned=PINNED, oracle=True, srs=None):
+    def __init__(self, ctx, k, seed, pinned=PINNED, oracle=True, srs=None, shape="config3"):
         """srs = (buffer, offsets) of a shared device SRS whose bases hold this
         k's g | lagrange | delta | double delta at the offsets; otherwise
-        this circuit gets its own."""
+        this circuit gets its own.  shape: "config3" (the single-proof
+        configuration) or "generic" (two gates with a rotation, two
+        permutation sets)."""
         self.ctx, self.k, self.seed = ctx, k, seed
-        c = OP.config3_circuit(k)
+        make_circuit, make_instance = SHAPES[shape]
+        c = make_circuit(k)
         c["blinding_factors"] = OP.blinding_factors(c)
         self.circuit = c
-        self.fixed, self.mapping, self.advice = OP.config3_instance(k, seed)
+        self.fixed, self.mapping, self.advice = make_instance(k, seed)
         self.dom = mzk.EvaluationDomain(ctx, c["degree"], k)
         n = self.n = self.dom.n
         if srs is None:
@@ -42,7 +48,7 @@ class Circuit:
             host = self.srs_buf.download((self.desc.srs_len, 12))
             g, lag, dl, ddl = (host[o:o + n] for o in self.offs)
             srs_h = {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}
-            self.okey = OP.keygen(OP.config3_circuit(k), self.fixed, self.mapping, srs_h, pinned)
+            self.okey = OP.keygen(make_circuit(k), self.fixed, self.mapping, srs_h, pinned)
 
     def blinds(self, seed):
         return O.rand_fr(5000 + seed, self.key.n_blinds)

@@ -168,3 +168,26 @@ def test_device_generated_config3_instance_verifies(ctx):
     assert OP.verify(okey, proof, OP.to_int(s))
     # a second fresh witness also satisfies the circuit
     assert mzk.create_proofs(ctx, [(inst.key, inst.witness(7), inst.blinds(8))], flags=mzk.PROVE_SELF_CHECK)
+
+
+@pytest.mark.parametrize("k", [5, 8])
+def test_generic_circuit_proof_equals_oracle(ctx, k):
+    """A circuit of another shape (two gates as a flattened program reading
+    a(wX), four permutation columns in two sets, the lookup): device keygen and
+    create_proof give the oracle's transcript, it verifies, the self-check
+    holds, and it proves through the proving service too."""
+    c = Circuit(ctx, k, seed=k + 60, shape="generic")
+    assert OP.to_int(c.key.repr) == c.okey.repr
+    bl = c.blinds(3)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = [srv.submit(c.key, c.advice, c.blinds(s)) for s in (3, 4)]
+    outs = [srv.wait(x)[0] for x in t]
+    srv.close()
+    assert outs[0] == proof and c.verify(outs[1])
+    bad = [a.copy() for a in c.advice]
+    bad[3][2] = OP.to_mont(OP.to_int(bad[3][2]) + 1)
+    with pytest.raises(mzk.MzkError, match="does not satisfy"):
+        mzk.create_proofs(ctx, [(c.key, bad, bl)], flags=mzk.PROVE_SELF_CHECK)

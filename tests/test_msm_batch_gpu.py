@@ -74,3 +74,38 @@ def test_batch_rejects_out_of_range_items(ctx):
     d_s = ctx.gen_rand_fr(2, 64)
     with pytest.raises(mzk.MzkError):
         ctx.msm_batch_device(d_bases, 64, [(d_s, 10, 60)])
+
+
+def test_config4_batch_at_full_sizes_matches_closed_form(ctx):
+    """The batched configuration at its own sizes: 64 MSMs of 2^U(12, 22)
+    points over one 2^22-point SRS of bases [r_i]G, one in four sparse (90 %
+    of scalars in {0, 1}).  Every item equals [sum_i s_i r_i]G (the scalar
+    inner product by the oracle, then one scalar multiplication of G), over
+    the plain SRS and over a width-20 window table of it (items of 2^18
+    points and more use the table)."""
+    srs_n, seed = 1 << 22, 0x5126
+    d_bases = ctx.gen_bases(seed, srs_n)
+    r = O.rand_fr(seed, srs_n)                       # the bases' discrete logs: the same stream
+    rng = np.random.default_rng(0xC4)
+    items, want, keep = [], [], []
+    g = O.g1_generator()
+    for m in range(64):
+        n = int(2 ** rng.uniform(12, 22))
+        d = ctx.gen_rand_fr(0xB100 + m, n)
+        s = d.download((n, 4))
+        if m % 4 == 3:
+            s = sparse(s, m)
+            d.upload(s)
+        keep.append(d)
+        items.append((d, 0, n))
+        want.append(O.g1_mul(g, O.fr_inner_product(s, r[:n])))
+    got = ctx.msm_batch_device(d_bases, srs_n, items)
+    for m in range(64):
+        assert np.array_equal(mzk.affine(got[m]), want[m]), m
+    c, rows = 20, mzk.Context.msm_table_rows(20)
+    table = ctx.alloc(rows * srs_n * 96)
+    ctx.gen_bases(seed, srs_n, out=table)
+    del d_bases
+    ctx.msm_window_table(table, srs_n, c, rows)
+    tabled = ctx.msm_batch_table_device(table, srs_n, c, rows, 1 << 18, items)
+    assert np.array_equal(tabled, got)

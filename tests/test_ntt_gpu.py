@@ -117,3 +117,31 @@ def test_ntt_2_24_roundtrip_and_spot_evaluations(ctx):
         assert np.array_equal(lag[i], O.eval_polynomial(a, O.fr_pow(omega, i)))
     for i in [0, 7, en - 3]:
         assert np.array_equal(ext[i], O.eval_polynomial(a, O.fr_op("mul", zeta, O.fr_pow(eomega, i))))
+
+
+def test_ntt_2_24_all_ops_match_oracle_in_full(ctx):
+    """The NTT sweep's largest size compared element by element with the
+    oracle: coeff_to_lagrange and lagrange_to_coeff at 2^24, coeff_to_extended
+    2^24 -> 2^26 and extended_to_coeff at 2^26."""
+    import gc
+    k = 24
+    g = mzk.EvaluationDomain(ctx, 5, k)
+    o = O.Domain(5, k)
+    n, en = g.n, g.extended_len
+    da = ctx.gen_rand_fr(0x2425, n)
+    a = da.download((n, 4))
+    out = ctx.alloc(en * 32)
+    for name in ("coeff_to_lagrange", "lagrange_to_coeff"):
+        g.op_device(name, da, out)
+        assert np.array_equal(out.download((n, 4)), getattr(o, name)(a)), name
+        gc.collect()
+    g.op_device("coeff_to_extended", da, out)
+    ext = out.download((en, 4))
+    want = o.coeff_to_extended(a)
+    assert np.array_equal(ext, want)
+    del want
+    gc.collect()
+    de = ctx.gen_rand_fr(0x2426, en)
+    e = de.download((en, 4))
+    g.op_device("extended_to_coeff", de, out)
+    assert np.array_equal(out.download((en, 4)), o.extended_to_coeff(e))

@@ -102,3 +102,42 @@ def test_intermediate_sets_follow_first_appearance():
     assert [si for _, si, _ in labels] == [0, 1, 2, 0, 2]
     with pytest.raises(ValueError):
         OP.intermediate_sets([("a", 1), ("a", 1)])
+
+
+@pytest.mark.parametrize("k", [5, 6])
+def test_quotient_work_count(k):
+    """The quotient of the single-proof configuration costs 37 Fr
+    multiplications per extended row (gate 5, permutation set and boundary
+    terms with the y-Horner steps, the lookup terms, the division by t(X)),
+    plus one for beta * g_coset: the work figure of the quotient's roofline,
+    counted on the oracle's restatement of evaluate_numerator with omega^idx
+    stepped as the reference steps it."""
+    c, key, _, _, _ = setup(k, 3)
+    E = key.dom.extended_len
+    cols = [O.rand_fr(70 + i, E) for i in range(7)]
+    _, count = O.count_fr_muls(OP.quotient, key, cols[:3], [cols[3]], [cols[4]], [cols[5]], [cols[6]], 1, 2, 3, 4,
+                               threads=1)
+    assert count == 37 * E + 1
+
+
+def test_generic_circuit_proofs_verify():
+    """Another circuit shape: two gates as one flattened program (with a(wX)),
+    four permutation columns in two sets (z of the first set opened at
+    w^-(bf+1) x too), three point sets in the multi-open."""
+    for k in (5, 6):
+        c = OP.generic_circuit(k)
+        fixed, mapping, adv = OP.generic_instance(k, k)
+        s = O.rand_fr(50 + k, 1)[0]
+        g, lag, dl, ddl = O.srs_setup(s, k)
+        key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"generic")
+        assert OP.n_perm_sets(c) == 2 and key.bf == 7
+        bl = [OP.to_int(v) for v in O.rand_fr(60 + k, OP.blind_count(c))]
+        proof = OP.create_proof(key, adv, bl)
+        assert len(proof) == 15 * 48 + 27 * 32
+        assert OP.verify(key, proof, OP.to_int(s))
+        bad = [a.copy() for a in adv]
+        bad[2][1] = OP.to_mont(OP.to_int(bad[2][1]) + 1)          # c breaks the first gate
+        assert not OP.verify(key, OP.create_proof(key, bad, bl), OP.to_int(s))
+        bad = [a.copy() for a in adv]
+        bad[3][1] = OP.to_mont(OP.to_int(bad[3][1]) + 1)          # d breaks the second gate
+        assert not OP.verify(key, OP.create_proof(key, bad, bl), OP.to_int(s))
