@@ -435,7 +435,23 @@ typedef struct mzk_plonk_key mzk_plonk_key;
 int mzk_keygen(mzk_ctx *ctx, mzk_domain *d, const mzk_circuit_desc *cs, const mzk_srs_desc *srs,
                const uint64_t *const *fixed_values, const uint32_t *perm_mapping, const uint8_t *pinned,
                size_t pinned_len, mzk_plonk_key **out);
+/* The same with the permutation polynomials' Lagrange values given (n_perm_cols
+ * HOST columns of 2^k Fr) instead of the copy mapping: a ProvingKey read from
+ * its file holds these (ProvingKey::read, plonk/mod.rs:421-453,
+ * permutation.rs:153-166). */
+int mzk_keygen_from_values(mzk_ctx *ctx, mzk_domain *d, const mzk_circuit_desc *cs, const mzk_srs_desc *srs,
+                           const uint64_t *const *fixed_values, const uint64_t *const *perm_values,
+                           const uint8_t *pinned, size_t pinned_len, mzk_plonk_key **out);
 int mzk_plonk_key_destroy(mzk_plonk_key *key);
+/* The transcript operations of one proof of this key, in order: one code per
+ * operation (MZK_TR_*).  A caller holding its own transcript object (the
+ * reference's CircuitTranscript) replays a proof into it with these: a
+ * point is 48 proof bytes, a scalar 32, a squeeze reads nothing. */
+#define MZK_TR_COMMON_FR 0   /* the VK's transcript_repr (not in the proof bytes) */
+#define MZK_TR_WRITE_POINT 1
+#define MZK_TR_WRITE_FR 2
+#define MZK_TR_SQUEEZE 3
+int mzk_plonk_key_transcript_layout(const mzk_plonk_key *key, uint8_t *ops, size_t cap, size_t *len);
 /* repr (optional): transcript_repr; proof_len: bytes of one proof;
  * n_blinds: the rng draws one proof takes (the order under
  * mzk_create_proofs) */

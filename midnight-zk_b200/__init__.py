@@ -110,6 +110,9 @@ SIGNATURES = {
     "mzk_vk_transcript_repr": (_i32, [_u32, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, _u64p]),
     "mzk_keygen": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                           ctypes.c_void_p, _sz, ctypes.POINTER(_vp)]),
+    "mzk_keygen_from_values": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, _sz, ctypes.POINTER(_vp)]),
+    "mzk_plonk_key_transcript_layout": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.POINTER(_sz)]),
     "mzk_plonk_key_destroy": (_i32, [_vp]),
     "mzk_plonk_key_info": (_i32, [_vp, _u64p, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
     "mzk_plonk_key_commitments": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p]),
@@ -960,7 +963,7 @@ class PlonkKey:
     host (n, 4) arrays; mapping: (n_perm_cols, n, 2) uint32 or None; srs:
     an SrsDesc.  The domain and the SRS buffer must outlive the key."""
 
-    def __init__(self, ctx, domain, circuit, srs, fixed_values, mapping=None, pinned=b""):
+    def __init__(self, ctx, domain, circuit, srs, fixed_values, mapping=None, pinned=b"", perm_values=None):
         self.ctx, self.domain, self.circuit = ctx, domain, circuit
         keep = []
 
@@ -1000,8 +1003,15 @@ class PlonkKey:
         mp = None if mapping is None else np.ascontiguousarray(mapping, np.uint32)
         pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
         h = _vp()
-        _check(lib().mzk_keygen(ctx.h, domain.h, ctypes.byref(cs), ctypes.byref(srs), fptrs,
-                                None if mp is None else mp.ctypes.data, pin, len(pinned), ctypes.byref(h)))
+        if perm_values is not None:
+            pv = [np.ascontiguousarray(v, np.uint64) for v in perm_values]
+            keep.append(pv)
+            pptrs = (ctypes.c_void_p * max(1, len(pv)))(*[v.ctypes.data for v in pv])
+            _check(lib().mzk_keygen_from_values(ctx.h, domain.h, ctypes.byref(cs), ctypes.byref(srs), fptrs, pptrs,
+                                                pin, len(pinned), ctypes.byref(h)))
+        else:
+            _check(lib().mzk_keygen(ctx.h, domain.h, ctypes.byref(cs), ctypes.byref(srs), fptrs,
+                                    None if mp is None else mp.ctypes.data, pin, len(pinned), ctypes.byref(h)))
         self.h = h.value
         repr_, plen, nbl = np.zeros(4, np.uint64), _sz(), _sz()
         _check(lib().mzk_plonk_key_info(self.h, _ptr(repr_), ctypes.byref(plen), ctypes.byref(nbl)))
@@ -1009,6 +1019,14 @@ class PlonkKey:
         self.fixed_coms = np.zeros((circuit["n_fixed"], 18), np.uint64)
         self.perm_coms = np.zeros((len(pc), 18), np.uint64)
         _check(lib().mzk_plonk_key_commitments(self.h, self.fixed_coms.ctypes.data, self.perm_coms.ctypes.data))
+
+    def transcript_layout(self):
+        """The MZK_TR_* operation codes of one proof, in order."""
+        n = _sz()
+        _check(lib().mzk_plonk_key_transcript_layout(self.h, None, 0, ctypes.byref(n)))
+        buf = (ctypes.c_uint8 * max(1, n.value))()
+        _check(lib().mzk_plonk_key_transcript_layout(self.h, buf, n.value, ctypes.byref(n)))
+        return bytes(buf[:n.value])
 
     def close(self):
         if getattr(self, "h", None):

@@ -437,9 +437,12 @@ Status vk_transcript_repr(uint32_t k, const uint64_t* fixed, size_t n_fixed, con
     return OK;
 }
 
+// perm_values (host, n_perm_cols columns of n Fr): the permutation
+// polynomials' Lagrange values as given (ProvingKey::read, permutation.rs:
+// 153-166); otherwise they are built from `mapping` (or the identity)
 Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const mzk_srs_desc* srs,
-              const uint64_t* const* fixed_values, const uint32_t* mapping, const uint8_t* pinned, size_t pinned_len,
-              PlonkKey** out) {
+              const uint64_t* const* fixed_values, const uint32_t* mapping, const uint64_t* const* perm_values,
+              const uint8_t* pinned, size_t pinned_len, PlonkKey** out) {
     MZK_TRY(check_circuit(d, cs));
     const uint32_t n = 1u << d->k, E = 1u << d->ext_k;
     if (!srs || !srs->srs) {
@@ -582,10 +585,21 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
             MZK_TRY(ctx->ensure("kg_mapping", (size_t)P * n * 8, &d_map));
             MZK_CUDA_CHECK(cudaMemcpyAsync(d_map, mapping, (size_t)P * n * 8, cudaMemcpyHostToDevice, st));
         }
-        k_perm_values<<<grid_of(ctx, (uint64_t)P * n), kThreads, 0, st>>>(
-            key->perm_lag[0], static_cast<const uint32_t*>(d_map), static_cast<const Fr*>(d_tab), d->lo[0], d->hi[0],
-            n, P);
-        MZK_LAUNCH_CHECK(ctx);
+        if (perm_values) {
+            for (uint32_t i = 0; i < P; i++) {
+                if (!perm_values[i]) {
+                    set_error("keygen: null permutation column");
+                    return ERR_ARG;
+                }
+                MZK_CUDA_CHECK(cudaMemcpyAsync(key->perm_lag[i], perm_values[i], (size_t)n * sizeof(Fr),
+                                               cudaMemcpyHostToDevice, st));
+            }
+        } else {
+            k_perm_values<<<grid_of(ctx, (uint64_t)P * n), kThreads, 0, st>>>(
+                key->perm_lag[0], static_cast<const uint32_t*>(d_map), static_cast<const Fr*>(d_tab), d->lo[0],
+                d->hi[0], n, P);
+            MZK_LAUNCH_CHECK(ctx);
+        }
         for (uint32_t i = 0; i < P; i++) {
             MZK_TRY(domain_op_device(ctx, d, OP_LAGRANGE_TO_COEFF, key->perm_lag[i], key->perm_coeff[i], st));
             MZK_TRY(domain_op_device(ctx, d, OP_COEFF_TO_EXTENDED, key->perm_coeff[i], key->perm_ext[i], st));
@@ -1483,8 +1497,60 @@ int mzk_keygen(mzk_ctx* ctx, mzk_domain* d, const mzk_circuit_desc* cs, const mz
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     cudaSetDevice(c->device);
     mzk::PlonkKey* key = nullptr;
-    MZK_TRY(mzk::keygen(c, mzk::domain_of(d), cs, srs, fixed_values, perm_mapping, pinned, pinned_len, &key));
+    MZK_TRY(mzk::keygen(c, mzk::domain_of(d), cs, srs, fixed_values, perm_mapping, nullptr, pinned, pinned_len,
+                        &key));
     *out = reinterpret_cast<mzk_plonk_key*>(key);
+    return mzk::OK;
+}
+
+int mzk_keygen_from_values(mzk_ctx* ctx, mzk_domain* d, const mzk_circuit_desc* cs, const mzk_srs_desc* srs,
+                           const uint64_t* const* fixed_values, const uint64_t* const* perm_values,
+                           const uint8_t* pinned, size_t pinned_len, mzk_plonk_key** out) {
+    if (!ctx || !d || !cs || !out || (pinned_len && !pinned) || (cs->n_perm_cols && !perm_values)) {
+        mzk::set_error("keygen: null argument");
+        return mzk::ERR_ARG;
+    }
+    *out = nullptr;
+    mzk::Context* c = mzk::context_of(ctx);
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    mzk::PlonkKey* key = nullptr;
+    MZK_TRY(mzk::keygen(c, mzk::domain_of(d), cs, srs, fixed_values, nullptr, perm_values, pinned, pinned_len, &key));
+    *out = reinterpret_cast<mzk_plonk_key*>(key);
+    return mzk::OK;
+}
+
+int mzk_plonk_key_transcript_layout(const mzk_plonk_key* key, uint8_t* ops, size_t cap, size_t* len) {
+    if (!key || !len) return mzk::ERR_ARG;
+    const mzk::PlonkKey* k = reinterpret_cast<const mzk::PlonkKey*>(key);
+    std::vector<uint8_t> v;
+    auto put = [&](uint8_t op, size_t times) { v.insert(v.end(), times, op); };
+    const size_t L = k->has_lookup ? 1 : 0, S = k->n_sets;
+    put(MZK_TR_COMMON_FR, 1);                  // vk.hash_into
+    put(MZK_TR_WRITE_POINT, k->n_advice);      // advice commitments
+    put(MZK_TR_SQUEEZE, 1);                    // theta
+    put(MZK_TR_WRITE_POINT, L);                // multiplicities
+    put(MZK_TR_SQUEEZE, 2);                    // beta, gamma
+    put(MZK_TR_WRITE_POINT, S + 2 * L);        // permutation products, logup helper and aggregator
+    put(MZK_TR_SQUEEZE, 2);                    // trash challenge, y
+    put(MZK_TR_WRITE_POINT, k->qdeg);          // quotient limbs
+    put(MZK_TR_SQUEEZE, 1);                    // x
+    put(MZK_TR_WRITE_FR, k->advice_queries.size() + k->fixed_queries.size() + k->n_perm + (S ? 3 * S - 1 : 0) +
+                             4 * L);          // evaluations
+    put(MZK_TR_SQUEEZE, 2);                    // x1, x2
+    put(MZK_TR_WRITE_POINT, 1);                // f
+    put(MZK_TR_SQUEEZE, 1);                    // x3
+    put(MZK_TR_WRITE_FR, k->open_sets.size()); // q evaluations
+    put(MZK_TR_SQUEEZE, 1);                    // x4
+    put(MZK_TR_WRITE_POINT, 1);                // pi
+    *len = v.size();
+    if (ops) {
+        if (cap < v.size()) {
+            mzk::set_error("transcript layout: output buffer too small");
+            return mzk::ERR_ARG;
+        }
+        std::memcpy(ops, v.data(), v.size());
+    }
     return mzk::OK;
 }
 
