@@ -47,6 +47,12 @@ int mzk_ctx_synchronize(mzk_ctx *ctx);
  * Turning profiling on resets the totals. */
 int mzk_ctx_set_profiling(mzk_ctx *ctx, int on);
 int mzk_ctx_phase_stats(mzk_ctx *ctx, double *ms_out, uint64_t *count_out, int max_phases);
+/* create_proof wall time per Fiat-Shamir phase since the last reset, summed
+ * over calls: 0 set-up, 1 advice, 2 multiplicities, 3 permutation / logup
+ * products, 4 cosets + quotient + limbs, 5 evaluations + linearization,
+ * 6 q polynomials + f, 7 q evaluations, 8 final polynomial + pi, and 9 the
+ * MSMs inside phases 1-8; reset != 0 zeroes the totals after reading. */
+int mzk_ctx_prove_phase_stats(mzk_ctx *ctx, double *ms_out, uint64_t *calls, int max_phases, int reset);
 /* Integer multiply-add throughput of this GPU (IMAD/s, carry-chained
  * mad.lo.cc/madc.hi pairs as the field code issues them) and 12-limb
  * Montgomery multiplications per second, measured by microbenchmark kernels.

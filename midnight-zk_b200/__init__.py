@@ -45,6 +45,7 @@ SIGNATURES = {
     "mzk_ctx_synchronize": (_i32, [_vp]),
     "mzk_ctx_set_profiling": (_i32, [_vp, _i32]),
     "mzk_ctx_phase_stats": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _u64p, _i32]),
+    "mzk_ctx_prove_phase_stats": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _u64p, _i32, _i32]),
     "mzk_probe_imad_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double)]),
     "mzk_msm_last_shape": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u64p]),
@@ -475,6 +476,16 @@ class Context:
         cnt = np.zeros(16, np.uint64)
         _check(lib().mzk_ctx_phase_stats(self.h, ms, _ptr(cnt), 16))
         return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(self.PHASES)}
+
+    PROVE_PHASES = ["setup", "advice", "multiplicities", "products", "quotient", "evaluations", "f",
+                    "q_evaluations", "pi", "msm"]
+
+    def prove_phase_stats(self, reset=False):
+        """create_proof wall time per phase (ms, summed) and the calls made."""
+        ms = (ctypes.c_double * len(self.PROVE_PHASES))()
+        calls = np.zeros(1, np.uint64)
+        _check(lib().mzk_ctx_prove_phase_stats(self.h, ms, _ptr(calls), len(ms), 1 if reset else 0))
+        return {name: ms[i] for i, name in enumerate(self.PROVE_PHASES)}, int(calls[0])
 
     def probe_imad_peak(self):
         """(IMAD/s, 12-limb Montgomery multiplications/s, {variant: IMAD/s}) of this GPU."""

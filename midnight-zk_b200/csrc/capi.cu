@@ -297,6 +297,19 @@ int mzk_ctx_phase_stats(mzk_ctx* ctx, double* ms_out, uint64_t* count_out, int m
     return mzk::OK;
 }
 
+int mzk_ctx_prove_phase_stats(mzk_ctx* ctx, double* ms_out, uint64_t* calls, int max_phases, int reset) {
+    if (int s = check_ctx(ctx)) return s;
+    Guard g(ctx);
+    for (int i = 0; i < max_phases && i < mzk::Context::kProvePhases; i++)
+        if (ms_out) ms_out[i] = ctx->impl.prove_ms[i];
+    if (calls) *calls = ctx->impl.prove_calls;
+    if (reset) {
+        for (int i = 0; i < mzk::Context::kProvePhases; i++) ctx->impl.prove_ms[i] = 0.0;
+        ctx->impl.prove_calls = 0;
+    }
+    return mzk::OK;
+}
+
 int mzk_msm_last_shape(mzk_ctx* ctx, int* c, int* windows, uint64_t* entries) {
     if (int s = check_ctx(ctx)) return s;
     Guard g(ctx);

@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -971,6 +972,15 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     }
     MsmTable table{srs.srs, srs.srs_len, srs.table_c, srs.table_rows, srs.table_min_n};
     const MsmTable* tab = srs.table_c > 0 ? &table : nullptr;
+    // wall time per phase (each ends with a stream sync)
+    using clock = std::chrono::steady_clock;
+    auto t_phase = clock::now();
+    auto phase_done = [&](int ph) {
+        const auto t = clock::now();
+        ctx->prove_ms[ph] += std::chrono::duration<double, std::milli>(t - t_phase).count();
+        t_phase = t;
+    };
+    ctx->prove_calls++;
     // scratch: every proof's buffers carved from one device buffer
     size_t total = 0, max_E = 0;
     for (size_t j = 0; j < count; j++) {
@@ -1039,10 +1049,15 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     std::vector<uint64_t> res;
     auto msm = [&]() -> Status {
         res.assign(items.size() * 18, 0);
+        MZK_CUDA_CHECK(cudaStreamSynchronize(st));  // the MSM time below is the MSMs' own
+        const auto t0 = clock::now();
         if (!items.empty()) MZK_TRY(run_msms(ctx, srs.srs, srs.srs_len, items, res.data(), flags, tab, st));
         MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+        ctx->prove_ms[9] += std::chrono::duration<double, std::milli>(clock::now() - t0).count();
         return OK;
     };
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    phase_done(0);
     // ---- 1. advice (parse_advices, prover.rs:604-627), theta -------------
     items.clear();
     for (auto& p : ps) {
@@ -1063,6 +1078,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         at += ps[j].key->n_advice;
         ps[j].theta = ps[j].tr.squeeze();
     }
+    phase_done(1);
     // ---- 2. multiplicities, beta, gamma ---------------------------------
     items.clear();
     MZK_CUDA_CHECK(cudaMemsetAsync(dmiss, 0, count * 4, st));
@@ -1099,6 +1115,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         p.beta = p.tr.squeeze();
         p.gamma = p.tr.squeeze();
     }
+    phase_done(2);
     // ---- 3. permutation products, logup helper and aggregator, trash, y --
     items.clear();
     for (auto& p : ps) {
@@ -1163,6 +1180,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         p.trash = p.tr.squeeze();  // no trashcans: nothing is committed after it
         p.y = p.tr.squeeze();
     }
+    phase_done(3);
     // ---- 4. cosets, quotient limbs, x -------------------------------------
     items.clear();
     for (auto& p : ps) {
@@ -1239,6 +1257,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         p.x = p.tr.squeeze();
         p.xn = fr_pow_u64(p.x, p.key->n);
     }
+    phase_done(4);
     // ---- 5. evaluations, linearization, x1, x2 ----------------------------
     {
         std::vector<EvalTask> tasks;
@@ -1301,6 +1320,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         }
         MZK_TRY(lincomb_many(ctx, lins, st));
     }
+    phase_done(5);
     // ---- 6. q polynomials, f = sum x2^s q_s / prod (X - p), its commitment, x3
     {
         std::vector<LinSpec> qs;
@@ -1349,6 +1369,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             ps[j].x3 = ps[j].tr.squeeze();
         }
     }
+    phase_done(6);
     // ---- 7. q evaluations at x3, x4 ---------------------------------------
     {
         const bool check = (flags & MZK_PROVE_SELF_CHECK) != 0;
@@ -1376,6 +1397,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             p.x4 = p.tr.squeeze();
         }
     }
+    phase_done(7);
     // ---- 8. final polynomial and pi ---------------------------------------
     // pi = (final - v) / (X - x3) with v = final(x3); kate_division drops the
     // remainder, so the quotient of final itself is the same polynomial
@@ -1409,6 +1431,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             std::memcpy(reqs[j].proof_out, pr.data(), pr.size());
         }
     }
+    phase_done(8);
     return OK;
 }
 

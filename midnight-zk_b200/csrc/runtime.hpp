@@ -61,6 +61,11 @@ struct Context {
     int prof_used = 0;
     double phase_ms[kPhases] = {};
     uint64_t phase_count[kPhases] = {};
+    // create_proof: wall time of each Fiat-Shamir phase (every phase ends
+    // with a stream sync), of the MSMs inside them, and calls made
+    static constexpr int kProvePhases = 10;
+    double prove_ms[kProvePhases] = {};
+    uint64_t prove_calls = 0;
     // Captured CUDA graphs (a proof's NTT sequence), keyed by every pointer and
     // setting their kernels use.  buf_generation is bumped whenever ensure()
     // replaces a buffer or a domain is destroyed: graphs of an older generation
