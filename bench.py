@@ -242,8 +242,11 @@ def measure_quotient(mzk, ctx, stream, k, reps, imad_peak):
 
 
 # fixed-base window tables of the resident SRS (prover keys, batched MSMs):
-# width 20, used by MSMs of 2^18 points and more
-TABLE_C, TABLE_MIN_N = 20, 1 << 18
+# width 20, used by batched-MSM items of 2^18 points and more, and by the
+# prover's MSMs of 2^20 points and more (a single proof's 2^18-point MSMs
+# measured faster without it: the table's one 2^19-bucket reduction per MSM
+# costs more than the windows it saves at that size)
+TABLE_C, TABLE_MIN_N, PROVER_TABLE_MIN_N = 20, 1 << 18, 1 << 20
 FR_ONE_MONT = [0x00000001fffffffe, 0x5884b7fa00034802, 0x998c4fefecbc4ff5, 0x1824b159acc5056f]  # R mod r
 SERVE_KS = (14, 16, 18, 20)
 SERVE_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
@@ -258,7 +261,7 @@ class PlonkKeys:
     window table.  One seeded Config3Instance per k gives the fixed columns,
     the key (device keygen) and fresh satisfying witnesses per request."""
 
-    def __init__(self, mzk, ctx, ks, table_c=TABLE_C, table_min_n=TABLE_MIN_N):
+    def __init__(self, mzk, ctx, ks, table_c=TABLE_C, table_min_n=PROVER_TABLE_MIN_N):
         self.mzk, self.ctx, self.ks = mzk, ctx, tuple(sorted(ks))
         kmax = max(ks)
         self.srs_len = (1 << kmax) + sum(3 << k for k in ks)

@@ -612,6 +612,11 @@ int mzk_srs_read_processed(mzk_ctx *ctx, const uint8_t *bytes, size_t len, size_
 typedef struct mzk_server mzk_server;
 int mzk_server_create(mzk_ctx *ctx, uint32_t max_batch, uint32_t lanes, uint64_t mem_budget_bytes,
                       uint32_t flags /* MZK_PROVE_* of every wave */, mzk_server **out);
+/* caps the rows (sum of 2^k) of one wave (0: no cap, the default); a wave's
+ * duration grows with its rows, so the cap bounds how long a request that
+ * arrives meanwhile waits behind it.  A single request larger than the cap
+ * still runs, alone. */
+int mzk_server_set_wave_rows(mzk_server *s, uint64_t max_rows);
 int mzk_server_submit(mzk_server *s, const mzk_proof_request *req, uint64_t *ticket);
 /* blocks until the request is done (its transcript in req->proof_out);
  * latency from submit to completion */

@@ -97,6 +97,7 @@ SIGNATURES = {
     "mzk_poly_inner_product_device": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u64p, ctypes.c_void_p, _sz]),
     "mzk_logup_device": (_i32, [_vp, _vp, ctypes.c_void_p]),
     "mzk_server_create": (_i32, [_vp, _u32, _u32, _u64, _u32, ctypes.POINTER(_vp)]),
+    "mzk_server_set_wave_rows": (_i32, [_vp, _u64]),
     "mzk_server_submit": (_i32, [_vp, ctypes.c_void_p, _u64p]),
     "mzk_server_wait": (_i32, [_vp, _u64, ctypes.POINTER(ctypes.c_double)]),
     "mzk_server_stats": (_i32, [_vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_double)]),
@@ -826,13 +827,15 @@ class EvaluationDomain:
 class ProvingServer:
     """Proving service with continuous batching over create_proof (mzk_server_*)."""
 
-    def __init__(self, ctx, max_batch=16, lanes=2, mem_budget_bytes=0, per_call=False, flags=0):
+    def __init__(self, ctx, max_batch=16, lanes=2, mem_budget_bytes=0, per_call=False, flags=0, max_wave_rows=0):
         self.ctx = ctx
         h = _vp()
         fl = flags | (PROVE_PLAIN if per_call else 0)
         _check(lib().mzk_server_create(ctx.h, int(max_batch), int(lanes), int(mem_budget_bytes), fl,
                                        ctypes.byref(h)))
         self.h = h.value
+        if max_wave_rows:
+            _check(lib().mzk_server_set_wave_rows(self.h, int(max_wave_rows)))
         ctx._servers.add(self)
         self._held = {}
 

@@ -945,6 +945,8 @@ uint64_t proof_device_bytes(const mzk_plonk_key* key) {
     return (proof_scratch_elems(k) + 8) * sizeof(Fr) + msm_entries * 4;
 }
 
+uint64_t proof_rows(const mzk_plonk_key* key) { return reinterpret_cast<const PlonkKey*>(key)->n; }
+
 Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, uint32_t flags, cudaStream_t st) {
     using namespace host;
     if (count == 0) return OK;

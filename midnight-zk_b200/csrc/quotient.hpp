@@ -105,6 +105,7 @@ Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag, Fr* c
 // create_proof with the Fiat-Shamir transcript (plonk.cu)
 Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, uint32_t flags, cudaStream_t st);
 uint64_t proof_device_bytes(const mzk_plonk_key* key);
+uint64_t proof_rows(const mzk_plonk_key* key);  // 2^k of the key
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st);
 

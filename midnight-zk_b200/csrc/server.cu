@@ -46,6 +46,7 @@ struct Request {
     mzk_proof_request req;
     const void* srs = nullptr;  // the SRS buffer of its key (waves share one)
     uint64_t bytes = 0;         // device scratch of the proof
+    uint64_t rows = 0;          // 2^k of its key
     double t_submit = 0, t_done = 0;
     int status = OK;
     std::string error;
@@ -59,6 +60,7 @@ struct Server {
     uint32_t max_batch = 1;
     uint32_t flags = 0;       // MZK_PROVE_* flags of every wave
     uint64_t mem_budget = 0;  // 0: no limit
+    uint64_t max_wave_rows = 0;  // 0: no limit on the rows (sum of 2^k) of one wave
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<uint64_t> queue;
@@ -75,6 +77,7 @@ struct Server {
     std::vector<uint64_t> take_wave(uint64_t* bytes) {
         std::vector<uint64_t> batch;
         *bytes = 0;
+        uint64_t rows = 0;
         // one wave takes at most its lane's share of the budget, so the other
         // lanes can admit requests beside it
         const uint64_t lane_cap = mem_budget / lanes.size();
@@ -85,6 +88,9 @@ struct Server {
                 ++it;
                 continue;
             }
+            // a wave's duration grows with its rows: the cap keeps requests that
+            // arrive meanwhile from waiting behind one long wave
+            if (max_wave_rows && !batch.empty() && rows + r.rows > max_wave_rows) break;
             const uint64_t wave_after = *bytes + r.bytes;
             // the first proof of a wave is admitted when nothing else is in flight,
             // so a proof larger than the budget still runs (alone)
@@ -93,6 +99,7 @@ struct Server {
                               (in_flight_bytes == 0 && batch.empty());
             if (!fits) break;
             *bytes += r.bytes;
+            rows += r.rows;
             batch.push_back(*it);
             it = queue.erase(it);
         }
@@ -190,6 +197,13 @@ extern "C" int mzk_server_create(mzk_ctx* ctx, uint32_t max_batch, uint32_t lane
     return mzk::OK;
 }
 
+extern "C" int mzk_server_set_wave_rows(mzk_server* s, uint64_t max_rows) {
+    if (!s) return mzk::ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->impl.mu);
+    s->impl.max_wave_rows = max_rows;
+    return mzk::OK;
+}
+
 extern "C" int mzk_server_submit(mzk_server* s, const mzk_proof_request* req, uint64_t* ticket) {
     if (!s || !req || !ticket || !req->key || !req->advice || !req->blinds || !req->proof_out) {
         mzk::set_error("server: null argument");
@@ -203,6 +217,7 @@ extern "C" int mzk_server_submit(mzk_server* s, const mzk_proof_request* req, ui
         mzk_plonk_key_srs(req->key, &srs);
         r->srs = srs.srs;
         r->bytes = mzk::proof_device_bytes(req->key);
+        r->rows = mzk::proof_rows(req->key);
         r->t_submit = mzk::now_ms();
         const uint64_t t = s->impl.next_ticket++;
         s->impl.reqs[t] = std::move(r);
