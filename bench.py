@@ -392,7 +392,7 @@ def measure_batched_msm(mzk, ctx, reps):
                              "equals_batched": bool(np.array_equal(tabled, together))}}
 
 
-def measure_serving(mzk, ctx, keys, n_requests, reps, max_batch, lanes, mem_budget):
+def measure_serving(mzk, ctx, keys, n_requests, reps, max_batch, lanes, mem_budget, max_wave_rows):
     """A stream of create_proof requests, k drawn from SERVE_KS with
     SERVE_WEIGHTS, a fresh seeded witness per request.  Closed loop (all
     requests queued at once): every mode `reps` times, median and spread of
@@ -444,7 +444,8 @@ def measure_serving(mzk, ctx, keys, n_requests, reps, max_batch, lanes, mem_budg
     modes = {
         "plain": {"max_batch": 1, "lanes": 1, "per_call": True},           # one proof, one MSM per call
         "one_proof_batched_msms": {"max_batch": 1, "lanes": 1},            # one proof, its MSMs batched
-        "served": {"max_batch": max_batch, "lanes": lanes, "mem_budget_bytes": mem_budget},
+        "served": {"max_batch": max_batch, "lanes": lanes, "mem_budget_bytes": mem_budget,
+                   "max_wave_rows": max_wave_rows},
     }
     out = {"requests": n_requests, "k_mix": dict(zip(map(str, SERVE_KS), SERVE_WEIGHTS)), "modes": modes,
            "repetitions": reps}
@@ -738,8 +739,11 @@ def run_ours(args):
             extra_prover["create_proof_k18"] = measure_proofs(mzk, ctx, keys, 18, 8, 8)
             extra_prover["create_proof_by_k"] = {str(k): measure_proofs(mzk, ctx, keys, k, reps, b)
                                                  for k, reps, b in ((14, 32, 16), (16, 32, 16), (20, 4, 2))}
-            extra_prover["serving"] = measure_serving(mzk, ctx, keys, args.serve_requests, args.serve_reps, 16, 2,
-                                                      48 << 30)
+            # served: 3 lanes, waves of at most 16 proofs and 2^21 rows (a lane
+            # sweep on the B200 put 3 lanes and the row cap ahead of 2 lanes
+            # and uncapped waves, in throughput and in p99)
+            extra_prover["serving"] = measure_serving(mzk, ctx, keys, args.serve_requests, args.serve_reps, 16, 3,
+                                                      48 << 30, 1 << 21)
             extra_prover["prover_srs_window_table"] = keys.table
             extra_prover["prover_keygen_s"] = keys.keygen_s
             keys.close()

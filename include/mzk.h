@@ -174,6 +174,7 @@ typedef struct mzk_domain mzk_domain;
 /* EvaluationDomain::new(j, k) (domain.rs:54-167): n = 2^k, extended domain
  * 2^extended_k >= n * (j - 1), coset generator zeta; twiddle tables on ctx's GPU. */
 int mzk_domain_create(mzk_ctx *ctx, uint32_t j, uint32_t k, mzk_domain **out);
+/* destroy a domain (and the keys built over it) before the context it was created on */
 int mzk_domain_destroy(mzk_domain *d);
 int mzk_domain_shape(const mzk_domain *d, uint32_t *k, uint32_t *extended_k);
 /* domain constants (Montgomery Fr): 0 omega, 1 omega_inv, 2 extended_omega,

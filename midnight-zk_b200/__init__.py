@@ -424,12 +424,14 @@ class Context:
         self.h = h.value
         self.device = device
         # objects that hold library handles tied to this context: closed
-        # (servers first, then domains, then buffers) before the context goes
-        self._servers, self._domains, self._buffers = weakref.WeakSet(), weakref.WeakSet(), weakref.WeakSet()
+        # (servers first, then proving keys, domains, buffers) before the
+        # context goes
+        self._servers, self._keys = weakref.WeakSet(), weakref.WeakSet()
+        self._domains, self._buffers = weakref.WeakSet(), weakref.WeakSet()
 
     def close(self):
         if getattr(self, "h", None):
-            for group in (self._servers, self._domains):
+            for group in (self._servers, self._keys, self._domains):
                 for obj in list(group):
                     obj.close()
             for buf in list(self._buffers):
@@ -1027,6 +1029,7 @@ class PlonkKey:
             _check(lib().mzk_keygen(ctx.h, domain.h, ctypes.byref(cs), ctypes.byref(srs), fptrs,
                                     None if mp is None else mp.ctypes.data, pin, len(pinned), ctypes.byref(h)))
         self.h = h.value
+        ctx._keys.add(self)
         repr_, plen, nbl = np.zeros(4, np.uint64), _sz(), _sz()
         _check(lib().mzk_plonk_key_info(self.h, _ptr(repr_), ctypes.byref(plen), ctypes.byref(nbl)))
         self.repr, self.proof_len, self.n_blinds = repr_, plen.value, nbl.value
