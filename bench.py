@@ -572,6 +572,18 @@ def max_over_ranks_of(x, world, device):
     return float(t.item())
 
 
+def all_gather_u64(arr, device):
+    """torch.distributed all-gather of a small uint64 array (as int64), the
+    exchange step of the point-split MSM; the list of every rank's array."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    t = torch.from_numpy(np.ascontiguousarray(arr, np.uint64).view(np.int64)).to(device)
+    out = [torch.empty_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(out, t)
+    return [o.cpu().numpy().view(np.uint64) for o in out]
+
+
 def run_reference(args):
     world, rank, _ = dist_init("gloo")
     if rank != 0:
@@ -703,6 +715,31 @@ def run_ours(args):
         "work": "97.0k IMAD per point (reference schedule c=17, 16 windows)",
     }
 
+    # strong scaling (N > 1): one 2^log_n MSM split across the ranks by
+    # points, the partials all-gathered over NCCL and added on the host
+    point_split = None
+    if world > 1:
+        def msm_slice(b, e):
+            return ctx.msm_device(mzk.DevicePtr(ds, b * 32), mzk.DevicePtr(db, b * 96), e - b)
+
+        def split_once():
+            return mzk.msm_point_split(msm_slice, n, rank, world, lambda a: all_gather_u64(a, "cuda"))
+
+        for _ in range(2):
+            split_once()
+        times = []
+        for _ in range(max(3, args.steps // 4)):
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            split_once()
+            torch.cuda.synchronize()
+            times.append(max_over_ranks((time.perf_counter() - t0) * 1e3))
+        sms = statistics.median(times)
+        point_split = {"n": n, "ranks": world, "ms": round(sms, 3), "mpts_per_s": round(n / (sms / 1e3) / 1e6, 2),
+                       "scaling": "strong", "exchange": "one all-gather of 144-byte partials (NCCL), host add",
+                       "timing": "wall clock per split MSM, max over ranks, median of runs"}
+
     e2e = None
     if not args.no_e2e:
         hs = torch.empty(n * 4, dtype=torch.int64, pin_memory=True)
@@ -781,7 +818,7 @@ def run_ours(args):
             "fp_mul_rate_g_per_s": round(fp_mul_rate / 1e9, 2),
             "imad_probe_t_per_s": {k: round(v / 1e12, 3) for k, v in imad_variants.items()},
             "madd_in_registers_g_per_s": round(madd_rate / 1e9, 3),
-            "ntt": extra_ntt, "quotient_k18": extra_q, **extra_prover,
+            "ntt": extra_ntt, "quotient_k18": extra_q, "point_split_msm": point_split, **extra_prover,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

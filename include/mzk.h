@@ -114,6 +114,10 @@ int mzk_memcpy_d2h(mzk_ctx *ctx, void *dst, const void *src, size_t bytes);
  * scalars: n x 4 u64 (Fq, Montgomery); bases: n x 12 u64 (G1Affine). HOST pointers.
  */
 int mzk_msm_g1(mzk_ctx *ctx, const uint64_t *scalars, const uint64_t *bases, size_t n, uint64_t out[18]);
+/* Host-side sum of `count` points in the MSM result layout (z = 1 or all
+ * zero), normalised the same way: the final add of a point-split MSM, whose
+ * ranks each return the partial sum of their slice of the points. */
+int mzk_g1_sum_host(const uint64_t *points, size_t count, uint64_t out[18]);
 /* Same with DEVICE pointers (inputs resident in HBM, e.g. a device SRS). */
 int mzk_msm_g1_device(mzk_ctx *ctx, const uint64_t *d_scalars, const uint64_t *d_bases, size_t n, uint64_t out[18]);
 /*

@@ -68,6 +68,7 @@ SIGNATURES = {
     "mzk_autotune_load": (_i32, [_vp, ctypes.c_char_p]),
     "mzk_msm_g1": (_i32, [_vp, _u64p, _u64p, _sz, _u64p]),
     "mzk_msm_g1_device": (_i32, [_vp, _vp, _vp, _sz, _u64p]),
+    "mzk_g1_sum_host": (_i32, [_u64p, _sz, _u64p]),
     "mzk_msm_g1_noalloc": (_i32, [_vp, _vp, _sz, _u64p, _vp]),
     "mzk_msm_g1_batch_device": (_i32, [_vp, _vp, _sz, _vp, _sz, _u64p]),
     "mzk_msm_set_window": (_i32, [_vp, _i32]),
@@ -408,7 +409,7 @@ class LogupDesc(ctypes.Structure):
 
 
 def _dptr(x):
-    return x.ptr if isinstance(x, DeviceBuffer) else int(x)
+    return x.ptr if hasattr(x, "ptr") else int(x)
 
 
 def _ptrs(xs):
@@ -565,10 +566,8 @@ class Context:
 
     def msm_device(self, d_scalars, d_bases, n):
         """MSM over device-resident inputs (pointers or DeviceBuffers)."""
-        ds = d_scalars.ptr if isinstance(d_scalars, DeviceBuffer) else int(d_scalars)
-        db = d_bases.ptr if isinstance(d_bases, DeviceBuffer) else int(d_bases)
         out = np.zeros(18, np.uint64)
-        _check(lib().mzk_msm_g1_device(self.h, ds, db, int(n), _ptr(out)))
+        _check(lib().mzk_msm_g1_device(self.h, _dptr(d_scalars), _dptr(d_bases), int(n), _ptr(out)))
         return out
 
     def msm_batch_device(self, d_bases, bases_len, items):
@@ -1186,6 +1185,32 @@ class Config3Instance:
         buf = self.ctx.alloc(out.nbytes)
         self.ctx.gen_rand_fr(seed, self.key.n_blinds, out=buf)
         return buf.download(out.shape)
+
+
+def g1_sum(points):
+    """Sum of points in the (count, 18) MSM result layout, normalised (host)."""
+    p = np.ascontiguousarray(points, np.uint64).reshape(-1, 18)
+    out = np.zeros(18, np.uint64)
+    _check(lib().mzk_g1_sum_host(_ptr(p) if p.size else None, p.shape[0], _ptr(out)))
+    return out
+
+
+def point_split_slice(n, rank, world):
+    """The contiguous point range [begin, end) rank `rank` of `world` takes."""
+    return n * rank // world, n * (rank + 1) // world
+
+
+def msm_point_split(msm_slice, n, rank, world, all_gather):
+    """One MSM of n points split across `world` ranks: this rank computes the
+    partial sum of its slice (msm_slice(begin, end) -> 18-u64 point, e.g. an
+    MSM over device-resident scalars and bases), one all-gather exchanges the
+    144-byte partials (all_gather(array) -> list of the ranks' arrays, e.g.
+    torch.distributed over NCCL or gloo), and every rank adds them on the
+    host.  Same point as the MSM over all n points."""
+    begin, end = point_split_slice(n, rank, world)
+    part = np.ascontiguousarray(msm_slice(begin, end), np.uint64).reshape(18)
+    parts = all_gather(part)
+    return g1_sum(np.stack(parts))
 
 
 def msm_pick_window(n):

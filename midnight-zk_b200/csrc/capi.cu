@@ -10,6 +10,7 @@
 
 #include "../../include/mzk.h"
 #include "grand.hpp"
+#include "host_ec.hpp"
 #include "ntt.hpp"
 #include "quotient.hpp"
 #include "runtime.hpp"
@@ -307,6 +308,36 @@ int mzk_ctx_prove_phase_stats(mzk_ctx* ctx, double* ms_out, uint64_t* calls, int
         for (int i = 0; i < mzk::Context::kProvePhases; i++) ctx->impl.prove_ms[i] = 0.0;
         ctx->impl.prove_calls = 0;
     }
+    return mzk::OK;
+}
+
+int mzk_g1_sum_host(const uint64_t* points, size_t count, uint64_t out[18]) {
+    if (!out || (count && !points)) {
+        mzk::set_error("g1_sum: null pointer");
+        return mzk::ERR_ARG;
+    }
+    namespace h = mzk::host;
+    h::Xyzz6 acc = h::infinity();
+    for (size_t i = 0; i < count; i++) {
+        const uint64_t* p = points + 18 * i;
+        bool zero = true, one = true;
+        for (int j = 0; j < 6; j++) {
+            zero = zero && p[12 + j] == 0;
+            one = one && p[12 + j] == h::ONE6[j];
+        }
+        if (zero) continue;
+        if (!one) {
+            mzk::set_error("g1_sum: point " + std::to_string(i) + " is not normalised (z must be 1 or the point all zero)");
+            return mzk::ERR_ARG;
+        }
+        h::Xyzz6 q;
+        std::memcpy(q.x.l, p, 48);
+        std::memcpy(q.y.l, p + 6, 48);
+        q.zz = h::one();
+        q.zzz = h::one();
+        acc = h::add(acc, q);
+    }
+    h::to_jacobian_normalised(acc, out);
     return mzk::OK;
 }
 
