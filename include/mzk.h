@@ -454,6 +454,28 @@ int mzk_keygen_from_values(mzk_ctx *ctx, mzk_domain *d, const mzk_circuit_desc *
                            const uint64_t *const *fixed_values, const uint64_t *const *perm_values,
                            const uint8_t *pinned, size_t pinned_len, mzk_plonk_key **out);
 int mzk_plonk_key_destroy(mzk_plonk_key *key);
+/* Key files (VerifyingKey::write / ProvingKey::write, plonk/mod.rs:95-113,
+ * 391-399; readers :120-196, :418-453) in SerdeFormat (utils/helpers.rs:
+ * 17-28): Processed writes commitments compressed (48 bytes), RawBytes and
+ * RawBytesUnchecked uncompressed (96 bytes); the polynomial slices of a PK
+ * are always raw Montgomery limbs (u32 big-endian counts and lengths).  A VK
+ * file is version 0x03, k, a u32 little-endian count and the fixed
+ * commitments, then the permutation commitments; a PK file is its VK file,
+ * the fixed columns' values and the permutation polynomials' values.
+ * mzk_vk_write / mzk_pk_write: *len = the file's size; out may be null to ask
+ * for it.  mzk_pk_read: a key from a PK file for the constraint system cs
+ * (the reader's ConcreteCircuit::configure) over domain d and the SRS, with
+ * the file's commitments (decoded and checked: encoding, x, y < p, curve and
+ * subgroup; RawBytesUnchecked checks nothing) and values (below r unless
+ * RawBytesUnchecked), as ProvingKey::read derives the rest. */
+#define MZK_SERDE_PROCESSED 0
+#define MZK_SERDE_RAW 1
+#define MZK_SERDE_RAW_UNCHECKED 2
+int mzk_vk_write(const mzk_plonk_key *key, int format, uint8_t *out, size_t cap, size_t *len);
+int mzk_pk_write(mzk_ctx *ctx, const mzk_plonk_key *key, int format, uint8_t *out, size_t cap, size_t *len);
+int mzk_pk_read(mzk_ctx *ctx, mzk_domain *d, const mzk_circuit_desc *cs, const mzk_srs_desc *srs,
+                const uint8_t *bytes, size_t len, int format, const uint8_t *pinned, size_t pinned_len,
+                mzk_plonk_key **out);
 /* The transcript operations of one proof of this key, in order: one code per
  * operation (MZK_TR_*).  A caller holding its own transcript object (the
  * reference's CircuitTranscript) replays a proof into it with these: a

@@ -116,6 +116,10 @@ SIGNATURES = {
     "mzk_keygen_from_values": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p, _sz, ctypes.POINTER(_vp)]),
     "mzk_plonk_key_transcript_layout": (_i32, [_vp, ctypes.c_void_p, _sz, ctypes.POINTER(_sz)]),
+    "mzk_vk_write": (_i32, [_vp, _i32, ctypes.c_void_p, _sz, ctypes.POINTER(_sz)]),
+    "mzk_pk_write": (_i32, [_vp, _vp, _i32, ctypes.c_void_p, _sz, ctypes.POINTER(_sz)]),
+    "mzk_pk_read": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _sz, _i32, ctypes.c_void_p,
+                           _sz, ctypes.POINTER(_vp)]),
     "mzk_plonk_key_destroy": (_i32, [_vp]),
     "mzk_plonk_key_info": (_i32, [_vp, _u64p, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
     "mzk_plonk_key_commitments": (_i32, [_vp, ctypes.c_void_p, ctypes.c_void_p]),
@@ -153,6 +157,7 @@ class ProofJob(ctypes.Structure):
                 ("lookup_blinds", (ctypes.c_uint64 * 4) * 8)]
 
 
+SERDE_PROCESSED, SERDE_RAW, SERDE_RAW_UNCHECKED = 0, 1, 2  # SerdeFormat (MZK_SERDE_*)
 PROVE_MSM_PER_CALL = 1  # MZK_PROVE_MSM_PER_CALL
 PROVE_NO_GRAPHS = 2  # MZK_PROVE_NO_GRAPHS
 PROVE_SELF_CHECK = 4  # MZK_PROVE_SELF_CHECK
@@ -978,7 +983,10 @@ class PlonkKey:
     host (n, 4) arrays; mapping: (n_perm_cols, n, 2) uint32 or None; srs:
     an SrsDesc.  The domain and the SRS buffer must outlive the key."""
 
-    def __init__(self, ctx, domain, circuit, srs, fixed_values, mapping=None, pinned=b"", perm_values=None):
+    def __init__(self, ctx, domain, circuit, srs, fixed_values=None, mapping=None, pinned=b"", perm_values=None,
+                 pk_bytes=None, pk_format=SERDE_PROCESSED):
+        """fixed_values (+ mapping or perm_values): keygen; pk_bytes: a key
+        read from a ProvingKey file (ProvingKey::read) in pk_format."""
         self.ctx, self.domain, self.circuit = ctx, domain, circuit
         keep = []
 
@@ -1011,13 +1019,19 @@ class PlonkKey:
         cs.n_lookups = len(lks)
         cs.lookups = arr(LookupShape, [LookupShape(lk["input"], lk["table"],
                                                    -1 if lk["selector"] is None else lk["selector"]) for lk in lks])
+        pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
+        h = _vp()
+        if pk_bytes is not None:
+            data = bytes(pk_bytes)
+            _check(lib().mzk_pk_read(ctx.h, domain.h, ctypes.byref(cs), ctypes.byref(srs), data, len(data), pk_format,
+                                     pin, len(pinned), ctypes.byref(h)))
+            self._finish(h)
+            return
         cols = [np.ascontiguousarray(v, np.uint64) for v in fixed_values]
         if any(c.shape != (domain.n, 4) for c in cols):
             raise MzkError(1, "keygen: every fixed column needs n Fr values")
         fptrs = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
         mp = None if mapping is None else np.ascontiguousarray(mapping, np.uint32)
-        pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
-        h = _vp()
         if perm_values is not None:
             pv = [np.ascontiguousarray(v, np.uint64) for v in perm_values]
             keep.append(pv)
@@ -1027,6 +1041,11 @@ class PlonkKey:
         else:
             _check(lib().mzk_keygen(ctx.h, domain.h, ctypes.byref(cs), ctypes.byref(srs), fptrs,
                                     None if mp is None else mp.ctypes.data, pin, len(pinned), ctypes.byref(h)))
+        self._finish(h)
+
+    def _finish(self, h):
+        ctx, circuit = self.ctx, self.circuit
+        pc = circuit["perm_cols"]
         self.h = h.value
         ctx._keys.add(self)
         repr_, plen, nbl = np.zeros(4, np.uint64), _sz(), _sz()
@@ -1035,6 +1054,22 @@ class PlonkKey:
         self.fixed_coms = np.zeros((circuit["n_fixed"], 18), np.uint64)
         self.perm_coms = np.zeros((len(pc), 18), np.uint64)
         _check(lib().mzk_plonk_key_commitments(self.h, self.fixed_coms.ctypes.data, self.perm_coms.ctypes.data))
+
+    def vk_bytes(self, fmt=SERDE_PROCESSED):
+        """VerifyingKey::write (plonk/mod.rs:95-113) of this key."""
+        n = _sz()
+        _check(lib().mzk_vk_write(self.h, fmt, None, 0, ctypes.byref(n)))
+        buf = (ctypes.c_uint8 * max(1, n.value))()
+        _check(lib().mzk_vk_write(self.h, fmt, buf, n.value, ctypes.byref(n)))
+        return bytes(buf[:n.value])
+
+    def pk_bytes(self, fmt=SERDE_PROCESSED):
+        """ProvingKey::write (plonk/mod.rs:391-399) of this key."""
+        n = _sz()
+        _check(lib().mzk_pk_write(self.ctx.h, self.h, fmt, None, 0, ctypes.byref(n)))
+        buf = (ctypes.c_uint8 * max(1, n.value))()
+        _check(lib().mzk_pk_write(self.ctx.h, self.h, fmt, buf, n.value, ctypes.byref(n)))
+        return bytes(buf[:n.value])
 
     def transcript_layout(self):
         """The MZK_TR_* operation codes of one proof, in order."""

@@ -46,6 +46,7 @@
 #include "ntt.hpp"
 #include "quotient.hpp"
 #include "runtime.hpp"
+#include "srs.hpp"
 #include "transcript.hpp"
 
 namespace mzk {
@@ -441,9 +442,11 @@ Status vk_transcript_repr(uint32_t k, const uint64_t* fixed, size_t n_fixed, con
 // perm_values (host, n_perm_cols columns of n Fr): the permutation
 // polynomials' Lagrange values as given (ProvingKey::read, permutation.rs:
 // 153-166); otherwise they are built from `mapping` (or the identity)
+// given_coms (optional, host): the fixed then permutation commitments in the
+// 18-u64 layout, as a key file holds them; otherwise they are computed
 Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const mzk_srs_desc* srs,
               const uint64_t* const* fixed_values, const uint32_t* mapping, const uint64_t* const* perm_values,
-              const uint8_t* pinned, size_t pinned_len, PlonkKey** out) {
+              const uint8_t* pinned, size_t pinned_len, PlonkKey** out, const uint64_t* given_coms = nullptr) {
     MZK_TRY(check_circuit(d, cs));
     const uint32_t n = 1u << d->k, E = 1u << d->ext_k;
     if (!srs || !srs->srs) {
@@ -642,7 +645,8 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     for (uint32_t i = 0; i < P; i++) items.push_back({key->perm_lag[i], srs->off_lagrange, n});
     std::vector<uint64_t> res(items.size() * 18);
     MsmTable table{srs->srs, srs->srs_len, srs->table_c, srs->table_rows, srs->table_min_n};
-    if (!items.empty())
+    if (given_coms) std::memcpy(res.data(), given_coms, res.size() * 8);
+    else if (!items.empty())
         MZK_TRY(run_msms(ctx, srs->srs, srs->srs_len, items, res.data(), 0, srs->table_c > 0 ? &table : nullptr, st));
     MZK_CUDA_CHECK(cudaStreamSynchronize(st));
     key->fixed_coms.resize(F);
@@ -678,6 +682,239 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
                     (key->qdeg - 1);
     *out = key.release();
     return OK;
+}
+
+// ------------------------------------------------------ key file formats ----
+// VerifyingKey::write / ProvingKey::write (plonk/mod.rs:95-113, 391-399) and
+// their readers (:120-196, :418-453).  SerdeFormat: Processed writes points
+// compressed (48 bytes); RawBytes and RawBytesUnchecked write them
+// uncompressed (96 bytes, G1Affine::to_uncompressed); field elements of the
+// polynomial slices are always the raw Montgomery limbs (Fq::write_raw,
+// fq.rs:912-917), each slice a u32 big-endian count of polynomials, each
+// polynomial a u32 big-endian length (helpers.rs:150-160, poly/mod.rs:544-550).
+namespace {
+
+void put_u32_le(std::vector<uint8_t>& v, uint32_t x) {
+    for (int b = 0; b < 4; b++) v.push_back((uint8_t)(x >> (8 * b)));
+}
+void put_u32_be(std::vector<uint8_t>& v, uint32_t x) {
+    for (int b = 3; b >= 0; b--) v.push_back((uint8_t)(x >> (8 * b)));
+}
+void put_point(std::vector<uint8_t>& v, const uint64_t* p18, int format) {
+    uint8_t enc[96];
+    if (format == MZK_SERDE_PROCESSED) {
+        host::g1_compress(p18, enc);
+        v.insert(v.end(), enc, enc + 48);
+    } else {
+        host::g1_uncompressed(p18, enc);
+        v.insert(v.end(), enc, enc + 96);
+    }
+}
+
+struct Reader {
+    const uint8_t* p;
+    size_t len, pos = 0;
+    bool take(size_t m, const uint8_t** out) {
+        if (len - pos < m) return false;
+        *out = p + pos;
+        pos += m;
+        return true;
+    }
+};
+
+// points of a key file into the 18-u64 layout.  Compressed encodings go
+// through the device decompression (flags, x < p, square root, subgroup);
+// uncompressed ones are recompressed and decompressed the same way, and the
+// decoded y must equal the given one (RawBytes), or are taken as they are
+// (RawBytesUnchecked)
+Status decode_points(Context* ctx, const std::vector<const uint8_t*>& enc, int format,
+                     std::vector<std::array<uint64_t, 18>>& pts, cudaStream_t st) {
+    const size_t m = enc.size();
+    pts.assign(m, {});
+    if (m == 0) return OK;
+    host::Fp6 r2;
+    static const uint64_t kR2[6] = {0xf4df1f341c341746ULL, 0x0a76e6a609d104f1ULL, 0x8de5476c4c95b6d5ULL,
+                                    0x67eb88a9939d83c0ULL, 0x9a793e85b519952dULL, 0x11988fe592cae3aaULL};
+    std::memcpy(r2.l, kR2, 48);
+    auto be48 = [](const uint8_t* b, uint64_t out[6]) {
+        for (int i = 0; i < 6; i++) {
+            uint64_t w = 0;
+            for (int k = 0; k < 8; k++) w = (w << 8) | b[47 - (8 * i + 7 - k)];
+            out[i] = w;
+        }
+    };
+    std::vector<uint8_t> comp(m * 48);
+    std::vector<std::array<uint64_t, 6>> ys(m);
+    for (size_t i = 0; i < m; i++) {
+        const uint8_t* e = enc[i];
+        if (format == MZK_SERDE_PROCESSED) {
+            std::memcpy(&comp[48 * i], e, 48);
+            continue;
+        }
+        // uncompressed: flags 0x80 (compressed) and 0x20 (sort) must be clear
+        if (e[0] & 0xa0) {
+            set_error("key file: bad uncompressed point encoding");
+            return ERR_ARG;
+        }
+        if (e[0] & 0x40) {  // identity: every other bit zero
+            for (int b = 1; b < 96; b++)
+                if (e[b]) {
+                    set_error("key file: bad identity encoding");
+                    return ERR_ARG;
+                }
+            if (e[0] != 0x40) {
+                set_error("key file: bad identity encoding");
+                return ERR_ARG;
+            }
+            std::memset(&comp[48 * i], 0, 48);
+            comp[48 * i] = 0xc0;
+            ys[i].fill(0);
+            continue;
+        }
+        uint64_t x[6], y[6];
+        be48(e, x);
+        be48(e + 48, y);
+        if (host::geq6(x, host::P6) || host::geq6(y, host::P6)) {
+            set_error("key file: coordinate not below p");
+            return ERR_ARG;
+        }
+        host::Fp6 xc, yc;
+        std::memcpy(xc.l, x, 48);
+        std::memcpy(yc.l, y, 48);
+        const host::Fp6 xm = host::canon(host::mul(xc, r2)), ym = host::canon(host::mul(yc, r2));
+        if (format == MZK_SERDE_RAW_UNCHECKED) {
+            std::memcpy(pts[i].data(), xm.l, 48);
+            std::memcpy(pts[i].data() + 6, ym.l, 48);
+            std::memcpy(pts[i].data() + 12, host::ONE6, 48);
+            continue;
+        }
+        std::memcpy(ys[i].data(), ym.l, 48);
+        uint64_t p18[18];
+        std::memcpy(p18, xm.l, 48);
+        std::memcpy(p18 + 6, ym.l, 48);
+        std::memcpy(p18 + 12, host::ONE6, 48);
+        host::g1_compress(p18, &comp[48 * i]);
+    }
+    if (format == MZK_SERDE_RAW_UNCHECKED) return OK;
+    void *d_in, *d_out, *d_st;
+    MZK_TRY(ctx->ensure("kf_enc", m * 48, &d_in));
+    MZK_TRY(ctx->ensure("kf_aff", m * 96, &d_out));
+    MZK_TRY(ctx->ensure("kf_status", m, &d_st));
+    MZK_CUDA_CHECK(cudaMemcpyAsync(d_in, comp.data(), m * 48, cudaMemcpyHostToDevice, st));
+    uint64_t invalid = 0;
+    MZK_TRY(g1_decompress_device(ctx, d_in, m, 1, d_out, static_cast<uint8_t*>(d_st), &invalid, st));
+    std::vector<uint64_t> aff(m * 12);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(aff.data(), d_out, m * 96, cudaMemcpyDeviceToHost, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (invalid) {
+        set_error("key file: " + std::to_string(invalid) + " invalid point(s) (encoding, curve or subgroup)");
+        return ERR_ARG;
+    }
+    for (size_t i = 0; i < m; i++) {
+        const uint64_t* a = &aff[12 * i];
+        bool zero = true;
+        for (int j = 0; j < 12; j++) zero = zero && a[j] == 0;
+        std::memcpy(pts[i].data(), a, 96);
+        if (!zero) std::memcpy(pts[i].data() + 12, host::ONE6, 48);
+        if (format == MZK_SERDE_RAW && !zero && std::memcmp(a + 6, ys[i].data(), 48) != 0) {
+            set_error("key file: point not on the curve");
+            return ERR_ARG;
+        }
+    }
+    return OK;
+}
+
+}  // namespace
+
+Status vk_serialize(const PlonkKey* k, int format, std::vector<uint8_t>& out) {
+    out.clear();
+    out.push_back(0x03);
+    out.push_back((uint8_t)k->k);
+    put_u32_le(out, (uint32_t)k->fixed_coms.size());
+    for (auto& c : k->fixed_coms) put_point(out, c.data(), format);
+    for (auto& c : k->perm_coms) put_point(out, c.data(), format);
+    return OK;
+}
+
+Status pk_serialize(Context* ctx, const PlonkKey* k, int format, std::vector<uint8_t>& out, cudaStream_t st) {
+    MZK_TRY(vk_serialize(k, format, out));
+    std::vector<uint8_t> vals((size_t)k->n * 32);
+    auto slice = [&](const std::vector<Fr*>& cols) -> Status {
+        put_u32_be(out, (uint32_t)cols.size());
+        for (Fr* c : cols) {
+            put_u32_be(out, k->n);
+            MZK_CUDA_CHECK(cudaMemcpyAsync(vals.data(), c, vals.size(), cudaMemcpyDeviceToHost, st));
+            MZK_CUDA_CHECK(cudaStreamSynchronize(st));
+            out.insert(out.end(), vals.begin(), vals.end());  // raw Montgomery limbs, little-endian
+        }
+        return OK;
+    };
+    MZK_TRY(slice(k->fixed_lag));
+    MZK_TRY(slice(k->perm_lag));
+    return OK;
+}
+
+Status pk_read(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const mzk_srs_desc* srs,
+               const uint8_t* bytes, size_t len, int format, const uint8_t* pinned, size_t pinned_len,
+               PlonkKey** out, cudaStream_t st) {
+    auto fail = [](const std::string& m) {
+        set_error("pk_read: " + m);
+        return ERR_ARG;
+    };
+    Reader r{bytes, len};
+    const uint8_t* p;
+    if (!r.take(2, &p)) return fail("short file");
+    if (p[0] != 0x03) return fail("unexpected version byte");
+    if (p[1] != d->k) return fail("k of the file differs from the domain's");
+    if (!r.take(4, &p)) return fail("short file");
+    const uint32_t nf = (uint32_t)p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24;
+    if (nf != cs->n_fixed) return fail("fixed column count differs from the constraint system's");
+    const size_t psz = format == MZK_SERDE_PROCESSED ? 48 : 96;
+    std::vector<const uint8_t*> enc;
+    for (uint32_t i = 0; i < nf + cs->n_perm_cols; i++) {
+        if (!r.take(psz, &p)) return fail("short file");
+        enc.push_back(p);
+    }
+    std::vector<std::array<uint64_t, 18>> pts;
+    MZK_TRY(decode_points(ctx, enc, format, pts, st));
+    std::vector<uint64_t> coms(pts.size() * 18);
+    for (size_t i = 0; i < pts.size(); i++) std::memcpy(&coms[18 * i], pts[i].data(), 144);
+    const uint32_t n = 1u << d->k;
+    auto read_slice = [&](uint32_t expect, std::vector<const uint64_t*>& cols) -> Status {
+        if (!r.take(4, &p)) return fail("short file");
+        const uint32_t cnt = (uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3];
+        if (cnt != expect) return fail("polynomial count differs from the constraint system's");
+        for (uint32_t c = 0; c < cnt; c++) {
+            if (!r.take(4, &p)) return fail("short file");
+            const uint32_t pl = (uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3];
+            if (pl != n) return fail("polynomial length differs from the domain's");
+            if (!r.take((size_t)n * 32, &p)) return fail("short file");
+            const uint64_t* v = reinterpret_cast<const uint64_t*>(p);  // raw little-endian limbs
+            if (format != MZK_SERDE_RAW_UNCHECKED)
+                for (uint32_t i = 0; i < n; i++)
+                    if (host::fr_geq(v + 4 * (size_t)i, host::R4)) return fail("field element not below r");
+            cols.push_back(v);
+        }
+        return OK;
+    };
+    std::vector<const uint64_t*> fixed, perm;
+    MZK_TRY(read_slice(cs->n_fixed, fixed));
+    MZK_TRY(read_slice(cs->n_perm_cols, perm));
+    if (r.pos != len) return fail("trailing bytes");
+    // the limbs are read in place: copy them to aligned host columns
+    std::vector<std::vector<uint64_t>> fcols(fixed.size()), pcols(perm.size());
+    std::vector<const uint64_t*> fptr, pptr;
+    for (size_t i = 0; i < fixed.size(); i++) {
+        fcols[i].resize((size_t)4 * n);
+        std::memcpy(fcols[i].data(), fixed[i], (size_t)n * 32);
+        fptr.push_back(fcols[i].data());
+    }
+    for (size_t i = 0; i < perm.size(); i++) {
+        pcols[i].resize((size_t)4 * n);
+        std::memcpy(pcols[i].data(), perm[i], (size_t)n * 32);
+        pptr.push_back(pcols[i].data());
+    }
+    return keygen(ctx, d, cs, srs, fptr.data(), nullptr, pptr.data(), pinned, pinned_len, out, coms.data());
 }
 
 // --------------------------------------------------------------- prover ----
@@ -1540,7 +1777,65 @@ int mzk_keygen_from_values(mzk_ctx* ctx, mzk_domain* d, const mzk_circuit_desc* 
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     cudaSetDevice(c->device);
     mzk::PlonkKey* key = nullptr;
-    MZK_TRY(mzk::keygen(c, mzk::domain_of(d), cs, srs, fixed_values, nullptr, perm_values, pinned, pinned_len, &key));
+    MZK_TRY(mzk::keygen(c, mzk::domain_of(d), cs, srs, fixed_values, nullptr, perm_values, pinned, pinned_len,
+                        &key));
+    *out = reinterpret_cast<mzk_plonk_key*>(key);
+    return mzk::OK;
+}
+
+int mzk_vk_write(const mzk_plonk_key* key, int format, uint8_t* out, size_t cap, size_t* len) {
+    if (!key || !len || format < 0 || format > 2) return mzk::ERR_ARG;
+    std::vector<uint8_t> v;
+    MZK_TRY(mzk::vk_serialize(reinterpret_cast<const mzk::PlonkKey*>(key), format, v));
+    *len = v.size();
+    if (out) {
+        if (cap < v.size()) {
+            mzk::set_error("vk_write: output buffer too small");
+            return mzk::ERR_ARG;
+        }
+        std::memcpy(out, v.data(), v.size());
+    }
+    return mzk::OK;
+}
+
+int mzk_pk_write(mzk_ctx* ctx, const mzk_plonk_key* key, int format, uint8_t* out, size_t cap, size_t* len) {
+    if (!ctx || !key || !len || format < 0 || format > 2) return mzk::ERR_ARG;
+    mzk::Context* c = mzk::context_of(ctx);
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    const mzk::PlonkKey* k = reinterpret_cast<const mzk::PlonkKey*>(key);
+    const size_t psz = format == MZK_SERDE_PROCESSED ? 48 : 96;
+    const size_t need = 6 + psz * (k->fixed_coms.size() + k->perm_coms.size()) + 8 +
+                        (k->fixed_coms.size() + k->perm_coms.size()) * (4 + (size_t)k->n * 32);
+    *len = need;
+    if (!out) return mzk::OK;
+    if (cap < need) {
+        mzk::set_error("pk_write: output buffer too small");
+        return mzk::ERR_ARG;
+    }
+    std::vector<uint8_t> v;
+    MZK_TRY(mzk::pk_serialize(c, k, format, v, c->stream));
+    if (v.size() != need) {
+        mzk::set_error("pk_write: internal size mismatch");
+        return mzk::ERR_STATE;
+    }
+    std::memcpy(out, v.data(), v.size());
+    return mzk::OK;
+}
+
+int mzk_pk_read(mzk_ctx* ctx, mzk_domain* d, const mzk_circuit_desc* cs, const mzk_srs_desc* srs,
+                const uint8_t* bytes, size_t len, int format, const uint8_t* pinned, size_t pinned_len,
+                mzk_plonk_key** out) {
+    if (!ctx || !d || !cs || !out || !bytes || format < 0 || format > 2 || (pinned_len && !pinned)) {
+        mzk::set_error("pk_read: bad argument");
+        return mzk::ERR_ARG;
+    }
+    *out = nullptr;
+    mzk::Context* c = mzk::context_of(ctx);
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    mzk::PlonkKey* key = nullptr;
+    MZK_TRY(mzk::pk_read(c, mzk::domain_of(d), cs, srs, bytes, len, format, pinned, pinned_len, &key, c->stream));
     *out = reinterpret_cast<mzk_plonk_key*>(key);
     return mzk::OK;
 }

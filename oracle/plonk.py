@@ -538,6 +538,31 @@ def vk_transcript_repr(k, fixed_coms, perm_coms, pinned_repr):
     return from_uniform_bytes(hashlib.blake2b(bytes(buf), digest_size=64, person=VK_PERSONAL).digest())
 
 
+def vk_bytes(key, processed=True):
+    """VerifyingKey::write (plonk/mod.rs:95-113): version, k, the u32 LE count
+    and the fixed commitments, then the permutation commitments; points
+    compressed (SerdeFormat::Processed) or uncompressed (RawBytes*)
+    (utils/helpers.rs:94-104)."""
+    enc = compress if processed else uncompressed
+    out = bytearray([VK_VERSION, key.circuit["k"]]) + len(key.fixed_coms).to_bytes(4, "little")
+    for c in key.fixed_coms + key.perm_coms:
+        out += enc(c)
+    return bytes(out)
+
+
+def pk_bytes(key, processed=True):
+    """ProvingKey::write (plonk/mod.rs:391-399): the VK, then the fixed
+    columns' values and the permutation polynomials' values as polynomial
+    slices (u32 BE count, per polynomial a u32 BE length and the raw Montgomery
+    limbs, helpers.rs:150-160, poly/mod.rs:544-550, fq.rs:912-917)."""
+    out = bytearray(vk_bytes(key, processed))
+    for cols in (key.fixed_values, key.perm_values):
+        out += len(cols).to_bytes(4, "big")
+        for c in cols:
+            out += c.shape[0].to_bytes(4, "big") + np.ascontiguousarray(c, "<u8").tobytes()
+    return bytes(out)
+
+
 # ------------------------------------------------------- shared identities --
 def l_i_range(key, x, xn, rotations):
     """EvaluationDomain::l_i_range (domain.rs:487-512): l_i(x) =

@@ -191,3 +191,57 @@ def test_generic_circuit_proof_equals_oracle(ctx, k):
     bad[3][2] = OP.to_mont(OP.to_int(bad[3][2]) + 1)
     with pytest.raises(mzk.MzkError, match="does not satisfy"):
         mzk.create_proofs(ctx, [(c.key, bad, bl)], flags=mzk.PROVE_SELF_CHECK)
+
+
+def test_key_files_equal_oracle_and_read_back(ctx, k5):
+    """VerifyingKey / ProvingKey files in the three SerdeFormats equal the
+    oracle's bytes; a key read from a PK file has the same transcript_repr and
+    gives the same proofs; damaged files are refused."""
+    key, ok = k5.key, k5.okey
+    for fmt, processed in ((mzk.SERDE_PROCESSED, True), (mzk.SERDE_RAW, False), (mzk.SERDE_RAW_UNCHECKED, False)):
+        assert key.vk_bytes(fmt) == OP.vk_bytes(ok, processed), fmt
+        pk = key.pk_bytes(fmt)
+        assert pk == OP.pk_bytes(ok, processed), fmt
+        back = mzk.PlonkKey(ctx, k5.dom, k5.circuit, k5.desc, pk_bytes=pk, pk_format=fmt,
+                            pinned=b"config-3 circuit: standard gate, copy cycles, range lookup")
+        assert np.array_equal(back.repr, key.repr) and back.pk_bytes(fmt) == pk
+        bl = k5.blinds(11)
+        assert mzk.create_proofs(ctx, [(back, k5.advice, bl)]) == mzk.create_proofs(ctx, [(key, k5.advice, bl)])
+        back.close()
+    pk = key.pk_bytes(mzk.SERDE_RAW)
+    bad_cases = {
+        "version": b"\x02" + pk[1:],
+        "truncated": pk[:-1],
+        "trailing": pk + b"\x00",
+        "not below r": pk[:-32] + b"\xff" * 32,
+        "not on the curve": pk[:6] + pk[6:54] + bytes(47) + b"\x05" + pk[102:],
+    }
+    for name, data in bad_cases.items():
+        with pytest.raises(mzk.MzkError):
+            mzk.PlonkKey(ctx, k5.dom, k5.circuit, k5.desc, pk_bytes=data, pk_format=mzk.SERDE_RAW)
+        assert name
+
+
+def test_transcript_layout_replays_the_proof(k5):
+    """A caller with its own transcript object replays a proof from the key's
+    transcript layout: the same absorbs and squeezes rebuild the same proof
+    bytes."""
+    from oracle import oracle as O
+    proof = mzk.create_proofs(k5.ctx, [(k5.key, k5.advice, k5.blinds(12))])[0]
+    t, pos = mzk.Transcript(), 0
+    for op in k5.key.transcript_layout():
+        if op == 0:
+            t.common_fr(k5.key.repr)
+        elif op == 1:
+            st, aff = O.g1_decompress(proof[pos:pos + 48])
+            p18 = np.zeros(18, np.uint64)
+            if np.any(aff):
+                p18[:12], p18[12:] = aff, O.fp_const(0)
+            t.write_point(p18)
+            pos += 48
+        elif op == 2:
+            t.write_fr(OP.to_mont(int.from_bytes(proof[pos:pos + 32], "little")))
+            pos += 32
+        else:
+            t.squeeze_challenge()
+    assert pos == len(proof) and t.finalize() == proof
