@@ -33,7 +33,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr uint32_t kInvChunk = 64;  // elements per thread of a batch inversion
-constexpr uint32_t kRecChunk = 64;  // elements per thread of a linear recurrence
+// elements per thread of a linear recurrence: up to 64, fewer when n is too
+// small to give every SM work (each thread's chunk is a serial chain)
+constexpr uint32_t kRecChunkMax = 64, kRecChunkMin = 4;
 constexpr uint32_t kScanItems = 8;  // elements per thread of a block scan
 constexpr uint32_t kMaxPermSetCols = 8;
 constexpr uint32_t kMaxLogupChunks = 8;
@@ -195,11 +197,11 @@ Status scan_exclusive(Context* ctx, const Fr* in, Fr* out, uint64_t n, cudaStrea
 // records L_t = its local y at tK; the true values at the chunk starts solve
 // the same recurrence over the L_t with k^K; a last pass adds k^(hi-i) Y_{t+1}.
 __global__ void __launch_bounds__(kThreads) k_rec_local(const Fr* __restrict__ c, Fr* __restrict__ y, uint64_t n,
-                                                        Fr k, Fr* __restrict__ lows) {
+                                                        Fr k, Fr* __restrict__ lows, uint32_t K) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t lo = t * kRecChunk;
+    const uint64_t lo = t * K;
     if (lo >= n) return;
-    const uint64_t hi = min(n, lo + kRecChunk);
+    const uint64_t hi = min(n, lo + K);
     Fr acc = fr_zero();
     for (uint64_t i = hi; i-- > lo;) {
         acc = fr_add(c[i], fr_mul(k, acc));
@@ -208,10 +210,10 @@ __global__ void __launch_bounds__(kThreads) k_rec_local(const Fr* __restrict__ c
     lows[t] = acc;
 }
 __global__ void __launch_bounds__(kThreads) k_rec_fix(Fr* __restrict__ y, uint64_t n, Fr k,
-                                                      const Fr* __restrict__ starts, uint64_t chunks) {
+                                                      const Fr* __restrict__ starts, uint64_t chunks, uint32_t K) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t + 1 >= chunks) return;  // the top chunk has a zero carry-in
-    const uint64_t lo = t * kRecChunk, hi = lo + kRecChunk;
+    const uint64_t lo = t * K, hi = lo + K;
     const Fr carry = starts[t + 1];
     Fr pw = k;  // k^(hi - i) for i = hi - 1
     for (uint64_t i = hi; i-- > lo;) {
@@ -223,18 +225,23 @@ __global__ void __launch_bounds__(kThreads) k_rec_fix(Fr* __restrict__ y, uint64
 // y (n) from c (n), in and out may not alias
 Status linrec_suffix(Context* ctx, const Fr* c, Fr* y, uint64_t n, const host::Fr4& k, cudaStream_t st, int depth = 0) {
     if (n == 0) return OK;
-    const uint64_t chunks = (n + kRecChunk - 1) / kRecChunk;
+    // the chunk length: 64 while that leaves at least 2 threads of 256 per SM
+    // per warp slot, down to 4 for smaller n; small recursion levels keep 64
+    uint32_t K = kRecChunkMax;
+    const uint64_t want_threads = (uint64_t)ctx->num_sms * kThreads * 2;
+    while (K > kRecChunkMin && n / K < want_threads && n > (uint64_t)kRecChunkMax * kRecChunkMax) K >>= 1;
+    const uint64_t chunks = (n + K - 1) / K;
     void* lows;
     MZK_TRY(ctx->ensure(("grand_rec_" + std::to_string(depth)).c_str(), 2 * chunks * sizeof(Fr), &lows));
     Fr* L = (Fr*)lows;
     Fr* Y = L + chunks;
-    k_rec_local<<<(uint32_t)((chunks + kThreads - 1) / kThreads), kThreads, 0, st>>>(c, y, n, to_dev(k), L);
+    k_rec_local<<<(uint32_t)((chunks + kThreads - 1) / kThreads), kThreads, 0, st>>>(c, y, n, to_dev(k), L, K);
     MZK_LAUNCH_CHECK(ctx);
     if (chunks > 1) {
-        host::Fr4 kk = k;  // k^kRecChunk
-        for (uint32_t b = 1; b < kRecChunk; b <<= 1) kk = host::fr_mul(kk, kk);
+        host::Fr4 kk = k;  // k^K
+        for (uint32_t b = 1; b < K; b <<= 1) kk = host::fr_mul(kk, kk);
         MZK_TRY(linrec_suffix(ctx, L, Y, chunks, kk, st, depth + 1));
-        k_rec_fix<<<(uint32_t)((chunks + kThreads - 1) / kThreads), kThreads, 0, st>>>(y, n, to_dev(k), Y, chunks);
+        k_rec_fix<<<(uint32_t)((chunks + kThreads - 1) / kThreads), kThreads, 0, st>>>(y, n, to_dev(k), Y, chunks, K);
         MZK_LAUNCH_CHECK(ctx);
     }
     return OK;
