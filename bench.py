@@ -60,6 +60,9 @@ def parse_args():
     p.add_argument("--no-extras", action="store_true", help="skip the NTT and quotient lines")
     p.add_argument("--ntt-log-n", type=int, default=24)
     p.add_argument("--no-prover", action="store_true", help="skip the proof-core, batched-MSM and serving lines")
+    p.add_argument("--create-proof-only", type=int, default=0, metavar="K",
+                   help="only time create_proof of the single-proof configuration at 2^K rows (profiling)")
+    p.add_argument("--prover-batch", type=int, default=8, help="proofs per call in --create-proof-only")
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-reps", type=int, default=3)
     return p.parse_args()
@@ -621,6 +624,28 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
+def run_create_proof_only(args):
+    """create_proof of config 3 at 2^K rows, one proof per call and batches of
+    --prover-batch (a short run for profilers); prints one JSON line."""
+    from _loader import load
+    mzk = load()
+    ctx = mzk.Context(0)
+    if not args.no_tune:
+        ds = ctx.gen_rand_fr(0xC0FFEE, 1 << args.create_proof_only)
+        db = ctx.gen_bases(0xBA5E, 1 << args.create_proof_only)
+        ctx.autotune(ds, db, msm_log_n=list(range(12, args.create_proof_only + 1)),
+                     ntt_log_n=list(range(12, args.create_proof_only + 3)), reps=2)
+        del ds, db
+    keys = PlonkKeys(mzk, ctx, (args.create_proof_only,))
+    r = measure_proofs(mzk, ctx, keys, args.create_proof_only, max(2, args.steps), args.prover_batch)
+    ph, calls = ctx.prove_phase_stats()
+    r["phase_ms_total"] = {k: round(v, 2) for k, v in ph.items()}
+    r["calls"] = calls
+    print(json.dumps({"create_proof": r}), flush=True)
+    keys.close()
+    ctx.close()
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -831,6 +856,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.create_proof_only:
+        run_create_proof_only(args)
     else:
         run_ours(args)
 
