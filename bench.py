@@ -244,12 +244,10 @@ def measure_quotient(mzk, ctx, stream, k, reps, imad_peak):
                            "the built-in fast path"}
 
 
-# fixed-base window tables of the resident SRS (prover keys, batched MSMs):
-# width 20, used by batched-MSM items of 2^18 points and more, and by the
-# prover's MSMs of 2^20 points and more (a single proof's 2^18-point MSMs
-# measured faster without it: the table's one 2^19-bucket reduction per MSM
-# costs more than the windows it saves at that size)
-TABLE_C, TABLE_MIN_N, PROVER_TABLE_MIN_N = 20, 1 << 18, 1 << 20
+# fixed-base window table of the resident SRS for the batched MSMs: width 20,
+# used by items of 2^18 points and more.  Prover keys take the width
+# prover_table_width(k) of their own SRS instead.
+TABLE_C, TABLE_MIN_N = 20, 1 << 18
 FR_ONE_MONT = [0x00000001fffffffe, 0x5884b7fa00034802, 0x998c4fefecbc4ff5, 0x1824b159acc5056f]  # R mod r
 SERVE_KS = (14, 16, 18, 20)
 SERVE_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
@@ -258,43 +256,39 @@ SERVE_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
 class PlonkKeys:
     """Proving keys of the single-proof configuration's circuit (standard gate,
     copy cycles over 10 % of the a and b cells, range lookup of a into a 2^16
-    table) for several k over ONE device SRS: the KZG test setup for one seeded
-    secret, g of 2^max k points (a prefix serves every smaller k) then each k's
-    lagrange, delta and double-delta bases, stored as row 0 of a fixed-base
-    window table.  One seeded Config3Instance per k gives the fixed columns,
+    table) for several k.  Each k has its own device SRS (the KZG test setup
+    for one seeded secret: g, lagrange, delta and double-delta bases of 2^k
+    points, as ParamsKZG downsized to k holds them) stored as row 0 of a
+    fixed-base window table of width prover_table_width(k) that every MSM of
+    the proof uses.  One seeded Config3Instance per k gives the fixed columns,
     the key (device keygen) and fresh satisfying witnesses per request."""
 
-    def __init__(self, mzk, ctx, ks, table_c=TABLE_C, table_min_n=PROVER_TABLE_MIN_N):
+    def __init__(self, mzk, ctx, ks, table=True):
         self.mzk, self.ctx, self.ks = mzk, ctx, tuple(sorted(ks))
-        kmax = max(ks)
-        self.srs_len = (1 << kmax) + sum(3 << k for k in ks)
-        self.table_rows = mzk.Context.msm_table_rows(table_c) if table_c else 1
-        self.srs = ctx.alloc(self.table_rows * self.srs_len * 96)
         secret = ctx.gen_rand_fr(0x5EC2E7, 1).download((1, 4))[0]
-        t0 = time.perf_counter()
-        self.doms, self.inst, off = {}, {}, 1 << kmax
-        offs = {}
+        self.doms, self.inst, self.srs, self.table = {}, {}, {}, {}
+        setup_s = build_s = key_s = 0.0
         for k in self.ks:
             n = 1 << k
+            c = mzk.prover_table_width(k) if table else 0
+            rows = mzk.Context.msm_table_rows(c) if c else 1
+            buf = ctx.alloc(rows * 4 * n * 96)
+            p = buf.ptr
+            t0 = time.perf_counter()
             dom = mzk.EvaluationDomain(ctx, mzk.CONFIG3_DEGREE, k)
-            p = self.srs.ptr
-            dom.srs_setup_device(secret, p if k == kmax else None, p + off * 96, p + (off + n) * 96,
-                                 p + (off + 2 * n) * 96)
-            offs[k] = (0, off, off + n, off + 2 * n)
-            off += 3 * n
-            self.doms[k] = dom
-        setup_s = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        if table_c:
-            ctx.msm_window_table(self.srs, self.srs_len, table_c, self.table_rows)
-        self.table = {"c": table_c, "rows": self.table_rows, "min_n": table_min_n,
-                      "bytes": self.table_rows * self.srs_len * 96, "build_s": round(time.perf_counter() - t0, 2),
-                      "srs_setup_s": round(setup_s, 2)}
-        t0 = time.perf_counter()
-        for k in self.ks:
-            desc = mzk.SrsDesc(self.srs.ptr, self.srs_len, *offs[k], table_c, self.table_rows, table_min_n)
-            self.inst[k] = mzk.Config3Instance(ctx, self.doms[k], desc, seed=0xC0F3 + k)
-        self.keygen_s = round(time.perf_counter() - t0, 2)
+            dom.srs_setup_device(secret, p, p + n * 96, p + 2 * n * 96, p + 3 * n * 96)
+            t1 = time.perf_counter()
+            if c:
+                ctx.msm_window_table(buf, 4 * n, c, rows)
+            t2 = time.perf_counter()
+            desc = mzk.SrsDesc(p, 4 * n, 0, n, 2 * n, 3 * n, c, rows, n if c else 0)
+            self.inst[k] = mzk.Config3Instance(ctx, dom, desc, seed=0xC0F3 + k)
+            setup_s, build_s, key_s = setup_s + t1 - t0, build_s + t2 - t1, key_s + time.perf_counter() - t2
+            self.doms[k], self.srs[k] = dom, buf
+            self.table[str(k)] = {"c": c, "rows": rows, "bytes": rows * 4 * n * 96}
+        self.table.update({"build_s": round(build_s, 2), "srs_setup_s": round(setup_s, 2),
+                           "min_n": "2^k (every MSM of the proof)"})
+        self.keygen_s = round(key_s, 2)
 
     def request(self, k, seed):
         inst = self.inst[k]
@@ -304,6 +298,7 @@ class PlonkKeys:
         self.inst.clear()
         for d in self.doms.values():
             d.close()
+        self.srs.clear()
 
 
 def measure_proofs(mzk, ctx, keys, k, reps, batch):

@@ -912,6 +912,23 @@ class SrsDesc(ctypes.Structure):
                 ("table_rows", ctypes.c_uint32), ("table_min_n", ctypes.c_uint64)]
 
 
+def prover_table_width(k):
+    """Width c of the fixed-base window table that made create_proof fastest
+    at 2^k rows on a B200 (config-3 circuit, 8 proofs per call; k = 18: no
+    table 33.0 ms per proof, c = 15 / 16 / 17 / 18: 28.4 / 27.5 / 27.9 / 29.2
+    ms; k = 20: no table 121.7, c = 18 99.1, c = 20 113.8 ms).  Each MSM of
+    2^k points then adds ceil(255 / c) + 1 table rows of points into one window
+    of 2^(c-1) buckets: wider tables mean fewer entries per point but more
+    buckets to reduce, and the best width grows with the point count."""
+    if k <= 14:
+        return 12
+    if k <= 18:
+        return 16
+    if k <= 20:
+        return 18
+    return 20
+
+
 class ProofRequest(ctypes.Structure):
     """mzk_proof_request (include/mzk.h)."""
     _fields_ = [("key", ctypes.c_void_p), ("advice", ctypes.c_void_p), ("advice_on_device", ctypes.c_int),

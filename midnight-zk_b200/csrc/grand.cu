@@ -32,7 +32,6 @@ namespace mzk {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr uint32_t kInvChunk = 64;  // elements per thread of a batch inversion
 // elements per thread of a linear recurrence: up to 64, fewer when n is too
 // small to give every SM work (each thread's chunk is a serial chain)
 constexpr uint32_t kRecChunkMax = 64, kRecChunkMin = 4;
@@ -76,41 +75,6 @@ uint32_t grid_for(const Context* ctx, uint64_t items, uint32_t threads) {
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((items + threads - 1) / threads, (uint64_t)ctx->num_sms * 16));
 }
 
-// ---- batch inversion: thread t takes the elements t, t + T, t + 2T, ... (T
-// threads), Montgomery's trick over them with one Fermat inversion.  Loads
-// and stores are coalesced; pre holds the forward prefix products.
-__global__ void __launch_bounds__(kThreads) k_batch_invert(Fr* __restrict__ a, Fr* __restrict__ pre, uint64_t n) {
-    const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    Fr acc = fr_one();
-    for (uint64_t i = t; i < n; i += T) {
-        pre[i] = acc;
-        const Fr v = a[i];
-        if (!fr_is_zero(v)) acc = fr_mul(acc, v);
-    }
-    acc = fr_inv(acc);
-    const uint64_t last = t + ((n - 1 - t) / T) * T;
-    for (uint64_t i = last;; i -= T) {
-        const Fr v = a[i];
-        if (!fr_is_zero(v)) {
-            a[i] = fr_mul(pre[i], acc);
-            acc = fr_mul(acc, v);
-        }
-        if (i < T) break;
-    }
-}
-
-Status batch_invert(Context* ctx, Fr* a, uint64_t n, cudaStream_t st) {
-    if (n == 0) return OK;
-    void* pre;
-    MZK_TRY(ctx->ensure("grand_pre", n * sizeof(Fr), &pre));
-    const uint64_t threads = std::max<uint64_t>(1, (n + kInvChunk - 1) / kInvChunk);
-    k_batch_invert<<<(uint32_t)((threads + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, (Fr*)pre, n);
-    MZK_LAUNCH_CHECK(ctx);
-    return OK;
-}
-
 // ---- exclusive scans (product or sum) of Fr values ----
 template <bool kMul>
 __device__ __forceinline__ Fr op(const Fr& a, const Fr& b) {
@@ -138,6 +102,77 @@ __device__ Fr block_exclusive(Fr v, Fr* sm, Fr* total) {
     const Fr ex = threadIdx.x ? sm[threadIdx.x - 1] : identity<kMul>();
     __syncthreads();
     return ex;
+}
+
+// block-wide exclusive suffix product of one value per thread: the product of
+// the values of the threads above this one
+__device__ Fr block_exclusive_suffix_product(Fr v, Fr* sm) {
+    sm[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+        Fr o = fr_one();
+        if (threadIdx.x + off < blockDim.x) o = sm[threadIdx.x + off];
+        __syncthreads();
+        if (threadIdx.x + off < blockDim.x) sm[threadIdx.x] = fr_mul(o, sm[threadIdx.x]);
+        __syncthreads();
+    }
+    const Fr ex = threadIdx.x + 1 < blockDim.x ? sm[threadIdx.x + 1] : fr_one();
+    __syncthreads();
+    return ex;
+}
+
+// ---- batch inversion (ff BatchInvert: zeros stay zero): a block takes
+// kThreads x C consecutive elements (thread t the elements t, t + kThreads,
+// ... of the block's range, so loads and stores are coalesced), each thread
+// multiplies its C non-zero elements in registers, the block combines the
+// threads' products by a prefix and a suffix scan in shared memory, and ONE
+// Fermat inversion per block gives every thread the inverse of its product
+// (prefix x suffix x 1/total); the backward pass then inverts each element.
+template <int C>
+__global__ void __launch_bounds__(kThreads) k_batch_invert(Fr* __restrict__ a, uint64_t n) {
+    __shared__ Fr sm[kThreads];
+    __shared__ Fr total_inv;
+    const uint64_t base = (uint64_t)blockIdx.x * kThreads * C + threadIdx.x;
+    Fr v[C], pre[C];
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+        const uint64_t i = base + (uint64_t)k * kThreads;
+        v[k] = i < n ? a[i] : fr_zero();
+    }
+    Fr acc = fr_one();
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+        pre[k] = acc;
+        if (!fr_is_zero(v[k])) acc = fr_mul(acc, v[k]);
+    }
+    Fr total;
+    const Fr below = block_exclusive<true>(acc, sm, &total);
+    const Fr above = block_exclusive_suffix_product(acc, sm);
+    if (threadIdx.x == 0) total_inv = fr_inv(total);
+    __syncthreads();
+    Fr inv = fr_mul(fr_mul(total_inv, below), above);  // 1 / acc
+#pragma unroll
+    for (int k = C - 1; k >= 0; k--) {
+        const uint64_t i = base + (uint64_t)k * kThreads;
+        if (!fr_is_zero(v[k])) {
+            if (i < n) a[i] = fr_mul(pre[k], inv);
+            inv = fr_mul(inv, v[k]);
+        }
+    }
+}
+
+Status batch_invert(Context* ctx, Fr* a, uint64_t n, cudaStream_t st) {
+    if (n == 0) return OK;
+    // 8 elements per thread for large n (one inversion per 2048 elements; 16
+    // would spill the registers), 4 when that would leave SMs without blocks
+    const uint64_t per8 = (uint64_t)kThreads * 8, per4 = (uint64_t)kThreads * 4;
+    if (n >= per8 * (uint64_t)ctx->num_sms * 2) {
+        k_batch_invert<8><<<(uint32_t)((n + per8 - 1) / per8), kThreads, 0, st>>>(a, n);
+    } else {
+        k_batch_invert<4><<<(uint32_t)((n + per4 - 1) / per4), kThreads, 0, st>>>(a, n);
+    }
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
 }
 
 // pass 1: out = exclusive scan within each tile of kThreads * kScanItems, sums[tile] = tile total

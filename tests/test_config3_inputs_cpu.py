@@ -35,3 +35,9 @@ def test_copy_cycles_form_a_permutation():
 def test_config3_circuit_shape():
     c = mzk.config3_circuit(18)
     assert c["degree"] == 5 and c["blinding_factors"] == 7 and c["n_advice"] == 3 and c["n_fixed"] == 7
+
+
+def test_prover_table_width_grows_with_k():
+    widths = [mzk.prover_table_width(k) for k in range(4, 27)]
+    assert widths == sorted(widths) and all(5 <= c <= 24 for c in widths)
+    assert all(mzk.Context.msm_table_rows(c) * c >= 256 for c in set(widths))

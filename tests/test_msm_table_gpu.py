@@ -106,16 +106,17 @@ def test_bad_tables_are_refused(ctx):
         ctx.msm_window_table(t, 64, 30, rows)                              # width outside [5, 24]
 
 
-def test_served_proofs_over_a_table_equal_the_untabled_proof(ctx):
+@pytest.mark.parametrize("c", [12, 16, 18])
+def test_served_proofs_over_a_table_equal_the_untabled_proof(ctx, c):
     """create_proof through the proving service with a key whose SRS is a
-    window table: every transcript equals the same proof with the key over
-    the plain SRS (and the oracle's)."""
+    window table (the widths prover_table_width gives): every transcript
+    equals the same proof with the key over the plain SRS (and the
+    oracle's)."""
     from _plonk_setup import PINNED, Circuit
     c8 = Circuit(ctx, 8, seed=91)
     n = c8.n
     blinds = [c8.blinds(s) for s in (92, 93, 94)]
     want = [mzk.create_proofs(ctx, [(c8.key, c8.advice, b)])[0] for b in blinds]
-    c = 16
     t, rows = make_table(ctx, c8.srs_buf.download((4 * n, 12)), c)
     desc = mzk.SrsDesc(t.ptr, 4 * n, 0, n, 2 * n, 3 * n, c, rows, 1)
     key = mzk.PlonkKey(ctx, c8.dom, c8.circuit, desc, c8.fixed, c8.mapping, PINNED)
