@@ -54,6 +54,7 @@ struct PassArgs {
     Fr* out;
     const Fr* tlo;
     const Fr* thi;
+    const Fr* ptw;  // the pass's twiddle table (Domain::pass_tw), or null: formed from tlo x thi
     uint32_t log_n, log_s, log_r;
     uint32_t n_real;   // elements present in `in`; larger indices read as zero
     int use_pre;       // multiply input element i by pre[i % 3] (coset scaling)
@@ -103,15 +104,20 @@ __device__ __forceinline__ uint32_t tw_swz(uint32_t u) { return u ^ (((u >> 3) ^
 // the last stage's half-size), runs the K radix-2 stages on them and stores
 // them back.  Stage s+t pairs rows r and r + q 2^(K-1-t); its twiddle is
 // w_R^(pos << (s+t)) with pos = r mod (q 2^(K-t)).
-template <int K>
+// Every product of a stage is issued unconditionally, so the stage is one
+// basic block whose independent carry chains the scheduler interleaves: a
+// butterfly with pos = 0 multiplies by w^0 = 1 (Montgomery one; the product
+// is the same canonical value).  In the pass's last round (kLast: q = 1,
+// j = 0) the pos = 0 butterflies are known at compile time and skipped.
+template <int K, bool kLast>
 __device__ __forceinline__ void dif_round(const FrPlanes& sx, const FrPlanes& sw, uint32_t s, uint32_t log_r,
                                           uint32_t log_b, uint32_t tile) {
-    const uint32_t log_q = log_r - s - K;
+    const uint32_t log_q = kLast ? 0u : log_r - s - K;
     const uint32_t B = 1u << log_b;
     for (uint32_t g = threadIdx.x; g < (tile >> K); g += blockDim.x) {
         const uint32_t b = g & (B - 1);
         const uint32_t rest = g >> log_b;
-        const uint32_t j = rest & ((1u << log_q) - 1);
+        const uint32_t j = kLast ? 0u : rest & ((1u << log_q) - 1);
         const uint32_t m0 = ((rest >> log_q) << (log_q + K)) + j;
         Fr x[1 << K];
 #pragma unroll
@@ -121,13 +127,17 @@ __device__ __forceinline__ void dif_round(const FrPlanes& sx, const FrPlanes& sw
             const int d = 1 << (K - 1 - t);
 #pragma unroll
             for (int i = 0; i < (1 << K); i++) {
-                if ((i & (2 * d - 1)) < d) {
+                const int off = i & (2 * d - 1);
+                if (off < d) {
                     const Fr x0 = x[i], x1 = x[i + d];
                     x[i] = fr_add(x0, x1);
-                    Fr v = fr_sub(x0, x1);
-                    const uint32_t pos = j + ((uint32_t)(i & (2 * d - 1)) << log_q);
-                    if (pos) v = fr_mul(v, sw.get(tw_swz(pos << (s + (uint32_t)t))));
-                    x[i + d] = v;
+                    const Fr v = fr_sub(x0, x1);
+                    if (kLast && off == 0) {
+                        x[i + d] = v;
+                    } else {
+                        const uint32_t pos = j + ((uint32_t)off << log_q);
+                        x[i + d] = fr_mul(v, sw.get(tw_swz(pos << (s + (uint32_t)t))));
+                    }
                 }
             }
         }
@@ -182,9 +192,17 @@ __global__ void __launch_bounds__(kNttThreads, 2) k_ntt_dif_pass(PassArgs a) {
     // stages in rounds of three (radix 8), the last round of one or two
     for (uint32_t s = 0; s < a.log_r;) {
         const uint32_t k = min(3u, a.log_r - s);
-        if (k == 3) dif_round<3>(sx, sw, s, a.log_r, log_b, tile);
-        else if (k == 2) dif_round<2>(sx, sw, s, a.log_r, log_b, tile);
-        else dif_round<1>(sx, sw, s, a.log_r, log_b, tile);
+        const bool last = s + k == a.log_r;
+        if (k == 3) {
+            if (last) dif_round<3, true>(sx, sw, s, a.log_r, log_b, tile);
+            else dif_round<3, false>(sx, sw, s, a.log_r, log_b, tile);
+        } else if (k == 2) {
+            if (last) dif_round<2, true>(sx, sw, s, a.log_r, log_b, tile);
+            else dif_round<2, false>(sx, sw, s, a.log_r, log_b, tile);
+        } else {
+            if (last) dif_round<1, true>(sx, sw, s, a.log_r, log_b, tile);
+            else dif_round<1, false>(sx, sw, s, a.log_r, log_b, tile);
+        }
         __syncthreads();
         s += k;
     }
@@ -196,10 +214,16 @@ __global__ void __launch_bounds__(kNttThreads, 2) k_ntt_dif_pass(PassArgs a) {
         const uint32_t j = c & ((1u << log_m) - 1);
         const uint32_t idx = ((c >> log_m) << a.log_s) + (m << log_m) + j;
         Fr v = sx.get(swz(e));
-        if (a.twiddle_after && j) {
-            const uint32_t k1 = __brev(m) >> (32 - a.log_r);
-            const uint32_t ex = (j * k1) << (a.log_n - a.log_s);  // (N/S) j k1 < N
-            v = fr_mul(v, root_pow(a.tlo, a.thi, ex & (N - 1)));
+        if (a.twiddle_after) {  // uniform; j k1 = 0 multiplies by w^0 = 1 (branch-free)
+            Fr w;
+            if (a.ptw) {  // uniform: one coalesced load at the element's offset in its segment
+                w = a.ptw[(m << log_m) + j];
+            } else {
+                const uint32_t k1 = __brev(m) >> (32 - a.log_r);
+                const uint32_t ex = ((j * k1) << (a.log_n - a.log_s)) & (N - 1);  // (N/S) j k1 < N
+                w = fr_mul(a.thi[ex >> kLoBits], a.tlo[ex & ((1u << kLoBits) - 1)]);
+            }
+            v = fr_mul(v, w);
         }
         if (a.bitrev_out) {
             const uint32_t o = a.log_n ? (__brev(idx) >> (32 - a.log_n)) : 0u;
@@ -235,6 +259,20 @@ __global__ void k_pow_table(Fr base, uint32_t count, Fr* __restrict__ out) {
     }
 }
 
+// tw[i] = w^((N/S) j bitrev_r(m)) for i = (m << (log_s - log_r)) + j < S: the
+// inter-pass twiddle of the element a pass writes at offset i of its segment
+__global__ void k_pass_twiddles(const Fr* __restrict__ tlo, const Fr* __restrict__ thi, uint32_t log_n,
+                                uint32_t log_s, uint32_t log_r, Fr* __restrict__ tw) {
+    const uint32_t S = 1u << log_s, N = 1u << log_n, log_m = log_s - log_r;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S; i += stride) {
+        const uint32_t m = i >> log_m, j = i & ((1u << log_m) - 1);
+        const uint32_t k1 = __brev(m) >> (32 - log_r);
+        const uint32_t ex = ((j * k1) << (log_n - log_s)) & (N - 1);
+        tw[i] = fr_mul(thi[ex >> kLoBits], tlo[ex & ((1u << kLoBits) - 1)]);
+    }
+}
+
 Fr to_dev(const host::Fr4& x) {
     Fr r;
     std::memcpy(r.l, x.l, 32);
@@ -254,9 +292,61 @@ uint32_t grid_for(Context* ctx, uint32_t n, uint32_t threads) {
 
 }  // namespace
 
+// log2 of the rows of each pass of a transform of 2^log_n elements under a
+// split mode: every pass keeps at least one stage and at most the tile's;
+// the remaining passes can always take what is left
+static std::vector<uint32_t> pass_logs(uint32_t log_n, int split) {
+    const uint32_t tile_log = std::min(kTileLog, log_n);
+    const uint32_t passes = (log_n + tile_log - 1) / tile_log;
+    std::vector<uint32_t> logs;
+    uint32_t log_s = log_n;
+    for (uint32_t p = 0; p < passes; p++) {
+        const uint32_t rem = passes - p;
+        uint32_t log_r = (log_s + rem - 1) / rem;  // even split, larger passes first
+        if (split == kSplitFront) log_r = std::min(tile_log, log_s - (rem - 1));
+        if (split == kSplitBack) log_r = std::max(1u, log_s - (rem - 1) * tile_log);
+        logs.push_back(log_r);
+        log_s -= log_r;
+    }
+    return logs;
+}
+
+static int split_of(const Context* ctx, uint32_t log_n) {
+    return log_n < (uint32_t)kTuneSlots ? ctx->tuned_ntt_split[log_n] : 0;
+}
+
+// The twiddle table of a non-last pass (Domain::pass_tw), built when missing.
+// Building allocates and synchronises `st` (so that other streams may read
+// the table at once), so it is skipped while `st` is being captured, and a
+// failed allocation is not an error: either way the pass forms its twiddles
+// from the split tables instead (the same values).
+static const Fr* pass_twiddles(Context* ctx, const Domain* d, int root, uint32_t log_n, uint32_t log_s,
+                               uint32_t log_r, cudaStream_t st) {
+    std::lock_guard<std::mutex> g(d->tw_mu);
+    const auto key = std::make_tuple(root, log_s, log_r);
+    const auto it = d->pass_tw.find(key);
+    if (it != d->pass_tw.end()) return it->second;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+    Fr* p = nullptr;
+    if (cudaMalloc(&p, ((size_t)1 << log_s) * sizeof(Fr)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    k_pass_twiddles<<<grid_for(ctx, 1u << log_s, 256), 256, 0, st>>>(d->lo[root], d->hi[root], log_n, log_s, log_r, p);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaFree(p);
+        return nullptr;
+    }
+    ctx->launches++;
+    d->pass_tw[key] = p;
+    return p;
+}
+
 Domain::~Domain() {
     for (auto& t : tables)
         if (t) cudaFree(t);
+    for (auto& kv : pass_tw) cudaFree(kv.second);
     if (d_tinv) cudaFree(d_tinv);
 }
 
@@ -339,46 +429,50 @@ Status domain_create(Context* ctx, uint32_t j, uint32_t k, Domain** out) {
             return ERR_CUDA;
         }
     }
+    // the pass twiddle tables of the split in force for each root's size
+    for (int r = 0; r < 4; r++) {
+        const uint32_t log_n = logs[r];
+        const std::vector<uint32_t> pl = pass_logs(log_n, split_of(ctx, log_n));
+        uint32_t log_s = log_n;
+        for (size_t p = 0; p + 1 < pl.size(); p++) {
+            pass_twiddles(ctx, d, r, log_n, log_s, pl[p], ctx->stream);
+            log_s -= pl[p];
+        }
+    }
     *out = d;
     return OK;
 }
 
-// Forward DIF passes over 2^log_n elements with root table `root` (0..3),
-// first pass reading `in` (n_real elements, optional coset scaling) and
-// writing `out`; later passes in place on `out`.  Output bit-reversed.
-// The DIF passes of one transform, ending in natural order: the last pass
-// writes every element to its bit-reversed position (times post[i % 3] when
-// post is given, only positions < m_out).  Since that pass's writes cross
-// blocks, it reads from the scratch buffer the earlier passes wrote, so `in`
-// and `out` may be the same buffer.  A transform of one tile (log_n <= 11) is
-// one block, which reads all before it writes.
+// The DIF passes of one transform over 2^log_n elements with root table
+// `root` (0..3), ending in natural order.  The first pass reads `in`
+// (n_real elements, optional coset scaling).  The last pass writes every
+// element to its bit-reversed position (times post[i % 3] when post is given,
+// only positions < m_out).  Since that pass's writes cross blocks, it reads
+// from the scratch buffer the earlier passes wrote, so `in` and `out` may be
+// the same buffer.  A transform of one tile (log_n <= 11) is one block,
+// which reads all before it writes.
 static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n, const Fr* in, Fr* out,
                          uint32_t n_real, bool coset, const host::Fr4* post, uint32_t m_out, cudaStream_t st) {
     const uint32_t N = 1u << log_n;
     const uint32_t tile = std::min(kTile, N);
-    const uint32_t tile_log = std::min(kTileLog, log_n);
-    const uint32_t passes = (log_n + tile_log - 1) / tile_log;
+    const std::vector<uint32_t> logs = pass_logs(log_n, split_of(ctx, log_n));
+    const uint32_t passes = (uint32_t)logs.size();
     Fr* tmp = nullptr;
     if (passes > 1) {
         void* p;
         MZK_TRY(ctx->ensure("ntt_tmp", (size_t)N * sizeof(Fr), &p));
         tmp = static_cast<Fr*>(p);
     }
-    const int split = log_n < (uint32_t)kTuneSlots ? ctx->tuned_ntt_split[log_n] : 0;
     uint32_t log_s = log_n;
     for (uint32_t p = 0; p < passes; p++) {
-        const uint32_t rem = passes - p;
-        // every pass keeps at least one stage and at most tile_log; the
-        // remaining passes can always take what is left
-        uint32_t log_r = (log_s + rem - 1) / rem;  // even split, larger passes first
-        if (split == kSplitFront) log_r = std::min(tile_log, log_s - (rem - 1));
-        if (split == kSplitBack) log_r = std::max(1u, log_s - (rem - 1) * tile_log);
+        const uint32_t log_r = logs[p];
         const bool last = p + 1 == passes;
         PassArgs a;
         a.in = p == 0 ? in : tmp;
         a.out = last ? out : tmp;
         a.tlo = d->lo[root];
         a.thi = d->hi[root];
+        a.ptw = last ? nullptr : pass_twiddles(ctx, d, root, log_n, log_s, log_r, st);
         a.log_n = log_n;
         a.log_s = log_s;
         a.log_r = log_r;

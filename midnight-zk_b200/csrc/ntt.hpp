@@ -1,6 +1,9 @@
 // ntt.hpp — device EvaluationDomain (proofs/src/poly/domain.rs:34-49).
 #pragma once
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "field.cuh"
@@ -35,6 +38,14 @@ struct Domain {
     Fr* lo[4] = {};
     Fr* hi[4] = {};
     void* d_tinv = nullptr;
+    // inter-pass twiddles of one non-last DIF pass, laid out as the pass
+    // writes its output: tw[(m << (log_s - log_r)) + j] = w^((N/S) j bitrev_r(m))
+    // for the pass over segments of S = 2^log_s elements with R = 2^log_r rows
+    // (N = 2^log_n of root r).  Keyed by (root, log_s, log_r); built for the
+    // split in force when the domain is created, and for another split the
+    // first time a transform outside stream capture uses it.
+    mutable std::mutex tw_mu;
+    mutable std::map<std::tuple<int, uint32_t, uint32_t>, Fr*> pass_tw;
     ~Domain();
 };
 

@@ -96,3 +96,24 @@ def test_ntt_sequence_graph_replays_equal_launches(ctx):
         assert c.graph_stats()[0] >= 3                 # recaptured after the domain went away
     finally:
         c.close()
+
+
+def test_graph_captured_before_its_pass_twiddle_tables_exist():
+    """A transform captured into a graph while the twiddle tables of its
+    passes do not exist yet (the NTT split changed after the domain was made,
+    and a table is never built during a capture) forms its inter-pass
+    twiddles from the small root tables instead: the captured proof's
+    commitments equal the eager launches', which build the tables."""
+    c = mzk.Context(0)
+    try:
+        st = Setup(c, 12, seed=37)
+        for lg in (st.g.k, st.g.extended_k):
+            c.set_tuned(c.TUNE_NTT_SPLIT, lg, 3)        # largest passes last: new pass shapes
+        jobs = [st.job(s)[0] for s in (43, 44)]
+        captured = st.g.prove_core_device(st.pk, jobs)
+        assert c.graph_stats()[0] == 2
+        eager = st.g.prove_core_device(st.pk, jobs, graphs=False)
+        assert np.array_equal(captured, eager)
+        assert np.array_equal(st.g.prove_core_device(st.pk, jobs), eager)   # replayed
+    finally:
+        c.close()
