@@ -63,6 +63,9 @@ def parse_args():
     p.add_argument("--create-proof-only", type=int, default=0, metavar="K",
                    help="only time create_proof of the single-proof configuration at 2^K rows (profiling)")
     p.add_argument("--prover-batch", type=int, default=8, help="proofs per call in --create-proof-only")
+    p.add_argument("--ntt-only", type=int, default=0, metavar="LOG_N",
+                   help="only time coeff_to_lagrange and lagrange_to_coeff at 2^LOG_N (profiling; even "
+                        "pass split, W + K transforms each, three passes each at 2^24)")
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-reps", type=int, default=3)
     return p.parse_args()
@@ -641,6 +644,35 @@ def run_create_proof_only(args):
     ctx.close()
 
 
+def run_ntt_only(args):
+    """The domain's two size-n transforms at 2^LOG_N, in place on seeded
+    inputs (a short run for profilers); prints one JSON line."""
+    import torch
+    from _loader import load
+    mzk = load()
+    ctx = mzk.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = 1 << args.ntt_only
+    dom = mzk.EvaluationDomain(ctx, 2, args.ntt_only)   # j = 2: the extended domain is n, no 4n tables
+    da = ctx.gen_rand_fr(0x7007, n)
+    out = {}
+    for name in ("coeff_to_lagrange", "lagrange_to_coeff"):
+        for _ in range(args.warmup):
+            dom.op_device(name, da, da)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            dom.op_device(name, da, da)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        imad = (n // 2) * args.ntt_only * IMAD_PER_FR_MUL
+        out[name] = {"n": n, "ms": round(ms, 3), "imad_t_per_s": round(imad / (ms / 1e3) / 1e12, 3)}
+    print(json.dumps({"ntt": out}), flush=True)
+    dom.close()
+    ctx.close()
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -853,6 +885,8 @@ def main():
         run_reference(args)
     elif args.create_proof_only:
         run_create_proof_only(args)
+    elif args.ntt_only:
+        run_ntt_only(args)
     else:
         run_ours(args)
 
