@@ -67,6 +67,23 @@ int mzk_probe_imad_peak(mzk_ctx *ctx, double *imad_per_s, double *fp_mul_per_s, 
  * any limb (expected 0). */
 int mzk_probe_fp_sqr_check(mzk_ctx *ctx, const uint64_t *d_values, size_t n, uint64_t *mismatches);
 
+/* Batch-affine bucket additions (the accumulation scheme of the reference's
+ * batch_add / Schedule, curves/src/msm.rs:58-144) per second on this GPU:
+ * each thread adds a point to each of B affine accumulators held in local
+ * memory, the B additions sharing one inversion by Montgomery's trick (6
+ * multiplications per addition plus the inversion's share).  out[0..3]: B =
+ * 16, 32, 64, 128 with a Fermat inversion; out[4..7]: the same with the
+ * binary extended Euclidean inversion.  A microbenchmark (no gathers, no
+ * bucket bookkeeping) that bounds the scheme against the mixed XYZZ
+ * addition that mzk_probe_imad_peak's variants[3] measures. */
+int mzk_probe_batch_affine(mzk_ctx *ctx, double out[8]);
+
+/* Self-check of the binary extended Euclidean inversion used by the batch
+ * inversion's per-block step and the batch-affine probe: for n device Fp
+ * values, counts those whose inverse differs from the Fermat power or does
+ * not give a^-1 a = 1 (expected 0; zeros are skipped). */
+int mzk_probe_fp_inv_check(mzk_ctx *ctx, const uint64_t *d_values, size_t n, uint64_t *mismatches);
+
 /* Captured CUDA graphs of this context: captures made and replays run (the
  * proof core's per-proof NTT sequences). */
 int mzk_ctx_graph_stats(mzk_ctx *ctx, uint64_t *captures, uint64_t *replays);
@@ -404,8 +421,10 @@ typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } m
  * Permutation columns: kind 0 advice, 1 fixed; sets of degree - 2 columns.
  * The query lists and their order are the reference's (they fix the order
  * of the evaluations in the proof).  Limits: 16 advice, 16 fixed, 16
- * permutation columns (8 sets), at most one lookup, no instance columns,
- * trashcans or simple selectors. */
+ * permutation columns (8 sets), at most 4 lookups (each one advice column
+ * into one fixed table column; their multiplicities, helpers and aggregators
+ * are committed, evaluated and opened lookup by lookup, as logup/prover.rs
+ * does), no instance columns, trashcans or simple selectors. */
 typedef struct {
     uint32_t degree;                   /* cs.degree() (plonk/circuit.rs:2174-2199), 3..9 */
     uint32_t blinding_factors;         /* cs.blinding_factors() (circuit.rs:2203-2245) */

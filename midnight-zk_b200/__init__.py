@@ -46,6 +46,8 @@ SIGNATURES = {
     "mzk_ctx_set_profiling": (_i32, [_vp, _i32]),
     "mzk_ctx_phase_stats": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _u64p, _i32]),
     "mzk_ctx_prove_phase_stats": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _u64p, _i32, _i32]),
+    "mzk_probe_batch_affine": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "mzk_probe_fp_inv_check": (_i32, [_vp, _vp, _sz, _u64p]),
     "mzk_probe_imad_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double)]),
     "mzk_msm_last_shape": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _u64p]),
@@ -546,6 +548,21 @@ class Context:
         ptr = d_values.ptr if isinstance(d_values, DeviceBuffer) else int(d_values)
         _check(lib().mzk_probe_fp_sqr_check(self.h, ptr, int(n), _ptr(out)))
         return int(out[0])
+
+    def probe_fp_inv_check(self, d_values, n):
+        """Values among n device Fp elements whose binary-Euclid inverse differs
+        from the Fermat power or fails a^-1 a = 1."""
+        out = np.zeros(1, np.uint64)
+        ptr = d_values.ptr if isinstance(d_values, DeviceBuffer) else int(d_values)
+        _check(lib().mzk_probe_fp_inv_check(self.h, ptr, int(n), _ptr(out)))
+        return int(out[0])
+
+    def probe_batch_affine(self):
+        """Batch-affine additions per second: {(batch, "fermat" | "binary"): rate}."""
+        v = (ctypes.c_double * 8)()
+        _check(lib().mzk_probe_batch_affine(self.h, v))
+        return {(b, inv): v[4 * j + i] for j, inv in enumerate(("fermat", "binary"))
+                for i, b in enumerate((16, 32, 64, 128))}
 
     def msm_last_shape(self):
         c, w, e = _i32(), _i32(), np.zeros(1, np.uint64)

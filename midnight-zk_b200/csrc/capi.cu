@@ -432,6 +432,26 @@ int mzk_probe_fp_sqr_check(mzk_ctx* ctx, const uint64_t* d_values, size_t n, uin
     return mzk::check_fp_sqr(&ctx->impl, d_values, n, mismatches);
 }
 
+int mzk_probe_fp_inv_check(mzk_ctx* ctx, const uint64_t* d_values, size_t n, uint64_t* mismatches) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!mismatches || (n && !d_values)) {
+        mzk::set_error("probe: null pointer");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    return mzk::check_fp_inv(&ctx->impl, d_values, n, mismatches);
+}
+
+int mzk_probe_batch_affine(mzk_ctx* ctx, double out[8]) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!out) {
+        mzk::set_error("probe: null pointer");
+        return mzk::ERR_ARG;
+    }
+    Guard g(ctx);
+    return mzk::probe_batch_affine(&ctx->impl, out);
+}
+
 int mzk_msm_g1_device(mzk_ctx* ctx, const uint64_t* d_scalars, const uint64_t* d_bases, size_t n, uint64_t out[18]) {
     if (int s = check_ctx(ctx)) return s;
     if (!out || (n && (!d_scalars || !d_bases))) {

@@ -340,6 +340,86 @@ __device__ __forceinline__ Fp fp_one() {
     for (int j = 0; j < 12; j++) r.l[j] = FpP::one(j);
     return r;
 }
+// out = a^-1 mod m for plain N-limb integers, a in [1, m), m odd and m < 2^(32N-1)
+// (so x + m never overflows): the binary extended Euclidean algorithm
+// (Hankerson, Menezes and Vanstone, Guide to Elliptic Curve Cryptography,
+// Algorithm 2.22).  u = a, v = m, x1 = 1, x2 = 0 with a x1 = u and a x2 = v
+// (mod m) throughout; halve the even one of u, v (and its x modulo m),
+// subtract the smaller from the larger, until u or v is 1.  Every outer step
+// ends with an even value to halve, so the bit lengths of u and v shrink by
+// at least one per step: at most 64 N steps.  Returns false for a = 0 (no
+// inverse) or if that bound were ever passed.  Shifts and subtractions on the
+// ALU pipe instead of the multiplications of a Fermat inversion: a single
+// thread finishes several times sooner.  Variable time in the value.
+template <int N>
+__device__ __forceinline__ bool u_is_one(const uint32_t* a) {
+    uint32_t acc = a[0] ^ 1u;
+#pragma unroll
+    for (int j = 1; j < N; j++) acc |= a[j];
+    return acc == 0;
+}
+template <int N>
+__device__ __forceinline__ void u_shr1(uint32_t* a) {
+#pragma unroll
+    for (int j = 0; j < N - 1; j++) a[j] = __funnelshift_r(a[j], a[j + 1], 1);
+    a[N - 1] >>= 1;
+}
+template <int N, class ModF>
+__device__ __noinline__ bool inv_binary_raw(uint32_t* out, const uint32_t* a, ModF modf) {
+    uint32_t u[N], v[N], x1[N], x2[N], t[N];
+    uint32_t nz = 0;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        u[j] = a[j];
+        v[j] = modf(j);
+        x1[j] = j == 0 ? 1u : 0u;
+        x2[j] = 0u;
+        nz |= a[j];
+    }
+    if (!nz) return false;
+    for (int step = 0; step <= 64 * N; step++) {
+        if (u_is_one<N>(u)) {
+#pragma unroll
+            for (int j = 0; j < N; j++) out[j] = x1[j];
+            return true;
+        }
+        if (u_is_one<N>(v)) {
+#pragma unroll
+            for (int j = 0; j < N; j++) out[j] = x2[j];
+            return true;
+        }
+        while (!(u[0] & 1u)) {
+            u_shr1<N>(u);
+            add_masked<N>(t, x1, 0u - (x1[0] & 1u), modf);  // x1 / 2 mod m
+#pragma unroll
+            for (int j = 0; j < N; j++) x1[j] = t[j];
+            u_shr1<N>(x1);
+        }
+        while (!(v[0] & 1u)) {
+            u_shr1<N>(v);
+            add_masked<N>(t, x2, 0u - (x2[0] & 1u), modf);
+#pragma unroll
+            for (int j = 0; j < N; j++) x2[j] = t[j];
+            u_shr1<N>(x2);
+        }
+        const bool u_ge = sub_n<N>(t, u, v) == 0;  // no borrow: u >= v
+        if (u_ge) {  // u -= v, x1 = x1 - x2 mod m
+            sub_n<N>(t, u, v);
+#pragma unroll
+            for (int j = 0; j < N; j++) u[j] = t[j];
+            const uint32_t bw = sub_n<N>(t, x1, x2);
+            add_masked<N>(x1, t, bw, modf);
+        } else {  // v -= u, x2 = x2 - x1 mod m
+            sub_n<N>(t, v, u);
+#pragma unroll
+            for (int j = 0; j < N; j++) v[j] = t[j];
+            const uint32_t bw = sub_n<N>(t, x2, x1);
+            add_masked<N>(x2, t, bw, modf);
+        }
+    }
+    return false;
+}
+
 // a^(p-2) by square-and-multiply over the constant exponent p-2 (Fermat);
 // used for single-point normalisation only.
 static __device__ __noinline__ Fp fp_inv(const Fp& a) {

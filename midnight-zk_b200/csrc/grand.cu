@@ -46,18 +46,18 @@ __device__ __forceinline__ bool fr_is_zero(const Fr& a) {
     return acc == 0;
 }
 
-// a^(r-2) (Fermat); r = 1 mod 2^32, so r - 2 has limbs (2^32 - 1, r_1 - 1, r_2..r_7)
-static_assert(FrP::mod(0) == 1u, "Fr modulus limb 0 is 1");
+// 1/a for a non-zero a (zero gives zero): the binary extended Euclidean
+// algorithm (inv_binary_raw) on the stored Montgomery limbs A = a R yields
+// A^-1 = a^-1 R^-1, and one Montgomery product with R^3 gives a^-1 R, the
+// Montgomery form of 1/a.  A block's single inversion is a serial chain on
+// one thread, and this finishes it several times sooner than a Fermat
+// power.  Variable time in the value.
 __device__ __noinline__ Fr fr_inv(const Fr& a) {
-    Fr acc = fr_one();
-    for (int limb = 7; limb >= 0; limb--) {
-        const uint32_t e = limb == 0 ? 0xffffffffu : (limb == 1 ? FrP::mod(1) - 1u : FrP::mod(limb));
-        for (int bit = 31; bit >= 0; bit--) {
-            acc = fr_mul(acc, acc);
-            if ((e >> bit) & 1u) acc = fr_mul(acc, a);
-        }
-    }
-    return acc;
+    Fr x, r2;
+    if (!inv_binary_raw<8>(x.l, a.l, FrMod())) return fr_zero();
+#pragma unroll
+    for (int j = 0; j < 8; j++) r2.l[j] = FrP::r2(j);
+    return fr_mul(x, fr_mul(r2, r2));  // x R^3 R^-1 = a^-1 R
 }
 
 Fr to_dev(const host::Fr4& h) {
@@ -125,11 +125,36 @@ __device__ Fr block_exclusive_suffix_product(Fr v, Fr* sm) {
 // kThreads x C consecutive elements (thread t the elements t, t + kThreads,
 // ... of the block's range, so loads and stores are coalesced), each thread
 // multiplies its C non-zero elements in registers, the block combines the
-// threads' products by a prefix and a suffix scan in shared memory, and ONE
-// Fermat inversion per block gives every thread the inverse of its product
+// threads' products by a prefix and a suffix scan in shared memory, and the
+// inverse of the block's total gives every thread the inverse of its product
 // (prefix x suffix x 1/total); the backward pass then inverts each element.
+// The inverse of the total is one Fermat inversion in the block when the
+// blocks fit one wave on the GPU; otherwise the totals are batch-inverted
+// first (k_invert_totals, then this function on the totals), since a serial
+// inversion per block would leave the SMs idle wave after wave.
+constexpr int kInvPerThread = 4;
+
 template <int C>
-__global__ void __launch_bounds__(kThreads) k_batch_invert(Fr* __restrict__ a, uint64_t n) {
+__global__ void __launch_bounds__(kThreads) k_invert_totals(const Fr* __restrict__ a, uint64_t n, Fr* __restrict__ tot) {
+    __shared__ Fr sm[kThreads];
+    const uint64_t base = (uint64_t)blockIdx.x * kThreads * C + threadIdx.x;
+    Fr acc = fr_one();
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+        const uint64_t i = base + (uint64_t)k * kThreads;
+        if (i < n) {
+            const Fr v = a[i];
+            if (!fr_is_zero(v)) acc = fr_mul(acc, v);
+        }
+    }
+    Fr total;
+    block_exclusive<true>(acc, sm, &total);
+    if (threadIdx.x == 0) tot[blockIdx.x] = total;  // non-zero: a product of non-zero elements (or one)
+}
+
+template <int C, bool kGivenInverse>
+__global__ void __launch_bounds__(kThreads) k_batch_invert(Fr* __restrict__ a, uint64_t n,
+                                                           const Fr* __restrict__ tot_inv) {
     __shared__ Fr sm[kThreads];
     __shared__ Fr total_inv;
     const uint64_t base = (uint64_t)blockIdx.x * kThreads * C + threadIdx.x;
@@ -148,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_invert(Fr* __restrict__ a, u
     Fr total;
     const Fr below = block_exclusive<true>(acc, sm, &total);
     const Fr above = block_exclusive_suffix_product(acc, sm);
-    if (threadIdx.x == 0) total_inv = fr_inv(total);
+    if (threadIdx.x == 0) total_inv = kGivenInverse ? tot_inv[blockIdx.x] : fr_inv(total);
     __syncthreads();
     Fr inv = fr_mul(fr_mul(total_inv, below), above);  // 1 / acc
 #pragma unroll
@@ -161,19 +186,32 @@ __global__ void __launch_bounds__(kThreads) k_batch_invert(Fr* __restrict__ a, u
     }
 }
 
-Status batch_invert(Context* ctx, Fr* a, uint64_t n, cudaStream_t st) {
+Status batch_invert_level(Context* ctx, Fr* a, uint64_t n, cudaStream_t st, int level) {
     if (n == 0) return OK;
-    // 8 elements per thread for large n (one inversion per 2048 elements; 16
-    // would spill the registers), 4 when that would leave SMs without blocks
-    const uint64_t per8 = (uint64_t)kThreads * 8, per4 = (uint64_t)kThreads * 4;
-    if (n >= per8 * (uint64_t)ctx->num_sms * 2) {
-        k_batch_invert<8><<<(uint32_t)((n + per8 - 1) / per8), kThreads, 0, st>>>(a, n);
-    } else {
-        k_batch_invert<4><<<(uint32_t)((n + per4 - 1) / per4), kThreads, 0, st>>>(a, n);
+    const uint64_t per = (uint64_t)kThreads * kInvPerThread;
+    const uint64_t blocks = (n + per - 1) / per;
+    if (blocks <= (uint64_t)ctx->num_sms * 2) {  // one wave at 2 blocks per SM
+        k_batch_invert<kInvPerThread, false><<<(uint32_t)blocks, kThreads, 0, st>>>(a, n, nullptr);
+        MZK_LAUNCH_CHECK(ctx);
+        return OK;
     }
+    if (level >= 4) {
+        set_error("batch_invert: too many elements");
+        return ERR_ARG;
+    }
+    static const char* const kTotNames[4] = {"grand_inv_tot0", "grand_inv_tot1", "grand_inv_tot2", "grand_inv_tot3"};
+    void* buf;
+    MZK_TRY(ctx->ensure(kTotNames[level], blocks * sizeof(Fr), &buf));
+    Fr* tot = static_cast<Fr*>(buf);
+    k_invert_totals<kInvPerThread><<<(uint32_t)blocks, kThreads, 0, st>>>(a, n, tot);
+    MZK_LAUNCH_CHECK(ctx);
+    MZK_TRY(batch_invert_level(ctx, tot, blocks, st, level + 1));
+    k_batch_invert<kInvPerThread, true><<<(uint32_t)blocks, kThreads, 0, st>>>(a, n, tot);
     MZK_LAUNCH_CHECK(ctx);
     return OK;
 }
+
+Status batch_invert(Context* ctx, Fr* a, uint64_t n, cudaStream_t st) { return batch_invert_level(ctx, a, n, st, 0); }
 
 // pass 1: out = exclusive scan within each tile of kThreads * kScanItems, sums[tile] = tile total
 template <bool kMul>

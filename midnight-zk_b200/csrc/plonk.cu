@@ -59,6 +59,7 @@ using host::Fr4;
 namespace {
 
 constexpr uint32_t kThreads = 256;
+constexpr uint32_t kMaxProofLookups = 4;  // lookups of one circuit in create_proof
 
 inline Fr to_dev(const Fr4& a) {
     Fr r;
@@ -245,16 +246,28 @@ struct PlonkKey {
     std::vector<mzk_flat_op> g_ops;
     mzk_flat_graph gates = {};
     std::vector<uint32_t> perm_kind, perm_index;
-    bool has_lookup = false;
-    mzk_lookup_shape lookup = {};
-    uint32_t n_uniq = 0;
+    // lookups, each one advice column into one fixed table column, with the
+    // table index of the multiplicity kernels (device)
+    struct Lookup {
+        mzk_lookup_shape shape = {};
+        uint32_t n_uniq = 0;
+        Fr* uniq = nullptr;       // distinct table values of the usable rows, in the index order
+        uint32_t* uid = nullptr;  // per usable row: its value's index in uniq
+        Fr* tinv = nullptr;       // per distinct value: 1 / (its copies in the table)
+    };
+    std::vector<Lookup> lookups;
+    // with more than one lookup the quotient takes them as helper programs
+    // (one per lookup; the single-lookup case uses the fused built-in term)
+    std::vector<uint64_t> lk_consts;
+    std::vector<int32_t> lk_rots;
+    std::vector<mzk_column_read> lk_reads;
+    std::vector<mzk_flat_op> lk_ops;
+    std::vector<mzk_flat_graph> lk_programs;
+    std::vector<uint32_t> lk_outputs;
     // device
     void* mem = nullptr;
     std::vector<Fr*> fixed_lag, fixed_coeff, fixed_ext, perm_lag, perm_coeff, perm_ext;
     Fr *l0 = nullptr, *l_last = nullptr, *l_active = nullptr, *ones = nullptr;
-    Fr* uniq = nullptr;     // distinct table values of the usable rows, in the index order
-    uint32_t* uid = nullptr;  // per usable row: its value's index in uniq
-    Fr* tinv = nullptr;     // per distinct value: 1 / (its copies in the table)
     mzk_srs_desc srs = {};
     // verifying key
     std::vector<std::array<uint64_t, 18>> fixed_coms, perm_coms;
@@ -289,7 +302,7 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
         return fail("1..16 advice and at most 16 fixed columns");
     if (cs->n_perm_cols > kQMaxPermCols || (cs->n_perm_cols + cs->degree - 3) / (cs->degree - 2) > kQMaxSets)
         return fail("at most 16 permutation columns in at most 8 sets");
-    if (cs->n_lookups > 1) return fail("at most one lookup");
+    if (cs->n_lookups > kMaxProofLookups) return fail("at most 4 lookups");
     if ((cs->n_advice_queries && !cs->advice_queries) || (cs->n_fixed_queries && !cs->fixed_queries))
         return fail("null query list");
     if ((cs->n_perm_cols && (!cs->perm_col_kind || !cs->perm_col_index)) || (cs->n_lookups && !cs->lookups))
@@ -411,6 +424,59 @@ void build_open_sets(PlonkKey* key, const std::vector<std::pair<std::pair<int, u
     for (uint32_t i : order) key->open_sets.push_back(sets[i]);
 }
 
+// The helper program of each lookup for the quotient (Evaluator::lookups_flat,
+// evaluation.rs:686-767, for one input expression: the compressed input and
+// table are the columns themselves, the sum of partial products is the
+// constant one).  Values: 0, 1 (constants), beta, theta, trash challenge, y,
+// the previous value, then the input, table and selector reads and the ops.
+void build_lookup_programs(PlonkKey* key) {
+    const uint32_t L = (uint32_t)key->lookups.size();
+    const Fr4 zero = host::fr_zero(), one = host::fr_one();
+    key->lk_consts.assign(zero.l, zero.l + 4);
+    key->lk_consts.insert(key->lk_consts.end(), one.l, one.l + 4);
+    key->lk_rots = {0};
+    key->lk_reads.clear();
+    key->lk_ops.clear();
+    key->lk_outputs.clear();
+    std::vector<uint32_t> n_reads(L);
+    for (uint32_t l = 0; l < L; l++) {
+        const mzk_lookup_shape& sh = key->lookups[l].shape;
+        key->lk_reads.push_back({1, sh.input_advice, 0, 7});
+        key->lk_reads.push_back({0, sh.table_fixed, 0, 8});
+        n_reads[l] = 2;
+        if (sh.selector_fixed >= 0) {
+            key->lk_reads.push_back({0, (uint32_t)sh.selector_fixed, 0, 9});
+            n_reads[l] = 3;
+        }
+        key->lk_ops.push_back({MZK_FLAT_MULADD, 10, 0, 3, 7});  // 0 theta + input
+        key->lk_ops.push_back({MZK_FLAT_ADD, 11, 10, 2, 0});    // + beta: the product
+        key->lk_ops.push_back({MZK_FLAT_MULADD, 12, 0, 3, 8});  // 0 theta + table
+        key->lk_ops.push_back({MZK_FLAT_ADD, 13, 12, 2, 0});    // + beta
+        for (uint32_t o : {1u, 11u, 13u, sh.selector_fixed >= 0 ? 9u : 1u}) key->lk_outputs.push_back(o);
+    }
+    key->lk_programs.assign(L, mzk_flat_graph{});
+    size_t r0 = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        mzk_flat_graph& g = key->lk_programs[l];
+        g.constants = key->lk_consts.data();
+        g.n_constants = 2;
+        g.rotations = key->lk_rots.data();
+        g.n_rotations = 1;
+        g.reads = key->lk_reads.data() + r0;
+        g.n_reads = n_reads[l];
+        g.ops = key->lk_ops.data() + 4 * (size_t)l;
+        g.n_ops = 4;
+        g.values_len = 14;
+        g.beta_idx = 2;
+        g.theta_idx = 3;
+        g.trash_challenge_idx = 4;
+        g.y_idx = 5;
+        g.previous_value_idx = 6;
+        g.result_idx = 13;
+        r0 += n_reads[l];
+    }
+}
+
 }  // namespace
 
 Status vk_transcript_repr(uint32_t k, const uint64_t* fixed, size_t n_fixed, const uint64_t* perm, size_t n_perm,
@@ -505,35 +571,39 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     }
     key->perm_kind.assign(cs->perm_col_kind, cs->perm_col_kind + P);
     key->perm_index.assign(cs->perm_col_index, cs->perm_col_index + P);
-    key->has_lookup = cs->n_lookups == 1;
-    if (key->has_lookup) key->lookup = cs->lookups[0];
+    const uint32_t L = cs->n_lookups;
+    key->lookups.resize(L);
+    for (uint32_t l = 0; l < L; l++) key->lookups[l].shape = cs->lookups[l];
     key->srs = *srs;
     const uint32_t F = cs->n_fixed, u = key->u;
-    // lookup table index (host): the distinct values of the table's usable
+    // lookup table indexes (host): the distinct values of each table's usable
     // rows in the order of the device search, each row's index, 1 / copies
-    std::vector<std::array<uint64_t, 4>> uniq;
-    std::vector<uint32_t> uid;
-    std::vector<Fr4> tinv;
-    if (key->has_lookup) {
-        const uint64_t* t = fixed_values[key->lookup.table_fixed];
+    std::vector<std::vector<std::array<uint64_t, 4>>> uniq(L);
+    std::vector<std::vector<uint32_t>> uid(L);
+    std::vector<std::vector<Fr4>> tinv(L);
+    bool need_ones = false;
+    size_t uniq_total = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        const uint64_t* t = fixed_values[key->lookups[l].shape.table_fixed];
         std::map<std::array<uint64_t, 4>, uint32_t> count;
         for (uint32_t i = 0; i < u; i++) count[{t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]}]++;
         std::map<std::array<uint64_t, 4>, uint32_t> index;
         for (auto& kv : count) {
             // the device compares the 64-bit words from the lowest: the map's order
-            index[kv.first] = (uint32_t)uniq.size();
-            uniq.push_back(kv.first);
-            tinv.push_back(host::fr_inv(host::fr_from_u64(kv.second)));
+            index[kv.first] = (uint32_t)uniq[l].size();
+            uniq[l].push_back(kv.first);
+            tinv[l].push_back(host::fr_inv(host::fr_from_u64(kv.second)));
         }
-        uid.resize(u);
-        for (uint32_t i = 0; i < u; i++) uid[i] = index[{t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]}];
-        key->n_uniq = (uint32_t)uniq.size();
+        uid[l].resize(u);
+        for (uint32_t i = 0; i < u; i++) uid[l][i] = index[{t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]}];
+        key->lookups[l].n_uniq = (uint32_t)uniq[l].size();
+        uniq_total += uniq[l].size();
+        need_ones = need_ones || key->lookups[l].shape.selector_fixed < 0;
     }
-    const bool need_ones = key->has_lookup && key->lookup.selector_fixed < 0;
     // one device allocation for the whole key
     const size_t fr_elems = (size_t)F * (2 * n + E) + (size_t)P * (2 * n + E) + 3 * (size_t)E + (need_ones ? n : 0) +
-                            2 * (size_t)key->n_uniq;
-    const size_t bytes = fr_elems * sizeof(Fr) + (size_t)u * 4 * key->has_lookup + 256;
+                            2 * uniq_total;
+    const size_t bytes = fr_elems * sizeof(Fr) + (size_t)u * 4 * L + 256;
     cudaError_t e = cudaMalloc(&key->mem, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -563,11 +633,11 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     key->l_last = take(E);
     key->l_active = take(E);
     if (need_ones) key->ones = take(n);
-    if (key->has_lookup) {
-        key->uniq = take(key->n_uniq);
-        key->tinv = take(key->n_uniq);
-        key->uid = reinterpret_cast<uint32_t*>(carve);
+    for (auto& lk : key->lookups) {
+        lk.uniq = take(lk.n_uniq);
+        lk.tinv = take(lk.n_uniq);
     }
+    for (uint32_t l = 0; l < L; l++) key->lookups[l].uid = reinterpret_cast<uint32_t*>(carve) + (size_t)l * u;
     // fixed columns
     for (uint32_t i = 0; i < F; i++) {
         MZK_CUDA_CHECK(cudaMemcpyAsync(key->fixed_lag[i], fixed_values[i], (size_t)n * sizeof(Fr),
@@ -634,11 +704,13 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         k_unit<<<grid_of(ctx, n), kThreads, 0, st>>>(key->ones, n, 0, n);
         MZK_LAUNCH_CHECK(ctx);
     }
-    if (key->has_lookup) {
-        MZK_CUDA_CHECK(cudaMemcpyAsync(key->uniq, uniq.data(), uniq.size() * 32, cudaMemcpyHostToDevice, st));
-        MZK_CUDA_CHECK(cudaMemcpyAsync(key->tinv, tinv.data(), tinv.size() * 32, cudaMemcpyHostToDevice, st));
-        MZK_CUDA_CHECK(cudaMemcpyAsync(key->uid, uid.data(), uid.size() * 4, cudaMemcpyHostToDevice, st));
+    for (uint32_t l = 0; l < L; l++) {
+        PlonkKey::Lookup& lk = key->lookups[l];
+        MZK_CUDA_CHECK(cudaMemcpyAsync(lk.uniq, uniq[l].data(), uniq[l].size() * 32, cudaMemcpyHostToDevice, st));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(lk.tinv, tinv[l].data(), tinv[l].size() * 32, cudaMemcpyHostToDevice, st));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(lk.uid, uid[l].data(), uid[l].size() * 4, cudaMemcpyHostToDevice, st));
     }
+    if (L > 1) build_lookup_programs(key.get());
     // VK commitments (Lagrange basis) as one batch
     std::vector<BatchItem> items;
     for (uint32_t i = 0; i < F; i++) items.push_back({key->fixed_lag[i], srs->off_lagrange, n});
@@ -663,17 +735,17 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         qs.push_back({{PlonkKey::P_PERM_Z, s}, 1});
     }
     for (uint32_t s = key->n_sets; s-- > 1;) qs.push_back({{PlonkKey::P_PERM_Z, s - 1}, key->last_rot()});
-    if (key->has_lookup) {
-        qs.push_back({{PlonkKey::P_M, 0}, 0});
-        qs.push_back({{PlonkKey::P_H, 0}, 0});
-        qs.push_back({{PlonkKey::P_AGG, 0}, 0});
-        qs.push_back({{PlonkKey::P_AGG, 0}, 1});
+    for (uint32_t l = 0; l < L; l++) {  // logup Evaluated::open per lookup
+        qs.push_back({{PlonkKey::P_M, l}, 0});
+        qs.push_back({{PlonkKey::P_H, l}, 0});
+        qs.push_back({{PlonkKey::P_AGG, l}, 0});
+        qs.push_back({{PlonkKey::P_AGG, l}, 1});
     }
     for (auto& q : key->fixed_queries) qs.push_back({{PlonkKey::P_FIXED, q.column}, q.rotation});
     for (uint32_t i = 0; i < P; i++) qs.push_back({{PlonkKey::P_PERM_FIXED, i}, 0});
     qs.push_back({{PlonkKey::P_LIN, 0}, 0});
     build_open_sets(key.get(), qs);
-    const uint32_t L = key->has_lookup ? 1 : 0, S = key->n_sets;
+    const uint32_t S = key->n_sets;
     const size_t points = cs->n_advice + L + S + 2 * L + key->qdeg + 2;
     const size_t scalars = key->advice_queries.size() + key->fixed_queries.size() + P + (S ? 3 * S - 1 : 0) + 4 * L +
                            key->open_sets.size();
@@ -926,13 +998,12 @@ struct FsProof {
     host::Transcript tr;
     Fr4 theta, beta, gamma, trash, y, x, xn, x1, x2, x3, x4;
     std::vector<Fr*> adv_lag, adv_coeff, adv_ext, z_lag, z_delta, z_coeff, z_ext, q, fdiv;
-    Fr *m_lag = nullptr, *m_delta = nullptr, *m_coeff = nullptr, *m_ext = nullptr;
-    Fr *h_lag = nullptr, *h_coeff = nullptr, *h_ext = nullptr;
-    Fr *Z_lag = nullptr, *Z_dd = nullptr, *Z_coeff = nullptr, *Z_ext = nullptr;
+    // per lookup: multiplicities, helper, aggregator
+    std::vector<Fr*> m_lag, m_delta, m_coeff, m_ext, h_lag, h_coeff, h_ext, Z_lag, Z_dd, Z_coeff, Z_ext;
+    std::vector<uint32_t*> counts;
     Fr *limbs = nullptr, *lin = nullptr, *f = nullptr, *fin = nullptr, *pi = nullptr, *tmp_a = nullptr,
        *tmp_b = nullptr;
     Fr* d_blinds = nullptr;
-    uint32_t* counts = nullptr;
     uint64_t f_len = 0;
     // blinding offsets (elements of req->blinds)
     size_t off_mult = 0, off_perm = 0, off_logup = 0, off_quot = 0;
@@ -942,9 +1013,11 @@ struct FsProof {
 
 size_t proof_scratch_elems(const PlonkKey* k) {
     const size_t n = k->n, E = (size_t)1 << k->dom->ext_k, A = k->n_advice, S = k->n_sets;
-    const size_t L = k->has_lookup ? 1 : 0, O = k->open_sets.size();
+    const size_t L = k->lookups.size(), O = k->open_sets.size();
+    size_t counts = 0;
+    for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8;
     return A * (2 * n + E) + S * (3 * n + E) + L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) + k->qdeg * n +
-           (4 + 2 * O + 2) * n + k->n_blinds + L * ((k->n_uniq + 7) / 8);
+           (4 + 2 * O + 2) * n + k->n_blinds + counts;
 }
 
 Status eval_many(Context* ctx, const std::vector<EvalTask>& in, std::vector<Fr4>& results, cudaStream_t st) {
@@ -1142,11 +1215,12 @@ Fr4 identities_at_x(const FsProof& p) {
             ids.push_back(fr_mul(fr_sub(left, right), active));
         }
     }
-    // the lookup (logup.rs:405-485): one input expression and one helper
-    if (k->has_lookup) {
-        const Fr4 m = p.ev_lk[0], h = p.ev_lk[1], Z = p.ev_lk[2], Zn = p.ev_lk[3];
-        const Fr4 f = adv(k->lookup.input_advice), t = fix(k->lookup.table_fixed);
-        const Fr4 sel = k->lookup.selector_fixed >= 0 ? fix((uint32_t)k->lookup.selector_fixed) : one;
+    // the lookups (logup.rs:405-485): one input expression and one helper each
+    for (size_t l = 0; l < k->lookups.size(); l++) {
+        const mzk_lookup_shape& sh = k->lookups[l].shape;
+        const Fr4 m = p.ev_lk[4 * l], h = p.ev_lk[4 * l + 1], Z = p.ev_lk[4 * l + 2], Zn = p.ev_lk[4 * l + 3];
+        const Fr4 f = adv(sh.input_advice), t = fix(sh.table_fixed);
+        const Fr4 sel = sh.selector_fixed >= 0 ? fix((uint32_t)sh.selector_fixed) : one;
         ids.push_back(fr_mul(fr_add(l_0, l_last), Z));
         ids.push_back(fr_sub(fr_mul(h, fr_add(f, p.beta)), one));
         Fr4 acc = fr_sub(fr_sub(Zn, Z), fr_mul(sel, h));
@@ -1163,9 +1237,9 @@ const Fr* open_poly(const FsProof& p, std::pair<int, uint32_t> id) {
     switch (id.first) {
         case PlonkKey::P_ADVICE: return p.adv_coeff[id.second];
         case PlonkKey::P_PERM_Z: return p.z_coeff[id.second];
-        case PlonkKey::P_M: return p.m_coeff;
-        case PlonkKey::P_H: return p.h_coeff;
-        case PlonkKey::P_AGG: return p.Z_coeff;
+        case PlonkKey::P_M: return p.m_coeff[id.second];
+        case PlonkKey::P_H: return p.h_coeff[id.second];
+        case PlonkKey::P_AGG: return p.Z_coeff[id.second];
         case PlonkKey::P_FIXED: return k->fixed_coeff[id.second];
         case PlonkKey::P_PERM_FIXED: return k->perm_coeff[id.second];
         default: return p.lin;
@@ -1257,10 +1331,12 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             p.z_coeff.push_back(take(n));
             p.z_ext.push_back(take(E));
         }
-        if (k->has_lookup) {
-            p.m_lag = take(n), p.m_delta = take(n), p.m_coeff = take(n), p.m_ext = take(E);
-            p.h_lag = take(n), p.h_coeff = take(n), p.h_ext = take(E);
-            p.Z_lag = take(n), p.Z_dd = take(n), p.Z_coeff = take(n), p.Z_ext = take(E);
+        for (size_t l = 0; l < k->lookups.size(); l++) {
+            p.m_lag.push_back(take(n)), p.m_delta.push_back(take(n)), p.m_coeff.push_back(take(n));
+            p.m_ext.push_back(take(E));
+            p.h_lag.push_back(take(n)), p.h_coeff.push_back(take(n)), p.h_ext.push_back(take(E));
+            p.Z_lag.push_back(take(n)), p.Z_dd.push_back(take(n)), p.Z_coeff.push_back(take(n));
+            p.Z_ext.push_back(take(E));
         }
         p.limbs = take((size_t)k->qdeg * n);
         p.lin = take(n), p.f = take(n), p.fin = take(n), p.pi = take(n);
@@ -1270,9 +1346,9 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         }
         p.tmp_a = take(n), p.tmp_b = take(n);
         p.d_blinds = take(k->n_blinds);
-        if (k->has_lookup) p.counts = reinterpret_cast<uint32_t*>(take((k->n_uniq + 7) / 8));
+        for (const auto& lk : k->lookups) p.counts.push_back(reinterpret_cast<uint32_t*>(take((lk.n_uniq + 7) / 8)));
         carve = start + proof_scratch_elems(k) + 8;
-        const size_t A = k->n_advice, L = k->has_lookup ? 1 : 0;
+        const size_t A = k->n_advice, L = k->lookups.size();
         p.off_mult = A * (k->bf + 1);
         p.off_perm = p.off_mult + L * (k->bf + 1);
         p.off_logup = p.off_perm + (size_t)k->n_sets * k->bf;
@@ -1324,19 +1400,22 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     for (size_t j = 0; j < count; j++) {
         FsProof& p = ps[j];
         const PlonkKey* k = p.key;
-        if (!k->has_lookup) continue;
         const uint32_t n = k->n, u = k->u;
-        const Fr* sel = k->lookup.selector_fixed >= 0 ? k->fixed_lag[k->lookup.selector_fixed] : nullptr;
-        MZK_CUDA_CHECK(cudaMemsetAsync(p.counts, 0, (size_t)k->n_uniq * 4, st));
-        k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(p.adv_lag[k->lookup.input_advice], sel, u, k->uniq,
-                                                             k->n_uniq, p.counts, static_cast<uint32_t*>(dmiss) + j);
-        MZK_LAUNCH_CHECK(ctx);
-        k_lookup_m<<<grid_of(ctx, u), kThreads, 0, st>>>(p.m_lag, k->uid, p.counts, k->tinv, u);
-        MZK_LAUNCH_CHECK(ctx);
-        MZK_CUDA_CHECK(cudaMemcpyAsync(p.m_lag + u, p.d_blinds + p.off_mult, (size_t)(n - u) * sizeof(Fr),
-                                       cudaMemcpyDeviceToDevice, st));
-        MZK_TRY(delta_device(ctx, p.m_lag, p.m_delta, n, 1, st));
-        items.push_back({p.m_delta, k->srs.off_lagrange_delta, n});
+        for (size_t l = 0; l < k->lookups.size(); l++) {
+            const PlonkKey::Lookup& lk = k->lookups[l];
+            const Fr* sel = lk.shape.selector_fixed >= 0 ? k->fixed_lag[lk.shape.selector_fixed] : nullptr;
+            MZK_CUDA_CHECK(cudaMemsetAsync(p.counts[l], 0, (size_t)lk.n_uniq * 4, st));
+            k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(p.adv_lag[lk.shape.input_advice], sel, u, lk.uniq,
+                                                                 lk.n_uniq, p.counts[l],
+                                                                 static_cast<uint32_t*>(dmiss) + j);
+            MZK_LAUNCH_CHECK(ctx);
+            k_lookup_m<<<grid_of(ctx, u), kThreads, 0, st>>>(p.m_lag[l], lk.uid, p.counts[l], lk.tinv, u);
+            MZK_LAUNCH_CHECK(ctx);
+            MZK_CUDA_CHECK(cudaMemcpyAsync(p.m_lag[l] + u, p.d_blinds + p.off_mult + l * (k->bf + 1),
+                                           (size_t)(n - u) * sizeof(Fr), cudaMemcpyDeviceToDevice, st));
+            MZK_TRY(delta_device(ctx, p.m_lag[l], p.m_delta[l], n, 1, st));
+            items.push_back({p.m_delta[l], k->srs.off_lagrange_delta, n});
+        }
     }
     MZK_TRY(msm());
     {
@@ -1350,7 +1429,8 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     }
     for (size_t j = 0, at = 0; j < count; j++) {
         FsProof& p = ps[j];
-        if (p.key->has_lookup) write_points(p, &res[18 * at++], 1);
+        write_points(p, &res[18 * at], p.key->lookups.size());
+        at += p.key->lookups.size();
         p.beta = p.tr.squeeze();
         p.gamma = p.tr.squeeze();
     }
@@ -1386,34 +1466,35 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 items.push_back({p.z_delta[s], k->srs.off_lagrange_delta, n});
             }
         }
-        if (k->has_lookup) {
-            const uint64_t* in[1] = {reinterpret_cast<const uint64_t*>(p.adv_lag[k->lookup.input_advice])};
-            uint64_t* ho[1] = {reinterpret_cast<uint64_t*>(p.h_lag)};
+        for (size_t l = 0; l < k->lookups.size(); l++) {
+            const mzk_lookup_shape& sh = k->lookups[l].shape;
+            const uint64_t* in[1] = {reinterpret_cast<const uint64_t*>(p.adv_lag[sh.input_advice])};
+            uint64_t* ho[1] = {reinterpret_cast<uint64_t*>(p.h_lag[l])};
             const uint32_t cols[1] = {1};
             mzk_logup_desc ld;
             std::memset(&ld, 0, sizeof(ld));
             ld.n_chunks = 1;
             ld.chunk_cols = cols;
             ld.inputs = in;
-            ld.table = reinterpret_cast<const uint64_t*>(k->fixed_lag[k->lookup.table_fixed]);
-            ld.selector = reinterpret_cast<const uint64_t*>(
-                k->lookup.selector_fixed >= 0 ? k->fixed_lag[k->lookup.selector_fixed] : k->ones);
-            ld.multiplicities = reinterpret_cast<const uint64_t*>(p.m_lag);
+            ld.table = reinterpret_cast<const uint64_t*>(k->fixed_lag[sh.table_fixed]);
+            ld.selector = reinterpret_cast<const uint64_t*>(sh.selector_fixed >= 0 ? k->fixed_lag[sh.selector_fixed]
+                                                                                     : k->ones);
+            ld.multiplicities = reinterpret_cast<const uint64_t*>(p.m_lag[l]);
             ld.blinding_factors = k->bf;
-            ld.blinds = p.req->blinds + 4 * p.off_logup;
+            ld.blinds = p.req->blinds + 4 * (p.off_logup + l * k->bf);
             std::memcpy(ld.beta, p.beta.l, 32);
             ld.helpers_out = ho;
-            ld.aggregator_out = reinterpret_cast<uint64_t*>(p.Z_lag);
+            ld.aggregator_out = reinterpret_cast<uint64_t*>(p.Z_lag[l]);
             MZK_TRY(logup_device(ctx, k->dom, &ld, st));
-            MZK_TRY(delta_device(ctx, p.Z_lag, p.Z_dd, n, 2, st));
-            items.push_back({p.h_lag, k->srs.off_lagrange, n});
-            items.push_back({p.Z_dd, k->srs.off_lagrange_double_delta, n});
+            MZK_TRY(delta_device(ctx, p.Z_lag[l], p.Z_dd[l], n, 2, st));
+            items.push_back({p.h_lag[l], k->srs.off_lagrange, n});
+            items.push_back({p.Z_dd[l], k->srs.off_lagrange_double_delta, n});
         }
     }
     MZK_TRY(msm());
     for (size_t j = 0, at = 0; j < count; j++) {
         FsProof& p = ps[j];
-        const size_t m = p.key->n_sets + (p.key->has_lookup ? 2 : 0);
+        const size_t m = p.key->n_sets + 2 * p.key->lookups.size();
         write_points(p, &res[18 * at], m);
         at += m;
         p.trash = p.tr.squeeze();  // no trashcans: nothing is committed after it
@@ -1437,10 +1518,10 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             co.push_back(p.z_coeff[s]);
             ex.push_back(p.z_ext[s]);
         }
-        if (k->has_lookup) {
-            lag.insert(lag.end(), {p.m_lag, p.h_lag, p.Z_lag});
-            co.insert(co.end(), {p.m_coeff, p.h_coeff, p.Z_coeff});
-            ex.insert(ex.end(), {p.m_ext, p.h_ext, p.Z_ext});
+        for (size_t l = 0; l < k->lookups.size(); l++) {
+            lag.insert(lag.end(), {p.m_lag[l], p.h_lag[l], p.Z_lag[l]});
+            co.insert(co.end(), {p.m_coeff[l], p.h_coeff[l], p.Z_coeff[l]});
+            ex.insert(ex.end(), {p.m_ext[l], p.h_ext[l], p.Z_ext[l]});
         }
         MZK_TRY(ntt_sequence(ctx, d, lag.data(), co.data(), ex.data(), (int)lag.size(),
                              !(flags & MZK_PROVE_NO_GRAPHS), st));
@@ -1468,14 +1549,30 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         q.perm_z = zs.data();
         q.chunk_len = k->chunk;
         q.blinding_factors = k->bf;
-        if (k->has_lookup) {
+        const size_t L = k->lookups.size();
+        std::vector<const uint64_t*> hext(L);
+        std::vector<mzk_lookup_arg> largs(L);
+        if (L == 1) {  // the fused built-in term
+            const mzk_lookup_shape& sh = k->lookups[0].shape;
             q.has_lookup = 1;
-            q.lookup_input_advice = k->lookup.input_advice;
-            q.lookup_table_fixed = k->lookup.table_fixed;
-            q.lookup_selector_fixed = k->lookup.selector_fixed;
-            q.lookup_h = reinterpret_cast<const uint64_t*>(p.h_ext);
-            q.lookup_z = reinterpret_cast<const uint64_t*>(p.Z_ext);
-            q.lookup_m = reinterpret_cast<const uint64_t*>(p.m_ext);
+            q.lookup_input_advice = sh.input_advice;
+            q.lookup_table_fixed = sh.table_fixed;
+            q.lookup_selector_fixed = sh.selector_fixed;
+            q.lookup_h = reinterpret_cast<const uint64_t*>(p.h_ext[0]);
+            q.lookup_z = reinterpret_cast<const uint64_t*>(p.Z_ext[0]);
+            q.lookup_m = reinterpret_cast<const uint64_t*>(p.m_ext[0]);
+        } else if (L > 1) {  // one helper program per lookup
+            for (size_t l = 0; l < L; l++) {
+                hext[l] = reinterpret_cast<const uint64_t*>(p.h_ext[l]);
+                largs[l].n_helpers = 1;
+                largs[l].programs = &k->lk_programs[l];
+                largs[l].outputs = &k->lk_outputs[4 * l];
+                largs[l].helpers = &hext[l];
+                largs[l].aggregator = reinterpret_cast<const uint64_t*>(p.Z_ext[l]);
+                largs[l].multiplicities = reinterpret_cast<const uint64_t*>(p.m_ext[l]);
+            }
+            q.n_lookups = (uint32_t)L;
+            q.lookups = largs.data();
         }
         q.l0 = reinterpret_cast<const uint64_t*>(k->l0);
         q.l_last = reinterpret_cast<const uint64_t*>(k->l_last);
@@ -1512,11 +1609,11 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 tasks.push_back(eval_task(p.z_coeff[s], n, fr_rot(d, p.x, 1)));
                 tasks.push_back(eval_task(p.z_coeff[s], n, fr_rot(d, p.x, k->last_rot())));
             }
-            if (k->has_lookup) {
-                tasks.push_back(eval_task(p.m_coeff, n, p.x));
-                tasks.push_back(eval_task(p.h_coeff, n, p.x));
-                tasks.push_back(eval_task(p.Z_coeff, n, p.x));
-                tasks.push_back(eval_task(p.Z_coeff, n, fr_rot(d, p.x, 1)));
+            for (size_t l = 0; l < k->lookups.size(); l++) {
+                tasks.push_back(eval_task(p.m_coeff[l], n, p.x));
+                tasks.push_back(eval_task(p.h_coeff[l], n, p.x));
+                tasks.push_back(eval_task(p.Z_coeff[l], n, p.x));
+                tasks.push_back(eval_task(p.Z_coeff[l], n, fr_rot(d, p.x, 1)));
             }
         }
         std::vector<Fr4> ev;
@@ -1533,7 +1630,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             grab(p.ev_fix, k->fixed_queries.size());
             grab(p.ev_pc, k->n_perm);
             grab(p.ev_sets, 3 * (size_t)k->n_sets);
-            grab(p.ev_lk, k->has_lookup ? 4 : 0);
+            grab(p.ev_lk, 4 * k->lookups.size());
             // transcript order (write_evals_to_transcript, permutation / logup evaluate)
             for (auto& v : p.ev_adv) p.tr.write_fr(v);
             for (auto& v : p.ev_fix) p.tr.write_fr(v);
@@ -1845,7 +1942,7 @@ int mzk_plonk_key_transcript_layout(const mzk_plonk_key* key, uint8_t* ops, size
     const mzk::PlonkKey* k = reinterpret_cast<const mzk::PlonkKey*>(key);
     std::vector<uint8_t> v;
     auto put = [&](uint8_t op, size_t times) { v.insert(v.end(), times, op); };
-    const size_t L = k->has_lookup ? 1 : 0, S = k->n_sets;
+    const size_t L = k->lookups.size(), S = k->n_sets;
     put(MZK_TR_COMMON_FR, 1);                  // vk.hash_into
     put(MZK_TR_WRITE_POINT, k->n_advice);      // advice commitments
     put(MZK_TR_SQUEEZE, 1);                    // theta

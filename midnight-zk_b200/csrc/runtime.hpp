@@ -182,6 +182,8 @@ enum MsmPhase { PH_HISTOGRAM = 0, PH_SCAN, PH_SCATTER, PH_ACCUMULATE, PH_FIXUP, 
 // rate of full 12-limb Montgomery multiplications, both per second
 Status probe_imad(Context* ctx, double* imad_per_s, double* fp_mul_per_s, double* variants);
 Status check_fp_sqr(Context* ctx, const void* d_values, size_t n, uint64_t* mismatches);
+Status check_fp_inv(Context* ctx, const void* d_values, size_t n, uint64_t* mismatches);
+Status probe_batch_affine(Context* ctx, double* out);
 
 // ---- synthetic inputs (gen.cu) ----
 Status gen_rand_fr(Context* ctx, uint64_t seed, uint64_t first, size_t n, void* d_out, cudaStream_t stream);

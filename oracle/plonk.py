@@ -299,12 +299,14 @@ def config3_instance(k, seed, table_bits=16, copy_fraction=0.10):
     return fixed, mapping, [a, b, cc_col]
 
 
-def generic_circuit(k):
+def generic_circuit(k, two_lookups=False):
     """A circuit of another shape: advice a, b, c, d with a queried at rotations
     0 and 1, fixed q1, q2, q3, q4, the table and the lookup selector; two gates
     as one flattened program, q1 a b + q2 a(wX) - q4 c and q3 (d - a^2), folded
     by Horner in y; the permutation over a, b, c, d (two sets of three and one
-    columns); a lookup of a into the table; degree 5."""
+    columns); a lookup of a into the table; degree 5.  two_lookups: a seventh
+    fixed column, the table of squares, and a second lookup, of d into it
+    without a selector."""
     zero, one = to_mont(0), to_mont(1)
     gates = {"constants": [zero, one], "rotations": [0, 1],
              # values: constants 0, 1; slots beta 2, theta 3, trash 4, y 5, previous 6; reads 7..15
@@ -315,12 +317,16 @@ def generic_circuit(k):
                      (2, 24, 9, 23, 0), (6, 25, 6, 5, 21), (6, 26, 25, 5, 24)],
              "values_len": 27, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
              "previous_value_idx": 6, "result_idx": 26}
-    return {"k": k, "degree": 5, "n_advice": 4, "n_fixed": 6,
+    nf = 7 if two_lookups else 6
+    lookups = [{"input": 0, "table": 4, "selector": 5}]
+    if two_lookups:
+        lookups.append({"input": 3, "table": 6, "selector": None})
+    return {"k": k, "degree": 5, "n_advice": 4, "n_fixed": nf,
             "advice_queries": [(0, 0), (1, 0), (2, 0), (3, 0), (0, 1)],
-            "fixed_queries": [(i, 0) for i in range(6)],
+            "fixed_queries": [(i, 0) for i in range(nf)],
             "gates": gates,
             "perm_cols": [(0, 0), (0, 1), (0, 2), (0, 3)],
-            "lookups": [{"input": 0, "table": 4, "selector": 5}]}
+            "lookups": lookups}
 
 
 def _cycles(rng, n, u, n_cols, cycle_cols, fraction, rows):
@@ -350,13 +356,15 @@ def _cycles(rng, n, u, n_cols, cycle_cols, fraction, rows):
     return mapping, vals
 
 
-def generic_instance(k, seed, table_bits=16, copy_fraction=0.10):
+def generic_instance(k, seed, table_bits=16, copy_fraction=0.10, two_lookups=False):
     """Seeded fixed columns, copy cycles (over the a and b cells of rows
     before the last usable row) and a satisfying witness of generic_circuit:
     a a table value, b uniform, c = q1 a b + q2 a(wX), d = a^2; the gate
     selectors q1, q2, q4 are zero from the last usable row on (its a(wX) is a
-    blinding row), q3 from the usable rows on."""
-    c = generic_circuit(k)
+    blinding row), q3 from the usable rows on.  two_lookups: the table of
+    squares t2[i] = i^2 (i < the table's rows; zero after), which holds every
+    usable d."""
+    c = generic_circuit(k, two_lookups)
     n = 1 << k
     bf = blinding_factors(c)
     u = n - bf - 1
@@ -391,7 +399,21 @@ def generic_instance(k, seed, table_bits=16, copy_fraction=0.10):
     cc_col[u - 1:] = 0
     d = _hadamard(a, a)
     d[u:] = 0
-    return [q1, q2, q3, q4, table, sel], mapping, [a, b, cc_col, d]
+    fixed = [q1, q2, q3, q4, table, sel]
+    if two_lookups:
+        squares = np.zeros((n, 4), np.uint64)
+        squares[:rows] = np.stack([to_mont(v * v) for v in range(rows)])
+        fixed.append(squares)
+    return fixed, mapping, [a, b, cc_col, d]
+
+
+def generic2_circuit(k):
+    """generic_circuit with its second lookup (d into the table of squares)."""
+    return generic_circuit(k, two_lookups=True)
+
+
+def generic2_instance(k, seed):
+    return generic_instance(k, seed, two_lookups=True)
 
 
 def _hadamard(x, y):
@@ -851,7 +873,7 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     d.perm_sigma = parr(key.perm_cosets)
     d.n_perm_sets, d.perm_z = len(z_e), parr(z_e)
     d.chunk_len, d.blinding_factors = c["degree"] - 2, key.bf
-    if c["lookups"]:
+    if len(c["lookups"]) == 1:
         lk = c["lookups"][0]
         d.has_lookup = 1
         d.lookup_input_advice, d.lookup_table_fixed = lk["input"], lk["table"]
@@ -867,7 +889,35 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     if c.get("gates") is not None:
         gate_values = O.flat_gates_eval(c["gates"], key.fixed_cosets, adv_e, [], c["k"], dom.extended_k,
                                         to_mont(beta), to_mont(theta), to_mont(trash), to_mont(y))
-    return dom.quotient_eval(d, True, threads, gate_values)
+    if len(c["lookups"]) <= 1:
+        return dom.quotient_eval(d, True, threads, gate_values)
+    # several lookups: the gate and permutation terms, then every lookup's
+    # terms (evaluation.rs:1034-1090) as single-input helper programs
+    # (Evaluator::lookups_flat, :686-767), then the division by t(X)
+    v = dom.quotient_eval(d, False, threads, gate_values)
+    lks = [{"programs": [g], "outputs": [outs], "helpers": [h_e[li]], "aggregator": Z_e[li],
+            "multiplicities": m_e[li]}
+           for li, (g, outs) in enumerate(lookup_program(lk) for lk in c["lookups"])]
+    v = O.flat_tail_eval(v, key.fixed_cosets, adv_e, [], c["k"], dom.extended_k, to_mont(beta), to_mont(theta),
+                         to_mont(trash), to_mont(y), key.l0, key.l_last, key.l_active, lookups=lks)
+    return dom.divide_by_vanishing_poly(v)
+
+
+def lookup_program(lk):
+    """The helper program of a lookup whose input is one advice column and
+    whose table is one fixed column: values 0, 1 (constants), beta, theta,
+    trash challenge, y, the previous value, the input, table and selector
+    reads; the compressed input and table (0 theta + column) plus beta; the
+    sum of partial products of one input is the constant one.  Returns
+    (graph, (sum_partial_products, product, table, selector) indices)."""
+    reads = [(1, lk["input"], 0, 7), (0, lk["table"], 0, 8)]
+    if lk["selector"] is not None:
+        reads.append((0, lk["selector"], 0, 9))
+    ops = [(6, 10, 0, 3, 7), (0, 11, 10, 2, 0), (6, 12, 0, 3, 8), (0, 13, 12, 2, 0)]
+    graph = {"constants": [np.zeros(4, np.uint64), O.fr_const(0)], "rotations": [0], "reads": reads, "ops": ops,
+             "values_len": 14, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
+             "previous_value_idx": 6, "result_idx": 13}
+    return graph, (1, 11, 13, 9 if lk["selector"] is not None else 1)
 
 
 def multi_open(key, tr, queries):

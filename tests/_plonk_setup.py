@@ -15,7 +15,8 @@ mzk = load()
 PINNED = b"config-3 circuit: standard gate, copy cycles, range lookup"
 
 
-SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.generic_circuit, OP.generic_instance)}
+SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.generic_circuit, OP.generic_instance),
+          "generic2": (OP.generic2_circuit, OP.generic2_instance)}
 
 
 class Circuit:
@@ -23,8 +24,9 @@ class Circuit:
         """srs = (buffer, offsets) of a shared device SRS whose bases hold this
         k's g | lagrange | delta | double delta at the offsets; otherwise
         this circuit gets its own.  shape: "config3" (the single-proof
-        configuration) or "generic" (two gates with a rotation, two
-        permutation sets)."""
+        configuration), "generic" (two gates with a rotation, two
+        permutation sets) or "generic2" (generic with a second lookup,
+        without a selector)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)

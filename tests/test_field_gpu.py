@@ -44,3 +44,24 @@ def test_square_matches_multiplication(ctx):
     buf.upload(vals)
     assert ctx.probe_fp_sqr_check(buf, vals.shape[0]) == 0
     assert ctx.probe_fp_sqr_check(buf, 0) == 0
+
+
+def test_binary_inverse_matches_fermat(ctx):
+    """The binary extended Euclidean inversion (the batch inversion's per-block
+    step uses it over Fr) equals the Fermat power over Fp and gives a^-1 a = 1,
+    on point coordinates, their lazily reduced representatives and the edge
+    values (zeros are skipped)."""
+    pts = O.gen_bases(92, 1 << 12)
+    coords = pts.reshape(-1, 6)
+    lazy = np.stack([limbs(int.from_bytes(c.tobytes(), "little") + P) for c in coords[:512]])
+    vals = np.concatenate([edge_values(), coords, lazy])
+    buf = ctx.alloc(vals.nbytes)
+    buf.upload(vals)
+    assert ctx.probe_fp_inv_check(buf, vals.shape[0]) == 0
+
+
+def test_batch_affine_probe_runs(ctx):
+    """The batch-affine microbenchmark reports a rate for every batch size and
+    inversion (its figures are recorded with the MSM design)."""
+    rates = ctx.probe_batch_affine()
+    assert len(rates) == 8 and all(r > 0 for r in rates.values())

@@ -29,10 +29,24 @@ def dev(ctx, a):
     return b
 
 
-@pytest.mark.parametrize("n", [1, 5, 64, 1000, 1 << 16])
+@pytest.mark.parametrize("n", [1, 5, 64, 1000, 1 << 16, (1 << 20) + 3])
 def test_batch_invert(ctx, n):
+    """Up to one wave of blocks: one inversion per block; 2^20 + 3: the block
+    totals are batch-inverted first."""
     a = O.rand_fr(n, n)
     a[:: max(1, n // 7)] = 0
+    b = dev(ctx, a)
+    ctx.batch_invert_device(b, n)
+    assert np.array_equal(b.download((n, 4)), O.batch_invert(a))
+
+
+def test_batch_invert_with_all_zero_blocks(ctx):
+    """Blocks whose elements are all zero (their total is the empty product
+    one) beside ordinary ones, on the path that inverts the block totals."""
+    n = 1 << 20
+    a = O.rand_fr(77, n)
+    a[:5000] = 0
+    a[700000:704096] = 0
     b = dev(ctx, a)
     ctx.batch_invert_device(b, n)
     assert np.array_equal(b.download((n, 4)), O.batch_invert(a))

@@ -120,6 +120,34 @@ def test_quotient_work_count(k):
     assert count == 37 * E + 1
 
 
+def test_two_lookup_circuit_proofs_verify():
+    """Two lookups, the second without a selector: multiplicities, helpers and
+    aggregators committed, evaluated and opened lookup by lookup; the
+    quotient takes the lookups as helper programs.  A proof verifies, a
+    tampered one does not, and an input outside its table is refused."""
+    k = 5
+    c = OP.generic2_circuit(k)
+    fixed, mapping, adv = OP.generic2_instance(k, 11)
+    s = O.rand_fr(58, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"generic2")
+    assert len(c["lookups"]) == 2 and key.bf == OP.blinding_factors(c)
+    bl = [OP.to_int(v) for v in O.rand_fr(68, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl)
+    A, L, S, qdeg = 4, 2, 2, 4
+    points = A + L + S + 2 * L + qdeg + 2                      # advice, m, z, (h, Z), limbs, f, pi
+    scalars_before_q = len(c["advice_queries"]) + len(c["fixed_queries"]) + 4 + (3 * S - 1) + 4 * L
+    assert (len(proof) - 48 * points - 32 * scalars_before_q) // 32 in range(2, 8)   # the q evaluations
+    assert OP.verify(key, proof, OP.to_int(s))
+    bad = bytearray(proof)
+    bad[4 * 48 + 48 + 5] ^= 1                                  # the second multiplicity commitment
+    assert not OP.verify(key, bytes(bad), OP.to_int(s))
+    wrong = [a.copy() for a in adv]
+    wrong[3][2] = OP.to_mont(OP.to_int(wrong[3][2]) + 1)       # d no longer a square in the table
+    with pytest.raises(ValueError):
+        OP.create_proof(key, wrong, bl)
+
+
 def test_generic_circuit_proofs_verify():
     """Another circuit shape: two gates as one flattened program (with a(wX)),
     four permutation columns in two sets (z of the first set opened at
