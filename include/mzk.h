@@ -285,7 +285,7 @@ typedef struct {
     uint32_t gate_fixed[5];   /* q_l, q_r, q_m, q_o, q_c */
     uint32_t gate_advice[3];  /* a, b, c */
     uint32_t n_perm_cols;
-    const uint32_t *perm_col_kind;     /* 0 advice, 1 fixed */
+    const uint32_t *perm_col_kind;     /* 0 advice, 1 fixed, 2 instance */
     const uint32_t *perm_col_index;
     const uint64_t *const *perm_sigma; /* permutation_pk_cosets, one per column */
     uint32_t n_perm_sets;
@@ -418,13 +418,17 @@ typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } m
  * gates null, the standard gate q_l a + q_r b + q_m a b + q_o c + q_c over
  * fixed columns gate_fixed and advice columns gate_advice (each queried at
  * rotation 0).
- * Permutation columns: kind 0 advice, 1 fixed; sets of degree - 2 columns.
+ * Permutation columns: kind 0 advice, 1 fixed, 2 instance; sets of degree - 2 columns.
  * The query lists and their order are the reference's (they fix the order
  * of the evaluations in the proof).  Limits: 16 advice, 16 fixed, 16
  * permutation columns (8 sets), at most 4 lookups (each one advice column
  * into one fixed table column; their multiplicities, helpers and aggregators
  * are committed, evaluated and opened lookup by lookup, as logup/prover.rs
- * does), no instance columns, trashcans or simple selectors. */
+ * does), at most 4 instance columns (the reference's default, without the
+ * committed-instances feature: every proof's instance values are absorbed
+ * into its transcript, compute_instances, prover.rs:475-539; gates may read
+ * them, `col_type` 2, at their queried rotations, and permutation columns of
+ * kind 2 are instance columns), no trashcans or simple selectors. */
 typedef struct {
     uint32_t degree;                   /* cs.degree() (plonk/circuit.rs:2174-2199), 3..9 */
     uint32_t blinding_factors;         /* cs.blinding_factors() (circuit.rs:2203-2245) */
@@ -437,6 +441,8 @@ typedef struct {
     const uint32_t *perm_col_kind, *perm_col_index;
     uint32_t n_lookups;
     const mzk_lookup_shape *lookups;
+    uint32_t n_instance;               /* instance columns (0..4) */
+    const mzk_query *instance_queries; uint32_t n_instance_queries;
 } mzk_circuit_desc;
 /* ParamsKZG's bases (params.rs:83-93) inside one DEVICE G1Affine buffer;
  * table_c > 0: srs is row 0 of a window table of that width and table_rows
@@ -498,7 +504,10 @@ int mzk_pk_read(mzk_ctx *ctx, mzk_domain *d, const mzk_circuit_desc *cs, const m
 /* The transcript operations of one proof of this key, in order: one code per
  * operation (MZK_TR_*).  A caller holding its own transcript object (the
  * reference's CircuitTranscript) replays a proof into it with these: a
- * point is 48 proof bytes, a scalar 32, a squeeze reads nothing. */
+ * point is 48 proof bytes, a scalar 32, a squeeze reads nothing.  A key with
+ * instance columns also absorbs, right after the VK's repr, each instance
+ * column's length and values (common, not in the proof bytes; the caller
+ * holds them): those operations depend on the request and are not listed. */
 #define MZK_TR_COMMON_FR 0   /* the VK's transcript_repr (not in the proof bytes) */
 #define MZK_TR_WRITE_POINT 1
 #define MZK_TR_WRITE_FR 2
@@ -521,13 +530,18 @@ int mzk_plonk_key_srs(const mzk_plonk_key *key, mzk_srs_desc *out);
  * every lookup (:168, bf each), then the degree - 2 quotient-limb blinds
  * (blind_quotient_limbs draws those from OsRng, prover.rs:774-785; taking them
  * from the caller makes proofs reproducible).  proof_out receives the
- * transcript bytes (Transcript::finalize). */
+ * transcript bytes (Transcript::finalize).  instance / instance_len: the
+ * values of each instance column of the key (HOST, Montgomery Fr, at most
+ * n - blinding_factors - 1 each, else MZK_ERR_ARG as Error::InstanceTooLarge;
+ * rows past a column's values are zero); null when the key has none. */
 typedef struct {
     const mzk_plonk_key *key;
     const uint64_t *const *advice;
     int advice_on_device;
     const uint64_t *blinds;  /* HOST, n_blinds Fr */
     uint8_t *proof_out;      /* HOST, at least proof_len bytes */
+    const uint64_t *const *instance;
+    const uint64_t *instance_len;
 } mzk_proof_request;
 /* create_proof (plonk/prover.rs:432-473) for `count` proofs, any keys over
  * one SRS buffer: each phase of the reference's Fiat-Shamir order (advice

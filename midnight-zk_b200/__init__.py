@@ -862,11 +862,11 @@ class ProvingServer:
         ctx._servers.add(self)
         self._held = {}
 
-    def submit(self, key, advice, blinds):
+    def submit(self, key, advice, blinds, instance=None):
         """Queue one proof of `key` (a PlonkKey) over the advice columns (host
-        arrays or DeviceBuffers) and the blinding values; wait() returns its
-        transcript."""
-        req, keep, out = _proof_request(key, advice, blinds)
+        arrays or DeviceBuffers), the blinding values and the instance columns'
+        values; wait() returns its transcript."""
+        req, keep, out = _proof_request(key, advice, blinds, instance)
         t = np.zeros(1, np.uint64)
         _check(lib().mzk_server_submit(self.h, ctypes.byref(req), _ptr(t)))
         self._held[int(t[0])] = (req, keep, out)
@@ -918,7 +918,9 @@ class CircuitDesc(ctypes.Structure):
                 ("gate_fixed", ctypes.c_uint32 * 5), ("gate_advice", ctypes.c_uint32 * 3),
                 ("gates", ctypes.c_void_p),
                 ("n_perm_cols", ctypes.c_uint32), ("perm_col_kind", ctypes.c_void_p),
-                ("perm_col_index", ctypes.c_void_p), ("n_lookups", ctypes.c_uint32), ("lookups", ctypes.c_void_p)]
+                ("perm_col_index", ctypes.c_void_p), ("n_lookups", ctypes.c_uint32), ("lookups", ctypes.c_void_p),
+                ("n_instance", ctypes.c_uint32), ("instance_queries", ctypes.c_void_p),
+                ("n_instance_queries", ctypes.c_uint32)]
 
 
 class SrsDesc(ctypes.Structure):
@@ -949,7 +951,8 @@ def prover_table_width(k):
 class ProofRequest(ctypes.Structure):
     """mzk_proof_request (include/mzk.h)."""
     _fields_ = [("key", ctypes.c_void_p), ("advice", ctypes.c_void_p), ("advice_on_device", ctypes.c_int),
-                ("blinds", ctypes.c_void_p), ("proof_out", ctypes.c_void_p)]
+                ("blinds", ctypes.c_void_p), ("proof_out", ctypes.c_void_p), ("instance", ctypes.c_void_p),
+                ("instance_len", ctypes.c_void_p)]
 
 
 
@@ -1012,8 +1015,9 @@ class PlonkKey:
 
     circuit: dict with degree, blinding_factors, n_advice, n_fixed,
     advice_queries / fixed_queries [(column, rotation)], gate_fixed (5),
-    gate_advice (3), perm_cols [(kind 0 advice | 1 fixed, column)], lookups
-    [{"input", "table", "selector" (None: constant one)}].  fixed_values:
+    gate_advice (3), perm_cols [(kind 0 advice | 1 fixed | 2 instance,
+    column)], lookups [{"input", "table", "selector" (None: constant one)}],
+    n_instance and instance_queries [(column, rotation)] (optional).  fixed_values:
     host (n, 4) arrays; mapping: (n_perm_cols, n, 2) uint32 or None; srs:
     an SrsDesc.  The domain and the SRS buffer must outlive the key."""
 
@@ -1053,6 +1057,10 @@ class PlonkKey:
         cs.n_lookups = len(lks)
         cs.lookups = arr(LookupShape, [LookupShape(lk["input"], lk["table"],
                                                    -1 if lk["selector"] is None else lk["selector"]) for lk in lks])
+        cs.n_instance = circuit.get("n_instance", 0)
+        iq = circuit.get("instance_queries", [])
+        cs.instance_queries = arr(Query, [Query(c, r) for c, r in iq])
+        cs.n_instance_queries = len(iq)
         pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
         h = _vp()
         if pk_bytes is not None:
@@ -1132,8 +1140,9 @@ class DevicePtr:
         self.buf, self.ptr = buf, _dptr(buf) + int(offset_bytes)
 
 
-def _proof_request(key, advice, blinds):
-    """A ProofRequest with the buffers it points to (kept alive by the caller)."""
+def _proof_request(key, advice, blinds, instance=None):
+    """A ProofRequest with the buffers it points to (kept alive by the caller).
+    instance: one host array of Fr values (m, 4) per instance column of the key."""
     on_dev = isinstance(advice[0], (DeviceBuffer, DevicePtr))
     keep = [key]
     if on_dev:
@@ -1153,19 +1162,30 @@ def _proof_request(key, advice, blinds):
     req = ProofRequest()
     req.key, req.advice, req.advice_on_device = key.h, ctypes.addressof(ptrs), 1 if on_dev else 0
     req.blinds, req.proof_out = bl.ctypes.data, ctypes.addressof(out)
+    ni = key.circuit.get("n_instance", 0)
+    inst = list(instance) if instance is not None else []
+    if len(inst) != ni:
+        raise MzkError(1, f"create_proof: {ni} instance columns expected, got {len(inst)}")
+    if ni:
+        icols = [np.ascontiguousarray(v, np.uint64).reshape(-1, 4) for v in inst]
+        iptrs = (ctypes.c_void_p * ni)(*[c.ctypes.data if c.shape[0] else None for c in icols])
+        ilen = np.array([c.shape[0] for c in icols], np.uint64)
+        keep.extend([icols, iptrs, ilen])
+        req.instance, req.instance_len = ctypes.addressof(iptrs), ilen.ctypes.data
     return req, keep, out
 
 
 def create_proofs(ctx, jobs, flags=0):
     """create_proof (proofs/src/plonk/prover.rs:432-473) for many proofs in
-    one call.  jobs: [(PlonkKey, advice columns, blinds)] where the advice
-    columns are host (n, 4) arrays or DeviceBuffers and blinds an (n_blinds, 4)
-    host array in the reference's draw order (include/mzk.h).  Returns the
-    proofs as bytes."""
+    one call.  jobs: [(PlonkKey, advice columns, blinds[, instance columns])]
+    where the advice columns are host (n, 4) arrays or DeviceBuffers, blinds an
+    (n_blinds, 4) host array in the reference's draw order (include/mzk.h) and
+    the instance columns host arrays of their values.  Returns the proofs as
+    bytes."""
     reqs = (ProofRequest * max(1, len(jobs)))()
     keep, outs = [], []
-    for i, (key, advice, blinds) in enumerate(jobs):
-        req, kp, out = _proof_request(key, advice, blinds)
+    for i, job in enumerate(jobs):
+        req, kp, out = _proof_request(*job)
         reqs[i] = req
         keep.append(kp)
         outs.append(out)

@@ -235,8 +235,8 @@ Fr4 l_i(const Domain* d, const Fr4& x, const Fr4& xn, int32_t i) {
 struct PlonkKey {
     const Domain* dom = nullptr;
     uint32_t k = 0, n = 0, u = 0, bf = 0, degree = 0, qdeg = 0, chunk = 0, n_sets = 0;
-    uint32_t n_advice = 0, n_fixed = 0, n_perm = 0;
-    std::vector<mzk_query> advice_queries, fixed_queries;
+    uint32_t n_advice = 0, n_fixed = 0, n_perm = 0, n_instance = 0;
+    std::vector<mzk_query> advice_queries, fixed_queries, instance_queries;
     uint32_t gate_fixed[5] = {}, gate_advice[3] = {};
     // custom gates as a flattened program (a validated copy), or the standard gate
     bool has_gates = false;
@@ -303,8 +303,10 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
     if (cs->n_perm_cols > kQMaxPermCols || (cs->n_perm_cols + cs->degree - 3) / (cs->degree - 2) > kQMaxSets)
         return fail("at most 16 permutation columns in at most 8 sets");
     if (cs->n_lookups > kMaxProofLookups) return fail("at most 4 lookups");
-    if ((cs->n_advice_queries && !cs->advice_queries) || (cs->n_fixed_queries && !cs->fixed_queries))
+    if ((cs->n_advice_queries && !cs->advice_queries) || (cs->n_fixed_queries && !cs->fixed_queries) ||
+        (cs->n_instance_queries && !cs->instance_queries))
         return fail("null query list");
+    if (cs->n_instance > kQMaxInstance) return fail("at most 4 instance columns");
     if ((cs->n_perm_cols && (!cs->perm_col_kind || !cs->perm_col_index)) || (cs->n_lookups && !cs->lookups))
         return fail("null column list");
     auto queried = [&](const mzk_query* q, uint32_t nq, uint32_t col) {
@@ -328,6 +330,14 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
             if (cs->fixed_queries[j].column == q.column && cs->fixed_queries[j].rotation == q.rotation)
                 return fail("duplicated fixed query");
     }
+    for (uint32_t i = 0; i < cs->n_instance_queries; i++) {
+        const mzk_query q = cs->instance_queries[i];
+        if (q.column >= cs->n_instance) return fail("instance query column out of range");
+        if (q.rotation <= -(int32_t)n || q.rotation >= (int32_t)n) return fail("rotation out of range");
+        for (uint32_t j = 0; j < i; j++)
+            if (cs->instance_queries[j].column == q.column && cs->instance_queries[j].rotation == q.rotation)
+                return fail("duplicated instance query");
+    }
     if (const mzk_flat_graph* g = cs->gates) {
         // every index the host evaluation at x uses is checked here; the
         // quotient checks the program again when it packs it
@@ -345,12 +355,16 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
             if (r.dst >= V || r.rot_idx >= g->n_rotations) return fail("gates: read index out of range");
             const int32_t rot = g->rotations[r.rot_idx];
             bool ok = false;
-            if (r.col_type == 0 || r.col_type == 1) {
-                const mzk_query* q = r.col_type == 0 ? cs->fixed_queries : cs->advice_queries;
-                const uint32_t nq = r.col_type == 0 ? cs->n_fixed_queries : cs->n_advice_queries;
+            if (r.col_type <= 2) {
+                const mzk_query* q = r.col_type == 0   ? cs->fixed_queries
+                                     : r.col_type == 1 ? cs->advice_queries
+                                                       : cs->instance_queries;
+                const uint32_t nq = r.col_type == 0   ? cs->n_fixed_queries
+                                    : r.col_type == 1 ? cs->n_advice_queries
+                                                      : cs->n_instance_queries;
                 for (uint32_t j = 0; j < nq; j++) ok = ok || (q[j].column == r.col_idx && q[j].rotation == rot);
             }
-            if (!ok) return fail("gates: a read is not a fixed or advice query of the circuit");
+            if (!ok) return fail("gates: a read is not a fixed, advice or instance query of the circuit");
         }
         for (uint32_t i = 0; i < g->n_ops; i++) {
             const mzk_flat_op& o = g->ops[i];
@@ -367,9 +381,10 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
     }
     for (uint32_t i = 0; i < cs->n_perm_cols; i++) {
         const uint32_t kind = cs->perm_col_kind[i], col = cs->perm_col_index[i];
-        if (kind > 1) return fail("permutation column kind must be 0 (advice) or 1 (fixed)");
-        if (kind == 0 ? !queried(cs->advice_queries, cs->n_advice_queries, col)
-                      : !queried(cs->fixed_queries, cs->n_fixed_queries, col))
+        if (kind > 2) return fail("permutation column kind must be 0 (advice), 1 (fixed) or 2 (instance)");
+        if (kind == 0   ? !queried(cs->advice_queries, cs->n_advice_queries, col)
+            : kind == 1 ? !queried(cs->fixed_queries, cs->n_fixed_queries, col)
+                        : !queried(cs->instance_queries, cs->n_instance_queries, col))
             return fail("a permutation column is not queried at rotation 0");
     }
     for (uint32_t i = 0; i < cs->n_lookups; i++) {
@@ -555,6 +570,8 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     key->n_fixed = cs->n_fixed;
     key->advice_queries.assign(cs->advice_queries, cs->advice_queries + cs->n_advice_queries);
     key->fixed_queries.assign(cs->fixed_queries, cs->fixed_queries + cs->n_fixed_queries);
+    key->n_instance = cs->n_instance;
+    key->instance_queries.assign(cs->instance_queries, cs->instance_queries + cs->n_instance_queries);
     std::memcpy(key->gate_fixed, cs->gate_fixed, sizeof(key->gate_fixed));
     std::memcpy(key->gate_advice, cs->gate_advice, sizeof(key->gate_advice));
     if (const mzk_flat_graph* g = cs->gates) {
@@ -998,6 +1015,7 @@ struct FsProof {
     host::Transcript tr;
     Fr4 theta, beta, gamma, trash, y, x, xn, x1, x2, x3, x4;
     std::vector<Fr*> adv_lag, adv_coeff, adv_ext, z_lag, z_delta, z_coeff, z_ext, q, fdiv;
+    std::vector<Fr*> inst_lag, inst_coeff, inst_ext;  // instance columns (zero past their values)
     // per lookup: multiplicities, helper, aggregator
     std::vector<Fr*> m_lag, m_delta, m_coeff, m_ext, h_lag, h_coeff, h_ext, Z_lag, Z_dd, Z_coeff, Z_ext;
     std::vector<uint32_t*> counts;
@@ -1008,7 +1026,7 @@ struct FsProof {
     // blinding offsets (elements of req->blinds)
     size_t off_mult = 0, off_perm = 0, off_logup = 0, off_quot = 0;
     // evaluations
-    std::vector<Fr4> ev_adv, ev_fix, ev_pc, ev_sets, ev_lk, q_x3;
+    std::vector<Fr4> ev_adv, ev_fix, ev_pc, ev_sets, ev_lk, ev_inst, q_x3;
 };
 
 size_t proof_scratch_elems(const PlonkKey* k) {
@@ -1016,8 +1034,8 @@ size_t proof_scratch_elems(const PlonkKey* k) {
     const size_t L = k->lookups.size(), O = k->open_sets.size();
     size_t counts = 0;
     for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8;
-    return A * (2 * n + E) + S * (3 * n + E) + L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) + k->qdeg * n +
-           (4 + 2 * O + 2) * n + k->n_blinds + counts;
+    return (A + k->n_instance) * (2 * n + E) + S * (3 * n + E) + L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) +
+           k->qdeg * n + (4 + 2 * O + 2) * n + k->n_blinds + counts;
 }
 
 Status eval_many(Context* ctx, const std::vector<EvalTask>& in, std::vector<Fr4>& results, cudaStream_t st) {
@@ -1143,6 +1161,11 @@ Fr4 identities_at_x(const FsProof& p) {
             if (k->fixed_queries[i].column == col && k->fixed_queries[i].rotation == 0) return p.ev_fix[i];
         return host::fr_zero();
     };
+    auto ins = [&](uint32_t col) {
+        for (size_t i = 0; i < k->instance_queries.size(); i++)
+            if (k->instance_queries[i].column == col && k->instance_queries[i].rotation == 0) return p.ev_inst[i];
+        return host::fr_zero();
+    };
     std::vector<Fr4> ids;
     if (k->has_gates) {
         // the flattened gates at x: each read is the evaluation of its query
@@ -1157,8 +1180,9 @@ Fr4 identities_at_x(const FsProof& p) {
         val[g.previous_value_idx] = host::fr_zero();
         for (uint32_t i = 0; i < g.n_reads; i++) {
             const mzk_column_read& r = g.reads[i];
-            const auto& qs = r.col_type == 0 ? k->fixed_queries : k->advice_queries;
-            const auto& ev = r.col_type == 0 ? p.ev_fix : p.ev_adv;
+            const auto& qs = r.col_type == 0 ? k->fixed_queries : r.col_type == 1 ? k->advice_queries
+                                                                                   : k->instance_queries;
+            const auto& ev = r.col_type == 0 ? p.ev_fix : r.col_type == 1 ? p.ev_adv : p.ev_inst;
             for (size_t j = 0; j < qs.size(); j++)
                 if (qs[j].column == r.col_idx && qs[j].rotation == g.rotations[r.rot_idx]) val[r.dst] = ev[j];
         }
@@ -1207,7 +1231,8 @@ Fr4 identities_at_x(const FsProof& p) {
             Fr4 left = z(s, 1), right = z(s, 0);
             Fr4 cur = fr_mul(fr_mul(p.beta, p.x), fr_pow_u64(delta, c0));
             for (uint32_t ci = c0; ci < c1; ci++) {
-                const Fr4 e = k->perm_kind[ci] == 0 ? adv(k->perm_index[ci]) : fix(k->perm_index[ci]);
+                const uint32_t kind = k->perm_kind[ci], col = k->perm_index[ci];
+                const Fr4 e = kind == 0 ? adv(col) : kind == 1 ? fix(col) : ins(col);
                 left = fr_mul(left, fr_add(fr_add(e, fr_mul(p.beta, p.ev_pc[ci])), p.gamma));
                 right = fr_mul(right, fr_add(fr_add(e, cur), p.gamma));
                 cur = fr_mul(cur, delta);
@@ -1282,6 +1307,21 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 set_error("create_proof: null advice column in request " + std::to_string(j));
                 return ERR_ARG;
             }
+        if (k->n_instance && (!reqs[j].instance || !reqs[j].instance_len)) {
+            set_error("create_proof: request " + std::to_string(j) + " has no instance columns");
+            return ERR_ARG;
+        }
+        for (uint32_t i = 0; i < k->n_instance; i++) {
+            if (reqs[j].instance_len[i] > k->u) {  // Error::InstanceTooLarge (prover.rs:500-502)
+                set_error("create_proof: request " + std::to_string(j) + ": instance column " + std::to_string(i) +
+                          " has more values than usable rows");
+                return ERR_ARG;
+            }
+            if (reqs[j].instance_len[i] && !reqs[j].instance[i]) {
+                set_error("create_proof: null instance column in request " + std::to_string(j));
+                return ERR_ARG;
+            }
+        }
     }
     MsmTable table{srs.srs, srs.srs_len, srs.table_c, srs.table_rows, srs.table_min_n};
     const MsmTable* tab = srs.table_c > 0 ? &table : nullptr;
@@ -1325,6 +1365,11 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             p.adv_coeff.push_back(take(n));
             p.adv_ext.push_back(take(E));
         }
+        for (uint32_t i = 0; i < k->n_instance; i++) {
+            p.inst_lag.push_back(take(n));
+            p.inst_coeff.push_back(take(n));
+            p.inst_ext.push_back(take(E));
+        }
         for (uint32_t s = 0; s < k->n_sets; s++) {
             p.z_lag.push_back(take(n));
             p.z_delta.push_back(take(n));
@@ -1356,6 +1401,22 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         MZK_CUDA_CHECK(cudaMemcpyAsync(p.d_blinds, reqs[j].blinds, k->n_blinds * sizeof(Fr), cudaMemcpyHostToDevice,
                                        st));
         p.tr.common_fr(k->repr);  // vk.hash_into (prover.rs:101)
+        // compute_instances (prover.rs:475-539): each instance column's length
+        // and values go into the transcript; its Lagrange form is the values
+        // padded with zeros
+        for (uint32_t i = 0; i < k->n_instance; i++) {
+            const uint64_t len = reqs[j].instance_len[i];
+            p.tr.common_fr(fr_from_u64(len));
+            for (uint64_t v = 0; v < len; v++) {
+                Fr4 x;
+                std::memcpy(x.l, reqs[j].instance[i] + 4 * v, 32);
+                p.tr.common_fr(x);
+            }
+            MZK_CUDA_CHECK(cudaMemsetAsync(p.inst_lag[i], 0, n * sizeof(Fr), st));
+            if (len)
+                MZK_CUDA_CHECK(cudaMemcpyAsync(p.inst_lag[i], reqs[j].instance[i], len * sizeof(Fr),
+                                               cudaMemcpyHostToDevice, st));
+        }
     }
     auto write_points = [&](FsProof& p, const uint64_t* res, size_t m) {
         for (size_t i = 0; i < m; i++) p.tr.write_point(res + 18 * i);
@@ -1443,8 +1504,10 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         if (k->n_sets) {
             std::vector<const uint64_t*> vals(k->n_perm), sig(k->n_perm);
             for (uint32_t c = 0; c < k->n_perm; c++) {
-                vals[c] = reinterpret_cast<const uint64_t*>(k->perm_kind[c] == 0 ? p.adv_lag[k->perm_index[c]]
-                                                                                  : k->fixed_lag[k->perm_index[c]]);
+                const uint32_t kind = k->perm_kind[c], col = k->perm_index[c];
+                vals[c] = reinterpret_cast<const uint64_t*>(kind == 0   ? p.adv_lag[col]
+                                                            : kind == 1 ? k->fixed_lag[col]
+                                                                        : p.inst_lag[col]);
                 sig[c] = reinterpret_cast<const uint64_t*>(k->perm_lag[c]);
             }
             std::vector<uint64_t*> zo(k->n_sets);
@@ -1513,6 +1576,11 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             co.push_back(p.adv_coeff[i]);
             ex.push_back(p.adv_ext[i]);
         }
+        for (uint32_t i = 0; i < k->n_instance; i++) {
+            lag.push_back(p.inst_lag[i]);
+            co.push_back(p.inst_coeff[i]);
+            ex.push_back(p.inst_ext[i]);
+        }
         for (uint32_t s = 0; s < k->n_sets; s++) {
             lag.push_back(p.z_lag[s]);
             co.push_back(p.z_coeff[s]);
@@ -1525,7 +1593,9 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         }
         MZK_TRY(ntt_sequence(ctx, d, lag.data(), co.data(), ex.data(), (int)lag.size(),
                              !(flags & MZK_PROVE_NO_GRAPHS), st));
-        std::vector<const uint64_t*> adv(k->n_advice), fixed(k->n_fixed), sig(k->n_perm), zs(k->n_sets);
+        std::vector<const uint64_t*> adv(k->n_advice), fixed(k->n_fixed), sig(k->n_perm), zs(k->n_sets),
+            inst(k->n_instance);
+        for (uint32_t i = 0; i < k->n_instance; i++) inst[i] = reinterpret_cast<const uint64_t*>(p.inst_ext[i]);
         for (uint32_t i = 0; i < k->n_advice; i++) adv[i] = reinterpret_cast<const uint64_t*>(p.adv_ext[i]);
         for (uint32_t i = 0; i < k->n_fixed; i++) fixed[i] = reinterpret_cast<const uint64_t*>(k->fixed_ext[i]);
         for (uint32_t i = 0; i < k->n_perm; i++) sig[i] = reinterpret_cast<const uint64_t*>(k->perm_ext[i]);
@@ -1541,6 +1611,8 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         std::memcpy(q.gate_fixed, k->gate_fixed, sizeof(q.gate_fixed));
         std::memcpy(q.gate_advice, k->gate_advice, sizeof(q.gate_advice));
         q.gates = k->has_gates ? &k->gates : nullptr;
+        q.instance = inst.data();
+        q.n_instance = k->n_instance;
         q.n_perm_cols = k->n_perm;
         q.perm_col_kind = k->perm_kind.data();
         q.perm_col_index = k->perm_index.data();
@@ -1596,6 +1668,9 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     phase_done(4);
     // ---- 5. evaluations, linearization, x1, x2 ----------------------------
     {
+        // instance evaluations are not in the transcript (no committed
+        // instances): only the self-check's identities at x use them
+        const bool with_instance = (flags & MZK_PROVE_SELF_CHECK) != 0;
         std::vector<EvalTask> tasks;
         for (auto& p : ps) {
             const PlonkKey* k = p.key;
@@ -1615,6 +1690,9 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 tasks.push_back(eval_task(p.Z_coeff[l], n, p.x));
                 tasks.push_back(eval_task(p.Z_coeff[l], n, fr_rot(d, p.x, 1)));
             }
+            if (with_instance)
+                for (auto& q : k->instance_queries)
+                    tasks.push_back(eval_task(p.inst_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
         }
         std::vector<Fr4> ev;
         MZK_TRY(eval_many(ctx, tasks, ev, st));
@@ -1631,6 +1709,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             grab(p.ev_pc, k->n_perm);
             grab(p.ev_sets, 3 * (size_t)k->n_sets);
             grab(p.ev_lk, 4 * k->lookups.size());
+            grab(p.ev_inst, with_instance ? k->instance_queries.size() : 0);
             // transcript order (write_evals_to_transcript, permutation / logup evaluate)
             for (auto& v : p.ev_adv) p.tr.write_fr(v);
             for (auto& v : p.ev_fix) p.tr.write_fr(v);

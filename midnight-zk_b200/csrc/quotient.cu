@@ -83,7 +83,9 @@ __global__ void __launch_bounds__(256) k_quotient(QuotientParams q) {
                 Fr right = ldfr(q.z[s], idx);
                 const uint32_t end = min(col + q.chunk_len, q.n_perm_cols);
                 for (uint32_t j = col; j < end; j++) {
-                    const Fr* colp = q.perm_kind[j] == 0 ? q.advice[q.perm_index[j]] : q.fixed[q.perm_index[j]];
+                    const Fr* colp = q.perm_kind[j] == 0   ? q.advice[q.perm_index[j]]
+                                     : q.perm_kind[j] == 1 ? q.fixed[q.perm_index[j]]
+                                                           : q.instance[q.perm_index[j]];
                     const Fr val = ldfr(colp, idx);
                     const Fr base = fr_add(val, q.gamma);
                     left = fr_mul(left, fr_add(base, fr_mul(q.beta, ldfr(q.sigma[j], idx))));
@@ -363,6 +365,11 @@ Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_de
     std::memset(&q, 0, sizeof(q));
     for (uint32_t i = 0; i < desc->n_advice; i++) q.advice[i] = reinterpret_cast<const Fr*>(desc->advice[i]);
     for (uint32_t i = 0; i < desc->n_fixed; i++) q.fixed[i] = reinterpret_cast<const Fr*>(desc->fixed[i]);
+    if (desc->n_instance > kQMaxInstance || (desc->n_instance && !desc->instance)) {
+        set_error("quotient: at most 4 instance columns");
+        return ERR_ARG;
+    }
+    for (uint32_t i = 0; i < desc->n_instance; i++) q.instance[i] = reinterpret_cast<const Fr*>(desc->instance[i]);
     const bool tail = desc->n_lookups || desc->n_trash;
     if (tail && desc->has_lookup) {
         set_error("quotient: give either the built-in lookup (has_lookup) or lookup / trash programs");
@@ -398,7 +405,7 @@ Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_de
     q.n_perm_cols = desc->n_perm_cols;
     for (uint32_t j = 0; j < desc->n_perm_cols; j++) {
         const uint32_t kind = desc->perm_col_kind[j], idx = desc->perm_col_index[j];
-        if (kind > 1 || idx >= (kind == 0 ? desc->n_advice : desc->n_fixed)) {
+        if (kind > 2 || idx >= (kind == 0 ? desc->n_advice : kind == 1 ? desc->n_fixed : desc->n_instance)) {
             set_error("quotient: permutation column out of range");
             return ERR_ARG;
         }

@@ -16,6 +16,7 @@ constexpr uint32_t kQMaxAdvice = 16, kQMaxFixed = 16, kQMaxPermCols = 16, kQMaxS
 struct QuotientParams {
     const Fr* advice[kQMaxAdvice];
     const Fr* fixed[kQMaxFixed];
+    const Fr* instance[4];  // kQMaxInstance: instance columns a permutation column may name
     const Fr* sigma[kQMaxPermCols];
     const Fr* z[kQMaxSets];
     const Fr *lh, *lz, *lm, *l0, *l_last, *l_active;

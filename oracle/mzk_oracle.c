@@ -1529,14 +1529,14 @@ static void quotient_eval(const or_quotient_desc *d, const or_domain *dom, int d
                 uint32_t end = col + d->chunk_len;
                 if (end > d->n_perm_cols) end = d->n_perm_cols;
                 for (uint32_t j = col; j < end; j++) {
-                    const u64 *val = (d->perm_col_kind[j] == 0 ? d->advice : d->fixed)[d->perm_col_index[j]] + 4 * idx;
+                    const u64 *val = (d->perm_col_kind[j] == 0 ? d->advice : d->perm_col_kind[j] == 1 ? d->fixed : d->instance)[d->perm_col_index[j]] + 4 * idx;
                     fr_mul(t, d->beta, d->perm_sigma[j] + 4 * idx);
                     fr_add(t, t, val);
                     fr_add(t, t, d->gamma);
                     fr_mul(left, left, t);
                 }
                 for (uint32_t j = col; j < end; j++) {
-                    const u64 *val = (d->perm_col_kind[j] == 0 ? d->advice : d->fixed)[d->perm_col_index[j]] + 4 * idx;
+                    const u64 *val = (d->perm_col_kind[j] == 0 ? d->advice : d->perm_col_kind[j] == 1 ? d->fixed : d->instance)[d->perm_col_index[j]] + 4 * idx;
                     fr_add(t, val, cur);
                     fr_add(t, t, d->gamma);
                     fr_mul(right, right, t);

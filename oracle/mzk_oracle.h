@@ -139,7 +139,7 @@ typedef struct {
     uint32_t gate_fixed[5];   /* q_l, q_r, q_m, q_o, q_c */
     uint32_t gate_advice[3];  /* a, b, c */
     uint32_t n_perm_cols;
-    const uint32_t *perm_col_kind;   /* 0 advice, 1 fixed */
+    const uint32_t *perm_col_kind;   /* 0 advice, 1 fixed, 2 instance */
     const uint32_t *perm_col_index;
     const uint64_t *const *perm_sigma; /* n_perm_cols cosets */
     uint32_t n_perm_sets;
@@ -153,6 +153,7 @@ typedef struct {
     const uint64_t *l0, *l_last, *l_active;
     uint64_t y[4], beta[4], gamma[4], theta[4];
     uint64_t extended_omega[4], g_coset[4];
+    const uint64_t *const *instance; uint32_t n_instance; /* permutation columns of kind 2 */
 } or_quotient_desc;
 /* out[i] = numerator nu at extended row i; divide != 0 multiplies by the
  * inverted vanishing polynomial (divide_by_vanishing_poly, domain.rs:361). */

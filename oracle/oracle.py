@@ -126,6 +126,7 @@ class QuotientDesc(ctypes.Structure):
     ("l0", ctypes.c_void_p), ("l_last", ctypes.c_void_p), ("l_active", ctypes.c_void_p),
     ("y", ctypes.c_uint64 * 4), ("beta", ctypes.c_uint64 * 4), ("gamma", ctypes.c_uint64 * 4),
     ("theta", ctypes.c_uint64 * 4), ("extended_omega", ctypes.c_uint64 * 4), ("g_coset", ctypes.c_uint64 * 4),
+    ("instance", ctypes.POINTER(ctypes.c_void_p)), ("n_instance", ctypes.c_uint32),
 ]
 
 

@@ -407,6 +407,44 @@ def generic_instance(k, seed, table_bits=16, copy_fraction=0.10, two_lookups=Fal
     return fixed, mapping, [a, b, cc_col, d]
 
 
+def instance_circuit(k):
+    """generic_circuit with one instance column (public inputs): a third gate
+    q5 (c - inst) over a seventh fixed column q5, and the instance column as a
+    fifth permutation column whose first rows are copies of c's."""
+    c = generic_circuit(k)
+    g = dict(c["gates"])
+    g["reads"] = g["reads"] + [(0, 6, 0, 27), (2, 0, 0, 28)]
+    g["ops"] = g["ops"] + [(1, 29, 13, 28, 0), (2, 30, 27, 29, 0), (6, 31, 26, 5, 30)]
+    g["values_len"], g["result_idx"] = 32, 31
+    c.update({"gates": g, "n_fixed": 7, "fixed_queries": [(i, 0) for i in range(7)], "n_instance": 1,
+              "instance_queries": [(0, 0)], "perm_cols": c["perm_cols"] + [(2, 0)]})
+    return c
+
+
+INSTANCE_ROWS = 3
+
+
+def instance_instance(k, seed):
+    """generic_instance's columns and witness with q5 = 1 on the first
+    INSTANCE_ROWS rows, the public values inst_i = c_i there, and copy
+    constraints between each instance cell and its c cell.  Returns
+    (fixed, mapping, advice, instances)."""
+    fixed, mapping, adv = generic_instance(k, seed)
+    n = 1 << k
+    q5 = np.zeros((n, 4), np.uint64)
+    q5[:INSTANCE_ROWS] = O.fr_const(0)
+    fixed = fixed + [q5]
+    m = np.zeros((5, n, 2), np.uint32)
+    m[:4] = mapping
+    m[4, :, 0] = 4
+    m[4, :, 1] = np.arange(n, dtype=np.uint32)
+    for r in range(INSTANCE_ROWS):
+        m[4, r] = (2, r)
+        m[2, r] = (4, r)
+    inst = [adv[2][:INSTANCE_ROWS].copy()]
+    return fixed, m, adv, inst
+
+
 def generic2_circuit(k):
     """generic_circuit with its second lookup (d into the table of squares)."""
     return generic_circuit(k, two_lookups=True)
@@ -597,6 +635,18 @@ def l_i_range(key, x, xn, rotations):
     return out
 
 
+def instance_evals(key, instances, x, xn):
+    """The instance query evaluations of the verifier (verifier.rs:205-242):
+    for the query (column, rotation), sum_j value_j l_{j - rotation}(x),
+    the Lagrange basis of the rows the values occupy."""
+    out = []
+    for col, rot in key.circuit.get("instance_queries", []):
+        vals = [to_int(v) for v in np.ascontiguousarray(instances[col], np.uint64).reshape(-1, 4)]
+        ls = l_i_range(key, x, xn, range(-rot, len(vals) - rot))
+        out.append(sum(v * li for v, li in zip(vals, ls)) % R)
+    return out
+
+
 def rotate(key, x, rot):
     """EvaluationDomain::rotate_omega (domain.rs:449-457)."""
     return x * (pow(key.omega, rot, R) if rot >= 0 else pow(key.omega_inv, -rot, R)) % R
@@ -613,13 +663,17 @@ def identities(key, ev, ch):
     bf = key.bf
     l_evals = l_i_range(key, x, xn, range(-(bf + 1), 1))
     l_last, l_blind, l_0 = l_evals[0], sum(l_evals[1:1 + bf]) % R, l_evals[1 + bf]
-    adv, fix = ev["advice"], ev["fixed"]
+    adv, fix, ins = ev["advice"], ev["fixed"], ev.get("instance", [])
     aq = lambda col: adv[query_index(c["advice_queries"], col)]
     fq = lambda col: fix[query_index(c["fixed_queries"], col)]
+    iq = lambda col: ins[query_index(c.get("instance_queries", []), col)]
+    col_eval = lambda kind, col: (aq, fq, iq)[kind](col)
     if c.get("gates") is not None:
         def read(col_type, col, rot):
             if col_type == 0:
                 return fix[query_index(c["fixed_queries"], col, rot)]
+            if col_type == 2:
+                return ins[query_index(c.get("instance_queries", []), col, rot)]
             return adv[query_index(c["advice_queries"], col, rot)]
         out = [program_at(c["gates"], read, ch)]
     else:
@@ -641,12 +695,12 @@ def identities(key, ev, ch):
             sig = ev["perm_common"][si * chunk:(si + 1) * chunk]
             left = s[1]
             for (kind, ci), se in zip(cols, sig):
-                e = aq(ci) if kind == 0 else fq(ci)
+                e = col_eval(kind, ci)
                 left = left * (e + beta * se + gamma) % R
             right = s[0]
             cur = beta * x % R * pow(dlt, si * chunk, R) % R
             for kind, ci in cols:
-                e = aq(ci) if kind == 0 else fq(ci)
+                e = col_eval(kind, ci)
                 right = right * (e + cur + gamma) % R
                 cur = cur * dlt % R
             out.append((left - right) * (1 - (l_last + l_blind)) % R)
@@ -722,12 +776,42 @@ def intermediate_sets(queries):
 
 
 # ---------------------------------------------------------------- prover --
-def create_proof(key, advice, blinds):
+def instance_columns(key, instances):
+    """compute_instances (prover.rs:475-539) without committed instances:
+    each column's values zero-padded to n (Lagrange form); more values than
+    usable rows is Error::InstanceTooLarge."""
+    c, n = key.circuit, key.n
+    instances = list(instances or [])
+    if len(instances) != c.get("n_instance", 0):
+        raise ValueError("wrong number of instance columns")
+    cols = []
+    for vals in instances:
+        vals = np.ascontiguousarray(vals, np.uint64).reshape(-1, 4)
+        if vals.shape[0] > key.u:
+            raise ValueError("instance too large")
+        col = np.zeros((n, 4), np.uint64)
+        col[:vals.shape[0]] = vals
+        cols.append(col)
+    return instances, cols
+
+
+def absorb_instances(tr, instances):
+    """The transcript part of compute_instances: each column's length, then
+    its values (common, prover.rs:503-512; verifier.rs:61-66)."""
+    for vals in instances:
+        vals = np.ascontiguousarray(vals, np.uint64).reshape(-1, 4)
+        tr.common_fr(vals.shape[0])
+        for v in vals:
+            tr.common_fr(to_int(v))
+
+
+def create_proof(key, advice, blinds, instances=None):
     """create_proof (plonk/prover.rs:432-473): compute_trace, then
     finalise_proof with the KZG multi_open (kzg/mod.rs:110-289).  advice:
     Lagrange values of every advice column (rows at and after the usable
     rows are replaced by blinding values); blinds: integers in the draw order
-    of the module doc.  Returns the proof bytes."""
+    of the module doc; instances: the values of each instance column.
+    Returns the proof bytes."""
     c, dom, srs = key.circuit, key.dom, key.srs
     n, u, bf, qdeg = key.n, key.u, key.bf, key.qdeg
     blinds = list(blinds)
@@ -735,8 +819,10 @@ def create_proof(key, advice, blinds):
         raise ValueError("wrong number of blinding values")
     bl = iter(blinds)
     take = lambda m: [next(bl) for _ in range(m)]
+    instances, inst = instance_columns(key, instances)
     tr = Transcript()
     tr.common_fr(key.repr)                                    # vk.hash_into (prover.rs:101)
+    absorb_instances(tr, instances)
     # parse_advices (prover.rs:541-632)
     adv = []
     for col in advice:
@@ -759,7 +845,7 @@ def create_proof(key, advice, blinds):
     perm_bl = [take(bf) for _ in range(S)]
     log_bl = [take(bf) for _ in c["lookups"]]
     # permutation products (permutation/prover.rs:81-255) and logup helper / aggregator
-    pvals = [adv[ci] if kind == 0 else key.fixed_values[ci] for kind, ci in c["perm_cols"]]
+    pvals = [(adv, key.fixed_values, inst)[kind][ci] for kind, ci in c["perm_cols"]]
     zs = O.permutation_z(pvals, key.perm_values, c["degree"] - 2, c["k"], to_mont(key.omega), to_mont(beta),
                          to_mont(gamma), bf, np.stack([np.stack([to_mont(v) for v in b]) for b in perm_bl]))
     hs, Zs = [], []
@@ -783,8 +869,10 @@ def create_proof(key, advice, blinds):
     h_c = [dom.lagrange_to_coeff(h) for h in hs]
     Z_c = [dom.lagrange_to_coeff(Z) for Z in Zs]
     ext = lambda p: dom.coeff_to_extended(p)
+    inst_c = [dom.lagrange_to_coeff(col) for col in inst]
     hpoly = quotient(key, [ext(p) for p in adv_c], [ext(p) for p in z_c], [ext(p) for p in m_c],
-                     [ext(p) for p in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta, trash=trash)
+                     [ext(p) for p in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta, trash=trash,
+                     inst_e=[ext(p) for p in inst_c])
     hcoeff = dom.extended_to_coeff(hpoly)[: (n - 1) * qdeg]
     limbs = [np.concatenate([hcoeff[i * (n - 1):(i + 1) * (n - 1)], np.zeros((1, 4), np.uint64)]) for i in range(qdeg)]
     for i, t in enumerate(take(qdeg - 1), start=1):         # blind_quotient_limbs (prover.rs:774-785)
@@ -845,7 +933,7 @@ def create_proof(key, advice, blinds):
     return bytes(tr.proof)
 
 
-def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None, trash=0):
+def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None, trash=0, inst_e=()):
     """compute_nu_poly + divide_by_vanishing_poly (prover.rs:634-715) through
     the C oracle's evaluate_numerator restatement."""
     c, dom = key.circuit, key.dom
@@ -884,10 +972,12 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
         getattr(d, name)[:] = [int(t) for t in to_mont(v)]
     d.extended_omega[:] = [int(t) for t in dom.get(2)]
     d.g_coset[:] = [int(t) for t in dom.get(3)]
-    keep.extend([adv_e, z_e, m_e, h_e, Z_e])
+    inst_e = list(inst_e)
+    d.instance, d.n_instance = parr(inst_e), len(inst_e)
+    keep.extend([adv_e, z_e, m_e, h_e, Z_e, inst_e])
     gate_values = None
     if c.get("gates") is not None:
-        gate_values = O.flat_gates_eval(c["gates"], key.fixed_cosets, adv_e, [], c["k"], dom.extended_k,
+        gate_values = O.flat_gates_eval(c["gates"], key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k,
                                         to_mont(beta), to_mont(theta), to_mont(trash), to_mont(y))
     if len(c["lookups"]) <= 1:
         return dom.quotient_eval(d, True, threads, gate_values)
@@ -898,7 +988,7 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     lks = [{"programs": [g], "outputs": [outs], "helpers": [h_e[li]], "aggregator": Z_e[li],
             "multiplicities": m_e[li]}
            for li, (g, outs) in enumerate(lookup_program(lk) for lk in c["lookups"])]
-    v = O.flat_tail_eval(v, key.fixed_cosets, adv_e, [], c["k"], dom.extended_k, to_mont(beta), to_mont(theta),
+    v = O.flat_tail_eval(v, key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k, to_mont(beta), to_mont(theta),
                          to_mont(trash), to_mont(y), key.l0, key.l_last, key.l_active, lookups=lks)
     return dom.divide_by_vanishing_poly(v)
 
@@ -957,26 +1047,30 @@ def multi_open(key, tr, queries):
 
 
 # --------------------------------------------------------------- verifier --
-def verify(key, proof, s_trapdoor):
+def verify(key, proof, s_trapdoor, instances=None):
     """prepare (plonk/verifier.rs:371-407: parse_trace, then
     verify_algebraic_constraints) and KZGCommitmentScheme::multi_prepare
     (kzg/mod.rs:291-491), finished by DualMSM::check (kzg/msm.rs:294-310)
     with the pairing e(pi, [s]G2) = e(C - vG + x3 pi, G2) replaced by the
     equivalent G1 check [s]pi = C - vG + x3 pi for the test setup's known s.
+    The instance columns' values are absorbed as the prover absorbs them
+    and their evaluations computed from the values (verifier.rs:205-242).
     Returns True or False; a malformed proof is False."""
     try:
-        return _verify(key, proof, s_trapdoor)
+        return _verify(key, proof, s_trapdoor, instances)
     except ValueError:
         return False
 
 
-def _verify(key, proof, s):
+def _verify(key, proof, s, instances=None):
     c = key.circuit
     n, bf, qdeg = key.n, key.bf, key.qdeg
     S = n_perm_sets(c)
     L = len(c["lookups"])
+    instances, _ = instance_columns(key, instances)
     tr = Transcript(proof)
     tr.common_fr(key.repr)
+    absorb_instances(tr, instances)
     adv_coms = [tr.read_point() for _ in range(c["n_advice"])]
     theta = tr.squeeze()
     m_coms = [tr.read_point() for _ in range(L)]
@@ -999,6 +1093,7 @@ def _verify(key, proof, s):
         sets.append([z0, z1, tr.read_fr() if si < S - 1 else None])
     ev["perm_sets"] = sets
     ev["lookups"] = [tuple(tr.read_fr() for _ in range(4)) for _ in range(L)]
+    ev["instance"] = instance_evals(key, instances, x, xn)
     ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta, "trash": trash, "y": y}
     const = horner(identities(key, ev, ch), y)
     # compute_linearization_commitment (linearization/verifier.rs:27-78)

@@ -16,7 +16,8 @@ PINNED = b"config-3 circuit: standard gate, copy cycles, range lookup"
 
 
 SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.generic_circuit, OP.generic_instance),
-          "generic2": (OP.generic2_circuit, OP.generic2_instance)}
+          "generic2": (OP.generic2_circuit, OP.generic2_instance),
+          "instance": (OP.instance_circuit, OP.instance_instance)}
 
 
 class Circuit:
@@ -25,14 +26,17 @@ class Circuit:
         k's g | lagrange | delta | double delta at the offsets; otherwise
         this circuit gets its own.  shape: "config3" (the single-proof
         configuration), "generic" (two gates with a rotation, two
-        permutation sets) or "generic2" (generic with a second lookup,
-        without a selector)."""
+        permutation sets), "generic2" (generic with a second lookup,
+        without a selector) or "instance" (generic with an instance column
+        read by a third gate and copied from c)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)
         c["blinding_factors"] = OP.blinding_factors(c)
         self.circuit = c
-        self.fixed, self.mapping, self.advice = make_instance(k, seed)
+        made = make_instance(k, seed)
+        self.fixed, self.mapping, self.advice = made[:3]
+        self.instances = made[3] if len(made) > 3 else None
         self.dom = mzk.EvaluationDomain(ctx, c["degree"], k)
         n = self.n = self.dom.n
         if srs is None:
@@ -55,8 +59,9 @@ class Circuit:
     def blinds(self, seed):
         return O.rand_fr(5000 + seed, self.key.n_blinds)
 
-    def oracle_proof(self, advice, blinds):
-        return OP.create_proof(self.okey, advice, [OP.to_int(v) for v in blinds])
+    def oracle_proof(self, advice, blinds, instances=None):
+        return OP.create_proof(self.okey, advice, [OP.to_int(v) for v in blinds],
+                               self.instances if instances is None else instances)
 
-    def verify(self, proof):
-        return OP.verify(self.okey, proof, OP.to_int(self.s))
+    def verify(self, proof, instances=None):
+        return OP.verify(self.okey, proof, OP.to_int(self.s), self.instances if instances is None else instances)

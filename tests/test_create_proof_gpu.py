@@ -218,6 +218,38 @@ def test_two_lookup_circuit_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, bad, bl)])
 
 
+@pytest.mark.parametrize("k", [5, 9])
+def test_instance_circuit_proof_equals_oracle(ctx, k):
+    """An instance column (public inputs) read by a gate and copied into an
+    advice column by the permutation: the values go into the transcript after
+    the VK hash, the device transcript equals the oracle's and verifies with
+    those public inputs, alone, in a batch and through the proving service;
+    other public inputs fail the self-check, and more values than usable rows
+    are refused."""
+    c = Circuit(ctx, k, seed=k + 80, shape="instance")
+    assert c.circuit["n_instance"] == 1 and c.instances is not None
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl, c.instances)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    both = mzk.create_proofs(ctx, [(c.key, c.advice, bl, c.instances), (c.key, c.advice, c.blinds(6), c.instances)])
+    assert both[0] == proof and c.verify(both[1])
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = srv.submit(c.key, c.advice, c.blinds(7), c.instances)
+    assert c.verify(srv.wait(t)[0])
+    srv.close()
+    other = [c.instances[0].copy()]
+    other[0][0] = OP.to_mont(OP.to_int(other[0][0]) + 1)
+    assert not c.verify(proof, other)
+    with pytest.raises(mzk.MzkError, match="does not satisfy"):
+        mzk.create_proofs(ctx, [(c.key, c.advice, bl, other)], flags=mzk.PROVE_SELF_CHECK)
+    with pytest.raises(mzk.MzkError, match="usable rows"):
+        too_many = np.tile(c.instances[0][:1], (c.n - c.circuit["blinding_factors"], 1))   # usable rows + 1
+        mzk.create_proofs(ctx, [(c.key, c.advice, bl, [too_many])])
+    with pytest.raises(mzk.MzkError):
+        mzk.create_proofs(ctx, [(c.key, c.advice, bl)])                # the instance column is missing
+
+
 def test_key_files_equal_oracle_and_read_back(ctx, k5):
     """VerifyingKey / ProvingKey files in the three SerdeFormats equal the
     oracle's bytes; a key read from a PK file has the same transcript_repr and

@@ -148,6 +148,31 @@ def test_two_lookup_circuit_proofs_verify():
         OP.create_proof(key, wrong, bl)
 
 
+def test_instance_circuit_proofs_verify():
+    """An instance column (public inputs): its values absorbed after the VK
+    hash (compute_instances), read by a gate and copied into c by the
+    permutation; the verifier evaluates it from the values.  The proof
+    verifies with its public inputs and not with others; too many values are
+    refused (Error::InstanceTooLarge)."""
+    k = 5
+    c = OP.instance_circuit(k)
+    fixed, mapping, adv, inst = OP.instance_instance(k, 12)
+    s = O.rand_fr(59, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"instance")
+    assert OP.n_perm_sets(c) == 2 and len(c["perm_cols"]) == 5
+    bl = [OP.to_int(v) for v in O.rand_fr(69, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl, inst)
+    assert OP.verify(key, proof, OP.to_int(s), inst)
+    other = [inst[0].copy()]
+    other[0][1] = OP.to_mont(OP.to_int(other[0][1]) + 1)
+    assert not OP.verify(key, proof, OP.to_int(s), other)
+    # a witness whose c disagrees with the public input fails the gate and the copy
+    assert not OP.verify(key, OP.create_proof(key, adv, bl, other), OP.to_int(s), other)
+    with pytest.raises(ValueError):
+        OP.create_proof(key, adv, bl, [np.tile(O.fr_const(0), (key.u + 1, 1))])
+
+
 def test_generic_circuit_proofs_verify():
     """Another circuit shape: two gates as one flattened program (with a(wX)),
     four permutation columns in two sets (z of the first set opened at
