@@ -372,8 +372,10 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumulate(const Affine* __r
     uint32_t nxt_hi = __ldg(offsets + k + 2);
     Xyzz acc;
     xyzz_set_inf(acc);
-    // the next entry's base is loaded one iteration ahead to hide the gather latency
+    // the next entry's base is loaded one iteration ahead, and the entry after
+    // it (its index) two ahead, to hide the gather latency
     uint32_t ent = __ldg(sorted + s);
+    uint32_t ent2 = s + 1 < e ? __ldg(sorted + s + 1) : 0u;
     Affine nxt = load_affine(bases, ent & 0x7fffffffu);
     for (uint32_t j = s; j < e; j++) {
         if (j == seg_hi) {
@@ -392,8 +394,9 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumulate(const Affine* __r
         Affine p = nxt;
         const uint32_t cur = ent;
         if (j + 1 < e) {
-            ent = __ldg(sorted + j + 1);
+            ent = ent2;
             nxt = load_affine(bases, ent & 0x7fffffffu);
+            if (j + 2 < e) ent2 = __ldg(sorted + j + 2);
         }
         if (aff_is_inf(p)) continue;
         p.y = fp_select((cur >> 31) != 0, fp_neg(p.y), p.y);
