@@ -428,7 +428,12 @@ typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } m
  * committed-instances feature: every proof's instance values are absorbed
  * into its transcript, compute_instances, prover.rs:475-539; gates may read
  * them, `col_type` 2, at their queried rotations, and permutation columns of
- * kind 2 are instance columns), no trashcans or simple selectors. */
+ * kind 2 are instance columns), at most 4 trashcans (trash/prover.rs: each an
+ * mzk_trash_arg whose program compresses the constraint expressions with the
+ * trash challenge, reading only queried columns, and whose selector is a
+ * fixed column queried at rotation 0; its `trash` pointer is not used here:
+ * the prover computes, commits, evaluates and opens the trash column), no
+ * simple selectors. */
 typedef struct {
     uint32_t degree;                   /* cs.degree() (plonk/circuit.rs:2174-2199), 3..9 */
     uint32_t blinding_factors;         /* cs.blinding_factors() (circuit.rs:2203-2245) */
@@ -443,6 +448,7 @@ typedef struct {
     const mzk_lookup_shape *lookups;
     uint32_t n_instance;               /* instance columns (0..4) */
     const mzk_query *instance_queries; uint32_t n_instance_queries;
+    uint32_t n_trash; const mzk_trash_arg *trash;
 } mzk_circuit_desc;
 /* ParamsKZG's bases (params.rs:83-93) inside one DEVICE G1Affine buffer;
  * table_c > 0: srs is row 0 of a window table of that width and table_rows

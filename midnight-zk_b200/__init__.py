@@ -920,7 +920,7 @@ class CircuitDesc(ctypes.Structure):
                 ("n_perm_cols", ctypes.c_uint32), ("perm_col_kind", ctypes.c_void_p),
                 ("perm_col_index", ctypes.c_void_p), ("n_lookups", ctypes.c_uint32), ("lookups", ctypes.c_void_p),
                 ("n_instance", ctypes.c_uint32), ("instance_queries", ctypes.c_void_p),
-                ("n_instance_queries", ctypes.c_uint32)]
+                ("n_instance_queries", ctypes.c_uint32), ("n_trash", ctypes.c_uint32), ("trash", ctypes.c_void_p)]
 
 
 class SrsDesc(ctypes.Structure):
@@ -1017,7 +1017,9 @@ class PlonkKey:
     advice_queries / fixed_queries [(column, rotation)], gate_fixed (5),
     gate_advice (3), perm_cols [(kind 0 advice | 1 fixed | 2 instance,
     column)], lookups [{"input", "table", "selector" (None: constant one)}],
-    n_instance and instance_queries [(column, rotation)] (optional).  fixed_values:
+    n_instance and instance_queries [(column, rotation)] (optional),
+    trashcans [{"program": flattened program, "selector": fixed column}]
+    (optional).  fixed_values:
     host (n, 4) arrays; mapping: (n_perm_cols, n, 2) uint32 or None; srs:
     an SrsDesc.  The domain and the SRS buffer must outlive the key."""
 
@@ -1061,6 +1063,19 @@ class PlonkKey:
         iq = circuit.get("instance_queries", [])
         cs.instance_queries = arr(Query, [Query(c, r) for c, r in iq])
         cs.n_instance_queries = len(iq)
+        tcs = circuit.get("trashcans", [])
+        if tcs:
+            targs = (TrashArg * len(tcs))()
+            for i, tc in enumerate(tcs):
+                g = tc["program"]
+                fg = g if isinstance(g, FlatGraph) else build_flat_graph(
+                    g["constants"], g["rotations"], g["reads"], g["ops"], g["values_len"], g["beta_idx"],
+                    g["theta_idx"], g["trash_challenge_idx"], g["y_idx"], g["previous_value_idx"], g["result_idx"])
+                keep.append(fg)
+                targs[i].program = fg
+                targs[i].selector_fixed = tc["selector"]
+            keep.append(targs)
+            cs.n_trash, cs.trash = len(tcs), ctypes.addressof(targs)
         pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
         h = _vp()
         if pk_bytes is not None:

@@ -60,6 +60,7 @@ namespace {
 
 constexpr uint32_t kThreads = 256;
 constexpr uint32_t kMaxProofLookups = 4;  // lookups of one circuit in create_proof
+constexpr uint32_t kMaxProofTrash = 4;    // trashcans of one circuit in create_proof
 
 inline Fr to_dev(const Fr4& a) {
     Fr r;
@@ -264,6 +265,16 @@ struct PlonkKey {
     std::vector<mzk_flat_op> lk_ops;
     std::vector<mzk_flat_graph> lk_programs;
     std::vector<uint32_t> lk_outputs;
+    // trashcans (trash/prover.rs): a validated copy of each program and its selector
+    struct Trash {
+        std::vector<uint64_t> consts;
+        std::vector<int32_t> rots;
+        std::vector<mzk_column_read> reads;
+        std::vector<mzk_flat_op> ops;
+        mzk_flat_graph program = {};
+        uint32_t selector = 0;
+    };
+    std::vector<Trash> trash;
     // device
     void* mem = nullptr;
     std::vector<Fr*> fixed_lag, fixed_coeff, fixed_ext, perm_lag, perm_coeff, perm_ext;
@@ -274,7 +285,7 @@ struct PlonkKey {
     Fr4 repr = {};
     // multi-open layout: polynomials (kind, index) and point sets sorted by
     // (size, first appearance), each with its polynomials and rotations
-    enum PolyKind { P_ADVICE = 0, P_PERM_Z, P_M, P_H, P_AGG, P_FIXED, P_PERM_FIXED, P_LIN };
+    enum PolyKind { P_ADVICE = 0, P_PERM_Z, P_M, P_H, P_AGG, P_FIXED, P_PERM_FIXED, P_LIN, P_TRASH };
     struct OpenSet {
         std::vector<std::pair<int, uint32_t>> polys;
         std::vector<int32_t> rots;
@@ -338,21 +349,21 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
             if (cs->instance_queries[j].column == q.column && cs->instance_queries[j].rotation == q.rotation)
                 return fail("duplicated instance query");
     }
-    if (const mzk_flat_graph* g = cs->gates) {
-        // every index the host evaluation at x uses is checked here; the
-        // quotient checks the program again when it packs it
+    // every index the host evaluation of a program at x uses is checked here;
+    // the quotient checks the program again when it packs it
+    auto check_program = [&](const mzk_flat_graph* g, const std::string& what) -> Status {
         const uint32_t V = g->values_len;
         if (V == 0 || V > kFlatMaxValues || g->n_constants > V || g->n_rotations > kFlatMaxRotations)
-            return fail("gates: bad values_len, constant count or rotation count");
+            return fail(what + ": bad values_len, constant count or rotation count");
         if ((g->n_constants && !g->constants) || (g->n_rotations && !g->rotations) || (g->n_reads && !g->reads) ||
             (g->n_ops && !g->ops))
-            return fail("gates: null array");
+            return fail(what + ": null array");
         for (uint32_t idx : {g->beta_idx, g->theta_idx, g->trash_challenge_idx, g->y_idx, g->previous_value_idx,
                              g->result_idx})
-            if (idx >= V) return fail("gates: slot index out of range");
+            if (idx >= V) return fail(what + ": slot index out of range");
         for (uint32_t i = 0; i < g->n_reads; i++) {
             const mzk_column_read& r = g->reads[i];
-            if (r.dst >= V || r.rot_idx >= g->n_rotations) return fail("gates: read index out of range");
+            if (r.dst >= V || r.rot_idx >= g->n_rotations) return fail(what + ": read index out of range");
             const int32_t rot = g->rotations[r.rot_idx];
             bool ok = false;
             if (r.col_type <= 2) {
@@ -364,13 +375,23 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
                                                       : cs->n_instance_queries;
                 for (uint32_t j = 0; j < nq; j++) ok = ok || (q[j].column == r.col_idx && q[j].rotation == rot);
             }
-            if (!ok) return fail("gates: a read is not a fixed, advice or instance query of the circuit");
+            if (!ok) return fail(what + ": a read is not a fixed, advice or instance query of the circuit");
         }
         for (uint32_t i = 0; i < g->n_ops; i++) {
             const mzk_flat_op& o = g->ops[i];
             if (o.kind > MZK_FLAT_MULADD || o.dst >= V || o.a >= V || o.b >= V || o.c >= V)
-                return fail("gates: op out of range");
+                return fail(what + ": op out of range");
         }
+        return OK;
+    };
+    if (cs->n_trash > kMaxProofTrash || (cs->n_trash && !cs->trash)) return fail("at most 4 trashcans");
+    for (uint32_t t = 0; t < cs->n_trash; t++) {
+        MZK_TRY(check_program(&cs->trash[t].program, "trashcan " + std::to_string(t)));
+        if (!queried(cs->fixed_queries, cs->n_fixed_queries, cs->trash[t].selector_fixed))
+            return fail("a trashcan selector is not a fixed column queried at rotation 0");
+    }
+    if (const mzk_flat_graph* g = cs->gates) {
+        MZK_TRY(check_program(g, "gates"));
     } else {
         for (int i = 0; i < 5; i++)
             if (!queried(cs->fixed_queries, cs->n_fixed_queries, cs->gate_fixed[i]))
@@ -572,6 +593,21 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     key->fixed_queries.assign(cs->fixed_queries, cs->fixed_queries + cs->n_fixed_queries);
     key->n_instance = cs->n_instance;
     key->instance_queries.assign(cs->instance_queries, cs->instance_queries + cs->n_instance_queries);
+    key->trash.resize(cs->n_trash);
+    for (uint32_t t = 0; t < cs->n_trash; t++) {
+        const mzk_flat_graph& g = cs->trash[t].program;
+        PlonkKey::Trash& tr = key->trash[t];
+        tr.consts.assign(g.constants, g.constants + 4 * (size_t)g.n_constants);
+        tr.rots.assign(g.rotations, g.rotations + g.n_rotations);
+        tr.reads.assign(g.reads, g.reads + g.n_reads);
+        tr.ops.assign(g.ops, g.ops + g.n_ops);
+        tr.program = g;
+        tr.program.constants = tr.consts.data();
+        tr.program.rotations = tr.rots.data();
+        tr.program.reads = tr.reads.data();
+        tr.program.ops = tr.ops.data();
+        tr.selector = cs->trash[t].selector_fixed;
+    }
     std::memcpy(key->gate_fixed, cs->gate_fixed, sizeof(key->gate_fixed));
     std::memcpy(key->gate_advice, cs->gate_advice, sizeof(key->gate_advice));
     if (const mzk_flat_graph* g = cs->gates) {
@@ -727,7 +763,9 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         MZK_CUDA_CHECK(cudaMemcpyAsync(lk.tinv, tinv[l].data(), tinv[l].size() * 32, cudaMemcpyHostToDevice, st));
         MZK_CUDA_CHECK(cudaMemcpyAsync(lk.uid, uid[l].data(), uid[l].size() * 4, cudaMemcpyHostToDevice, st));
     }
-    if (L > 1) build_lookup_programs(key.get());
+    // the quotient's built-in lookup term serves a single lookup without
+    // trashcans; otherwise every lookup goes to it as a helper program
+    if (L > 1 || (L && cs->n_trash)) build_lookup_programs(key.get());
     // VK commitments (Lagrange basis) as one batch
     std::vector<BatchItem> items;
     for (uint32_t i = 0; i < F; i++) items.push_back({key->fixed_lag[i], srs->off_lagrange, n});
@@ -758,14 +796,16 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         qs.push_back({{PlonkKey::P_AGG, l}, 0});
         qs.push_back({{PlonkKey::P_AGG, l}, 1});
     }
+    for (uint32_t t = 0; t < cs->n_trash; t++) qs.push_back({{PlonkKey::P_TRASH, t}, 0});  // trash Evaluated::open
     for (auto& q : key->fixed_queries) qs.push_back({{PlonkKey::P_FIXED, q.column}, q.rotation});
     for (uint32_t i = 0; i < P; i++) qs.push_back({{PlonkKey::P_PERM_FIXED, i}, 0});
     qs.push_back({{PlonkKey::P_LIN, 0}, 0});
     build_open_sets(key.get(), qs);
     const uint32_t S = key->n_sets;
-    const size_t points = cs->n_advice + L + S + 2 * L + key->qdeg + 2;
+    const size_t T = cs->n_trash;
+    const size_t points = cs->n_advice + L + S + 2 * L + T + key->qdeg + 2;
     const size_t scalars = key->advice_queries.size() + key->fixed_queries.size() + P + (S ? 3 * S - 1 : 0) + 4 * L +
-                           key->open_sets.size();
+                           T + key->open_sets.size();
     key->proof_len = 48 * points + 32 * scalars;
     key->n_blinds = (size_t)cs->n_advice * (key->bf + 1) + L * (key->bf + 1) + (size_t)S * key->bf + L * key->bf +
                     (key->qdeg - 1);
@@ -1016,6 +1056,7 @@ struct FsProof {
     Fr4 theta, beta, gamma, trash, y, x, xn, x1, x2, x3, x4;
     std::vector<Fr*> adv_lag, adv_coeff, adv_ext, z_lag, z_delta, z_coeff, z_ext, q, fdiv;
     std::vector<Fr*> inst_lag, inst_coeff, inst_ext;  // instance columns (zero past their values)
+    std::vector<Fr*> trash_lag, trash_coeff, trash_ext;  // trash columns
     // per lookup: multiplicities, helper, aggregator
     std::vector<Fr*> m_lag, m_delta, m_coeff, m_ext, h_lag, h_coeff, h_ext, Z_lag, Z_dd, Z_coeff, Z_ext;
     std::vector<uint32_t*> counts;
@@ -1026,7 +1067,7 @@ struct FsProof {
     // blinding offsets (elements of req->blinds)
     size_t off_mult = 0, off_perm = 0, off_logup = 0, off_quot = 0;
     // evaluations
-    std::vector<Fr4> ev_adv, ev_fix, ev_pc, ev_sets, ev_lk, ev_inst, q_x3;
+    std::vector<Fr4> ev_adv, ev_fix, ev_pc, ev_sets, ev_lk, ev_inst, ev_trash, q_x3;
 };
 
 size_t proof_scratch_elems(const PlonkKey* k) {
@@ -1034,8 +1075,8 @@ size_t proof_scratch_elems(const PlonkKey* k) {
     const size_t L = k->lookups.size(), O = k->open_sets.size();
     size_t counts = 0;
     for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8;
-    return (A + k->n_instance) * (2 * n + E) + S * (3 * n + E) + L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) +
-           k->qdeg * n + (4 + 2 * O + 2) * n + k->n_blinds + counts;
+    return (A + k->n_instance + k->trash.size()) * (2 * n + E) + S * (3 * n + E) +
+           L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) + k->qdeg * n + (4 + 2 * O + 2) * n + k->n_blinds + counts;
 }
 
 Status eval_many(Context* ctx, const std::vector<EvalTask>& in, std::vector<Fr4>& results, cudaStream_t st) {
@@ -1167,10 +1208,9 @@ Fr4 identities_at_x(const FsProof& p) {
         return host::fr_zero();
     };
     std::vector<Fr4> ids;
-    if (k->has_gates) {
-        // the flattened gates at x: each read is the evaluation of its query
-        // (partially_evaluate_identities evaluates the same expressions)
-        const mzk_flat_graph& g = k->gates;
+    // a flattened program at x: each read is the evaluation of its query
+    // (partially_evaluate_identities evaluates the same expressions)
+    auto program_at_x = [&](const mzk_flat_graph& g) {
         std::vector<Fr4> val(g.values_len, host::fr_zero());
         for (uint32_t i = 0; i < g.n_constants; i++) std::memcpy(val[i].l, g.constants + 4 * (size_t)i, 32);
         val[g.beta_idx] = p.beta;
@@ -1199,7 +1239,10 @@ Fr4 identities_at_x(const FsProof& p) {
                 default: val[o.dst] = fr_add(fr_mul(x, y2), z); break;
             }
         }
-        ids.push_back(val[g.result_idx]);
+        return val[g.result_idx];
+    };
+    if (k->has_gates) {
+        ids.push_back(program_at_x(k->gates));
     } else {
         // the standard gate
         const Fr4 a = adv(k->gate_advice[0]), b = adv(k->gate_advice[1]), c = adv(k->gate_advice[2]);
@@ -1252,6 +1295,12 @@ Fr4 identities_at_x(const FsProof& p) {
         acc = fr_add(fr_mul(acc, fr_add(t, p.beta)), m);
         ids.push_back(fr_mul(acc, active));
     }
+    // the trashcans (trash.rs:60-86): compressed - (1 - q) trash
+    for (size_t t = 0; t < k->trash.size(); t++) {
+        const Fr4 compressed = program_at_x(k->trash[t].program);
+        const Fr4 q = fix(k->trash[t].selector);
+        ids.push_back(fr_sub(compressed, fr_mul(fr_sub(one, q), p.ev_trash[t])));
+    }
     Fr4 acc = host::fr_zero();
     for (const Fr4& v : ids) acc = fr_add(fr_mul(acc, p.y), v);
     return acc;
@@ -1267,6 +1316,7 @@ const Fr* open_poly(const FsProof& p, std::pair<int, uint32_t> id) {
         case PlonkKey::P_AGG: return p.Z_coeff[id.second];
         case PlonkKey::P_FIXED: return k->fixed_coeff[id.second];
         case PlonkKey::P_PERM_FIXED: return k->perm_coeff[id.second];
+        case PlonkKey::P_TRASH: return p.trash_coeff[id.second];
         default: return p.lin;
     }
 }
@@ -1369,6 +1419,11 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             p.inst_lag.push_back(take(n));
             p.inst_coeff.push_back(take(n));
             p.inst_ext.push_back(take(E));
+        }
+        for (size_t t = 0; t < k->trash.size(); t++) {
+            p.trash_lag.push_back(take(n));
+            p.trash_coeff.push_back(take(n));
+            p.trash_ext.push_back(take(E));
         }
         for (uint32_t s = 0; s < k->n_sets; s++) {
             p.z_lag.push_back(take(n));
@@ -1560,7 +1615,33 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         const size_t m = p.key->n_sets + 2 * p.key->lookups.size();
         write_points(p, &res[18 * at], m);
         at += m;
-        p.trash = p.tr.squeeze();  // no trashcans: nothing is committed after it
+        p.trash = p.tr.squeeze();
+    }
+    // y is not drawn yet: a trash program reads no y slot (its slot is zero)
+    static const uint64_t kNoY[4] = {0, 0, 0, 0};
+    // the trash columns (trash/prover.rs:29-77): each trashcan's constraint
+    // expressions over the Lagrange columns, compressed with the trash
+    // challenge, committed in the Lagrange basis; then y
+    items.clear();
+    for (auto& p : ps) {
+        const PlonkKey* k = p.key;
+        if (k->trash.empty()) continue;
+        std::vector<const uint64_t*> fl(k->n_fixed), al(k->n_advice), il(k->n_instance);
+        for (uint32_t i = 0; i < k->n_fixed; i++) fl[i] = reinterpret_cast<const uint64_t*>(k->fixed_lag[i]);
+        for (uint32_t i = 0; i < k->n_advice; i++) al[i] = reinterpret_cast<const uint64_t*>(p.adv_lag[i]);
+        for (uint32_t i = 0; i < k->n_instance; i++) il[i] = reinterpret_cast<const uint64_t*>(p.inst_lag[i]);
+        for (size_t t = 0; t < k->trash.size(); t++) {
+            MZK_TRY(flat_program_rows(ctx, k->dom, k->trash[t].program, fl.data(), k->n_fixed, al.data(), k->n_advice,
+                                      il.data(), k->n_instance, p.beta.l, p.theta.l, p.trash.l, kNoY,
+                                      reinterpret_cast<uint64_t*>(p.trash_lag[t]), st));
+            items.push_back({p.trash_lag[t], k->srs.off_lagrange, k->n});
+        }
+    }
+    if (!items.empty()) MZK_TRY(msm());
+    for (size_t j = 0, at = 0; j < count; j++) {
+        FsProof& p = ps[j];
+        write_points(p, &res[18 * at], p.key->trash.size());
+        at += p.key->trash.size();
         p.y = p.tr.squeeze();
     }
     phase_done(3);
@@ -1580,6 +1661,11 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             lag.push_back(p.inst_lag[i]);
             co.push_back(p.inst_coeff[i]);
             ex.push_back(p.inst_ext[i]);
+        }
+        for (size_t t = 0; t < k->trash.size(); t++) {
+            lag.push_back(p.trash_lag[t]);
+            co.push_back(p.trash_coeff[t]);
+            ex.push_back(p.trash_ext[t]);
         }
         for (uint32_t s = 0; s < k->n_sets; s++) {
             lag.push_back(p.z_lag[s]);
@@ -1624,7 +1710,17 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         const size_t L = k->lookups.size();
         std::vector<const uint64_t*> hext(L);
         std::vector<mzk_lookup_arg> largs(L);
-        if (L == 1) {  // the fused built-in term
+        std::vector<mzk_trash_arg> targs(k->trash.size());
+        for (size_t t = 0; t < k->trash.size(); t++) {
+            targs[t].program = k->trash[t].program;
+            targs[t].selector_fixed = k->trash[t].selector;
+            targs[t].trash = reinterpret_cast<const uint64_t*>(p.trash_ext[t]);
+        }
+        if (!targs.empty()) {
+            q.n_trash = (uint32_t)targs.size();
+            q.trash = targs.data();
+        }
+        if (L == 1 && targs.empty()) {  // the fused built-in term
             const mzk_lookup_shape& sh = k->lookups[0].shape;
             q.has_lookup = 1;
             q.lookup_input_advice = sh.input_advice;
@@ -1633,7 +1729,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             q.lookup_h = reinterpret_cast<const uint64_t*>(p.h_ext[0]);
             q.lookup_z = reinterpret_cast<const uint64_t*>(p.Z_ext[0]);
             q.lookup_m = reinterpret_cast<const uint64_t*>(p.m_ext[0]);
-        } else if (L > 1) {  // one helper program per lookup
+        } else if (L >= 1) {  // one helper program per lookup
             for (size_t l = 0; l < L; l++) {
                 hext[l] = reinterpret_cast<const uint64_t*>(p.h_ext[l]);
                 largs[l].n_helpers = 1;
@@ -1690,6 +1786,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 tasks.push_back(eval_task(p.Z_coeff[l], n, p.x));
                 tasks.push_back(eval_task(p.Z_coeff[l], n, fr_rot(d, p.x, 1)));
             }
+            for (size_t t = 0; t < k->trash.size(); t++) tasks.push_back(eval_task(p.trash_coeff[t], n, p.x));
             if (with_instance)
                 for (auto& q : k->instance_queries)
                     tasks.push_back(eval_task(p.inst_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
@@ -1709,6 +1806,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             grab(p.ev_pc, k->n_perm);
             grab(p.ev_sets, 3 * (size_t)k->n_sets);
             grab(p.ev_lk, 4 * k->lookups.size());
+            grab(p.ev_trash, k->trash.size());
             grab(p.ev_inst, with_instance ? k->instance_queries.size() : 0);
             // transcript order (write_evals_to_transcript, permutation / logup evaluate)
             for (auto& v : p.ev_adv) p.tr.write_fr(v);
@@ -1720,6 +1818,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 if (s + 1 < k->n_sets) p.tr.write_fr(p.ev_sets[3 * s + 2]);
             }
             for (auto& v : p.ev_lk) p.tr.write_fr(v);
+            for (auto& v : p.ev_trash) p.tr.write_fr(v);
             // L'(X) = -sum_i (x^n - 1) (x^(n-1))^i h_i(X): the identities are
             // all constants here (no simple selectors)
             const Fr4 sf = fr_pow_u64(p.x, k->n - 1);
@@ -2028,11 +2127,13 @@ int mzk_plonk_key_transcript_layout(const mzk_plonk_key* key, uint8_t* ops, size
     put(MZK_TR_WRITE_POINT, L);                // multiplicities
     put(MZK_TR_SQUEEZE, 2);                    // beta, gamma
     put(MZK_TR_WRITE_POINT, S + 2 * L);        // permutation products, logup helper and aggregator
-    put(MZK_TR_SQUEEZE, 2);                    // trash challenge, y
+    put(MZK_TR_SQUEEZE, 1);                    // trash challenge
+    put(MZK_TR_WRITE_POINT, k->trash.size());  // trash columns
+    put(MZK_TR_SQUEEZE, 1);                    // y
     put(MZK_TR_WRITE_POINT, k->qdeg);          // quotient limbs
     put(MZK_TR_SQUEEZE, 1);                    // x
     put(MZK_TR_WRITE_FR, k->advice_queries.size() + k->fixed_queries.size() + k->n_perm + (S ? 3 * S - 1 : 0) +
-                             4 * L);          // evaluations
+                             4 * L + k->trash.size());  // evaluations
     put(MZK_TR_SQUEEZE, 2);                    // x1, x2
     put(MZK_TR_WRITE_POINT, 1);                // f
     put(MZK_TR_SQUEEZE, 1);                    // x3

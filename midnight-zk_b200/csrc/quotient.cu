@@ -344,6 +344,55 @@ Status pack_programs(Context* ctx, const Domain* d, const mzk_quotient_desc* des
 
 }  // namespace
 
+// One flattened program evaluated at every row of the n-point domain over
+// Lagrange columns (rotations are whole rows): the trash argument's
+// compressed constraint expressions (trash/prover.rs, `evaluate` over the
+// Lagrange values, folded with the trash challenge by the program itself).
+Status flat_program_rows(Context* ctx, const Domain* d, const mzk_flat_graph& g, const uint64_t* const* fixed,
+                         uint32_t n_fixed, const uint64_t* const* advice, uint32_t n_advice,
+                         const uint64_t* const* instance, uint32_t n_instance, const uint64_t beta[4],
+                         const uint64_t theta[4], const uint64_t trash[4], const uint64_t y[4], uint64_t* out,
+                         cudaStream_t st) {
+    if (n_fixed > kQMaxFixed || n_advice > kQMaxAdvice || n_instance > kQMaxInstance) {
+        set_error("flat program: too many columns");
+        return ERR_ARG;
+    }
+    mzk_quotient_desc desc;  // only the challenge slots are read from it
+    std::memset(&desc, 0, sizeof(desc));
+    std::memcpy(desc.beta, beta, 32);
+    std::memcpy(desc.theta, theta, 32);
+    std::memcpy(desc.trash_challenge, trash, 32);
+    std::memcpy(desc.y, y, 32);
+    const uint32_t n_cols[3] = {n_fixed, n_advice, n_instance};
+    const uint32_t n = 1u << d->k;
+    std::vector<uint32_t> W;
+    std::string err;
+    GatesParams gp;
+    std::memset(&gp, 0, sizeof(gp));
+    gp.prog = pack_program(W, g, n_cols, &desc, 0, n, err);
+    if (!err.empty()) {
+        set_error("flat program: " + err);
+        return ERR_ARG;
+    }
+    for (uint32_t i = 0; i < n_fixed; i++) gp.cols.c[0][i] = reinterpret_cast<const Fr*>(fixed[i]);
+    for (uint32_t i = 0; i < n_advice; i++) gp.cols.c[1][i] = reinterpret_cast<const Fr*>(advice[i]);
+    for (uint32_t i = 0; i < n_instance; i++) gp.cols.c[2][i] = reinterpret_cast<const Fr*>(instance[i]);
+    const size_t bytes = W.size() * 4;
+    void *dev, *host;
+    MZK_TRY(ctx->ensure("flat_rows", bytes, &dev));
+    MZK_TRY(ctx->ensure_pinned(bytes, &host));
+    std::memcpy(host, W.data(), bytes);
+    MZK_CUDA_CHECK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, st));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(st));  // the pinned staging is reused by the next call
+    gp.words = static_cast<const uint32_t*>(dev);
+    gp.log_n = d->k;
+    gp.out = reinterpret_cast<Fr*>(out);
+    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 127) / 128, (uint32_t)ctx->num_sms * 8));
+    k_gates_flat<<<blocks, 128, 0, st>>>(gp);
+    MZK_LAUNCH_CHECK(ctx);
+    return OK;
+}
+
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st) {
     if (desc->k != d->k || desc->extended_k != d->ext_k) {

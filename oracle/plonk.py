@@ -187,12 +187,13 @@ class Transcript:
 # ---------------------------------------------------------------- circuit --
 def blinding_factors(circuit):
     """ConstraintSystem::blinding_factors (plonk/circuit.rs:2203-2245) for this
-    shape: max(3, max advice queries per column) + helper chunks + 3."""
+    shape: max(3, max advice queries per column) + trashcans + helper chunks
+    + 3."""
     per_col = {}
     for col, _ in circuit["advice_queries"]:
         per_col[col] = per_col.get(col, 0) + 1
     f = max(3, max(per_col.values(), default=1))
-    return f + len(circuit["lookups"]) + 3
+    return f + len(circuit.get("trashcans", [])) + len(circuit["lookups"]) + 3
 
 
 def n_perm_sets(circuit):
@@ -356,15 +357,16 @@ def _cycles(rng, n, u, n_cols, cycle_cols, fraction, rows):
     return mapping, vals
 
 
-def generic_instance(k, seed, table_bits=16, copy_fraction=0.10, two_lookups=False):
+def generic_instance(k, seed, table_bits=16, copy_fraction=0.10, two_lookups=False, circuit=None):
     """Seeded fixed columns, copy cycles (over the a and b cells of rows
     before the last usable row) and a satisfying witness of generic_circuit:
     a a table value, b uniform, c = q1 a b + q2 a(wX), d = a^2; the gate
     selectors q1, q2, q4 are zero from the last usable row on (its a(wX) is a
     blinding row), q3 from the usable rows on.  two_lookups: the table of
     squares t2[i] = i^2 (i < the table's rows; zero after), which holds every
-    usable d."""
-    c = generic_circuit(k, two_lookups)
+    usable d.  circuit: the circuit whose blinding factors fix the usable rows
+    (default generic_circuit's)."""
+    c = circuit if circuit is not None else generic_circuit(k, two_lookups)
     n = 1 << k
     bf = blinding_factors(c)
     u = n - bf - 1
@@ -419,6 +421,30 @@ def instance_circuit(k):
     c.update({"gates": g, "n_fixed": 7, "fixed_queries": [(i, 0) for i in range(7)], "n_instance": 1,
               "instance_queries": [(0, 0)], "perm_cols": c["perm_cols"] + [(2, 0)]})
     return c
+
+
+def trash_circuit(k):
+    """generic_circuit with a trashcan (trash.rs): constraint expressions
+    d - a^2 and q1 a b + q2 a(wX) - q4 c folded with the trash challenge, the
+    selector q3 (non-zero only on rows where both vanish).  With the
+    trashcan the lookup goes to the quotient as a helper program."""
+    zero, one = to_mont(0), to_mont(1)
+    program = {"constants": [zero, one], "rotations": [0, 1],
+               # values: constants 0, 1; slots beta 2, theta 3, trash 4, y 5, previous 6; reads 7..14
+               "reads": [(0, 0, 0, 7), (0, 1, 0, 8), (0, 3, 0, 9), (1, 0, 0, 10), (1, 1, 0, 11), (1, 2, 0, 12),
+                         (1, 3, 0, 13), (1, 0, 1, 14)],
+               "ops": [(2, 15, 10, 11, 0), (2, 16, 7, 15, 0), (2, 17, 8, 14, 0), (0, 18, 16, 17, 0),
+                       (2, 19, 9, 12, 0), (1, 20, 18, 19, 0), (3, 21, 10, 0, 0), (1, 22, 13, 21, 0),
+                       (6, 23, 6, 4, 22), (6, 24, 23, 4, 20)],
+               "values_len": 25, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
+               "previous_value_idx": 6, "result_idx": 24}
+    c = generic_circuit(k)
+    c["trashcans"] = [{"program": program, "selector": 2}]
+    return c
+
+
+def trash_instance(k, seed):
+    return generic_instance(k, seed, circuit=trash_circuit(k))
 
 
 INSTANCE_ROWS = 3
@@ -714,6 +740,13 @@ def identities(key, ev, ch):
         fb = (f + beta) % R
         out.append((h * fb - 1) % R)              # one input: product f+beta, sum of partial products 1
         out.append(((Zn - Z - sel * h) * (table + beta) + m) * (1 - (l_last + l_blind)) % R)
+    # trashcans (trash.rs:60-86): compressed - (1 - q) trash
+    for ti, tc in enumerate(c.get("trashcans", [])):
+        def read(col_type, col, rot):
+            qs = (c["fixed_queries"], c["advice_queries"], c.get("instance_queries", []))[col_type]
+            return (fix, adv, ins)[col_type][query_index(qs, col, rot)]
+        compressed = program_at(tc["program"], read, ch)
+        out.append((compressed - (1 - fq(tc["selector"])) * ev["trash"][ti]) % R)
     return [v % R for v in out]
 
 
@@ -861,6 +894,11 @@ def create_proof(key, advice, blinds, instances=None):
         tr.write_point(commit(h, srs["lagrange"]))
         tr.write_point(commit(delta(Z, 2), srs["double_delta"]))
     trash = tr.squeeze()
+    # trash columns (trash/prover.rs:29-77): the constraint expressions over
+    # the Lagrange columns, compressed with the trash challenge
+    trs = [trash_column(key, tc["program"], adv, inst, beta, theta, trash) for tc in c.get("trashcans", [])]
+    for t in trs:
+        tr.write_point(commit(t, srs["lagrange"]))
     y = tr.squeeze()
     # coefficient forms and cosets
     adv_c = [dom.lagrange_to_coeff(a) for a in adv]
@@ -870,9 +908,10 @@ def create_proof(key, advice, blinds, instances=None):
     Z_c = [dom.lagrange_to_coeff(Z) for Z in Zs]
     ext = lambda p: dom.coeff_to_extended(p)
     inst_c = [dom.lagrange_to_coeff(col) for col in inst]
+    t_c = [dom.lagrange_to_coeff(t) for t in trs]
     hpoly = quotient(key, [ext(p) for p in adv_c], [ext(p) for p in z_c], [ext(p) for p in m_c],
                      [ext(p) for p in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta, trash=trash,
-                     inst_e=[ext(p) for p in inst_c])
+                     inst_e=[ext(p) for p in inst_c], trash_e=[ext(p) for p in t_c])
     hcoeff = dom.extended_to_coeff(hpoly)[: (n - 1) * qdeg]
     limbs = [np.concatenate([hcoeff[i * (n - 1):(i + 1) * (n - 1)], np.zeros((1, 4), np.uint64)]) for i in range(qdeg)]
     for i, t in enumerate(take(qdeg - 1), start=1):         # blind_quotient_limbs (prover.rs:774-785)
@@ -906,6 +945,9 @@ def create_proof(key, advice, blinds, instances=None):
         ev["lookups"].append(e)
         for v in e:
             tr.write_fr(v)
+    ev["trash"] = [eval_at(t, x) for t in t_c]                 # trash/prover.rs:80-92
+    for v in ev["trash"]:
+        tr.write_fr(v)
     # linearization (linearization/prover.rs:41-86): every identity is a
     # constant, so L'(X) = -sum_i (x^n - 1) (x^(n-1))^i h_i(X)
     sf = pow(x, n - 1, R)
@@ -924,6 +966,8 @@ def create_proof(key, advice, blinds, instances=None):
         q.append((("h", li, 0), x, h_c[li]))
         q.append((("Z", li), x, Z_c[li]))
         q.append((("Z", li), x_next, Z_c[li]))
+    for ti, t in enumerate(t_c):
+        q.append((("trash", ti), x, t))
     for col, rot in c["fixed_queries"]:
         q.append((("fixed", col), rotate(key, x, rot), key.fixed_polys[col]))
     for i, p in enumerate(key.perm_polys):
@@ -933,7 +977,21 @@ def create_proof(key, advice, blinds, instances=None):
     return bytes(tr.proof)
 
 
-def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None, trash=0, inst_e=()):
+def trash_column(key, graph, adv, inst, beta, theta, trash):
+    """Argument::commit's compressed expression (trash/prover.rs:46-62): the
+    program (the constraint expressions folded with the trash challenge) at
+    every row of the n-point domain over the Lagrange columns, rotations in
+    rows.  Pure Python per row: small domains."""
+    n = key.n
+    cols = (key.fixed_values, adv, inst)
+    ch = (to_mont(beta), to_mont(theta), to_mont(trash), np.zeros(4, np.uint64))
+    out = np.zeros((n, 4), np.uint64)
+    for r in range(n):
+        out[r] = O._run_program(graph, cols, r, n, 0, ch)[graph["result_idx"]]
+    return out
+
+
+def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None, trash=0, inst_e=(), trash_e=()):
     """compute_nu_poly + divide_by_vanishing_poly (prover.rs:634-715) through
     the C oracle's evaluate_numerator restatement."""
     c, dom = key.circuit, key.dom
@@ -961,7 +1019,8 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     d.perm_sigma = parr(key.perm_cosets)
     d.n_perm_sets, d.perm_z = len(z_e), parr(z_e)
     d.chunk_len, d.blinding_factors = c["degree"] - 2, key.bf
-    if len(c["lookups"]) == 1:
+    tcs = c.get("trashcans", [])
+    if len(c["lookups"]) == 1 and not tcs:
         lk = c["lookups"][0]
         d.has_lookup = 1
         d.lookup_input_advice, d.lookup_table_fixed = lk["input"], lk["table"]
@@ -979,17 +1038,19 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     if c.get("gates") is not None:
         gate_values = O.flat_gates_eval(c["gates"], key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k,
                                         to_mont(beta), to_mont(theta), to_mont(trash), to_mont(y))
-    if len(c["lookups"]) <= 1:
+    if len(c["lookups"]) <= 1 and not tcs:
         return dom.quotient_eval(d, True, threads, gate_values)
-    # several lookups: the gate and permutation terms, then every lookup's
-    # terms (evaluation.rs:1034-1090) as single-input helper programs
-    # (Evaluator::lookups_flat, :686-767), then the division by t(X)
+    # several lookups, or trashcans: the gate and permutation terms, then
+    # every lookup's terms (evaluation.rs:1034-1090) as single-input helper
+    # programs (Evaluator::lookups_flat, :686-767) and every trashcan's term
+    # (:1093-1109), then the division by t(X)
     v = dom.quotient_eval(d, False, threads, gate_values)
     lks = [{"programs": [g], "outputs": [outs], "helpers": [h_e[li]], "aggregator": Z_e[li],
             "multiplicities": m_e[li]}
            for li, (g, outs) in enumerate(lookup_program(lk) for lk in c["lookups"])]
+    tas = [{"program": tc["program"], "selector": tc["selector"], "trash": trash_e[ti]} for ti, tc in enumerate(tcs)]
     v = O.flat_tail_eval(v, key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k, to_mont(beta), to_mont(theta),
-                         to_mont(trash), to_mont(y), key.l0, key.l_last, key.l_active, lookups=lks)
+                         to_mont(trash), to_mont(y), key.l0, key.l_last, key.l_active, lookups=lks, trashcans=tas)
     return dom.divide_by_vanishing_poly(v)
 
 
@@ -1078,7 +1139,9 @@ def _verify(key, proof, s, instances=None):
     gamma = tr.squeeze()
     z_coms = [tr.read_point() for _ in range(S)]
     hz_coms = [(tr.read_point(), tr.read_point()) for _ in range(L)]
-    trash = tr.squeeze()                           # trash challenge (no trashcans)
+    trash = tr.squeeze()
+    T = len(c.get("trashcans", []))
+    trash_coms = [tr.read_point() for _ in range(T)]
     y = tr.squeeze()
     limb_coms = [tr.read_point() for _ in range(qdeg)]
     x = tr.squeeze()
@@ -1093,6 +1156,7 @@ def _verify(key, proof, s, instances=None):
         sets.append([z0, z1, tr.read_fr() if si < S - 1 else None])
     ev["perm_sets"] = sets
     ev["lookups"] = [tuple(tr.read_fr() for _ in range(4)) for _ in range(L)]
+    ev["trash"] = [tr.read_fr() for _ in range(T)]
     ev["instance"] = instance_evals(key, instances, x, xn)
     ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta, "trash": trash, "y": y}
     const = horner(identities(key, ev, ch), y)
@@ -1114,6 +1178,8 @@ def _verify(key, proof, s, instances=None):
         q.append((("h", li, 0), x, hz_coms[li][0], h))
         q.append((("Z", li), x, hz_coms[li][1], Z))
         q.append((("Z", li), x_next, hz_coms[li][1], Zn))
+    for ti in range(T):
+        q.append((("trash", ti), x, trash_coms[ti], ev["trash"][ti]))
     for qi, (col, rot) in enumerate(c["fixed_queries"]):
         q.append((("fixed", col), rotate(key, x, rot), key.fixed_coms[col], ev["fixed"][qi]))
     for i, com in enumerate(key.perm_coms):

@@ -17,7 +17,8 @@ PINNED = b"config-3 circuit: standard gate, copy cycles, range lookup"
 
 SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.generic_circuit, OP.generic_instance),
           "generic2": (OP.generic2_circuit, OP.generic2_instance),
-          "instance": (OP.instance_circuit, OP.instance_instance)}
+          "instance": (OP.instance_circuit, OP.instance_instance),
+          "trash": (OP.trash_circuit, OP.trash_instance)}
 
 
 class Circuit:
@@ -27,8 +28,9 @@ class Circuit:
         this circuit gets its own.  shape: "config3" (the single-proof
         configuration), "generic" (two gates with a rotation, two
         permutation sets), "generic2" (generic with a second lookup,
-        without a selector) or "instance" (generic with an instance column
-        read by a third gate and copied from c)."""
+        without a selector), "instance" (generic with an instance column
+        read by a third gate and copied from c) or "trash" (generic with a
+        trashcan)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)

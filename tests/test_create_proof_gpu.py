@@ -250,6 +250,34 @@ def test_instance_circuit_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, c.advice, bl)])                # the instance column is missing
 
 
+@pytest.mark.parametrize("k", [5, 9])
+def test_trash_circuit_proof_equals_oracle(ctx, k):
+    """A trashcan: its column (constraint expressions folded with the trash
+    challenge, evaluated on the device over the Lagrange columns) committed
+    after the trash challenge and before y, evaluated and opened at x; the
+    lookup goes to the quotient as a helper program.  The device transcript
+    equals the oracle's and verifies, alone, in a batch and through the
+    proving service; a witness breaking a trashed constraint fails the
+    self-check."""
+    c = Circuit(ctx, k, seed=k + 90, shape="trash")
+    assert len(c.circuit["trashcans"]) == 1
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    both = mzk.create_proofs(ctx, [(c.key, c.advice, bl), (c.key, c.advice, c.blinds(6))])
+    assert both[0] == proof and c.verify(both[1])
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = srv.submit(c.key, c.advice, c.blinds(7))
+    assert c.verify(srv.wait(t)[0])
+    srv.close()
+    assert replay(c.key, proof) == proof                    # the layout lists the trash commitment and evaluation
+    bad = [a.copy() for a in c.advice]
+    bad[3][1] = OP.to_mont(OP.to_int(bad[3][1]) + 1)          # d != a^2 on a row where q3 is set
+    with pytest.raises(mzk.MzkError, match="does not satisfy"):
+        mzk.create_proofs(ctx, [(c.key, bad, bl)], flags=mzk.PROVE_SELF_CHECK)
+
+
 def test_key_files_equal_oracle_and_read_back(ctx, k5):
     """VerifyingKey / ProvingKey files in the three SerdeFormats equal the
     oracle's bytes; a key read from a PK file has the same transcript_repr and
@@ -279,16 +307,14 @@ def test_key_files_equal_oracle_and_read_back(ctx, k5):
         assert name
 
 
-def test_transcript_layout_replays_the_proof(k5):
-    """A caller with its own transcript object replays a proof from the key's
-    transcript layout: the same absorbs and squeezes rebuild the same proof
-    bytes."""
+def replay(key, proof):
+    """The proof's transcript rebuilt from the key's transcript layout by a
+    separate transcript object; returns its final bytes."""
     from oracle import oracle as O
-    proof = mzk.create_proofs(k5.ctx, [(k5.key, k5.advice, k5.blinds(12))])[0]
     t, pos = mzk.Transcript(), 0
-    for op in k5.key.transcript_layout():
+    for op in key.transcript_layout():
         if op == 0:
-            t.common_fr(k5.key.repr)
+            t.common_fr(key.repr)
         elif op == 1:
             st, aff = O.g1_decompress(proof[pos:pos + 48])
             p18 = np.zeros(18, np.uint64)
@@ -301,4 +327,13 @@ def test_transcript_layout_replays_the_proof(k5):
             pos += 32
         else:
             t.squeeze_challenge()
-    assert pos == len(proof) and t.finalize() == proof
+    assert pos == len(proof)
+    return t.finalize()
+
+
+def test_transcript_layout_replays_the_proof(k5):
+    """A caller with its own transcript object replays a proof from the key's
+    transcript layout: the same absorbs and squeezes rebuild the same proof
+    bytes."""
+    proof = mzk.create_proofs(k5.ctx, [(k5.key, k5.advice, k5.blinds(12))])[0]
+    assert replay(k5.key, proof) == proof

@@ -173,6 +173,28 @@ def test_instance_circuit_proofs_verify():
         OP.create_proof(key, adv, bl, [np.tile(O.fr_const(0), (key.u + 1, 1))])
 
 
+def test_trash_circuit_proofs_verify():
+    """A trashcan: its column (the constraint expressions folded with the
+    trash challenge) committed after the trash challenge, evaluated and
+    opened at x, its term compressed - (1 - q) trash in the identities; the
+    lookup then goes to the quotient as a helper program.  The proof
+    verifies; a witness breaking a trashed constraint on a selected row does
+    not."""
+    k = 5
+    c = OP.trash_circuit(k)
+    fixed, mapping, adv = OP.trash_instance(k, 13)
+    s = O.rand_fr(57, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"trash")
+    assert key.bf == OP.blinding_factors(OP.generic_circuit(k)) + 1
+    bl = [OP.to_int(v) for v in O.rand_fr(67, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl)
+    assert OP.verify(key, proof, OP.to_int(s))
+    bad = [a.copy() for a in adv]
+    bad[3][1] = OP.to_mont(OP.to_int(bad[3][1]) + 1)          # d != a^2 on a row where q3 is set
+    assert not OP.verify(key, OP.create_proof(key, bad, bl), OP.to_int(s))
+
+
 def test_generic_circuit_proofs_verify():
     """Another circuit shape: two gates as one flattened program (with a(wX)),
     four permutation columns in two sets (z of the first set opened at
