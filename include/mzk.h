@@ -432,8 +432,16 @@ typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } m
  * mzk_trash_arg whose program compresses the constraint expressions with the
  * trash challenge, reading only queried columns, and whose selector is a
  * fixed column queried at rotation 0; its `trash` pointer is not used here:
- * the prover computes, commits, evaluates and opens the trash column), no
- * simple selectors. */
+ * the prover computes, commits, evaluates and opens the trash column), and
+ * simple selectors: with `gates` given, n_gate_polys > 0 lists each gate
+ * polynomial in order (Gate::polynomials of every gate) by the value slot
+ * that holds it in the gates program (gate_poly_values; the operand the
+ * program folds into its Horner chain in y) and by its simple selector's
+ * fixed column (gate_poly_selector, -1 for none).  Those fixed columns are
+ * evaluated as one in the identities and are neither written to the
+ * transcript nor opened; their polynomials enter the linearization, scaled by
+ * the identity (partially_evaluate_identities, plonk/mod.rs:502-608;
+ * compute_linearization_poly, linearization/prover.rs:41-86). */
 typedef struct {
     uint32_t degree;                   /* cs.degree() (plonk/circuit.rs:2174-2199), 3..9 */
     uint32_t blinding_factors;         /* cs.blinding_factors() (circuit.rs:2203-2245) */
@@ -449,6 +457,9 @@ typedef struct {
     uint32_t n_instance;               /* instance columns (0..4) */
     const mzk_query *instance_queries; uint32_t n_instance_queries;
     uint32_t n_trash; const mzk_trash_arg *trash;
+    uint32_t n_gate_polys;
+    const uint32_t *gate_poly_values;  /* value slot of each gate polynomial in `gates` */
+    const int32_t *gate_poly_selector; /* its simple selector's fixed column, or -1 */
 } mzk_circuit_desc;
 /* ParamsKZG's bases (params.rs:83-93) inside one DEVICE G1Affine buffer;
  * table_c > 0: srs is row 0 of a window table of that width and table_rows

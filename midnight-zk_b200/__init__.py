@@ -920,7 +920,9 @@ class CircuitDesc(ctypes.Structure):
                 ("n_perm_cols", ctypes.c_uint32), ("perm_col_kind", ctypes.c_void_p),
                 ("perm_col_index", ctypes.c_void_p), ("n_lookups", ctypes.c_uint32), ("lookups", ctypes.c_void_p),
                 ("n_instance", ctypes.c_uint32), ("instance_queries", ctypes.c_void_p),
-                ("n_instance_queries", ctypes.c_uint32), ("n_trash", ctypes.c_uint32), ("trash", ctypes.c_void_p)]
+                ("n_instance_queries", ctypes.c_uint32), ("n_trash", ctypes.c_uint32), ("trash", ctypes.c_void_p),
+                ("n_gate_polys", ctypes.c_uint32), ("gate_poly_values", ctypes.c_void_p),
+                ("gate_poly_selector", ctypes.c_void_p)]
 
 
 class SrsDesc(ctypes.Structure):
@@ -1019,7 +1021,8 @@ class PlonkKey:
     column)], lookups [{"input", "table", "selector" (None: constant one)}],
     n_instance and instance_queries [(column, rotation)] (optional),
     trashcans [{"program": flattened program, "selector": fixed column}]
-    (optional).  fixed_values:
+    (optional), gate_polys [(value slot, simple selector fixed column or
+    None)] per gate polynomial (optional, with "gates").  fixed_values:
     host (n, 4) arrays; mapping: (n_perm_cols, n, 2) uint32 or None; srs:
     an SrsDesc.  The domain and the SRS buffer must outlive the key."""
 
@@ -1076,6 +1079,11 @@ class PlonkKey:
                 targs[i].selector_fixed = tc["selector"]
             keep.append(targs)
             cs.n_trash, cs.trash = len(tcs), ctypes.addressof(targs)
+        gpolys = circuit.get("gate_polys", [])
+        if gpolys:
+            cs.n_gate_polys = len(gpolys)
+            cs.gate_poly_values = arr(ctypes.c_uint32, [slot for slot, _ in gpolys])
+            cs.gate_poly_selector = arr(ctypes.c_int32, [-1 if sel is None else sel for _, sel in gpolys])
         pin = ctypes.create_string_buffer(bytes(pinned), max(1, len(pinned)))
         h = _vp()
         if pk_bytes is not None:

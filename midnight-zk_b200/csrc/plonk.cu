@@ -275,6 +275,12 @@ struct PlonkKey {
         uint32_t selector = 0;
     };
     std::vector<Trash> trash;
+    // simple selectors: the gates program's slot of each gate polynomial, its
+    // selector's fixed column (-1: none), and which fixed columns are simple
+    std::vector<uint32_t> gate_poly_values;
+    std::vector<int32_t> gate_poly_selector;
+    std::vector<uint8_t> simple_col;
+    bool is_simple(uint32_t fixed_col) const { return fixed_col < simple_col.size() && simple_col[fixed_col]; }
     // device
     void* mem = nullptr;
     std::vector<Fr*> fixed_lag, fixed_coeff, fixed_ext, perm_lag, perm_coeff, perm_ext;
@@ -390,6 +396,16 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
         if (!queried(cs->fixed_queries, cs->n_fixed_queries, cs->trash[t].selector_fixed))
             return fail("a trashcan selector is not a fixed column queried at rotation 0");
     }
+    if (cs->n_gate_polys) {
+        if (!cs->gates || !cs->gate_poly_values || !cs->gate_poly_selector)
+            return fail("gate polynomials need the gates program and both arrays");
+        for (uint32_t i = 0; i < cs->n_gate_polys; i++) {
+            if (cs->gate_poly_values[i] >= cs->gates->values_len) return fail("gate polynomial slot out of range");
+            const int32_t sel = cs->gate_poly_selector[i];
+            if (sel >= 0 && !queried(cs->fixed_queries, cs->n_fixed_queries, (uint32_t)sel))
+                return fail("a simple selector is not a fixed column queried at rotation 0");
+        }
+    }
     if (const mzk_flat_graph* g = cs->gates) {
         MZK_TRY(check_program(g, "gates"));
     } else {
@@ -465,6 +481,14 @@ void build_open_sets(PlonkKey* key, const std::vector<std::pair<std::pair<int, u
 // table are the columns themselves, the sum of partial products is the
 // constant one).  Values: 0, 1 (constants), beta, theta, trash challenge, y,
 // the previous value, then the input, table and selector reads and the ops.
+// the fixed evaluations a proof writes: every fixed query but those of simple
+// selectors (write_evals_to_transcript, prover.rs:857-862)
+size_t fixed_written(const PlonkKey& k) {
+    size_t m = 0;
+    for (auto& q : k.fixed_queries) m += k.is_simple(q.column) ? 0 : 1;
+    return m;
+}
+
 void build_lookup_programs(PlonkKey* key) {
     const uint32_t L = (uint32_t)key->lookups.size();
     const Fr4 zero = host::fr_zero(), one = host::fr_one();
@@ -607,6 +631,12 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         tr.program.reads = tr.reads.data();
         tr.program.ops = tr.ops.data();
         tr.selector = cs->trash[t].selector_fixed;
+    }
+    key->simple_col.assign(cs->n_fixed, 0);
+    for (uint32_t i = 0; i < cs->n_gate_polys; i++) {
+        key->gate_poly_values.push_back(cs->gate_poly_values[i]);
+        key->gate_poly_selector.push_back(cs->gate_poly_selector[i]);
+        if (cs->gate_poly_selector[i] >= 0) key->simple_col[cs->gate_poly_selector[i]] = 1;
     }
     std::memcpy(key->gate_fixed, cs->gate_fixed, sizeof(key->gate_fixed));
     std::memcpy(key->gate_advice, cs->gate_advice, sizeof(key->gate_advice));
@@ -797,15 +827,16 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         qs.push_back({{PlonkKey::P_AGG, l}, 1});
     }
     for (uint32_t t = 0; t < cs->n_trash; t++) qs.push_back({{PlonkKey::P_TRASH, t}, 0});  // trash Evaluated::open
-    for (auto& q : key->fixed_queries) qs.push_back({{PlonkKey::P_FIXED, q.column}, q.rotation});
+    for (auto& q : key->fixed_queries)  // a simple selector is not opened (prover.rs:913-918)
+        if (!key->is_simple(q.column)) qs.push_back({{PlonkKey::P_FIXED, q.column}, q.rotation});
     for (uint32_t i = 0; i < P; i++) qs.push_back({{PlonkKey::P_PERM_FIXED, i}, 0});
     qs.push_back({{PlonkKey::P_LIN, 0}, 0});
     build_open_sets(key.get(), qs);
     const uint32_t S = key->n_sets;
     const size_t T = cs->n_trash;
     const size_t points = cs->n_advice + L + S + 2 * L + T + key->qdeg + 2;
-    const size_t scalars = key->advice_queries.size() + key->fixed_queries.size() + P + (S ? 3 * S - 1 : 0) + 4 * L +
-                           T + key->open_sets.size();
+    const size_t scalars = key->advice_queries.size() + fixed_written(*key) + P + (S ? 3 * S - 1 : 0) + 4 * L + T +
+                           key->open_sets.size();
     key->proof_len = 48 * points + 32 * scalars;
     key->n_blinds = (size_t)cs->n_advice * (key->bf + 1) + L * (key->bf + 1) + (size_t)S * key->bf + L * key->bf +
                     (key->qdeg - 1);
@@ -1064,6 +1095,7 @@ struct FsProof {
        *tmp_b = nullptr;
     Fr* d_blinds = nullptr;
     uint64_t f_len = 0;
+    Fr4 lin_c = {};  // the linearization's constant term C (when the identities were evaluated)
     // blinding offsets (elements of req->blinds)
     size_t off_mult = 0, off_perm = 0, off_logup = 0, off_quot = 0;
     // evaluations
@@ -1184,10 +1216,11 @@ Status lincomb_many(Context* ctx, const std::vector<LinSpec>& specs, cudaStream_
     return OK;
 }
 
-// the identities of partially_evaluate_identities (plonk/mod.rs:519-608),
-// every one fully evaluated, folded in y by Horner (the linearization's
-// constant term, linearization/prover.rs:52-69)
-Fr4 identities_at_x(const FsProof& p) {
+// the identities of partially_evaluate_identities (plonk/mod.rs:502-608) in
+// order, each with the fixed column of its simple selector (-1: none, the
+// identity is fully evaluated); a simple selector's evaluation is one here
+// (ev_fix holds one for its queries)
+std::vector<std::pair<int32_t, Fr4>> identities_at_x(const FsProof& p) {
     using namespace host;
     const PlonkKey* k = p.key;
     const Domain* d = k->dom;
@@ -1207,7 +1240,7 @@ Fr4 identities_at_x(const FsProof& p) {
             if (k->instance_queries[i].column == col && k->instance_queries[i].rotation == 0) return p.ev_inst[i];
         return host::fr_zero();
     };
-    std::vector<Fr4> ids;
+    std::vector<std::pair<int32_t, Fr4>> ids;
     // a flattened program at x: each read is the evaluation of its query
     // (partially_evaluate_identities evaluates the same expressions)
     auto program_at_x = [&](const mzk_flat_graph& g) {
@@ -1239,10 +1272,16 @@ Fr4 identities_at_x(const FsProof& p) {
                 default: val[o.dst] = fr_add(fr_mul(x, y2), z); break;
             }
         }
-        return val[g.result_idx];
+        return val;
     };
     if (k->has_gates) {
-        ids.push_back(program_at_x(k->gates));
+        const std::vector<Fr4> val = program_at_x(k->gates);
+        if (k->gate_poly_values.empty()) {
+            ids.push_back({-1, val[k->gates.result_idx]});  // all gate polynomials, already folded in y
+        } else {
+            for (size_t i = 0; i < k->gate_poly_values.size(); i++)
+                ids.push_back({k->gate_poly_selector[i], val[k->gate_poly_values[i]]});
+        }
     } else {
         // the standard gate
         const Fr4 a = adv(k->gate_advice[0]), b = adv(k->gate_advice[1]), c = adv(k->gate_advice[2]);
@@ -1251,7 +1290,7 @@ Fr4 identities_at_x(const FsProof& p) {
         g = fr_add(g, fr_mul(fr_mul(fix(k->gate_fixed[2]), a), b));
         g = fr_add(g, fr_mul(fix(k->gate_fixed[3]), c));
         g = fr_add(g, fix(k->gate_fixed[4]));
-        ids.push_back(g);
+        ids.push_back({-1, g});
     }
     // l_last, l_blind, l_0 (l_i_range over -(bf + 1) ..= 0)
     const int32_t bf = (int32_t)k->bf;
@@ -1264,9 +1303,9 @@ Fr4 identities_at_x(const FsProof& p) {
     const uint32_t S = k->n_sets;
     if (S) {
         auto z = [&](uint32_t s, int which) { return p.ev_sets[3 * s + which]; };
-        ids.push_back(fr_mul(l_0, fr_sub(one, z(0, 0))));
-        ids.push_back(fr_mul(fr_sub(fr_mul(z(S - 1, 0), z(S - 1, 0)), z(S - 1, 0)), l_last));
-        for (uint32_t s = 1; s < S; s++) ids.push_back(fr_mul(fr_sub(z(s, 0), z(s - 1, 2)), l_0));
+        ids.push_back({-1, fr_mul(l_0, fr_sub(one, z(0, 0)))});
+        ids.push_back({-1, fr_mul(fr_sub(fr_mul(z(S - 1, 0), z(S - 1, 0)), z(S - 1, 0)), l_last)});
+        for (uint32_t s = 1; s < S; s++) ids.push_back({-1, fr_mul(fr_sub(z(s, 0), z(s - 1, 2)), l_0)});
         Fr4 delta;
         std::memcpy(delta.l, host::FR_DELTA4, 32);
         for (uint32_t s = 0; s < S; s++) {
@@ -1280,7 +1319,7 @@ Fr4 identities_at_x(const FsProof& p) {
                 right = fr_mul(right, fr_add(fr_add(e, cur), p.gamma));
                 cur = fr_mul(cur, delta);
             }
-            ids.push_back(fr_mul(fr_sub(left, right), active));
+            ids.push_back({-1, fr_mul(fr_sub(left, right), active)});
         }
     }
     // the lookups (logup.rs:405-485): one input expression and one helper each
@@ -1289,21 +1328,35 @@ Fr4 identities_at_x(const FsProof& p) {
         const Fr4 m = p.ev_lk[4 * l], h = p.ev_lk[4 * l + 1], Z = p.ev_lk[4 * l + 2], Zn = p.ev_lk[4 * l + 3];
         const Fr4 f = adv(sh.input_advice), t = fix(sh.table_fixed);
         const Fr4 sel = sh.selector_fixed >= 0 ? fix((uint32_t)sh.selector_fixed) : one;
-        ids.push_back(fr_mul(fr_add(l_0, l_last), Z));
-        ids.push_back(fr_sub(fr_mul(h, fr_add(f, p.beta)), one));
+        ids.push_back({-1, fr_mul(fr_add(l_0, l_last), Z)});
+        ids.push_back({-1, fr_sub(fr_mul(h, fr_add(f, p.beta)), one)});
         Fr4 acc = fr_sub(fr_sub(Zn, Z), fr_mul(sel, h));
         acc = fr_add(fr_mul(acc, fr_add(t, p.beta)), m);
-        ids.push_back(fr_mul(acc, active));
+        ids.push_back({-1, fr_mul(acc, active)});
     }
     // the trashcans (trash.rs:60-86): compressed - (1 - q) trash
     for (size_t t = 0; t < k->trash.size(); t++) {
-        const Fr4 compressed = program_at_x(k->trash[t].program);
+        const Fr4 compressed = program_at_x(k->trash[t].program)[k->trash[t].program.result_idx];
         const Fr4 q = fix(k->trash[t].selector);
-        ids.push_back(fr_sub(compressed, fr_mul(fr_sub(one, q), p.ev_trash[t])));
+        ids.push_back({-1, fr_sub(compressed, fr_mul(fr_sub(one, q), p.ev_trash[t]))});
     }
-    Fr4 acc = host::fr_zero();
-    for (const Fr4& v : ids) acc = fr_add(fr_mul(acc, p.y), v);
-    return acc;
+    return ids;
+}
+
+// compute_linearization_poly's split (linearization/prover.rs:41-86): the
+// identity j of M gets y^(M-1-j); fully evaluated identities add up to the
+// constant C, the others scale their selector's fixed polynomial in L'(X)
+Fr4 linearization_split(const std::vector<std::pair<int32_t, Fr4>>& ids, const Fr4& y,
+                        std::vector<std::pair<uint32_t, Fr4>>* selector_terms) {
+    using namespace host;
+    Fr4 c = host::fr_zero(), pw = host::fr_one();
+    for (size_t j = ids.size(); j-- > 0;) {
+        const Fr4 v = fr_mul(pw, ids[j].second);
+        if (ids[j].first < 0) c = fr_add(c, v);
+        else if (selector_terms) selector_terms->push_back({(uint32_t)ids[j].first, v});
+        pw = fr_mul(pw, y);
+    }
+    return c;
 }
 
 const Fr* open_poly(const FsProof& p, std::pair<int, uint32_t> id) {
@@ -1764,16 +1817,21 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     phase_done(4);
     // ---- 5. evaluations, linearization, x1, x2 ----------------------------
     {
-        // instance evaluations are not in the transcript (no committed
-        // instances): only the self-check's identities at x use them
-        const bool with_instance = (flags & MZK_PROVE_SELF_CHECK) != 0;
+        // the identities at x are evaluated for the self-check, and for keys
+        // with simple selectors, whose linearization polynomial needs them;
+        // instance evaluations (not in the transcript: no committed
+        // instances) only for those
+        const bool check = (flags & MZK_PROVE_SELF_CHECK) != 0;
+        auto need_ids = [&](const PlonkKey* k) { return check || !k->gate_poly_values.empty(); };
         std::vector<EvalTask> tasks;
         for (auto& p : ps) {
             const PlonkKey* k = p.key;
             const Domain* d = k->dom;
             const uint64_t n = k->n;
             for (auto& q : k->advice_queries) tasks.push_back(eval_task(p.adv_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
-            for (auto& q : k->fixed_queries) tasks.push_back(eval_task(k->fixed_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
+            for (auto& q : k->fixed_queries)  // a simple selector's evaluation is one, not computed
+                if (!k->is_simple(q.column))
+                    tasks.push_back(eval_task(k->fixed_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
             for (uint32_t i = 0; i < k->n_perm; i++) tasks.push_back(eval_task(k->perm_coeff[i], n, p.x));
             for (uint32_t s = 0; s < k->n_sets; s++) {
                 tasks.push_back(eval_task(p.z_coeff[s], n, p.x));
@@ -1787,7 +1845,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 tasks.push_back(eval_task(p.Z_coeff[l], n, fr_rot(d, p.x, 1)));
             }
             for (size_t t = 0; t < k->trash.size(); t++) tasks.push_back(eval_task(p.trash_coeff[t], n, p.x));
-            if (with_instance)
+            if (need_ids(k))
                 for (auto& q : k->instance_queries)
                     tasks.push_back(eval_task(p.inst_coeff[q.column], n, fr_rot(d, p.x, q.rotation)));
         }
@@ -1802,15 +1860,19 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 at += m;
             };
             grab(p.ev_adv, k->advice_queries.size());
-            grab(p.ev_fix, k->fixed_queries.size());
+            std::vector<Fr4> fix_written;
+            grab(fix_written, fixed_written(*k));
+            p.ev_fix.clear();
+            for (size_t i = 0, w = 0; i < k->fixed_queries.size(); i++)
+                p.ev_fix.push_back(k->is_simple(k->fixed_queries[i].column) ? host::fr_one() : fix_written[w++]);
             grab(p.ev_pc, k->n_perm);
             grab(p.ev_sets, 3 * (size_t)k->n_sets);
             grab(p.ev_lk, 4 * k->lookups.size());
             grab(p.ev_trash, k->trash.size());
-            grab(p.ev_inst, with_instance ? k->instance_queries.size() : 0);
+            grab(p.ev_inst, need_ids(k) ? k->instance_queries.size() : 0);
             // transcript order (write_evals_to_transcript, permutation / logup evaluate)
             for (auto& v : p.ev_adv) p.tr.write_fr(v);
-            for (auto& v : p.ev_fix) p.tr.write_fr(v);
+            for (auto& v : fix_written) p.tr.write_fr(v);
             for (auto& v : p.ev_pc) p.tr.write_fr(v);
             for (uint32_t s = 0; s < k->n_sets; s++) {
                 p.tr.write_fr(p.ev_sets[3 * s]);
@@ -1827,6 +1889,11 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             for (uint32_t i = 0; i < k->qdeg; i++) {
                 ls.terms.push_back({p.limbs + (size_t)i * k->n, k->n, to_dev(s)});
                 s = fr_mul(s, sf);
+            }
+            if (need_ids(k)) {  // + sum of simple selectors' fixed polynomials times their identities
+                std::vector<std::pair<uint32_t, Fr4>> sel_terms;
+                p.lin_c = linearization_split(identities_at_x(p), p.y, &sel_terms);
+                for (auto& t : sel_terms) ls.terms.push_back({k->fixed_coeff[t.first], k->n, to_dev(t.second)});
             }
             lins.push_back(ls);
             p.x1 = p.tr.squeeze();
@@ -1902,7 +1969,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 // L'(x) = -C holds iff the witness satisfies every identity
                 // (the reference's debug assertion, prover.rs:404-408)
                 const Fr4 lin_x = ev[at++];
-                if (!fr_eq(lin_x, fr_neg(identities_at_x(p)))) {
+                if (!fr_eq(lin_x, fr_neg(p.lin_c))) {
                     set_error("create_proof: request " + std::to_string(j) +
                               ": the witness does not satisfy the circuit (L'(x) != -C)");
                     return ERR_ARG;
@@ -2132,7 +2199,7 @@ int mzk_plonk_key_transcript_layout(const mzk_plonk_key* key, uint8_t* ops, size
     put(MZK_TR_SQUEEZE, 1);                    // y
     put(MZK_TR_WRITE_POINT, k->qdeg);          // quotient limbs
     put(MZK_TR_SQUEEZE, 1);                    // x
-    put(MZK_TR_WRITE_FR, k->advice_queries.size() + k->fixed_queries.size() + k->n_perm + (S ? 3 * S - 1 : 0) +
+    put(MZK_TR_WRITE_FR, k->advice_queries.size() + mzk::fixed_written(*k) + k->n_perm + (S ? 3 * S - 1 : 0) +
                              4 * L + k->trash.size());  // evaluations
     put(MZK_TR_SQUEEZE, 2);                    // x1, x2
     put(MZK_TR_WRITE_POINT, 1);                // f

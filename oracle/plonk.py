@@ -423,6 +423,29 @@ def instance_circuit(k):
     return c
 
 
+def selector_circuit(k):
+    """generic_circuit with q3 a simple selector: its second gate
+    polynomial q3 (d - a^2) is listed with q3 as selector, so q3 is evaluated
+    as one at x, not written to the transcript nor opened, and its fixed
+    polynomial enters the linearization scaled by d(x) - a(x)^2."""
+    c = generic_circuit(k)
+    c["gate_polys"] = [(21, None), (24, 2)]
+    return c
+
+
+def selector_instance(k, seed):
+    """generic_instance with the simple selector q3 boolean: one on the usable
+    rows."""
+    fixed, mapping, adv = generic_instance(k, seed, circuit=selector_circuit(k))
+    n = 1 << k
+    u = n - blinding_factors(selector_circuit(k)) - 1
+    q3 = np.zeros((n, 4), np.uint64)
+    q3[:u] = O.fr_const(0)
+    fixed = list(fixed)
+    fixed[2] = q3
+    return fixed, mapping, adv
+
+
 def trash_circuit(k):
     """generic_circuit with a trashcan (trash.rs): constraint expressions
     d - a^2 and q1 a b + q2 a(wX) - q4 c folded with the trash challenge, the
@@ -683,7 +706,9 @@ def identities(key, ev, ch):
     identity fully evaluated: the gate polynomials, then the permutation
     expressions (permutation.rs:195-290), then each lookup's boundary, helper
     and accumulator expressions (logup.rs:405-485).  ev: evaluations by name;
-    ch: challenges.  Returns the list of identity values."""
+    ch: challenges.  Returns the identities in order, each with the fixed
+    column of its simple selector (None: fully evaluated); a simple
+    selector's evaluation in ev["fixed"] is one (verifier.rs:250-259)."""
     c = key.circuit
     x, xn, beta, gamma, theta = ch["x"], ch["xn"], ch["beta"], ch["gamma"], ch["theta"]
     bf = key.bf
@@ -701,20 +726,24 @@ def identities(key, ev, ch):
             if col_type == 2:
                 return ins[query_index(c.get("instance_queries", []), col, rot)]
             return adv[query_index(c["advice_queries"], col, rot)]
-        out = [program_at(c["gates"], read, ch)]
+        if c.get("gate_polys"):
+            vals = program_at(c["gates"], read, ch, all_values=True)
+            out = [(sel, vals[slot]) for slot, sel in c["gate_polys"]]
+        else:
+            out = [(None, program_at(c["gates"], read, ch))]
     else:
         gf, ga = c["gate_fixed"], c["gate_advice"]
         ql, qr, qm, qo, qc = (fq(i) for i in gf)
         a, b, cc = (aq(i) for i in ga)
-        out = [(ql * a + qr * b + qm * a * b + qo * cc + qc) % R]
+        out = [(None, (ql * a + qr * b + qm * a * b + qo * cc + qc) % R)]
     # permutation
     sets = ev["perm_sets"]
     chunk = c["degree"] - 2
     if sets:
-        out.append(l_0 * (1 - sets[0][0]) % R)
-        out.append((sets[-1][0] * sets[-1][0] - sets[-1][0]) * l_last % R)
+        out.append((None, l_0 * (1 - sets[0][0]) % R))
+        out.append((None, (sets[-1][0] * sets[-1][0] - sets[-1][0]) * l_last % R))
         for i in range(1, len(sets)):
-            out.append((sets[i][0] - sets[i - 1][2]) * l_0 % R)
+            out.append((None, (sets[i][0] - sets[i - 1][2]) * l_0 % R))
         dlt = to_int(O.fr_const(5))
         for si, s in enumerate(sets):
             cols = c["perm_cols"][si * chunk:(si + 1) * chunk]
@@ -729,28 +758,28 @@ def identities(key, ev, ch):
                 e = col_eval(kind, ci)
                 right = right * (e + cur + gamma) % R
                 cur = cur * dlt % R
-            out.append((left - right) * (1 - (l_last + l_blind)) % R)
+            out.append((None, (left - right) * (1 - (l_last + l_blind)) % R))
     # lookups
     for li, lk in enumerate(c["lookups"]):
         m, h, Z, Zn = ev["lookups"][li]
         f = aq(lk["input"])
         table = fq(lk["table"])
         sel = fq(lk["selector"]) if lk["selector"] is not None else 1
-        out.append((l_0 + l_last) * Z % R)
+        out.append((None, (l_0 + l_last) * Z % R))
         fb = (f + beta) % R
-        out.append((h * fb - 1) % R)              # one input: product f+beta, sum of partial products 1
-        out.append(((Zn - Z - sel * h) * (table + beta) + m) * (1 - (l_last + l_blind)) % R)
+        out.append((None, (h * fb - 1) % R))              # one input: product f+beta, sum of partial products 1
+        out.append((None, ((Zn - Z - sel * h) * (table + beta) + m) * (1 - (l_last + l_blind)) % R))
     # trashcans (trash.rs:60-86): compressed - (1 - q) trash
     for ti, tc in enumerate(c.get("trashcans", [])):
         def read(col_type, col, rot):
             qs = (c["fixed_queries"], c["advice_queries"], c.get("instance_queries", []))[col_type]
             return (fix, adv, ins)[col_type][query_index(qs, col, rot)]
         compressed = program_at(tc["program"], read, ch)
-        out.append((compressed - (1 - fq(tc["selector"])) * ev["trash"][ti]) % R)
-    return [v % R for v in out]
+        out.append((None, (compressed - (1 - fq(tc["selector"])) * ev["trash"][ti]) % R))
+    return [(sel, v % R) for sel, v in out]
 
 
-def program_at(graph, read, ch):
+def program_at(graph, read, ch, all_values=False):
     """A flattened program (FlatGraphEvaluator, evaluation.rs:148-213) at one
     point with Python integers: each read is read(col_type, column, rotation)
     (the query's evaluation at x), the previous value zero, the challenge
@@ -768,7 +797,28 @@ def program_at(graph, read, ch):
     for kind, dst, a, b, c in graph["ops"]:
         x, y2, z = vals[a], vals[b], vals[c]
         vals[dst] = [x + y2, x - y2, x * y2, x * x, 2 * x, -x, x * y2 + z][kind] % R
-    return vals[graph["result_idx"]]
+    return vals if all_values else vals[graph["result_idx"]]
+
+
+def simple_selectors(circuit):
+    """The fixed columns of simple selectors (ConstraintSystem::
+    has_simple_selector_col): the selectors of the listed gate polynomials."""
+    return {sel for _, sel in circuit.get("gate_polys", []) if sel is not None}
+
+
+def linearization_split(tagged, y):
+    """compute_linearization_poly's split (linearization/prover.rs:41-86):
+    identity j of M gets y^(M-1-j); the untagged ones sum to the constant C,
+    a tagged one scales its simple selector's fixed polynomial.  Returns
+    (C, [(fixed column, coefficient)])."""
+    c, terms, pw = 0, [], 1
+    for sel, v in reversed(tagged):
+        if sel is None:
+            c = (c + pw * v) % R
+        else:
+            terms.append((sel, pw * v % R))
+        pw = pw * y % R
+    return c, terms
 
 
 def horner(values, y):
@@ -922,10 +972,15 @@ def create_proof(key, advice, blinds, instances=None):
     x = tr.squeeze()
     xn = pow(x, n, R)
     # evaluations (prover.rs:798-868, permutation/prover.rs:270-335, logup/prover.rs:318-352)
+    simple = simple_selectors(c)
     ev = {"advice": [eval_at(adv_c[col], rotate(key, x, rot)) for col, rot in c["advice_queries"]],
-          "fixed": [eval_at(key.fixed_polys[col], rotate(key, x, rot)) for col, rot in c["fixed_queries"]]}
-    for v in ev["advice"] + ev["fixed"]:
+          "fixed": [1 if col in simple else eval_at(key.fixed_polys[col], rotate(key, x, rot))
+                    for col, rot in c["fixed_queries"]]}
+    for v in ev["advice"]:
         tr.write_fr(v)
+    for (col, _), v in zip(c["fixed_queries"], ev["fixed"]):
+        if col not in simple:                                  # a simple selector's is not written
+            tr.write_fr(v)
     ev["perm_common"] = [eval_at(p, x) for p in key.perm_polys]
     for v in ev["perm_common"]:
         tr.write_fr(v)
@@ -948,10 +1003,20 @@ def create_proof(key, advice, blinds, instances=None):
     ev["trash"] = [eval_at(t, x) for t in t_c]                 # trash/prover.rs:80-92
     for v in ev["trash"]:
         tr.write_fr(v)
-    # linearization (linearization/prover.rs:41-86): every identity is a
-    # constant, so L'(X) = -sum_i (x^n - 1) (x^(n-1))^i h_i(X)
+    # linearization (linearization/prover.rs:41-86): L'(X) = sum over the
+    # identities with a simple selector of y^(M-1-j) id_j(x) S_j(X), minus
+    # sum_i (x^n - 1) (x^(n-1))^i h_i(X)
     sf = pow(x, n - 1, R)
-    lin = O.poly_inner_product(limbs, [to_mont(-(xn - 1) * pow(sf, i, R)) for i in range(qdeg)])
+    polys = list(limbs)
+    coefs = [to_mont(-(xn - 1) * pow(sf, i, R)) for i in range(qdeg)]
+    if simple:
+        ev["instance"] = [eval_at(inst_c[col], rotate(key, x, rot)) for col, rot in c.get("instance_queries", [])]
+        ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta, "trash": trash, "y": y}
+        _, terms = linearization_split(identities(key, ev, ch), y)
+        for sel, v in terms:
+            polys.append(key.fixed_polys[sel])
+            coefs.append(to_mont(v))
+    lin = O.poly_inner_product(polys, coefs)
     # queries (prover.rs:871-933)
     q = []
     for col, rot in c["advice_queries"]:
@@ -969,7 +1034,8 @@ def create_proof(key, advice, blinds, instances=None):
     for ti, t in enumerate(t_c):
         q.append((("trash", ti), x, t))
     for col, rot in c["fixed_queries"]:
-        q.append((("fixed", col), rotate(key, x, rot), key.fixed_polys[col]))
+        if col not in simple:                                  # prover.rs:913-918
+            q.append((("fixed", col), rotate(key, x, rot), key.fixed_polys[col]))
     for i, p in enumerate(key.perm_polys):
         q.append((("perm_fixed", i), x, p))
     q.append((("lin",), x, lin))
@@ -1147,8 +1213,9 @@ def _verify(key, proof, s, instances=None):
     x = tr.squeeze()
     sf = pow(x, n - 1, R)
     xn = sf * x % R
+    simple = simple_selectors(c)
     ev = {"advice": [tr.read_fr() for _ in c["advice_queries"]],
-          "fixed": [tr.read_fr() for _ in c["fixed_queries"]]}
+          "fixed": [1 if col in simple else tr.read_fr() for col, _ in c["fixed_queries"]]}
     ev["perm_common"] = [tr.read_fr() for _ in c["perm_cols"]]
     sets = []
     for si in range(S):
@@ -1159,9 +1226,10 @@ def _verify(key, proof, s, instances=None):
     ev["trash"] = [tr.read_fr() for _ in range(T)]
     ev["instance"] = instance_evals(key, instances, x, xn)
     ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta, "trash": trash, "y": y}
-    const = horner(identities(key, ev, ch), y)
+    const, terms = linearization_split(identities(key, ev, ch), y)
     # compute_linearization_commitment (linearization/verifier.rs:27-78)
-    lin_com = pt_lincomb(limb_coms, [(1 - xn) * pow(sf, i, R) for i in range(qdeg)])
+    lin_com = pt_lincomb(limb_coms + [key.fixed_coms[sel] for sel, _ in terms],
+                         [(1 - xn) * pow(sf, i, R) for i in range(qdeg)] + [v for _, v in terms])
     lin_eval = -const % R
     x_next, x_last = rotate(key, x, 1), rotate(key, x, -(bf + 1))
     q = []   # (label, point, commitment, eval)
@@ -1181,7 +1249,8 @@ def _verify(key, proof, s, instances=None):
     for ti in range(T):
         q.append((("trash", ti), x, trash_coms[ti], ev["trash"][ti]))
     for qi, (col, rot) in enumerate(c["fixed_queries"]):
-        q.append((("fixed", col), rotate(key, x, rot), key.fixed_coms[col], ev["fixed"][qi]))
+        if col not in simple:
+            q.append((("fixed", col), rotate(key, x, rot), key.fixed_coms[col], ev["fixed"][qi]))
     for i, com in enumerate(key.perm_coms):
         q.append((("perm_fixed", i), x, com, ev["perm_common"][i]))
     q.append((("lin",), x, lin_com, lin_eval))

@@ -18,7 +18,8 @@ PINNED = b"config-3 circuit: standard gate, copy cycles, range lookup"
 SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.generic_circuit, OP.generic_instance),
           "generic2": (OP.generic2_circuit, OP.generic2_instance),
           "instance": (OP.instance_circuit, OP.instance_instance),
-          "trash": (OP.trash_circuit, OP.trash_instance)}
+          "trash": (OP.trash_circuit, OP.trash_instance),
+          "selector": (OP.selector_circuit, OP.selector_instance)}
 
 
 class Circuit:
@@ -29,8 +30,8 @@ class Circuit:
         configuration), "generic" (two gates with a rotation, two
         permutation sets), "generic2" (generic with a second lookup,
         without a selector), "instance" (generic with an instance column
-        read by a third gate and copied from c) or "trash" (generic with a
-        trashcan)."""
+        read by a third gate and copied from c), "trash" (generic with a
+        trashcan) or "selector" (generic with a simple selector)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)

@@ -278,6 +278,33 @@ def test_trash_circuit_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, bad, bl)], flags=mzk.PROVE_SELF_CHECK)
 
 
+@pytest.mark.parametrize("k", [5, 9])
+def test_simple_selector_proof_equals_oracle(ctx, k):
+    """A simple selector (q3 of the second gate polynomial): its evaluation is
+    one in the identities, it is neither written nor opened, and its fixed
+    polynomial enters the linearization scaled by the gate polynomial at x.
+    The device transcript equals the oracle's and verifies, in a batch and
+    through the proving service, and replays from the layout; a witness
+    breaking the selected gate fails the self-check."""
+    c = Circuit(ctx, k, seed=k + 100, shape="selector")
+    assert c.circuit["gate_polys"][1][1] == 2
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    assert replay(c.key, proof) == proof
+    both = mzk.create_proofs(ctx, [(c.key, c.advice, bl), (c.key, c.advice, c.blinds(6))])
+    assert both[0] == proof and c.verify(both[1])
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = srv.submit(c.key, c.advice, c.blinds(7))
+    assert c.verify(srv.wait(t)[0])
+    srv.close()
+    bad = [a.copy() for a in c.advice]
+    bad[3][1] = OP.to_mont(OP.to_int(bad[3][1]) + 1)          # d != a^2 on a selected row
+    with pytest.raises(mzk.MzkError, match="does not satisfy"):
+        mzk.create_proofs(ctx, [(c.key, bad, bl)], flags=mzk.PROVE_SELF_CHECK)
+
+
 def test_key_files_equal_oracle_and_read_back(ctx, k5):
     """VerifyingKey / ProvingKey files in the three SerdeFormats equal the
     oracle's bytes; a key read from a PK file has the same transcript_repr and
