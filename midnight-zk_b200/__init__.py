@@ -937,7 +937,8 @@ def prover_table_width(k):
     """Width c of the fixed-base window table that made create_proof fastest
     at 2^k rows on a B200 (config-3 circuit, 8 proofs per call; k = 18: no
     table 33.0 ms per proof, c = 15 / 16 / 17 / 18: 28.4 / 27.5 / 27.9 / 29.2
-    ms; k = 20: no table 121.7, c = 18 99.1, c = 20 113.8 ms).  Each MSM of
+    ms; k = 20, 2 per call: no table 121.7, c = 17 / 18 / 19 / 20: 92.5 / 94.9
+    / 99.6 / 113.8 ms).  Each MSM of
     2^k points then adds ceil(255 / c) + 1 table rows of points into one window
     of 2^(c-1) buckets: wider tables mean fewer entries per point but more
     buckets to reduce, and the best width grows with the point count."""
@@ -946,7 +947,7 @@ def prover_table_width(k):
     if k <= 18:
         return 16
     if k <= 20:
-        return 18
+        return 17
     return 20
 
 
