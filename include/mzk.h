@@ -411,6 +411,12 @@ typedef struct { uint32_t column; int32_t rotation; } mzk_query;
  * rotation 0) and whose table expression is one fixed column, with a fixed
  * selector column or none (selector_fixed = -1: the constant one). */
 typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } mzk_lookup_shape;
+/* A lookup of a tuple of advice columns into a tuple of fixed columns (1..4
+ * of each, queried at rotation 0), both compressed with theta by Horner in
+ * the tuple's order as the reference compresses lookup expressions; with
+ * mzk_circuit_desc.lookup_tuples given it replaces the shape's input and
+ * table columns (the shape's selector still applies). */
+typedef struct { uint32_t width; uint32_t input_advice[4]; uint32_t table_fixed[4]; } mzk_lookup_tuple;
 /* The constraint system a key is built for.  Gates: any custom gates as the
  * reference flattens them (`gates`, an mzk_flat_graph whose result is the
  * Horner-in-y combination of every gate polynomial, evaluation.rs:148-213;
@@ -421,8 +427,9 @@ typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } m
  * Permutation columns: kind 0 advice, 1 fixed, 2 instance; sets of degree - 2 columns.
  * The query lists and their order are the reference's (they fix the order
  * of the evaluations in the proof).  Limits: 16 advice, 16 fixed, 16
- * permutation columns (8 sets), at most 4 lookups (each one advice column
- * into one fixed table column; their multiplicities, helpers and aggregators
+ * permutation columns (8 sets), at most 4 lookups (each one advice column,
+ * or a tuple of them, into one fixed table column or a tuple of them; their
+ * multiplicities, helpers and aggregators
  * are committed, evaluated and opened lookup by lookup, as logup/prover.rs
  * does), at most 4 instance columns (the reference's default, without the
  * committed-instances feature: every proof's instance values are absorbed
@@ -460,6 +467,7 @@ typedef struct {
     uint32_t n_gate_polys;
     const uint32_t *gate_poly_values;  /* value slot of each gate polynomial in `gates` */
     const int32_t *gate_poly_selector; /* its simple selector's fixed column, or -1 */
+    const mzk_lookup_tuple *lookup_tuples; /* null, or one per lookup */
 } mzk_circuit_desc;
 /* ParamsKZG's bases (params.rs:83-93) inside one DEVICE G1Affine buffer;
  * table_c > 0: srs is row 0 of a window table of that width and table_rows

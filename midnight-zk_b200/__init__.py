@@ -922,7 +922,13 @@ class CircuitDesc(ctypes.Structure):
                 ("n_instance", ctypes.c_uint32), ("instance_queries", ctypes.c_void_p),
                 ("n_instance_queries", ctypes.c_uint32), ("n_trash", ctypes.c_uint32), ("trash", ctypes.c_void_p),
                 ("n_gate_polys", ctypes.c_uint32), ("gate_poly_values", ctypes.c_void_p),
-                ("gate_poly_selector", ctypes.c_void_p)]
+                ("gate_poly_selector", ctypes.c_void_p), ("lookup_tuples", ctypes.c_void_p)]
+
+
+class LookupTuple(ctypes.Structure):
+    """mzk_lookup_tuple (include/mzk.h)."""
+    _fields_ = [("width", ctypes.c_uint32), ("input_advice", ctypes.c_uint32 * 4),
+                ("table_fixed", ctypes.c_uint32 * 4)]
 
 
 class SrsDesc(ctypes.Structure):
@@ -1019,7 +1025,9 @@ class PlonkKey:
     circuit: dict with degree, blinding_factors, n_advice, n_fixed,
     advice_queries / fixed_queries [(column, rotation)], gate_fixed (5),
     gate_advice (3), perm_cols [(kind 0 advice | 1 fixed | 2 instance,
-    column)], lookups [{"input", "table", "selector" (None: constant one)}],
+    column)], lookups [{"input", "table", "selector" (None: constant one)}]
+    (input and table a column or a list of up to four columns, compressed with
+    theta),
     n_instance and instance_queries [(column, rotation)] (optional),
     trashcans [{"program": flattened program, "selector": fixed column}]
     (optional), gate_polys [(value slot, simple selector fixed column or
@@ -1061,8 +1069,21 @@ class PlonkKey:
         cs.perm_col_index = arr(ctypes.c_uint32, [ci for _, ci in pc])
         lks = circuit["lookups"]
         cs.n_lookups = len(lks)
-        cs.lookups = arr(LookupShape, [LookupShape(lk["input"], lk["table"],
+        cols = lambda v: list(v) if isinstance(v, (list, tuple)) else [v]
+        cs.lookups = arr(LookupShape, [LookupShape(cols(lk["input"])[0], cols(lk["table"])[0],
                                                    -1 if lk["selector"] is None else lk["selector"]) for lk in lks])
+        if any(len(cols(lk["input"])) > 1 or len(cols(lk["table"])) > 1 for lk in lks):
+            tuples = []
+            for lk in lks:
+                ins, tab = cols(lk["input"]), cols(lk["table"])
+                if len(ins) != len(tab) or not 1 <= len(ins) <= 4:
+                    raise MzkError(1, "keygen: a lookup tuple needs 1..4 input and as many table columns")
+                t = LookupTuple()
+                t.width = len(ins)
+                t.input_advice[:len(ins)] = ins
+                t.table_fixed[:len(tab)] = tab
+                tuples.append(t)
+            cs.lookup_tuples = arr(LookupTuple, tuples)
         cs.n_instance = circuit.get("n_instance", 0)
         iq = circuit.get("instance_queries", [])
         cs.instance_queries = arr(Query, [Query(c, r) for c, r in iq])

@@ -127,20 +127,33 @@ __device__ __forceinline__ int cmp_words(const Fr& a, const Fr& b) {
 // compute_multiplicities, counting half (logup/prover.rs:432-445): every
 // selected input row of the usable rows adds one to its table value's count;
 // a value not in the table sets *missing (the reference panics)
-__global__ void k_lookup_count(const Fr* __restrict__ input, const Fr* __restrict__ selector, uint32_t usable,
+// A lookup's input columns (a tuple of up to four, compared element by
+// element against the tuples of the table index)
+struct LookupInputs {
+    const Fr* col[4];
+    uint32_t width;
+};
+__device__ __forceinline__ int cmp_tuple(const Fr* __restrict__ uniq, uint32_t t, const LookupInputs& in, uint32_t i) {
+    for (uint32_t e = 0; e < in.width; e++)
+        if (const int c = cmp_words(uniq[(size_t)t * in.width + e], in.col[e][i])) return c;
+    return 0;
+}
+// (with a tuple, the reference matches the theta-compressed values; the
+// tuples match exactly when those do, up to a collision of probability
+// ~n^2 / r)
+__global__ void k_lookup_count(LookupInputs in, const Fr* __restrict__ selector, uint32_t usable,
                                const Fr* __restrict__ uniq, uint32_t n_uniq, uint32_t* __restrict__ counts,
                                uint32_t* __restrict__ missing) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < usable; i += stride) {
         if (selector && fr_is_zero_dev(selector[i])) continue;
-        const Fr v = input[i];
         uint32_t lo = 0, hi = n_uniq;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (cmp_words(uniq[mid], v) < 0) lo = mid + 1;
+            if (cmp_tuple(uniq, mid, in, i) < 0) lo = mid + 1;
             else hi = mid;
         }
-        if (lo < n_uniq && cmp_words(uniq[lo], v) == 0) atomicAdd(&counts[lo], 1u);
+        if (lo < n_uniq && cmp_tuple(uniq, lo, in, i) == 0) atomicAdd(&counts[lo], 1u);
         else atomicOr(missing, 1u);
     }
 }
@@ -251,8 +264,10 @@ struct PlonkKey {
     // table index of the multiplicity kernels (device)
     struct Lookup {
         mzk_lookup_shape shape = {};
+        uint32_t width = 1;                 // the input and table tuples' length
+        uint32_t in[4] = {}, tab[4] = {};   // advice input and fixed table columns
         uint32_t n_uniq = 0;
-        Fr* uniq = nullptr;       // distinct table values of the usable rows, in the index order
+        Fr* uniq = nullptr;       // distinct table tuples of the usable rows, in the index order (width each)
         uint32_t* uid = nullptr;  // per usable row: its value's index in uniq
         Fr* tinv = nullptr;       // per distinct value: 1 / (its copies in the table)
     };
@@ -424,6 +439,14 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
                         : !queried(cs->instance_queries, cs->n_instance_queries, col))
             return fail("a permutation column is not queried at rotation 0");
     }
+    for (uint32_t i = 0; i < cs->n_lookups && cs->lookup_tuples; i++) {
+        const mzk_lookup_tuple& t = cs->lookup_tuples[i];
+        if (t.width < 1 || t.width > 4) return fail("a lookup tuple has 1..4 columns");
+        for (uint32_t e = 0; e < t.width; e++)
+            if (!queried(cs->advice_queries, cs->n_advice_queries, t.input_advice[e]) ||
+                !queried(cs->fixed_queries, cs->n_fixed_queries, t.table_fixed[e]))
+                return fail("a lookup column is not queried at rotation 0");
+    }
     for (uint32_t i = 0; i < cs->n_lookups; i++) {
         const mzk_lookup_shape& l = cs->lookups[i];
         if (!queried(cs->advice_queries, cs->n_advice_queries, l.input_advice) ||
@@ -498,24 +521,34 @@ void build_lookup_programs(PlonkKey* key) {
     key->lk_reads.clear();
     key->lk_ops.clear();
     key->lk_outputs.clear();
-    std::vector<uint32_t> n_reads(L);
+    std::vector<uint32_t> n_reads(L), n_ops(L), vlen(L), result(L);
     for (uint32_t l = 0; l < L; l++) {
-        const mzk_lookup_shape& sh = key->lookups[l].shape;
-        key->lk_reads.push_back({1, sh.input_advice, 0, 7});
-        key->lk_reads.push_back({0, sh.table_fixed, 0, 8});
-        n_reads[l] = 2;
-        if (sh.selector_fixed >= 0) {
-            key->lk_reads.push_back({0, (uint32_t)sh.selector_fixed, 0, 9});
-            n_reads[l] = 3;
+        const PlonkKey::Lookup& lk = key->lookups[l];
+        const uint32_t w = lk.width, sel_slot = 7 + 2 * w, base = sel_slot + 1;
+        // reads: the inputs at 7.., the table at 7 + w.., the selector after them
+        for (uint32_t e = 0; e < w; e++) key->lk_reads.push_back({1, lk.in[e], 0, 7 + e});
+        for (uint32_t e = 0; e < w; e++) key->lk_reads.push_back({0, lk.tab[e], 0, 7 + w + e});
+        n_reads[l] = 2 * w;
+        if (lk.shape.selector_fixed >= 0) {
+            key->lk_reads.push_back({0, (uint32_t)lk.shape.selector_fixed, 0, sel_slot});
+            n_reads[l]++;
         }
-        key->lk_ops.push_back({MZK_FLAT_MULADD, 10, 0, 3, 7});  // 0 theta + input
-        key->lk_ops.push_back({MZK_FLAT_ADD, 11, 10, 2, 0});    // + beta: the product
-        key->lk_ops.push_back({MZK_FLAT_MULADD, 12, 0, 3, 8});  // 0 theta + table
-        key->lk_ops.push_back({MZK_FLAT_ADD, 13, 12, 2, 0});    // + beta
-        for (uint32_t o : {1u, 11u, 13u, sh.selector_fixed >= 0 ? 9u : 1u}) key->lk_outputs.push_back(o);
+        // theta-Horner of the inputs (from 0 theta + the first), + beta: the
+        // product; the same for the table
+        for (uint32_t e = 0; e < w; e++) key->lk_ops.push_back({MZK_FLAT_MULADD, base + e, e ? base + e - 1 : 0, 3, 7 + e});
+        key->lk_ops.push_back({MZK_FLAT_ADD, base + w, base + w - 1, 2, 0});
+        const uint32_t tb = base + w + 1;
+        for (uint32_t e = 0; e < w; e++)
+            key->lk_ops.push_back({MZK_FLAT_MULADD, tb + e, e ? tb + e - 1 : 0, 3, 7 + w + e});
+        key->lk_ops.push_back({MZK_FLAT_ADD, tb + w, tb + w - 1, 2, 0});
+        n_ops[l] = 2 * w + 2;
+        vlen[l] = tb + w + 1;
+        result[l] = tb + w;
+        for (uint32_t o : {1u, base + w, tb + w, lk.shape.selector_fixed >= 0 ? sel_slot : 1u})
+            key->lk_outputs.push_back(o);
     }
     key->lk_programs.assign(L, mzk_flat_graph{});
-    size_t r0 = 0;
+    size_t r0 = 0, o0 = 0;
     for (uint32_t l = 0; l < L; l++) {
         mzk_flat_graph& g = key->lk_programs[l];
         g.constants = key->lk_consts.data();
@@ -524,16 +557,17 @@ void build_lookup_programs(PlonkKey* key) {
         g.n_rotations = 1;
         g.reads = key->lk_reads.data() + r0;
         g.n_reads = n_reads[l];
-        g.ops = key->lk_ops.data() + 4 * (size_t)l;
-        g.n_ops = 4;
-        g.values_len = 14;
+        g.ops = key->lk_ops.data() + o0;
+        g.n_ops = n_ops[l];
+        g.values_len = vlen[l];
         g.beta_idx = 2;
         g.theta_idx = 3;
         g.trash_challenge_idx = 4;
         g.y_idx = 5;
         g.previous_value_idx = 6;
-        g.result_idx = 13;
+        g.result_idx = result[l];
         r0 += n_reads[l];
+        o0 += n_ops[l];
     }
 }
 
@@ -656,36 +690,55 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     key->perm_index.assign(cs->perm_col_index, cs->perm_col_index + P);
     const uint32_t L = cs->n_lookups;
     key->lookups.resize(L);
-    for (uint32_t l = 0; l < L; l++) key->lookups[l].shape = cs->lookups[l];
+    for (uint32_t l = 0; l < L; l++) {
+        PlonkKey::Lookup& lk = key->lookups[l];
+        lk.shape = cs->lookups[l];
+        if (cs->lookup_tuples) {
+            lk.width = cs->lookup_tuples[l].width;
+            for (uint32_t e = 0; e < lk.width; e++) {
+                lk.in[e] = cs->lookup_tuples[l].input_advice[e];
+                lk.tab[e] = cs->lookup_tuples[l].table_fixed[e];
+            }
+        } else {
+            lk.width = 1;
+            lk.in[0] = lk.shape.input_advice;
+            lk.tab[0] = lk.shape.table_fixed;
+        }
+    }
     key->srs = *srs;
     const uint32_t F = cs->n_fixed, u = key->u;
-    // lookup table indexes (host): the distinct values of each table's usable
-    // rows in the order of the device search, each row's index, 1 / copies
-    std::vector<std::vector<std::array<uint64_t, 4>>> uniq(L);
+    // lookup table indexes (host): the distinct table tuples of the usable
+    // rows in the order of the device search (element by element, each from
+    // its lowest 64-bit word: the map's order), each row's index, 1 / copies
+    std::vector<std::vector<uint64_t>> uniq(L);
     std::vector<std::vector<uint32_t>> uid(L);
     std::vector<std::vector<Fr4>> tinv(L);
     bool need_ones = false;
     size_t uniq_total = 0;
     for (uint32_t l = 0; l < L; l++) {
-        const uint64_t* t = fixed_values[key->lookups[l].shape.table_fixed];
-        std::map<std::array<uint64_t, 4>, uint32_t> count;
-        for (uint32_t i = 0; i < u; i++) count[{t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]}]++;
-        std::map<std::array<uint64_t, 4>, uint32_t> index;
+        const PlonkKey::Lookup& lk = key->lookups[l];
+        auto row_key = [&](uint32_t i) {
+            std::vector<uint64_t> kv(4 * lk.width);
+            for (uint32_t e = 0; e < lk.width; e++) std::memcpy(&kv[4 * e], fixed_values[lk.tab[e]] + 4 * (size_t)i, 32);
+            return kv;
+        };
+        std::map<std::vector<uint64_t>, uint32_t> count;
+        for (uint32_t i = 0; i < u; i++) count[row_key(i)]++;
+        std::map<std::vector<uint64_t>, uint32_t> index;
         for (auto& kv : count) {
-            // the device compares the 64-bit words from the lowest: the map's order
-            index[kv.first] = (uint32_t)uniq[l].size();
-            uniq[l].push_back(kv.first);
+            index[kv.first] = (uint32_t)(uniq[l].size() / (4 * lk.width));
+            uniq[l].insert(uniq[l].end(), kv.first.begin(), kv.first.end());
             tinv[l].push_back(host::fr_inv(host::fr_from_u64(kv.second)));
         }
         uid[l].resize(u);
-        for (uint32_t i = 0; i < u; i++) uid[l][i] = index[{t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]}];
-        key->lookups[l].n_uniq = (uint32_t)uniq[l].size();
-        uniq_total += uniq[l].size();
-        need_ones = need_ones || key->lookups[l].shape.selector_fixed < 0;
+        for (uint32_t i = 0; i < u; i++) uid[l][i] = index[row_key(i)];
+        key->lookups[l].n_uniq = (uint32_t)count.size();
+        uniq_total += (size_t)count.size() * (lk.width + 1);
+        need_ones = need_ones || lk.shape.selector_fixed < 0;
     }
     // one device allocation for the whole key
     const size_t fr_elems = (size_t)F * (2 * n + E) + (size_t)P * (2 * n + E) + 3 * (size_t)E + (need_ones ? n : 0) +
-                            2 * uniq_total;
+                            uniq_total;
     const size_t bytes = fr_elems * sizeof(Fr) + (size_t)u * 4 * L + 256;
     cudaError_t e = cudaMalloc(&key->mem, bytes);
     if (e != cudaSuccess) {
@@ -717,7 +770,7 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     key->l_active = take(E);
     if (need_ones) key->ones = take(n);
     for (auto& lk : key->lookups) {
-        lk.uniq = take(lk.n_uniq);
+        lk.uniq = take((size_t)lk.n_uniq * lk.width);
         lk.tinv = take(lk.n_uniq);
     }
     for (uint32_t l = 0; l < L; l++) key->lookups[l].uid = reinterpret_cast<uint32_t*>(carve) + (size_t)l * u;
@@ -789,13 +842,15 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     }
     for (uint32_t l = 0; l < L; l++) {
         PlonkKey::Lookup& lk = key->lookups[l];
-        MZK_CUDA_CHECK(cudaMemcpyAsync(lk.uniq, uniq[l].data(), uniq[l].size() * 32, cudaMemcpyHostToDevice, st));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(lk.uniq, uniq[l].data(), uniq[l].size() * 8, cudaMemcpyHostToDevice, st));
         MZK_CUDA_CHECK(cudaMemcpyAsync(lk.tinv, tinv[l].data(), tinv[l].size() * 32, cudaMemcpyHostToDevice, st));
         MZK_CUDA_CHECK(cudaMemcpyAsync(lk.uid, uid[l].data(), uid[l].size() * 4, cudaMemcpyHostToDevice, st));
     }
-    // the quotient's built-in lookup term serves a single lookup without
-    // trashcans; otherwise every lookup goes to it as a helper program
-    if (L > 1 || (L && cs->n_trash)) build_lookup_programs(key.get());
+    // the quotient's built-in lookup term serves a single one-column lookup
+    // without trashcans; otherwise every lookup goes to it as a helper program
+    bool tuples = false;
+    for (auto& lk : key->lookups) tuples = tuples || lk.width > 1;
+    if (L > 1 || (L && (cs->n_trash || tuples))) build_lookup_programs(key.get());
     // VK commitments (Lagrange basis) as one batch
     std::vector<BatchItem> items;
     for (uint32_t i = 0; i < F; i++) items.push_back({key->fixed_lag[i], srs->off_lagrange, n});
@@ -1090,6 +1145,7 @@ struct FsProof {
     std::vector<Fr*> trash_lag, trash_coeff, trash_ext;  // trash columns
     // per lookup: multiplicities, helper, aggregator
     std::vector<Fr*> m_lag, m_delta, m_coeff, m_ext, h_lag, h_coeff, h_ext, Z_lag, Z_dd, Z_coeff, Z_ext;
+    std::vector<Fr*> f_lag, t_lag;  // theta-compressed input and table of a tuple lookup (else null)
     std::vector<uint32_t*> counts;
     Fr *limbs = nullptr, *lin = nullptr, *f = nullptr, *fin = nullptr, *pi = nullptr, *tmp_a = nullptr,
        *tmp_b = nullptr;
@@ -1106,7 +1162,7 @@ size_t proof_scratch_elems(const PlonkKey* k) {
     const size_t n = k->n, E = (size_t)1 << k->dom->ext_k, A = k->n_advice, S = k->n_sets;
     const size_t L = k->lookups.size(), O = k->open_sets.size();
     size_t counts = 0;
-    for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8;
+    for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8 + (lk.width > 1 ? 2 * n : 0);
     return (A + k->n_instance + k->trash.size()) * (2 * n + E) + S * (3 * n + E) +
            L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) + k->qdeg * n + (4 + 2 * O + 2) * n + k->n_blinds + counts;
 }
@@ -1322,11 +1378,17 @@ std::vector<std::pair<int32_t, Fr4>> identities_at_x(const FsProof& p) {
             ids.push_back({-1, fr_mul(fr_sub(left, right), active)});
         }
     }
-    // the lookups (logup.rs:405-485): one input expression and one helper each
+    // the lookups (logup.rs:405-485): one input (a column or a theta-compressed
+    // tuple of columns) and one helper each
     for (size_t l = 0; l < k->lookups.size(); l++) {
-        const mzk_lookup_shape& sh = k->lookups[l].shape;
+        const PlonkKey::Lookup& lk = k->lookups[l];
+        const mzk_lookup_shape& sh = lk.shape;
         const Fr4 m = p.ev_lk[4 * l], h = p.ev_lk[4 * l + 1], Z = p.ev_lk[4 * l + 2], Zn = p.ev_lk[4 * l + 3];
-        const Fr4 f = adv(sh.input_advice), t = fix(sh.table_fixed);
+        Fr4 f = host::fr_zero(), t = host::fr_zero();
+        for (uint32_t e = 0; e < lk.width; e++) {
+            f = fr_add(fr_mul(f, p.theta), adv(lk.in[e]));
+            t = fr_add(fr_mul(t, p.theta), fix(lk.tab[e]));
+        }
         const Fr4 sel = sh.selector_fixed >= 0 ? fix((uint32_t)sh.selector_fixed) : one;
         ids.push_back({-1, fr_mul(fr_add(l_0, l_last), Z)});
         ids.push_back({-1, fr_sub(fr_mul(h, fr_add(f, p.beta)), one)});
@@ -1490,6 +1552,9 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             p.h_lag.push_back(take(n)), p.h_coeff.push_back(take(n)), p.h_ext.push_back(take(E));
             p.Z_lag.push_back(take(n)), p.Z_dd.push_back(take(n)), p.Z_coeff.push_back(take(n));
             p.Z_ext.push_back(take(E));
+            const bool tuple = k->lookups[l].width > 1;
+            p.f_lag.push_back(tuple ? take(n) : nullptr);
+            p.t_lag.push_back(tuple ? take(n) : nullptr);
         }
         p.limbs = take((size_t)k->qdeg * n);
         p.lin = take(n), p.f = take(n), p.fin = take(n), p.pi = take(n);
@@ -1574,8 +1639,10 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             const PlonkKey::Lookup& lk = k->lookups[l];
             const Fr* sel = lk.shape.selector_fixed >= 0 ? k->fixed_lag[lk.shape.selector_fixed] : nullptr;
             MZK_CUDA_CHECK(cudaMemsetAsync(p.counts[l], 0, (size_t)lk.n_uniq * 4, st));
-            k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(p.adv_lag[lk.shape.input_advice], sel, u, lk.uniq,
-                                                                 lk.n_uniq, p.counts[l],
+            LookupInputs li{};
+            li.width = lk.width;
+            for (uint32_t e = 0; e < lk.width; e++) li.col[e] = p.adv_lag[lk.in[e]];
+            k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(li, sel, u, lk.uniq, lk.n_uniq, p.counts[l],
                                                                  static_cast<uint32_t*>(dmiss) + j);
             MZK_LAUNCH_CHECK(ctx);
             k_lookup_m<<<grid_of(ctx, u), kThreads, 0, st>>>(p.m_lag[l], lk.uid, p.counts[l], lk.tinv, u);
@@ -1605,6 +1672,28 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     }
     phase_done(2);
     // ---- 3. permutation products, logup helper and aggregator, trash, y --
+    // a tuple lookup's input and table, compressed with theta (Horner in the
+    // tuple's order: the first column gets theta^(w-1)), in the Lagrange basis
+    {
+        std::vector<LinSpec> comp;
+        for (auto& p : ps) {
+            const PlonkKey* k = p.key;
+            for (size_t l = 0; l < k->lookups.size(); l++) {
+                const PlonkKey::Lookup& lk = k->lookups[l];
+                if (lk.width < 2) continue;
+                LinSpec fs{p.f_lag[l], k->n, {}}, ts{p.t_lag[l], k->n, {}};
+                Fr4 pw = host::fr_one();
+                for (uint32_t e = lk.width; e-- > 0;) {
+                    fs.terms.push_back({p.adv_lag[lk.in[e]], k->n, to_dev(pw)});
+                    ts.terms.push_back({k->fixed_lag[lk.tab[e]], k->n, to_dev(pw)});
+                    pw = fr_mul(pw, p.theta);
+                }
+                comp.push_back(fs);
+                comp.push_back(ts);
+            }
+        }
+        MZK_TRY(lincomb_many(ctx, comp, st));
+    }
     items.clear();
     for (auto& p : ps) {
         const PlonkKey* k = p.key;
@@ -1639,7 +1728,9 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         }
         for (size_t l = 0; l < k->lookups.size(); l++) {
             const mzk_lookup_shape& sh = k->lookups[l].shape;
-            const uint64_t* in[1] = {reinterpret_cast<const uint64_t*>(p.adv_lag[sh.input_advice])};
+            const bool tuple = k->lookups[l].width > 1;
+            const uint64_t* in[1] = {
+                reinterpret_cast<const uint64_t*>(tuple ? p.f_lag[l] : p.adv_lag[sh.input_advice])};
             uint64_t* ho[1] = {reinterpret_cast<uint64_t*>(p.h_lag[l])};
             const uint32_t cols[1] = {1};
             mzk_logup_desc ld;
@@ -1647,7 +1738,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             ld.n_chunks = 1;
             ld.chunk_cols = cols;
             ld.inputs = in;
-            ld.table = reinterpret_cast<const uint64_t*>(k->fixed_lag[sh.table_fixed]);
+            ld.table = reinterpret_cast<const uint64_t*>(tuple ? p.t_lag[l] : k->fixed_lag[sh.table_fixed]);
             ld.selector = reinterpret_cast<const uint64_t*>(sh.selector_fixed >= 0 ? k->fixed_lag[sh.selector_fixed]
                                                                                      : k->ones);
             ld.multiplicities = reinterpret_cast<const uint64_t*>(p.m_lag[l]);
@@ -1773,7 +1864,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             q.n_trash = (uint32_t)targs.size();
             q.trash = targs.data();
         }
-        if (L == 1 && targs.empty()) {  // the fused built-in term
+        if (L == 1 && k->lk_programs.empty()) {  // the fused built-in term (one column, no trashcans)
             const mzk_lookup_shape& sh = k->lookups[0].shape;
             q.has_lookup = 1;
             q.lookup_input_advice = sh.input_advice;

@@ -423,6 +423,19 @@ def instance_circuit(k):
     return c
 
 
+def tuple_circuit(k):
+    """generic_circuit whose lookup takes the tuple (a, d) into the tuple
+    (table, table of squares), both compressed with theta, with the selector
+    column: the multi-column table lookup."""
+    c = generic_circuit(k, two_lookups=True)
+    c["lookups"] = [{"input": [0, 3], "table": [4, 6], "selector": 5}]
+    return c
+
+
+def tuple_instance(k, seed):
+    return generic_instance(k, seed, two_lookups=True, circuit=tuple_circuit(k))
+
+
 def selector_circuit(k):
     """generic_circuit with q3 a simple selector: its second gate
     polynomial q3 (d - a^2) is listed with q3 as selector, so q3 is evaluated
@@ -762,8 +775,11 @@ def identities(key, ev, ch):
     # lookups
     for li, lk in enumerate(c["lookups"]):
         m, h, Z, Zn = ev["lookups"][li]
-        f = aq(lk["input"])
-        table = fq(lk["table"])
+        ins, tab = lookup_columns(lk)
+        f = table = 0
+        for e in range(len(ins)):
+            f = (f * theta + aq(ins[e])) % R
+            table = (table * theta + fq(tab[e])) % R
         sel = fq(lk["selector"]) if lk["selector"] is not None else 1
         out.append((None, (l_0 + l_last) * Z % R))
         fb = (f + beta) % R
@@ -919,7 +935,10 @@ def create_proof(key, advice, blinds, instances=None):
     ms = []
     for lk in c["lookups"]:
         sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
-        ms.append(compute_multiplicities(sel, [adv[lk["input"]]], key.fixed_values[lk["table"]], u, take(bf + 1)))
+        ins, tab = lookup_columns(lk)
+        f = adv[ins[0]] if len(ins) == 1 else compress_columns([adv[i] for i in ins], theta)
+        t = key.fixed_values[tab[0]] if len(tab) == 1 else compress_columns([key.fixed_values[i] for i in tab], theta)
+        ms.append(compute_multiplicities(sel, [f], t, u, take(bf + 1)))
     for m in ms:
         tr.write_point(commit(delta(m, 1), srs["delta"]))
     beta = tr.squeeze()
@@ -934,7 +953,10 @@ def create_proof(key, advice, blinds, instances=None):
     hs, Zs = [], []
     for li, lk in enumerate(c["lookups"]):
         sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
-        (h,), Z = O.logup([[adv[lk["input"]]]], key.fixed_values[lk["table"]], sel, ms[li], to_mont(beta), bf,
+        ins, tab = lookup_columns(lk)
+        f = adv[ins[0]] if len(ins) == 1 else compress_columns([adv[i] for i in ins], theta)
+        t = key.fixed_values[tab[0]] if len(tab) == 1 else compress_columns([key.fixed_values[i] for i in tab], theta)
+        (h,), Z = O.logup([[f]], t, sel, ms[li], to_mont(beta), bf,
                           np.stack([to_mont(v) for v in log_bl[li]]))
         hs.append(h)
         Zs.append(Z)
@@ -1086,7 +1108,8 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     d.n_perm_sets, d.perm_z = len(z_e), parr(z_e)
     d.chunk_len, d.blinding_factors = c["degree"] - 2, key.bf
     tcs = c.get("trashcans", [])
-    if len(c["lookups"]) == 1 and not tcs:
+    builtin = len(c["lookups"]) == 1 and not tcs and len(lookup_columns(c["lookups"][0])[0]) == 1
+    if builtin:
         lk = c["lookups"][0]
         d.has_lookup = 1
         d.lookup_input_advice, d.lookup_table_fixed = lk["input"], lk["table"]
@@ -1104,7 +1127,7 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     if c.get("gates") is not None:
         gate_values = O.flat_gates_eval(c["gates"], key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k,
                                         to_mont(beta), to_mont(theta), to_mont(trash), to_mont(y))
-    if len(c["lookups"]) <= 1 and not tcs:
+    if builtin or (not c["lookups"] and not tcs):
         return dom.quotient_eval(d, True, threads, gate_values)
     # several lookups, or trashcans: the gate and permutation terms, then
     # every lookup's terms (evaluation.rs:1034-1090) as single-input helper
@@ -1120,21 +1143,42 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     return dom.divide_by_vanishing_poly(v)
 
 
+def lookup_columns(lk):
+    """(input advice columns, table fixed columns) of a lookup: one column
+    each, or tuples of the same length."""
+    ins = list(lk["input"]) if isinstance(lk["input"], (list, tuple)) else [lk["input"]]
+    tab = list(lk["table"]) if isinstance(lk["table"], (list, tuple)) else [lk["table"]]
+    return ins, tab
+
+
+def compress_columns(cols, theta):
+    """The theta-compression of a tuple of columns (compress_expressions:
+    Horner in the tuple's order, the first column times theta^(w-1))."""
+    w = len(cols)
+    return O.poly_inner_product(list(cols), [to_mont(pow(theta, w - 1 - e, R)) for e in range(w)])
+
+
 def lookup_program(lk):
-    """The helper program of a lookup whose input is one advice column and
-    whose table is one fixed column: values 0, 1 (constants), beta, theta,
-    trash challenge, y, the previous value, the input, table and selector
-    reads; the compressed input and table (0 theta + column) plus beta; the
+    """The helper program of a lookup whose input is one advice column (or a
+    tuple) and whose table is one fixed column (or a tuple): values 0, 1
+    (constants), beta, theta, trash challenge, y, the previous value, the
+    input reads, the table reads, the selector read; the theta-compressed
+    input and table (Horner from 0 theta + the first column) plus beta; the
     sum of partial products of one input is the constant one.  Returns
     (graph, (sum_partial_products, product, table, selector) indices)."""
-    reads = [(1, lk["input"], 0, 7), (0, lk["table"], 0, 8)]
+    ins, tab = lookup_columns(lk)
+    w = len(ins)
+    sel_slot, base = 7 + 2 * w, 8 + 2 * w
+    reads = [(1, c, 0, 7 + e) for e, c in enumerate(ins)] + [(0, c, 0, 7 + w + e) for e, c in enumerate(tab)]
     if lk["selector"] is not None:
-        reads.append((0, lk["selector"], 0, 9))
-    ops = [(6, 10, 0, 3, 7), (0, 11, 10, 2, 0), (6, 12, 0, 3, 8), (0, 13, 12, 2, 0)]
+        reads.append((0, lk["selector"], 0, sel_slot))
+    tb = base + w + 1
+    ops = [(6, base + e, base + e - 1 if e else 0, 3, 7 + e) for e in range(w)] + [(0, base + w, base + w - 1, 2, 0)]
+    ops += [(6, tb + e, tb + e - 1 if e else 0, 3, 7 + w + e) for e in range(w)] + [(0, tb + w, tb + w - 1, 2, 0)]
     graph = {"constants": [np.zeros(4, np.uint64), O.fr_const(0)], "rotations": [0], "reads": reads, "ops": ops,
-             "values_len": 14, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
-             "previous_value_idx": 6, "result_idx": 13}
-    return graph, (1, 11, 13, 9 if lk["selector"] is not None else 1)
+             "values_len": tb + w + 1, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
+             "previous_value_idx": 6, "result_idx": tb + w}
+    return graph, (1, base + w, tb + w, sel_slot if lk["selector"] is not None else 1)
 
 
 def multi_open(key, tr, queries):

@@ -305,6 +305,31 @@ def test_simple_selector_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, bad, bl)], flags=mzk.PROVE_SELF_CHECK)
 
 
+@pytest.mark.parametrize("k", [5, 9])
+def test_tuple_lookup_proof_equals_oracle(ctx, k):
+    """A lookup of the tuple (a, d) into (table, squares): multiplicities by
+    matching tuples against the key's tuple index, the logup helper over the
+    theta-compressed input and table, the quotient's lookup term as a tuple
+    helper program.  The device transcript equals the oracle's and verifies,
+    in a batch and through the proving service; a tuple outside the table is
+    refused."""
+    c = Circuit(ctx, k, seed=k + 110, shape="tuple")
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    both = mzk.create_proofs(ctx, [(c.key, c.advice, bl), (c.key, c.advice, c.blinds(6))])
+    assert both[0] == proof and c.verify(both[1])
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = srv.submit(c.key, c.advice, c.blinds(7))
+    assert c.verify(srv.wait(t)[0])
+    srv.close()
+    bad = [a.copy() for a in c.advice]
+    bad[3][1] = OP.to_mont(OP.to_int(bad[3][1]) + 1)          # (a, d) no longer a row of the table
+    with pytest.raises(mzk.MzkError, match="not in the table"):
+        mzk.create_proofs(ctx, [(c.key, bad, bl)])
+
+
 def test_key_files_equal_oracle_and_read_back(ctx, k5):
     """VerifyingKey / ProvingKey files in the three SerdeFormats equal the
     oracle's bytes; a key read from a PK file has the same transcript_repr and

@@ -218,6 +218,25 @@ def test_simple_selector_proofs_verify():
     assert not OP.verify(key, OP.create_proof(key, bad, bl), OP.to_int(s))
 
 
+def test_tuple_lookup_proofs_verify():
+    """A lookup of the tuple (a, d) into (table, squares), compressed with
+    theta on both sides: the proof verifies; a witness whose tuple is not a
+    table row (d != a^2 on a selected row) is refused by the prover."""
+    k = 5
+    c = OP.tuple_circuit(k)
+    fixed, mapping, adv = OP.tuple_instance(k, 15)
+    s = O.rand_fr(55, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"tuple")
+    bl = [OP.to_int(v) for v in O.rand_fr(65, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl)
+    assert OP.verify(key, proof, OP.to_int(s))
+    bad = [a.copy() for a in adv]
+    bad[3][1] = OP.to_mont(OP.to_int(bad[3][1]) + 1)
+    with pytest.raises(ValueError):
+        OP.create_proof(key, bad, bl)
+
+
 def test_generic_circuit_proofs_verify():
     """Another circuit shape: two gates as one flattened program (with a(wX)),
     four permutation columns in two sets (z of the first set opened at
