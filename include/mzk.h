@@ -411,12 +411,19 @@ typedef struct { uint32_t column; int32_t rotation; } mzk_query;
  * rotation 0) and whose table expression is one fixed column, with a fixed
  * selector column or none (selector_fixed = -1: the constant one). */
 typedef struct { uint32_t input_advice, table_fixed; int32_t selector_fixed; } mzk_lookup_shape;
-/* A lookup of a tuple of advice columns into a tuple of fixed columns (1..4
- * of each, queried at rotation 0), both compressed with theta by Horner in
- * the tuple's order as the reference compresses lookup expressions; with
- * mzk_circuit_desc.lookup_tuples given it replaces the shape's input and
- * table columns (the shape's selector still applies). */
-typedef struct { uint32_t width; uint32_t input_advice[4]; uint32_t table_fixed[4]; } mzk_lookup_tuple;
+/* A lookup of n_inputs parallel tuples of advice columns into one tuple of
+ * fixed columns (width 1..4 columns each, queried at rotation 0; 1..8
+ * inputs), every tuple compressed with theta by Horner in its order as the
+ * reference compresses lookup expressions; the inputs are split into helper
+ * chunks by degree (Argument::chunk_by_degree, logup.rs:223-337: at most
+ * next_pow2(degree - 1) inputs per helper), one helper polynomial each.
+ * With mzk_circuit_desc.lookup_tuples given it replaces the shape's input
+ * and table columns (the shape's selector still applies). */
+typedef struct {
+    uint32_t width, n_inputs;
+    uint32_t input_advice[8][4];
+    uint32_t table_fixed[4];
+} mzk_lookup_tuple;
 /* The constraint system a key is built for.  Gates: any custom gates as the
  * reference flattens them (`gates`, an mzk_flat_graph whose result is the
  * Horner-in-y combination of every gate polynomial, evaluation.rs:148-213;

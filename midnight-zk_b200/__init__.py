@@ -927,8 +927,17 @@ class CircuitDesc(ctypes.Structure):
 
 class LookupTuple(ctypes.Structure):
     """mzk_lookup_tuple (include/mzk.h)."""
-    _fields_ = [("width", ctypes.c_uint32), ("input_advice", ctypes.c_uint32 * 4),
-                ("table_fixed", ctypes.c_uint32 * 4)]
+    _fields_ = [("width", ctypes.c_uint32), ("n_inputs", ctypes.c_uint32),
+                ("input_advice", (ctypes.c_uint32 * 4) * 8), ("table_fixed", ctypes.c_uint32 * 4)]
+
+
+def lookup_columns(lk):
+    """(input tuples, table tuple) of a lookup dict: "input" a column or a
+    tuple (list) of columns, or "inputs" a list of such tuples (parallel
+    inputs); "table" a column or a tuple."""
+    one = lambda v: list(v) if isinstance(v, (list, tuple)) else [v]
+    ins = [one(t) for t in lk["inputs"]] if "inputs" in lk else [one(lk["input"])]
+    return ins, one(lk["table"])
 
 
 class SrsDesc(ctypes.Structure):
@@ -1027,7 +1036,7 @@ class PlonkKey:
     gate_advice (3), perm_cols [(kind 0 advice | 1 fixed | 2 instance,
     column)], lookups [{"input", "table", "selector" (None: constant one)}]
     (input and table a column or a list of up to four columns, compressed with
-    theta),
+    theta; or "inputs", a list of up to eight such input tuples),
     n_instance and instance_queries [(column, rotation)] (optional),
     trashcans [{"program": flattened program, "selector": fixed column}]
     (optional), gate_polys [(value slot, simple selector fixed column or
@@ -1069,18 +1078,18 @@ class PlonkKey:
         cs.perm_col_index = arr(ctypes.c_uint32, [ci for _, ci in pc])
         lks = circuit["lookups"]
         cs.n_lookups = len(lks)
-        cols = lambda v: list(v) if isinstance(v, (list, tuple)) else [v]
-        cs.lookups = arr(LookupShape, [LookupShape(cols(lk["input"])[0], cols(lk["table"])[0],
-                                                   -1 if lk["selector"] is None else lk["selector"]) for lk in lks])
-        if any(len(cols(lk["input"])) > 1 or len(cols(lk["table"])) > 1 for lk in lks):
+        shapes = [lookup_columns(lk) for lk in lks]
+        cs.lookups = arr(LookupShape, [LookupShape(ins[0][0], tab[0], -1 if lk["selector"] is None else lk["selector"])
+                                       for lk, (ins, tab) in zip(lks, shapes)])
+        if any(len(ins) > 1 or len(tab) > 1 for ins, tab in shapes):
             tuples = []
-            for lk in lks:
-                ins, tab = cols(lk["input"]), cols(lk["table"])
-                if len(ins) != len(tab) or not 1 <= len(ins) <= 4:
-                    raise MzkError(1, "keygen: a lookup tuple needs 1..4 input and as many table columns")
+            for ins, tab in shapes:
+                if not 1 <= len(tab) <= 4 or not 1 <= len(ins) <= 8 or any(len(t) != len(tab) for t in ins):
+                    raise MzkError(1, "keygen: a lookup takes 1..8 input tuples of the table tuple's 1..4 columns")
                 t = LookupTuple()
-                t.width = len(ins)
-                t.input_advice[:len(ins)] = ins
+                t.width, t.n_inputs = len(tab), len(ins)
+                for i, tup in enumerate(ins):
+                    t.input_advice[i][:len(tup)] = tup
                 t.table_fixed[:len(tab)] = tab
                 tuples.append(t)
             cs.lookup_tuples = arr(LookupTuple, tuples)

@@ -264,16 +264,23 @@ struct PlonkKey {
     // table index of the multiplicity kernels (device)
     struct Lookup {
         mzk_lookup_shape shape = {};
-        uint32_t width = 1;                 // the input and table tuples' length
-        uint32_t in[4] = {}, tab[4] = {};   // advice input and fixed table columns
+        uint32_t width = 1;                  // the input and table tuples' length
+        uint32_t n_inputs = 1;               // parallel input tuples
+        uint32_t in[8][4] = {}, tab[4] = {}; // advice input tuples and fixed table columns
+        uint32_t per_helper = 1;             // inputs per helper chunk (the last may hold fewer)
+        uint32_t h0 = 0;                     // the first helper's index among all lookups' helpers
+        uint32_t n_helpers() const { return (n_inputs + per_helper - 1) / per_helper; }
+        uint32_t chunk_inputs(uint32_t c) const { return std::min(per_helper, n_inputs - c * per_helper); }
         uint32_t n_uniq = 0;
         Fr* uniq = nullptr;       // distinct table tuples of the usable rows, in the index order (width each)
         uint32_t* uid = nullptr;  // per usable row: its value's index in uniq
         Fr* tinv = nullptr;       // per distinct value: 1 / (its copies in the table)
     };
     std::vector<Lookup> lookups;
+    uint32_t n_helpers = 0;  // helper polynomials of all lookups
     // with more than one lookup the quotient takes them as helper programs
-    // (one per lookup; the single-lookup case uses the fused built-in term)
+    // (one per helper chunk, indexed like the helpers; the single one-column
+    // lookup uses the fused built-in term)
     std::vector<uint64_t> lk_consts;
     std::vector<int32_t> lk_rots;
     std::vector<mzk_column_read> lk_reads;
@@ -320,6 +327,14 @@ struct PlonkKey {
 };
 
 namespace {
+
+// parallel lookup inputs per helper polynomial for inputs of degree one:
+// next_pow2(cs.degree() - 1) (nb_parallel_lookups_per_chunk, logup.rs:168-183)
+uint32_t lookup_per_helper(uint32_t degree) {
+    uint32_t p = 1;
+    while (p < degree - 1) p <<= 1;
+    return p;
+}
 
 Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
     auto fail = [](const std::string& m) {
@@ -442,10 +457,20 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
     for (uint32_t i = 0; i < cs->n_lookups && cs->lookup_tuples; i++) {
         const mzk_lookup_tuple& t = cs->lookup_tuples[i];
         if (t.width < 1 || t.width > 4) return fail("a lookup tuple has 1..4 columns");
-        for (uint32_t e = 0; e < t.width; e++)
-            if (!queried(cs->advice_queries, cs->n_advice_queries, t.input_advice[e]) ||
-                !queried(cs->fixed_queries, cs->n_fixed_queries, t.table_fixed[e]))
+        if (t.n_inputs < 1 || t.n_inputs > 8) return fail("a lookup has 1..8 input tuples");
+        // the helper constraint of a chunk has degree 1 + its inputs, at most
+        // next_pow2(degree - 1) inputs (nb_parallel_lookups_per_chunk,
+        // logup.rs:168-183), within cs.degree() as the reference's degree()
+        // makes it (circuit.rs:2174-2199, logup.rs:186-212)
+        if (t.n_inputs > 1 && lookup_per_helper(cs->degree) + 1 > cs->degree)
+            return fail("parallel lookup inputs need cs.degree() - 1 to be a power of two");
+        for (uint32_t e = 0; e < t.width; e++) {
+            if (!queried(cs->fixed_queries, cs->n_fixed_queries, t.table_fixed[e]))
                 return fail("a lookup column is not queried at rotation 0");
+            for (uint32_t j = 0; j < t.n_inputs; j++)
+                if (!queried(cs->advice_queries, cs->n_advice_queries, t.input_advice[j][e]))
+                    return fail("a lookup column is not queried at rotation 0");
+        }
     }
     for (uint32_t i = 0; i < cs->n_lookups; i++) {
         const mzk_lookup_shape& l = cs->lookups[i];
@@ -499,11 +524,6 @@ void build_open_sets(PlonkKey* key, const std::vector<std::pair<std::pair<int, u
     for (uint32_t i : order) key->open_sets.push_back(sets[i]);
 }
 
-// The helper program of each lookup for the quotient (Evaluator::lookups_flat,
-// evaluation.rs:686-767, for one input expression: the compressed input and
-// table are the columns themselves, the sum of partial products is the
-// constant one).  Values: 0, 1 (constants), beta, theta, trash challenge, y,
-// the previous value, then the input, table and selector reads and the ops.
 // the fixed evaluations a proof writes: every fixed query but those of simple
 // selectors (write_evals_to_transcript, prover.rs:857-862)
 size_t fixed_written(const PlonkKey& k) {
@@ -512,8 +532,17 @@ size_t fixed_written(const PlonkKey& k) {
     return m;
 }
 
+// The helper program of each lookup chunk for the quotient
+// (Evaluator::lookups_flat, evaluation.rs:691-770): every input tuple of the
+// chunk theta-compressed (Horner in the tuple's order) plus beta, f_j; their
+// product; the sum of partial products sum_j prod_{k!=j} f_k (one input: the
+// constant one); for the first chunk also the compressed table plus beta and
+// the selector (the quotient reads those from the first chunk only, as
+// evaluation.rs:1066-1069 does).  The partial products come from prefix and
+// suffix products: the same field values as the reference's per-j loops.
+// Values: 0, 1 (constants), beta, theta, trash challenge, y, the previous
+// value, then the reads and the ops.
 void build_lookup_programs(PlonkKey* key) {
-    const uint32_t L = (uint32_t)key->lookups.size();
     const Fr4 zero = host::fr_zero(), one = host::fr_one();
     key->lk_consts.assign(zero.l, zero.l + 4);
     key->lk_consts.insert(key->lk_consts.end(), one.l, one.l + 4);
@@ -521,53 +550,89 @@ void build_lookup_programs(PlonkKey* key) {
     key->lk_reads.clear();
     key->lk_ops.clear();
     key->lk_outputs.clear();
-    std::vector<uint32_t> n_reads(L), n_ops(L), vlen(L), result(L);
-    for (uint32_t l = 0; l < L; l++) {
-        const PlonkKey::Lookup& lk = key->lookups[l];
-        const uint32_t w = lk.width, sel_slot = 7 + 2 * w, base = sel_slot + 1;
-        // reads: the inputs at 7.., the table at 7 + w.., the selector after them
-        for (uint32_t e = 0; e < w; e++) key->lk_reads.push_back({1, lk.in[e], 0, 7 + e});
-        for (uint32_t e = 0; e < w; e++) key->lk_reads.push_back({0, lk.tab[e], 0, 7 + w + e});
-        n_reads[l] = 2 * w;
-        if (lk.shape.selector_fixed >= 0) {
-            key->lk_reads.push_back({0, (uint32_t)lk.shape.selector_fixed, 0, sel_slot});
-            n_reads[l]++;
+    const uint32_t H = key->n_helpers;
+    std::vector<uint32_t> n_reads(H), n_ops(H), vlen(H), result(H);
+    for (const PlonkKey::Lookup& lk : key->lookups) {
+        for (uint32_t c = 0; c < lk.n_helpers(); c++) {
+            const uint32_t h = lk.h0 + c, w = lk.width, m = lk.chunk_inputs(c), i0 = c * lk.per_helper;
+            const size_t r_start = key->lk_reads.size(), o_start = key->lk_ops.size();
+            uint32_t slot = 7;
+            auto op = [&](uint32_t kind, uint32_t a, uint32_t b, uint32_t cc) {
+                key->lk_ops.push_back({kind, slot, a, b, cc});
+                return slot++;
+            };
+            // reads: the chunk's input tuples, then (first chunk) the table and selector
+            std::vector<uint32_t> in_at(m * w), tab_at(w);
+            for (uint32_t j = 0; j < m; j++)
+                for (uint32_t e = 0; e < w; e++) {
+                    key->lk_reads.push_back({1, lk.in[i0 + j][e], 0, slot});
+                    in_at[j * w + e] = slot++;
+                }
+            uint32_t sel = 1;
+            if (c == 0) {
+                for (uint32_t e = 0; e < w; e++) {
+                    key->lk_reads.push_back({0, lk.tab[e], 0, slot});
+                    tab_at[e] = slot++;
+                }
+                if (lk.shape.selector_fixed >= 0) {
+                    key->lk_reads.push_back({0, (uint32_t)lk.shape.selector_fixed, 0, slot});
+                    sel = slot++;
+                }
+            }
+            // f_j = Horner_theta(tuple j) + beta
+            std::vector<uint32_t> f(m);
+            for (uint32_t j = 0; j < m; j++) {
+                uint32_t acc = 0;
+                for (uint32_t e = 0; e < w; e++) acc = op(MZK_FLAT_MULADD, acc, 3, in_at[j * w + e]);
+                f[j] = op(MZK_FLAT_ADD, acc, 2, 0);
+            }
+            uint32_t table = 1;
+            if (c == 0) {
+                uint32_t acc = 0;
+                for (uint32_t e = 0; e < w; e++) acc = op(MZK_FLAT_MULADD, acc, 3, tab_at[e]);
+                table = op(MZK_FLAT_ADD, acc, 2, 0);
+            }
+            uint32_t product = f[0], spp = 1;
+            if (m > 1) {
+                // pre[j] = f_0 .. f_(j-1), suf[j] = f_(j+1) .. f_(m-1)
+                std::vector<uint32_t> pre(m), suf(m);
+                pre[1] = f[0];
+                for (uint32_t j = 2; j < m; j++) pre[j] = op(MZK_FLAT_MUL, pre[j - 1], f[j - 1], 0);
+                product = op(MZK_FLAT_MUL, pre[m - 1], f[m - 1], 0);
+                suf[m - 2] = f[m - 1];
+                for (uint32_t j = m - 2; j-- > 0;) suf[j] = op(MZK_FLAT_MUL, f[j + 1], suf[j + 1], 0);
+                spp = suf[0];
+                for (uint32_t j = 1; j + 1 < m; j++) spp = op(MZK_FLAT_ADD, spp, op(MZK_FLAT_MUL, pre[j], suf[j], 0), 0);
+                spp = op(MZK_FLAT_ADD, spp, pre[m - 1], 0);
+            }
+            n_reads[h] = (uint32_t)(key->lk_reads.size() - r_start);
+            n_ops[h] = (uint32_t)(key->lk_ops.size() - o_start);
+            vlen[h] = slot;
+            result[h] = spp;
+            for (uint32_t o : {spp, product, table, sel}) key->lk_outputs.push_back(o);
         }
-        // theta-Horner of the inputs (from 0 theta + the first), + beta: the
-        // product; the same for the table
-        for (uint32_t e = 0; e < w; e++) key->lk_ops.push_back({MZK_FLAT_MULADD, base + e, e ? base + e - 1 : 0, 3, 7 + e});
-        key->lk_ops.push_back({MZK_FLAT_ADD, base + w, base + w - 1, 2, 0});
-        const uint32_t tb = base + w + 1;
-        for (uint32_t e = 0; e < w; e++)
-            key->lk_ops.push_back({MZK_FLAT_MULADD, tb + e, e ? tb + e - 1 : 0, 3, 7 + w + e});
-        key->lk_ops.push_back({MZK_FLAT_ADD, tb + w, tb + w - 1, 2, 0});
-        n_ops[l] = 2 * w + 2;
-        vlen[l] = tb + w + 1;
-        result[l] = tb + w;
-        for (uint32_t o : {1u, base + w, tb + w, lk.shape.selector_fixed >= 0 ? sel_slot : 1u})
-            key->lk_outputs.push_back(o);
     }
-    key->lk_programs.assign(L, mzk_flat_graph{});
+    key->lk_programs.assign(H, mzk_flat_graph{});
     size_t r0 = 0, o0 = 0;
-    for (uint32_t l = 0; l < L; l++) {
-        mzk_flat_graph& g = key->lk_programs[l];
+    for (uint32_t h = 0; h < H; h++) {
+        mzk_flat_graph& g = key->lk_programs[h];
         g.constants = key->lk_consts.data();
         g.n_constants = 2;
         g.rotations = key->lk_rots.data();
         g.n_rotations = 1;
         g.reads = key->lk_reads.data() + r0;
-        g.n_reads = n_reads[l];
+        g.n_reads = n_reads[h];
         g.ops = key->lk_ops.data() + o0;
-        g.n_ops = n_ops[l];
-        g.values_len = vlen[l];
+        g.n_ops = n_ops[h];
+        g.values_len = vlen[h];
         g.beta_idx = 2;
         g.theta_idx = 3;
         g.trash_challenge_idx = 4;
         g.y_idx = 5;
         g.previous_value_idx = 6;
-        g.result_idx = result[l];
-        r0 += n_reads[l];
-        o0 += n_ops[l];
+        g.result_idx = result[h];
+        r0 += n_reads[h];
+        o0 += n_ops[h];
     }
 }
 
@@ -694,16 +759,21 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         PlonkKey::Lookup& lk = key->lookups[l];
         lk.shape = cs->lookups[l];
         if (cs->lookup_tuples) {
-            lk.width = cs->lookup_tuples[l].width;
+            const mzk_lookup_tuple& t = cs->lookup_tuples[l];
+            lk.width = t.width;
+            lk.n_inputs = t.n_inputs;
             for (uint32_t e = 0; e < lk.width; e++) {
-                lk.in[e] = cs->lookup_tuples[l].input_advice[e];
-                lk.tab[e] = cs->lookup_tuples[l].table_fixed[e];
+                for (uint32_t j = 0; j < lk.n_inputs; j++) lk.in[j][e] = t.input_advice[j][e];
+                lk.tab[e] = t.table_fixed[e];
             }
         } else {
             lk.width = 1;
-            lk.in[0] = lk.shape.input_advice;
+            lk.in[0][0] = lk.shape.input_advice;
             lk.tab[0] = lk.shape.table_fixed;
         }
+        lk.per_helper = lookup_per_helper(cs->degree);
+        lk.h0 = key->n_helpers;
+        key->n_helpers += lk.n_helpers();
     }
     key->srs = *srs;
     const uint32_t F = cs->n_fixed, u = key->u;
@@ -847,9 +917,9 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         MZK_CUDA_CHECK(cudaMemcpyAsync(lk.uid, uid[l].data(), uid[l].size() * 4, cudaMemcpyHostToDevice, st));
     }
     // the quotient's built-in lookup term serves a single one-column lookup
-    // without trashcans; otherwise every lookup goes to it as a helper program
+    // without trashcans; otherwise every lookup goes to it as helper programs
     bool tuples = false;
-    for (auto& lk : key->lookups) tuples = tuples || lk.width > 1;
+    for (auto& lk : key->lookups) tuples = tuples || lk.width > 1 || lk.n_inputs > 1;
     if (L > 1 || (L && (cs->n_trash || tuples))) build_lookup_programs(key.get());
     // VK commitments (Lagrange basis) as one batch
     std::vector<BatchItem> items;
@@ -875,9 +945,10 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
         qs.push_back({{PlonkKey::P_PERM_Z, s}, 1});
     }
     for (uint32_t s = key->n_sets; s-- > 1;) qs.push_back({{PlonkKey::P_PERM_Z, s - 1}, key->last_rot()});
-    for (uint32_t l = 0; l < L; l++) {  // logup Evaluated::open per lookup
+    for (uint32_t l = 0; l < L; l++) {  // logup Evaluated::open per lookup (logup/prover.rs:357-392)
         qs.push_back({{PlonkKey::P_M, l}, 0});
-        qs.push_back({{PlonkKey::P_H, l}, 0});
+        for (uint32_t c = 0; c < key->lookups[l].n_helpers(); c++)
+            qs.push_back({{PlonkKey::P_H, key->lookups[l].h0 + c}, 0});
         qs.push_back({{PlonkKey::P_AGG, l}, 0});
         qs.push_back({{PlonkKey::P_AGG, l}, 1});
     }
@@ -889,8 +960,9 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     build_open_sets(key.get(), qs);
     const uint32_t S = key->n_sets;
     const size_t T = cs->n_trash;
-    const size_t points = cs->n_advice + L + S + 2 * L + T + key->qdeg + 2;
-    const size_t scalars = key->advice_queries.size() + fixed_written(*key) + P + (S ? 3 * S - 1 : 0) + 4 * L + T +
+    const size_t H = key->n_helpers;
+    const size_t points = cs->n_advice + L + S + H + L + T + key->qdeg + 2;
+    const size_t scalars = key->advice_queries.size() + fixed_written(*key) + P + (S ? 3 * S - 1 : 0) + 3 * L + H + T +
                            key->open_sets.size();
     key->proof_len = 48 * points + 32 * scalars;
     key->n_blinds = (size_t)cs->n_advice * (key->bf + 1) + L * (key->bf + 1) + (size_t)S * key->bf + L * key->bf +
@@ -1143,9 +1215,11 @@ struct FsProof {
     std::vector<Fr*> adv_lag, adv_coeff, adv_ext, z_lag, z_delta, z_coeff, z_ext, q, fdiv;
     std::vector<Fr*> inst_lag, inst_coeff, inst_ext;  // instance columns (zero past their values)
     std::vector<Fr*> trash_lag, trash_coeff, trash_ext;  // trash columns
-    // per lookup: multiplicities, helper, aggregator
+    // per lookup: multiplicities and aggregator; per helper (Lookup::h0 + chunk): helper
     std::vector<Fr*> m_lag, m_delta, m_coeff, m_ext, h_lag, h_coeff, h_ext, Z_lag, Z_dd, Z_coeff, Z_ext;
-    std::vector<Fr*> f_lag, t_lag;  // theta-compressed input and table of a tuple lookup (else null)
+    // theta-compressed inputs (per input tuple) and table of a tuple lookup (else empty / null)
+    std::vector<std::vector<Fr*>> f_lag;
+    std::vector<Fr*> t_lag;
     std::vector<uint32_t*> counts;
     Fr *limbs = nullptr, *lin = nullptr, *f = nullptr, *fin = nullptr, *pi = nullptr, *tmp_a = nullptr,
        *tmp_b = nullptr;
@@ -1162,9 +1236,10 @@ size_t proof_scratch_elems(const PlonkKey* k) {
     const size_t n = k->n, E = (size_t)1 << k->dom->ext_k, A = k->n_advice, S = k->n_sets;
     const size_t L = k->lookups.size(), O = k->open_sets.size();
     size_t counts = 0;
-    for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8 + (lk.width > 1 ? 2 * n : 0);
+    for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8 + (lk.width > 1 ? (lk.n_inputs + 1) * n : 0);
     return (A + k->n_instance + k->trash.size()) * (2 * n + E) + S * (3 * n + E) +
-           L * ((3 * n + E) + (2 * n + E) + (3 * n + E)) + k->qdeg * n + (4 + 2 * O + 2) * n + k->n_blinds + counts;
+           L * ((3 * n + E) + (3 * n + E)) + k->n_helpers * (2 * n + E) + k->qdeg * n + (4 + 2 * O + 2) * n +
+           k->n_blinds + counts;
 }
 
 Status eval_many(Context* ctx, const std::vector<EvalTask>& in, std::vector<Fr4>& results, cudaStream_t st) {
@@ -1378,23 +1453,42 @@ std::vector<std::pair<int32_t, Fr4>> identities_at_x(const FsProof& p) {
             ids.push_back({-1, fr_mul(fr_sub(left, right), active)});
         }
     }
-    // the lookups (logup.rs:405-485): one input (a column or a theta-compressed
-    // tuple of columns) and one helper each
-    for (size_t l = 0; l < k->lookups.size(); l++) {
+    // the lookups (Evaluated::expressions, logup.rs:405-485): the boundary,
+    // one helper constraint per chunk of input tuples (each a column or a
+    // theta-compressed tuple of columns), the accumulator
+    for (size_t l = 0, e0 = 0; l < k->lookups.size(); l++) {
         const PlonkKey::Lookup& lk = k->lookups[l];
         const mzk_lookup_shape& sh = lk.shape;
-        const Fr4 m = p.ev_lk[4 * l], h = p.ev_lk[4 * l + 1], Z = p.ev_lk[4 * l + 2], Zn = p.ev_lk[4 * l + 3];
-        Fr4 f = host::fr_zero(), t = host::fr_zero();
-        for (uint32_t e = 0; e < lk.width; e++) {
-            f = fr_add(fr_mul(f, p.theta), adv(lk.in[e]));
-            t = fr_add(fr_mul(t, p.theta), fix(lk.tab[e]));
-        }
+        const uint32_t H = lk.n_helpers();
+        const Fr4 m = p.ev_lk[e0], Z = p.ev_lk[e0 + 1 + H], Zn = p.ev_lk[e0 + 2 + H];
+        Fr4 t = host::fr_zero();
+        for (uint32_t e = 0; e < lk.width; e++) t = fr_add(fr_mul(t, p.theta), fix(lk.tab[e]));
         const Fr4 sel = sh.selector_fixed >= 0 ? fix((uint32_t)sh.selector_fixed) : one;
         ids.push_back({-1, fr_mul(fr_add(l_0, l_last), Z)});
-        ids.push_back({-1, fr_sub(fr_mul(h, fr_add(f, p.beta)), one)});
-        Fr4 acc = fr_sub(fr_sub(Zn, Z), fr_mul(sel, h));
+        Fr4 sum_h = host::fr_zero();
+        for (uint32_t c = 0; c < H; c++) {
+            const Fr4 h = p.ev_lk[e0 + 1 + c];
+            std::vector<Fr4> fb;
+            for (uint32_t j = c * lk.per_helper; j < c * lk.per_helper + lk.chunk_inputs(c); j++) {
+                Fr4 f = host::fr_zero();
+                for (uint32_t e = 0; e < lk.width; e++) f = fr_add(fr_mul(f, p.theta), adv(lk.in[j][e]));
+                fb.push_back(fr_add(f, p.beta));
+            }
+            Fr4 product = one, spp = host::fr_zero();
+            for (size_t j = 0; j < fb.size(); j++) {
+                Fr4 partial = one;
+                for (size_t i = 0; i < fb.size(); i++)
+                    if (i != j) partial = fr_mul(partial, fb[i]);
+                spp = fr_add(spp, partial);
+                product = fr_mul(product, fb[j]);
+            }
+            ids.push_back({-1, fr_sub(fr_mul(h, product), spp)});
+            sum_h = fr_add(sum_h, h);
+        }
+        Fr4 acc = fr_sub(fr_sub(Zn, Z), fr_mul(sel, sum_h));
         acc = fr_add(fr_mul(acc, fr_add(t, p.beta)), m);
         ids.push_back({-1, fr_mul(acc, active)});
+        e0 += 3 + H;
     }
     // the trashcans (trash.rs:60-86): compressed - (1 - q) trash
     for (size_t t = 0; t < k->trash.size(); t++) {
@@ -1549,13 +1643,15 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         for (size_t l = 0; l < k->lookups.size(); l++) {
             p.m_lag.push_back(take(n)), p.m_delta.push_back(take(n)), p.m_coeff.push_back(take(n));
             p.m_ext.push_back(take(E));
-            p.h_lag.push_back(take(n)), p.h_coeff.push_back(take(n)), p.h_ext.push_back(take(E));
             p.Z_lag.push_back(take(n)), p.Z_dd.push_back(take(n)), p.Z_coeff.push_back(take(n));
             p.Z_ext.push_back(take(E));
-            const bool tuple = k->lookups[l].width > 1;
-            p.f_lag.push_back(tuple ? take(n) : nullptr);
-            p.t_lag.push_back(tuple ? take(n) : nullptr);
+            const PlonkKey::Lookup& lk = k->lookups[l];
+            p.f_lag.emplace_back();
+            for (uint32_t j = 0; lk.width > 1 && j < lk.n_inputs; j++) p.f_lag.back().push_back(take(n));
+            p.t_lag.push_back(lk.width > 1 ? take(n) : nullptr);
         }
+        for (uint32_t h = 0; h < k->n_helpers; h++)
+            p.h_lag.push_back(take(n)), p.h_coeff.push_back(take(n)), p.h_ext.push_back(take(E));
         p.limbs = take((size_t)k->qdeg * n);
         p.lin = take(n), p.f = take(n), p.fin = take(n), p.pi = take(n);
         for (size_t s = 0; s < k->open_sets.size(); s++) {
@@ -1639,12 +1735,14 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             const PlonkKey::Lookup& lk = k->lookups[l];
             const Fr* sel = lk.shape.selector_fixed >= 0 ? k->fixed_lag[lk.shape.selector_fixed] : nullptr;
             MZK_CUDA_CHECK(cudaMemsetAsync(p.counts[l], 0, (size_t)lk.n_uniq * 4, st));
-            LookupInputs li{};
-            li.width = lk.width;
-            for (uint32_t e = 0; e < lk.width; e++) li.col[e] = p.adv_lag[lk.in[e]];
-            k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(li, sel, u, lk.uniq, lk.n_uniq, p.counts[l],
-                                                                 static_cast<uint32_t*>(dmiss) + j);
-            MZK_LAUNCH_CHECK(ctx);
+            for (uint32_t i = 0; i < lk.n_inputs; i++) {  // every input tuple counts into one m
+                LookupInputs li{};
+                li.width = lk.width;
+                for (uint32_t e = 0; e < lk.width; e++) li.col[e] = p.adv_lag[lk.in[i][e]];
+                k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(li, sel, u, lk.uniq, lk.n_uniq, p.counts[l],
+                                                                     static_cast<uint32_t*>(dmiss) + j);
+                MZK_LAUNCH_CHECK(ctx);
+            }
             k_lookup_m<<<grid_of(ctx, u), kThreads, 0, st>>>(p.m_lag[l], lk.uid, p.counts[l], lk.tinv, u);
             MZK_LAUNCH_CHECK(ctx);
             MZK_CUDA_CHECK(cudaMemcpyAsync(p.m_lag[l] + u, p.d_blinds + p.off_mult + l * (k->bf + 1),
@@ -1672,8 +1770,9 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     }
     phase_done(2);
     // ---- 3. permutation products, logup helper and aggregator, trash, y --
-    // a tuple lookup's input and table, compressed with theta (Horner in the
-    // tuple's order: the first column gets theta^(w-1)), in the Lagrange basis
+    // a tuple lookup's input tuples and table, compressed with theta (Horner
+    // in the tuple's order: the first column gets theta^(w-1)), in the
+    // Lagrange basis
     {
         std::vector<LinSpec> comp;
         for (auto& p : ps) {
@@ -1681,15 +1780,17 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             for (size_t l = 0; l < k->lookups.size(); l++) {
                 const PlonkKey::Lookup& lk = k->lookups[l];
                 if (lk.width < 2) continue;
-                LinSpec fs{p.f_lag[l], k->n, {}}, ts{p.t_lag[l], k->n, {}};
-                Fr4 pw = host::fr_one();
-                for (uint32_t e = lk.width; e-- > 0;) {
-                    fs.terms.push_back({p.adv_lag[lk.in[e]], k->n, to_dev(pw)});
-                    ts.terms.push_back({k->fixed_lag[lk.tab[e]], k->n, to_dev(pw)});
-                    pw = fr_mul(pw, p.theta);
-                }
-                comp.push_back(fs);
+                std::vector<Fr> pw(lk.width);
+                Fr4 w = host::fr_one();
+                for (uint32_t e = lk.width; e-- > 0;) pw[e] = to_dev(w), w = fr_mul(w, p.theta);
+                LinSpec ts{p.t_lag[l], k->n, {}};
+                for (uint32_t e = 0; e < lk.width; e++) ts.terms.push_back({k->fixed_lag[lk.tab[e]], k->n, pw[e]});
                 comp.push_back(ts);
+                for (uint32_t i = 0; i < lk.n_inputs; i++) {
+                    LinSpec fs{p.f_lag[l][i], k->n, {}};
+                    for (uint32_t e = 0; e < lk.width; e++) fs.terms.push_back({p.adv_lag[lk.in[i][e]], k->n, pw[e]});
+                    comp.push_back(fs);
+                }
             }
         }
         MZK_TRY(lincomb_many(ctx, comp, st));
@@ -1727,17 +1828,24 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             }
         }
         for (size_t l = 0; l < k->lookups.size(); l++) {
-            const mzk_lookup_shape& sh = k->lookups[l].shape;
-            const bool tuple = k->lookups[l].width > 1;
-            const uint64_t* in[1] = {
-                reinterpret_cast<const uint64_t*>(tuple ? p.f_lag[l] : p.adv_lag[sh.input_advice])};
-            uint64_t* ho[1] = {reinterpret_cast<uint64_t*>(p.h_lag[l])};
-            const uint32_t cols[1] = {1};
+            const PlonkKey::Lookup& lk = k->lookups[l];
+            const mzk_lookup_shape& sh = lk.shape;
+            const bool tuple = lk.width > 1;
+            const uint32_t H = lk.n_helpers();
+            std::vector<const uint64_t*> in(lk.n_inputs);
+            for (uint32_t i = 0; i < lk.n_inputs; i++)
+                in[i] = reinterpret_cast<const uint64_t*>(tuple ? p.f_lag[l][i] : p.adv_lag[lk.in[i][0]]);
+            std::vector<uint64_t*> ho(H);
+            std::vector<uint32_t> cols(H);
+            for (uint32_t c = 0; c < H; c++) {
+                ho[c] = reinterpret_cast<uint64_t*>(p.h_lag[lk.h0 + c]);
+                cols[c] = lk.chunk_inputs(c);
+            }
             mzk_logup_desc ld;
             std::memset(&ld, 0, sizeof(ld));
-            ld.n_chunks = 1;
-            ld.chunk_cols = cols;
-            ld.inputs = in;
+            ld.n_chunks = H;
+            ld.chunk_cols = cols.data();
+            ld.inputs = in.data();
             ld.table = reinterpret_cast<const uint64_t*>(tuple ? p.t_lag[l] : k->fixed_lag[sh.table_fixed]);
             ld.selector = reinterpret_cast<const uint64_t*>(sh.selector_fixed >= 0 ? k->fixed_lag[sh.selector_fixed]
                                                                                      : k->ones);
@@ -1745,18 +1853,19 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             ld.blinding_factors = k->bf;
             ld.blinds = p.req->blinds + 4 * (p.off_logup + l * k->bf);
             std::memcpy(ld.beta, p.beta.l, 32);
-            ld.helpers_out = ho;
+            ld.helpers_out = ho.data();
             ld.aggregator_out = reinterpret_cast<uint64_t*>(p.Z_lag[l]);
             MZK_TRY(logup_device(ctx, k->dom, &ld, st));
             MZK_TRY(delta_device(ctx, p.Z_lag[l], p.Z_dd[l], n, 2, st));
-            items.push_back({p.h_lag[l], k->srs.off_lagrange, n});
+            // per lookup its helpers, then its aggregator (prover.rs:221-227)
+            for (uint32_t c = 0; c < H; c++) items.push_back({p.h_lag[lk.h0 + c], k->srs.off_lagrange, n});
             items.push_back({p.Z_dd[l], k->srs.off_lagrange_double_delta, n});
         }
     }
     MZK_TRY(msm());
     for (size_t j = 0, at = 0; j < count; j++) {
         FsProof& p = ps[j];
-        const size_t m = p.key->n_sets + 2 * p.key->lookups.size();
+        const size_t m = p.key->n_sets + p.key->n_helpers + p.key->lookups.size();
         write_points(p, &res[18 * at], m);
         at += m;
         p.trash = p.tr.squeeze();
@@ -1817,9 +1926,14 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             ex.push_back(p.z_ext[s]);
         }
         for (size_t l = 0; l < k->lookups.size(); l++) {
-            lag.insert(lag.end(), {p.m_lag[l], p.h_lag[l], p.Z_lag[l]});
-            co.insert(co.end(), {p.m_coeff[l], p.h_coeff[l], p.Z_coeff[l]});
-            ex.insert(ex.end(), {p.m_ext[l], p.h_ext[l], p.Z_ext[l]});
+            lag.insert(lag.end(), {p.m_lag[l], p.Z_lag[l]});
+            co.insert(co.end(), {p.m_coeff[l], p.Z_coeff[l]});
+            ex.insert(ex.end(), {p.m_ext[l], p.Z_ext[l]});
+        }
+        for (uint32_t h = 0; h < k->n_helpers; h++) {
+            lag.push_back(p.h_lag[h]);
+            co.push_back(p.h_coeff[h]);
+            ex.push_back(p.h_ext[h]);
         }
         MZK_TRY(ntt_sequence(ctx, d, lag.data(), co.data(), ex.data(), (int)lag.size(),
                              !(flags & MZK_PROVE_NO_GRAPHS), st));
@@ -1852,7 +1966,8 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         q.chunk_len = k->chunk;
         q.blinding_factors = k->bf;
         const size_t L = k->lookups.size();
-        std::vector<const uint64_t*> hext(L);
+        std::vector<const uint64_t*> hext(k->n_helpers);
+        for (uint32_t h = 0; h < k->n_helpers; h++) hext[h] = reinterpret_cast<const uint64_t*>(p.h_ext[h]);
         std::vector<mzk_lookup_arg> largs(L);
         std::vector<mzk_trash_arg> targs(k->trash.size());
         for (size_t t = 0; t < k->trash.size(); t++) {
@@ -1873,13 +1988,13 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             q.lookup_h = reinterpret_cast<const uint64_t*>(p.h_ext[0]);
             q.lookup_z = reinterpret_cast<const uint64_t*>(p.Z_ext[0]);
             q.lookup_m = reinterpret_cast<const uint64_t*>(p.m_ext[0]);
-        } else if (L >= 1) {  // one helper program per lookup
+        } else if (L >= 1) {  // one helper program per chunk
             for (size_t l = 0; l < L; l++) {
-                hext[l] = reinterpret_cast<const uint64_t*>(p.h_ext[l]);
-                largs[l].n_helpers = 1;
-                largs[l].programs = &k->lk_programs[l];
-                largs[l].outputs = &k->lk_outputs[4 * l];
-                largs[l].helpers = &hext[l];
+                const PlonkKey::Lookup& lk = k->lookups[l];
+                largs[l].n_helpers = lk.n_helpers();
+                largs[l].programs = &k->lk_programs[lk.h0];
+                largs[l].outputs = &k->lk_outputs[4 * (size_t)lk.h0];
+                largs[l].helpers = &hext[lk.h0];
                 largs[l].aggregator = reinterpret_cast<const uint64_t*>(p.Z_ext[l]);
                 largs[l].multiplicities = reinterpret_cast<const uint64_t*>(p.m_ext[l]);
             }
@@ -1929,9 +2044,10 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 tasks.push_back(eval_task(p.z_coeff[s], n, fr_rot(d, p.x, 1)));
                 tasks.push_back(eval_task(p.z_coeff[s], n, fr_rot(d, p.x, k->last_rot())));
             }
-            for (size_t l = 0; l < k->lookups.size(); l++) {
+            for (size_t l = 0; l < k->lookups.size(); l++) {  // Committed::evaluate (logup/prover.rs:318-355)
                 tasks.push_back(eval_task(p.m_coeff[l], n, p.x));
-                tasks.push_back(eval_task(p.h_coeff[l], n, p.x));
+                for (uint32_t c = 0; c < k->lookups[l].n_helpers(); c++)
+                    tasks.push_back(eval_task(p.h_coeff[k->lookups[l].h0 + c], n, p.x));
                 tasks.push_back(eval_task(p.Z_coeff[l], n, p.x));
                 tasks.push_back(eval_task(p.Z_coeff[l], n, fr_rot(d, p.x, 1)));
             }
@@ -1958,7 +2074,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 p.ev_fix.push_back(k->is_simple(k->fixed_queries[i].column) ? host::fr_one() : fix_written[w++]);
             grab(p.ev_pc, k->n_perm);
             grab(p.ev_sets, 3 * (size_t)k->n_sets);
-            grab(p.ev_lk, 4 * k->lookups.size());
+            grab(p.ev_lk, 3 * k->lookups.size() + k->n_helpers);
             grab(p.ev_trash, k->trash.size());
             grab(p.ev_inst, need_ids(k) ? k->instance_queries.size() : 0);
             // transcript order (write_evals_to_transcript, permutation / logup evaluate)
@@ -2284,14 +2400,14 @@ int mzk_plonk_key_transcript_layout(const mzk_plonk_key* key, uint8_t* ops, size
     put(MZK_TR_SQUEEZE, 1);                    // theta
     put(MZK_TR_WRITE_POINT, L);                // multiplicities
     put(MZK_TR_SQUEEZE, 2);                    // beta, gamma
-    put(MZK_TR_WRITE_POINT, S + 2 * L);        // permutation products, logup helper and aggregator
+    put(MZK_TR_WRITE_POINT, S + k->n_helpers + L);  // permutation products, logup helpers and aggregators
     put(MZK_TR_SQUEEZE, 1);                    // trash challenge
     put(MZK_TR_WRITE_POINT, k->trash.size());  // trash columns
     put(MZK_TR_SQUEEZE, 1);                    // y
     put(MZK_TR_WRITE_POINT, k->qdeg);          // quotient limbs
     put(MZK_TR_SQUEEZE, 1);                    // x
     put(MZK_TR_WRITE_FR, k->advice_queries.size() + mzk::fixed_written(*k) + k->n_perm + (S ? 3 * S - 1 : 0) +
-                             4 * L + k->trash.size());  // evaluations
+                             3 * L + k->n_helpers + k->trash.size());  // evaluations
     put(MZK_TR_SQUEEZE, 2);                    // x1, x2
     put(MZK_TR_WRITE_POINT, 1);                // f
     put(MZK_TR_SQUEEZE, 1);                    // x3

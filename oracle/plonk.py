@@ -193,7 +193,7 @@ def blinding_factors(circuit):
     for col, _ in circuit["advice_queries"]:
         per_col[col] = per_col.get(col, 0) + 1
     f = max(3, max(per_col.values(), default=1))
-    return f + len(circuit.get("trashcans", [])) + len(circuit["lookups"]) + 3
+    return f + len(circuit.get("trashcans", [])) + sum(len(lookup_chunks(circuit, lk)) for lk in circuit["lookups"]) + 3
 
 
 def n_perm_sets(circuit):
@@ -434,6 +434,38 @@ def tuple_circuit(k):
 
 def tuple_instance(k, seed):
     return generic_instance(k, seed, two_lookups=True, circuit=tuple_circuit(k))
+
+
+def parallel_circuit(k):
+    """generic_circuit with the table of squares and three more advice
+    columns e, f, g (queried at rotation 0, in no gate nor permutation), and
+    two lookups with parallel inputs: a, e, f, a, e into the table with the
+    selector (five inputs: two helper chunks at degree 5, of four and one),
+    and the tuples (a, d), (e, g) into (table, squares) without a selector
+    (one chunk of two theta-compressed inputs)."""
+    c = generic_circuit(k, two_lookups=True)
+    c["n_advice"] = 7
+    c["advice_queries"] = c["advice_queries"] + [(4, 0), (5, 0), (6, 0)]
+    c["lookups"] = [{"inputs": [0, 4, 5, 0, 4], "table": 4, "selector": 5},
+                    {"inputs": [[0, 3], [4, 6]], "table": [4, 6], "selector": None}]
+    return c
+
+
+def parallel_instance(k, seed):
+    """generic_instance's columns with e, f table values on the usable rows
+    and g = e^2 (zero past the usable rows)."""
+    c = parallel_circuit(k)
+    fixed, mapping, adv = generic_instance(k, seed, two_lookups=True, circuit=c)
+    n = 1 << k
+    u = n - blinding_factors(c) - 1
+    rows = min(1 << 16, u)
+    rng = np.random.default_rng(seed + 77)
+    e, f = (np.zeros((n, 4), np.uint64) for _ in range(2))
+    e[:u] = np.stack([to_mont(int(v)) for v in rng.integers(0, rows, size=u)])
+    f[:u] = np.stack([to_mont(int(v)) for v in rng.integers(0, rows, size=u)])
+    g = _hadamard(e, e)
+    g[u:] = 0
+    return fixed, mapping, adv + [e, f, g]
 
 
 def selector_circuit(k):
@@ -772,19 +804,32 @@ def identities(key, ev, ch):
                 right = right * (e + cur + gamma) % R
                 cur = cur * dlt % R
             out.append((None, (left - right) * (1 - (l_last + l_blind)) % R))
-    # lookups
+    # lookups: the boundary, one helper constraint per chunk, the accumulator
     for li, lk in enumerate(c["lookups"]):
-        m, h, Z, Zn = ev["lookups"][li]
-        ins, tab = lookup_columns(lk)
-        f = table = 0
-        for e in range(len(ins)):
-            f = (f * theta + aq(ins[e])) % R
-            table = (table * theta + fq(tab[e])) % R
+        m, hs, Z, Zn = ev["lookups"][li]
+        _, tab = lookup_columns(lk)
+        table = 0
+        for col in tab:
+            table = (table * theta + fq(col)) % R
         sel = fq(lk["selector"]) if lk["selector"] is not None else 1
         out.append((None, (l_0 + l_last) * Z % R))
-        fb = (f + beta) % R
-        out.append((None, (h * fb - 1) % R))              # one input: product f+beta, sum of partial products 1
-        out.append((None, ((Zn - Z - sel * h) * (table + beta) + m) * (1 - (l_last + l_blind)) % R))
+        for chunk, h in zip(lookup_chunks(c, lk), hs):
+            fb = []
+            for tup in chunk:
+                f = 0
+                for col in tup:
+                    f = (f * theta + aq(col)) % R
+                fb.append((f + beta) % R)
+            product, spp = 1, 0
+            for j in range(len(fb)):
+                partial = 1
+                for i in range(len(fb)):
+                    if i != j:
+                        partial = partial * fb[i] % R
+                spp += partial
+                product = product * fb[j] % R
+            out.append((None, (h * product - spp) % R))
+        out.append((None, ((Zn - Z - sel * sum(hs)) * (table + beta) + m) * (1 - (l_last + l_blind)) % R))
     # trashcans (trash.rs:60-86): compressed - (1 - q) trash
     for ti, tc in enumerate(c.get("trashcans", [])):
         def read(col_type, col, rot):
@@ -932,13 +977,15 @@ def create_proof(key, advice, blinds, instances=None):
         tr.write_point(commit(a, srs["lagrange"]))
     theta = tr.squeeze()
     # multiplicities (logup/prover.rs:95-184), committed in delta form
-    ms = []
+    ms, fs, ts = [], [], []
     for lk in c["lookups"]:
         sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
         ins, tab = lookup_columns(lk)
-        f = adv[ins[0]] if len(ins) == 1 else compress_columns([adv[i] for i in ins], theta)
+        fl = [adv[tup[0]] if len(tup) == 1 else compress_columns([adv[i] for i in tup], theta) for tup in ins]
         t = key.fixed_values[tab[0]] if len(tab) == 1 else compress_columns([key.fixed_values[i] for i in tab], theta)
-        ms.append(compute_multiplicities(sel, [f], t, u, take(bf + 1)))
+        ms.append(compute_multiplicities(sel, fl, t, u, take(bf + 1)))
+        fs.append(fl)
+        ts.append(t)
     for m in ms:
         tr.write_point(commit(delta(m, 1), srs["delta"]))
     beta = tr.squeeze()
@@ -950,20 +997,19 @@ def create_proof(key, advice, blinds, instances=None):
     pvals = [(adv, key.fixed_values, inst)[kind][ci] for kind, ci in c["perm_cols"]]
     zs = O.permutation_z(pvals, key.perm_values, c["degree"] - 2, c["k"], to_mont(key.omega), to_mont(beta),
                          to_mont(gamma), bf, np.stack([np.stack([to_mont(v) for v in b]) for b in perm_bl]))
-    hs, Zs = [], []
+    hs, Zs = [], []   # hs: per lookup, its helpers (one per chunk of inputs)
     for li, lk in enumerate(c["lookups"]):
         sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
-        ins, tab = lookup_columns(lk)
-        f = adv[ins[0]] if len(ins) == 1 else compress_columns([adv[i] for i in ins], theta)
-        t = key.fixed_values[tab[0]] if len(tab) == 1 else compress_columns([key.fixed_values[i] for i in tab], theta)
-        (h,), Z = O.logup([[f]], t, sel, ms[li], to_mont(beta), bf,
-                          np.stack([to_mont(v) for v in log_bl[li]]))
-        hs.append(h)
+        per = lookup_per_helper(c)
+        chunks = [fs[li][i:i + per] for i in range(0, len(fs[li]), per)]
+        hl, Z = O.logup(chunks, ts[li], sel, ms[li], to_mont(beta), bf, np.stack([to_mont(v) for v in log_bl[li]]))
+        hs.append(list(hl))
         Zs.append(Z)
     for z in zs:
         tr.write_point(commit(delta(z, 1), srs["delta"]))
-    for h, Z in zip(hs, Zs):
-        tr.write_point(commit(h, srs["lagrange"]))
+    for hl, Z in zip(hs, Zs):                                  # prover.rs:221-227
+        for h in hl:
+            tr.write_point(commit(h, srs["lagrange"]))
         tr.write_point(commit(delta(Z, 2), srs["double_delta"]))
     trash = tr.squeeze()
     # trash columns (trash/prover.rs:29-77): the constraint expressions over
@@ -976,13 +1022,13 @@ def create_proof(key, advice, blinds, instances=None):
     adv_c = [dom.lagrange_to_coeff(a) for a in adv]
     z_c = [dom.lagrange_to_coeff(z) for z in zs]
     m_c = [dom.lagrange_to_coeff(m) for m in ms]
-    h_c = [dom.lagrange_to_coeff(h) for h in hs]
+    h_c = [[dom.lagrange_to_coeff(h) for h in hl] for hl in hs]
     Z_c = [dom.lagrange_to_coeff(Z) for Z in Zs]
     ext = lambda p: dom.coeff_to_extended(p)
     inst_c = [dom.lagrange_to_coeff(col) for col in inst]
     t_c = [dom.lagrange_to_coeff(t) for t in trs]
     hpoly = quotient(key, [ext(p) for p in adv_c], [ext(p) for p in z_c], [ext(p) for p in m_c],
-                     [ext(p) for p in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta, trash=trash,
+                     [[ext(p) for p in hl] for hl in h_c], [ext(p) for p in Z_c], y, beta, gamma, theta, trash=trash,
                      inst_e=[ext(p) for p in inst_c], trash_e=[ext(p) for p in t_c])
     hcoeff = dom.extended_to_coeff(hpoly)[: (n - 1) * qdeg]
     limbs = [np.concatenate([hcoeff[i * (n - 1):(i + 1) * (n - 1)], np.zeros((1, 4), np.uint64)]) for i in range(qdeg)]
@@ -1018,9 +1064,9 @@ def create_proof(key, advice, blinds, instances=None):
     ev["perm_sets"] = sets
     ev["lookups"] = []
     for li in range(len(c["lookups"])):
-        e = (eval_at(m_c[li], x), eval_at(h_c[li], x), eval_at(Z_c[li], x), eval_at(Z_c[li], x_next))
+        e = (eval_at(m_c[li], x), [eval_at(h, x) for h in h_c[li]], eval_at(Z_c[li], x), eval_at(Z_c[li], x_next))
         ev["lookups"].append(e)
-        for v in e:
+        for v in (e[0], *e[1], e[2], e[3]):
             tr.write_fr(v)
     ev["trash"] = [eval_at(t, x) for t in t_c]                 # trash/prover.rs:80-92
     for v in ev["trash"]:
@@ -1050,7 +1096,8 @@ def create_proof(key, advice, blinds, instances=None):
         q.append((("perm", si), x_last, z_c[si]))
     for li in range(len(c["lookups"])):
         q.append((("m", li), x, m_c[li]))
-        q.append((("h", li, 0), x, h_c[li]))
+        for j, h in enumerate(h_c[li]):
+            q.append((("h", li, j), x, h))
         q.append((("Z", li), x, Z_c[li]))
         q.append((("Z", li), x_next, Z_c[li]))
     for ti, t in enumerate(t_c):
@@ -1108,13 +1155,14 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     d.n_perm_sets, d.perm_z = len(z_e), parr(z_e)
     d.chunk_len, d.blinding_factors = c["degree"] - 2, key.bf
     tcs = c.get("trashcans", [])
-    builtin = len(c["lookups"]) == 1 and not tcs and len(lookup_columns(c["lookups"][0])[0]) == 1
+    shapes = [lookup_columns(lk) for lk in c["lookups"]]
+    builtin = len(shapes) == 1 and not tcs and len(shapes[0][0]) == 1 and len(shapes[0][1]) == 1
     if builtin:
         lk = c["lookups"][0]
         d.has_lookup = 1
-        d.lookup_input_advice, d.lookup_table_fixed = lk["input"], lk["table"]
+        d.lookup_input_advice, d.lookup_table_fixed = shapes[0][0][0][0], shapes[0][1][0]
         d.lookup_selector_fixed = -1 if lk["selector"] is None else lk["selector"]
-        d.lookup_h, d.lookup_z, d.lookup_m = h_e[0].ctypes.data, Z_e[0].ctypes.data, m_e[0].ctypes.data
+        d.lookup_h, d.lookup_z, d.lookup_m = h_e[0][0].ctypes.data, Z_e[0].ctypes.data, m_e[0].ctypes.data
     d.l0, d.l_last, d.l_active = key.l0.ctypes.data, key.l_last.ctypes.data, key.l_active.ctypes.data
     for name, v in (("y", y), ("beta", beta), ("gamma", gamma), ("theta", theta)):
         getattr(d, name)[:] = [int(t) for t in to_mont(v)]
@@ -1129,14 +1177,16 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
                                         to_mont(beta), to_mont(theta), to_mont(trash), to_mont(y))
     if builtin or (not c["lookups"] and not tcs):
         return dom.quotient_eval(d, True, threads, gate_values)
-    # several lookups, or trashcans: the gate and permutation terms, then
-    # every lookup's terms (evaluation.rs:1034-1090) as single-input helper
-    # programs (Evaluator::lookups_flat, :686-767) and every trashcan's term
-    # (:1093-1109), then the division by t(X)
+    # several lookups, tuples, parallel inputs or trashcans: the gate and
+    # permutation terms, then every lookup's terms (evaluation.rs:1034-1090)
+    # as one helper program per chunk (Evaluator::lookups_flat, :691-770) and
+    # every trashcan's term (:1093-1109), then the division by t(X)
     v = dom.quotient_eval(d, False, threads, gate_values)
-    lks = [{"programs": [g], "outputs": [outs], "helpers": [h_e[li]], "aggregator": Z_e[li],
-            "multiplicities": m_e[li]}
-           for li, (g, outs) in enumerate(lookup_program(lk) for lk in c["lookups"])]
+    lks = []
+    for li, lk in enumerate(c["lookups"]):
+        progs = [lookup_program(lk, chunk, first=j == 0) for j, chunk in enumerate(lookup_chunks(c, lk))]
+        lks.append({"programs": [g for g, _ in progs], "outputs": [o for _, o in progs], "helpers": list(h_e[li]),
+                    "aggregator": Z_e[li], "multiplicities": m_e[li]})
     tas = [{"program": tc["program"], "selector": tc["selector"], "trash": trash_e[ti]} for ti, tc in enumerate(tcs)]
     v = O.flat_tail_eval(v, key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k, to_mont(beta), to_mont(theta),
                          to_mont(trash), to_mont(y), key.l0, key.l_last, key.l_active, lookups=lks, trashcans=tas)
@@ -1144,11 +1194,31 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
 
 
 def lookup_columns(lk):
-    """(input advice columns, table fixed columns) of a lookup: one column
-    each, or tuples of the same length."""
-    ins = list(lk["input"]) if isinstance(lk["input"], (list, tuple)) else [lk["input"]]
-    tab = list(lk["table"]) if isinstance(lk["table"], (list, tuple)) else [lk["table"]]
-    return ins, tab
+    """(input tuples, table tuple) of a lookup: "input" one advice column or
+    a tuple (list) of them, or "inputs" a list of such tuples (parallel
+    lookups into one table, BatchedArgument::new, logup.rs:226-262); "table"
+    one fixed column or a tuple of the inputs' width."""
+    one = lambda v: list(v) if isinstance(v, (list, tuple)) else [v]
+    ins = [one(t) for t in lk["inputs"]] if "inputs" in lk else [one(lk["input"])]
+    return ins, one(lk["table"])
+
+
+def lookup_per_helper(circuit):
+    """Parallel inputs per helper polynomial for inputs of degree one:
+    next_pow2(cs.degree() - 1) (nb_parallel_lookups_per_chunk, logup.rs:
+    168-183)."""
+    p = 1
+    while p < circuit["degree"] - 1:
+        p *= 2
+    return p
+
+
+def lookup_chunks(circuit, lk):
+    """The lookup's input tuples split into helper chunks
+    (chunk_by_degree, logup.rs:289-300)."""
+    ins, _ = lookup_columns(lk)
+    per = lookup_per_helper(circuit)
+    return [ins[i:i + per] for i in range(0, len(ins), per)]
 
 
 def compress_columns(cols, theta):
@@ -1158,27 +1228,72 @@ def compress_columns(cols, theta):
     return O.poly_inner_product(list(cols), [to_mont(pow(theta, w - 1 - e, R)) for e in range(w)])
 
 
-def lookup_program(lk):
-    """The helper program of a lookup whose input is one advice column (or a
-    tuple) and whose table is one fixed column (or a tuple): values 0, 1
+def lookup_program(lk, chunk, first=True):
+    """The helper program of one chunk of a lookup's input tuples
+    (Evaluator::lookups_flat, evaluation.rs:691-770): values 0, 1
     (constants), beta, theta, trash challenge, y, the previous value, the
-    input reads, the table reads, the selector read; the theta-compressed
-    input and table (Horner from 0 theta + the first column) plus beta; the
-    sum of partial products of one input is the constant one.  Returns
-    (graph, (sum_partial_products, product, table, selector) indices)."""
-    ins, tab = lookup_columns(lk)
-    w = len(ins)
-    sel_slot, base = 7 + 2 * w, 8 + 2 * w
-    reads = [(1, c, 0, 7 + e) for e, c in enumerate(ins)] + [(0, c, 0, 7 + w + e) for e, c in enumerate(tab)]
-    if lk["selector"] is not None:
-        reads.append((0, lk["selector"], 0, sel_slot))
-    tb = base + w + 1
-    ops = [(6, base + e, base + e - 1 if e else 0, 3, 7 + e) for e in range(w)] + [(0, base + w, base + w - 1, 2, 0)]
-    ops += [(6, tb + e, tb + e - 1 if e else 0, 3, 7 + w + e) for e in range(w)] + [(0, tb + w, tb + w - 1, 2, 0)]
+    reads; every input tuple theta-compressed (Horner from 0 theta + the
+    first column) plus beta, f_j; the product of the f_j and the sum of
+    partial products sum_j prod_{i!=j} f_i (each by a loop over i, as the
+    reference builds it; one input: the constant one); for the first chunk
+    the compressed table plus beta and the selector.  Returns (graph,
+    (sum_partial_products, product, table, selector) indices)."""
+    _, tab = lookup_columns(lk)
+    reads, ops = [], []
+    slot = [7]
+
+    def new():
+        slot[0] += 1
+        return slot[0] - 1
+
+    def op(kind, a, b, cc=0):
+        d = new()
+        ops.append((kind, d, a, b, cc))
+        return d
+    in_at = [[None] * len(tup) for tup in chunk]
+    for j, tup in enumerate(chunk):
+        for e, col in enumerate(tup):
+            in_at[j][e] = new()
+            reads.append((1, col, 0, in_at[j][e]))
+    table = sel = 1
+    if first:
+        tab_at = []
+        for col in tab:
+            tab_at.append(new())
+            reads.append((0, col, 0, tab_at[-1]))
+        if lk["selector"] is not None:
+            sel = new()
+            reads.append((0, lk["selector"], 0, sel))
+    f = []
+    for j in range(len(chunk)):
+        acc = 0
+        for e in range(len(chunk[j])):
+            acc = op(6, acc, 3, in_at[j][e])
+        f.append(op(0, acc, 2))
+    if first:
+        acc = 0
+        for t in tab_at:
+            acc = op(6, acc, 3, t)
+        table = op(0, acc, 2)
+    product, spp = f[0], 1
+    if len(f) > 1:
+        partials = []
+        for j in range(len(f)):
+            acc = 1
+            for i in range(len(f)):
+                if i != j:
+                    acc = op(2, acc, f[i])
+            partials.append(acc)
+        spp = partials[0]
+        for pj in partials[1:]:
+            spp = op(0, spp, pj)
+        product = f[0]
+        for fj in f[1:]:
+            product = op(2, product, fj)
     graph = {"constants": [np.zeros(4, np.uint64), O.fr_const(0)], "rotations": [0], "reads": reads, "ops": ops,
-             "values_len": tb + w + 1, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
-             "previous_value_idx": 6, "result_idx": tb + w}
-    return graph, (1, base + w, tb + w, sel_slot if lk["selector"] is not None else 1)
+             "values_len": slot[0], "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
+             "previous_value_idx": 6, "result_idx": spp}
+    return graph, (spp, product, table, sel)
 
 
 def multi_open(key, tr, queries):
@@ -1248,7 +1363,10 @@ def _verify(key, proof, s, instances=None):
     beta = tr.squeeze()
     gamma = tr.squeeze()
     z_coms = [tr.read_point() for _ in range(S)]
-    hz_coms = [(tr.read_point(), tr.read_point()) for _ in range(L)]
+    hz_coms = []   # per lookup: (its helpers' commitments, its aggregator's)
+    for lk in c["lookups"]:
+        hl = [tr.read_point() for _ in lookup_chunks(c, lk)]
+        hz_coms.append((hl, tr.read_point()))
     trash = tr.squeeze()
     T = len(c.get("trashcans", []))
     trash_coms = [tr.read_point() for _ in range(T)]
@@ -1266,7 +1384,8 @@ def _verify(key, proof, s, instances=None):
         z0, z1 = tr.read_fr(), tr.read_fr()
         sets.append([z0, z1, tr.read_fr() if si < S - 1 else None])
     ev["perm_sets"] = sets
-    ev["lookups"] = [tuple(tr.read_fr() for _ in range(4)) for _ in range(L)]
+    ev["lookups"] = [(tr.read_fr(), [tr.read_fr() for _ in lookup_chunks(c, lk)], tr.read_fr(), tr.read_fr())
+                     for lk in c["lookups"]]
     ev["trash"] = [tr.read_fr() for _ in range(T)]
     ev["instance"] = instance_evals(key, instances, x, xn)
     ch = {"x": x, "xn": xn, "beta": beta, "gamma": gamma, "theta": theta, "trash": trash, "y": y}
@@ -1285,9 +1404,10 @@ def _verify(key, proof, s, instances=None):
     for si in reversed(range(S - 1)):
         q.append((("perm", si), x_last, z_coms[si], sets[si][2]))
     for li in range(L):
-        m, h, Z, Zn = ev["lookups"][li]
+        m, hs, Z, Zn = ev["lookups"][li]
         q.append((("m", li), x, m_coms[li], m))
-        q.append((("h", li, 0), x, hz_coms[li][0], h))
+        for j, h in enumerate(hs):
+            q.append((("h", li, j), x, hz_coms[li][0][j], h))
         q.append((("Z", li), x, hz_coms[li][1], Z))
         q.append((("Z", li), x_next, hz_coms[li][1], Zn))
     for ti in range(T):

@@ -20,7 +20,8 @@ SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.g
           "instance": (OP.instance_circuit, OP.instance_instance),
           "trash": (OP.trash_circuit, OP.trash_instance),
           "selector": (OP.selector_circuit, OP.selector_instance),
-          "tuple": (OP.tuple_circuit, OP.tuple_instance)}
+          "tuple": (OP.tuple_circuit, OP.tuple_instance),
+          "parallel": (OP.parallel_circuit, OP.parallel_instance)}
 
 
 class Circuit:
@@ -32,8 +33,10 @@ class Circuit:
         permutation sets), "generic2" (generic with a second lookup,
         without a selector), "instance" (generic with an instance column
         read by a third gate and copied from c), "trash" (generic with a
-        trashcan), "selector" (generic with a simple selector) or "tuple"
-        (generic with a lookup of the tuple (a, d) into (table, squares))."""
+        trashcan), "selector" (generic with a simple selector), "tuple"
+        (generic with a lookup of the tuple (a, d) into (table, squares)) or
+        "parallel" (lookups with parallel inputs: two helper chunks, and
+        two tuples in one chunk)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)

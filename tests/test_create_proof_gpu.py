@@ -330,6 +330,32 @@ def test_tuple_lookup_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, bad, bl)])
 
 
+@pytest.mark.parametrize("k", [5, 9])
+def test_parallel_lookup_proof_equals_oracle(ctx, k):
+    """Lookups with parallel inputs: five columns into one table (helper
+    chunks of four and one at degree 5, committed, evaluated and opened per
+    chunk, one quotient helper program each, with the partial products) and
+    two theta-compressed tuples into (table, squares) in one chunk.  The
+    device transcript equals the oracle's and verifies, in a batch and
+    through the proving service; an input outside its table is refused."""
+    c = Circuit(ctx, k, seed=k + 120, shape="parallel")
+    assert c.key.proof_len == len(c.oracle_proof(c.advice, c.blinds(4)))
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    both = mzk.create_proofs(ctx, [(c.key, c.advice, bl), (c.key, c.advice, c.blinds(6))])
+    assert both[0] == proof and c.verify(both[1])
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = srv.submit(c.key, c.advice, c.blinds(7))
+    assert c.verify(srv.wait(t)[0])
+    srv.close()
+    bad = [a.copy() for a in c.advice]
+    bad[5][2] = OP.to_mont((1 << 16) + 5)                      # f outside the table on a selected row
+    with pytest.raises(mzk.MzkError, match="not in the table"):
+        mzk.create_proofs(ctx, [(c.key, bad, bl)])
+
+
 def test_key_files_equal_oracle_and_read_back(ctx, k5):
     """VerifyingKey / ProvingKey files in the three SerdeFormats equal the
     oracle's bytes; a key read from a PK file has the same transcript_repr and

@@ -237,6 +237,38 @@ def test_tuple_lookup_proofs_verify():
         OP.create_proof(key, bad, bl)
 
 
+def test_parallel_lookup_proofs_verify():
+    """Lookups with parallel inputs (five columns into one table: helper
+    chunks of four and one at degree 5; two theta-compressed tuples): the
+    blinding factors count the three helpers, the proof verifies, a wrong
+    helper evaluation or an input value outside the table is refused."""
+    k = 5
+    c = OP.parallel_circuit(k)
+    assert [len(OP.lookup_chunks(c, lk)) for lk in c["lookups"]] == [2, 1]
+    assert [len(ch) for ch in OP.lookup_chunks(c, c["lookups"][0])] == [4, 1]
+    assert OP.blinding_factors(c) == 3 + 3 + 3
+    fixed, mapping, adv = OP.parallel_instance(k, 21)
+    s = O.rand_fr(56, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"parallel")
+    bl = [OP.to_int(v) for v in O.rand_fr(66, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl)
+    assert OP.verify(key, proof, OP.to_int(s))
+    # the evaluations start after 7 advice, 2 multiplicity, 2 permutation,
+    # 3 helper, 2 aggregator and 4 quotient-limb points; the lookups' come
+    # after 8 advice, 7 fixed, 4 permutation-column and 5 permutation-set
+    # evaluations as m, h0, h1, Z, Z(wx) of the first lookup: flip the low
+    # bit of its second helper's
+    at = 20 * 48 + (8 + 7 + 4 + 5 + 2) * 32
+    bad = bytearray(proof)
+    bad[at] ^= 1
+    assert not OP.verify(key, bytes(bad), OP.to_int(s))
+    worse = [a.copy() for a in adv]
+    worse[5][2] = OP.to_mont((1 << 16) + 5)                     # f outside the table on a selected row
+    with pytest.raises(ValueError):
+        OP.create_proof(key, worse, bl)
+
+
 def test_generic_circuit_proofs_verify():
     """Another circuit shape: two gates as one flattened program (with a(wX)),
     four permutation columns in two sets (z of the first set opened at
