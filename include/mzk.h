@@ -146,7 +146,7 @@ int mzk_msm_g1_device(mzk_ctx *ctx, const uint64_t *d_scalars, const uint64_t *d
  * scratch is one fixed device array of about 21 MB inside this library, held
  * by every GPU that loads it until the process exits.  n must not exceed
  * 65536 (larger n returns MZK_ERR_ARG).  The first call on a device looks up
- * that array's device address (make it before any stream capture); with CUDA's
+ * that array's device address; with CUDA's
  * lazy module loading that first call is also when the module and its array
  * are loaded onto the device, so make it before the host reserves the rest of
  * the device's memory.  Runs on `stream` (NULL: the default stream), which
