@@ -832,7 +832,7 @@ def run_ours(args):
         f1.synchronize()
         ems = max_over_ranks(f0.elapsed_time(f1) / args.steps)
         e2e = {"value": round(world * n / (ems / 1e3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(ems, 3),
-               "h2d_bytes_per_step": n * 32 + n * 96, "d2h_bytes_per_step": windows * 192 + 4 * (2 if n >= 1 << 20 else 1),
+               "h2d_bytes_per_step": n * 32 + n * 96, "d2h_bytes_per_step": windows * 192 + 4 * (3 if n >= 1 << 20 else 1),
                "api": "mzk_msm_g1 (host pointers, pinned)"}
 
     extra_ntt = extra_q = None

@@ -83,7 +83,7 @@ Status Context::ensure_pinned(size_t bytes, void** out) {
 
 Status Context::phase_begin(int phase, cudaStream_t st) {
     if (!profiling) return OK;
-    if (prof_used >= kMaxEvents / 2) {
+    if (prof_used >= kMaxRecords) {
         set_error("profiling: too many open phases");
         return ERR_STATE;
     }
@@ -121,8 +121,8 @@ Context::~Context() {
         if (kv.second.p) cudaFree(kv.second.p);
     if (pinned) cudaFreeHost(pinned);
     if (gen_table) cudaFree(gen_table);
-    if (ev_copy) cudaEventDestroy(ev_copy);
-    if (ev_copy2) cudaEventDestroy(ev_copy2);
+    for (cudaEvent_t ev : ev_copy)
+        if (ev) cudaEventDestroy(ev);
     for (int i = 0; i < kMaxEvents; i++)
         if (prof_ev[i]) cudaEventDestroy(prof_ev[i]);
     if (stream) cudaStreamDestroy(stream);
@@ -184,8 +184,8 @@ int mzk_ctx_create(int device, mzk_ctx** out) {
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->impl.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->impl.copy_stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->impl.ev_copy, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->impl.ev_copy2, cudaEventDisableTiming);
+    for (cudaEvent_t& ev : c->impl.ev_copy)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         mzk::set_error(std::string("context setup: ") + cudaGetErrorString(e));
         delete c;
@@ -462,8 +462,19 @@ int mzk_msm_g1_device(mzk_ctx* ctx, const uint64_t* d_scalars, const uint64_t* d
     return mzk::msm_g1_device(&ctx->impl, d_scalars, d_bases, n, out, ctx->impl.stream, nullptr);
 }
 
-// host-buffer MSMs of at least this many points upload and compute in two parts
+// host-buffer MSMs of at least this many points upload and compute in parts
 constexpr size_t kPipelineMinPoints = size_t(1) << 20;
+// Cumulative point fractions of the parts of a pipelined host MSM.  At 2^24
+// the upload (128 bytes a point at the host link's ~55 GB/s) takes ~39 ms
+// and the sort and accumulation ~84 ms, both linear in the points; every
+// part after the first adds one bucket set that the reduction merges key by
+// key (one full XYZZ addition per key, ~4 ms at c = 20).  Three parts
+// balance the two: the compute stream waits for the first 12 % only, and
+// each later part is up before the one before it has been accumulated.
+constexpr int kHostParts = 3;
+constexpr double kPartEnd[kHostParts] = {0.12, 0.40, 1.0};
+static_assert(kHostParts <= mzk::kMaxMsmParts, "parts of a pipelined MSM");
+static_assert(2 * kHostParts <= mzk::Context::kCopyEvents, "two upload events per part");
 
 int mzk_msm_g1(mzk_ctx* ctx, const uint64_t* scalars, const uint64_t* bases, size_t n, uint64_t out[18]) {
     if (int s = check_ctx(ctx)) return s;
@@ -484,23 +495,27 @@ int mzk_msm_g1(mzk_ctx* ctx, const uint64_t* scalars, const uint64_t* bases, siz
     char* dba = static_cast<char*>(db);
     const char* hsc = reinterpret_cast<const char*>(scalars);
     const char* hba = reinterpret_cast<const char*>(bases);
-    // Scalars first on the compute stream (the digit passes need only them),
-    // bases on the copy stream, overlapping the sort.  Large MSMs go in two
-    // parts: the first ~30 % of the points is sorted and accumulated while the
-    // rest is still uploading (the accumulation of 30 % of the points takes
-    // about as long as the upload of the other 70 %).
-    const size_t first = n >= kPipelineMinPoints ? (n * 3 / 10) & ~(size_t)1023 : n;
-    MZK_CUDA_CHECK(cudaMemcpyAsync(dsc, hsc, first * 32, cudaMemcpyHostToDevice, c->stream));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(dba, hba, first * 96, cudaMemcpyHostToDevice, c->copy_stream));
-    MZK_CUDA_CHECK(cudaEventRecord(c->ev_copy, c->copy_stream));
-    if (first == n) return mzk::msm_g1_device(c, ds, db, n, out, c->stream, c->ev_copy);
-    MZK_CUDA_CHECK(cudaMemcpyAsync(dsc + first * 32, hsc + first * 32, (n - first) * 32, cudaMemcpyHostToDevice,
-                                   c->copy_stream));
-    MZK_CUDA_CHECK(cudaMemcpyAsync(dba + first * 96, hba + first * 96, (n - first) * 96, cudaMemcpyHostToDevice,
-                                   c->copy_stream));
-    MZK_CUDA_CHECK(cudaEventRecord(c->ev_copy2, c->copy_stream));
-    const mzk::MsmPart parts[2] = {{0, first, nullptr, c->ev_copy}, {first, n, c->ev_copy2, c->ev_copy2}};
-    return mzk::msm_g1_parts(c, ds, db, n, out, c->stream, parts, 2);
+    // The first part's scalars go on the compute stream (its digit passes
+    // need only them), everything else on the copy stream in part order:
+    // the first part's bases, then each later part's scalars and bases, each
+    // marked by its own event, so part p is sorted once its scalars are up
+    // and accumulated once its bases are, while later parts still upload.
+    const int P = n >= kPipelineMinPoints ? kHostParts : 1;
+    size_t end[kHostParts];
+    for (int p = 0; p < P; p++)
+        end[p] = p + 1 == P ? n : (size_t)((double)n * kPartEnd[p]) & ~(size_t)1023;
+    mzk::MsmPart parts[kHostParts];
+    for (int p = 0; p < P; p++) {
+        const size_t b0 = p ? end[p - 1] : 0, np = end[p] - b0;
+        cudaStream_t sst = p ? c->copy_stream : c->stream;
+        MZK_CUDA_CHECK(cudaMemcpyAsync(dsc + b0 * 32, hsc + b0 * 32, np * 32, cudaMemcpyHostToDevice, sst));
+        if (p) MZK_CUDA_CHECK(cudaEventRecord(c->ev_copy[2 * p], c->copy_stream));
+        MZK_CUDA_CHECK(cudaMemcpyAsync(dba + b0 * 96, hba + b0 * 96, np * 96, cudaMemcpyHostToDevice, c->copy_stream));
+        MZK_CUDA_CHECK(cudaEventRecord(c->ev_copy[2 * p + 1], c->copy_stream));
+        parts[p] = {b0, end[p], p ? c->ev_copy[2 * p] : nullptr, c->ev_copy[2 * p + 1]};
+    }
+    if (P == 1) return mzk::msm_g1_device(c, ds, db, n, out, c->stream, c->ev_copy[1]);
+    return mzk::msm_g1_parts(c, ds, db, n, out, c->stream, parts, P);
 }
 
 int mzk_gen_rand_fr_device(mzk_ctx* ctx, uint64_t seed, uint64_t first, size_t n, uint64_t* d_out) {

@@ -492,12 +492,16 @@ __device__ __forceinline__ uint32_t find_win(const WinDev* wins, uint32_t n_wins
     return lo;
 }
 
-// buckets2/offsets2 (optional): a second bucket set over the same keys (the
-// second part of a pipelined MSM), added bucket by bucket
-__global__ void __launch_bounds__(kReduceThreads) k_group_sums(const Xyzz* __restrict__ buckets,
-                                                               const uint32_t* __restrict__ offsets,
-                                                               const Xyzz* __restrict__ buckets2,
-                                                               const uint32_t* __restrict__ offsets2,
+// The bucket sets of an MSM over the same keys (one per part of a pipelined
+// MSM), added bucket by bucket; a key is empty in a set when its offsets
+// say so (its bucket is then never written)
+struct BucketSets {
+    const Xyzz* buckets[kMaxMsmParts];
+    const uint32_t* offsets[kMaxMsmParts];
+    uint32_t n;
+};
+
+__global__ void __launch_bounds__(kReduceThreads) k_group_sums(const BucketSets sets,
                                                                const WinDev* __restrict__ wins, uint32_t n_wins,
                                                                uint32_t total_groups, Xyzz* __restrict__ run_out,
                                                                Xyzz* __restrict__ tot_out) {
@@ -510,8 +514,10 @@ __global__ void __launch_bounds__(kReduceThreads) k_group_sums(const Xyzz* __res
     xyzz_set_inf(tot);
     for (int b = (1 << wd.glen_log) - 1; b >= 0; b--) {
         const uint32_t key = key0 + (uint32_t)b;
-        if (offsets[key + 1] > offsets[key]) run = xyzz_add(run, load_xyzz(&buckets[key]));
-        if (buckets2 && offsets2[key + 1] > offsets2[key]) run = xyzz_add(run, load_xyzz(&buckets2[key]));
+#pragma unroll
+        for (uint32_t s = 0; s < kMaxMsmParts; s++)
+            if (s < sets.n && sets.offsets[s][key + 1] > sets.offsets[s][key])
+                run = xyzz_add(run, load_xyzz(&sets.buckets[s][key]));
         tot = xyzz_add(tot, run);
     }
     store_xyzz(&run_out[gid], run);
@@ -603,12 +609,11 @@ uint32_t plane_split(uint64_t slots, uint32_t max_groups, int num_sms) {
 // steps 1-3 on `st`.  partial holds slots * split plane partials and may be
 // q itself when split == 1; q holds slots plane sums.  Returns the launch
 // error, if any; adds the launches to *launches when given.
-cudaError_t launch_reduce(const Xyzz* buckets, const uint32_t* offsets, const Xyzz* buckets2,
-                          const uint32_t* offsets2, const WinDev* d_wins, uint32_t n_wins, uint64_t groups,
+cudaError_t launch_reduce(const BucketSets& sets, const WinDev* d_wins, uint32_t n_wins, uint64_t groups,
                           uint64_t slots, uint32_t split, Xyzz* run, Xyzz* tot, Xyzz* partial, Xyzz* q, Xyzz* wsum,
                           uint64_t* launches, cudaStream_t st) {
     k_group_sums<<<(uint32_t)((groups + kReduceThreads - 1) / kReduceThreads), kReduceThreads, 0, st>>>(
-        buckets, offsets, buckets2, offsets2, d_wins, n_wins, (uint32_t)groups, run, tot);
+        sets, d_wins, n_wins, (uint32_t)groups, run, tot);
     k_plane_sums<<<(uint32_t)(slots * split), kReduceThreads, kReduceThreads * sizeof(Xyzz), st>>>(
         run, tot, d_wins, n_wins, split, split == 1 ? q : partial);
     uint64_t n = 3;
@@ -702,8 +707,10 @@ Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, si
 
     void *counts, *sorted, *partials, *owner, *run, *tot, *planes, *wsum;
     void *offsets[kMaxMsmParts] = {}, *buckets[kMaxMsmParts] = {};
-    static const char* const kOffsetNames[kMaxMsmParts] = {"msm_offsets", "msm_offsets2"};
-    static const char* const kBucketNames[kMaxMsmParts] = {"msm_buckets", "msm_buckets2"};
+    static const char* const kOffsetNames[kMaxMsmParts] = {"msm_offsets", "msm_offsets2", "msm_offsets3",
+                                                            "msm_offsets4"};
+    static const char* const kBucketNames[kMaxMsmParts] = {"msm_buckets", "msm_buckets2", "msm_buckets3",
+                                                            "msm_buckets4"};
     MZK_TRY(ctx->ensure("msm_counts", ((size_t)sh.keys + 1) * 4, &counts));
     for (int p = 0; p < n_parts; p++) {
         MZK_TRY(ctx->ensure(kOffsetNames[p], ((size_t)sh.keys + 2) * 4, &offsets[p]));
@@ -787,8 +794,13 @@ Status msm_g1_parts(Context* ctx, const void* d_scalars, const void* d_bases, si
         MZK_CUDA_CHECK(cudaMemcpyAsync(host_entries + p, off + sh.keys, 4, cudaMemcpyDeviceToHost, st));
     }
     MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
-    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets[0], (const uint32_t*)offsets[0], (const Xyzz*)buckets[1],
-                                 (const uint32_t*)offsets[1], (const WinDev*)d_wins, (uint32_t)wins.size(),
+    BucketSets sets{};
+    sets.n = (uint32_t)n_parts;
+    for (int p = 0; p < n_parts; p++) {
+        sets.buckets[p] = (const Xyzz*)buckets[p];
+        sets.offsets[p] = (const uint32_t*)offsets[p];
+    }
+    MZK_CUDA_CHECK(launch_reduce(sets, (const WinDev*)d_wins, (uint32_t)wins.size(),
                                  total_groups, slots, split, (Xyzz*)run, (Xyzz*)tot, (Xyzz*)planes, (Xyzz*)q,
                                  (Xyzz*)wsum, &ctx->launches, st));
     MZK_TRY(ctx->phase_end(st));
@@ -1082,9 +1094,9 @@ Status msm_g1_batch_device(Context* ctx, const void* d_bases, size_t bases_len, 
     MZK_LAUNCH_CHECK(ctx);
     MZK_TRY(ctx->phase_end(st));
     MZK_TRY(ctx->phase_begin(PH_REDUCE, st));
-    MZK_CUDA_CHECK(launch_reduce((const Xyzz*)buckets, (const uint32_t*)offsets, nullptr, nullptr,
-                                 (const WinDev*)d_wins, (uint32_t)n_wins, groups, slots, split, (Xyzz*)run, (Xyzz*)tot, (Xyzz*)planes,
-                                 (Xyzz*)q, (Xyzz*)wsum, &ctx->launches, st));
+    const BucketSets sets{{(const Xyzz*)buckets}, {(const uint32_t*)offsets}, 1};
+    MZK_CUDA_CHECK(launch_reduce(sets, (const WinDev*)d_wins, (uint32_t)n_wins, groups, slots, split, (Xyzz*)run,
+                                 (Xyzz*)tot, (Xyzz*)planes, (Xyzz*)q, (Xyzz*)wsum, &ctx->launches, st));
     MZK_TRY(ctx->phase_end(st));
     MZK_CUDA_CHECK(cudaMemcpyAsync(host_wsum, wsum, n_wins * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));
     MZK_CUDA_CHECK(cudaStreamSynchronize(st));
@@ -1280,8 +1292,9 @@ Status msm_g1_noalloc_queued(unsigned char* base, int sms, const void* d_scalars
     append_windows(sh, 0, wins, total_groups, slots);
     WinDev* d_wins = reinterpret_cast<WinDev*>(base + kNaWinsOff);
     MZK_CUDA_CHECK(cudaMemcpyAsync(d_wins, wins.data(), wins.size() * sizeof(WinDev), cudaMemcpyHostToDevice, st));
-    MZK_CUDA_CHECK(launch_reduce(buckets, offsets, nullptr, nullptr, d_wins, (uint32_t)wins.size(), total_groups,
-                                 slots, 1, run, tot, planes, planes, wsum, nullptr, st));
+    const BucketSets sets{{buckets}, {offsets}, 1};
+    MZK_CUDA_CHECK(launch_reduce(sets, d_wins, (uint32_t)wins.size(), total_groups, slots, 1, run, tot, planes, planes,
+                                 wsum, nullptr, st));
     // window sums to host memory owned by this function (no pinned allocation)
     host::Xyzz6 hs[kNaMaxWindows];
     MZK_CUDA_CHECK(cudaMemcpyAsync(hs, wsum, (size_t)sh.windows * sizeof(Xyzz), cudaMemcpyDeviceToHost, st));

@@ -37,7 +37,9 @@ struct Context {
     int num_sms = 0;
     cudaStream_t stream = nullptr;       // compute stream
     cudaStream_t copy_stream = nullptr;  // host->device copies overlapped with compute
-    cudaEvent_t ev_copy = nullptr, ev_copy2 = nullptr;  // uploads of the first and second part
+    // uploads of a pipelined host MSM: per part its scalars (2p) and bases (2p + 1)
+    static constexpr int kCopyEvents = 8;
+    cudaEvent_t ev_copy[kCopyEvents] = {};
     std::recursive_mutex mu;
     std::map<std::string, DevBuf> bufs;
     void* pinned = nullptr;
@@ -54,10 +56,11 @@ struct Context {
     uint64_t launches = 0;
     // per-phase device timing with CUDA events on the launching stream
     bool profiling = false;
-    static constexpr int kPhases = 16;
-    static constexpr int kMaxEvents = 2 * kPhases;
+    static constexpr int kPhases = 16;      // phase kinds
+    static constexpr int kMaxRecords = 64;  // phases recorded between two collections
+    static constexpr int kMaxEvents = 2 * kMaxRecords;
     cudaEvent_t prof_ev[kMaxEvents] = {};
-    int prof_phase[kMaxEvents / 2] = {};
+    int prof_phase[kMaxRecords] = {};
     int prof_used = 0;
     double phase_ms[kPhases] = {};
     uint64_t phase_count[kPhases] = {};
@@ -132,7 +135,7 @@ Status msm_g1_device(Context* ctx, const void* d_scalars, const void* d_bases, s
 // stream waits on a part's scalars_ready before sorting its digits and on its
 // bases_ready before accumulating, so the upload of later parts overlaps the
 // accumulation of earlier ones.  Same result as one part.
-constexpr int kMaxMsmParts = 2;
+constexpr int kMaxMsmParts = 4;
 struct MsmPart {
     size_t begin, end;
     cudaEvent_t scalars_ready, bases_ready;  // optional

@@ -436,6 +436,32 @@ def tuple_instance(k, seed):
     return generic_instance(k, seed, two_lookups=True, circuit=tuple_circuit(k))
 
 
+def nolookup_circuit(k):
+    """generic_circuit without its lookup: no multiplicity, helper or
+    aggregator commitments, and one blinding factor fewer."""
+    c = generic_circuit(k)
+    c["lookups"] = []
+    return c
+
+
+def nolookup_instance(k, seed):
+    return generic_instance(k, seed, circuit=nolookup_circuit(k))
+
+
+def bare_circuit(k):
+    """generic_circuit with neither its lookup nor its permutation: the
+    gates alone (no z, m, h or Z commitments, no permutation polynomials in
+    the key)."""
+    c = nolookup_circuit(k)
+    c["perm_cols"] = []
+    return c
+
+
+def bare_instance(k, seed):
+    fixed, mapping, adv = generic_instance(k, seed, circuit=bare_circuit(k))
+    return fixed, mapping[:0], adv
+
+
 def parallel_circuit(k):
     """generic_circuit with the table of squares and three more advice
     columns e, f, g (queried at rotation 0, in no gate nor permutation), and
@@ -644,7 +670,7 @@ def keygen(circuit, fixed_values, mapping, srs, pinned_repr):
     omega_pows = dom.coeff_to_lagrange(x_poly)          # omega^r, r = 0..n-1
     P = len(circuit["perm_cols"])
     dlt = to_int(O.fr_const(5))
-    deltaomega = np.stack([scale(omega_pows, pow(dlt, c, R)) for c in range(P)])
+    deltaomega = np.stack([scale(omega_pows, pow(dlt, c, R)) for c in range(P)]) if P else None
     if mapping is None:
         mapping = np.zeros((P, n, 2), np.uint32)
         for c in range(P):
@@ -996,7 +1022,7 @@ def create_proof(key, advice, blinds, instances=None):
     # permutation products (permutation/prover.rs:81-255) and logup helper / aggregator
     pvals = [(adv, key.fixed_values, inst)[kind][ci] for kind, ci in c["perm_cols"]]
     zs = O.permutation_z(pvals, key.perm_values, c["degree"] - 2, c["k"], to_mont(key.omega), to_mont(beta),
-                         to_mont(gamma), bf, np.stack([np.stack([to_mont(v) for v in b]) for b in perm_bl]))
+                         to_mont(gamma), bf, np.stack([np.stack([to_mont(v) for v in b]) for b in perm_bl])) if S else []
     hs, Zs = [], []   # hs: per lookup, its helpers (one per chunk of inputs)
     for li, lk in enumerate(c["lookups"]):
         sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))

@@ -21,7 +21,9 @@ SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.g
           "trash": (OP.trash_circuit, OP.trash_instance),
           "selector": (OP.selector_circuit, OP.selector_instance),
           "tuple": (OP.tuple_circuit, OP.tuple_instance),
-          "parallel": (OP.parallel_circuit, OP.parallel_instance)}
+          "parallel": (OP.parallel_circuit, OP.parallel_instance),
+          "nolookup": (OP.nolookup_circuit, OP.nolookup_instance),
+          "bare": (OP.bare_circuit, OP.bare_instance)}
 
 
 class Circuit:
@@ -36,7 +38,8 @@ class Circuit:
         trashcan), "selector" (generic with a simple selector), "tuple"
         (generic with a lookup of the tuple (a, d) into (table, squares)) or
         "parallel" (lookups with parallel inputs: two helper chunks, and
-        two tuples in one chunk)."""
+        two tuples in one chunk), "nolookup" (generic without its lookup) or
+        "bare" (generic without lookup and permutation)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)

@@ -356,6 +356,28 @@ def test_parallel_lookup_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, bad, bl)])
 
 
+@pytest.mark.parametrize("shape", ["nolookup", "bare"])
+@pytest.mark.parametrize("k", [5, 9])
+def test_circuits_without_lookup_or_permutation_equal_oracle(ctx, k, shape):
+    """A circuit without lookups, and one without lookups and permutation
+    (no z, m, h or Z; a key without permutation polynomials): the device
+    transcript equals the oracle's and verifies, alone, in a batch with the
+    other shape's proofs and through the proving service."""
+    c = Circuit(ctx, k, seed=k + 130, shape=shape)
+    assert c.key.proof_len == len(c.oracle_proof(c.advice, c.blinds(4)))
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    other = Circuit(ctx, k, seed=k + 140, shape="generic", srs=(c.srs_buf, c.offs, c.desc, c.s))
+    mixed = mzk.create_proofs(ctx, [(c.key, c.advice, bl), (other.key, other.advice, other.blinds(6))])
+    assert mixed[0] == proof and other.verify(mixed[1])
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = srv.submit(c.key, c.advice, c.blinds(7))
+    assert c.verify(srv.wait(t)[0])
+    srv.close()
+
+
 def test_key_files_equal_oracle_and_read_back(ctx, k5):
     """VerifyingKey / ProvingKey files in the three SerdeFormats equal the
     oracle's bytes; a key read from a PK file has the same transcript_repr and

@@ -173,20 +173,22 @@ def test_full_size_closed_form(ctx, log_n):
 
 
 @pytest.mark.parametrize("log_n,extra", [(20, 0), (20, 777), (24, 0)])
-def test_host_buffers_two_part_upload(ctx, log_n, extra):
-    """Host-buffer MSMs of 2^20 points and more upload and compute in two
-    parts (the first ~30 % of the points, then the rest): the result equals
-    the device-resident call on the same data and the closed form, with
-    zero scalars and one repeated bucket straddling the part boundary."""
+def test_host_buffers_pipelined_upload(ctx, log_n, extra):
+    """Host-buffer MSMs of 2^20 points and more upload and compute in three
+    parts (ending at 12 %, 40 % and 100 % of the points, each part with its
+    own bucket set): the result equals the device-resident call on the same
+    data and the closed form, with zero scalars and one repeated bucket
+    straddling every part boundary."""
     n = (1 << log_n) + extra
     seed_s, seed_r = 0xC0DE + log_n + extra, 0xFACE + log_n + extra
     hs = ctx.gen_rand_fr(seed_s, n).download((n, 4))
     db = ctx.gen_bases(seed_r, n)
     hb = db.download((n, 12))
-    first = (n * 3 // 10) & ~1023
-    hs[first - 300:first + 300] = 0
-    hs[first - 2000:first - 1000] = O.fr_const(0)  # scalar one: all in bucket 1 of window 0
-    hs[first + 1000:first + 2000] = O.fr_const(0)
+    for frac in (0.12, 0.40):
+        end = int(n * frac) & ~1023
+        hs[end - 300:end + 300] = 0
+        hs[end - 2000:end - 1000] = O.fr_const(0)  # scalar one: all in bucket 1 of window 0
+        hs[end + 1000:end + 2000] = O.fr_const(0)
     hs[-5:] = 0
     ds = ctx.alloc(hs.nbytes)
     ds.upload(hs)
@@ -195,3 +197,25 @@ def test_host_buffers_two_part_upload(ctx, log_n, extra):
     del db, hb
     r = O.rand_fr(seed_r, n)
     assert np.array_equal(mzk.affine(got), O.g1_mul(O.g1_generator(), O.fr_inner_product(hs, r)))
+
+
+def test_phase_profiling_of_pipelined_and_device_msms(ctx):
+    """Per-phase device timing (mzk_ctx_set_profiling / phase_stats): a
+    host-buffer MSM of 2^20 points records every phase of each of its three
+    parts plus the reduction, a device-resident one each phase once; the
+    results equal the unprofiled calls."""
+    n = 1 << 20
+    ds = ctx.gen_rand_fr(0xBEEF, n)
+    db = ctx.gen_bases(0xCAFE, n)
+    hs, hb = ds.download((n, 4)), db.download((n, 12))
+    want = ctx.msm_device(ds, db, n)
+    for call, parts in ((lambda: ctx.msm_best(hs, hb), 3), (lambda: ctx.msm_device(ds, db, n), 1)):
+        ctx.set_profiling(True)
+        try:
+            assert np.array_equal(call(), want)
+            st = ctx.phase_stats()
+        finally:
+            ctx.set_profiling(False)
+        for phase in ("histogram", "scan", "scatter", "accumulate", "fixup"):
+            assert st[phase][1] == parts and st[phase][0] > 0, (phase, st)
+        assert st["reduce"][1] == 1

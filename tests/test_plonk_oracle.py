@@ -269,6 +269,32 @@ def test_parallel_lookup_proofs_verify():
         OP.create_proof(key, worse, bl)
 
 
+@pytest.mark.parametrize("shape", ["nolookup", "bare"])
+def test_circuits_without_lookup_or_permutation_verify(shape):
+    """A circuit without lookups (blinding factors one fewer, no m / h / Z in
+    the transcript) and one without lookups and permutation (no z either, no
+    permutation polynomials in the key): the proofs verify and a witness that
+    breaks a gate is rejected."""
+    k = 5
+    c = getattr(OP, shape + "_circuit")(k)
+    fixed, mapping, adv = getattr(OP, shape + "_instance")(k, 23)
+    assert OP.blinding_factors(c) == 6 and not c["lookups"]
+    s = O.rand_fr(57, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, shape.encode())
+    bl = [OP.to_int(v) for v in O.rand_fr(67, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl)
+    S = OP.n_perm_sets(c)
+    assert S == (2 if shape == "nolookup" else 0)
+    points = 4 + S + 4 + 2                                      # advice, z, limbs, f, pi
+    scalars_before_q = len(c["advice_queries"]) + len(c["fixed_queries"]) + len(c["perm_cols"]) + (3 * S - 1 if S else 0)
+    assert (len(proof) - 48 * points - 32 * scalars_before_q) // 32 in range(2, 8)
+    assert OP.verify(key, proof, OP.to_int(s))
+    bad = [a.copy() for a in adv]
+    bad[2][1] = OP.to_mont(OP.to_int(bad[2][1]) + 1)           # c breaks the first gate
+    assert not OP.verify(key, OP.create_proof(key, bad, bl), OP.to_int(s))
+
+
 def test_generic_circuit_proofs_verify():
     """Another circuit shape: two gates as one flattened program (with a(wX)),
     four permutation columns in two sets (z of the first set opened at
