@@ -475,6 +475,14 @@ typedef struct {
     const uint32_t *gate_poly_values;  /* value slot of each gate polynomial in `gates` */
     const int32_t *gate_poly_selector; /* its simple selector's fixed column, or -1 */
     const mzk_lookup_tuple *lookup_tuples; /* null, or one per lookup */
+    /* null, or every lookup input element as an expression: the programs of
+     * lookup 0's input tuples element by element, then lookup 1's, ...
+     * (n_inputs x width each, 1 x 1 without lookup_tuples), each evaluating
+     * one input expression (BatchedArgument's input_expressions, logup.rs:
+     * 47-58: any product or sum of fixed, advice and instance queries at any
+     * rotation) into result_idx; it then replaces input_advice.  A program
+     * that only reads an advice column at rotation 0 is that column. */
+    const mzk_flat_graph *lookup_input_programs;
 } mzk_circuit_desc;
 /* ParamsKZG's bases (params.rs:83-93) inside one DEVICE G1Affine buffer;
  * table_c > 0: srs is row 0 of a window table of that width and table_rows

@@ -922,7 +922,8 @@ class CircuitDesc(ctypes.Structure):
                 ("n_instance", ctypes.c_uint32), ("instance_queries", ctypes.c_void_p),
                 ("n_instance_queries", ctypes.c_uint32), ("n_trash", ctypes.c_uint32), ("trash", ctypes.c_void_p),
                 ("n_gate_polys", ctypes.c_uint32), ("gate_poly_values", ctypes.c_void_p),
-                ("gate_poly_selector", ctypes.c_void_p), ("lookup_tuples", ctypes.c_void_p)]
+                ("gate_poly_selector", ctypes.c_void_p), ("lookup_tuples", ctypes.c_void_p),
+                ("lookup_input_programs", ctypes.c_void_p)]
 
 
 class LookupTuple(ctypes.Structure):
@@ -934,10 +935,26 @@ class LookupTuple(ctypes.Structure):
 def lookup_columns(lk):
     """(input tuples, table tuple) of a lookup dict: "input" a column or a
     tuple (list) of columns, or "inputs" a list of such tuples (parallel
-    inputs); "table" a column or a tuple."""
+    inputs); "table" a column or a tuple.  An input element is an advice
+    column or an expression: a flattened program (dict with the FlatGraph
+    fields, or a FlatGraph) whose result_idx holds its value."""
     one = lambda v: list(v) if isinstance(v, (list, tuple)) else [v]
     ins = [one(t) for t in lk["inputs"]] if "inputs" in lk else [one(lk["input"])]
     return ins, one(lk["table"])
+
+
+def _program(g):
+    """A FlatGraph from a program dict (a FlatGraph is returned as it is)."""
+    if isinstance(g, FlatGraph):
+        return g
+    return build_flat_graph(g["constants"], g["rotations"], g["reads"], g["ops"], g["values_len"], g["beta_idx"],
+                            g["theta_idx"], g["trash_challenge_idx"], g["y_idx"], g["previous_value_idx"],
+                            g["result_idx"])
+
+
+def _column_program(col):
+    """The program of a plain lookup input: advice column `col` at rotation 0."""
+    return build_flat_graph(np.zeros((0, 4), np.uint64), [0], [(1, col, 0, 5)], [], 6, 0, 1, 2, 3, 4, 5)
 
 
 class SrsDesc(ctypes.Structure):
@@ -1036,7 +1053,8 @@ class PlonkKey:
     gate_advice (3), perm_cols [(kind 0 advice | 1 fixed | 2 instance,
     column)], lookups [{"input", "table", "selector" (None: constant one)}]
     (input and table a column or a list of up to four columns, compressed with
-    theta; or "inputs", a list of up to eight such input tuples),
+    theta; or "inputs", a list of up to eight such input tuples; an input
+    element may be an expression, a flattened program dict),
     n_instance and instance_queries [(column, rotation)] (optional),
     trashcans [{"program": flattened program, "selector": fixed column}]
     (optional), gate_polys [(value slot, simple selector fixed column or
@@ -1079,7 +1097,8 @@ class PlonkKey:
         lks = circuit["lookups"]
         cs.n_lookups = len(lks)
         shapes = [lookup_columns(lk) for lk in lks]
-        cs.lookups = arr(LookupShape, [LookupShape(ins[0][0], tab[0], -1 if lk["selector"] is None else lk["selector"])
+        col = lambda el: el if isinstance(el, (int, np.integer)) else 0   # a program's slot in the column fields
+        cs.lookups = arr(LookupShape, [LookupShape(col(ins[0][0]), tab[0], -1 if lk["selector"] is None else lk["selector"])
                                        for lk, (ins, tab) in zip(lks, shapes)])
         if any(len(ins) > 1 or len(tab) > 1 for ins, tab in shapes):
             tuples = []
@@ -1089,10 +1108,16 @@ class PlonkKey:
                 t = LookupTuple()
                 t.width, t.n_inputs = len(tab), len(ins)
                 for i, tup in enumerate(ins):
-                    t.input_advice[i][:len(tup)] = tup
+                    t.input_advice[i][:len(tup)] = [col(el) for el in tup]
                 t.table_fixed[:len(tab)] = tab
                 tuples.append(t)
             cs.lookup_tuples = arr(LookupTuple, tuples)
+        elements = [el for ins, _ in shapes for tup in ins for el in tup]
+        if any(not isinstance(el, (int, np.integer)) for el in elements):
+            progs = [_column_program(int(el)) if isinstance(el, (int, np.integer)) else _program(el)
+                     for el in elements]
+            keep.extend(progs)
+            cs.lookup_input_programs = arr(FlatGraph, progs)
         cs.n_instance = circuit.get("n_instance", 0)
         iq = circuit.get("instance_queries", [])
         cs.instance_queries = arr(Query, [Query(c, r) for c, r in iq])

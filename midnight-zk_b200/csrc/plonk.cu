@@ -267,6 +267,7 @@ struct PlonkKey {
         uint32_t width = 1;                  // the input and table tuples' length
         uint32_t n_inputs = 1;               // parallel input tuples
         uint32_t in[8][4] = {}, tab[4] = {}; // advice input tuples and fixed table columns
+        int32_t expr[8][4];                  // input element's program in lk_exprs, or -1: the column in[][]
         uint32_t per_helper = 1;             // inputs per helper chunk (the last may hold fewer)
         uint32_t h0 = 0;                     // the first helper's index among all lookups' helpers
         uint32_t n_helpers() const { return (n_inputs + per_helper - 1) / per_helper; }
@@ -278,6 +279,30 @@ struct PlonkKey {
     };
     std::vector<Lookup> lookups;
     uint32_t n_helpers = 0;  // helper polynomials of all lookups
+    // a validated copy of a flattened program
+    struct Program {
+        std::vector<uint64_t> consts;
+        std::vector<int32_t> rots;
+        std::vector<mzk_column_read> reads;
+        std::vector<mzk_flat_op> ops;
+        mzk_flat_graph g = {};
+        void assign(const mzk_flat_graph& src) {
+            consts.assign(src.constants, src.constants + 4 * (size_t)src.n_constants);
+            rots.assign(src.rotations, src.rotations + src.n_rotations);
+            reads.assign(src.reads, src.reads + src.n_reads);
+            ops.assign(src.ops, src.ops + src.n_ops);
+            g = src;
+            g.constants = consts.data();
+            g.rotations = rots.data();
+            g.reads = reads.data();
+            g.ops = ops.data();
+        }
+    };
+    // lookup input expressions that are not plain advice columns; the proof
+    // evaluates each over the Lagrange rows (multiplicities, helpers) and over
+    // the extended coset, where the lookup programs read it as advice column
+    // n_advice + its index
+    std::vector<Program> lk_exprs;
     // with more than one lookup the quotient takes them as helper programs
     // (one per helper chunk, indexed like the helpers; the single one-column
     // lookup uses the fused built-in term)
@@ -328,12 +353,52 @@ struct PlonkKey {
 
 namespace {
 
-// parallel lookup inputs per helper polynomial for inputs of degree one:
-// next_pow2(cs.degree() - 1) (nb_parallel_lookups_per_chunk, logup.rs:168-183)
-uint32_t lookup_per_helper(uint32_t degree) {
+// a program that only reads one advice column at rotation 0 into its result:
+// that column (else -1)
+int plain_advice(const mzk_flat_graph& g) {
+    if (g.n_ops || g.n_reads != 1) return -1;
+    const mzk_column_read& r = g.reads[0];
+    if (r.col_type != 1 || g.rotations[r.rot_idx] != 0 || r.dst != g.result_idx) return -1;
+    return (int)r.col_idx;
+}
+
+// Expression::degree (circuit.rs:1074-1086) of a program's result: a column
+// read has degree 1, a constant or challenge slot 0, a product the sum of
+// its factors' degrees, a sum the larger one
+uint32_t program_degree(const mzk_flat_graph& g) {
+    std::vector<uint32_t> deg(g.values_len, 0);
+    for (uint32_t i = 0; i < g.n_reads; i++) deg[g.reads[i].dst] = 1;
+    for (uint32_t i = 0; i < g.n_ops; i++) {
+        const mzk_flat_op& o = g.ops[i];
+        switch (o.kind) {
+            case MZK_FLAT_MUL: deg[o.dst] = deg[o.a] + deg[o.b]; break;
+            case MZK_FLAT_SQUARE: deg[o.dst] = 2 * deg[o.a]; break;
+            case MZK_FLAT_DOUBLE:
+            case MZK_FLAT_NEGATE: deg[o.dst] = deg[o.a]; break;
+            case MZK_FLAT_MULADD: deg[o.dst] = std::max(deg[o.a] + deg[o.b], deg[o.c]); break;
+            default: deg[o.dst] = std::max(deg[o.a], deg[o.b]); break;  // add, sub
+        }
+    }
+    return deg[g.result_idx];
+}
+
+// parallel lookup inputs per helper polynomial (nb_parallel_lookups_per_chunk,
+// logup.rs:168-183): next_pow2(cs.degree() - 1) / the inputs' largest degree
+uint32_t lookup_per_helper(uint32_t degree, uint32_t input_degree) {
     uint32_t p = 1;
     while (p < degree - 1) p <<= 1;
-    return p;
+    return p / std::max(1u, input_degree);
+}
+
+// the largest degree of lookup l's input expressions (1 for columns)
+uint32_t lookup_input_degree(const mzk_circuit_desc* cs, uint32_t l) {
+    if (!cs->lookup_input_programs) return 1;
+    uint32_t at = 0;
+    for (uint32_t i = 0; i < l; i++) at += cs->lookup_tuples ? cs->lookup_tuples[i].n_inputs * cs->lookup_tuples[i].width : 1;
+    const uint32_t m = cs->lookup_tuples ? cs->lookup_tuples[l].n_inputs * cs->lookup_tuples[l].width : 1;
+    uint32_t d = 0;
+    for (uint32_t e = 0; e < m; e++) d = std::max(d, program_degree(cs->lookup_input_programs[at + e]));
+    return d;
 }
 
 Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
@@ -462,19 +527,35 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
         // next_pow2(degree - 1) inputs (nb_parallel_lookups_per_chunk,
         // logup.rs:168-183), within cs.degree() as the reference's degree()
         // makes it (circuit.rs:2174-2199, logup.rs:186-212)
-        if (t.n_inputs > 1 && lookup_per_helper(cs->degree) + 1 > cs->degree)
-            return fail("parallel lookup inputs need cs.degree() - 1 to be a power of two");
+
         for (uint32_t e = 0; e < t.width; e++) {
             if (!queried(cs->fixed_queries, cs->n_fixed_queries, t.table_fixed[e]))
                 return fail("a lookup column is not queried at rotation 0");
-            for (uint32_t j = 0; j < t.n_inputs; j++)
+            for (uint32_t j = 0; j < t.n_inputs && !cs->lookup_input_programs; j++)
                 if (!queried(cs->advice_queries, cs->n_advice_queries, t.input_advice[j][e]))
                     return fail("a lookup column is not queried at rotation 0");
         }
     }
+    if (cs->lookup_input_programs) {
+        for (uint32_t i = 0, at = 0; i < cs->n_lookups; i++) {
+            const uint32_t m = cs->lookup_tuples ? cs->lookup_tuples[i].n_inputs * cs->lookup_tuples[i].width : 1;
+            for (uint32_t e = 0; e < m; e++, at++)
+                MZK_TRY(check_program(&cs->lookup_input_programs[at],
+                                      "lookup " + std::to_string(i) + " input " + std::to_string(e)));
+        }
+    }
+    // each helper constraint h prod_j (f_j + beta) = sum_j prod_(k != j) (f_k + beta)
+    // has degree 1 + (inputs of its chunk) x (input degree), within cs.degree()
+    // as the reference's degree() makes it (circuit.rs:2174-2199, logup.rs:186-212)
+    for (uint32_t i = 0; i < cs->n_lookups; i++) {
+        const uint32_t n_in = cs->lookup_tuples ? cs->lookup_tuples[i].n_inputs : 1;
+        const uint32_t d_in = lookup_input_degree(cs, i), per = lookup_per_helper(cs->degree, d_in);
+        if (per == 0 || std::min(per, n_in) * d_in + 1 > cs->degree)
+            return fail("lookup " + std::to_string(i) + ": its helper constraints exceed cs.degree()");
+    }
     for (uint32_t i = 0; i < cs->n_lookups; i++) {
         const mzk_lookup_shape& l = cs->lookups[i];
-        if (!queried(cs->advice_queries, cs->n_advice_queries, l.input_advice) ||
+        if ((!cs->lookup_input_programs && !queried(cs->advice_queries, cs->n_advice_queries, l.input_advice)) ||
             !queried(cs->fixed_queries, cs->n_fixed_queries, l.table_fixed) ||
             (l.selector_fixed >= 0 && !queried(cs->fixed_queries, cs->n_fixed_queries, (uint32_t)l.selector_fixed)))
             return fail("a lookup column is not queried at rotation 0");
@@ -540,8 +621,11 @@ size_t fixed_written(const PlonkKey& k) {
 // the selector (the quotient reads those from the first chunk only, as
 // evaluation.rs:1066-1069 does).  The partial products come from prefix and
 // suffix products: the same field values as the reference's per-j loops.
-// Values: 0, 1 (constants), beta, theta, trash challenge, y, the previous
-// value, then the reads and the ops.
+// An input expression that is not a plain advice column is read as the
+// extra advice column n_advice + its index (its values on the extended coset,
+// which the proof evaluates before the quotient).  Values: 0, 1 (constants),
+// beta, theta, trash challenge, y, the previous value, then the reads and
+// the ops.
 void build_lookup_programs(PlonkKey* key) {
     const Fr4 zero = host::fr_zero(), one = host::fr_one();
     key->lk_consts.assign(zero.l, zero.l + 4);
@@ -565,7 +649,8 @@ void build_lookup_programs(PlonkKey* key) {
             std::vector<uint32_t> in_at(m * w), tab_at(w);
             for (uint32_t j = 0; j < m; j++)
                 for (uint32_t e = 0; e < w; e++) {
-                    key->lk_reads.push_back({1, lk.in[i0 + j][e], 0, slot});
+                    const int32_t x = lk.expr[i0 + j][e];
+                    key->lk_reads.push_back({1, x >= 0 ? key->n_advice + (uint32_t)x : lk.in[i0 + j][e], 0, slot});
                     in_at[j * w + e] = slot++;
                 }
             uint32_t sel = 1;
@@ -755,7 +840,11 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     key->perm_index.assign(cs->perm_col_index, cs->perm_col_index + P);
     const uint32_t L = cs->n_lookups;
     key->lookups.resize(L);
-    for (uint32_t l = 0; l < L; l++) {
+    size_t n_programs = 0;  // lookup input programs given
+    for (uint32_t l = 0; l < L && cs->lookup_input_programs; l++)
+        n_programs += cs->lookup_tuples ? cs->lookup_tuples[l].n_inputs * cs->lookup_tuples[l].width : 1;
+    key->lk_exprs.reserve(n_programs);  // no reallocation: each Program's graph points into itself
+    for (uint32_t l = 0, at = 0; l < L; l++) {
         PlonkKey::Lookup& lk = key->lookups[l];
         lk.shape = cs->lookups[l];
         if (cs->lookup_tuples) {
@@ -771,9 +860,27 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
             lk.in[0][0] = lk.shape.input_advice;
             lk.tab[0] = lk.shape.table_fixed;
         }
-        lk.per_helper = lookup_per_helper(cs->degree);
+        for (uint32_t j = 0; j < 8; j++)
+            for (uint32_t e = 0; e < 4; e++) lk.expr[j][e] = -1;
+        for (uint32_t j = 0; j < lk.n_inputs && cs->lookup_input_programs; j++)
+            for (uint32_t e = 0; e < lk.width; e++) {
+                const mzk_flat_graph& g = cs->lookup_input_programs[at++];
+                const int col = plain_advice(g);
+                if (col >= 0) {
+                    lk.in[j][e] = (uint32_t)col;
+                } else {
+                    lk.expr[j][e] = (int32_t)key->lk_exprs.size();
+                    key->lk_exprs.emplace_back();
+                    key->lk_exprs.back().assign(g);
+                }
+            }
+        lk.per_helper = lookup_per_helper(cs->degree, lookup_input_degree(cs, l));
         lk.h0 = key->n_helpers;
         key->n_helpers += lk.n_helpers();
+    }
+    if (cs->n_advice + key->lk_exprs.size() > kQMaxAdvice) {
+        set_error("keygen: advice columns and lookup input expressions exceed 16 quotient columns");
+        return ERR_ARG;
     }
     key->srs = *srs;
     const uint32_t F = cs->n_fixed, u = key->u;
@@ -918,7 +1025,7 @@ Status keygen(Context* ctx, const Domain* d, const mzk_circuit_desc* cs, const m
     }
     // the quotient's built-in lookup term serves a single one-column lookup
     // without trashcans; otherwise every lookup goes to it as helper programs
-    bool tuples = false;
+    bool tuples = !key->lk_exprs.empty();
     for (auto& lk : key->lookups) tuples = tuples || lk.width > 1 || lk.n_inputs > 1;
     if (L > 1 || (L && (cs->n_trash || tuples))) build_lookup_programs(key.get());
     // VK commitments (Lagrange basis) as one batch
@@ -1220,6 +1327,8 @@ struct FsProof {
     // theta-compressed inputs (per input tuple) and table of a tuple lookup (else empty / null)
     std::vector<std::vector<Fr*>> f_lag;
     std::vector<Fr*> t_lag;
+    // the key's lookup input expressions over the Lagrange rows and the extended coset
+    std::vector<Fr*> e_lag, e_ext;
     std::vector<uint32_t*> counts;
     Fr *limbs = nullptr, *lin = nullptr, *f = nullptr, *fin = nullptr, *pi = nullptr, *tmp_a = nullptr,
        *tmp_b = nullptr;
@@ -1232,14 +1341,20 @@ struct FsProof {
     std::vector<Fr4> ev_adv, ev_fix, ev_pc, ev_sets, ev_lk, ev_inst, ev_trash, q_x3;
 };
 
+// input element e of lookup input tuple i over the Lagrange rows: its
+// expression's values, or its advice column
+const Fr* lookup_input_lag(const FsProof& p, const PlonkKey::Lookup& lk, uint32_t i, uint32_t e) {
+    return lk.expr[i][e] >= 0 ? p.e_lag[lk.expr[i][e]] : p.adv_lag[lk.in[i][e]];
+}
+
 size_t proof_scratch_elems(const PlonkKey* k) {
     const size_t n = k->n, E = (size_t)1 << k->dom->ext_k, A = k->n_advice, S = k->n_sets;
     const size_t L = k->lookups.size(), O = k->open_sets.size();
     size_t counts = 0;
     for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8 + (lk.width > 1 ? (lk.n_inputs + 1) * n : 0);
     return (A + k->n_instance + k->trash.size()) * (2 * n + E) + S * (3 * n + E) +
-           L * ((3 * n + E) + (3 * n + E)) + k->n_helpers * (2 * n + E) + k->qdeg * n + (4 + 2 * O + 2) * n +
-           k->n_blinds + counts;
+           L * ((3 * n + E) + (3 * n + E)) + k->n_helpers * (2 * n + E) + k->lk_exprs.size() * (n + E) +
+           k->qdeg * n + (4 + 2 * O + 2) * n + k->n_blinds + counts;
 }
 
 Status eval_many(Context* ctx, const std::vector<EvalTask>& in, std::vector<Fr4>& results, cudaStream_t st) {
@@ -1471,7 +1586,11 @@ std::vector<std::pair<int32_t, Fr4>> identities_at_x(const FsProof& p) {
             std::vector<Fr4> fb;
             for (uint32_t j = c * lk.per_helper; j < c * lk.per_helper + lk.chunk_inputs(c); j++) {
                 Fr4 f = host::fr_zero();
-                for (uint32_t e = 0; e < lk.width; e++) f = fr_add(fr_mul(f, p.theta), adv(lk.in[j][e]));
+                for (uint32_t e = 0; e < lk.width; e++) {
+                    const int32_t x = lk.expr[j][e];
+                    const Fr4 v = x >= 0 ? program_at_x(k->lk_exprs[x].g)[k->lk_exprs[x].g.result_idx] : adv(lk.in[j][e]);
+                    f = fr_add(fr_mul(f, p.theta), v);
+                }
                 fb.push_back(fr_add(f, p.beta));
             }
             Fr4 product = one, spp = host::fr_zero();
@@ -1652,6 +1771,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         }
         for (uint32_t h = 0; h < k->n_helpers; h++)
             p.h_lag.push_back(take(n)), p.h_coeff.push_back(take(n)), p.h_ext.push_back(take(E));
+        for (size_t x = 0; x < k->lk_exprs.size(); x++) p.e_lag.push_back(take(n)), p.e_ext.push_back(take(E));
         p.limbs = take((size_t)k->qdeg * n);
         p.lin = take(n), p.f = take(n), p.fin = take(n), p.pi = take(n);
         for (size_t s = 0; s < k->open_sets.size(); s++) {
@@ -1727,10 +1847,23 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     // ---- 2. multiplicities, beta, gamma ---------------------------------
     items.clear();
     MZK_CUDA_CHECK(cudaMemsetAsync(dmiss, 0, count * 4, st));
+    static const uint64_t kZero4[4] = {0, 0, 0, 0};
     for (size_t j = 0; j < count; j++) {
         FsProof& p = ps[j];
         const PlonkKey* k = p.key;
         const uint32_t n = k->n, u = k->u;
+        // the lookup input expressions at every row (evaluate over n rows,
+        // rotations wrapping, as compute_multiplicities_parallel does)
+        if (!k->lk_exprs.empty()) {
+            std::vector<const uint64_t*> fl(k->n_fixed), al(k->n_advice), il(k->n_instance);
+            for (uint32_t i = 0; i < k->n_fixed; i++) fl[i] = reinterpret_cast<const uint64_t*>(k->fixed_lag[i]);
+            for (uint32_t i = 0; i < k->n_advice; i++) al[i] = reinterpret_cast<const uint64_t*>(p.adv_lag[i]);
+            for (uint32_t i = 0; i < k->n_instance; i++) il[i] = reinterpret_cast<const uint64_t*>(p.inst_lag[i]);
+            for (size_t x = 0; x < k->lk_exprs.size(); x++)
+                MZK_TRY(flat_program_rows(ctx, k->dom, k->lk_exprs[x].g, fl.data(), k->n_fixed, al.data(), k->n_advice,
+                                          il.data(), k->n_instance, kZero4, p.theta.l, kZero4, kZero4,
+                                          reinterpret_cast<uint64_t*>(p.e_lag[x]), st));
+        }
         for (size_t l = 0; l < k->lookups.size(); l++) {
             const PlonkKey::Lookup& lk = k->lookups[l];
             const Fr* sel = lk.shape.selector_fixed >= 0 ? k->fixed_lag[lk.shape.selector_fixed] : nullptr;
@@ -1738,7 +1871,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             for (uint32_t i = 0; i < lk.n_inputs; i++) {  // every input tuple counts into one m
                 LookupInputs li{};
                 li.width = lk.width;
-                for (uint32_t e = 0; e < lk.width; e++) li.col[e] = p.adv_lag[lk.in[i][e]];
+                for (uint32_t e = 0; e < lk.width; e++) li.col[e] = lookup_input_lag(p, lk, i, e);
                 k_lookup_count<<<grid_of(ctx, u), kThreads, 0, st>>>(li, sel, u, lk.uniq, lk.n_uniq, p.counts[l],
                                                                      static_cast<uint32_t*>(dmiss) + j);
                 MZK_LAUNCH_CHECK(ctx);
@@ -1788,7 +1921,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
                 comp.push_back(ts);
                 for (uint32_t i = 0; i < lk.n_inputs; i++) {
                     LinSpec fs{p.f_lag[l][i], k->n, {}};
-                    for (uint32_t e = 0; e < lk.width; e++) fs.terms.push_back({p.adv_lag[lk.in[i][e]], k->n, pw[e]});
+                    for (uint32_t e = 0; e < lk.width; e++) fs.terms.push_back({lookup_input_lag(p, lk, i, e), k->n, pw[e]});
                     comp.push_back(fs);
                 }
             }
@@ -1834,7 +1967,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             const uint32_t H = lk.n_helpers();
             std::vector<const uint64_t*> in(lk.n_inputs);
             for (uint32_t i = 0; i < lk.n_inputs; i++)
-                in[i] = reinterpret_cast<const uint64_t*>(tuple ? p.f_lag[l][i] : p.adv_lag[lk.in[i][0]]);
+                in[i] = reinterpret_cast<const uint64_t*>(tuple ? p.f_lag[l][i] : lookup_input_lag(p, lk, i, 0));
             std::vector<uint64_t*> ho(H);
             std::vector<uint32_t> cols(H);
             for (uint32_t c = 0; c < H; c++) {
@@ -1944,12 +2077,19 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         for (uint32_t i = 0; i < k->n_fixed; i++) fixed[i] = reinterpret_cast<const uint64_t*>(k->fixed_ext[i]);
         for (uint32_t i = 0; i < k->n_perm; i++) sig[i] = reinterpret_cast<const uint64_t*>(k->perm_ext[i]);
         for (uint32_t s = 0; s < k->n_sets; s++) zs[s] = reinterpret_cast<const uint64_t*>(p.z_ext[s]);
+        // the lookup input expressions on the extended coset, read by the
+        // lookup programs as the advice columns after the circuit's
+        for (size_t x = 0; x < k->lk_exprs.size(); x++)
+            MZK_TRY(flat_program_rows(ctx, d, k->lk_exprs[x].g, fixed.data(), k->n_fixed, adv.data(), k->n_advice,
+                                      inst.data(), k->n_instance, kZero4, p.theta.l, kZero4, kZero4,
+                                      reinterpret_cast<uint64_t*>(p.e_ext[x]), st, true));
+        for (size_t x = 0; x < k->lk_exprs.size(); x++) adv.push_back(reinterpret_cast<const uint64_t*>(p.e_ext[x]));
         mzk_quotient_desc q;
         std::memset(&q, 0, sizeof(q));
         q.k = d->k;
         q.extended_k = d->ext_k;
         q.advice = adv.data();
-        q.n_advice = k->n_advice;
+        q.n_advice = (uint32_t)adv.size();
         q.fixed = fixed.data();
         q.n_fixed = k->n_fixed;
         std::memcpy(q.gate_fixed, k->gate_fixed, sizeof(q.gate_fixed));

@@ -347,12 +347,14 @@ Status pack_programs(Context* ctx, const Domain* d, const mzk_quotient_desc* des
 // One flattened program evaluated at every row of the n-point domain over
 // Lagrange columns (rotations are whole rows): the trash argument's
 // compressed constraint expressions (trash/prover.rs, `evaluate` over the
-// Lagrange values, folded with the trash challenge by the program itself).
+// Lagrange values, folded with the trash challenge by the program itself)
+// and the lookup input expressions.  extended: at every row of the extended
+// coset over coset columns (the lookup input expressions the quotient reads).
 Status flat_program_rows(Context* ctx, const Domain* d, const mzk_flat_graph& g, const uint64_t* const* fixed,
                          uint32_t n_fixed, const uint64_t* const* advice, uint32_t n_advice,
                          const uint64_t* const* instance, uint32_t n_instance, const uint64_t beta[4],
                          const uint64_t theta[4], const uint64_t trash[4], const uint64_t y[4], uint64_t* out,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool extended) {
     if (n_fixed > kQMaxFixed || n_advice > kQMaxAdvice || n_instance > kQMaxInstance) {
         set_error("flat program: too many columns");
         return ERR_ARG;
@@ -364,12 +366,12 @@ Status flat_program_rows(Context* ctx, const Domain* d, const mzk_flat_graph& g,
     std::memcpy(desc.trash_challenge, trash, 32);
     std::memcpy(desc.y, y, 32);
     const uint32_t n_cols[3] = {n_fixed, n_advice, n_instance};
-    const uint32_t n = 1u << d->k;
+    const uint32_t log_scale = extended ? d->ext_k - d->k : 0u, n = 1u << (d->k + log_scale);
     std::vector<uint32_t> W;
     std::string err;
     GatesParams gp;
     std::memset(&gp, 0, sizeof(gp));
-    gp.prog = pack_program(W, g, n_cols, &desc, 0, n, err);
+    gp.prog = pack_program(W, g, n_cols, &desc, log_scale, n, err);
     if (!err.empty()) {
         set_error("flat program: " + err);
         return ERR_ARG;
@@ -385,7 +387,7 @@ Status flat_program_rows(Context* ctx, const Domain* d, const mzk_flat_graph& g,
     MZK_CUDA_CHECK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, st));
     MZK_CUDA_CHECK(cudaStreamSynchronize(st));  // the pinned staging is reused by the next call
     gp.words = static_cast<const uint32_t*>(dev);
-    gp.log_n = d->k;
+    gp.log_n = d->k + log_scale;
     gp.out = reinterpret_cast<Fr*>(out);
     const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 127) / 128, (uint32_t)ctx->num_sms * 8));
     k_gates_flat<<<blocks, 128, 0, st>>>(gp);

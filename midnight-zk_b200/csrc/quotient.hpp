@@ -107,12 +107,14 @@ Status ntt_sequence(Context* ctx, const Domain* d, const void* const* lag, Fr* c
 Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, uint32_t flags, cudaStream_t st);
 uint64_t proof_device_bytes(const mzk_plonk_key* key);
 uint64_t proof_rows(const mzk_plonk_key* key);  // 2^k of the key
-// one flattened program at every row of the n-point domain over Lagrange columns
+// one flattened program at every row of the n-point domain over Lagrange
+// columns, or (extended) at every row of the extended coset over the
+// columns' coset values, a rotation of r rows then 2^(ext_k - k) r rows
 Status flat_program_rows(Context* ctx, const Domain* d, const mzk_flat_graph& g, const uint64_t* const* fixed,
                          uint32_t n_fixed, const uint64_t* const* advice, uint32_t n_advice,
                          const uint64_t* const* instance, uint32_t n_instance, const uint64_t beta[4],
                          const uint64_t theta[4], const uint64_t trash[4], const uint64_t y[4], uint64_t* out,
-                         cudaStream_t st);
+                         cudaStream_t st, bool extended = false);
 Status quotient_eval_device(Context* ctx, const Domain* d, const mzk_quotient_desc* desc, int divide, void* d_out,
                             cudaStream_t st);
 

@@ -462,6 +462,34 @@ def bare_instance(k, seed):
     return fixed, mapping[:0], adv
 
 
+def _expr_program(rotations, reads, ops, values_len, result_idx):
+    """A lookup input expression as a flattened program: constants 0 and 1,
+    challenge slots 2-6 (beta, theta, trash challenge, y, previous value)."""
+    return {"constants": [to_mont(0), to_mont(1)], "rotations": rotations, "reads": reads, "ops": ops,
+            "values_len": values_len, "beta_idx": 2, "theta_idx": 3, "trash_challenge_idx": 4, "y_idx": 5,
+            "previous_value_idx": 6, "result_idx": result_idx}
+
+
+def expr_circuit(k):
+    """generic_circuit with the table of squares and lookups whose inputs are
+    expressions: a(wX) and d - a^2 + a into the table, selected by q4 (one on
+    the rows before the last usable one, where a(wX) is still a table value;
+    the second input has degree 2, so a helper takes two inputs at degree 5),
+    and the tuple (a, a * a) into (table, squares) without a selector."""
+    c = generic_circuit(k, two_lookups=True)
+    a_next = _expr_program([0, 1], [(1, 0, 1, 7)], [], 8, 7)
+    d_minus = _expr_program([0], [(1, 3, 0, 7), (1, 0, 0, 8)], [(2, 9, 8, 8, 0), (1, 10, 7, 9, 0), (0, 11, 10, 8, 0)],
+                            12, 11)
+    a_sq = _expr_program([0], [(1, 0, 0, 7)], [(3, 8, 7, 0, 0)], 9, 8)
+    c["lookups"] = [{"inputs": [[a_next], [d_minus]], "table": 4, "selector": 3},
+                    {"input": [0, a_sq], "table": [4, 6], "selector": None}]
+    return c
+
+
+def expr_instance(k, seed):
+    return generic_instance(k, seed, two_lookups=True, circuit=expr_circuit(k))
+
+
 def parallel_circuit(k):
     """generic_circuit with the table of squares and three more advice
     columns e, f, g (queried at rotation 0, in no gate nor permutation), and
@@ -790,6 +818,12 @@ def identities(key, ev, ch):
     fq = lambda col: fix[query_index(c["fixed_queries"], col)]
     iq = lambda col: ins[query_index(c.get("instance_queries", []), col)]
     col_eval = lambda kind, col: (aq, fq, iq)[kind](col)
+
+    def read_query(col_type, col, rot):
+        qs = (c["fixed_queries"], c["advice_queries"], c.get("instance_queries", []))[col_type]
+        return (fix, adv, ins)[col_type][query_index(qs, col, rot)]
+    # a lookup input element at x: its advice column's evaluation, or its expression's value
+    lookup_input_at = lambda el: aq(el) if is_column(el) else program_at(el, read_query, ch)
     if c.get("gates") is not None:
         def read(col_type, col, rot):
             if col_type == 0:
@@ -843,8 +877,8 @@ def identities(key, ev, ch):
             fb = []
             for tup in chunk:
                 f = 0
-                for col in tup:
-                    f = (f * theta + aq(col)) % R
+                for el in tup:
+                    f = (f * theta + lookup_input_at(el)) % R
                 fb.append((f + beta) % R)
             product, spp = 1, 0
             for j in range(len(fb)):
@@ -1004,10 +1038,14 @@ def create_proof(key, advice, blinds, instances=None):
     theta = tr.squeeze()
     # multiplicities (logup/prover.rs:95-184), committed in delta form
     ms, fs, ts = [], [], []
-    for lk in c["lookups"]:
+    # the input expressions over the Lagrange rows (compute_multiplicities_parallel)
+    ex_lag = {pos: trash_column(key, g, adv, inst, 0, theta, 0) for pos, g in lookup_exprs(c)}
+    for li, lk in enumerate(c["lookups"]):
         sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
         ins, tab = lookup_columns(lk)
-        fl = [adv[tup[0]] if len(tup) == 1 else compress_columns([adv[i] for i in tup], theta) for tup in ins]
+        col = lambda ti, ei, el: adv[el] if is_column(el) else ex_lag[(li, ti, ei)]
+        fl = [col(ti, 0, tup[0]) if len(tup) == 1 else compress_columns([col(ti, ei, el) for ei, el in enumerate(tup)],
+                                                                         theta) for ti, tup in enumerate(ins)]
         t = key.fixed_values[tab[0]] if len(tab) == 1 else compress_columns([key.fixed_values[i] for i in tab], theta)
         ms.append(compute_multiplicities(sel, fl, t, u, take(bf + 1)))
         fs.append(fl)
@@ -1026,7 +1064,7 @@ def create_proof(key, advice, blinds, instances=None):
     hs, Zs = [], []   # hs: per lookup, its helpers (one per chunk of inputs)
     for li, lk in enumerate(c["lookups"]):
         sel = key.fixed_values[lk["selector"]] if lk["selector"] is not None else np.tile(O.fr_const(0), (n, 1))
-        per = lookup_per_helper(c)
+        per = lookup_per_helper(c, lk)
         chunks = [fs[li][i:i + per] for i in range(0, len(fs[li]), per)]
         hl, Z = O.logup(chunks, ts[li], sel, ms[li], to_mont(beta), bf, np.stack([to_mont(v) for v in log_bl[li]]))
         hs.append(list(hl))
@@ -1182,7 +1220,8 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     d.chunk_len, d.blinding_factors = c["degree"] - 2, key.bf
     tcs = c.get("trashcans", [])
     shapes = [lookup_columns(lk) for lk in c["lookups"]]
-    builtin = len(shapes) == 1 and not tcs and len(shapes[0][0]) == 1 and len(shapes[0][1]) == 1
+    builtin = (len(shapes) == 1 and not tcs and len(shapes[0][0]) == 1 and len(shapes[0][1]) == 1
+               and is_column(shapes[0][0][0][0]))
     if builtin:
         lk = c["lookups"][0]
         d.has_lookup = 1
@@ -1208,13 +1247,23 @@ def quotient(key, adv_e, z_e, m_e, h_e, Z_e, y, beta, gamma, theta, threads=None
     # as one helper program per chunk (Evaluator::lookups_flat, :691-770) and
     # every trashcan's term (:1093-1109), then the division by t(X)
     v = dom.quotient_eval(d, False, threads, gate_values)
+    # the input expressions on the extended coset, read as advice columns
+    # after the circuit's
+    zero = np.zeros(4, np.uint64)
+    exprs = lookup_exprs(c)
+    ex_e = [O.flat_gates_eval(g, key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k, zero, to_mont(theta), zero,
+                              zero) for _, g in exprs]
+    ex_col = {pos: len(adv_e) + j for j, (pos, _) in enumerate(exprs)}
     lks = []
     for li, lk in enumerate(c["lookups"]):
-        progs = [lookup_program(lk, chunk, first=j == 0) for j, chunk in enumerate(lookup_chunks(c, lk))]
+        per = lookup_per_helper(c, lk)
+        col = lambda ti, ei, el: el if is_column(el) else ex_col[(li, ti, ei)]
+        progs = [lookup_program(lk, chunk, first=j == 0, col=col, t0=j * per)
+                 for j, chunk in enumerate(lookup_chunks(c, lk))]
         lks.append({"programs": [g for g, _ in progs], "outputs": [o for _, o in progs], "helpers": list(h_e[li]),
                     "aggregator": Z_e[li], "multiplicities": m_e[li]})
     tas = [{"program": tc["program"], "selector": tc["selector"], "trash": trash_e[ti]} for ti, tc in enumerate(tcs)]
-    v = O.flat_tail_eval(v, key.fixed_cosets, adv_e, inst_e, c["k"], dom.extended_k, to_mont(beta), to_mont(theta),
+    v = O.flat_tail_eval(v, key.fixed_cosets, list(adv_e) + ex_e, inst_e, c["k"], dom.extended_k, to_mont(beta), to_mont(theta),
                          to_mont(trash), to_mont(y), key.l0, key.l_last, key.l_active, lookups=lks, trashcans=tas)
     return dom.divide_by_vanishing_poly(v)
 
@@ -1229,21 +1278,52 @@ def lookup_columns(lk):
     return ins, one(lk["table"])
 
 
-def lookup_per_helper(circuit):
-    """Parallel inputs per helper polynomial for inputs of degree one:
-    next_pow2(cs.degree() - 1) (nb_parallel_lookups_per_chunk, logup.rs:
-    168-183)."""
+def is_column(el):
+    """A lookup input element that is an advice column (else an expression)."""
+    return isinstance(el, (int, np.integer))
+
+
+def program_degree(graph):
+    """Expression::degree (plonk/circuit.rs:1074-1086) of a program's result:
+    a column read 1, a constant or challenge slot 0, a product the sum of its
+    factors' degrees, a sum the larger one."""
+    deg = [0] * graph["values_len"]
+    for _, _, _, dst in graph["reads"]:
+        deg[dst] = 1
+    for kind, dst, a, b, cc in graph["ops"]:
+        deg[dst] = (max(deg[a], deg[b]) if kind in (0, 1) else deg[a] + deg[b] if kind == 2 else
+                    2 * deg[a] if kind == 3 else deg[a] if kind in (4, 5) else max(deg[a] + deg[b], deg[cc]))
+    return deg[graph["result_idx"]]
+
+
+def lookup_exprs(circuit):
+    """The lookup input elements that are expressions, in order (lookup,
+    input tuple, element): [((lookup, tuple, element), program)]."""
+    out = []
+    for li, lk in enumerate(circuit["lookups"]):
+        for ti, tup in enumerate(lookup_columns(lk)[0]):
+            out.extend(((li, ti, ei), el) for ei, el in enumerate(tup) if not is_column(el))
+    return out
+
+
+def lookup_per_helper(circuit, lk=None):
+    """Parallel inputs per helper polynomial (nb_parallel_lookups_per_chunk,
+    logup.rs:168-183): next_pow2(cs.degree() - 1) over the largest degree
+    of the lookup's input expressions (1 for columns)."""
     p = 1
     while p < circuit["degree"] - 1:
         p *= 2
-    return p
+    d = 1
+    if lk is not None:
+        d = max(1 if is_column(el) else program_degree(el) for tup in lookup_columns(lk)[0] for el in tup)
+    return p // d
 
 
 def lookup_chunks(circuit, lk):
     """The lookup's input tuples split into helper chunks
     (chunk_by_degree, logup.rs:289-300)."""
     ins, _ = lookup_columns(lk)
-    per = lookup_per_helper(circuit)
+    per = lookup_per_helper(circuit, lk)
     return [ins[i:i + per] for i in range(0, len(ins), per)]
 
 
@@ -1254,7 +1334,7 @@ def compress_columns(cols, theta):
     return O.poly_inner_product(list(cols), [to_mont(pow(theta, w - 1 - e, R)) for e in range(w)])
 
 
-def lookup_program(lk, chunk, first=True):
+def lookup_program(lk, chunk, first=True, col=lambda ti, ei, el: el, t0=0):
     """The helper program of one chunk of a lookup's input tuples
     (Evaluator::lookups_flat, evaluation.rs:691-770): values 0, 1
     (constants), beta, theta, trash challenge, y, the previous value, the
@@ -1262,8 +1342,11 @@ def lookup_program(lk, chunk, first=True):
     first column) plus beta, f_j; the product of the f_j and the sum of
     partial products sum_j prod_{i!=j} f_i (each by a loop over i, as the
     reference builds it; one input: the constant one); for the first chunk
-    the compressed table plus beta and the selector.  Returns (graph,
-    (sum_partial_products, product, table, selector) indices)."""
+    the compressed table plus beta and the selector.  col(tuple, element,
+    input) gives the advice column a read takes (an expression input's
+    values sit in an extra column), t0 the index of the chunk's first tuple.
+    Returns (graph, (sum_partial_products, product, table, selector)
+    indices)."""
     _, tab = lookup_columns(lk)
     reads, ops = [], []
     slot = [7]
@@ -1278,15 +1361,15 @@ def lookup_program(lk, chunk, first=True):
         return d
     in_at = [[None] * len(tup) for tup in chunk]
     for j, tup in enumerate(chunk):
-        for e, col in enumerate(tup):
+        for e, el in enumerate(tup):
             in_at[j][e] = new()
-            reads.append((1, col, 0, in_at[j][e]))
+            reads.append((1, col(t0 + j, e, el), 0, in_at[j][e]))
     table = sel = 1
     if first:
         tab_at = []
-        for col in tab:
+        for tcol in tab:
             tab_at.append(new())
-            reads.append((0, col, 0, tab_at[-1]))
+            reads.append((0, tcol, 0, tab_at[-1]))
         if lk["selector"] is not None:
             sel = new()
             reads.append((0, lk["selector"], 0, sel))

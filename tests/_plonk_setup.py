@@ -23,7 +23,8 @@ SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.g
           "tuple": (OP.tuple_circuit, OP.tuple_instance),
           "parallel": (OP.parallel_circuit, OP.parallel_instance),
           "nolookup": (OP.nolookup_circuit, OP.nolookup_instance),
-          "bare": (OP.bare_circuit, OP.bare_instance)}
+          "bare": (OP.bare_circuit, OP.bare_instance),
+          "expr": (OP.expr_circuit, OP.expr_instance)}
 
 
 class Circuit:
@@ -38,8 +39,9 @@ class Circuit:
         trashcan), "selector" (generic with a simple selector), "tuple"
         (generic with a lookup of the tuple (a, d) into (table, squares)) or
         "parallel" (lookups with parallel inputs: two helper chunks, and
-        two tuples in one chunk), "nolookup" (generic without its lookup) or
-        "bare" (generic without lookup and permutation)."""
+        two tuples in one chunk), "nolookup" (generic without its lookup),
+        "bare" (generic without lookup and permutation) or "expr" (lookups
+        whose inputs are expressions: a rotation, products)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)

@@ -356,6 +356,41 @@ def test_parallel_lookup_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, bad, bl)])
 
 
+@pytest.mark.parametrize("k", [5, 9])
+def test_expression_lookup_inputs_equal_oracle(ctx, k):
+    """Lookup inputs that are expressions (a(wX) and d - a^2 + a into the
+    table, the tuple (a, a * a) into (table, squares)): each evaluated over
+    the Lagrange rows for the multiplicities and helpers and over the
+    extended coset for the quotient, and at x for the identities.  The device
+    transcript equals the oracle's and verifies, in a batch and through the
+    proving service; an input outside the table is refused; an input
+    expression whose degree leaves no room for a helper constraint is refused
+    by keygen."""
+    c = Circuit(ctx, k, seed=k + 150, shape="expr")
+    assert c.key.proof_len == len(c.oracle_proof(c.advice, c.blinds(4)))
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    both = mzk.create_proofs(ctx, [(c.key, c.advice, bl), (c.key, c.advice, c.blinds(6))])
+    assert both[0] == proof and c.verify(both[1])
+    srv = mzk.ProvingServer(ctx, max_batch=4)
+    t = srv.submit(c.key, c.advice, c.blinds(7))
+    assert c.verify(srv.wait(t)[0])
+    srv.close()
+    bad = [a.copy() for a in c.advice]
+    bad[0][3] = OP.to_mont((1 << 16) + 9)                       # a(wX) on row 2 outside the table
+    with pytest.raises(mzk.MzkError, match="not in the table"):
+        mzk.create_proofs(ctx, [(c.key, bad, bl)])
+    if k == 5:
+        deep = OP.expr_circuit(k)
+        a5 = OP._expr_program([0], [(1, 0, 0, 7)], [(3, 8, 7, 0, 0), (3, 9, 8, 0, 0), (2, 10, 9, 7, 0)], 11, 10)
+        deep["lookups"] = [{"input": a5, "table": 4, "selector": 3}]   # a^5: degree 5 > next_pow2(5 - 1)
+        deep["blinding_factors"] = OP.blinding_factors(c.circuit)
+        with pytest.raises(mzk.MzkError, match="exceed cs.degree"):
+            mzk.PlonkKey(ctx, c.dom, deep, c.desc, c.fixed, c.mapping, b"deep")
+
+
 @pytest.mark.parametrize("shape", ["nolookup", "bare"])
 @pytest.mark.parametrize("k", [5, 9])
 def test_circuits_without_lookup_or_permutation_equal_oracle(ctx, k, shape):

@@ -269,6 +269,29 @@ def test_parallel_lookup_proofs_verify():
         OP.create_proof(key, worse, bl)
 
 
+def test_expression_lookup_inputs_verify():
+    """Lookup inputs that are expressions (a(wX), d - a^2 + a, a * a): their
+    degree sets the inputs per helper (two at degree 5 for a degree-2 input),
+    the proof verifies, and a witness whose rotated input leaves the table
+    on a selected row is refused by the prover."""
+    k = 5
+    c = OP.expr_circuit(k)
+    assert [OP.lookup_per_helper(c, lk) for lk in c["lookups"]] == [2, 2]
+    assert [len(OP.lookup_chunks(c, lk)) for lk in c["lookups"]] == [1, 1]
+    assert len(OP.lookup_exprs(c)) == 3 and OP.blinding_factors(c) == 3 + 2 + 3
+    fixed, mapping, adv = OP.expr_instance(k, 24)
+    s = O.rand_fr(58, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"expr")
+    bl = [OP.to_int(v) for v in O.rand_fr(68, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl)
+    assert OP.verify(key, proof, OP.to_int(s))
+    bad = [a.copy() for a in adv]
+    bad[0][3] = OP.to_mont((1 << 16) + 9)                       # a(wX) on row 2 outside the table
+    with pytest.raises(ValueError):
+        OP.create_proof(key, bad, bl)
+
+
 @pytest.mark.parametrize("shape", ["nolookup", "bare"])
 def test_circuits_without_lookup_or_permutation_verify(shape):
     """A circuit without lookups (blinding factors one fewer, no m / h / Z in
