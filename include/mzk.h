@@ -434,15 +434,15 @@ typedef struct {
  * Permutation columns: kind 0 advice, 1 fixed, 2 instance; sets of degree - 2 columns.
  * The query lists and their order are the reference's (they fix the order
  * of the evaluations in the proof).  Limits: 16 advice, 16 fixed, 16
- * permutation columns (8 sets), at most 4 lookups (each one advice column,
- * or a tuple of them, into one fixed table column or a tuple of them; their
- * multiplicities, helpers and aggregators
+ * permutation columns (8 sets), at most 8 lookups (each one advice column
+ * or expression, or a tuple of them, into one fixed table column or a tuple
+ * of them; their multiplicities, helpers and aggregators
  * are committed, evaluated and opened lookup by lookup, as logup/prover.rs
  * does), at most 4 instance columns (the reference's default, without the
  * committed-instances feature: every proof's instance values are absorbed
  * into its transcript, compute_instances, prover.rs:475-539; gates may read
  * them, `col_type` 2, at their queried rotations, and permutation columns of
- * kind 2 are instance columns), at most 4 trashcans (trash/prover.rs: each an
+ * kind 2 are instance columns), at most 8 trashcans (trash/prover.rs: each an
  * mzk_trash_arg whose program compresses the constraint expressions with the
  * trash challenge, reading only queried columns, and whose selector is a
  * fixed column queried at rotation 0; its `trash` pointer is not used here:

@@ -59,8 +59,8 @@ using host::Fr4;
 namespace {
 
 constexpr uint32_t kThreads = 256;
-constexpr uint32_t kMaxProofLookups = 4;  // lookups of one circuit in create_proof
-constexpr uint32_t kMaxProofTrash = 4;    // trashcans of one circuit in create_proof
+constexpr uint32_t kMaxProofLookups = kQMaxLookups;  // lookups of one circuit in create_proof
+constexpr uint32_t kMaxProofTrash = kQMaxTrash;      // trashcans of one circuit in create_proof
 
 inline Fr to_dev(const Fr4& a) {
     Fr r;
@@ -414,7 +414,7 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
         return fail("1..16 advice and at most 16 fixed columns");
     if (cs->n_perm_cols > kQMaxPermCols || (cs->n_perm_cols + cs->degree - 3) / (cs->degree - 2) > kQMaxSets)
         return fail("at most 16 permutation columns in at most 8 sets");
-    if (cs->n_lookups > kMaxProofLookups) return fail("at most 4 lookups");
+    if (cs->n_lookups > kMaxProofLookups) return fail("at most 8 lookups");
     if ((cs->n_advice_queries && !cs->advice_queries) || (cs->n_fixed_queries && !cs->fixed_queries) ||
         (cs->n_instance_queries && !cs->instance_queries))
         return fail("null query list");
@@ -485,7 +485,7 @@ Status check_circuit(const Domain* d, const mzk_circuit_desc* cs) {
         }
         return OK;
     };
-    if (cs->n_trash > kMaxProofTrash || (cs->n_trash && !cs->trash)) return fail("at most 4 trashcans");
+    if (cs->n_trash > kMaxProofTrash || (cs->n_trash && !cs->trash)) return fail("at most 8 trashcans");
     for (uint32_t t = 0; t < cs->n_trash; t++) {
         MZK_TRY(check_program(&cs->trash[t].program, "trashcan " + std::to_string(t)));
         if (!queried(cs->fixed_queries, cs->n_fixed_queries, cs->trash[t].selector_fixed))

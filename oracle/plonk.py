@@ -569,6 +569,26 @@ def trash_instance(k, seed):
     return generic_instance(k, seed, circuit=trash_circuit(k))
 
 
+def many_circuit(k):
+    """generic_circuit with the table of squares, five lookups (a into the
+    table with and without the selector, d into the squares with and
+    without it, the tuple (a, d) into (table, squares) with q4) and five
+    trashcans (trash_circuit's program, each with its own selector column
+    among q3 and the lookup selector): more lookups and trashcans than a
+    smaller key takes."""
+    c = generic_circuit(k, two_lookups=True)
+    c["lookups"] = [{"input": 0, "table": 4, "selector": 5}, {"input": 3, "table": 6, "selector": None},
+                    {"input": 0, "table": 4, "selector": None}, {"input": 3, "table": 6, "selector": 5},
+                    {"input": [0, 3], "table": [4, 6], "selector": 3}]
+    program = trash_circuit(k)["trashcans"][0]["program"]
+    c["trashcans"] = [{"program": program, "selector": sel} for sel in (2, 2, 5, 2, 5)]
+    return c
+
+
+def many_instance(k, seed):
+    return generic_instance(k, seed, two_lookups=True, circuit=many_circuit(k))
+
+
 INSTANCE_ROWS = 3
 
 

@@ -24,7 +24,8 @@ SHAPES = {"config3": (OP.config3_circuit, OP.config3_instance), "generic": (OP.g
           "parallel": (OP.parallel_circuit, OP.parallel_instance),
           "nolookup": (OP.nolookup_circuit, OP.nolookup_instance),
           "bare": (OP.bare_circuit, OP.bare_instance),
-          "expr": (OP.expr_circuit, OP.expr_instance)}
+          "expr": (OP.expr_circuit, OP.expr_instance),
+          "many": (OP.many_circuit, OP.many_instance)}
 
 
 class Circuit:
@@ -40,8 +41,9 @@ class Circuit:
         (generic with a lookup of the tuple (a, d) into (table, squares)) or
         "parallel" (lookups with parallel inputs: two helper chunks, and
         two tuples in one chunk), "nolookup" (generic without its lookup),
-        "bare" (generic without lookup and permutation) or "expr" (lookups
-        whose inputs are expressions: a rotation, products)."""
+        "bare" (generic without lookup and permutation), "expr" (lookups
+        whose inputs are expressions: a rotation, products) or "many" (five
+        lookups and five trashcans)."""
         self.ctx, self.k, self.seed = ctx, k, seed
         make_circuit, make_instance = SHAPES[shape]
         c = make_circuit(k)

@@ -356,6 +356,21 @@ def test_parallel_lookup_proof_equals_oracle(ctx, k):
         mzk.create_proofs(ctx, [(c.key, bad, bl)])
 
 
+@pytest.mark.parametrize("k", [6, 9])
+def test_five_lookups_and_five_trashcans_equal_oracle(ctx, k):
+    """Five lookups and five trashcans (more than a key of four of each
+    takes): the device transcript equals the oracle's and verifies, alone
+    and in a batch."""
+    c = Circuit(ctx, k, seed=k + 160, shape="many")
+    assert c.key.proof_len == len(c.oracle_proof(c.advice, c.blinds(4)))
+    bl = c.blinds(5)
+    proof = mzk.create_proofs(ctx, [(c.key, c.advice, bl)], flags=mzk.PROVE_SELF_CHECK)[0]
+    assert proof == c.oracle_proof(c.advice, bl)
+    assert c.verify(proof)
+    both = mzk.create_proofs(ctx, [(c.key, c.advice, c.blinds(6)), (c.key, c.advice, bl)])
+    assert both[1] == proof and c.verify(both[0])
+
+
 @pytest.mark.parametrize("k", [5, 9])
 def test_expression_lookup_inputs_equal_oracle(ctx, k):
     """Lookup inputs that are expressions (a(wX) and d - a^2 + a into the

@@ -269,6 +269,24 @@ def test_parallel_lookup_proofs_verify():
         OP.create_proof(key, worse, bl)
 
 
+def test_five_lookups_and_five_trashcans_verify():
+    """Five lookups (with and without selectors, a tuple) and five
+    trashcans: the proof verifies and a tampered evaluation is rejected."""
+    k = 6
+    c = OP.many_circuit(k)
+    assert OP.blinding_factors(c) == 3 + 5 + 5 + 3
+    fixed, mapping, adv = OP.many_instance(k, 25)
+    s = O.rand_fr(59, 1)[0]
+    g, lag, dl, ddl = O.srs_setup(s, k)
+    key = OP.keygen(c, fixed, mapping, {"g": g, "lagrange": lag, "delta": dl, "double_delta": ddl}, b"many")
+    bl = [OP.to_int(v) for v in O.rand_fr(69, OP.blind_count(c))]
+    proof = OP.create_proof(key, adv, bl)
+    assert OP.verify(key, proof, OP.to_int(s))
+    bad = bytearray(proof)
+    bad[-48 * 2 - 32 * 3] ^= 1                                   # a q evaluation
+    assert not OP.verify(key, bytes(bad), OP.to_int(s))
+
+
 def test_expression_lookup_inputs_verify():
     """Lookup inputs that are expressions (a(wX), d - a^2 + a, a * a): their
     degree sets the inputs per helper (two at degree 5 for a degree-2 input),
