@@ -49,9 +49,12 @@ __device__ __forceinline__ Fr root_pow(const Fr* __restrict__ tlo, const Fr* __r
     return fr_mul(thi[e >> kLoBits], lo);
 }
 
+// transforms of one batched launch (blockIdx.y picks one)
+constexpr uint32_t kNttBatch = 64;
+
 struct PassArgs {
-    const Fr* in;
-    Fr* out;
+    const Fr* in[kNttBatch];
+    Fr* out[kNttBatch];
     const Fr* tlo;
     const Fr* thi;
     const Fr* ptw;  // the pass's twiddle table (Domain::pass_tw), or null: formed from tlo x thi
@@ -176,7 +179,7 @@ __global__ void __launch_bounds__(kNttThreads, 2) k_ntt_dif_pass(PassArgs a) {
         const uint32_t c = c0 + (b << cstep_log);
         vidx[q] = ((c >> log_m) << a.log_s) + (m << log_m) + (c & ((1u << log_m) - 1));
         v[q] = fr_zero();
-        if (e < tile && vidx[q] < a.n_real) v[q] = a.in[vidx[q]];
+        if (e < tile && vidx[q] < a.n_real) v[q] = a.in[blockIdx.y][vidx[q]];
     }
 #pragma unroll
     for (int q = 0; q < kPer; q++) {
@@ -232,10 +235,10 @@ __global__ void __launch_bounds__(kNttThreads, 2) k_ntt_dif_pass(PassArgs a) {
                     const uint32_t r = o % 3;
                     v = fr_mul(v, a.post[r]);
                 }
-                a.out[o] = v;
+                a.out[blockIdx.y][o] = v;
             }
         } else {
-            a.out[idx] = v;
+            a.out[blockIdx.y][idx] = v;
         }
     }
 }
@@ -443,57 +446,100 @@ Status domain_create(Context* ctx, uint32_t j, uint32_t k, Domain** out) {
     return OK;
 }
 
-// The DIF passes of one transform over 2^log_n elements with root table
-// `root` (0..3), ending in natural order.  The first pass reads `in`
-// (n_real elements, optional coset scaling).  The last pass writes every
-// element to its bit-reversed position (times post[i % 3] when post is given,
-// only positions < m_out).  Since that pass's writes cross blocks, it reads
-// from the scratch buffer the earlier passes wrote, so `in` and `out` may be
-// the same buffer.  A transform of one tile (log_n <= 11) is one block,
-// which reads all before it writes.
-static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n, const Fr* in, Fr* out,
-                         uint32_t n_real, bool coset, const host::Fr4* post, uint32_t m_out, cudaStream_t st) {
+// The DIF passes of T transforms over 2^log_n elements each with root table
+// `root` (0..3), ending in natural order, up to kNttBatch transforms per
+// launch (blockIdx.y: the transform; every transform has its own slice of
+// the scratch).  The first pass reads in[t] (n_real elements, optional coset
+// scaling).  The last pass writes every element to its bit-reversed position
+// (times post[i % 3] when post is given, only positions < m_out).  Since
+// that pass's writes cross blocks, it reads from the scratch the earlier
+// passes wrote, so in[t] and out[t] may be the same buffer.  A transform of
+// one tile (log_n <= 11) is one block, which reads all before it writes.
+static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n, const Fr* const* in,
+                         Fr* const* out, uint32_t T, uint32_t n_real, bool coset, const host::Fr4* post,
+                         uint32_t m_out, cudaStream_t st) {
     const uint32_t N = 1u << log_n;
     const uint32_t tile = std::min(kTile, N);
     const std::vector<uint32_t> logs = pass_logs(log_n, split_of(ctx, log_n));
     const uint32_t passes = (uint32_t)logs.size();
+    // transforms per launch: at most kNttBatch and 2^25 elements of scratch
+    // (large transforms fill the GPU alone)
+    const uint32_t TB = std::min({T, kNttBatch, std::max(1u, (1u << 25) >> log_n)});
     Fr* tmp = nullptr;
     if (passes > 1) {
         void* p;
-        MZK_TRY(ctx->ensure("ntt_tmp", (size_t)N * sizeof(Fr), &p));
+        MZK_TRY(ctx->ensure("ntt_tmp", (size_t)TB * N * sizeof(Fr), &p));
         tmp = static_cast<Fr*>(p);
     }
-    uint32_t log_s = log_n;
-    for (uint32_t p = 0; p < passes; p++) {
-        const uint32_t log_r = logs[p];
-        const bool last = p + 1 == passes;
-        PassArgs a;
-        a.in = p == 0 ? in : tmp;
-        a.out = last ? out : tmp;
-        a.tlo = d->lo[root];
-        a.thi = d->hi[root];
-        a.ptw = last ? nullptr : pass_twiddles(ctx, d, root, log_n, log_s, log_r, st);
-        a.log_n = log_n;
-        a.log_s = log_s;
-        a.log_r = log_r;
-        a.n_real = p == 0 ? n_real : N;
-        a.use_pre = (p == 0 && coset) ? 1 : 0;
-        a.twiddle_after = last ? 0 : 1;
-        a.pre[0] = to_dev(host::fr_one());
-        a.pre[1] = to_dev(d->zeta);
-        a.pre[2] = to_dev(d->zeta2);
-        a.bitrev_out = last ? 1 : 0;
-        a.use_post = post ? 1 : 0;
-        a.m_out = m_out;
-        for (int i = 0; i < 3; i++) a.post[i] = to_dev(post ? post[i] : host::fr_one());
-        const size_t smem = (size_t)tile * sizeof(Fr) + (size_t)(1u << log_r) / 2 * sizeof(Fr);
-        k_ntt_dif_pass<<<N / tile, kNttThreads, smem, st>>>(a);
-        MZK_LAUNCH_CHECK(ctx);
-        log_s -= log_r;
+    for (uint32_t t0 = 0; t0 < T; t0 += TB) {
+        const uint32_t tb = std::min(TB, T - t0);
+        uint32_t log_s = log_n;
+        for (uint32_t p = 0; p < passes; p++) {
+            const uint32_t log_r = logs[p];
+            const bool last = p + 1 == passes;
+            PassArgs a;
+            for (uint32_t t = 0; t < tb; t++) {
+                a.in[t] = p == 0 ? in[t0 + t] : tmp + (size_t)t * N;
+                a.out[t] = last ? out[t0 + t] : tmp + (size_t)t * N;
+            }
+            a.tlo = d->lo[root];
+            a.thi = d->hi[root];
+            a.ptw = last ? nullptr : pass_twiddles(ctx, d, root, log_n, log_s, log_r, st);
+            a.log_n = log_n;
+            a.log_s = log_s;
+            a.log_r = log_r;
+            a.n_real = p == 0 ? n_real : N;
+            a.use_pre = (p == 0 && coset) ? 1 : 0;
+            a.twiddle_after = last ? 0 : 1;
+            a.pre[0] = to_dev(host::fr_one());
+            a.pre[1] = to_dev(d->zeta);
+            a.pre[2] = to_dev(d->zeta2);
+            a.bitrev_out = last ? 1 : 0;
+            a.use_post = post ? 1 : 0;
+            a.m_out = m_out;
+            for (int i = 0; i < 3; i++) a.post[i] = to_dev(post ? post[i] : host::fr_one());
+            const size_t smem = (size_t)tile * sizeof(Fr) + (size_t)(1u << log_r) / 2 * sizeof(Fr);
+            k_ntt_dif_pass<<<dim3(N / tile, tb), kNttThreads, smem, st>>>(a);
+            MZK_LAUNCH_CHECK(ctx);
+            log_s -= log_r;
+        }
     }
     return OK;
 }
 
+static Status dif_passes(Context* ctx, const Domain* d, int root, uint32_t log_n, const Fr* in, Fr* out,
+                         uint32_t n_real, bool coset, const host::Fr4* post, uint32_t m_out, cudaStream_t st) {
+    return dif_passes(ctx, d, root, log_n, &in, &out, 1, n_real, coset, post, m_out, st);
+}
+
+// The same domain operation on T inputs of equal size, their passes
+// launched together (the transforms of many polynomials of one domain).
+Status domain_op_batch(Context* ctx, const Domain* d, int op, const void* const* ins, void* const* outs, uint32_t T,
+                       cudaStream_t st) {
+    if (T == 0) return OK;
+    const uint32_t k = d->k, ek = d->ext_k;
+    const uint32_t n = 1u << k, en = 1u << ek;
+    const Fr* const* in = reinterpret_cast<const Fr* const*>(ins);
+    Fr* const* out = reinterpret_cast<Fr* const*>(outs);
+    switch (op) {
+        case OP_COEFF_TO_LAGRANGE:
+            return dif_passes(ctx, d, 0, k, in, out, T, n, false, nullptr, n, st);
+        case OP_LAGRANGE_TO_COEFF: {
+            const host::Fr4 post[3] = {d->ifft_div, d->ifft_div, d->ifft_div};
+            return dif_passes(ctx, d, 1, k, in, out, T, n, false, post, n, st);
+        }
+        case OP_COEFF_TO_EXTENDED:
+            return dif_passes(ctx, d, 2, ek, in, out, T, n, true, nullptr, en, st);
+        case OP_EXTENDED_TO_COEFF: {
+            const host::Fr4 post[3] = {d->ext_ifft_div, host::fr_mul(d->ext_ifft_div, d->zeta2),
+                                       host::fr_mul(d->ext_ifft_div, d->zeta)};
+            return dif_passes(ctx, d, 3, ek, in, out, T, en, false, post, en, st);
+        }
+        default:
+            set_error("domain: batched operation must be C2L, L2C, C2E or E2C");
+            return ERR_ARG;
+    }
+}
 
 Status domain_op_device(Context* ctx, const Domain* d, int op, const void* d_in, void* d_out, cudaStream_t st) {
     const uint32_t k = d->k, ek = d->ext_k;

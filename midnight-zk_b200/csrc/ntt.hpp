@@ -52,6 +52,10 @@ struct Domain {
 Status domain_create(Context* ctx, uint32_t j, uint32_t k, Domain** out);
 // d_in / d_out device pointers (may alias for the in-place operations)
 Status domain_op_device(Context* ctx, const Domain* d, int op, const void* d_in, void* d_out, cudaStream_t st);
+// the same operation (C2L, L2C, C2E or E2C) on T inputs of the domain, up to
+// 64 transforms per launch of each pass
+Status domain_op_batch(Context* ctx, const Domain* d, int op, const void* const* ins, void* const* outs, uint32_t T,
+                       cudaStream_t st);
 size_t domain_op_in_len(const Domain* d, int op);
 size_t domain_op_out_len(const Domain* d, int op);
 

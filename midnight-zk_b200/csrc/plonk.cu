@@ -2033,11 +2033,11 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
     phase_done(3);
     // ---- 4. cosets, quotient limbs, x -------------------------------------
     items.clear();
-    for (auto& p : ps) {
+    // every polynomial of a proof that the quotient reads on the extended
+    // coset: Lagrange -> coefficients -> coset
+    auto ntt_lists = [](const FsProof& p, std::vector<const void*>& lag, std::vector<Fr*>& co,
+                        std::vector<Fr*>& ex) {
         const PlonkKey* k = p.key;
-        const Domain* d = k->dom;
-        std::vector<const void*> lag;
-        std::vector<Fr*> co, ex;
         for (uint32_t i = 0; i < k->n_advice; i++) {
             lag.push_back(p.adv_lag[i]);
             co.push_back(p.adv_coeff[i]);
@@ -2068,8 +2068,41 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             co.push_back(p.h_coeff[h]);
             ex.push_back(p.h_ext[h]);
         }
-        MZK_TRY(ntt_sequence(ctx, d, lag.data(), co.data(), ex.data(), (int)lag.size(),
-                             !(flags & MZK_PROVE_NO_GRAPHS), st));
+    };
+    // the transforms of all proofs of one domain together, one launch per
+    // pass for up to 64 polynomials (MZK_PROVE_NO_GRAPHS: proof by proof,
+    // kernel by kernel, the plain form)
+    const bool batched_ntt = !(flags & MZK_PROVE_NO_GRAPHS);
+    if (batched_ntt) {
+        std::map<const Domain*, std::array<std::vector<void*>, 3>> by_dom;
+        for (auto& p : ps) {
+            std::vector<const void*> lag;
+            std::vector<Fr*> co, ex;
+            ntt_lists(p, lag, co, ex);
+            auto& g = by_dom[p.key->dom];
+            for (size_t i = 0; i < lag.size(); i++) {
+                g[0].push_back(const_cast<void*>(lag[i]));
+                g[1].push_back(co[i]);
+                g[2].push_back(ex[i]);
+            }
+        }
+        for (auto& kv : by_dom) {
+            auto& g = kv.second;
+            MZK_TRY(domain_op_batch(ctx, kv.first, OP_LAGRANGE_TO_COEFF, const_cast<const void* const*>(g[0].data()),
+                                    g[1].data(), (uint32_t)g[0].size(), st));
+            MZK_TRY(domain_op_batch(ctx, kv.first, OP_COEFF_TO_EXTENDED, const_cast<const void* const*>(g[1].data()),
+                                    g[2].data(), (uint32_t)g[1].size(), st));
+        }
+    }
+    for (auto& p : ps) {
+        const PlonkKey* k = p.key;
+        const Domain* d = k->dom;
+        if (!batched_ntt) {
+            std::vector<const void*> lag;
+            std::vector<Fr*> co, ex;
+            ntt_lists(p, lag, co, ex);
+            MZK_TRY(ntt_sequence(ctx, d, lag.data(), co.data(), ex.data(), (int)lag.size(), false, st));
+        }
         std::vector<const uint64_t*> adv(k->n_advice), fixed(k->n_fixed), sig(k->n_perm), zs(k->n_sets),
             inst(k->n_instance);
         for (uint32_t i = 0; i < k->n_instance; i++) inst[i] = reinterpret_cast<const uint64_t*>(p.inst_ext[i]);
