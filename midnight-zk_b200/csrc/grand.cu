@@ -320,6 +320,90 @@ Status linrec_suffix(Context* ctx, const Fr* c, Fr* y, uint64_t n, const host::F
     return OK;
 }
 
+// The same recurrences for T tasks of one length n, blockIdx.y picking the
+// task: its input, output and factor, and its slice of the chunk values.
+constexpr uint32_t kRecBatch = 32;
+struct RecTasks {
+    const Fr* c[kRecBatch];
+    Fr* y[kRecBatch];
+    Fr k[kRecBatch];
+};
+__global__ void __launch_bounds__(kThreads) k_rec_local_batch(const RecTasks t, uint64_t n, Fr* __restrict__ lows,
+                                                              uint64_t chunks, uint32_t K) {
+    const uint32_t j = blockIdx.y;
+    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t lo = c * K;
+    if (lo >= n) return;
+    const uint64_t hi = min(n, lo + K);
+    const Fr k = t.k[j];
+    const Fr* __restrict__ in = t.c[j];
+    Fr* __restrict__ y = t.y[j];
+    Fr acc = fr_zero();
+    for (uint64_t i = hi; i-- > lo;) {
+        acc = fr_add(in[i], fr_mul(k, acc));
+        y[i] = acc;
+    }
+    lows[2 * chunks * j + c] = acc;
+}
+__global__ void __launch_bounds__(kThreads) k_rec_fix_batch(const RecTasks t, uint64_t n, const Fr* __restrict__ lows,
+                                                            uint64_t chunks, uint32_t K) {
+    const uint32_t j = blockIdx.y;
+    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c + 1 >= chunks) return;  // the top chunk has a zero carry-in
+    const uint64_t lo = c * K, hi = lo + K;
+    const Fr k = t.k[j];
+    const Fr carry = lows[2 * chunks * j + chunks + c + 1];  // Y of the chunk above
+    Fr* __restrict__ y = t.y[j];
+    Fr pw = k;
+    for (uint64_t i = hi; i-- > lo;) {
+        y[i] = fr_add(y[i], fr_mul(pw, carry));
+        pw = fr_mul(pw, k);
+    }
+}
+
+// linrec_suffix for T tasks of one length: y[j] (n) from c[j] (n) with
+// factor k[j]; the chunk values of every level sit in one buffer per level
+// (task j: its lows L_j then its starts Y_j)
+Status linrec_suffix_batch(Context* ctx, const Fr* const* c, Fr* const* y, const host::Fr4* k, uint32_t T, uint64_t n,
+                           cudaStream_t st, int depth = 0) {
+    if (n == 0 || T == 0) return OK;
+    uint32_t K = kRecChunkMax;
+    const uint64_t want_threads = (uint64_t)ctx->num_sms * kThreads * 2;
+    while (K > kRecChunkMin && n * T / K < want_threads && n > (uint64_t)kRecChunkMax * kRecChunkMax) K >>= 1;
+    const uint64_t chunks = (n + K - 1) / K;
+    for (uint32_t j0 = 0; j0 < T; j0 += kRecBatch) {
+        const uint32_t tb = std::min(kRecBatch, T - j0);
+        void* lows;
+        MZK_TRY(ctx->ensure(("grand_recb_" + std::to_string(depth)).c_str(), 2 * chunks * tb * sizeof(Fr), &lows));
+        Fr* L = (Fr*)lows;
+        RecTasks t;
+        for (uint32_t j = 0; j < tb; j++) {
+            t.c[j] = c[j0 + j];
+            t.y[j] = y[j0 + j];
+            t.k[j] = to_dev(k[j0 + j]);
+        }
+        const dim3 grid((uint32_t)((chunks + kThreads - 1) / kThreads), tb);
+        k_rec_local_batch<<<grid, kThreads, 0, st>>>(t, n, L, chunks, K);
+        MZK_LAUNCH_CHECK(ctx);
+        if (chunks > 1) {
+            // the chunk starts: the same recurrence over the lows with k^K
+            std::vector<const Fr*> lc(tb);
+            std::vector<Fr*> ly(tb);
+            std::vector<host::Fr4> kk(tb);
+            for (uint32_t j = 0; j < tb; j++) {
+                lc[j] = L + 2 * chunks * j;
+                ly[j] = L + 2 * chunks * j + chunks;
+                kk[j] = k[j0 + j];
+                for (uint32_t b = 1; b < K; b <<= 1) kk[j] = host::fr_mul(kk[j], kk[j]);
+            }
+            MZK_TRY(linrec_suffix_batch(ctx, lc.data(), ly.data(), kk.data(), tb, chunks, st, depth + 1));
+            k_rec_fix_batch<<<grid, kThreads, 0, st>>>(t, n, L, chunks, K);
+            MZK_LAUNCH_CHECK(ctx);
+        }
+    }
+    return OK;
+}
+
 // ---- permutation argument ----
 struct PermCols {
     const Fr* values[kMaxPermSetCols];
@@ -600,6 +684,14 @@ Status kate_division_device(Context* ctx, const void* a, uint64_t n, const uint6
     if (n < 2) return OK;
     // q_i = a_{i+1} + b q_{i+1}, q_{n-1} = 0
     return linrec_suffix(ctx, static_cast<const Fr*>(a) + 1, static_cast<Fr*>(q), n - 1, to_host(b), st);
+}
+
+Status kate_division_batch(Context* ctx, const void* const* a, void* const* q, const host::Fr4* b, uint32_t T,
+                           uint64_t n, cudaStream_t st) {
+    if (n < 2 || T == 0) return OK;
+    std::vector<const Fr*> c(T);
+    for (uint32_t j = 0; j < T; j++) c[j] = static_cast<const Fr*>(a[j]) + 1;
+    return linrec_suffix_batch(ctx, c.data(), reinterpret_cast<Fr* const*>(q), b, T, n - 1, st);
 }
 
 }  // namespace mzk

@@ -17,6 +17,10 @@ Status eval_polynomial_device(Context* ctx, const void* poly, uint64_t n, const 
                               cudaStream_t st);
 // q (n - 1) = a (n) / (X - b) (utils/arithmetic.rs:106-125)
 Status kate_division_device(Context* ctx, const void* a, uint64_t n, const uint64_t b[4], void* q, cudaStream_t st);
+// the same for T polynomials of one length n: q[j] = a[j] / (X - b[j]), their
+// recurrences launched together (a, q: device pointers; b: host)
+Status kate_division_batch(Context* ctx, const void* const* a, void* const* q, const host::Fr4* b, uint32_t T,
+                           uint64_t n, cudaStream_t st);
 // kzg/mod.rs:125-147 poly_inner_product over m device polynomials (host
 // tables of pointers, lengths and scalars)
 Status poly_inner_product_device(Context* ctx, const uint64_t* const* polys, const uint64_t* lens, uint32_t m,

@@ -38,6 +38,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/mzk.h"
@@ -1320,6 +1321,7 @@ struct FsProof {
     host::Transcript tr;
     Fr4 theta, beta, gamma, trash, y, x, xn, x1, x2, x3, x4;
     std::vector<Fr*> adv_lag, adv_coeff, adv_ext, z_lag, z_delta, z_coeff, z_ext, q, fdiv;
+    std::vector<Fr*> qt;  // per point set: the intermediate quotient of its divisions
     std::vector<Fr*> inst_lag, inst_coeff, inst_ext;  // instance columns (zero past their values)
     std::vector<Fr*> trash_lag, trash_coeff, trash_ext;  // trash columns
     // per lookup: multiplicities and aggregator; per helper (Lookup::h0 + chunk): helper
@@ -1330,8 +1332,7 @@ struct FsProof {
     // the key's lookup input expressions over the Lagrange rows and the extended coset
     std::vector<Fr*> e_lag, e_ext;
     std::vector<uint32_t*> counts;
-    Fr *limbs = nullptr, *lin = nullptr, *f = nullptr, *fin = nullptr, *pi = nullptr, *tmp_a = nullptr,
-       *tmp_b = nullptr;
+    Fr *limbs = nullptr, *lin = nullptr, *f = nullptr, *fin = nullptr, *pi = nullptr;
     Fr* d_blinds = nullptr;
     uint64_t f_len = 0;
     Fr4 lin_c = {};  // the linearization's constant term C (when the identities were evaluated)
@@ -1354,7 +1355,7 @@ size_t proof_scratch_elems(const PlonkKey* k) {
     for (const auto& lk : k->lookups) counts += (lk.n_uniq + 7) / 8 + (lk.width > 1 ? (lk.n_inputs + 1) * n : 0);
     return (A + k->n_instance + k->trash.size()) * (2 * n + E) + S * (3 * n + E) +
            L * ((3 * n + E) + (3 * n + E)) + k->n_helpers * (2 * n + E) + k->lk_exprs.size() * (n + E) +
-           k->qdeg * n + (4 + 2 * O + 2) * n + k->n_blinds + counts;
+           k->qdeg * n + (4 + 3 * O) * n + k->n_blinds + counts;
 }
 
 Status eval_many(Context* ctx, const std::vector<EvalTask>& in, std::vector<Fr4>& results, cudaStream_t st) {
@@ -1777,8 +1778,8 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         for (size_t s = 0; s < k->open_sets.size(); s++) {
             p.q.push_back(take(n));
             p.fdiv.push_back(take(n));
+            p.qt.push_back(take(n));
         }
-        p.tmp_a = take(n), p.tmp_b = take(n);
         p.d_blinds = take(k->n_blinds);
         for (const auto& lk : k->lookups) p.counts.push_back(reinterpret_cast<uint32_t*>(take((lk.n_uniq + 7) / 8)));
         carve = start + proof_scratch_elems(k) + 8;
@@ -2298,6 +2299,36 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             }
         }
         MZK_TRY(lincomb_many(ctx, qs, st));
+        // each set's q divided by (X - x_r) for its points in turn
+        // (kzg/mod.rs:219-240): stage r of every set of every proof at once,
+        // grouped by length n - r; the divisions of a set alternate between
+        // its fdiv and qt so that the last one lands in fdiv
+        size_t max_rots = 0;
+        for (auto& p : ps)
+            for (auto& os : p.key->open_sets) max_rots = std::max(max_rots, os.rots.size());
+        auto div_out = [](FsProof& p, size_t s, size_t r) {
+            const size_t R = p.key->open_sets[s].rots.size();
+            return (R - 1 - r) % 2 == 0 ? p.fdiv[s] : p.qt[s];
+        };
+        for (size_t r = 0; r < max_rots; r++) {
+            std::map<uint64_t, std::tuple<std::vector<const void*>, std::vector<void*>, std::vector<Fr4>>> by_len;
+            for (auto& p : ps) {
+                const PlonkKey* k = p.key;
+                for (size_t s = 0; s < k->open_sets.size(); s++) {
+                    const auto& rots = k->open_sets[s].rots;
+                    if (r >= rots.size()) continue;
+                    auto& g = by_len[(uint64_t)k->n - r];
+                    std::get<0>(g).push_back(r == 0 ? p.q[s] : div_out(p, s, r - 1));
+                    std::get<1>(g).push_back(div_out(p, s, r));
+                    std::get<2>(g).push_back(fr_rot(k->dom, p.x, rots[r]));
+                }
+            }
+            for (auto& kv : by_len) {
+                auto& g = kv.second;
+                MZK_TRY(kate_division_batch(ctx, std::get<0>(g).data(), std::get<1>(g).data(), std::get<2>(g).data(),
+                                            (uint32_t)std::get<0>(g).size(), kv.first, st));
+            }
+        }
         std::vector<LinSpec> fs;
         items.clear();
         for (auto& p : ps) {
@@ -2305,16 +2336,7 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
             LinSpec ls{p.f, 0, {}};
             Fr4 pw = host::fr_one();
             for (size_t s = 0; s < k->open_sets.size(); s++) {
-                const Fr* src = p.q[s];
-                uint64_t len = k->n;
-                const auto& rots = k->open_sets[s].rots;
-                for (size_t r = 0; r < rots.size(); r++) {
-                    Fr* dst = r + 1 == rots.size() ? p.fdiv[s] : (src == p.tmp_a ? p.tmp_b : p.tmp_a);
-                    const Fr4 pt = fr_rot(k->dom, p.x, rots[r]);
-                    MZK_TRY(kate_division_device(ctx, src, len, pt.l, dst, st));
-                    src = dst;
-                    len -= 1;
-                }
+                const uint64_t len = k->n - k->open_sets[s].rots.size();
                 ls.terms.push_back({p.fdiv[s], len, to_dev(pw)});
                 ls.len = std::max<uint64_t>(ls.len, len);
                 pw = fr_mul(pw, p.x2);
@@ -2377,9 +2399,18 @@ Status create_proofs(Context* ctx, const mzk_proof_request* reqs, size_t count, 
         }
         MZK_TRY(lincomb_many(ctx, fins, st));
         items.clear();
+        std::map<uint64_t, std::tuple<std::vector<const void*>, std::vector<void*>, std::vector<Fr4>>> by_len;
         for (auto& p : ps) {
-            MZK_TRY(kate_division_device(ctx, p.fin, p.key->n, p.x3.l, p.pi, st));
+            auto& g = by_len[p.key->n];
+            std::get<0>(g).push_back(p.fin);
+            std::get<1>(g).push_back(p.pi);
+            std::get<2>(g).push_back(p.x3);
             items.push_back({p.pi, p.key->srs.off_g, (uint64_t)p.key->n - 1});
+        }
+        for (auto& kv : by_len) {
+            auto& g = kv.second;
+            MZK_TRY(kate_division_batch(ctx, std::get<0>(g).data(), std::get<1>(g).data(), std::get<2>(g).data(),
+                                        (uint32_t)std::get<0>(g).size(), kv.first, st));
         }
         MZK_TRY(msm());
         for (size_t j = 0; j < count; j++) {
