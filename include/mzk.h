@@ -214,6 +214,14 @@ int mzk_domain_constant(const mzk_domain *d, int which, int idx, uint64_t out[4]
 int mzk_domain_op(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *in, uint64_t *out);
 /* DEVICE buffers; in == out allowed for ops 0, 1, 3, 5; op 4 overwrites in. */
 int mzk_domain_op_device(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *d_in, uint64_t *d_out);
+/* The same operation (0-3) on `count` polynomials of the domain: d_in[i] ->
+ * d_out[i] (HOST arrays of DEVICE pointers; d_in[i] == d_out[i] allowed),
+ * the transforms' passes launched together, up to 64 polynomials per launch,
+ * where a small domain alone fills few of the GPU's blocks (the evaluator's
+ * per-polynomial coeff_to_extended and lagrange_to_coeff calls,
+ * evaluation.rs:846-960, prover.rs:634-771).  Same results as one call each. */
+int mzk_domain_op_batch_device(mzk_ctx *ctx, mzk_domain *d, int op, const uint64_t *const *d_in,
+                               uint64_t *const *d_out, size_t count);
 
 /* ---- quotient evaluation (proofs/src/plonk/evaluation.rs:818-1114) ------ */
 /* Custom gates of any circuit as the reference flattens them

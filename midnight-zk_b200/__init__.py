@@ -81,6 +81,7 @@ SIGNATURES = {
     "mzk_domain_constant": (_i32, [_vp, _i32, _i32, _u64p]),
     "mzk_domain_op": (_i32, [_vp, _vp, _i32, _u64p, _u64p]),
     "mzk_domain_op_device": (_i32, [_vp, _vp, _i32, _vp, _vp]),
+    "mzk_domain_op_batch_device": (_i32, [_vp, _vp, _i32, _vp, _vp, _sz]),
     "mzk_quotient_eval_device": (_i32, [_vp, _vp, ctypes.c_void_p, _i32, _vp]),
     "mzk_compute_h_poly_device": (_i32, [_vp, _vp, ctypes.c_void_p, _vp, _sz, _u64p, _u64p, _vp]),
     "mzk_prove_core_device": (_i32, [_vp, _vp, ctypes.c_void_p, ctypes.c_void_p, _sz, _u32, _u64p]),
@@ -845,6 +846,15 @@ class EvaluationDomain:
         di = d_in.ptr if isinstance(d_in, DeviceBuffer) else int(d_in)
         do = d_out.ptr if isinstance(d_out, DeviceBuffer) else int(d_out)
         _check(lib().mzk_domain_op_device(self.ctx.h, self.h, self.OPS[name], di, do))
+
+    def op_batch_device(self, name, d_ins, d_outs):
+        """The same operation on many device buffers, launched together."""
+        ptr = lambda b: b.ptr if isinstance(b, DeviceBuffer) else int(b)
+        ins = (ctypes.c_void_p * max(1, len(d_ins)))(*[ptr(b) for b in d_ins])
+        outs = (ctypes.c_void_p * max(1, len(d_outs)))(*[ptr(b) for b in d_outs])
+        if len(d_ins) != len(d_outs):
+            raise MzkError(1, "domain op batch: inputs and outputs differ in number")
+        _check(lib().mzk_domain_op_batch_device(self.ctx.h, self.h, self.OPS[name], ins, outs, len(d_ins)))
 
 
 class ProvingServer:

@@ -637,6 +637,29 @@ int mzk_domain_op_device(mzk_ctx* ctx, mzk_domain* d, int op, const uint64_t* d_
     return mzk::OK;
 }
 
+int mzk_domain_op_batch_device(mzk_ctx* ctx, mzk_domain* d, int op, const uint64_t* const* d_in,
+                               uint64_t* const* d_out, size_t count) {
+    if (int s = check_ctx(ctx)) return s;
+    if (!d || (count && (!d_in || !d_out))) {
+        mzk::set_error("domain op batch: null argument");
+        return mzk::ERR_ARG;
+    }
+    if (op < mzk::OP_COEFF_TO_LAGRANGE || op > mzk::OP_EXTENDED_TO_COEFF || count > 0xffffffffu) {
+        mzk::set_error("domain op batch: the operation must be 0-3");
+        return mzk::ERR_ARG;
+    }
+    for (size_t i = 0; i < count; i++)
+        if (!d_in[i] || !d_out[i]) {
+            mzk::set_error("domain op batch: null polynomial");
+            return mzk::ERR_ARG;
+        }
+    Guard g(ctx);
+    MZK_TRY(mzk::domain_op_batch(&ctx->impl, d->impl, op, reinterpret_cast<const void* const*>(d_in),
+                                 reinterpret_cast<void* const*>(d_out), (uint32_t)count, ctx->impl.stream));
+    MZK_CUDA_CHECK(cudaStreamSynchronize(ctx->impl.stream));
+    return mzk::OK;
+}
+
 int mzk_domain_op(mzk_ctx* ctx, mzk_domain* d, int op, const uint64_t* in, uint64_t* out) {
     if (int s = check_ctx(ctx)) return s;
     if (!d || !in || !out) {

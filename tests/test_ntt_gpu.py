@@ -145,3 +145,34 @@ def test_ntt_2_24_all_ops_match_oracle_in_full(ctx):
     e = de.download((en, 4))
     g.op_device("extended_to_coeff", de, out)
     assert np.array_equal(out.download((en, 4)), o.extended_to_coeff(e))
+
+
+@pytest.mark.parametrize("k,count", [(10, 70), (14, 5), (18, 3)])
+def test_batched_domain_ops_equal_single_calls(ctx, k, count):
+    """mzk_domain_op_batch_device: every operation 0-3 on `count` device
+    polynomials (70: two launches of up to 64 at k = 10) equals one
+    mzk_domain_op_device call each, in place as well, and the batch of
+    coefficient-to-Lagrange transforms equals the oracle's FFT."""
+    g = mzk.EvaluationDomain(ctx, 5, k)
+    n, en = g.n, g.extended_len
+    sizes = {"coeff_to_lagrange": (n, n), "lagrange_to_coeff": (n, n), "coeff_to_extended": (n, en),
+             "extended_to_coeff": (en, en)}
+    for name, (li, lo) in sizes.items():
+        ins = [ctx.gen_rand_fr(0x5000 + 97 * i + li, li) for i in range(count)]
+        outs = [ctx.alloc(lo * 32) for _ in range(count)]
+        g.op_batch_device(name, ins, outs)
+        for i in (0, count // 2, count - 1):
+            want = ctx.alloc(lo * 32)
+            g.op_device(name, ins[i], want)
+            assert np.array_equal(outs[i].download((lo, 4)), want.download((lo, 4))), (name, i)
+        if li == lo:  # in place
+            g.op_batch_device(name, ins, ins)
+            assert all(np.array_equal(ins[i].download((li, 4)), outs[i].download((lo, 4))) for i in (0, count - 1))
+    if k == 10:
+        a = ctx.gen_rand_fr(77, n)
+        out = ctx.alloc(n * 32)
+        g.op_batch_device("coeff_to_lagrange", [a], [out])
+        assert np.array_equal(out.download((n, 4)), O.Domain(5, k).coeff_to_lagrange(a.download((n, 4))))
+    with pytest.raises(mzk.MzkError):
+        g.op_batch_device("extended_to_lagrange", [a if k == 10 else ctx.alloc(en * 32)], [ctx.alloc(n * 32)])
+    g.close()
