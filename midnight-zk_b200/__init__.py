@@ -980,7 +980,9 @@ def prover_table_width(k):
     at 2^k rows on a B200 (config-3 circuit, 8 proofs per call; k = 18: no
     table 33.0 ms per proof, c = 15 / 16 / 17 / 18: 28.4 / 27.5 / 27.9 / 29.2
     ms; k = 20, 2 per call: no table 121.7, c = 17 / 18 / 19 / 20: 92.5 / 94.9
-    / 99.6 / 113.8 ms).  Each MSM of
+    / 99.6 / 113.8 ms; 16 per call, k = 14: c = 11 / 12 / 13 / 14 / 16: 52.9 /
+    52.4 / 52.0 / 52.5 / 56.6 ms per call, k = 16: c = 14 / 15 / 16 / 17 / 18:
+    124.1 / 123.6 / 122.7 / 131.0 / 146.4 ms).  Each MSM of
     2^k points then adds ceil(255 / c) + 1 table rows of points into one window
     of 2^(c-1) buckets: wider tables mean fewer entries per point but more
     buckets to reduce, and the best width grows with the point count."""
