@@ -597,7 +597,9 @@ typedef struct {
  * logup helper / aggregator, trash challenge, y; quotient limbs, x;
  * evaluations; multi_open with f, x3, the q evaluations, x4 and pi,
  * kzg/mod.rs:110-289) runs for every proof before the next, its MSMs as one
- * batched MSM (or, with MZK_PROVE_MSM_PER_CALL, one call each).  Flags:
+ * batched MSM (or, with MZK_PROVE_MSM_PER_CALL, one call each); the
+ * polynomial transforms of all proofs of one domain run together (or, with
+ * MZK_PROVE_NO_GRAPHS, proof by proof, kernel by kernel).  Flags:
  * MZK_PROVE_MSM_PER_CALL, MZK_PROVE_NO_GRAPHS (above) and: */
 #define MZK_PROVE_SELF_CHECK 4u /* also check L'(x) = -C (prover.rs:404-408): an unsatisfied witness fails */
 int mzk_create_proofs(mzk_ctx *ctx, const mzk_proof_request *reqs, size_t count, uint32_t flags);
